@@ -1,0 +1,98 @@
+// xm_internal.h -- device data layout and kernel interface of libefdc_xm.
+//
+// Layout ("bricks"): the structured grid is cut into 32x8-cell tiles.  Tiles
+// holding at least one water cell are stored contiguously, ordered along a
+// Morton (Z) curve of their tile coordinates; inside a tile a cell's slot is
+// ty*32+tx.  Slot d = tile*256 + ty*32 + tx.  Tile 0 is a ghost tile (all
+// land).  Neighbours come from the slot position plus a 4-entry tile
+// neighbour table, so no per-cell index arrays are read in the solver: E/W
+// neighbours are adjacent words and N/S neighbours are the rows above and
+// below, which keeps every warp access a contiguous 32-cell row.
+//
+// Land slots (padding inside a tile, and tile 0) stand for EFDC+'s ghost cell
+// LC (a missing neighbour maps to LC, EFDC/cellmap.f90:80-134): they hold the
+// host's element-LC values and are never written by the solver.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace xm {
+
+constexpr int TX = 32;
+constexpr int TY = 8;
+constexpr int TILE = TX * TY;  // 256 slots per tile
+constexpr int NT = TILE;       // threads per CTA in the cell kernels
+constexpr int MT_MAX = 16;     // max harmonic constituents per call
+
+enum SlotKind : uint8_t { LAND = 0, WATER = 1, OPENBC = 2 };
+
+// Static per-slot model data (FP64).  Land slots hold element LC.
+struct DevStatic {
+  const int4 *tnbr;       // [ntile] (w, e, s, n) neighbour tiles, 0 = ghost tile
+  const uint8_t *kind;    // [nslot]
+  const int *lidx;        // [nslot] L of the slot, 0 for land
+  const double *dxyp, *dxyip, *dxiu, *dyiu, *dxiv, *dyiv, *dxyu, *dxyv;
+  const double *hruo, *hrvo, *subo, *svbo, *sbxo, *sbyo, *belv;
+  const double *rcx;      // RCX = RCY: 1 on water, 0 on ghosts (calpuv2c.f90:97-102)
+  const double *fsgzu, *fsgzv;  // 0.5/DXYU, 0.5/DXYV (calpuv2c.f90:111-116)
+};
+
+// Per-step state and work arrays (tile layout).
+struct DevState {
+  double *p, *hp, *h1p, *hu, *hv, *uhdye, *vhdxe, *sub, *svb, *sbx, *sby;
+  int *lmaskdry, *iscdry, *lopenbcdry, *natdry, *oldmask;
+  const double *fcaxe, *fcaye, *fxe, *fye, *tsx, *tsy, *tbx, *tby, *qsume;
+  double *uhe, *vhe, *hpi, *hui, *hvi, *qdwaste, *vdwaste;
+  double *uhdy1e, *vhdx1e, *sub1, *svb1, *fp1, *fuhdye, *fvhdxe;
+  double *fp, *cc, *cs, *cw, *ce, *cn;  // unscaled system (FP64)
+  // wet/dry scratch: decision codes and the new face switches of a sweep
+  int *wd_act;
+  double *sub_n, *svb_n, *sbx_n, *sby_n;
+  int *wasted;  // 1 where NDRYSTP volume wasting fired this step
+};
+
+// Scaled system and CG vectors.
+struct DevSystem {
+  double *ccc, *ccs, *ccw, *cce, *ccn, *fptmp;  // FP64 scaled coefficients, b
+  double *r, *pa, *pb, *ap;                      // FP64 CG vectors (p double-buffered)
+  float *ccc32, *ccs32, *ccw32, *cce32, *ccn32;  // FP32 copies (MIXED)
+  float *r32, *pa32, *pb32, *ap32, *x32;         // FP32 inner CG vectors
+};
+
+// Device-side control block of one solve.  Written by the "last CTA" of each
+// reduction; read by the host once per solve.
+struct Ctl {
+  double rpcg, alpha, beta, rsq, papcg;
+  double rsq64, rsq_target;       // MIXED: outer residual, inner target
+  double ccmnm_int, ccmnm_bc;     // min CC over interior / open-BC cells
+  int iter, done, status, parity; // status: enum efdc_xm_status
+  int inner_iter, outer, idone;   // MIXED bookkeeping (idone: inner solve finished)
+  int asym;                       // 1 if the scaled operator is not symmetric
+  int icordry;                    // wet/dry re-solve flag
+  int nneg, nnonfinite, nwasted;
+  unsigned int counter;           // last-CTA arrival counter
+  unsigned int counter2;
+};
+
+// Open-boundary cells (packed W, E, S, N in the reference's loop order).
+struct DevObc {
+  int n;                 // total number of open-boundary cells
+  int mtide;
+  const int *slot;       // [n] slot of the boundary cell
+  const int *nbr;        // [n] slot of its interior neighbour (LEC/LWC/LNC/LSC)
+  const int *side;       // [n] 0 W, 1 E, 2 S, 3 N
+  const int *ispb;       // [n]
+  const double *pcb, *psb;  // [n*mtide], index k*mtide+m
+  const double *pser;    // [n] per-step series part
+  const int *side_start; // [5] prefix offsets of the sides
+};
+
+struct StepScalars {
+  double delt, deltd2, delti, g, gi, hdry, rsqm, snlt, ritb1;
+  int isdry, ndrystp, isbal, iterm;
+  double cosv[MT_MAX], sinv[MT_MAX];
+};
+
+}  // namespace xm

@@ -1,0 +1,72 @@
+// xm_kernels.h -- launch interface between the host orchestration (xm_capi.cu)
+// and the kernel files (xm_step.cu FP64, xm_mixed.cu FP32 inner solve).
+#pragma once
+
+#include <algorithm>
+
+#include "../../include/efdc_xm.h"
+#include "xm_internal.h"
+
+namespace xm {
+
+struct Launch {
+  int grid;          // CTAs of the grid-stride cell kernels
+  int ntile;         // tiles including the ghost tile 0
+  cudaStream_t stream;
+};
+
+// One array to move between host order (element L at [L-1]) and tile order.
+struct CopyJob {
+  const void *host_order;  // device staging buffer in host (L) order
+  void *dev;               // tile-order device array
+  int is_int;              // 0 double, 1 LOGICAL (0/1), 2 raw int, 3 double water-only
+};
+
+void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c);
+void launch_assemble(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
+                     Ctl *ctl, double *part);
+void launch_obc(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B,
+                const StepScalars &c, Ctl *ctl, bool serial);
+void launch_obc_reset(const Launch &l, const DevObc &B, const DevState &X);
+void launch_scale(const Launch &l, const DevStatic &S, const DevState &X, const DevSystem &Y,
+                  Ctl *ctl, int mixed);
+void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
+                    double *part);
+void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
+                    double *part, double rsqm, int iterm);
+void launch_mx_resid(const Launch &l, const DevStatic &S, const DevSystem &Y, const double *P,
+                     Ctl *ctl, double *part, double rsqm, double rel_tol);
+void launch_mx_apply(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P);
+void launch_mx_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
+                    double *part, int inner_cap, int total_cap);
+void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
+                      double *part);
+void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
+                      double *part, double rsqm, int iterm);
+void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
+                      double *part);
+void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
+                      double *part, int inner_cap, int total_cap);
+void launch_backsub(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c);
+void launch_obc_hp(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B,
+                   const StepScalars &c);
+void launch_wd_legacy(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
+                      Ctl *ctl, int check);
+void launch_wd99(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
+                 Ctl *ctl);
+void launch_final(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
+                  Ctl *ctl);
+void launch_scatter(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx, int nslot,
+                    int lc);
+void launch_gather(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx, int nslot);
+
+void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
+                        int mixed);
+
+// process-wide count of kernel launches (measurement hook)
+void count_launches(int n);
+
+int occupancy_blocks_per_sm();
+int occupancy_blocks_per_sm_mixed();
+
+}  // namespace xm

@@ -1,0 +1,958 @@
+// xm_step.cu -- FP64 kernels of one external-mode step (everything except the
+// FP32 inner solve).  Compiled with -fmad=false: every statement rounds as
+// the reference's SSE2 ReleaseDP64 build does (no fused multiply-add), so the
+// per-cell arithmetic matches EFDC+ statement by statement; only the order of
+// the global dot products differs (fixed-order tree instead of serial).
+//
+// Each kernel is a grid-stride loop over tiles (one 256-thread CTA processes a
+// whole 32x8 tile per iteration); tile 0 is the ghost tile and is skipped.
+
+#include "xm_common.cuh"
+#include "xm_kernels.h"
+
+namespace xm {
+
+#define TILE_LOOP(ntile)                                                      \
+  for (int tile = blockIdx.x + 1; tile < (ntile); tile += gridDim.x)
+
+// ---------------------------------------------------------------------------
+// calpuv2c.f90:164-293: switches, explicit transports, time-level advance, FP1
+__global__ void __launch_bounds__(NT) k_begin(DevStatic S, DevState X, StepScalars c, int ntile) {
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    const double sub = X.sub[d], svb = X.svb[d];
+    if (c.isdry > 0) {  // :172-190
+      X.iscdry[d] = 0;
+      X.sub1[d] = sub;
+      X.svb1[d] = svb;
+      X.oldmask[d] = X.lmaskdry[d];
+      if (c.ndrystp < 0 && c.isbal > 0) X.qdwaste[d] = 0.;
+      X.wasted[d] = 0;
+    }
+    const double P = X.p[d];
+    const double uhdye = X.uhdye[d], vhdxe = X.vhdxe[d];
+    // :214-220
+    X.fuhdye[d] = uhdye - c.deltd2 * sub * S.hruo[d] * X.hu[d] * (P - X.p[q.w]) +
+                  sub * c.delt * S.dxiu[d] *
+                      (S.dxyu[d] * (X.tsx[d] - c.ritb1 * X.tbx[d]) + X.fcaxe[d] + 0.0 -
+                       c.snlt * X.fxe[d]);
+    X.fvhdxe[d] = vhdxe - c.deltd2 * svb * S.hrvo[d] * X.hv[d] * (P - X.p[q.s]) +
+                  svb * c.delt * S.dyiv[d] *
+                      (S.dxyv[d] * (X.tsy[d] - c.ritb1 * X.tby[d]) - X.fcaye[d] + 0.0 -
+                       c.snlt * X.fye[d]);
+    if (c.isdry > 0) {  // :246-253
+      X.sub[d] = S.subo[d];
+      X.svb[d] = S.svbo[d];
+      X.sbx[d] = S.sbxo[d];
+      X.sby[d] = S.sbyo[d];
+    }
+    // :256-266
+    X.uhdy1e[d] = uhdye;
+    X.vhdx1e[d] = vhdxe;
+    X.h1p[d] = X.hp[d];
+    // :282-290
+    const double C1 = 0.5 * c.g;
+    X.fp1[d] = c.delti * S.dxyp[d] * P -
+               C1 * (X.uhdye[q.e] - uhdye + X.vhdxe[q.n] - vhdxe);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// calpuv2c.f90:306-344 (FP, CS, CW, CE, CN, CC) and the minimum of CC over
+// the non-open-boundary cells (:360-368; the open-boundary cells' CC is
+// replaced by SETOPENBC and enters through k_obc).
+__global__ void __launch_bounds__(NT) k_assemble(DevStatic S, DevState X, StepScalars c, int ntile,
+                                                Ctl *ctl, double *part) {
+  __shared__ double sh[32];
+  double mn = 1.e+18;
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    const uint8_t kd = S.kind[d];
+    if (kd == LAND) continue;
+    double C1 = 0.5 * c.g;
+    const double sub = X.sub[d], svb = X.svb[d], sube = X.sub[q.e], svbn = X.svb[q.n];
+    X.fp[d] = X.fp1[d] - C1 * (sube * X.fuhdye[q.e] - sub * X.fuhdye[d] +
+                               svbn * X.fvhdxe[q.n] - svb * X.fvhdxe[d] - 2.0 * X.qsume[d]);
+    C1 = -0.5 * c.deltd2 * c.g;
+    const double cs = C1 * svb * S.hrvo[d] * S.rcx[d] * X.hv[d];
+    const double cw = C1 * sub * S.hruo[d] * S.rcx[d] * X.hu[d];
+    const double ce = C1 * sube * S.hruo[q.e] * S.rcx[q.e] * X.hu[q.e];
+    const double cn = C1 * svbn * S.hrvo[q.n] * S.rcx[q.n] * X.hv[q.n];
+    const double cc = c.delti * S.dxyp[d] - cs - cw - ce - cn;
+    X.cs[d] = cs;
+    X.cw[d] = cw;
+    X.ce[d] = ce;
+    X.cn[d] = cn;
+    X.cc[d] = cc;
+    if (kd == WATER) mn = fmin(mn, cc);
+  }
+  mn = block_min(mn, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = mn;
+  if (arrive_last(&ctl->counter)) {
+    double m = 1.e+18;
+    for (int i = threadIdx.x; i < gridDim.x; i += NT) m = fmin(m, __ldcg(&part[i]));
+    m = block_min(m, sh);
+    if (threadIdx.x == 0) {
+      ctl->ccmnm_int = m;
+      ctl->ccmnm_bc = 1.e+18;
+      ctl->asym = 0;
+      ctl->counter = 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SETOPENBC (setopenbc.f90:22-206) + SETOPENBC2 (setopenbc2.f90:17-46) for one
+// boundary cell k.  Returns CC of the cell.  `apply` updates the interior
+// neighbour's FP and coupling; the parallel kernel uses it only when the host
+// proved every target unique and not itself a boundary cell.
+__device__ __forceinline__ double obc_cell(const DevStatic &S, const DevState &X,
+                                           const DevObc &B, const StepScalars &c, int k) {
+  const int d = B.slot[k], nb = B.nbr[k], side = B.side[k], ispb = B.ispb[k];
+  const double D = c.deltd2, G = c.g, HDRY2 = 0.2 * c.hdry;
+  X.cc[d] = c.delti * S.dxyp[d];
+  X.cs[d] = 0.;
+  X.cw[d] = 0.;
+  X.ce[d] = 0.;
+  X.cn[d] = 0.;
+  if (!X.lopenbcdry[d]) {
+    double fp = B.pser ? B.pser[k] : 0.0;
+    for (int m = 0; m < B.mtide; ++m) {
+      const double TC = c.cosv[m], TS = c.sinv[m];
+      fp = fp + B.pcb[k * B.mtide + m] * TC + B.psb[k * B.mtide + m] * TS;
+    }
+    if (ispb == 1 || ispb == 2) {  // radiation
+      if (side == 0) {  // W, face at LEC(L)
+        const double CET = 0.5 * D * G * S.hruo[nb] * S.rcx[nb] * X.hu[nb];
+        const double TMP = D * sqrt(G * X.hu[nb]) * S.dxiu[nb];
+        X.cc[d] = CET * (1. + TMP) / TMP;
+        X.ce[d] = -CET;
+        fp = CET * (2. * fp - sqrt(G * X.hu[nb]) * X.fuhdye[nb] * S.dyiu[nb] / X.hu[nb]) / TMP;
+      } else if (side == 1) {  // E, own west face
+        const double CWT = 0.5 * D * G * S.hruo[d] * S.rcx[d] * X.hu[d];
+        const double TMP = D * sqrt(G * X.hu[d]) * S.dxiu[d];
+        X.cc[d] = CWT * (1. + TMP) / TMP;
+        X.cw[d] = -CWT;
+        fp = CWT * (2. * fp + sqrt(G * X.hu[d]) * X.fuhdye[d] * S.dyiu[d] / X.hu[d]) / TMP;
+      } else if (side == 2) {  // S, face at LNC(L)
+        const double CNT = 0.5 * D * G * S.hrvo[nb] * S.rcx[nb] * X.hv[nb];
+        const double TMP = D * sqrt(G * X.hv[nb]) * S.dyiv[nb];
+        X.cc[d] = CNT * (1. + TMP) / TMP;
+        X.cn[d] = -CNT;
+        fp = CNT * (2. * fp - sqrt(G * X.hv[nb]) * X.fvhdxe[nb] * S.dxiv[nb] / X.hv[nb]) / TMP;
+      } else {  // N, own south face
+        const double CST = 0.5 * D * G * S.hrvo[d] * S.rcx[d] * X.hv[d];
+        const double TMP = D * sqrt(G * X.hv[d]) * S.dyiv[d];
+        X.cc[d] = CST * (1. + TMP) / TMP;
+        X.cs[d] = -CST;
+        fp = CST * (2. * fp + sqrt(G * X.hv[d]) * X.fvhdxe[d] * S.dxiv[d] / X.hv[d]) / TMP;
+      }
+    } else {  // clamped elevation
+      const double FP1G = fp / G - HDRY2;
+      double CT;
+      if (FP1G < S.belv[d] || FP1G < S.belv[nb]) {
+        fp = (S.belv[d] + HDRY2) * G;
+        CT = 0.;
+        X.lopenbcdry[d] = 1;
+      } else if (side == 0) {
+        CT = 0.5 * D * G * S.hruo[nb] * S.rcx[nb] * X.hu[nb];
+      } else if (side == 1) {
+        CT = 0.5 * D * G * S.hruo[d] * S.rcx[d] * X.hu[d];
+      } else if (side == 2) {
+        CT = 0.5 * D * G * S.hrvo[nb] * S.rcx[nb] * X.hv[nb];
+      } else {
+        CT = 0.5 * D * G * S.hrvo[d] * S.rcx[d] * X.hv[d];
+      }
+      X.fp[nb] = X.fp[nb] + CT * fp;
+      fp = c.delti * S.dxyp[d] * fp;
+    }
+    X.fp[d] = fp;
+  }
+  return X.cc[d];
+}
+
+__device__ __forceinline__ void obc2_cell(const DevState &X, const DevObc &B, int k) {
+  if (B.ispb[k] != 0) return;
+  const int nb = B.nbr[k];
+  switch (B.side[k]) {
+    case 0: X.cw[nb] = 0.; break;
+    case 1: X.ce[nb] = 0.; break;
+    case 2: X.cs[nb] = 0.; break;
+    default: X.cn[nb] = 0.; break;
+  }
+}
+
+// One CTA; boundary cells in parallel (hazard-free layouts only).
+__global__ void __launch_bounds__(NT) k_obc_parallel(DevStatic S, DevState X, DevObc B,
+                                                    StepScalars c, Ctl *ctl) {
+  __shared__ double sh[32];
+  double mn = 1.e+18;
+  for (int k = threadIdx.x; k < B.n; k += NT) mn = fmin(mn, obc_cell(S, X, B, c, k));
+  __syncthreads();
+  for (int k = threadIdx.x; k < B.n; k += NT) obc2_cell(X, B, k);
+  mn = block_min(mn, sh);
+  if (threadIdx.x == 0) ctl->ccmnm_bc = mn;
+}
+
+// One thread, the reference's exact loop order (layouts where boundary cells
+// share or are each other's interior neighbours).
+__global__ void k_obc_serial(DevStatic S, DevState X, DevObc B, StepScalars c, Ctl *ctl) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double mn = 1.e+18;
+  for (int k = 0; k < B.n; ++k) mn = fmin(mn, obc_cell(S, X, B, c, k));
+  for (int k = 0; k < B.n; ++k) obc2_cell(X, B, k);
+  ctl->ccmnm_bc = mn;
+}
+
+// calpuv2c.f90:150-157: LOPENBCDRY=.FALSE. on the open-boundary cells
+__global__ void k_obc_reset(DevObc B, DevState X) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B.n; k += gridDim.x * blockDim.x)
+    X.lopenbcdry[B.slot[k]] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// calpuv2c.f90:371-399: scale by the minimum diagonal; FP32 copies for MIXED.
+// Also flags an unsymmetric operator (CE(L) /= CW(LE) or CN(L) /= CS(LN)),
+// which only a radiation boundary with a closed interior face produces.
+__global__ void __launch_bounds__(NT) k_scale(DevStatic S, DevState X, DevSystem Y, int ntile,
+                                             Ctl *ctl, int mixed) {
+  const double CCMNM = fmin(ctl->ccmnm_int, ctl->ccmnm_bc);
+  const double CCMNMI = 1. / CCMNM;
+  bool asym = false;
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    const double cs = X.cs[d], cw = X.cw[d], ce = X.ce[d], cn = X.cn[d];
+    asym |= (ce != X.cw[q.e]) || (cn != X.cs[q.n]);
+    const double ccs = cs * CCMNMI, ccw = cw * CCMNMI, cce = ce * CCMNMI,
+                 ccn = cn * CCMNMI, ccc = X.cc[d] * CCMNMI;
+    const double fpt = X.fp[d] * CCMNMI;
+    Y.ccs[d] = ccs;
+    Y.ccw[d] = ccw;
+    Y.cce[d] = cce;
+    Y.ccn[d] = ccn;
+    Y.ccc[d] = ccc;
+    Y.fptmp[d] = fpt;
+    if (mixed) {
+      Y.ccs32[d] = float(ccs);
+      Y.ccw32[d] = float(ccw);
+      Y.cce32[d] = float(cce);
+      Y.ccn32[d] = float(ccn);
+      Y.ccc32[d] = float(ccc);
+    }
+  }
+  if (__syncthreads_or(asym) && threadIdx.x == 0) atomicOr(&ctl->asym, 1);
+}
+
+// ---------------------------------------------------------------------------
+// CONGRAD in FP64 (congrad.f90:54-187).  Vectors: P (the state array), r,
+// p double-buffered (pa/pb, selected by ctl->parity), Ap.  z = CCCI*r with
+// CCCI = 1./CCC is recomputed where needed instead of stored.
+
+__device__ __forceinline__ double rcp_rn(double x) { return 1. / x; }
+
+// :54-88 initial residual, z0, RPCG.
+__global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double *P, int ntile,
+                                               Ctl *ctl, double *part) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    const double ccc = Y.ccc[d];
+    const double r = Y.fptmp[d] - ccc * P[d] - Y.ccn[d] * P[q.n] - Y.ccs[d] * P[q.s] -
+                     Y.ccw[d] * P[q.w] - Y.cce[d] * P[q.e];
+    const double z = r * rcp_rn(ccc);
+    Y.r[d] = r;
+    Y.pa[d] = z;
+    acc += r * z;
+  }
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+  if (arrive_last(&ctl->counter)) {
+    const double rpcg = reduce_partials(part, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+      ctl->rpcg = rpcg;
+      ctl->beta = 0.0;
+      ctl->parity = 0;
+      ctl->iter = 0;
+      ctl->rsq = 0.0;
+      ctl->status = 0;
+      ctl->done = (rpcg == 0.0) ? 1 : 0;  // :88 RETURN
+      if (!isfinite(rpcg)) {
+        ctl->done = 1;
+        ctl->status = EFDC_XM_NONFINITE;
+      }
+      ctl->counter = 0;
+    }
+  }
+}
+
+// :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA).
+template <bool SYM>
+__global__ void __launch_bounds__(NT) k_cg_matvec(DevStatic S, DevSystem Y, int ntile, Ctl *ctl,
+                                                 double *part) {
+  __shared__ double sh[32];
+  if (ctl->done) return;
+  const double beta = ctl->beta;
+  const bool par = ctl->parity;
+  const double *__restrict__ pold = par ? Y.pb : Y.pa;
+  double *__restrict__ pnew = par ? Y.pa : Y.pb;
+  const bool asym = !SYM || ctl->asym;
+  double acc = 0.0;
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    // PCG = TMPCG + BETA*PCG at the cell and its neighbours (:151-162)
+    auto pc = [&](int j) { return rcp_rn(Y.ccc[j]) * Y.r[j] + beta * pold[j]; };
+    const double p = pc(d), pn = pc(q.n), pe = pc(q.e), pw = pc(q.w), ps = pc(q.s);
+    const double ccs = Y.ccs[d], ccw = Y.ccw[d];
+    double ccn, cce;
+    if (asym) {
+      ccn = Y.ccn[d];
+      cce = Y.cce[d];
+    } else {
+      ccn = Y.ccs[q.n];
+      cce = Y.ccw[q.e];
+    }
+    const double ap = Y.ccc[d] * p + ccs * ps + ccn * pn + ccw * pw + cce * pe;  // :114
+    pnew[d] = p;
+    Y.ap[d] = ap;
+    acc += ap * p;
+  }
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+  if (arrive_last(&ctl->counter)) {
+    const double papcg = reduce_partials(part, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+      ctl->papcg = papcg;
+      ctl->alpha = ctl->rpcg / papcg;  // :124
+      ctl->counter = 0;
+    }
+  }
+}
+
+// :127-149 (P, RCG update, RPCGN, RSQ, BETA) and the stop test :165.
+__global__ void __launch_bounds__(NT) k_cg_update(DevStatic S, DevSystem Y, double *P, int ntile,
+                                                 Ctl *ctl, double *part, double rsqm, int iterm) {
+  __shared__ double sh[32];
+  if (ctl->done) return;
+  const double alpha = ctl->alpha;
+  const double *__restrict__ pnew = ctl->parity ? Y.pa : Y.pb;
+  double a1 = 0.0, a2 = 0.0;
+  TILE_LOOP(ntile) {
+    const int d = tile * TILE + threadIdx.x;
+    if (S.kind[d] == LAND) continue;
+    const double p = pnew[d];
+    P[d] = P[d] + alpha * p;
+    const double r = Y.r[d] - alpha * Y.ap[d];
+    Y.r[d] = r;
+    const double z = rcp_rn(Y.ccc[d]) * r;
+    a1 += r * z;
+    a2 += r * r;
+  }
+  a1 = block_sum(a1, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = a1;
+  a2 = block_sum(a2, sh);
+  if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = a2;
+  if (arrive_last(&ctl->counter)) {
+    const double rpcgn = reduce_partials(part, gridDim.x, sh);
+    const double rsq = reduce_partials(part + gridDim.x, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+      const double beta = rpcgn / ctl->rpcg;
+      ctl->beta = beta;
+      ctl->rpcg = rpcgn;
+      ctl->rsq = rsq;
+      const int it = ctl->iter + 1;
+      ctl->iter = it;
+      if (!isfinite(rsq) || !isfinite(ctl->alpha)) {
+        ctl->done = 1;
+        ctl->status = EFDC_XM_NONFINITE;
+      } else if (rsq <= rsqm) {
+        ctl->done = 1;
+      } else if (it >= iterm) {
+        ctl->done = 1;
+        ctl->status = EFDC_XM_CG_MAXITER;
+      } else {
+        ctl->parity ^= 1;
+      }
+      ctl->counter = 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MIXED outer step: r = b - A*P in FP64 (the FP64 refinement residual),
+// RSQ in FP64, and the FP32 inner system r32, z32 = r32/CCC.  Leaves P alone.
+__global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, DevSystem Y, const double *P,
+                                                int ntile, Ctl *ctl, double *part, double rsqm,
+                                                double rel_tol) {
+  __shared__ double sh[32];
+  double a1 = 0.0, a2 = 0.0;
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    const double r = Y.fptmp[d] - Y.ccc[d] * P[d] - Y.ccn[d] * P[q.n] - Y.ccs[d] * P[q.s] -
+                     Y.ccw[d] * P[q.w] - Y.cce[d] * P[q.e];
+    const float r32 = float(r);
+    const float z32 = r32 * __frcp_rn(Y.ccc32[d]);
+    Y.r32[d] = r32;
+    Y.pa32[d] = z32;
+    Y.x32[d] = 0.f;
+    a1 += r * r;
+    a2 += double(r32) * double(z32);
+  }
+  a1 = block_sum(a1, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = a1;
+  a2 = block_sum(a2, sh);
+  if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = a2;
+  if (arrive_last(&ctl->counter)) {
+    const double rsq = reduce_partials(part, gridDim.x, sh);
+    const double rz = reduce_partials(part + gridDim.x, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+      ctl->rsq64 = rsq;
+      ctl->rsq = rsq;
+      ctl->rpcg = rz;
+      ctl->beta = 0.0;
+      ctl->parity = 0;
+      ctl->inner_iter = 0;
+      ctl->idone = 0;
+      ctl->outer += 1;
+      const double tgt = fmax(rsq * rel_tol * rel_tol, 0.1 * rsqm);
+      ctl->rsq_target = tgt;
+      if (!isfinite(rsq)) {
+        ctl->done = 1;
+        ctl->status = EFDC_XM_NONFINITE;
+      } else if (rsq <= rsqm || rz == 0.0) {
+        ctl->done = 1;
+      } else {
+        ctl->done = 0;
+      }
+      ctl->counter = 0;
+    }
+  }
+}
+
+// MIXED: P += x32 (the FP32 correction), x32 = 0.
+__global__ void __launch_bounds__(NT) k_mx_apply(DevStatic S, DevSystem Y, double *P, int ntile) {
+  TILE_LOOP(ntile) {
+    const int d = tile * TILE + threadIdx.x;
+    if (S.kind[d] == LAND) continue;
+    P[d] = P[d] + double(Y.x32[d]);
+  }
+}
+
+// Standalone CONGRAD: a caller-assembled scaled system.  Land slots are made
+// inert (CCC=1, couplings 0, b=0), FP32 copies made for MIXED, and the
+// symmetry of the given CCE/CCN against CCW(LE)/CCS(LN) is recorded.
+__global__ void __launch_bounds__(NT) k_sys_prepare(DevStatic S, DevSystem Y, int ntile, Ctl *ctl,
+                                                   int mixed) {
+  bool asym = false;
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) {
+      Y.ccc[d] = 1.0;
+      Y.ccs[d] = Y.ccw[d] = Y.cce[d] = Y.ccn[d] = Y.fptmp[d] = 0.0;
+      Y.ccc32[d] = 1.0f;
+      Y.ccs32[d] = Y.ccw32[d] = Y.cce32[d] = Y.ccn32[d] = 0.0f;
+      continue;
+    }
+    const double cce = Y.cce[d], ccn = Y.ccn[d];
+    // a land neighbour is zeroed by this kernel too: compare with 0 there
+    const double ccw_e = (S.kind[q.e] == LAND) ? 0.0 : Y.ccw[q.e];
+    const double ccs_n = (S.kind[q.n] == LAND) ? 0.0 : Y.ccs[q.n];
+    asym |= (cce != ccw_e) || (ccn != ccs_n);
+    if (mixed) {
+      Y.ccc32[d] = float(Y.ccc[d]);
+      Y.ccs32[d] = float(Y.ccs[d]);
+      Y.ccw32[d] = float(Y.ccw[d]);
+      Y.cce32[d] = float(cce);
+      Y.ccn32[d] = float(ccn);
+    }
+  }
+  if (__syncthreads_or(asym) && threadIdx.x == 0) atomicOr(&ctl->asym, 1);
+}
+
+// ---------------------------------------------------------------------------
+// calpuv2c.f90:416-437 face discharges and unit-width discharges.
+__global__ void __launch_bounds__(NT) k_backsub(DevStatic S, DevState X, StepScalars c, int ntile) {
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    const double P = X.p[d];
+    const double u = X.sub[d] *
+                     (X.fuhdye[d] - c.deltd2 * S.hruo[d] * S.rcx[d] * X.hu[d] * (P - X.p[q.w]));
+    const double v = X.svb[d] *
+                     (X.fvhdxe[d] - c.deltd2 * S.hrvo[d] * S.rcx[d] * X.hv[d] * (P - X.p[q.s]));
+    X.uhdye[d] = u;
+    X.vhdxe[d] = v;
+    X.uhe[d] = u * S.dyiu[d];
+    X.vhe[d] = v * S.dxiv[d];
+  }
+}
+
+// calpuv2c.f90:466-486 continuity.
+__global__ void __launch_bounds__(NT) k_continuity(DevStatic S, DevState X, StepScalars c,
+                                                  int ntile) {
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    X.hp[d] = X.h1p[d] +
+              c.deltd2 * S.dxyip[d] *
+                  (2. * X.qsume[d] -
+                   (X.uhdye[q.e] + X.uhdy1e[q.e] - X.uhdye[d] - X.uhdy1e[d] + X.vhdxe[q.n] +
+                    X.vhdx1e[q.n] - X.vhdxe[d] - X.vhdx1e[d]));
+  }
+}
+
+// calpuv2c.f90:489-535 depths of the open-boundary cells (+ drying of a
+// boundary cell).  Concurrent zero-writes to shared faces are benign.
+__global__ void k_obc_hp(DevStatic S, DevState X, DevObc B, StepScalars c) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B.n; k += gridDim.x * blockDim.x) {
+    const int d = B.slot[k];
+    double hp = c.gi * X.p[d] - S.belv[d];
+    if (c.isdry > 0) {
+      const double h1p = X.h1p[d];
+      const int obd = X.lopenbcdry[d];
+      if ((obd || (h1p < 0.9 * c.hdry && hp < h1p) || hp < 0.) && X.iscdry[d] == 0) {
+        if (hp <= 0. && obd)
+          hp = 0.2 * c.hdry;
+        else
+          hp = fmin(fmax(h1p, 0.1 * c.hdry), 0.9 * c.hdry);
+        X.iscdry[d] = 1;
+        const Nb q = neighbours_of_slot(S.tnbr, d);
+        X.sub[d] = 0.;
+        X.svb[d] = 0.;
+        X.sub[q.e] = 0.;
+        X.svb[q.n] = 0.;
+        X.sbx[d] = 0.;
+        X.sby[d] = 0.;
+        X.sbx[q.e] = 0.;
+        X.sby[q.n] = 0.;
+        X.uhdye[d] = 0.;
+        X.uhdye[q.e] = 0.;
+        X.vhdxe[d] = 0.;
+        X.vhdxe[q.n] = 0.;
+        X.lopenbcdry[d] = 1;
+        X.cc[d] = c.delti * S.dxyp[d];
+        const double p = (hp + S.belv[d]) * c.g;
+        X.p[d] = p;
+        X.fp1[d] = c.delti * S.dxyp[d] * p;
+      }
+    }
+    X.hp[d] = hp;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// ISDRY>0: P = G*(HP+BELV) (:560-570) fused with the legacy drying check,
+// ISDRY 1..97 (:574-603).  All face writes are zeros, so the order of the
+// reference's serial loop does not matter.
+__global__ void __launch_bounds__(NT) k_wd_legacy(DevStatic S, DevState X, StepScalars c,
+                                                 int ntile, Ctl *ctl, int check) {
+  bool flag = false;
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    const double hp = X.hp[d];
+    X.p[d] = c.g * (hp + S.belv[d]);
+    if (check && hp <= c.hdry) {
+      if (X.iscdry[d] == 0) {
+        X.iscdry[d] = 1;
+        flag = true;
+      }
+      X.sub[d] = 0.;
+      X.svb[d] = 0.;
+      X.sub[q.e] = 0.;
+      X.svb[q.n] = 0.;
+      X.sbx[d] = 0.;
+      X.sby[d] = 0.;
+      X.sbx[q.e] = 0.;
+      X.sby[q.n] = 0.;
+    }
+  }
+  if (__syncthreads_or(flag) && threadIdx.x == 0) atomicOr(&ctl->icordry, 1);
+}
+
+// ISDRY=99 (:606-734), pass 1: P update and each cell's decision, from
+// unmodified data.  Code bits: 1 the cell writes its faces; 2 rising fast
+// enough to re-wet (then 4/8/16/32 re-open W/E/S/N); 64 the ISCDRY-only
+// branches (rising too slowly, or drying).
+enum : int { WD_ACT = 1, WD_FAST = 2, WD_RW = 4, WD_RE = 8, WD_RS = 16, WD_RN = 32, WD_SLOW = 64 };
+
+__global__ void __launch_bounds__(NT) k_wd99_decide(DevStatic S, DevState X, StepScalars c,
+                                                   int ntile) {
+  const double HDRY = c.hdry, HDRY2 = 2. * HDRY, HDRY90 = 0.9 * HDRY;
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) {
+      X.wd_act[d] = 0;
+      continue;
+    }
+    const double hp = X.hp[d], h1p = X.h1p[d];
+    X.p[d] = c.g * (hp + S.belv[d]);
+    int act = 0;
+    if (hp <= HDRY) {
+      const double DHPDT = hp - h1p;
+      if (DHPDT > 0.0) {
+        act = WD_ACT;
+        const double DHPDT2 = (HDRY - h1p) * 0.01;
+        if (DHPDT > DHPDT2) {
+          act |= WD_FAST;
+          if (S.subo[d] > 0.5 && X.uhdye[d] > 0.0 && X.hp[q.w] > HDRY2) act |= WD_RW;
+          if (S.subo[q.e] > 0.5 && X.uhdye[q.e] < 0.0 && X.hp[q.e] > HDRY2) act |= WD_RE;
+          if (S.svbo[d] > 0.5 && X.vhdxe[d] > 0.0 && X.hp[q.s] > HDRY2) act |= WD_RS;
+          if (S.svbo[q.n] > 0.5 && X.vhdxe[q.n] < 0.0 && X.hp[q.n] > HDRY2) act |= WD_RN;
+        } else {
+          act |= WD_SLOW;
+        }
+      } else if (hp < HDRY90 || h1p < HDRY) {
+        act = WD_ACT | WD_SLOW;
+      }
+    }
+    X.wd_act[d] = act;
+  }
+}
+
+// ISDRY=99 pass 2: the face values the reference's serial L-order loop
+// leaves (a face shared by cells L and LW is last written by L), the ISCDRY
+// updates and the re-solve flag, into the *_n scratch arrays.
+__global__ void __launch_bounds__(NT) k_wd99_apply(DevStatic S, DevState X, int ntile, Ctl *ctl) {
+  bool flag = false;
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    const int a = X.wd_act[d], aw = X.wd_act[q.w], as = X.wd_act[q.s];
+    const double subo = S.subo[d], svbo = S.svbo[d];
+    // the west face SUB(L) (owners: L, then LW as its east face)
+    double sub, sbx, svb, sby;
+    if (a & WD_ACT) {
+      const bool o = a & WD_RW;
+      sub = o ? subo : 0.0;
+      sbx = o ? S.sbxo[d] : 0.0;
+    } else if (aw & WD_ACT) {
+      const bool o = aw & WD_RE;
+      sub = o ? subo : 0.0;
+      sbx = o ? S.sbxo[d] : 0.0;
+    } else {
+      sub = X.sub[d];
+      sbx = X.sbx[d];
+    }
+    if (a & WD_ACT) {
+      const bool o = a & WD_RS;
+      svb = o ? svbo : 0.0;
+      sby = o ? S.sbyo[d] : 0.0;
+    } else if (as & WD_ACT) {
+      const bool o = as & WD_RN;
+      svb = o ? svbo : 0.0;
+      sby = o ? S.sbyo[d] : 0.0;
+    } else {
+      svb = X.svb[d];
+      sby = X.sby[d];
+    }
+    X.sub_n[d] = sub;
+    X.sbx_n[d] = sbx;
+    X.svb_n[d] = svb;
+    X.sby_n[d] = sby;
+    if (a & WD_FAST) {
+      const double ww = (a & WD_RW) ? subo : 0.0;
+      const double we = (a & WD_RE) ? S.subo[q.e] : 0.0;
+      const double ws = (a & WD_RS) ? svbo : 0.0;
+      const double wn = (a & WD_RN) ? S.svbo[q.n] : 0.0;
+      const double RDRY = ww + we + ws + wn;
+      X.iscdry[d] = (RDRY < 0.5) ? 1 : 0;
+      // values seen by L before its own writes
+      const double SUBW = (aw & WD_ACT) ? ((aw & WD_RE) ? subo : 0.0) : X.sub[d];
+      const double SUBE = X.sub[q.e];
+      const double SVBS = (as & WD_ACT) ? ((as & WD_RN) ? svbo : 0.0) : X.svb[d];
+      const double SVBN = X.svb[q.n];
+      if (fabs(ww - SUBW) > 0.5 || fabs(we - SUBE) > 0.5 || fabs(ws - SVBS) > 0.5 ||
+          fabs(wn - SVBN) > 0.5)
+        flag = true;
+    } else if (a & WD_SLOW) {
+      if (X.iscdry[d] == 0) {
+        X.iscdry[d] = 1;
+        flag = true;
+      }
+    }
+  }
+  if (__syncthreads_or(flag) && threadIdx.x == 0) atomicOr(&ctl->icordry, 1);
+}
+
+__global__ void __launch_bounds__(NT) k_wd99_commit(DevStatic S, DevState X, int ntile) {
+  TILE_LOOP(ntile) {
+    const int d = tile * TILE + threadIdx.x;
+    if (S.kind[d] == LAND) continue;
+    X.sub[d] = X.sub_n[d];
+    X.svb[d] = X.svb_n[d];
+    X.sbx[d] = X.sbx_n[d];
+    X.sby[d] = X.sby_n[d];
+  }
+}
+
+// ISDRY>0 without a drying check (ISDRY=98): only the P update.
+// (k_wd_legacy with check=0.)
+
+// ---------------------------------------------------------------------------
+// :838-889 volume wasting of isolated wet cells (NDRYSTP<0) and the later
+// H1P/QDWASTE fix-up of the wasted cells (:1003-1025).
+__global__ void __launch_bounds__(NT) k_fin_waste(DevStatic S, DevState X, StepScalars c,
+                                                 int ntile, Ctl *ctl) {
+  const int NTMP = abs(c.ndrystp);
+  int nw = 0;
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    const double hp = X.hp[d];
+    if (hp >= c.hdry) {
+      const double RDRY = X.sub[d] + X.sub[q.e] + X.svb[d] + X.svb[q.n];
+      if (RDRY > 0.5) {
+        X.natdry[d] = 0;
+      } else {
+        const int nat = X.natdry[d] + 1;
+        X.natdry[d] = nat;
+        if (nat > NTMP) {
+          const double bl = S.belv[d];
+          double RVAL = 0.0;
+          if (S.subo[q.e] > 0.5 && S.belv[q.e] < bl) RVAL = RVAL + 1.;
+          if (S.subo[d] > 0.5 && S.belv[q.w] < bl) RVAL = RVAL + 1.;
+          if (S.svbo[q.n] > 0.5 && S.belv[q.n] < bl) RVAL = RVAL + 1.;
+          if (S.svbo[d] > 0.5 && S.belv[q.s] < bl) RVAL = RVAL + 1.;
+          if (RVAL > 0. || hp < c.hdry * 2.) {
+            const double HOLDTMP = hp;
+            const double hnew = 0.90 * c.hdry;
+            X.hp[d] = hnew;
+            X.h1p[d] = 0.90 * c.hdry;
+            X.natdry[d] = 0;
+            X.qdwaste[d] = (c.isbal == 0) ? 0.0 : c.delti * S.dxyp[d] * (HOLDTMP - hnew);
+            X.vdwaste[d] = X.vdwaste[d] + S.dxyp[d] * (HOLDTMP - hnew);
+            X.wasted[d] = 1;
+            ++nw;
+          }
+        }
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) nw += __shfl_down_sync(0xffffffffu, nw, o);
+  if ((threadIdx.x & 31) == 0 && nw) atomicAdd(&ctl->nwasted, nw);
+}
+
+// :893-931 final P (ISDRY=0), HU, HV, reciprocals, LMASKDRY; NEGDEP count.
+__global__ void __launch_bounds__(NT) k_fin(DevStatic S, DevState X, StepScalars c, int ntile,
+                                           Ctl *ctl) {
+  int nneg = 0, nbad = 0;
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    const double hp = X.hp[d];
+    if (c.isdry == 0) X.p[d] = c.g * (hp + S.belv[d]);
+    const double dxyp = S.dxyp[d];
+    const double hu = (dxyp * hp + S.dxyp[q.w] * X.hp[q.w]) * S.fsgzu[d];
+    const double hv = (dxyp * hp + S.dxyp[q.s] * X.hp[q.s]) * S.fsgzv[d];
+    X.hu[d] = hu;
+    X.hv[d] = hv;
+    X.hpi[d] = 1. / hp;
+    X.hui[d] = 1. / hu;
+    X.hvi[d] = 1. / hv;
+    if (c.isdry > 0) {
+      int mask = 1;
+      if (hp < c.hdry) {
+        int IUW = 0, IUE = 0, IVS = 0, IVN = 0;
+        if (X.sub1[d] < 0.5 && X.sub[d] < 0.5) IUE = 1;
+        if (X.sub1[q.e] < 0.5 && X.sub[q.e] < 0.5) IUW = 1;
+        if (X.svb1[d] < 0.5 && X.svb[d] < 0.5) IVS = 1;
+        if (X.svb1[q.n] < 0.5 && X.svb[q.n] < 0.5) IVN = 1;
+        if (IUW + IUE + IVS + IVN == 4) mask = 0;
+      }
+      X.lmaskdry[d] = mask;
+    }
+    if (hp <= 0.) ++nneg;
+    if (!isfinite(X.p[d])) ++nbad;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    nneg += __shfl_down_sync(0xffffffffu, nneg, o);
+    nbad += __shfl_down_sync(0xffffffffu, nbad, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (nneg) atomicAdd(&ctl->nneg, nneg);
+    if (nbad) atomicAdd(&ctl->nnonfinite, nbad);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host order <-> tile order.  A land slot receives element LC of the host
+// array (the ghost value); gathers write water slots only.
+__global__ void k_scatter(const CopyJob *jobs, int njob, const int *lidx, int nslot, int lc) {
+  const int j = blockIdx.y;
+  if (j >= njob) return;
+  const CopyJob J = jobs[j];
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nslot; d += gridDim.x * blockDim.x) {
+    const int L = lidx[d];
+    if (L < 2 && J.is_int == 3) continue;  // water-only: leave land slots as they are
+    const int src = (L >= 2 ? L : lc) - 1;
+    if (J.is_int == 1 || J.is_int == 2)
+      static_cast<int *>(J.dev)[d] = (J.is_int == 1)
+                                         ? (static_cast<const int *>(J.host_order)[src] != 0 ? 1 : 0)
+                                         : static_cast<const int *>(J.host_order)[src];
+    else
+      static_cast<double *>(J.dev)[d] = static_cast<const double *>(J.host_order)[src];
+  }
+}
+
+__global__ void k_gather(const CopyJob *jobs, int njob, const int *lidx, int nslot) {
+  const int j = blockIdx.y;
+  if (j >= njob) return;
+  const CopyJob J = jobs[j];
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nslot; d += gridDim.x * blockDim.x) {
+    const int L = lidx[d];
+    if (L < 2) continue;
+    if (J.is_int == 1 || J.is_int == 2)
+      static_cast<int *>(const_cast<void *>(J.host_order))[L - 1] = static_cast<const int *>(J.dev)[d];
+    else
+      static_cast<double *>(const_cast<void *>(J.host_order))[L - 1] =
+          static_cast<const double *>(J.dev)[d];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launch wrappers
+void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c) {
+  k_begin<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile);
+  count_launches(1);
+}
+void launch_assemble(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
+                     Ctl *ctl, double *part) {
+  k_assemble<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile, ctl, part);
+  count_launches(1);
+}
+void launch_obc(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B,
+                const StepScalars &c, Ctl *ctl, bool serial) {
+  if (B.n == 0) return;
+  if (serial)
+    k_obc_serial<<<1, 1, 0, l.stream>>>(S, X, B, c, ctl);
+  else
+    k_obc_parallel<<<1, NT, 0, l.stream>>>(S, X, B, c, ctl);
+  count_launches(1);
+}
+void launch_obc_reset(const Launch &l, const DevObc &B, const DevState &X) {
+  if (B.n == 0) return;
+  k_obc_reset<<<(B.n + 255) / 256, 256, 0, l.stream>>>(B, X);
+  count_launches(1);
+}
+void launch_scale(const Launch &l, const DevStatic &S, const DevState &X, const DevSystem &Y,
+                  Ctl *ctl, int mixed) {
+  k_scale<<<l.grid, NT, 0, l.stream>>>(S, X, Y, l.ntile, ctl, mixed);
+  count_launches(1);
+}
+void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
+                    double *part) {
+  k_cg_init<<<l.grid, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part);
+  count_launches(1);
+}
+void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
+                    double *part, double rsqm, int iterm) {
+  k_cg_matvec<true><<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
+  count_launches(1);
+  k_cg_update<<<l.grid, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part, rsqm, iterm);
+  count_launches(1);
+}
+void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
+                      double *part) {
+  k_cg_matvec<true><<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
+  count_launches(1);
+}
+void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
+                      double *part, double rsqm, int iterm) {
+  k_cg_update<<<l.grid, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part, rsqm, iterm);
+  count_launches(1);
+}
+void launch_mx_resid(const Launch &l, const DevStatic &S, const DevSystem &Y, const double *P,
+                     Ctl *ctl, double *part, double rsqm, double rel_tol) {
+  k_mx_resid<<<l.grid, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part, rsqm, rel_tol);
+  count_launches(1);
+}
+void launch_mx_apply(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P) {
+  k_mx_apply<<<l.grid, NT, 0, l.stream>>>(S, Y, P, l.ntile);
+  count_launches(1);
+}
+void launch_backsub(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c) {
+  k_backsub<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile);
+  count_launches(1);
+  k_continuity<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile);
+  count_launches(1);
+}
+void launch_obc_hp(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B,
+                   const StepScalars &c) {
+  if (B.n == 0) return;
+  k_obc_hp<<<(B.n + 255) / 256, 256, 0, l.stream>>>(S, X, B, c);
+  count_launches(1);
+}
+void launch_wd_legacy(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
+                      Ctl *ctl, int check) {
+  k_wd_legacy<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile, ctl, check);
+  count_launches(1);
+}
+void launch_wd99(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
+                 Ctl *ctl) {
+  k_wd99_decide<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile);
+  count_launches(1);
+  k_wd99_apply<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, ctl);
+  count_launches(1);
+  k_wd99_commit<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+  count_launches(1);
+}
+void launch_final(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
+                  Ctl *ctl) {
+  if (c.isdry > 0 && c.ndrystp < 0) {
+    k_fin_waste<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile, ctl);
+    count_launches(1);
+  }
+  k_fin<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile, ctl);
+  count_launches(1);
+}
+void launch_scatter(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx, int nslot,
+                    int lc) {
+  if (njob == 0) return;
+  dim3 g(std::min((nslot + 255) / 256, 2048), njob);
+  k_scatter<<<g, 256, 0, st>>>(jobs, njob, lidx, nslot, lc);
+  count_launches(1);
+}
+void launch_gather(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx, int nslot) {
+  if (njob == 0) return;
+  dim3 g(std::min((nslot + 255) / 256, 2048), njob);
+  k_gather<<<g, 256, 0, st>>>(jobs, njob, lidx, nslot);
+  count_launches(1);
+}
+
+void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
+                        int mixed) {
+  k_sys_prepare<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, mixed);
+  count_launches(1);
+}
+
+int occupancy_blocks_per_sm() {
+  int a = 0, b = 0, c = 0, d = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_matvec<true>, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cg_update, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_assemble, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_mx_resid, NT, 0);
+  int m = std::min(std::min(a, b), std::min(c, d));
+  return m > 0 ? m : 1;
+}
+
+}  // namespace xm

@@ -1,0 +1,320 @@
+"""ctypes mirror of include/efdc_xm.h and a thin host-side wrapper.
+
+This is how Python callers (the tests, bench.py, a calibration harness) reach
+the CUDA library ``libefdc_xm.so``; Fortran callers bind the same symbols
+through ISO_C_BINDING (see the Fortran shim sources in ``fortran/``).
+
+Array convention: every per-cell array is a contiguous numpy array laid out
+like EFDC+'s 1-based Fortran array, element L at index L-1.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libefdc_xm.so"
+
+OK, CG_MAXITER, WETDRY_MAXSWEEP, NEG_DEPTH, NONFINITE, CUDA_ERROR, DEVICE_TIMEOUT, \
+    BAD_ARGUMENT, UNSUPPORTED = range(9)
+STATUS_NAMES = {0: "OK", 1: "CG_MAXITER", 2: "WETDRY_MAXSWEEP", 3: "NEG_DEPTH",
+                4: "NONFINITE", 5: "CUDA_ERROR", 6: "DEVICE_TIMEOUT",
+                7: "BAD_ARGUMENT", 8: "UNSUPPORTED"}
+PREC_FP64, PREC_MIXED = 0, 1
+SIDES = ("W", "E", "S", "N")
+
+_pd = C.POINTER(C.c_double)
+_pi = C.POINTER(C.c_int32)
+
+
+class Obc(C.Structure):
+    _fields_ = [("n", C.c_int32), ("l", _pi), ("ispb", _pi), ("pcb", _pd),
+                ("psb", _pd), ("ld", C.c_int32)]
+
+
+class Grid(C.Structure):
+    _fields_ = [("la", C.c_int32), ("lc", C.c_int32), ("il", _pi), ("jl", _pi),
+                ("lnc", _pi), ("lsc", _pi), ("lec", _pi), ("lwc", _pi),
+                ("dxyp", _pd), ("dxyip", _pd), ("dxiu", _pd), ("dyiu", _pd),
+                ("dxiv", _pd), ("dyiv", _pd), ("dxyu", _pd), ("dxyv", _pd),
+                ("hruo", _pd), ("hrvo", _pd), ("subo", _pd), ("svbo", _pd),
+                ("sbxo", _pd), ("sbyo", _pd), ("belv", _pd), ("mtide", C.c_int32),
+                ("tcp", _pd), ("obc", Obc * 4)]
+
+
+class Params(C.Structure):
+    _fields_ = [("delt", C.c_double), ("g", C.c_double), ("hdry", C.c_double),
+                ("rsqm", C.c_double), ("tn", C.c_double), ("pi2", C.c_double),
+                ("snlt", C.c_double), ("ritb1", C.c_double), ("iterm", C.c_int32),
+                ("isdry", C.c_int32), ("ndrystp", C.c_int32), ("isbal", C.c_int32),
+                ("n", C.c_int32), ("ntstbc", C.c_int32), ("max_sweeps", C.c_int32),
+                ("precision", C.c_int32), ("mixed_rsq_factor", C.c_double)]
+
+
+class Fields(C.Structure):
+    _fields_ = [("p", _pd), ("hp", _pd), ("h1p", _pd), ("hu", _pd), ("hv", _pd),
+                ("uhdye", _pd), ("vhdxe", _pd), ("sub", _pd), ("svb", _pd),
+                ("sbx", _pd), ("sby", _pd), ("lmaskdry", _pi), ("iscdry", _pi),
+                ("lopenbcdry", _pi), ("natdry", _pi), ("fcaxe", _pd), ("fcaye", _pd),
+                ("fxe", _pd), ("fye", _pd), ("tsx", _pd), ("tsy", _pd), ("tbx", _pd),
+                ("tby", _pd), ("qsume", _pd), ("pser", _pd * 4), ("uhe", _pd),
+                ("vhe", _pd), ("hpi", _pd), ("hui", _pd), ("hvi", _pd),
+                ("qdwaste", _pd), ("vdwaste", _pd), ("lwet", _pi), ("ldry", _pi),
+                ("ccc", _pd), ("ccs", _pd), ("ccw", _pd), ("cce", _pd), ("ccn", _pd),
+                ("fptmp", _pd)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iters_last", C.c_int32),
+                ("iters_total", C.c_int32), ("solves", C.c_int32),
+                ("lawet", C.c_int32), ("ladry", C.c_int32), ("n_negdep", C.c_int32),
+                ("n_wasted", C.c_int32), ("outer_refinements", C.c_int32),
+                ("rsq_last", C.c_double), ("ccmnm_last", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class KTime(C.Structure):
+    _fields_ = [("ms_matvec", C.c_double), ("ms_update", C.c_double), ("reps", C.c_int32),
+                ("ncells", C.c_int32), ("nslots", C.c_int32)]
+
+
+FIELD_DOUBLE_INOUT = ("p", "hp", "h1p", "hu", "hv", "uhdye", "vhdxe", "sub", "svb",
+                      "sbx", "sby")
+FIELD_INT_INOUT = ("lmaskdry", "iscdry", "lopenbcdry", "natdry")
+FIELD_IN = ("fcaxe", "fcaye", "fxe", "fye", "tsx", "tsy", "tbx", "tby", "qsume")
+FIELD_OUT = ("uhe", "vhe", "hpi", "hui", "hvi", "qdwaste", "vdwaste")
+FIELD_DIAG = ("ccc", "ccs", "ccw", "cce", "ccn", "fptmp")
+
+
+def _dp(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_pd)
+
+
+def _ip(a):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_pi)
+
+
+def make_grid(g: dict):
+    """Build a Grid struct from a scenario grid dict.  Returns (struct, keepalive)."""
+    keep = []
+
+    def d(name):
+        a = np.ascontiguousarray(g[name], dtype=np.float64)
+        keep.append(a)
+        return _dp(a)
+
+    def i(name):
+        a = np.ascontiguousarray(g[name], dtype=np.int32)
+        keep.append(a)
+        return _ip(a)
+
+    s = Grid()
+    s.la = int(g["la"])
+    s.lc = int(g["lc"])
+    for k in ("il", "jl", "lnc", "lsc", "lec", "lwc"):
+        setattr(s, k, i(k))
+    for k in ("dxyp", "dxyip", "dxiu", "dyiu", "dxiv", "dyiv", "dxyu", "dxyv",
+              "hruo", "hrvo", "subo", "svbo", "sbxo", "sbyo", "belv"):
+        setattr(s, k, d(k))
+    s.mtide = int(g["mtide"])
+    tcp = np.ascontiguousarray(g["tcp"], dtype=np.float64)
+    keep.append(tcp)
+    s.tcp = _dp(tcp)
+    for k, side in enumerate(SIDES):
+        o = g["obc"][side]
+        n = len(o["l"])
+        l = np.ascontiguousarray(o["l"], dtype=np.int32)
+        isp = np.ascontiguousarray(o["ispb"], dtype=np.int32)
+        # column-major PCB(LL,M) with leading dimension n == row-major [m, ll]
+        pcb = np.ascontiguousarray(o["pcb"], dtype=np.float64).reshape(-1)
+        psb = np.ascontiguousarray(o["psb"], dtype=np.float64).reshape(-1)
+        keep += [l, isp, pcb, psb]
+        s.obc[k] = Obc(n, _ip(l), _ip(isp), _dp(pcb), _dp(psb), max(n, 1))
+    return s, keep
+
+
+def make_params(p: dict, *, n: int, tn: float, precision: int = PREC_FP64):
+    s = Params()
+    s.delt = p["dt"]
+    s.g = p["g"]
+    s.hdry = p["hdry"]
+    s.rsqm = p["rsqm"]
+    s.tn = tn
+    s.pi2 = p["pi2"]
+    s.snlt = p["snlt"]
+    s.ritb1 = p["ritb1"]
+    s.iterm = p["iterm"]
+    s.isdry = p["isdry"]
+    s.ndrystp = p["ndrystp"]
+    s.isbal = p["isbal"]
+    s.n = n
+    s.ntstbc = p.get("ntstbc", 0)
+    s.max_sweeps = p.get("max_sweeps", 500)
+    s.precision = precision
+    s.mixed_rsq_factor = p.get("mixed_rsq_factor", 0.0)
+    return s
+
+
+def make_fields(st: dict, *, diag: bool = False, lists: bool = False):
+    """Build a Fields struct over the numpy arrays of a state dict (in place)."""
+    s = Fields()
+    keep = []
+    for k in FIELD_DOUBLE_INOUT + FIELD_IN + FIELD_OUT:
+        a = st.get(k)
+        if a is not None:
+            setattr(s, k, _dp(a))
+    for k in FIELD_INT_INOUT:
+        a = st.get(k)
+        if a is not None:
+            setattr(s, k, _ip(a))
+    for k, side in enumerate(SIDES):
+        a = st["pser"].get(side) if "pser" in st else None
+        if a is not None and a.size:
+            s.pser[k] = _dp(a)
+    if lists:
+        n = st["p"].size
+        for k in ("lwet", "ldry"):
+            if k not in st:
+                st[k] = np.zeros(n, np.int32)
+            setattr(s, k, _ip(st[k]))
+    if diag:
+        n = st["p"].size
+        for k in FIELD_DIAG:
+            if k not in st:
+                st[k] = np.zeros(n)
+            setattr(s, k, _dp(st[k]))
+    return s, keep
+
+
+class CudaLibraryMissing(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load(path: str | os.PathLike | None = None):
+    """Load libefdc_xm.so (built in-tree by build.py).  Fails loudly when it is
+    missing: there is no CPU fallback."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise CudaLibraryMissing(
+            f"{p} not found: build it with `python {PKG_DIR / 'build.py'}` "
+            "(the solver has no CPU fallback)")
+    lib = C.CDLL(str(p))
+    lib.efdc_xm_abi_version.restype = C.c_int32
+    lib.efdc_xm_last_error.restype = C.c_char_p
+    lib.efdc_xm_create.restype = C.c_void_p
+    lib.efdc_xm_create.argtypes = [C.POINTER(Grid), C.c_int32]
+    lib.efdc_xm_destroy.argtypes = [C.c_void_p]
+    for name in ("efdc_xm_step",):
+        fn = getattr(lib, name)
+        fn.restype = C.c_int32
+        fn.argtypes = [C.c_void_p, C.POINTER(Params), C.POINTER(Fields), C.POINTER(Stats)]
+    lib.efdc_xm_upload.restype = C.c_int32
+    lib.efdc_xm_upload.argtypes = [C.c_void_p, C.POINTER(Fields)]
+    lib.efdc_xm_download.restype = C.c_int32
+    lib.efdc_xm_download.argtypes = [C.c_void_p, C.POINTER(Fields)]
+    lib.efdc_xm_step_device.restype = C.c_int32
+    lib.efdc_xm_step_device.argtypes = [C.c_void_p, C.POINTER(Params), C.POINTER(Stats)]
+    lib.efdc_xm_stream.restype = C.c_void_p
+    lib.efdc_xm_stream.argtypes = [C.c_void_p]
+    lib.efdc_xm_kernel_launches.restype = C.c_int64
+    lib.efdc_xm_time_kernels.restype = C.c_int32
+    lib.efdc_xm_time_kernels.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(KTime)]
+    lib.efdc_xm_congrad.restype = C.c_int32
+    lib.efdc_xm_congrad.argtypes = [C.c_void_p] + [_pd] * 8 + [C.c_double, C.c_int32,
+                                                                C.c_int32, _pi, _pd]
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class Solver:
+    """Host-side handle over one efdc_xm context (one basin on one GPU)."""
+
+    def __init__(self, grid: dict, device: int = 0, lib=None):
+        """Create a context for the static model ``grid`` on CUDA device ``device``."""
+        self.lib = lib or load()
+        self._grid, self._keep = make_grid(grid)
+        self.ctx = self.lib.efdc_xm_create(C.byref(self._grid), device)
+        if not self.ctx:
+            raise RuntimeError("efdc_xm_create failed: " + self.last_error())
+        self.la = int(grid["la"])
+        self.lc = int(grid["lc"])
+
+    def last_error(self) -> str:
+        return self.lib.efdc_xm_last_error().decode()
+
+    def close(self):
+        if self.ctx:
+            self.lib.efdc_xm_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):  # pragma: no cover - best effort
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, params: Params, state: dict, *, diag=False, lists=False) -> Stats:
+        f, _k = make_fields(state, diag=diag, lists=lists)
+        st = Stats()
+        rc = self.lib.efdc_xm_step(self.ctx, C.byref(params), C.byref(f), C.byref(st))
+        if rc in (CUDA_ERROR, BAD_ARGUMENT, UNSUPPORTED, DEVICE_TIMEOUT):
+            raise RuntimeError(f"efdc_xm_step: {STATUS_NAMES.get(rc, rc)}: {self.last_error()}")
+        return st
+
+    def upload(self, state: dict):
+        f, _k = make_fields(state)
+        rc = self.lib.efdc_xm_upload(self.ctx, C.byref(f))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_upload: {self.last_error()}")
+
+    def download(self, state: dict, *, diag=False, lists=False):
+        f, _k = make_fields(state, diag=diag, lists=lists)
+        rc = self.lib.efdc_xm_download(self.ctx, C.byref(f))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_download: {self.last_error()}")
+
+    def step_device(self, params: Params) -> Stats:
+        st = Stats()
+        rc = self.lib.efdc_xm_step_device(self.ctx, C.byref(params), C.byref(st))
+        if rc in (CUDA_ERROR, BAD_ARGUMENT, UNSUPPORTED, DEVICE_TIMEOUT):
+            raise RuntimeError(f"efdc_xm_step_device: {STATUS_NAMES.get(rc, rc)}: "
+                               f"{self.last_error()}")
+        return st
+
+    def stream(self) -> int:
+        return int(self.lib.efdc_xm_stream(self.ctx) or 0)
+
+    def time_kernels(self, precision: int, reps: int = 20) -> KTime:
+        kt = KTime()
+        rc = self.lib.efdc_xm_time_kernels(self.ctx, precision, reps, C.byref(kt))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_time_kernels: {self.last_error()}")
+        return kt
+
+    def congrad(self, ccc, ccs, ccn, ccw, cce, ccci, fptmp, p, rsqm, iterm,
+                precision=PREC_FP64):
+        it = C.c_int32(0)
+        rsq = C.c_double(0.0)
+        rc = self.lib.efdc_xm_congrad(self.ctx, _dp(ccc), _dp(ccs), _dp(ccn), _dp(ccw),
+                                      _dp(cce), _dp(ccci), _dp(fptmp), _dp(p),
+                                      float(rsqm), int(iterm), int(precision),
+                                      C.byref(it), C.byref(rsq))
+        return rc, it.value, rsq.value

@@ -1,0 +1,217 @@
+/*
+ * efdc_xm.h -- C-ABI of the B200 external-mode free-surface solver.
+ *
+ * Drop-in for EFDC+ 8.5's 2TL external mode:
+ *   SUBROUTINE CALPUV2C        EFDC/calpuv2c.f90:1-1191  (called at EFDC/hdmt2t.f90:509)
+ *   SUBROUTINE CONGRAD         EFDC/congrad.f90:1-191    (called at EFDC/calpuv2c.f90:409)
+ *   SUBROUTINE SETOPENBC(2)    EFDC/setopenbc.f90, EFDC/setopenbc2.f90
+ *   SUBROUTINE NEGDEP (check)  EFDC/negdep.f90:34-45
+ *
+ * Conventions
+ *   - Every per-cell array is the base address of the Fortran array indexed
+ *     1..LC (or 1..LCM): element L lives at ptr[L-1].  Cells L=2..LA are water
+ *     cells in CELLMAP order (EFDC/cellmap.f90:13-28); L=1 and L=LC are the
+ *     ghost cells, and a missing neighbour is LC (EFDC/cellmap.f90:80-134).
+ *   - Reals are double (the ReleaseDP64 build: /real_size:64).
+ *   - Fortran LOGICAL(4) is passed as int32_t: nonzero = .TRUE. on input;
+ *     the library writes 1 for .TRUE. and 0 for .FALSE.
+ *   - No call aborts the process: failures that STOP in the reference are
+ *     returned as a status code (enum efdc_xm_status) and the last message is
+ *     available from efdc_xm_last_error().
+ *   - A context is bound to one CUDA device and is not thread-safe; use one
+ *     context per host thread.  Calls return after the device work finished.
+ *
+ * The library has no PyTorch dependency.
+ */
+#ifndef EFDC_XM_H
+#define EFDC_XM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EFDC_XM_ABI_VERSION 1
+
+/* Status codes.  The reference STOPs where these are returned. */
+enum efdc_xm_status {
+  EFDC_XM_OK = 0,
+  EFDC_XM_CG_MAXITER = 1,      /* RSQ > RSQM after ITERM iterations: congrad.f90:171-184 */
+  EFDC_XM_WETDRY_MAXSWEEP = 2, /* NCORDRY reached 500: calpuv2c.f90:597-601, 726-749      */
+  EFDC_XM_NEG_DEPTH = 3,       /* some HP <= 0 after the step: negdep.f90:34-45 (non-fatal) */
+  EFDC_XM_NONFINITE = 4,       /* NaN/Inf in the CG scalars or in the new P                  */
+  EFDC_XM_CUDA_ERROR = 5,
+  EFDC_XM_DEVICE_TIMEOUT = 6,  /* a bounded device-side wait ran out                          */
+  EFDC_XM_BAD_ARGUMENT = 7,
+  EFDC_XM_UNSUPPORTED = 8      /* an option this library does not implement (see message)    */
+};
+
+/* Arithmetic of the solve. */
+enum efdc_xm_precision {
+  EFDC_XM_PREC_FP64 = 0,  /* FP64 assembly and FP64 Jacobi-PCG, as the DP build          */
+  EFDC_XM_PREC_MIXED = 1  /* FP64 assembly; FP32 inner PCG with FP64 dot products inside
+                             FP64 iterative refinement r = b - A P; P stays FP64          */
+};
+
+/* One side of open (elevation) boundary cells, e.g. NPBW/LPBW/ISPBW/PCBW/PSBW. */
+typedef struct efdc_xm_obc {
+  int32_t n;           /* NPBW: number of cells on this side                           */
+  const int32_t *l;    /* LPBW(1..n): L index of each boundary cell (setbcs.f90:178)  */
+  const int32_t *ispb; /* ISPBW(1..n): 0 clamped, 1/2 radiation (setopenbc.f90:54)   */
+  const double *pcb;   /* PCBW(LL,M): cosine amplitude G*A*cos(phase), column-major   */
+  const double *psb;   /* PSBW(LL,M): sine amplitude   G*A*sin(phase)                 */
+  int32_t ld;          /* leading dimension of pcb/psb (NPBWM); >= n                   */
+} efdc_xm_obc;
+
+enum { EFDC_XM_OBC_W = 0, EFDC_XM_OBC_E = 1, EFDC_XM_OBC_S = 2, EFDC_XM_OBC_N = 3 };
+
+/* Static model description: copied by efdc_xm_create, not referenced afterwards. */
+typedef struct efdc_xm_grid {
+  int32_t la;                          /* LA: last water cell                        */
+  int32_t lc;                          /* LC = LA+1: ghost cell                      */
+  const int32_t *il, *jl;              /* IL, JL (cellmap.f90:18-19)                 */
+  const int32_t *lnc, *lsc, *lec, *lwc;/* neighbour maps (cellmap.f90:80-134)        */
+  const double *dxyp, *dxyip;          /* aaefdc.f90:2171-2190 metrics               */
+  const double *dxiu, *dyiu, *dxiv, *dyiv, *dxyu, *dxyv;
+  const double *hruo, *hrvo;           /* HRUO=SUBO*DYU/DXU, HRVO=SVBO*DXV/DYV       */
+  const double *subo, *svbo, *sbxo, *sbyo; /* permanent face switches (setbcs.f90:1052) */
+  const double *belv;                  /* bed elevation                              */
+  int32_t mtide;                       /* number of harmonic constituents            */
+  const double *tcp;                   /* TCP(1..mtide): periods (s)                 */
+  efdc_xm_obc obc[4];                  /* W, E, S, N open boundaries                 */
+} efdc_xm_grid;
+
+/* Per-call scalars (values of MODULE GLOBAL at the call). */
+typedef struct efdc_xm_params {
+  double delt;       /* DELT: DT, or DTDYN when ISDYNSTP/=0 (calpuv2c.f90:128-136)   */
+  double g;          /* G                                                             */
+  double hdry;       /* HDRY                                                          */
+  double rsqm;       /* RSQM: absolute squared-residual stop of CONGRAD               */
+  double tn;         /* TN of SETOPENBC: DT*N+TCON*TBEGIN, or TIMESEC                 */
+  double pi2;        /* PI2 = 2*PI with PI=3.1415926535898 (aaefdc.f90:650-651)       */
+  double snlt;       /* SNLT                                                          */
+  double ritb1;      /* RITB1 (1.0 when ISITB=0, caltbxy.f90:104)                     */
+  int32_t iterm;     /* ITERM: CG iteration cap                                       */
+  int32_t isdry;     /* ISDRY: 0, 1..97 (legacy) or 99                                */
+  int32_t ndrystp;   /* NDRYSTP (<0: waste volume of isolated cells)                  */
+  int32_t isbal;     /* ISBAL (keeps QDWASTE when > 0)                                */
+  int32_t n;         /* N, time step counter (for the LDRY list rule)                 */
+  int32_t ntstbc;    /* NTSTBC                                                        */
+  int32_t max_sweeps;/* wet/dry re-solve cap; the reference uses 500                  */
+  int32_t precision; /* enum efdc_xm_precision (ignored by the CPU oracle)             */
+  double mixed_rsq_factor; /* MIXED only: stop when the FP64 RSQ <= factor*RSQM; 0 selects
+                              the default 0.01 (the FP32 path converges past RSQM so that
+                              its surface stays within 1e-6 m of the FP64 solve)        */
+} efdc_xm_params;
+
+/* Per-call arrays.  "in/out" arrays are read and overwritten.  Optional outputs
+ * may be NULL. */
+typedef struct efdc_xm_fields {
+  /* state, in/out */
+  double *p, *hp, *h1p;               /* P, HP, H1P (H1P <- HP at entry, calpuv2c.f90:264) */
+  double *hu, *hv;                    /* HU, HV (recomputed at exit, :896-899)       */
+  double *uhdye, *vhdxe;              /* UHDYE, VHDXE face discharges                */
+  double *sub, *svb, *sbx, *sby;      /* face switches (wet/dry changes them)        */
+  int32_t *lmaskdry;                  /* LMASKDRY (LOGICAL)                          */
+  int32_t *iscdry;                    /* ISCDRY                                      */
+  int32_t *lopenbcdry;                /* LOPENBCDRY (LOGICAL)                        */
+  int32_t *natdry;                    /* NATDRY (isolated-step counter)              */
+  /* explicit terms from the upstream producers, in */
+  const double *fcaxe, *fcaye, *fxe, *fye;
+  const double *tsx, *tsy, *tbx, *tby;
+  const double *qsume;
+  /* per open-boundary cell: PSERT+0.5*PSERZDF+PSERST+0.5*PSERZDS (with the
+   * NPFORT coordinate blend already applied), i.e. FP(L) before the harmonic
+   * sum of setopenbc.f90:47-52.  NULL = zero. */
+  const double *pser[4];
+  /* outputs */
+  double *uhe, *vhe;                  /* unit-width discharges (:432-435)            */
+  double *hpi, *hui, *hvi;            /* reciprocals (:902-906)                      */
+  double *qdwaste, *vdwaste;          /* volume wasting (NDRYSTP<0), optional        */
+  int32_t *lwet, *ldry;               /* LWET(1..LAWET), LDRY(1..LADRY), optional    */
+  /* optional diagnostics: the scaled system of the last sweep, as CONGRAD saw it */
+  double *ccc, *ccs, *ccw, *cce, *ccn, *fptmp;
+} efdc_xm_fields;
+
+typedef struct efdc_xm_stats {
+  int32_t status;       /* enum efdc_xm_status                                   */
+  int32_t iters_last;   /* IDRYTBP: CG iterations of the last solve              */
+  int32_t iters_total;  /* CG iterations summed over the wet/dry sweeps          */
+  int32_t solves;       /* CONGRAD calls (1 + NCORDRY)                           */
+  int32_t lawet, ladry; /* LAWET, LADRY                                          */
+  int32_t n_negdep;     /* cells with HP <= 0                                    */
+  int32_t n_wasted;     /* cells whose volume was wasted (NNATDRY)               */
+  int32_t outer_refinements; /* MIXED: FP64 refinement passes                    */
+  double rsq_last;      /* RSQ at exit of the last solve                         */
+  double ccmnm_last;    /* CCMNM of the last sweep                               */
+} efdc_xm_stats;
+
+typedef struct efdc_xm_ctx efdc_xm_ctx;
+
+/* Version of this header the library was built with. */
+int32_t efdc_xm_abi_version(void);
+
+/* Last error message of the calling thread ("" if none). */
+const char *efdc_xm_last_error(void);
+
+/* Create a solver context on CUDA device `device` for the static model `grid`.
+ * Replaces the first-call block of CALPUV2C (calpuv2c.f90:59-126) and the
+ * static arrays of MODULE GLOBAL it reads.  Returns NULL on failure. */
+efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *grid, int32_t device);
+
+void efdc_xm_destroy(efdc_xm_ctx *ctx);
+
+/* One external-mode step on host arrays: CALL CALPUV2C (hdmt2t.f90:509).
+ * Uploads the fields, runs the whole step on the GPU (assembly, open BCs,
+ * scaling, PCG, back-substitution, continuity, wet/dry sweeps, finalisation,
+ * wet lists, negative-depth check) and writes the outputs back. */
+int32_t efdc_xm_step(efdc_xm_ctx *ctx, const efdc_xm_params *prm,
+                     efdc_xm_fields *f, efdc_xm_stats *stats);
+
+/* Device-resident form of efdc_xm_step for callers that keep the state on the
+ * GPU between steps: upload once, step many times, download when needed. */
+int32_t efdc_xm_upload(efdc_xm_ctx *ctx, const efdc_xm_fields *f);
+int32_t efdc_xm_step_device(efdc_xm_ctx *ctx, const efdc_xm_params *prm,
+                            efdc_xm_stats *stats);
+int32_t efdc_xm_download(efdc_xm_ctx *ctx, efdc_xm_fields *f);
+
+/* Standalone replacement of CONGRAD (congrad.f90:1-191) for callers that
+ * assemble the scaled system themselves (e.g. calpuv9c.f90:446).  Arrays are
+ * 1-based Fortran arrays as above; P is the initial guess and the result.
+ * precision selects FP64 or MIXED.  *iters = ITER at exit (IDRYTBP). */
+int32_t efdc_xm_congrad(efdc_xm_ctx *ctx, const double *ccc, const double *ccs,
+                        const double *ccn, const double *ccw, const double *cce,
+                        const double *ccci, const double *fptmp, double *p,
+                        double rsqm, int32_t iterm, int32_t precision,
+                        int32_t *iters, double *rsq);
+
+/* ---- Extensions with no counterpart in the reference (measurement hooks) ---- */
+
+/* The CUDA stream (cudaStream_t) every call of this context runs on, so a
+ * caller can order its own work or CUDA events against the solver. */
+void *efdc_xm_stream(efdc_xm_ctx *ctx);
+
+/* Number of kernels this library has launched in the process so far. */
+int64_t efdc_xm_kernel_launches(void);
+
+/* Average device time (CUDA events on the context's stream) of the CG
+ * iteration kernels on the system currently assembled in the context:
+ * `reps` matrix-vector (p update + A*p + p.Ap) and update (x, r, r.z, r.r)
+ * launches of the given precision.  Leaves P unchanged. */
+typedef struct efdc_xm_ktime {
+  double ms_matvec;     /* per launch */
+  double ms_update;     /* per launch */
+  int32_t reps;
+  int32_t ncells;       /* water cells, LA-1 */
+  int32_t nslots;       /* tile slots processed per launch (incl. land padding) */
+} efdc_xm_ktime;
+int32_t efdc_xm_time_kernels(efdc_xm_ctx *ctx, int32_t precision, int32_t reps,
+                             efdc_xm_ktime *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EFDC_XM_H */

@@ -1,0 +1,848 @@
+// efdc_oracle.cpp -- TEST INFRASTRUCTURE ONLY: CPU FP64 restatement of EFDC+
+// 8.5 CALPUV2C / CONGRAD / SETOPENBC / SETOPENBC2 / NEGDEP (check part).
+// Parity against the reference is UNPINNED (no compiler, no reference tests);
+// see efdc_oracle.h.  Each block cites the Fortran it restates.
+//
+// Build: g++ -O2 -std=c++17 -fopenmp -ffp-contract=off -fPIC -shared
+// (oracle/Makefile).  -ffp-contract=off keeps every a*b+c as two roundings,
+// as the SSE2 ReleaseDP64 build does.
+
+#include "efdc_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// 1-based view of a caller array: element L is at b[L-1].
+template <class T>
+struct F {
+  T *b;
+  T &operator[](long L) const { return b[L - 1]; }
+};
+
+struct Side {
+  int n = 0;
+  std::vector<int> l, ispb;        // 1..n stored at [ll-1]
+  std::vector<double> pcb, psb;    // [(m-1)*n + (ll-1)]
+};
+
+}  // namespace
+
+struct oracle_ctx {
+  int la = 0, lc = 0, nthreads = 1, noptimal = 1, ldmopt = 1;
+  // static arrays, 1-based (index 0 unused), length lc+2
+  std::vector<int> lnc, lsc, lec, lwc;
+  std::vector<double> dxyp, dxyip, dxiu, dyiu, dxiv, dyiv, dxyu, dxyv, hruo,
+      hrvo, subo, svbo, sbxo, sbyo, belv;
+  int mtide = 0;
+  std::vector<double> tcp;
+  Side side[4];
+  std::vector<int> lobcs;  // S, W, E, N order (setbcs.f90:882-935)
+  // SAVEd work arrays of CALPUV2C / CONGRAD
+  std::vector<double> fp1, fp, fuhdye, fvhdxe, cs, cw, ce, cn, cc, ccs, ccw,
+      cce, ccn, ccc, ccci, fptmp, rcx, rcy, sub1, svb1, fsgzu, fsgzv, uhdy1e,
+      vhdx1e;
+  std::vector<double> pcg, pnv, pev, pwv, psv, rcg, apcg, tmpcg;
+  std::vector<int> oldmask;
+};
+
+namespace {
+
+template <class Fn>
+void for_domains(const oracle_ctx *c, Fn &&fn) {
+  // !$OMP PARALLEL DO over ND=1,NOPTIMAL with LF=2+(ND-1)*LDMOPT (calpuv2c.f90:164-167)
+  const int nopt = c->noptimal, ldm = c->ldmopt, la = c->la;
+#pragma omp parallel for num_threads(nopt) schedule(static, 1) if (nopt > 1)
+  for (int nd = 1; nd <= nopt; ++nd) {
+    const int lf = 2 + (nd - 1) * ldm;
+    const int ll = std::min(lf + ldm - 1, la);
+    for (int L = lf; L <= ll; ++L) fn(L);
+  }
+}
+
+template <class T>
+void copy1(std::vector<T> &dst, const T *src, int lc) {
+  dst.assign(lc + 2, T(0));
+  if (src)
+    for (int L = 1; L <= lc; ++L) dst[L] = src[L - 1];
+}
+
+// CONGRAD body (congrad.f90:54-187) on the context's scaled system.
+// p is the caller's 1-based P. Returns 0 or EFDC_XM_CG_MAXITER / NONFINITE.
+int congrad(oracle_ctx *c, F<double> P, double rsqm, int iterm, int *iters_out,
+            double *rsq_out) {
+  const int la = c->la;
+  const int *LNC = c->lnc.data(), *LSC = c->lsc.data(), *LEC = c->lec.data(),
+            *LWC = c->lwc.data();
+  double *PCG = c->pcg.data(), *PN = c->pnv.data(), *PE = c->pev.data(),
+         *PW = c->pwv.data(), *PS = c->psv.data(), *RCG = c->rcg.data(),
+         *APCG = c->apcg.data(), *TMPCG = c->tmpcg.data();
+  const double *CCC = c->ccc.data(), *CCS = c->ccs.data(), *CCN = c->ccn.data(),
+               *CCW = c->ccw.data(), *CCE = c->cce.data(),
+               *CCCI = c->ccci.data(), *FPTMP = c->fptmp.data();
+
+  // :54-77  neighbour gathers of P, then the initial residual
+  for_domains(c, [&](int L) {
+    PN[L] = P[LNC[L]];
+    PE[L] = P[LEC[L]];
+    PW[L] = P[LWC[L]];
+    PS[L] = P[LSC[L]];
+  });
+  for_domains(c, [&](int L) {
+    RCG[L] = FPTMP[L] - CCC[L] * P[L] - CCN[L] * PN[L] - CCS[L] * PS[L] -
+             CCW[L] * PW[L] - CCE[L] * PE[L];
+  });
+  // :79-88
+  for (int L = 2; L <= la; ++L) PCG[L] = RCG[L] * CCCI[L];
+  double RPCG = 0.;
+  for (int L = 2; L <= la; ++L) RPCG = RPCG + RCG[L] * PCG[L];
+  *rsq_out = 0.;
+  if (RPCG == 0.0) {  // :88 "DS-INTL SINGLE LINE": ITER is left untouched
+    *iters_out = 0;
+    return EFDC_XM_OK;
+  }
+
+  double RSQ = 0.;
+  int iter;
+  const int nopt = c->noptimal, ldm = c->ldmopt;
+  for (iter = 1; iter <= iterm; ++iter) {  // :91
+    double PAPCG = 0., ALPHA = 0., RPCGN = 0., BETA = 0.;
+#pragma omp parallel num_threads(nopt) if (nopt > 1)
+    {
+#pragma omp for schedule(static, 1)
+      for (int nd = 1; nd <= nopt; ++nd) {  // :93-105
+        const int lf = 2 + (nd - 1) * ldm, ll = std::min(lf + ldm - 1, la);
+        for (int L = lf; L <= ll; ++L) {
+          PN[L] = PCG[LNC[L]];
+          PE[L] = PCG[LEC[L]];
+          PW[L] = PCG[LWC[L]];
+          PS[L] = PCG[LSC[L]];
+        }
+      }
+#pragma omp for schedule(static, 1)
+      for (int nd = 1; nd <= nopt; ++nd) {  // :107-116
+        const int lf = 2 + (nd - 1) * ldm, ll = std::min(lf + ldm - 1, la);
+        for (int L = lf; L <= ll; ++L)
+          APCG[L] = CCC[L] * PCG[L] + CCS[L] * PS[L] + CCN[L] * PN[L] +
+                    CCW[L] * PW[L] + CCE[L] * PE[L];
+      }
+#pragma omp single
+      {  // :118-125 serial dot "to prevent roundoff error"
+        PAPCG = 0.;
+        for (int L = 2; L <= la; ++L) PAPCG = PAPCG + APCG[L] * PCG[L];
+        ALPHA = RPCG / PAPCG;
+      }
+#pragma omp for schedule(static, 1)
+      for (int nd = 1; nd <= nopt; ++nd) {  // :127-137
+        const int lf = 2 + (nd - 1) * ldm, ll = std::min(lf + ldm - 1, la);
+        for (int L = lf; L <= ll; ++L) {
+          P[L] = P[L] + ALPHA * PCG[L];
+          RCG[L] = RCG[L] - ALPHA * APCG[L];
+          TMPCG[L] = CCCI[L] * RCG[L];
+        }
+      }
+#pragma omp single
+      {  // :139-149
+        RPCGN = 0.;
+        RSQ = 0.;
+        for (int L = 2; L <= la; ++L) {
+          RPCGN = RPCGN + RCG[L] * TMPCG[L];
+          RSQ = RSQ + RCG[L] * RCG[L];
+        }
+        BETA = RPCGN / RPCG;
+        RPCG = RPCGN;
+      }
+      if (RSQ > rsqm) {  // :151-162
+#pragma omp for schedule(static, 1)
+        for (int nd = 1; nd <= nopt; ++nd) {
+          const int lf = 2 + (nd - 1) * ldm, ll = std::min(lf + ldm - 1, la);
+          for (int L = lf; L <= ll; ++L) PCG[L] = TMPCG[L] + BETA * PCG[L];
+        }
+      }
+    }
+    if (!std::isfinite(RSQ) || !std::isfinite(ALPHA)) {
+      *iters_out = iter;
+      *rsq_out = RSQ;
+      return EFDC_XM_NONFINITE;
+    }
+    if (RSQ <= rsqm) break;  // :165-167
+  }
+  *rsq_out = RSQ;
+  if (RSQ > rsqm) {  // :171-184 (the reference dumps and STOPs)
+    *iters_out = iterm;
+    return EFDC_XM_CG_MAXITER;
+  }
+  *iters_out = iter;  // IDRYTBP = ITER (:187)
+  return EFDC_XM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+oracle_ctx *oracle_create(const efdc_xm_grid *g, int nthreads, int noptimal_cap) {
+  if (!g || g->la < 2 || g->lc != g->la + 1) return nullptr;
+  oracle_ctx *c = new oracle_ctx();
+  c->la = g->la;
+  c->lc = g->lc;
+  c->nthreads = std::max(1, nthreads);
+  // calpuv2c.f90:61-62
+  c->noptimal = std::min(std::min(c->nthreads, std::max(1, noptimal_cap)),
+                         std::max(c->la / 100, 1));
+  c->ldmopt = int(double(c->la - 1) / double(c->noptimal)) + 1;
+  const int lc = c->lc;
+  copy1(c->lnc, g->lnc, lc);
+  copy1(c->lsc, g->lsc, lc);
+  copy1(c->lec, g->lec, lc);
+  copy1(c->lwc, g->lwc, lc);
+  copy1(c->dxyp, g->dxyp, lc);
+  copy1(c->dxyip, g->dxyip, lc);
+  copy1(c->dxiu, g->dxiu, lc);
+  copy1(c->dyiu, g->dyiu, lc);
+  copy1(c->dxiv, g->dxiv, lc);
+  copy1(c->dyiv, g->dyiv, lc);
+  copy1(c->dxyu, g->dxyu, lc);
+  copy1(c->dxyv, g->dxyv, lc);
+  copy1(c->hruo, g->hruo, lc);
+  copy1(c->hrvo, g->hrvo, lc);
+  copy1(c->subo, g->subo, lc);
+  copy1(c->svbo, g->svbo, lc);
+  copy1(c->sbxo, g->sbxo, lc);
+  copy1(c->sbyo, g->sbyo, lc);
+  copy1(c->belv, g->belv, lc);
+  c->mtide = g->mtide;
+  c->tcp.assign(g->tcp ? g->tcp : nullptr, g->tcp ? g->tcp + g->mtide : nullptr);
+  for (int s = 0; s < 4; ++s) {
+    const efdc_xm_obc &o = g->obc[s];
+    Side &d = c->side[s];
+    d.n = o.n;
+    d.l.assign(o.l, o.l + o.n);
+    d.ispb.assign(o.ispb, o.ispb + o.n);
+    d.pcb.assign(size_t(o.n) * std::max(g->mtide, 0), 0.0);
+    d.psb.assign(size_t(o.n) * std::max(g->mtide, 0), 0.0);
+    for (int m = 0; m < g->mtide; ++m)
+      for (int ll = 0; ll < o.n; ++ll) {
+        d.pcb[size_t(m) * o.n + ll] = o.pcb ? o.pcb[size_t(m) * o.ld + ll] : 0.0;
+        d.psb[size_t(m) * o.n + ll] = o.psb ? o.psb[size_t(m) * o.ld + ll] : 0.0;
+      }
+  }
+  // LOBCS order: S, W, E, N
+  const int order[4] = {EFDC_XM_OBC_S, EFDC_XM_OBC_W, EFDC_XM_OBC_E, EFDC_XM_OBC_N};
+  for (int k = 0; k < 4; ++k)
+    for (int l : c->side[order[k]].l) c->lobcs.push_back(l);
+
+  const size_t n = size_t(lc) + 2;
+  for (auto *v : {&c->fp1, &c->fp, &c->fuhdye, &c->fvhdxe, &c->cs, &c->cw,
+                  &c->ce, &c->cn, &c->cc, &c->ccs, &c->ccw, &c->cce, &c->ccn,
+                  &c->ccc, &c->ccci, &c->fptmp, &c->rcx, &c->rcy, &c->sub1,
+                  &c->svb1, &c->fsgzu, &c->fsgzv, &c->uhdy1e, &c->vhdx1e,
+                  &c->pcg, &c->pnv, &c->pev, &c->pwv, &c->psv, &c->rcg,
+                  &c->apcg, &c->tmpcg})
+    v->assign(n, 0.0);
+  c->oldmask.assign(n, 0);
+  // first-call initialisation (calpuv2c.f90:97-123)
+  std::fill(c->rcx.begin(), c->rcx.end(), 1.0);
+  std::fill(c->rcy.begin(), c->rcy.end(), 1.0);
+  c->rcx[1] = c->rcy[1] = 0.;
+  c->rcx[lc] = c->rcy[lc] = 0.;
+  std::fill(c->cc.begin(), c->cc.end(), 1.0);
+  std::fill(c->fsgzu.begin(), c->fsgzu.end(), 1.0);
+  std::fill(c->fsgzv.begin(), c->fsgzv.end(), 1.0);
+  for (int L = 2; L <= c->la; ++L) {
+    c->fsgzu[L] = 0.5 / c->dxyu[L];
+    c->fsgzv[L] = 0.5 / c->dxyv[L];
+  }
+  return c;
+}
+
+void oracle_destroy(oracle_ctx *c) { delete c; }
+
+int oracle_noptimal(const oracle_ctx *c) { return c ? c->noptimal : 0; }
+
+int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
+                efdc_xm_stats *st) {
+  efdc_xm_stats dummy;
+  if (!st) st = &dummy;
+  std::memset(st, 0, sizeof(*st));
+  const int la = c->la, lc = c->lc;
+  const int *LNC = c->lnc.data(), *LSC = c->lsc.data(), *LEC = c->lec.data(),
+            *LWC = c->lwc.data();
+  const double *DXYP = c->dxyp.data(), *DXYIP = c->dxyip.data(),
+               *DXIU = c->dxiu.data(), *DYIU = c->dyiu.data(),
+               *DXIV = c->dxiv.data(), *DYIV = c->dyiv.data(),
+               *DXYU = c->dxyu.data(), *DXYV = c->dxyv.data(),
+               *HRUO = c->hruo.data(), *HRVO = c->hrvo.data(),
+               *SUBO = c->subo.data(), *SVBO = c->svbo.data(),
+               *SBXO = c->sbxo.data(), *SBYO = c->sbyo.data(),
+               *BELV = c->belv.data();
+  double *FP1 = c->fp1.data(), *FP = c->fp.data(), *FUHDYE = c->fuhdye.data(),
+         *FVHDXE = c->fvhdxe.data(), *CS = c->cs.data(), *CW = c->cw.data(),
+         *CE = c->ce.data(), *CN = c->cn.data(), *CC = c->cc.data(),
+         *CCS = c->ccs.data(), *CCW = c->ccw.data(), *CCE = c->cce.data(),
+         *CCN = c->ccn.data(), *CCC = c->ccc.data(), *CCCI = c->ccci.data(),
+         *FPTMP = c->fptmp.data(), *RCX = c->rcx.data(), *RCY = c->rcy.data(),
+         *SUB1 = c->sub1.data(), *SVB1 = c->svb1.data(),
+         *FSGZU = c->fsgzu.data(), *FSGZV = c->fsgzv.data(),
+         *UHDY1E = c->uhdy1e.data(), *VHDX1E = c->vhdx1e.data();
+  int *OLDMASK = c->oldmask.data();
+
+  F<double> P{f->p}, HP{f->hp}, H1P{f->h1p}, HU{f->hu}, HV{f->hv},
+      UHDYE{f->uhdye}, VHDXE{f->vhdxe}, SUB{f->sub}, SVB{f->svb}, SBX{f->sbx},
+      SBY{f->sby};
+  F<int32_t> LMASKDRY{f->lmaskdry}, ISCDRY{f->iscdry},
+      LOPENBCDRY{f->lopenbcdry}, NATDRY{f->natdry};
+  std::vector<double> zeros(size_t(lc) + 1, 0.0);
+  auto cin = [&](const double *p) { return F<const double>{p ? p : zeros.data()}; };
+  F<const double> FCAXE = cin(f->fcaxe), FCAYE = cin(f->fcaye), FXE = cin(f->fxe),
+                  FYE = cin(f->fye), TSX = cin(f->tsx), TSY = cin(f->tsy),
+                  TBX = cin(f->tbx), TBY = cin(f->tby), QSUME = cin(f->qsume);
+  std::vector<double> qdw_local, vdw_local, uhe_l, vhe_l, hpi_l, hui_l, hvi_l;
+  auto opt = [&](double *p, std::vector<double> &store) {
+    if (p) return F<double>{p};
+    store.assign(size_t(lc) + 1, 0.0);
+    return F<double>{store.data()};
+  };
+  F<double> QDWASTE = opt(f->qdwaste, qdw_local), VDWASTE = opt(f->vdwaste, vdw_local),
+            UHE = opt(f->uhe, uhe_l), VHE = opt(f->vhe, vhe_l),
+            HPI = opt(f->hpi, hpi_l), HUI = opt(f->hui, hui_l),
+            HVI = opt(f->hvi, hvi_l);
+
+  const double G = prm->g;
+  const double GI = 1. / G;  // aaefdc.f90:648
+  // calpuv2c.f90:128-136
+  const double DELT = prm->delt;
+  const double DELTD2 = 0.5 * DELT;
+  const double DELTI = 1. / DELT;
+  const double HDRY = prm->hdry;
+  const int ISDRY = prm->isdry, NDRYSTP = prm->ndrystp;
+  const double RITB1 = prm->ritb1, SNLT = prm->snlt;
+  const double FPGXE = 0., FPGYE = 0.;  // BSC <= 1e-6: no baroclinic term
+  const int max_sweeps = prm->max_sweeps > 0 ? prm->max_sweeps : 500;
+
+  int NCORDRY = 0;
+  // :150-157
+  if (ISDRY > 0)
+    for (int L : c->lobcs) LOPENBCDRY[L] = 0;
+
+  std::vector<int> nnatdry_flag(size_t(lc) + 1, 0);
+
+  // ---- first domain loop (:164-293) ----
+  for_domains(c, [&](int L) {
+    if (ISDRY > 0) {  // :172-190
+      ISCDRY[L] = 0;
+      SUB1[L] = SUB[L];
+      SVB1[L] = SVB[L];
+      OLDMASK[L] = LMASKDRY[L];
+      if (NDRYSTP < 0 && prm->isbal > 0) QDWASTE[L] = 0.;
+    }
+    {  // :214-220 explicit external transports
+      const int LS = LSC[L], LW = LWC[L];
+      FUHDYE[L] = UHDYE[L] - DELTD2 * SUB[L] * HRUO[L] * HU[L] * (P[L] - P[LW]) +
+                  SUB[L] * DELT * DXIU[L] *
+                      (DXYU[L] * (TSX[L] - RITB1 * TBX[L]) + FCAXE[L] + FPGXE -
+                       SNLT * FXE[L]);
+      FVHDXE[L] = VHDXE[L] - DELTD2 * SVB[L] * HRVO[L] * HV[L] * (P[L] - P[LS]) +
+                  SVB[L] * DELT * DYIV[L] *
+                      (DXYV[L] * (TSY[L] - RITB1 * TBY[L]) - FCAYE[L] + FPGYE -
+                       SNLT * FYE[L]);
+    }
+    if (ISDRY > 0) {  // :246-253
+      SUB[L] = SUBO[L];
+      SVB[L] = SVBO[L];
+      SBX[L] = SBXO[L];
+      SBY[L] = SBYO[L];
+    }
+    // :256-266 advance the external variables (the 2D ones this library owns)
+    UHDY1E[L] = UHDYE[L];
+    VHDX1E[L] = VHDXE[L];
+    H1P[L] = HP[L];
+    {  // :282-290
+      const double C1 = 0.5 * G;
+      const int LE = LEC[L], LN = LNC[L];
+      FP1[L] = DELTI * DXYP[L] * P[L] -
+               C1 * (UHDYE[LE] - UHDYE[L] + VHDXE[LN] - VHDXE[L]);
+    }
+  });
+
+  int iters_total = 0, solves = 0, last_iters = 0, status = EFDC_XM_OK;
+  double last_rsq = 0., last_ccmnm = 0.;
+
+  for (;;) {  // ---- 1000 CONTINUE (:298) ----
+    // :306-344 new-time-level continuity terms and the coefficients
+    for_domains(c, [&](int L) {
+      double C1 = 0.5 * G;
+      const int LE = LEC[L], LN = LNC[L];
+      FP[L] = FP1[L] - C1 * (SUB[LE] * FUHDYE[LE] - SUB[L] * FUHDYE[L] +
+                             SVB[LN] * FVHDXE[LN] - SVB[L] * FVHDXE[L] -
+                             2.0 * QSUME[L]);
+      C1 = -0.5 * DELTD2 * G;
+      CS[L] = C1 * SVB[L] * HRVO[L] * RCY[L] * HV[L];
+      CW[L] = C1 * SUB[L] * HRUO[L] * RCX[L] * HU[L];
+      CE[L] = C1 * SUB[LE] * HRUO[LE] * RCX[LE] * HU[LE];
+      CN[L] = C1 * SVB[LN] * HRVO[LN] * RCY[LN] * HV[LN];
+      CC[L] = DELTI * DXYP[L] - CS[L] - CW[L] - CE[L] - CN[L];
+    });
+
+    // :349 SETOPENBC(DELTD2,DELTI,HU,HV)  (setopenbc.f90:1-206)
+    if (!c->lobcs.empty()) {
+      const double D_LTD2 = DELTD2, DE_TI = DELTI;
+      const double HDRY2 = 0.2 * HDRY;
+      const double TN = prm->tn;
+      std::vector<double> CCCOS(size_t(std::max(c->mtide, 1))),
+          SSSIN(size_t(std::max(c->mtide, 1)));
+      for (int m = 0; m < c->mtide; ++m) {  // :24-29
+        double TM = std::fmod(TN, c->tcp[m]);
+        TM = prm->pi2 * TM / c->tcp[m];
+        CCCOS[m] = std::cos(TM);
+        SSSIN[m] = std::sin(TM);
+      }
+      auto target = [&](const Side &s, const double *pser, int ll, int L) {
+        // FP(L)=PSERT+...(series part supplied by the caller), then :47-52
+        double v = pser ? pser[ll] : 0.0;
+        for (int m = 0; m < c->mtide; ++m) {
+          const double TC = CCCOS[m], TS = SSSIN[m];
+          v = v + s.pcb[size_t(m) * s.n + ll] * TC + s.psb[size_t(m) * s.n + ll] * TS;
+        }
+        (void)L;
+        return v;
+      };
+      {  // WEST :32-74
+        const Side &s = c->side[EFDC_XM_OBC_W];
+        for (int ll = 0; ll < s.n; ++ll) {
+          const int L = s.l[ll];
+          CC[L] = DELTI * DXYP[L];
+          CS[L] = 0.; CW[L] = 0.; CE[L] = 0.; CN[L] = 0.;
+          if (LOPENBCDRY[L]) continue;
+          FP[L] = target(s, f->pser[EFDC_XM_OBC_W], ll, L);
+          const int LE = LEC[L];
+          if (s.ispb[ll] == 1 || s.ispb[ll] == 2) {
+            const double CET = 0.5 * D_LTD2 * G * HRUO[LE] * RCX[LE] * HU[LE];
+            const double TMP = D_LTD2 * std::sqrt(G * HU[LE]) * DXIU[LE];
+            CC[L] = CET * (1. + TMP) / TMP;
+            CE[L] = -CET;
+            FP[L] = CET * (2. * FP[L] - std::sqrt(G * HU[LE]) * FUHDYE[LE] * DYIU[LE] / HU[LE]) / TMP;
+          } else {
+            const double FP1G = FP[L] / G - HDRY2;
+            double CET;
+            if (FP1G < BELV[L] || FP1G < BELV[LE]) {
+              FP[L] = (BELV[L] + HDRY2) * G;
+              CET = 0.;
+              LOPENBCDRY[L] = 1;
+            } else {
+              CET = 0.5 * D_LTD2 * G * HRUO[LE] * RCX[LE] * HU[LE];
+            }
+            FP[LE] = FP[LE] + CET * FP[L];
+            FP[L] = DE_TI * DXYP[L] * FP[L];
+          }
+        }
+      }
+      {  // EAST :77-118
+        const Side &s = c->side[EFDC_XM_OBC_E];
+        for (int ll = 0; ll < s.n; ++ll) {
+          const int L = s.l[ll];
+          CC[L] = DELTI * DXYP[L];
+          CS[L] = 0.; CW[L] = 0.; CE[L] = 0.; CN[L] = 0.;
+          if (LOPENBCDRY[L]) continue;
+          FP[L] = target(s, f->pser[EFDC_XM_OBC_E], ll, L);
+          if (s.ispb[ll] == 1 || s.ispb[ll] == 2) {
+            const double CWT = 0.5 * D_LTD2 * G * HRUO[L] * RCX[L] * HU[L];
+            const double TMP = D_LTD2 * std::sqrt(G * HU[L]) * DXIU[L];
+            CC[L] = CWT * (1. + TMP) / TMP;
+            CW[L] = -CWT;
+            FP[L] = CWT * (2. * FP[L] + std::sqrt(G * HU[L]) * FUHDYE[L] * DYIU[L] / HU[L]) / TMP;
+          } else {
+            const int LW = LWC[L];
+            const double FP1G = FP[L] / G - HDRY2;
+            double CWT;
+            if (FP1G < BELV[L] || FP1G < BELV[LW]) {
+              FP[L] = (BELV[L] + HDRY2) * G;
+              CWT = 0.;
+              LOPENBCDRY[L] = 1;
+            } else {
+              CWT = 0.5 * D_LTD2 * G * HRUO[L] * RCX[L] * HU[L];
+            }
+            FP[LW] = FP[LW] + CWT * FP[L];
+            FP[L] = DE_TI * DXYP[L] * FP[L];
+          }
+        }
+      }
+      {  // SOUTH :121-163
+        const Side &s = c->side[EFDC_XM_OBC_S];
+        for (int ll = 0; ll < s.n; ++ll) {
+          const int L = s.l[ll];
+          const int LN = LNC[L];
+          CC[L] = DELTI * DXYP[L];
+          CS[L] = 0.; CW[L] = 0.; CE[L] = 0.; CN[L] = 0.;
+          if (LOPENBCDRY[L]) continue;
+          FP[L] = target(s, f->pser[EFDC_XM_OBC_S], ll, L);
+          if (s.ispb[ll] == 1 || s.ispb[ll] == 2) {
+            const double CNT = 0.5 * D_LTD2 * G * HRVO[LN] * RCY[LN] * HV[LN];
+            const double TMP = D_LTD2 * std::sqrt(G * HV[LN]) * DYIV[LN];
+            CC[L] = CNT * (1. + TMP) / TMP;
+            CN[L] = -CNT;
+            FP[L] = CNT * (2. * FP[L] - std::sqrt(G * HV[LN]) * FVHDXE[LN] * DXIV[LN] / HV[LN]) / TMP;
+          } else {
+            const double FP1G = FP[L] / G - HDRY2;
+            double CNT;
+            if (FP1G < BELV[L] || FP1G < BELV[LN]) {
+              FP[L] = (BELV[L] + HDRY2) * G;
+              CNT = 0.;
+              LOPENBCDRY[L] = 1;
+            } else {
+              CNT = 0.5 * D_LTD2 * G * HRVO[LN] * RCY[LN] * HV[LN];
+            }
+            FP[LN] = FP[LN] + CNT * FP[L];
+            FP[L] = DE_TI * DXYP[L] * FP[L];
+          }
+        }
+      }
+      {  // NORTH :166-206
+        const Side &s = c->side[EFDC_XM_OBC_N];
+        for (int ll = 0; ll < s.n; ++ll) {
+          const int L = s.l[ll];
+          const int LS = LSC[L];
+          CC[L] = DELTI * DXYP[L];
+          CS[L] = 0.; CW[L] = 0.; CE[L] = 0.; CN[L] = 0.;
+          if (LOPENBCDRY[L]) continue;
+          FP[L] = target(s, f->pser[EFDC_XM_OBC_N], ll, L);
+          if (s.ispb[ll] == 1 || s.ispb[ll] == 2) {
+            const double CST = 0.5 * D_LTD2 * G * HRVO[L] * RCY[L] * HV[L];
+            const double TMP = D_LTD2 * std::sqrt(G * HV[L]) * DYIV[L];
+            CC[L] = CST * (1. + TMP) / TMP;
+            CS[L] = -CST;
+            FP[L] = CST * (2. * FP[L] + std::sqrt(G * HV[L]) * FVHDXE[L] * DXIV[L] / HV[L]) / TMP;
+          } else {
+            const double FP1G = FP[L] / G - HDRY2;
+            double CST;
+            if (FP1G < BELV[L] || FP1G < BELV[LS]) {
+              FP[L] = (BELV[L] + HDRY2) * G;
+              CST = 0.;
+              LOPENBCDRY[L] = 1;
+            } else {
+              CST = 0.5 * D_LTD2 * G * HRVO[L] * RCY[L] * HV[L];
+            }
+            FP[LS] = FP[LS] + CST * FP[L];
+            FP[L] = DE_TI * DXYP[L] * FP[L];
+          }
+        }
+      }
+    }
+
+    // :360-377 minimum diagonal (order-free), FPTMP=FP
+    double CCMNM = 1.e+18;
+    for (int L = 2; L <= la; ++L) {
+      CCMNM = std::min(CCMNM, CC[L]);
+      FPTMP[L] = FP[L];
+    }
+    const double CCMNMI = 1. / CCMNM;
+    // :380 SETOPENBC2 (setopenbc2.f90:17-46)
+    {
+      const Side &w = c->side[EFDC_XM_OBC_W], &e = c->side[EFDC_XM_OBC_E],
+                 &s = c->side[EFDC_XM_OBC_S], &n = c->side[EFDC_XM_OBC_N];
+      for (int ll = 0; ll < w.n; ++ll)
+        if (w.ispb[ll] == 0) CW[LEC[w.l[ll]]] = 0.;
+      for (int ll = 0; ll < e.n; ++ll)
+        if (e.ispb[ll] == 0) CE[LWC[e.l[ll]]] = 0.;
+      for (int ll = 0; ll < s.n; ++ll)
+        if (s.ispb[ll] == 0) CS[LNC[s.l[ll]]] = 0.;
+      for (int ll = 0; ll < n.n; ++ll)
+        if (n.ispb[ll] == 0) CN[LSC[n.l[ll]]] = 0.;
+    }
+    // :384-399 scale by the minimum diagonal
+    for_domains(c, [&](int L) {
+      CCS[L] = CS[L] * CCMNMI;
+      CCW[L] = CW[L] * CCMNMI;
+      CCE[L] = CE[L] * CCMNMI;
+      CCN[L] = CN[L] * CCMNMI;
+      CCC[L] = CC[L] * CCMNMI;
+      FPTMP[L] = FPTMP[L] * CCMNMI;
+      CCCI[L] = 1. / CCC[L];
+    });
+
+    // :409 CONGRAD
+    int iters = 0;
+    double rsq = 0.;
+    const int cg = congrad(c, P, prm->rsqm, prm->iterm, &iters, &rsq);
+    iters_total += iters;
+    last_iters = iters;
+    last_rsq = rsq;
+    last_ccmnm = CCMNM;
+    ++solves;
+    if (cg != EFDC_XM_OK) {
+      status = cg;
+      break;
+    }
+
+    // :416-437 face discharges
+    for_domains(c, [&](int L) {
+      const int LS = LSC[L], LW = LWC[L];
+      UHDYE[L] = SUB[L] * (FUHDYE[L] - DELTD2 * HRUO[L] * RCX[L] * HU[L] * (P[L] - P[LW]));
+      VHDXE[L] = SVB[L] * (FVHDXE[L] - DELTD2 * HRVO[L] * RCY[L] * HV[L] * (P[L] - P[LS]));
+    });
+    for_domains(c, [&](int L) {
+      UHE[L] = UHDYE[L] * DYIU[L];
+      VHE[L] = VHDXE[L] * DXIV[L];
+    });
+    // :466-486 continuity
+    for_domains(c, [&](int L) {
+      const int LE = LEC[L], LN = LNC[L];
+      HP[L] = H1P[L] + DELTD2 * DXYIP[L] *
+                           (2. * QSUME[L] - (UHDYE[LE] + UHDY1E[LE] - UHDYE[L] - UHDY1E[L] +
+                                             VHDXE[LN] + VHDX1E[LN] - VHDXE[L] - VHDX1E[L]));
+    });
+    // :489-535 open boundaries
+    for (int L : c->lobcs) {
+      HP[L] = GI * P[L] - BELV[L];
+      if (ISDRY > 0) {
+        if ((LOPENBCDRY[L] || (H1P[L] < 0.9 * HDRY && HP[L] < H1P[L]) || HP[L] < 0.) &&
+            ISCDRY[L] == 0) {
+          if (HP[L] <= 0. && LOPENBCDRY[L]) {
+            HP[L] = 0.2 * HDRY;
+          } else {
+            HP[L] = std::min(std::max(H1P[L], 0.1 * HDRY), 0.9 * HDRY);
+          }
+          ISCDRY[L] = 1;
+          const int LE = LEC[L], LN = LNC[L];
+          SUB[L] = 0.; SVB[L] = 0.; SUB[LE] = 0.; SVB[LN] = 0.;
+          SBX[L] = 0.; SBY[L] = 0.; SBX[LE] = 0.; SBY[LN] = 0.;
+          UHDYE[L] = 0.; UHDYE[LE] = 0.; VHDXE[L] = 0.; VHDXE[LN] = 0.;
+          LOPENBCDRY[L] = 1;
+          CC[L] = DELTI * DXYP[L];
+          P[L] = (HP[L] + BELV[L]) * G;
+          FP1[L] = DELTI * DXYP[L] * P[L];
+        }
+      }
+    }
+    // :557-571 intermediate P update
+    if (ISDRY > 0) for_domains(c, [&](int L) { P[L] = G * (HP[L] + BELV[L]); });
+
+    // :574-603 legacy drying check, ISDRY 1..97 (serial in the reference)
+    if (ISDRY > 0 && ISDRY < 98) {
+      int ICORDRY = 0;
+      for (int L = 2; L <= la; ++L) {
+        const int LE = LEC[L], LN = LNC[L];
+        if (HP[L] <= HDRY) {
+          if (ISCDRY[L] == 0) {
+            ISCDRY[L] = 1;
+            ICORDRY = 1;
+          }
+          SUB[L] = 0.; SVB[L] = 0.; SUB[LE] = 0.; SVB[LN] = 0.;
+          SBX[L] = 0.; SBY[L] = 0.; SBX[LE] = 0.; SBY[LN] = 0.;
+        }
+      }
+      if (ICORDRY == 1) {
+        ++NCORDRY;
+        if (NCORDRY < max_sweeps) continue;
+        status = EFDC_XM_WETDRY_MAXSWEEP;
+        break;
+      }
+    }
+
+    // :606-734 ISDRY=99 drying/rewetting.  Restated with the 1-thread (serial
+    // L-order) semantics: the reference's OMP split can race on faces shared
+    // by two domains; the serial order is its thread-count-1 result.
+    if (ISDRY == 99) {
+      const double HDRY2 = 2. * HDRY;
+      const double HDRY90 = 0.9 * HDRY;
+      int ICORDRY = 0;
+      for (int L = 2; L <= la; ++L) {
+        const int LW = LWC[L], LE = LEC[L], LS = LSC[L], LN = LNC[L];
+        if (HP[L] <= HDRY) {
+          const double SUBW = SUB[L], SUBE = SUB[LE], SVBS = SVB[L], SVBN = SVB[LN];
+          const double DHPDT = (HP[L] - H1P[L]);
+          if (DHPDT > 0.0) {
+            SUB[L] = 0.0; SUB[LE] = 0.0; SVB[L] = 0.0; SVB[LN] = 0.0;
+            SBX[L] = 0.0; SBX[LE] = 0.0; SBY[L] = 0.0; SBY[LN] = 0.0;
+            const double DHPDT2 = (HDRY - H1P[L]) * 0.01;
+            if (DHPDT > DHPDT2) {
+              if (SUBO[L] > 0.5)
+                if (UHDYE[L] > 0.0 && HP[LW] > HDRY2) { SUB[L] = SUBO[L]; SBX[L] = SBXO[L]; }
+              if (SUBO[LE] > 0.5)
+                if (UHDYE[LE] < 0.0 && HP[LE] > HDRY2) { SUB[LE] = SUBO[LE]; SBX[LE] = SBXO[LE]; }
+              if (SVBO[L] > 0.5)
+                if (VHDXE[L] > 0.0 && HP[LS] > HDRY2) { SVB[L] = SVBO[L]; SBY[L] = SBYO[L]; }
+              if (SVBO[LN] > 0.5)
+                if (VHDXE[LN] < 0.0 && HP[LN] > HDRY2) { SVB[LN] = SVBO[LN]; SBY[LN] = SBYO[LN]; }
+              const double RDRY = SUB[L] + SUB[LE] + SVB[L] + SVB[LN];
+              ISCDRY[L] = (RDRY < 0.5) ? 1 : 0;
+              if (std::fabs(SUB[L] - SUBW) > 0.5) ICORDRY = 1;
+              else if (std::fabs(SUB[LE] - SUBE) > 0.5) ICORDRY = 1;
+              else if (std::fabs(SVB[L] - SVBS) > 0.5) ICORDRY = 1;
+              else if (std::fabs(SVB[LN] - SVBN) > 0.5) ICORDRY = 1;
+            } else {
+              if (ISCDRY[L] == 0) {
+                ISCDRY[L] = 1;
+                ICORDRY = 1;
+              }
+            }
+          } else if (HP[L] < HDRY90 || H1P[L] < HDRY) {
+            SUB[L] = 0.0; SUB[LE] = 0.0; SVB[L] = 0.0; SVB[LN] = 0.0;
+            SBX[L] = 0.0; SBX[LE] = 0.0; SBY[L] = 0.0; SBY[LN] = 0.0;
+            if (ISCDRY[L] == 0) {
+              ISCDRY[L] = 1;
+              ICORDRY = 1;
+            }
+          }
+        }
+      }
+      if (ICORDRY > 0) {
+        ++NCORDRY;
+        if (NCORDRY < max_sweeps) continue;
+        status = EFDC_XM_WETDRY_MAXSWEEP;
+        break;
+      }
+    }
+    break;
+  }
+
+  st->iters_last = last_iters;
+  st->iters_total = iters_total;
+  st->solves = solves;
+  st->rsq_last = last_rsq;
+  st->ccmnm_last = last_ccmnm;
+  if (status == EFDC_XM_CG_MAXITER || status == EFDC_XM_NONFINITE ||
+      status == EFDC_XM_WETDRY_MAXSWEEP) {
+    st->status = status;
+    return status;
+  }
+
+  // ---- final domain loop (:829-969), 1-thread order: volume wasting for all
+  // cells first, then the depth updates that read neighbour HP.
+  int n_wasted = 0;
+  if (ISDRY > 0 && NDRYSTP < 0) {  // :838-889
+    const int NTMP = std::abs(NDRYSTP);
+    for (int L = 2; L <= la; ++L) {
+      if (HP[L] >= HDRY) {
+        const int LW = LWC[L], LE = LEC[L], LS = LSC[L], LN = LNC[L];
+        const double RDRY = SUB[L] + SUB[LE] + SVB[L] + SVB[LN];
+        if (RDRY > 0.5) {
+          NATDRY[L] = 0;
+        } else {
+          NATDRY[L] = NATDRY[L] + 1;
+          if (NATDRY[L] > NTMP) {
+            double RVAL = 0.0;
+            if (SUBO[LE] > 0.5 && BELV[LE] < BELV[L]) RVAL = RVAL + 1.;
+            if (SUBO[L] > 0.5 && BELV[LW] < BELV[L]) RVAL = RVAL + 1.;
+            if (SVBO[LN] > 0.5 && BELV[LN] < BELV[L]) RVAL = RVAL + 1.;
+            if (SVBO[L] > 0.5 && BELV[LS] < BELV[L]) RVAL = RVAL + 1.;
+            if (RVAL > 0. || HP[L] < HDRY * 2.) {
+              const double HOLDTMP = HP[L];
+              H1P[L] = HP[L];
+              HP[L] = 0.90 * HDRY;
+              NATDRY[L] = 0;
+              QDWASTE[L] = DELTI * DXYP[L] * (HOLDTMP - HP[L]);
+              VDWASTE[L] = VDWASTE[L] + DXYP[L] * (HOLDTMP - HP[L]);
+              nnatdry_flag[L] = 1;
+              ++n_wasted;
+            }
+          }
+        }
+      }
+    }
+  }
+  for_domains(c, [&](int L) {
+    if (ISDRY == 0) P[L] = G * (HP[L] + BELV[L]);  // :893-897
+  });
+  for_domains(c, [&](int L) {  // :898-906
+    const int LS = LSC[L], LW = LWC[L];
+    HU[L] = (DXYP[L] * HP[L] + DXYP[LW] * HP[LW]) * FSGZU[L];
+    HV[L] = (DXYP[L] * HP[L] + DXYP[LS] * HP[LS]) * FSGZV[L];
+  });
+  for_domains(c, [&](int L) {
+    HPI[L] = 1. / HP[L];
+    HUI[L] = 1. / HU[L];
+    HVI[L] = 1. / HV[L];
+  });
+  if (ISDRY > 0) {  // :910-931
+    for_domains(c, [&](int L) {
+      LMASKDRY[L] = 1;
+      if (HP[L] < HDRY) {
+        const int LE = LEC[L], LN = LNC[L];
+        int IUW = 0, IUE = 0, IVS = 0, IVN = 0;
+        if (SUB1[L] < 0.5 && SUB[L] < 0.5) IUE = 1;
+        if (SUB1[LE] < 0.5 && SUB[LE] < 0.5) IUW = 1;
+        if (SVB1[L] < 0.5 && SVB[L] < 0.5) IVS = 1;
+        if (SVB1[LN] < 0.5 && SVB[LN] < 0.5) IVN = 1;
+        if (IUW + IUE + IVS + IVN == 4) LMASKDRY[L] = 0;
+      }
+    });
+  }
+  // :1003-1025 wasted cells: H1P reset, QDWASTE kept only with ISBAL>0
+  if (n_wasted > 0) {
+    for (int L = 2; L <= la; ++L)
+      if (nnatdry_flag[L]) {
+        H1P[L] = 0.90 * HDRY;
+        if (prm->isbal == 0) QDWASTE[L] = 0.0;
+      }
+  }
+  // NEGDEP check (negdep.f90:34-45)
+  int nneg = 0;
+  for (int L = 2; L <= la; ++L)
+    if (HP[L] <= 0.) ++nneg;
+  // wet/dry cell lists (:1061-1080)
+  int lawet = 0, ladry = 0;
+  if (ISDRY == 0) {
+    lawet = la - 1;
+    if (f->lwet)
+      for (int L = 2; L <= la; ++L) f->lwet[L - 2] = L;
+  } else {
+    for (int L = 2; L <= la; ++L) {
+      if (LMASKDRY[L]) {
+        if (f->lwet) f->lwet[lawet] = L;
+        ++lawet;
+      } else if (OLDMASK[L] || prm->n < prm->ntstbc + 1) {
+        if (f->ldry) f->ldry[ladry] = L;
+        ++ladry;
+      }
+    }
+  }
+  st->lawet = lawet;
+  st->ladry = ladry;
+  st->n_negdep = nneg;
+  st->n_wasted = n_wasted;
+  for (int L = 2; L <= la; ++L)
+    if (!std::isfinite(P[L])) {
+      status = EFDC_XM_NONFINITE;
+      break;
+    }
+  if (status == EFDC_XM_OK && nneg > 0) status = EFDC_XM_NEG_DEPTH;
+  // optional diagnostics of the last sweep
+  if (f->ccc) for (int L = 1; L <= lc; ++L) f->ccc[L - 1] = CCC[L];
+  if (f->ccs) for (int L = 1; L <= lc; ++L) f->ccs[L - 1] = CCS[L];
+  if (f->ccw) for (int L = 1; L <= lc; ++L) f->ccw[L - 1] = CCW[L];
+  if (f->cce) for (int L = 1; L <= lc; ++L) f->cce[L - 1] = CCE[L];
+  if (f->ccn) for (int L = 1; L <= lc; ++L) f->ccn[L - 1] = CCN[L];
+  if (f->fptmp) for (int L = 1; L <= lc; ++L) f->fptmp[L - 1] = FPTMP[L];
+  st->status = status;
+  return status;
+}
+
+int oracle_congrad(oracle_ctx *c, const double *ccc, const double *ccs,
+                   const double *ccn, const double *ccw, const double *cce,
+                   const double *ccci, const double *fptmp, double *p,
+                   double rsqm, int iterm, int *iters, double *rsq) {
+  const int lc = c->lc;
+  for (int L = 1; L <= lc; ++L) {
+    c->ccc[L] = ccc[L - 1];
+    c->ccs[L] = ccs[L - 1];
+    c->ccn[L] = ccn[L - 1];
+    c->ccw[L] = ccw[L - 1];
+    c->cce[L] = cce[L - 1];
+    c->ccci[L] = ccci[L - 1];
+    c->fptmp[L] = fptmp[L - 1];
+  }
+  int it = 0;
+  double r = 0.;
+  const int s = congrad(c, F<double>{p}, rsqm, iterm, &it, &r);
+  if (iters) *iters = it;
+  if (rsq) *rsq = r;
+  return s;
+}
+
+}  // extern "C"

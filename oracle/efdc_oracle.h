@@ -1,0 +1,55 @@
+/*
+ * efdc_oracle.h -- TEST INFRASTRUCTURE ONLY (the checker, never the product).
+ *
+ * CPU FP64 restatement of EFDC+ 8.5's 2TL external mode, used by tests/ and by
+ * bench.py's CPU-baseline leg to check and time the CUDA library.  Nothing in
+ * the shipped library links or calls this code.
+ *
+ * Parity status: UNPINNED by the reference.  EFDC+ is Intel-Fortran-only
+ * (IFPORT, Windows NetCDF libraries), no Fortran compiler exists in this
+ * build environment, and the reference ships no tests, golden vectors or
+ * result files for this path.  The restatement is instead cross-checked by
+ * independent properties (direct sparse solve of the assembled system, lake
+ * at rest, mirror symmetry, volume telescoping, thread-count invariance); see
+ * tests/test_oracle_*.py.
+ *
+ * Arithmetic rules followed so that the statement-level rounding matches the
+ * ReleaseDP64 build (/real_size:64 /fp:source, no /Qx => SSE2, no FMA):
+ *   - FP64 everywhere, compiled with -ffp-contract=off, no -ffast-math;
+ *   - Fortran left-to-right evaluation of each statement, same statement order;
+ *   - serial, L-ordered dot products (congrad.f90:118-149);
+ *   - libm sin/cos/sqrt/fmod.
+ */
+#ifndef EFDC_ORACLE_H
+#define EFDC_ORACLE_H
+
+#include "../include/efdc_xm.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_ctx oracle_ctx;
+
+/* nthreads: NTHREADS of the reference; noptimal_cap: the "8" of
+ * NOPTIMAL=MIN(NTHREADS,8,MAX(LA/100,1)) (calpuv2c.f90:61); pass 8 for the
+ * reference behaviour, or a larger cap to use more host cores. */
+oracle_ctx *oracle_create(const efdc_xm_grid *grid, int nthreads, int noptimal_cap);
+void oracle_destroy(oracle_ctx *c);
+int oracle_noptimal(const oracle_ctx *c);
+
+/* One CALPUV2C call (calpuv2c.f90:128-1187 restricted to BSC=0, MDCHH=0,
+ * ISITB=0, ISVEG=0, ISGWIE=0, IGRIDV=0). Returns the status code. */
+int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
+                efdc_xm_stats *st);
+
+/* CONGRAD on a caller-assembled scaled system (congrad.f90:54-187). */
+int oracle_congrad(oracle_ctx *c, const double *ccc, const double *ccs,
+                   const double *ccn, const double *ccw, const double *cce,
+                   const double *ccci, const double *fptmp, double *p,
+                   double rsqm, int iterm, int *iters, double *rsq);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

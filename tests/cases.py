@@ -1,0 +1,35 @@
+"""Seeded scenario cases shared by the CPU and GPU tests (small sizes)."""
+from __future__ import annotations
+
+import numpy as np
+
+import scenario as S
+
+# name -> (builder, steps, tidal-time multiplier)
+GOLDEN = ("basin_fp64", "radiation_all_sides", "tidal_flat_99", "legacy_dry_1", "noise_forcing")
+
+
+def build(name):
+    if name == "basin_fp64":  # config-1 layout, 12 steps
+        return S.config1(seed=11), 12, 1.0
+    if name == "radiation_all_sides":
+        scn = S.make_scenario(48, 36, seed=12, obc_sides=("W", "E", "S", "N"), ispb=1,
+                              amp=0.3, dt=20.0, land_frac=0.05, explicit_noise=1e-4)
+        return scn, 10, 20.0
+    if name == "tidal_flat_99":
+        return S.tidal_flat(n=48, seed=13, dt=5.0), 40, 60.0
+    if name == "legacy_dry_1":
+        scn = S.tidal_flat(n=40, seed=14, dt=5.0)
+        scn.params["isdry"] = 1
+        scn.params["ndrystp"] = 0
+        return scn, 30, 60.0
+    if name == "noise_forcing":  # clamped W + radiation E, explicit terms
+        scn = S.make_scenario(60, 40, seed=15, obc_sides=("W",), amp=0.4, dt=10.0,
+                              explicit_noise=3e-4, datum=35.0, snlt=1.0)
+        return scn, 10, 10.0
+    raise KeyError(name)
+
+
+def state_err(a, b, la, key="p", g=S.G):
+    d = np.abs(a[key][1:la] - b[key][1:la])
+    return float(d.max() / (g if key == "p" else 1.0))

@@ -1,0 +1,89 @@
+"""CPU checks of the C-ABI library: it loads, exports every function declared
+in include/efdc_xm.h, and the ctypes mirror matches the C struct layout.
+No compute call is made without a GPU."""
+import ctypes as C
+import json
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+import efdc_xm as X
+
+REPO = Path(__file__).resolve().parents[1]
+HEADER = REPO / "include" / "efdc_xm.h"
+
+
+def declared_functions():
+    txt = HEADER.read_text()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(efdc_xm_\w+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = X.load()
+    out = subprocess.run(["nm", "-D", "--defined-only", str(X.LIB_PATH)], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (efdc_xm_\w+)", out))
+    for fn in declared_functions():
+        assert fn in exported, fn
+        assert getattr(lib, fn) is not None
+
+
+def test_abi_version():
+    lib = X.load()
+    m = re.search(r"#define EFDC_XM_ABI_VERSION (\d+)", HEADER.read_text())
+    assert lib.efdc_xm_abi_version() == int(m.group(1))
+
+
+STRUCTS = {
+    "efdc_xm_obc": X.Obc, "efdc_xm_grid": X.Grid, "efdc_xm_params": X.Params,
+    "efdc_xm_fields": X.Fields, "efdc_xm_stats": X.Stats,
+}
+
+
+def test_ctypes_layout_matches_header(tmp_path):
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){",
+             'printf("{");']
+    first = True
+    for cname, cls in STRUCTS.items():
+        for fname, _ in cls._fields_:
+            sep = "" if first else ","
+            first = False
+            lines.append(f'printf("{sep}\\"{cname}.{fname}\\": %zu", offsetof({cname}, {fname}));')
+        lines.append(f'printf(",\\"{cname}.__size__\\": %zu", sizeof({cname}));')
+    lines += ['printf("}");', "return 0;}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", str(src), "-o", str(exe)], check=True)
+    got = json.loads(subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout)
+    for cname, cls in STRUCTS.items():
+        for fname, _ in cls._fields_:
+            assert got[f"{cname}.{fname}"] == getattr(cls, fname).offset, f"{cname}.{fname}"
+        assert got[f"{cname}.__size__"] == C.sizeof(cls), cname
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-GPU behaviour")
+def test_create_without_gpu_fails_loudly():
+    """No CPU fallback: without a device the context cannot be created."""
+    import scenario as S
+    scn = S.make_scenario(12, 10, seed=1)
+    with pytest.raises(RuntimeError, match="efdc_xm_create failed"):
+        X.Solver(scn.grid)
+
+
+def test_fortran_shim_binds_declared_symbols():
+    """The Fortran binding module names exactly the C entry points it uses."""
+    f90 = (REPO / "efdcplus8.5_b200" / "fortran" / "efdc_xm_bind.f90").read_text()
+    bound = set(re.findall(r"BIND\(C,\s*NAME='(efdc_xm_\w+)'\)", f90, flags=re.I))
+    assert bound and bound <= set(declared_functions())
