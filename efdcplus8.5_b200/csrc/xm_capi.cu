@@ -72,7 +72,7 @@ struct DevBuf {
 struct efdc_xm_ctx {
   int device = 0;
   int la = 0, lc = 0;
-  int ntile = 0, nslot = 0, grid = 1, nsm = 0;
+  int ntile = 0, nslot = 0, grid = 1, grid_cg = 1, grid_mv64 = 1, grid_cg32 = 1, nsm = 0;
   cudaStream_t stream = nullptr;
   std::vector<DevBuf> bufs;
   // host copies of the layout
@@ -116,7 +116,7 @@ struct efdc_xm_ctx {
     bufs.push_back(b);
     return static_cast<T *>(b.p);
   }
-  xm::Launch L() const { return xm::Launch{grid, ntile, stream}; }
+  xm::Launch L() const { return xm::Launch{grid, grid_cg, grid_mv64, grid_cg32, ntile, stream}; }
 };
 
 namespace {
@@ -239,10 +239,10 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double rsqm_ref, int iterm, int *iter
                 int *status, int *outer, double factor) {
   const xm::Launch l = c->L();
   // the FP32 path stops on the FP64 residual, past the reference's RSQM
-  const double rsqm = rsqm_ref * (factor > 0 ? factor : 0.01);
+  const double rsqm = rsqm_ref * (factor > 0 ? factor : 0.1);
   const int total_cap = 2 * iterm + 50;
   const int max_outer = 30;
-  const double rel_tol = 1e-4;
+  const double rel_tol = 1e-6;  // inner: |r| down 1e-6 (FP32 reaches ~1e-7 here)
   // reset the solve bookkeeping
   int rc = read_ctl(c);
   if (rc) return rc;
@@ -428,8 +428,13 @@ efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *g, int32_t device) {
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail("stream creation failed");
   cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
-  const int occ = std::min(xm::occupancy_blocks_per_sm(), xm::occupancy_blocks_per_sm_mixed());
+  const int occ = xm::occupancy_blocks_per_sm();
+  const int occ_cg = xm::occupancy_blocks_per_sm_cg();
+  const int occ_cg32 = xm::occupancy_blocks_per_sm_mixed();
   c->grid = std::max(1, std::min(c->ntile - 1, c->nsm * occ));
+  c->grid_cg = std::max(1, std::min((c->ntile - 1 + 3) / 4, c->nsm * occ_cg));
+  c->grid_cg32 = std::max(1, std::min((c->ntile - 1 + 3) / 4, c->nsm * occ_cg32));
+  c->grid_mv64 = std::max(1, std::min((c->ntile - 1 + 3) / 4, c->nsm * xm::occupancy_blocks_per_sm_mv64()));
 
   std::vector<int4> tnbr(c->ntile, int4{0, 0, 0, 0});
   std::vector<uint8_t> kind(c->nslot, xm::LAND);
@@ -526,7 +531,7 @@ efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *g, int32_t device) {
   Y.r32 = Fl(); Y.pa32 = Fl(); Y.pb32 = Fl(); Y.ap32 = Fl(); Y.x32 = Fl();
   c->ptmp = D();
   c->ctl = c->alloc<Ctl>(1);
-  c->part = c->alloc<double>(size_t(2) * c->grid + 64);
+  c->part = c->alloc<double>(size_t(2) * std::max(c->grid, std::max(c->grid_cg, c->grid_cg32)) + 64);
   if (!Y.x32 || !c->ctl || !c->part) return bail("cudaMalloc failed (device memory)");
   if (cudaHostAlloc(reinterpret_cast<void **>(&c->ctl_h), sizeof(Ctl), cudaHostAllocDefault) != cudaSuccess)
     return bail("cudaHostAlloc failed");

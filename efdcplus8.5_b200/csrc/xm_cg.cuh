@@ -1,0 +1,130 @@
+// xm_cg.cuh -- bodies of the CG iteration kernels, shared by the FP64 drop-in
+// (xm_step.cu, compiled without FMA contraction so each statement rounds as in
+// congrad.f90) and the FP32 inner solve of the MIXED form (xm_mixed.cu).
+//
+// A thread owns 4 consecutive cells of a tile row (see RowGeo).  Land slots
+// are inert by construction (r = p = 0, CCC = 1, couplings 0), so the cell
+// loops run unconditionally; only the residual kernels, which read P at
+// land slots (P(LC), the ghost value), mask with the slot kind.
+#pragma once
+
+#include "xm_common.cuh"
+
+namespace xm {
+
+__device__ __forceinline__ float rcpT(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcpT(double x) { return 1. / x; }
+
+// The CG kernels loop over the active tiles, 4 per CTA iteration; past the
+// end a thread works on tile 0 (the ghost tile, all inert) with stores off,
+// so that every lane of a row takes part in the shuffles.
+#define CG_TILE_LOOP(ntile)                                                         \
+  const int sub_ = threadIdx.x / TPT, q_ = threadIdx.x % TPT;                       \
+  for (int base_ = blockIdx.x * TILES_PER_CTA; base_ < (ntile) - 1;                 \
+       base_ += gridDim.x * TILES_PER_CTA)
+
+#define CG_TILE_GEO(S)                                                              \
+  const int ti_ = base_ + sub_;                                                     \
+  const bool valid = ti_ < ntile - 1;                                               \
+  const RowGeo g = row_geo((S).tnbr, valid ? ti_ + 1 : 0, q_)
+
+// PCG = CCCI*RCG + BETA*PCG (congrad.f90:133-159) on the cell's row vector and
+// its N/S rows and E/W neighbours, then APCG = CCC*P + CCS*PS + CCN*PN + CCW*PW
+// + CCE*PE (congrad.f90:114).  Stores p_new and Ap; returns the cell part of
+// p.Ap.  With asym == false, CCN(L) = CCS(LN) and CCE(L) = CCW(LE).
+template <class T>
+__device__ __forceinline__ double matvec_row(const RowGeo &g, bool valid, const T *__restrict__ r,
+                                             const T *__restrict__ ccc,
+                                             const T *__restrict__ pold, T *__restrict__ pnew,
+                                             const T *__restrict__ ccs, const T *__restrict__ ccw,
+                                             const T *__restrict__ cce, const T *__restrict__ ccn,
+                                             T *__restrict__ ap, T beta, bool asym) {
+  const V4<T> r0 = ld4(r + g.d0), c0 = ld4(ccc + g.d0), o0 = ld4(pold + g.d0);
+  const V4<T> rn = ld4(r + g.dn), cn_ = ld4(ccc + g.dn), on = ld4(pold + g.dn);
+  const V4<T> rs = ld4(r + g.ds), cs_ = ld4(ccc + g.ds), os = ld4(pold + g.ds);
+  auto pc = [&](T rr, T cc, T po) { return rcpT(cc) * rr + beta * po; };
+  const V4<T> p = {pc(r0.x, c0.x, o0.x), pc(r0.y, c0.y, o0.y), pc(r0.z, c0.z, o0.z),
+                   pc(r0.w, c0.w, o0.w)};
+  const V4<T> pn = {pc(rn.x, cn_.x, on.x), pc(rn.y, cn_.y, on.y), pc(rn.z, cn_.z, on.z),
+                    pc(rn.w, cn_.w, on.w)};
+  const V4<T> ps = {pc(rs.x, cs_.x, os.x), pc(rs.y, cs_.y, os.y), pc(rs.z, cs_.z, os.z),
+                    pc(rs.w, cs_.w, os.w)};
+  T pw = from_west(p), pe = from_east(p);
+  if (g.cx == 0) pw = pc(r[g.dwe], ccc[g.dwe], pold[g.dwe]);
+  if (g.cx == ROWT - 1) pe = pc(r[g.dee], ccc[g.dee], pold[g.dee]);
+  const V4<T> ks = ld4(ccs + g.d0), kw = ld4(ccw + g.d0);
+  V4<T> kn, ke;
+  if (asym) {
+    kn = ld4(ccn + g.d0);
+    ke = ld4(cce + g.d0);
+  } else {
+    kn = ld4(ccs + g.dn);
+    T kwe = from_east(kw);
+    if (g.cx == ROWT - 1) kwe = ccw[g.dee];
+    ke = {kw.y, kw.z, kw.w, kwe};
+  }
+  V4<T> a;
+  a.x = c0.x * p.x + ks.x * ps.x + kn.x * pn.x + kw.x * pw + ke.x * p.y;
+  a.y = c0.y * p.y + ks.y * ps.y + kn.y * pn.y + kw.y * p.x + ke.y * p.z;
+  a.z = c0.z * p.z + ks.z * ps.z + kn.z * pn.z + kw.z * p.y + ke.z * p.w;
+  a.w = c0.w * p.w + ks.w * ps.w + kn.w * pn.w + kw.w * p.z + ke.w * pe;
+  if (!valid) return 0.0;
+  st4(pnew + g.d0, p);
+  st4(ap + g.d0, a);
+  return double(a.x) * double(p.x) + double(a.y) * double(p.y) + double(a.z) * double(p.z) +
+         double(a.w) * double(p.w);
+}
+
+// X = X + ALPHA*PCG, RCG = RCG - ALPHA*APCG, TMPCG = CCCI*RCG (congrad.f90:
+// 133-135) and the parts of r.z and r.r (:143-146).
+template <class T>
+__device__ __forceinline__ void update_row(const RowGeo &g, bool valid, T *__restrict__ x,
+                                           const T *__restrict__ pnew, T *__restrict__ r,
+                                           const T *__restrict__ ap, const T *__restrict__ ccc,
+                                           T alpha, double &rz, double &rr) {
+  if (!valid) return;
+  V4<T> xv = ld4(x + g.d0), rv = ld4(r + g.d0);
+  const V4<T> pv = ld4(pnew + g.d0), av = ld4(ap + g.d0), cv = ld4(ccc + g.d0);
+  xv.x = xv.x + alpha * pv.x;
+  xv.y = xv.y + alpha * pv.y;
+  xv.z = xv.z + alpha * pv.z;
+  xv.w = xv.w + alpha * pv.w;
+  rv.x = rv.x - alpha * av.x;
+  rv.y = rv.y - alpha * av.y;
+  rv.z = rv.z - alpha * av.z;
+  rv.w = rv.w - alpha * av.w;
+  st4(x + g.d0, xv);
+  st4(r + g.d0, rv);
+  const T z0 = rcpT(cv.x) * rv.x, z1 = rcpT(cv.y) * rv.y, z2 = rcpT(cv.z) * rv.z,
+          z3 = rcpT(cv.w) * rv.w;
+  rz += double(rv.x) * double(z0) + double(rv.y) * double(z1) + double(rv.z) * double(z2) +
+        double(rv.w) * double(z3);
+  rr += double(rv.x) * double(rv.x) + double(rv.y) * double(rv.y) + double(rv.z) * double(rv.z) +
+        double(rv.w) * double(rv.w);
+}
+
+// RCG = FPTMP - CCC*P - CCN*PN - CCS*PS - CCW*PW - CCE*PE (congrad.f90:72) in
+// FP64 on a row vector; land slots give 0.
+__device__ __forceinline__ V4<double> residual_row(const RowGeo &g, const uint8_t *kind,
+                                                   const double *__restrict__ P,
+                                                   const DevSystem &Y) {
+  const V4<double> x = ld4(P + g.d0), xn = ld4(P + g.dn), xs = ld4(P + g.ds);
+  double xw = from_west(x), xe = from_east(x);
+  if (g.cx == 0) xw = P[g.dwe];
+  if (g.cx == ROWT - 1) xe = P[g.dee];
+  const V4<double> b = ld4(Y.fptmp + g.d0), c = ld4(Y.ccc + g.d0), kn = ld4(Y.ccn + g.d0),
+                   ks = ld4(Y.ccs + g.d0), kw = ld4(Y.ccw + g.d0), ke = ld4(Y.cce + g.d0);
+  const uchar4 kd = *reinterpret_cast<const uchar4 *>(kind + g.d0);
+  V4<double> r;
+  r.x = b.x - c.x * x.x - kn.x * xn.x - ks.x * xs.x - kw.x * xw - ke.x * x.y;
+  r.y = b.y - c.y * x.y - kn.y * xn.y - ks.y * xs.y - kw.y * x.x - ke.y * x.z;
+  r.z = b.z - c.z * x.z - kn.z * xn.z - ks.z * xs.z - kw.z * x.y - ke.z * x.w;
+  r.w = b.w - c.w * x.w - kn.w * xn.w - ks.w * xs.w - kw.w * x.z - ke.w * xe;
+  if (kd.x == LAND) r.x = 0.;
+  if (kd.y == LAND) r.y = 0.;
+  if (kd.z == LAND) r.z = 0.;
+  if (kd.w == LAND) r.w = 0.;
+  return r;
+}
+
+}  // namespace xm

@@ -81,4 +81,69 @@ __device__ __forceinline__ double reduce_partials(const double *part, int nblk, 
   return block_sum(s, sh);
 }
 
+// ---------------------------------------------------------------------------
+// Row-vector geometry of the CG kernels: a thread owns 4 consecutive cells of
+// one tile row (8 threads per row, 64 per tile, 4 tiles per 256-thread CTA).
+// Row vectors are 16 B (FP32) / 32 B (FP64) aligned, so they move as 128-bit
+// loads; the E/W neighbours of the vector come from the adjacent lanes of the
+// row (warp shuffles) and, at the tile edge, from the neighbour tile.
+constexpr int CPT = 4;              // cells per thread
+constexpr int ROWT = TX / CPT;      // threads per row (8)
+constexpr int TPT = TILE / CPT;     // threads per tile (64)
+constexpr int TILES_PER_CTA = NT / TPT;  // 4
+
+struct RowGeo {
+  int d0;      // first slot of the thread's 4 cells
+  int dn, ds;  // first slots of the same 4 columns in the rows above / below
+  int dwe;     // slot west of cell 0 (used when cx == 0)
+  int dee;     // slot east of cell 3 (used when cx == ROWT-1)
+  int cx;      // column group 0..7
+};
+
+__device__ __forceinline__ RowGeo row_geo(const int4 *__restrict__ tnbr, int tile, int q) {
+  const int cx = q & (ROWT - 1), ty = q / ROWT;
+  const int4 nb = __ldg(&tnbr[tile]);  // (w, e, s, n)
+  RowGeo g;
+  g.cx = cx;
+  g.d0 = tile * TILE + ty * TX + cx * CPT;
+  g.dn = (ty < TY - 1) ? g.d0 + TX : nb.w * TILE + cx * CPT;
+  g.ds = (ty > 0) ? g.d0 - TX : nb.z * TILE + (TY - 1) * TX + cx * CPT;
+  g.dwe = nb.x * TILE + ty * TX + (TX - 1);
+  g.dee = nb.y * TILE + ty * TX;
+  return g;
+}
+
+template <class T>
+struct V4 {
+  T x, y, z, w;
+};
+
+__device__ __forceinline__ V4<float> ld4(const float *p) {
+  const float4 v = *reinterpret_cast<const float4 *>(p);
+  return {v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ V4<double> ld4(const double *p) {
+  const double2 a = reinterpret_cast<const double2 *>(p)[0];
+  const double2 b = reinterpret_cast<const double2 *>(p)[1];
+  return {a.x, a.y, b.x, b.y};
+}
+__device__ __forceinline__ void st4(float *p, const V4<float> &v) {
+  *reinterpret_cast<float4 *>(p) = make_float4(v.x, v.y, v.z, v.w);
+}
+__device__ __forceinline__ void st4(double *p, const V4<double> &v) {
+  reinterpret_cast<double2 *>(p)[0] = make_double2(v.x, v.y);
+  reinterpret_cast<double2 *>(p)[1] = make_double2(v.z, v.w);
+}
+
+// value of the west neighbour of cell 0 / east neighbour of cell 3, from the
+// adjacent lane of the row (the tile-edge lanes substitute their own load)
+template <class T>
+__device__ __forceinline__ T from_west(const V4<T> &v) {
+  return __shfl_up_sync(0xffffffffu, v.w, 1, ROWT);
+}
+template <class T>
+__device__ __forceinline__ T from_east(const V4<T> &v) {
+  return __shfl_down_sync(0xffffffffu, v.x, 1, ROWT);
+}
+
 }  // namespace xm

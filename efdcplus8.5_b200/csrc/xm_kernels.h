@@ -10,7 +10,10 @@
 namespace xm {
 
 struct Launch {
-  int grid;          // CTAs of the grid-stride cell kernels
+  int grid;          // CTAs of the grid-stride cell kernels (one tile per CTA pass)
+  int grid_cg;       // CTAs of the FP64 CG kernels (four tiles per CTA pass)
+  int grid_mv64;     // CTAs of the FP64 matrix-vector kernel (register-heavy)
+  int grid_cg32;     // CTAs of the FP32 CG kernels (four tiles per CTA pass)
   int ntile;         // tiles including the ghost tile 0
   cudaStream_t stream;
 };
@@ -67,6 +70,8 @@ void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y,
 void count_launches(int n);
 
 int occupancy_blocks_per_sm();
+int occupancy_blocks_per_sm_cg();
+int occupancy_blocks_per_sm_mv64();
 int occupancy_blocks_per_sm_mixed();
 
 }  // namespace xm

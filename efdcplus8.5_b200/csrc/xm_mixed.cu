@@ -7,15 +7,13 @@
 // The outer FP64 loop (xm_step.cu: k_mx_resid / k_mx_apply) keeps P in FP64
 // and stops on the reference's own criterion, the FP64 RSQ <= RSQM.
 
-#include "xm_common.cuh"
+#include "xm_cg.cuh"
 #include "xm_kernels.h"
 
 namespace xm {
 
 #define TILE_LOOP(ntile)                                                      \
   for (int tile = blockIdx.x + 1; tile < (ntile); tile += gridDim.x)
-
-__device__ __forceinline__ float rcpf(float x) { return __frcp_rn(x); }
 
 // p = z + beta*p_old at the cell and its neighbours, Ap, p.Ap, ALPHA.
 __global__ void __launch_bounds__(NT) k_mx_matvec(DevStatic S, DevSystem Y, int ntile, Ctl *ctl,
@@ -24,30 +22,14 @@ __global__ void __launch_bounds__(NT) k_mx_matvec(DevStatic S, DevSystem Y, int 
   if (ctl->done | ctl->idone) return;
   const float beta = float(ctl->beta);
   const bool par = ctl->parity;
-  const float *__restrict__ pold = par ? Y.pb32 : Y.pa32;
-  float *__restrict__ pnew = par ? Y.pa32 : Y.pb32;
+  const float *pold = par ? Y.pb32 : Y.pa32;
+  float *pnew = par ? Y.pa32 : Y.pb32;
   const bool asym = ctl->asym;
-  const float *__restrict__ r = Y.r32;
-  const float *__restrict__ ccc = Y.ccc32;
   double acc = 0.0;
-  TILE_LOOP(ntile) {
-    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
-    const int d = q.d;
-    if (S.kind[d] == LAND) continue;
-    auto pc = [&](int j) { return fmaf(beta, pold[j], r[j] * rcpf(ccc[j])); };
-    const float p = pc(d), pn = pc(q.n), pe = pc(q.e), pw = pc(q.w), ps = pc(q.s);
-    float ccn, cce;
-    if (asym) {
-      ccn = Y.ccn32[d];
-      cce = Y.cce32[d];
-    } else {
-      ccn = Y.ccs32[q.n];
-      cce = Y.ccw32[q.e];
-    }
-    const float ap = ccc[d] * p + Y.ccs32[d] * ps + ccn * pn + Y.ccw32[d] * pw + cce * pe;
-    pnew[d] = p;
-    Y.ap32[d] = ap;
-    acc += double(ap) * double(p);
+  CG_TILE_LOOP(ntile) {
+    CG_TILE_GEO(S);
+    acc += matvec_row<float>(g, valid, Y.r32, Y.ccc32, pold, pnew, Y.ccs32, Y.ccw32, Y.cce32,
+                             Y.ccn32, Y.ap32, beta, asym);
   }
   acc = block_sum(acc, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = acc;
@@ -67,17 +49,11 @@ __global__ void __launch_bounds__(NT) k_mx_update(DevStatic S, DevSystem Y, int 
   __shared__ double sh[32];
   if (ctl->done | ctl->idone) return;
   const float alpha = float(ctl->alpha);
-  const float *__restrict__ pnew = ctl->parity ? Y.pa32 : Y.pb32;
+  const float *pnew = ctl->parity ? Y.pa32 : Y.pb32;
   double a1 = 0.0, a2 = 0.0;
-  TILE_LOOP(ntile) {
-    const int d = tile * TILE + threadIdx.x;
-    if (S.kind[d] == LAND) continue;
-    Y.x32[d] = fmaf(alpha, pnew[d], Y.x32[d]);
-    const float r = fmaf(-alpha, Y.ap32[d], Y.r32[d]);
-    Y.r32[d] = r;
-    const float z = r * rcpf(Y.ccc32[d]);
-    a1 += double(r) * double(z);
-    a2 += double(r) * double(r);
+  CG_TILE_LOOP(ntile) {
+    CG_TILE_GEO(S);
+    update_row<float>(g, valid, Y.x32, pnew, Y.r32, Y.ap32, Y.ccc32, alpha, a1, a2);
   }
   a1 = block_sum(a1, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = a1;
@@ -108,19 +84,19 @@ __global__ void __launch_bounds__(NT) k_mx_update(DevStatic S, DevSystem Y, int 
 
 void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {
-  k_mx_matvec<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
+  k_mx_matvec<<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
   count_launches(1);
 }
 void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part, int inner_cap, int total_cap) {
-  k_mx_update<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part, inner_cap, total_cap);
+  k_mx_update<<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part, inner_cap, total_cap);
   count_launches(1);
 }
 void launch_mx_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                     double *part, int inner_cap, int total_cap) {
-  k_mx_matvec<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
+  k_mx_matvec<<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
   count_launches(1);
-  k_mx_update<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part, inner_cap, total_cap);
+  k_mx_update<<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part, inner_cap, total_cap);
   count_launches(1);
 }
 

@@ -7,7 +7,7 @@
 // Each kernel is a grid-stride loop over tiles (one 256-thread CTA processes a
 // whole 32x8 tile per iteration); tile 0 is the ghost tile and is skipped.
 
-#include "xm_common.cuh"
+#include "xm_cg.cuh"
 #include "xm_kernels.h"
 
 namespace xm {
@@ -253,24 +253,21 @@ __global__ void __launch_bounds__(NT) k_scale(DevStatic S, DevState X, DevSystem
 // p double-buffered (pa/pb, selected by ctl->parity), Ap.  z = CCCI*r with
 // CCCI = 1./CCC is recomputed where needed instead of stored.
 
-__device__ __forceinline__ double rcp_rn(double x) { return 1. / x; }
-
-// :54-88 initial residual, z0, RPCG.
+// :54-88 initial residual, z0 = CCCI*r, RPCG.
 __global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double *P, int ntile,
                                                Ctl *ctl, double *part) {
   __shared__ double sh[32];
   double acc = 0.0;
-  TILE_LOOP(ntile) {
-    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
-    const int d = q.d;
-    if (S.kind[d] == LAND) continue;
-    const double ccc = Y.ccc[d];
-    const double r = Y.fptmp[d] - ccc * P[d] - Y.ccn[d] * P[q.n] - Y.ccs[d] * P[q.s] -
-                     Y.ccw[d] * P[q.w] - Y.cce[d] * P[q.e];
-    const double z = r * rcp_rn(ccc);
-    Y.r[d] = r;
-    Y.pa[d] = z;
-    acc += r * z;
+  CG_TILE_LOOP(ntile) {
+    CG_TILE_GEO(S);
+    const V4<double> r = residual_row(g, S.kind, P, Y);
+    const V4<double> c = ld4(Y.ccc + g.d0);
+    const V4<double> z = {r.x * rcpT(c.x), r.y * rcpT(c.y), r.z * rcpT(c.z), r.w * rcpT(c.w)};
+    if (valid) {
+      st4(Y.r + g.d0, r);
+      st4(Y.pa + g.d0, z);
+      acc += r.x * z.x + r.y * z.y + r.z * z.z + r.w * z.w;
+    }
   }
   acc = block_sum(acc, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = acc;
@@ -294,37 +291,20 @@ __global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double
 }
 
 // :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA).
-template <bool SYM>
 __global__ void __launch_bounds__(NT) k_cg_matvec(DevStatic S, DevSystem Y, int ntile, Ctl *ctl,
                                                  double *part) {
   __shared__ double sh[32];
   if (ctl->done) return;
   const double beta = ctl->beta;
   const bool par = ctl->parity;
-  const double *__restrict__ pold = par ? Y.pb : Y.pa;
-  double *__restrict__ pnew = par ? Y.pa : Y.pb;
-  const bool asym = !SYM || ctl->asym;
+  const double *pold = par ? Y.pb : Y.pa;
+  double *pnew = par ? Y.pa : Y.pb;
+  const bool asym = ctl->asym;
   double acc = 0.0;
-  TILE_LOOP(ntile) {
-    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
-    const int d = q.d;
-    if (S.kind[d] == LAND) continue;
-    // PCG = TMPCG + BETA*PCG at the cell and its neighbours (:151-162)
-    auto pc = [&](int j) { return rcp_rn(Y.ccc[j]) * Y.r[j] + beta * pold[j]; };
-    const double p = pc(d), pn = pc(q.n), pe = pc(q.e), pw = pc(q.w), ps = pc(q.s);
-    const double ccs = Y.ccs[d], ccw = Y.ccw[d];
-    double ccn, cce;
-    if (asym) {
-      ccn = Y.ccn[d];
-      cce = Y.cce[d];
-    } else {
-      ccn = Y.ccs[q.n];
-      cce = Y.ccw[q.e];
-    }
-    const double ap = Y.ccc[d] * p + ccs * ps + ccn * pn + ccw * pw + cce * pe;  // :114
-    pnew[d] = p;
-    Y.ap[d] = ap;
-    acc += ap * p;
+  CG_TILE_LOOP(ntile) {
+    CG_TILE_GEO(S);
+    acc += matvec_row<double>(g, valid, Y.r, Y.ccc, pold, pnew, Y.ccs, Y.ccw, Y.cce, Y.ccn, Y.ap,
+                              beta, asym);
   }
   acc = block_sum(acc, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = acc;
@@ -344,18 +324,11 @@ __global__ void __launch_bounds__(NT) k_cg_update(DevStatic S, DevSystem Y, doub
   __shared__ double sh[32];
   if (ctl->done) return;
   const double alpha = ctl->alpha;
-  const double *__restrict__ pnew = ctl->parity ? Y.pa : Y.pb;
+  const double *pnew = ctl->parity ? Y.pa : Y.pb;
   double a1 = 0.0, a2 = 0.0;
-  TILE_LOOP(ntile) {
-    const int d = tile * TILE + threadIdx.x;
-    if (S.kind[d] == LAND) continue;
-    const double p = pnew[d];
-    P[d] = P[d] + alpha * p;
-    const double r = Y.r[d] - alpha * Y.ap[d];
-    Y.r[d] = r;
-    const double z = rcp_rn(Y.ccc[d]) * r;
-    a1 += r * z;
-    a2 += r * r;
+  CG_TILE_LOOP(ntile) {
+    CG_TILE_GEO(S);
+    update_row<double>(g, valid, P, pnew, Y.r, Y.ap, Y.ccc, alpha, a1, a2);
   }
   a1 = block_sum(a1, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = a1;
@@ -389,25 +362,27 @@ __global__ void __launch_bounds__(NT) k_cg_update(DevStatic S, DevSystem Y, doub
 
 // ---------------------------------------------------------------------------
 // MIXED outer step: r = b - A*P in FP64 (the FP64 refinement residual),
-// RSQ in FP64, and the FP32 inner system r32, z32 = r32/CCC.  Leaves P alone.
+// RSQ in FP64, and the FP32 inner system r32, z32 = r32/CCC, x32 = 0.
 __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, DevSystem Y, const double *P,
                                                 int ntile, Ctl *ctl, double *part, double rsqm,
                                                 double rel_tol) {
   __shared__ double sh[32];
   double a1 = 0.0, a2 = 0.0;
-  TILE_LOOP(ntile) {
-    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
-    const int d = q.d;
-    if (S.kind[d] == LAND) continue;
-    const double r = Y.fptmp[d] - Y.ccc[d] * P[d] - Y.ccn[d] * P[q.n] - Y.ccs[d] * P[q.s] -
-                     Y.ccw[d] * P[q.w] - Y.cce[d] * P[q.e];
-    const float r32 = float(r);
-    const float z32 = r32 * __frcp_rn(Y.ccc32[d]);
-    Y.r32[d] = r32;
-    Y.pa32[d] = z32;
-    Y.x32[d] = 0.f;
-    a1 += r * r;
-    a2 += double(r32) * double(z32);
+  CG_TILE_LOOP(ntile) {
+    CG_TILE_GEO(S);
+    const V4<double> r = residual_row(g, S.kind, P, Y);
+    const V4<float> c = ld4(Y.ccc32 + g.d0);
+    const V4<float> r32 = {float(r.x), float(r.y), float(r.z), float(r.w)};
+    const V4<float> z32 = {r32.x * rcpT(c.x), r32.y * rcpT(c.y), r32.z * rcpT(c.z),
+                           r32.w * rcpT(c.w)};
+    if (valid) {
+      st4(Y.r32 + g.d0, r32);
+      st4(Y.pa32 + g.d0, z32);
+      st4(Y.x32 + g.d0, V4<float>{0.f, 0.f, 0.f, 0.f});
+      a1 += r.x * r.x + r.y * r.y + r.z * r.z + r.w * r.w;
+      a2 += double(r32.x) * double(z32.x) + double(r32.y) * double(z32.y) +
+            double(r32.z) * double(z32.z) + double(r32.w) * double(z32.w);
+    }
   }
   a1 = block_sum(a1, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = a1;
@@ -440,15 +415,22 @@ __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, DevSystem Y, const
   }
 }
 
-// MIXED: P += x32 (the FP32 correction), x32 = 0.
+// MIXED: P += x32 (the FP32 correction).
 __global__ void __launch_bounds__(NT) k_mx_apply(DevStatic S, DevSystem Y, double *P, int ntile) {
-  TILE_LOOP(ntile) {
-    const int d = tile * TILE + threadIdx.x;
-    if (S.kind[d] == LAND) continue;
-    P[d] = P[d] + double(Y.x32[d]);
+  CG_TILE_LOOP(ntile) {
+    CG_TILE_GEO(S);
+    if (!valid) continue;
+    V4<double> x = ld4(P + g.d0);
+    const V4<float> d = ld4(Y.x32 + g.d0);
+    x.x = x.x + double(d.x);
+    x.y = x.y + double(d.y);
+    x.z = x.z + double(d.z);
+    x.w = x.w + double(d.w);
+    st4(P + g.d0, x);
   }
 }
 
+// ---------------------------------------------------------------------------
 // Standalone CONGRAD: a caller-assembled scaled system.  Land slots are made
 // inert (CCC=1, couplings 0, b=0), FP32 copies made for MIXED, and the
 // symmetry of the given CCE/CCN against CCW(LE)/CCS(LN) is recorded.
@@ -861,33 +843,33 @@ void launch_scale(const Launch &l, const DevStatic &S, const DevState &X, const 
 }
 void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                     double *part) {
-  k_cg_init<<<l.grid, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part);
+  k_cg_init<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part);
   count_launches(1);
 }
 void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                     double *part, double rsqm, int iterm) {
-  k_cg_matvec<true><<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
+  k_cg_matvec<<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
   count_launches(1);
-  k_cg_update<<<l.grid, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part, rsqm, iterm);
+  k_cg_update<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part, rsqm, iterm);
   count_launches(1);
 }
 void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {
-  k_cg_matvec<true><<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
+  k_cg_matvec<<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
   count_launches(1);
 }
 void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                       double *part, double rsqm, int iterm) {
-  k_cg_update<<<l.grid, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part, rsqm, iterm);
+  k_cg_update<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part, rsqm, iterm);
   count_launches(1);
 }
 void launch_mx_resid(const Launch &l, const DevStatic &S, const DevSystem &Y, const double *P,
                      Ctl *ctl, double *part, double rsqm, double rel_tol) {
-  k_mx_resid<<<l.grid, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part, rsqm, rel_tol);
+  k_mx_resid<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part, rsqm, rel_tol);
   count_launches(1);
 }
 void launch_mx_apply(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P) {
-  k_mx_apply<<<l.grid, NT, 0, l.stream>>>(S, Y, P, l.ntile);
+  k_mx_apply<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, l.ntile);
   count_launches(1);
 }
 void launch_backsub(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c) {
@@ -946,12 +928,27 @@ void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y,
 }
 
 int occupancy_blocks_per_sm() {
+  int a = 0, b = 0, c = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_assemble, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_begin, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_fin, NT, 0);
+  const int m = std::min(a, std::min(b, c));
+  return m > 0 ? m : 1;
+}
+
+int occupancy_blocks_per_sm_mv64() {
+  int a = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_matvec, NT, 0);
+  return a > 0 ? a : 1;
+}
+
+int occupancy_blocks_per_sm_cg() {
   int a = 0, b = 0, c = 0, d = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_matvec<true>, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_mx_apply, NT, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cg_update, NT, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_assemble, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_cg_init, NT, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_mx_resid, NT, 0);
-  int m = std::min(std::min(a, b), std::min(c, d));
+  const int m = std::min(std::min(a, b), std::min(c, d));
   return m > 0 ? m : 1;
 }
 

@@ -102,8 +102,9 @@ typedef struct efdc_xm_params {
   int32_t max_sweeps;/* wet/dry re-solve cap; the reference uses 500                  */
   int32_t precision; /* enum efdc_xm_precision (ignored by the CPU oracle)             */
   double mixed_rsq_factor; /* MIXED only: stop when the FP64 RSQ <= factor*RSQM; 0 selects
-                              the default 0.01 (the FP32 path converges past RSQM so that
-                              its surface stays within 1e-6 m of the FP64 solve)        */
+                              the default 0.1 (the FP32 path converges a little past
+                              RSQM so that its per-step surface error against the FP64
+                              solve stays well inside 1e-6 m)                         */
 } efdc_xm_params;
 
 /* Per-call arrays.  "in/out" arrays are read and overwritten.  Optional outputs

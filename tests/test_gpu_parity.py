@@ -41,7 +41,9 @@ def run_both(scn, steps, tm=1.0, precision=X.PREC_FP64, same_input=False, lists=
         prm = X.make_params(scn.params, n=n, tn=scn.tn(n) * tm, precision=precision)
         a = sol.step(prm, sg, lists=lists)
         b = orc.step(X.make_params(scn.params, n=n, tn=scn.tn(n) * tm), so, lists=lists)
-        out.append((a.as_dict(), b.as_dict(), sg, so))
+        snap = lambda d: {k: (v.copy() if isinstance(v, np.ndarray) else v)  # noqa: E731
+                          for k, v in d.items()}
+        out.append((a.as_dict(), b.as_dict(), snap(sg), snap(so)))
     sol.close()
     orc.close()
     return out
@@ -100,11 +102,28 @@ def test_fp64_config1_long_run():
 
 
 def test_mixed_config1_within_1e6_m():
+    """Solver error of the MIXED form: from the same inputs, every step's
+    surface is within 1e-6 m of the FP64 oracle's."""
     scn = S.config1()
-    res = run_both(scn, 300, precision=X.PREC_MIXED)
+    res = run_both(scn, 300, precision=X.PREC_MIXED, same_input=True)
     worst = max(eta_err(sg, so, scn.la) for _, _, sg, so in res)
     assert worst <= 1e-6, worst
     assert all(a["status"] == X.OK for a, _, _, _ in res)
+
+
+def test_mixed_free_run_drift_matches_fp64_tolerance():
+    """Run freely for 300 steps, the MIXED trajectory departs from the FP64
+    oracle's by no more than the oracle's own trajectory departs when RSQM is
+    tightened 100x: the drift comes from RSQM, not from FP32."""
+    scn = S.config1()
+    res = run_both(scn, 300, precision=X.PREC_MIXED)
+    drift_mixed = max(eta_err(sg, so, scn.la) for _, _, sg, so in res)
+    tight = S.config1()
+    tight.params["rsqm"] = scn.params["rsqm"] * 1e-2
+    a, _ = O.run(scn, 300)
+    b, _ = O.run(tight, 300)
+    drift_fp64 = eta_err(a, b, scn.la)
+    assert drift_mixed <= 2.0 * drift_fp64 + 1e-7, (drift_mixed, drift_fp64)
 
 
 def test_mixed_wetdry_masks_bit_exact_stepwise():
