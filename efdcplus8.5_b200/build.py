@@ -23,6 +23,7 @@ SOURCES = {
     "xm_step.cu": ["-fmad=false"],
     "xm_mixed.cu": [],
     "xm_capi.cu": [],
+    "xm_noalloc.cu": ["-fmad=false"],
 }
 
 

@@ -61,6 +61,7 @@ uint64_t morton2(uint32_t x, uint32_t y) {
 
 namespace xm {
 void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void set_last_error_str(const char *msg) { g_last_error = msg ? msg : ""; }
 }  // namespace xm
 
 // A device buffer owned by the context.

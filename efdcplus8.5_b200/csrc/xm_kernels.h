@@ -66,6 +66,9 @@ void launch_gather(cudaStream_t st, const CopyJob *jobs, int njob, const int *li
 void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                         int mixed);
 
+// sets the message returned by efdc_xm_last_error() for this thread
+void set_last_error_str(const char *msg);
+
 // process-wide count of kernel launches (measurement hook)
 void count_launches(int n);
 

@@ -236,6 +236,9 @@ def load(path: str | os.PathLike | None = None):
     lib.efdc_xm_kernel_launches.restype = C.c_int64
     lib.efdc_xm_time_kernels.restype = C.c_int32
     lib.efdc_xm_time_kernels.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(KTime)]
+    lib.efdc_xm_congrad_noalloc.restype = C.c_int32
+    lib.efdc_xm_congrad_noalloc.argtypes = [C.c_int32] + [C.c_void_p] * 11 + [
+        C.c_double, C.c_int32, C.c_void_p, _pi, _pd]
     lib.efdc_xm_congrad.restype = C.c_int32
     lib.efdc_xm_congrad.argtypes = [C.c_void_p] + [_pd] * 8 + [C.c_double, C.c_int32,
                                                                 C.c_int32, _pi, _pd]

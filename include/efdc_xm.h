@@ -211,6 +211,36 @@ typedef struct efdc_xm_ktime {
 int32_t efdc_xm_time_kernels(efdc_xm_ctx *ctx, int32_t precision, int32_t reps,
                              efdc_xm_ktime *out);
 
+/* ---- Entry point with no counterpart in the reference ----
+ *
+ * CONGRAD that allocates nothing.  For callers that cannot let this library
+ * allocate GPU memory: a host code that gives all of its device memory to its
+ * own pool or budget, a time-critical loop where an allocation could stall or
+ * fail, or a caller whose data already sit in device arrays it manages (CUDA
+ * Fortran device arrays, a framework's tensors).  It solves the same system
+ * as efdc_xm_congrad (congrad.f90:54-187, FP64, CCCI recomputed as 1/CCC) on
+ * the reference's own layout, without a context:
+ *   - every array is a DEVICE pointer to a 1-based Fortran-layout array
+ *     (element L at [L-1], L = 1..LC with LC = LA+1); P is the initial guess
+ *     and receives the result; iters and rsq are host pointers;
+ *   - the solver's vectors live in one fixed array of device memory declared
+ *     at file scope in the library, sized for at most
+ *     EFDC_XM_NOALLOC_MAX_CELLS water cells (12.6 MB); every GPU that loads
+ *     the library holds it until the process exits.  Larger LA is rejected
+ *     with EFDC_XM_BAD_ARGUMENT and a message (efdc_xm_last_error);
+ *   - the first call on a device looks up that array's device address (with
+ *     that device current) and keeps it, so make the first call on each
+ *     device before any stream capture;
+ *   - all calls share the array: calls that overlap on the GPU (other
+ *     streams, other host threads) race; the call returns after its work on
+ *     `stream` (a cudaStream_t, NULL = legacy default stream) finished. */
+#define EFDC_XM_NOALLOC_MAX_CELLS 524288
+int32_t efdc_xm_congrad_noalloc(int32_t la, const int32_t *lnc, const int32_t *lsc,
+                                const int32_t *lec, const int32_t *lwc, const double *ccc,
+                                const double *ccs, const double *ccn, const double *ccw,
+                                const double *cce, const double *fptmp, double *p, double rsqm,
+                                int32_t iterm, void *stream, int32_t *iters, double *rsq);
+
 #ifdef __cplusplus
 }
 #endif
