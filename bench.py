@@ -52,7 +52,7 @@ UNIT = "cell-iter/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--size", type=int, default=2048)
@@ -92,7 +92,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
@@ -176,7 +176,7 @@ def transfer_bytes(state, lc, la, isdry):
     """Bytes efdc_xm_step moves per call for a Fortran-shim-like field set:
     uploads LC elements of every input/in-out array, downloads LA-1 elements of
     every output/in-out array (mirrors efdc_xm_upload/efdc_xm_download)."""
-    dbl_in = ["p", "hp", "h1p", "hu", "hv", "uhdye", "vhdxe", "sub", "svb", "sbx", "sby",
+    dbl_in = ["p", "hp", "hu", "hv", "uhdye", "vhdxe", "sub", "svb", "sbx", "sby",
               "fcaxe", "fcaye", "fxe", "fye", "tsx", "tsy", "tbx", "tby", "qsume", "qdwaste",
               "vdwaste"]
     int_in = ["lmaskdry", "iscdry", "lopenbcdry", "natdry"]
@@ -210,7 +210,7 @@ def ours(args):
     def params(n, prec):
         return X.make_params(scn.params, n=n, tn=scn.tn(n), precision=prec)
 
-    def run(prec, steps, warmup, clocks=False):
+    def run(prec, steps, warmup):
         st = scn.copy_state()
         sol.upload(st)
         n = 0
@@ -220,7 +220,6 @@ def ours(args):
             assert s.status in (X.OK, X.NEG_DEPTH), s.as_dict()
         barrier()
         torch.cuda.synchronize()
-        ck = Clocks(local) if clocks else None
         l0 = lib.efdc_xm_kernel_launches()
         times, iters, outer = [], [], []
         for _ in range(steps):
@@ -240,14 +239,14 @@ def ours(args):
         torch.cuda.synchronize()
         barrier()
         launches = lib.efdc_xm_kernel_launches() - l0
-        clk = ck.stop() if ck else None
         out = scn.copy_state()
         sol.download(out)
-        return dict(times=times, iters=iters, outer=outer, launches=launches, clocks=clk,
-                    state=out)
+        return dict(times=times, iters=iters, outer=outer, launches=launches, state=out)
 
+    ck = Clocks(local)
     r64 = run(X.PREC_FP64, args.steps, args.warmup)
-    rmx = run(X.PREC_MIXED, args.steps, args.warmup, clocks=True)
+    rmx = run(X.PREC_MIXED, args.steps, args.warmup)
+    clocks = ck.stop()
     cells = scn.ncell
     credit = cells * sum(r64["iters"])  # FP64 iterations of the same steps
     t_mx = sum(rmx["times"]) / 1000.0
@@ -264,22 +263,24 @@ def ours(args):
     kt = sol.time_kernels(X.PREC_MIXED, reps=20)
     kt64 = sol.time_kernels(X.PREC_FP64, reps=20)
     peak, peak_kind = measured_peaks()
-    # algorithmic bytes per water cell: matvec reads r, CCC, p_old, CCS, CCW,
-    # writes p_new, Ap (FP32: 7 x 4 B); FP64 drop-in: 7 x 8 B
-    bytes_mv = 28.0 * kt.ncells
+    # algorithmic bytes per water cell: the FP32 matvec of the Jacobi-scaled
+    # system reads r, p_old, AS, AW and writes p_new, Ap (6 x 4 B); the FP64
+    # drop-in's reads r, CCC, p_old, CCS, CCW and writes p_new, Ap (7 x 8 B)
+    bytes_mv = 24.0 * kt.ncells
     achieved = bytes_mv / (kt.ms_matvec * 1e-3) / 1e9
     traffic = None
     tf = REPO / "profiles" / "traffic.json"
     if tf.exists():
-        t = json.loads(tf.read_text()).get("k_mx_matvec")
-        if t:
+        tj = json.loads(tf.read_text())
+        t = tj.get("k_mx_matvec")
+        if t and "k_mx_matvec" not in tj.get("stale_for", []):
             traffic = float(t["dram_bytes_per_cell"]) * kt.ncells
-    roof = {"bound": "hbm", "kernel": "k_mx_matvec (FP32 p-update + A*p + p.Ap)",
+    roof = {"bound": "hbm", "kernel": "k_mx_matvec (FP32 p-update + Ahat*p + p.Ap)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_kind": peak_kind, "traffic": traffic,
             "ms_per_launch": kt.ms_matvec, "bytes_per_launch": bytes_mv,
-            "update_kernel": {"ms_per_launch": kt.ms_update, "bytes_per_launch": 28.0 * kt.ncells,
-                              "achieved": 28.0 * kt.ncells / (kt.ms_update * 1e-3) / 1e9},
+            "update_kernel": {"ms_per_launch": kt.ms_update, "bytes_per_launch": 24.0 * kt.ncells,
+                              "achieved": 24.0 * kt.ncells / (kt.ms_update * 1e-3) / 1e9},
             "fp64_matvec": {"ms_per_launch": kt64.ms_matvec, "bytes_per_launch": 56.0 * kt.ncells,
                             "achieved": 56.0 * kt.ncells / (kt64.ms_matvec * 1e-3) / 1e9}}
 
@@ -344,12 +345,12 @@ def ours(args):
             "data": "synthetic (seeded)", "config": cfg,
             "fp64_value": fp64_value, "speedup_vs_fp64": value / fp64_value,
             "fp64_ms_per_step": 1000 * t_64 / args.steps,
-            "iters_fp64": r64["iters"], "iters_mixed_inner": rmx["iters"],
-            "outer_refinements": rmx["outer"],
+            "iters_fp64_total": int(sum(r64["iters"])), "iters_mixed_inner_total": int(sum(rmx["iters"])),
+            "outer_refinements_per_step": float(np.mean(rmx["outer"])),
             "max_eta_diff_mixed_vs_fp64_m": eta_err,
             "solves_per_s": world * args.steps / t_mx, "cell_steps_per_s": world * cells * args.steps / t_mx,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": int(rmx["launches"]), "clocks": rmx["clocks"],
+            "gpu_launches": int(rmx["launches"]), "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     sol.close()

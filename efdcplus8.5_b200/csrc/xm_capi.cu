@@ -73,7 +73,7 @@ struct DevBuf {
 struct efdc_xm_ctx {
   int device = 0;
   int la = 0, lc = 0;
-  int ntile = 0, nslot = 0, grid = 1, grid_cg = 1, grid_mv64 = 1, grid_cg32 = 1, nsm = 0;
+  int ntile = 0, nslot = 0, grid = 1, grid_cg = 1, grid_mv64 = 1, grid_cg32 = 1, grid_up32 = 1, nsm = 0;
   cudaStream_t stream = nullptr;
   std::vector<DevBuf> bufs;
   // host copies of the layout
@@ -95,6 +95,7 @@ struct efdc_xm_ctx {
   int max_jobs = 0;
   // open boundaries
   bool obc_serial = false;
+  bool may_asym = false;  // a radiation boundary exists: the operator can be unsymmetric
   int nobc = 0;
   int side_n[4] = {0, 0, 0, 0};
   std::vector<double> tcp;
@@ -117,7 +118,7 @@ struct efdc_xm_ctx {
     bufs.push_back(b);
     return static_cast<T *>(b.p);
   }
-  xm::Launch L() const { return xm::Launch{grid, grid_cg, grid_mv64, grid_cg32, ntile, stream}; }
+  xm::Launch L() const { return xm::Launch{grid, grid_cg, grid_mv64, grid_cg32, grid_up32, ntile, stream}; }
 };
 
 namespace {
@@ -436,6 +437,7 @@ efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *g, int32_t device) {
   c->grid_cg = std::max(1, std::min((c->ntile - 1 + 3) / 4, c->nsm * occ_cg));
   c->grid_cg32 = std::max(1, std::min((c->ntile - 1 + 3) / 4, c->nsm * occ_cg32));
   c->grid_mv64 = std::max(1, std::min((c->ntile - 1 + 3) / 4, c->nsm * xm::occupancy_blocks_per_sm_mv64()));
+  c->grid_up32 = std::max(1, std::min((c->ntile - 1 + 3) / 4, c->nsm * xm::occupancy_blocks_per_sm_mixed_update()));
 
   std::vector<int4> tnbr(c->ntile, int4{0, 0, 0, 0});
   std::vector<uint8_t> kind(c->nslot, xm::LAND);
@@ -476,6 +478,7 @@ efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *g, int32_t device) {
         bpsb.push_back(o.psb ? o.psb[size_t(m) * o.ld + ll] : 0.0);
       }
       kind[c->slot_of_L[L]] = xm::OPENBC;
+      if (o.ispb[ll] == 1 || o.ispb[ll] == 2) c->may_asym = true;
     }
   }
   c->nobc = int(bslot.size());
@@ -528,11 +531,12 @@ efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *g, int32_t device) {
   xm::DevSystem &Y = c->Y;
   Y.ccc = D(); Y.ccs = D(); Y.ccw = D(); Y.cce = D(); Y.ccn = D(); Y.fptmp = D();
   Y.r = D(); Y.pa = D(); Y.pb = D(); Y.ap = D();
-  Y.ccc32 = Fl(); Y.ccs32 = Fl(); Y.ccw32 = Fl(); Y.cce32 = Fl(); Y.ccn32 = Fl();
+  Y.as32 = Fl(); Y.aw32 = Fl(); Y.ae32 = Fl(); Y.an32 = Fl();
   Y.r32 = Fl(); Y.pa32 = Fl(); Y.pb32 = Fl(); Y.ap32 = Fl(); Y.x32 = Fl();
   c->ptmp = D();
   c->ctl = c->alloc<Ctl>(1);
-  c->part = c->alloc<double>(size_t(2) * std::max(c->grid, std::max(c->grid_cg, c->grid_cg32)) + 64);
+  c->part = c->alloc<double>(size_t(2) * std::max(std::max(c->grid, c->grid_up32),
+                                                  std::max(c->grid_cg, c->grid_cg32)) + 64);
   if (!Y.x32 || !c->ctl || !c->part) return bail("cudaMalloc failed (device memory)");
   if (cudaHostAlloc(reinterpret_cast<void **>(&c->ctl_h), sizeof(Ctl), cudaHostAllocDefault) != cudaSuccess)
     return bail("cudaHostAlloc failed");
@@ -540,14 +544,9 @@ efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *g, int32_t device) {
   // land slots of the scaled system: CCC=1 keeps them inert in the CG
   {
     std::vector<double> one(ns, 0.0);
-    std::vector<float> onef(ns, 0.0f);
     for (size_t d = 0; d < ns; ++d)
-      if (kind[d] == xm::LAND) {
-        one[d] = 1.0;
-        onef[d] = 1.0f;
-      }
+      if (kind[d] == xm::LAND) one[d] = 1.0;
     cudaMemcpy(Y.ccc, one.data(), ns * sizeof(double), cudaMemcpyHostToDevice);
-    cudaMemcpy(Y.ccc32, onef.data(), ns * sizeof(float), cudaMemcpyHostToDevice);
     // RCX/RCY: 1 on water cells, 0 on the ghosts (calpuv2c.f90:97-102)
     std::vector<double> rc(ns, 0.0), fu(ns, 1.0), fv(ns, 1.0);
     for (int L = 2; L <= la; ++L) {
@@ -622,7 +621,7 @@ int32_t efdc_xm_upload(efdc_xm_ctx *c, const efdc_xm_fields *f) {
   CK(cudaSetDevice(c->device));
   xm::DevState &X = c->X;
   std::vector<Xfer> xs = {
-      {f->p, X.p, 0}, {f->hp, X.hp, 0}, {f->h1p, X.h1p, 0}, {f->hu, X.hu, 0}, {f->hv, X.hv, 0},
+      {f->p, X.p, 0}, {f->hp, X.hp, 0}, {f->hu, X.hu, 0}, {f->hv, X.hv, 0},
       {f->uhdye, X.uhdye, 0}, {f->vhdxe, X.vhdxe, 0}, {f->sub, X.sub, 0}, {f->svb, X.svb, 0},
       {f->sbx, X.sbx, 0}, {f->sby, X.sby, 0}, {f->lmaskdry, X.lmaskdry, 1},
       {f->iscdry, X.iscdry, 2}, {f->lopenbcdry, X.lopenbcdry, 1}, {f->natdry, X.natdry, 2},
@@ -634,6 +633,13 @@ int32_t efdc_xm_upload(efdc_xm_ctx *c, const efdc_xm_fields *f) {
       {f->vdwaste, X.vdwaste, 0}};
   int rc = upload_arrays(c, xs);
   if (rc) return rc;
+  // the second buffer of each time-level pair starts as a copy (its land
+  // slots must hold the ghost values too); the H1P input is not used because
+  // a step begins with H1P = HP (calpuv2c.f90:264)
+  const size_t nb = size_t(c->nslot) * sizeof(double);
+  if (f->uhdye) CK(cudaMemcpyAsync(X.uhdy1e, X.uhdye, nb, cudaMemcpyDeviceToDevice, c->stream));
+  if (f->vhdxe) CK(cudaMemcpyAsync(X.vhdx1e, X.vhdxe, nb, cudaMemcpyDeviceToDevice, c->stream));
+  if (f->hp) CK(cudaMemcpyAsync(X.h1p, X.hp, nb, cudaMemcpyDeviceToDevice, c->stream));
   if (c->nobc > 0) {
     int k = 0;
     for (int s = 0; s < 4; ++s)
@@ -720,14 +726,20 @@ int32_t efdc_xm_step_device(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_s
   c->ctl_h->counter = 0;
   if ((rc = write_ctl(c))) return stats->status = rc;
 
-  xm::launch_begin(l, c->S, c->X, s);
+  // time levels by buffer swap: after it the *1 buffers hold the entry values
+  // (UHDY1E=UHDYE, VHDX1E=VHDXE, H1P=HP, calpuv2c.f90:256-264) and the
+  // others are rewritten for every water cell before they are read
+  std::swap(c->X.uhdye, c->X.uhdy1e);
+  std::swap(c->X.vhdxe, c->X.vhdx1e);
+  std::swap(c->X.hp, c->X.h1p);
+  xm::launch_begin(c->L(), c->S, c->X, s);
   if (prm->isdry > 0) xm::launch_obc_reset(l, c->B, c->X);
   CK(cudaGetLastError());
   int ncordry = 0, status = EFDC_XM_OK;
   for (;;) {  // 1000 CONTINUE
     xm::launch_assemble(l, c->S, c->X, s, c->ctl, c->part);
     xm::launch_obc(l, c->S, c->X, c->B, s, c->ctl, c->obc_serial);
-    xm::launch_scale(l, c->S, c->X, c->Y, c->ctl, mixed ? 1 : 0);
+    xm::launch_scale(l, c->S, c->X, c->Y, c->ctl, mixed ? 1 : 0, c->may_asym ? 1 : 0);
     CK(cudaGetLastError());
     int iters = 0, st = 0, outer = 0;
     double rsq = 0;
@@ -735,6 +747,11 @@ int32_t efdc_xm_step_device(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_s
                              prm->mixed_rsq_factor)
                : solve_fp64(c, c->X.p, prm->rsqm, prm->iterm, &iters, &rsq, &st);
     if (rc) return stats->status = rc;
+    if (c->ctl_h->asym & 2) {
+      set_error("the scaled operator is unsymmetric although the model has no radiation "
+                "boundary (check SUBO/SVBO next to the open-boundary cells)");
+      return stats->status = EFDC_XM_UNSUPPORTED;
+    }
     stats->iters_last = iters;
     stats->iters_total += iters;
     stats->solves += 1;

@@ -75,6 +75,76 @@ __device__ __forceinline__ double matvec_row(const RowGeo &g, bool valid, const 
          double(a.w) * double(p.w);
 }
 
+// MIXED inner CG on the Jacobi-scaled system (unit diagonal): p = r + beta*p
+// at the row vector and its halo, Ap = p + AS*pS + AN*pN + AW*pW + AE*pE, and
+// the part of p.Ap.  Symmetric: AN(L) = AS(LN), AE(L) = AW(LE).
+__device__ __forceinline__ double matvec_row_scaled(const RowGeo &g, bool valid,
+                                                    const float *__restrict__ r,
+                                                    const float *__restrict__ pold,
+                                                    float *__restrict__ pnew,
+                                                    const float *__restrict__ as,
+                                                    const float *__restrict__ aw,
+                                                    const float *__restrict__ ae,
+                                                    const float *__restrict__ an,
+                                                    float *__restrict__ ap, float beta, bool asym) {
+  const V4<float> r0 = ld4(r + g.d0), o0 = ld4(pold + g.d0);
+  const V4<float> rn = ld4(r + g.dn), on = ld4(pold + g.dn);
+  const V4<float> rs = ld4(r + g.ds), os = ld4(pold + g.ds);
+  const V4<float> p = {fmaf(beta, o0.x, r0.x), fmaf(beta, o0.y, r0.y), fmaf(beta, o0.z, r0.z),
+                       fmaf(beta, o0.w, r0.w)};
+  const V4<float> pn = {fmaf(beta, on.x, rn.x), fmaf(beta, on.y, rn.y), fmaf(beta, on.z, rn.z),
+                        fmaf(beta, on.w, rn.w)};
+  const V4<float> ps = {fmaf(beta, os.x, rs.x), fmaf(beta, os.y, rs.y), fmaf(beta, os.z, rs.z),
+                        fmaf(beta, os.w, rs.w)};
+  float pw = from_west(p), pe = from_east(p);
+  if (g.cx == 0) pw = fmaf(beta, pold[g.dwe], r[g.dwe]);
+  if (g.cx == ROWT - 1) pe = fmaf(beta, pold[g.dee], r[g.dee]);
+  const V4<float> ks = ld4(as + g.d0), kw = ld4(aw + g.d0);
+  V4<float> kn, ke;
+  if (asym) {
+    kn = ld4(an + g.d0);
+    ke = ld4(ae + g.d0);
+  } else {
+    kn = ld4(as + g.dn);
+    float kwe = from_east(kw);
+    if (g.cx == ROWT - 1) kwe = aw[g.dee];
+    ke = {kw.y, kw.z, kw.w, kwe};
+  }
+  V4<float> a;
+  a.x = p.x + ks.x * ps.x + kn.x * pn.x + kw.x * pw + ke.x * p.y;
+  a.y = p.y + ks.y * ps.y + kn.y * pn.y + kw.y * p.x + ke.y * p.z;
+  a.z = p.z + ks.z * ps.z + kn.z * pn.z + kw.z * p.y + ke.z * p.w;
+  a.w = p.w + ks.w * ps.w + kn.w * pn.w + kw.w * p.z + ke.w * pe;
+  if (!valid) return 0.0;
+  st4(pnew + g.d0, p);
+  st4(ap + g.d0, a);
+  return double(a.x) * double(p.x) + double(a.y) * double(p.y) + double(a.z) * double(p.z) +
+         double(a.w) * double(p.w);
+}
+
+// MIXED: x += alpha*p, r -= alpha*Ap and the part of r.r (= r.z, unit diagonal).
+__device__ __forceinline__ void update_row_scaled(const RowGeo &g, bool valid, float *__restrict__ x,
+                                                  const float *__restrict__ pnew,
+                                                  float *__restrict__ r,
+                                                  const float *__restrict__ ap, float alpha,
+                                                  double &rr) {
+  if (!valid) return;
+  V4<float> xv = ld4(x + g.d0), rv = ld4(r + g.d0);
+  const V4<float> pv = ld4(pnew + g.d0), av = ld4(ap + g.d0);
+  xv.x = fmaf(alpha, pv.x, xv.x);
+  xv.y = fmaf(alpha, pv.y, xv.y);
+  xv.z = fmaf(alpha, pv.z, xv.z);
+  xv.w = fmaf(alpha, pv.w, xv.w);
+  rv.x = fmaf(-alpha, av.x, rv.x);
+  rv.y = fmaf(-alpha, av.y, rv.y);
+  rv.z = fmaf(-alpha, av.z, rv.z);
+  rv.w = fmaf(-alpha, av.w, rv.w);
+  st4(x + g.d0, xv);
+  st4(r + g.d0, rv);
+  rr += double(rv.x) * double(rv.x) + double(rv.y) * double(rv.y) + double(rv.z) * double(rv.z) +
+        double(rv.w) * double(rv.w);
+}
+
 // X = X + ALPHA*PCG, RCG = RCG - ALPHA*APCG, TMPCG = CCCI*RCG (congrad.f90:
 // 133-135) and the parts of r.z and r.r (:143-146).
 template <class T>
@@ -107,13 +177,23 @@ __device__ __forceinline__ void update_row(const RowGeo &g, bool valid, T *__res
 // FP64 on a row vector; land slots give 0.
 __device__ __forceinline__ V4<double> residual_row(const RowGeo &g, const uint8_t *kind,
                                                    const double *__restrict__ P,
-                                                   const DevSystem &Y) {
+                                                   const DevSystem &Y, bool asym) {
   const V4<double> x = ld4(P + g.d0), xn = ld4(P + g.dn), xs = ld4(P + g.ds);
   double xw = from_west(x), xe = from_east(x);
   if (g.cx == 0) xw = P[g.dwe];
   if (g.cx == ROWT - 1) xe = P[g.dee];
-  const V4<double> b = ld4(Y.fptmp + g.d0), c = ld4(Y.ccc + g.d0), kn = ld4(Y.ccn + g.d0),
-                   ks = ld4(Y.ccs + g.d0), kw = ld4(Y.ccw + g.d0), ke = ld4(Y.cce + g.d0);
+  const V4<double> b = ld4(Y.fptmp + g.d0), c = ld4(Y.ccc + g.d0), ks = ld4(Y.ccs + g.d0),
+                   kw = ld4(Y.ccw + g.d0);
+  V4<double> kn, ke;
+  if (asym) {
+    kn = ld4(Y.ccn + g.d0);
+    ke = ld4(Y.cce + g.d0);
+  } else {  // CCN(L) = CCS(LN), CCE(L) = CCW(LE)
+    kn = ld4(Y.ccs + g.dn);
+    double kwe = from_east(kw);
+    if (g.cx == ROWT - 1) kwe = Y.ccw[g.dee];
+    ke = {kw.y, kw.z, kw.w, kwe};
+  }
   const uchar4 kd = *reinterpret_cast<const uchar4 *>(kind + g.d0);
   V4<double> r;
   r.x = b.x - c.x * x.x - kn.x * xn.x - ks.x * xs.x - kw.x * xw - ke.x * x.y;

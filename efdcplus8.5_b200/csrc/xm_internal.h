@@ -57,8 +57,11 @@ struct DevState {
 struct DevSystem {
   double *ccc, *ccs, *ccw, *cce, *ccn, *fptmp;  // FP64 scaled coefficients, b
   double *r, *pa, *pb, *ap;                      // FP64 CG vectors (p double-buffered)
-  float *ccc32, *ccs32, *ccw32, *cce32, *ccn32;  // FP32 copies (MIXED)
-  float *r32, *pa32, *pb32, *ap32, *x32;         // FP32 inner CG vectors
+  // MIXED: the FP32 inner system is the Jacobi-scaled operator
+  // Ahat = D^-1/2 A D^-1/2 (unit diagonal, D = CCC), so CG on it equals
+  // Jacobi-PCG on A and needs no diagonal array:
+  float *as32, *aw32, *ae32, *an32;              // off-diagonals of Ahat (E/N only if unsymmetric)
+  float *r32, *pa32, *pb32, *ap32, *x32;         // FP32 inner CG vectors (scaled)
 };
 
 // Device-side control block of one solve.  Written by the "last CTA" of each

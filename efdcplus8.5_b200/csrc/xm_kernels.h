@@ -13,7 +13,8 @@ struct Launch {
   int grid;          // CTAs of the grid-stride cell kernels (one tile per CTA pass)
   int grid_cg;       // CTAs of the FP64 CG kernels (four tiles per CTA pass)
   int grid_mv64;     // CTAs of the FP64 matrix-vector kernel (register-heavy)
-  int grid_cg32;     // CTAs of the FP32 CG kernels (four tiles per CTA pass)
+  int grid_cg32;     // CTAs of the FP32 matrix-vector kernel (four tiles per CTA pass)
+  int grid_up32;     // CTAs of the FP32 update kernel
   int ntile;         // tiles including the ghost tile 0
   cudaStream_t stream;
 };
@@ -32,7 +33,7 @@ void launch_obc(const Launch &l, const DevStatic &S, const DevState &X, const De
                 const StepScalars &c, Ctl *ctl, bool serial);
 void launch_obc_reset(const Launch &l, const DevObc &B, const DevState &X);
 void launch_scale(const Launch &l, const DevStatic &S, const DevState &X, const DevSystem &Y,
-                  Ctl *ctl, int mixed);
+                  Ctl *ctl, int mixed, int write_cross);
 void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                     double *part);
 void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
@@ -76,5 +77,6 @@ int occupancy_blocks_per_sm();
 int occupancy_blocks_per_sm_cg();
 int occupancy_blocks_per_sm_mv64();
 int occupancy_blocks_per_sm_mixed();
+int occupancy_blocks_per_sm_mixed_update();
 
 }  // namespace xm

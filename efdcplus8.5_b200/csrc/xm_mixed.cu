@@ -16,7 +16,7 @@ namespace xm {
   for (int tile = blockIdx.x + 1; tile < (ntile); tile += gridDim.x)
 
 // p = z + beta*p_old at the cell and its neighbours, Ap, p.Ap, ALPHA.
-__global__ void __launch_bounds__(NT) k_mx_matvec(DevStatic S, DevSystem Y, int ntile, Ctl *ctl,
+__global__ void __launch_bounds__(NT, 5) k_mx_matvec(DevStatic S, DevSystem Y, int ntile, Ctl *ctl,
                                                  double *part) {
   __shared__ double sh[32];
   if (ctl->done | ctl->idone) return;
@@ -28,8 +28,8 @@ __global__ void __launch_bounds__(NT) k_mx_matvec(DevStatic S, DevSystem Y, int 
   double acc = 0.0;
   CG_TILE_LOOP(ntile) {
     CG_TILE_GEO(S);
-    acc += matvec_row<float>(g, valid, Y.r32, Y.ccc32, pold, pnew, Y.ccs32, Y.ccw32, Y.cce32,
-                             Y.ccn32, Y.ap32, beta, asym);
+    acc += matvec_row_scaled(g, valid, Y.r32, pold, pnew, Y.as32, Y.aw32, Y.ae32, Y.an32, Y.ap32,
+                             beta, asym);
   }
   acc = block_sum(acc, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = acc;
@@ -50,18 +50,16 @@ __global__ void __launch_bounds__(NT) k_mx_update(DevStatic S, DevSystem Y, int 
   if (ctl->done | ctl->idone) return;
   const float alpha = float(ctl->alpha);
   const float *pnew = ctl->parity ? Y.pa32 : Y.pb32;
-  double a1 = 0.0, a2 = 0.0;
+  double a1 = 0.0;
   CG_TILE_LOOP(ntile) {
     CG_TILE_GEO(S);
-    update_row<float>(g, valid, Y.x32, pnew, Y.r32, Y.ap32, Y.ccc32, alpha, a1, a2);
+    update_row_scaled(g, valid, Y.x32, pnew, Y.r32, Y.ap32, alpha, a1);
   }
   a1 = block_sum(a1, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = a1;
-  a2 = block_sum(a2, sh);
-  if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = a2;
   if (arrive_last(&ctl->counter)) {
-    const double rz = reduce_partials(part, gridDim.x, sh);
-    const double rr = reduce_partials(part + gridDim.x, gridDim.x, sh);
+    const double rz = reduce_partials(part, gridDim.x, sh);  // r.z = r.r (unit diagonal)
+    const double rr = rz;
     if (threadIdx.x == 0) {
       ctl->beta = rz / ctl->rpcg;
       ctl->rpcg = rz;
@@ -89,23 +87,27 @@ void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, C
 }
 void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part, int inner_cap, int total_cap) {
-  k_mx_update<<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part, inner_cap, total_cap);
+  k_mx_update<<<l.grid_up32, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part, inner_cap, total_cap);
   count_launches(1);
 }
 void launch_mx_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                     double *part, int inner_cap, int total_cap) {
   k_mx_matvec<<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
   count_launches(1);
-  k_mx_update<<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part, inner_cap, total_cap);
+  k_mx_update<<<l.grid_up32, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part, inner_cap, total_cap);
   count_launches(1);
 }
 
-int occupancy_blocks_per_sm_mixed() {
-  int a = 0, b = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_mx_matvec, NT, 0);
+int occupancy_blocks_per_sm_mixed_update() {
+  int b = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_mx_update, NT, 0);
-  const int m = std::min(a, b);
-  return m > 0 ? m : 1;
+  return b > 0 ? b : 1;
+}
+
+int occupancy_blocks_per_sm_mixed() {
+  int a = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_mx_matvec, NT, 0);
+  return a > 0 ? a : 1;
 }
 
 }  // namespace xm

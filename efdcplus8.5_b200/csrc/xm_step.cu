@@ -32,7 +32,9 @@ __global__ void __launch_bounds__(NT) k_begin(DevStatic S, DevState X, StepScala
       X.wasted[d] = 0;
     }
     const double P = X.p[d];
-    const double uhdye = X.uhdye[d], vhdxe = X.vhdxe[d];
+    // the host swapped UHDYE<->UHDY1E, VHDXE<->VHDX1E and HP<->H1P before this
+    // step: the *1 buffers hold the values at entry (calpuv2c.f90:256-264)
+    const double uhdye = X.uhdy1e[d], vhdxe = X.vhdx1e[d];
     // :214-220
     X.fuhdye[d] = uhdye - c.deltd2 * sub * S.hruo[d] * X.hu[d] * (P - X.p[q.w]) +
                   sub * c.delt * S.dxiu[d] *
@@ -48,14 +50,10 @@ __global__ void __launch_bounds__(NT) k_begin(DevStatic S, DevState X, StepScala
       X.sbx[d] = S.sbxo[d];
       X.sby[d] = S.sbyo[d];
     }
-    // :256-266
-    X.uhdy1e[d] = uhdye;
-    X.vhdx1e[d] = vhdxe;
-    X.h1p[d] = X.hp[d];
     // :282-290
     const double C1 = 0.5 * c.g;
     X.fp1[d] = c.delti * S.dxyp[d] * P -
-               C1 * (X.uhdye[q.e] - uhdye + X.vhdxe[q.n] - vhdxe);
+               C1 * (X.uhdy1e[q.e] - uhdye + X.vhdx1e[q.n] - vhdxe);
   }
 }
 
@@ -185,16 +183,24 @@ __device__ __forceinline__ void obc2_cell(const DevState &X, const DevObc &B, in
   }
 }
 
-// One CTA; boundary cells in parallel (hazard-free layouts only).
+// Boundary cells in parallel, one thread each (hazard-free layouts only: no
+// two cells share an interior target and no target is a boundary cell, so
+// SETOPENBC's and SETOPENBC2's writes to the targets commute).  The minimum
+// CC of the boundary cells goes to ctl->ccmnm_bc by an atomic min on the bit
+// pattern, which orders non-negative doubles like their values (CC >= 0 here).
 __global__ void __launch_bounds__(NT) k_obc_parallel(DevStatic S, DevState X, DevObc B,
                                                     StepScalars c, Ctl *ctl) {
   __shared__ double sh[32];
   double mn = 1.e+18;
-  for (int k = threadIdx.x; k < B.n; k += NT) mn = fmin(mn, obc_cell(S, X, B, c, k));
-  __syncthreads();
-  for (int k = threadIdx.x; k < B.n; k += NT) obc2_cell(X, B, k);
+  const int k = blockIdx.x * NT + threadIdx.x;
+  if (k < B.n) {
+    mn = obc_cell(S, X, B, c, k);
+    obc2_cell(X, B, k);
+  }
   mn = block_min(mn, sh);
-  if (threadIdx.x == 0) ctl->ccmnm_bc = mn;
+  if (threadIdx.x == 0)
+    atomicMin(reinterpret_cast<unsigned long long *>(&ctl->ccmnm_bc),
+              static_cast<unsigned long long>(__double_as_longlong(fmax(mn, 0.0))));
 }
 
 // One thread, the reference's exact loop order (layouts where boundary cells
@@ -218,7 +224,7 @@ __global__ void k_obc_reset(DevObc B, DevState X) {
 // Also flags an unsymmetric operator (CE(L) /= CW(LE) or CN(L) /= CS(LN)),
 // which only a radiation boundary with a closed interior face produces.
 __global__ void __launch_bounds__(NT) k_scale(DevStatic S, DevState X, DevSystem Y, int ntile,
-                                             Ctl *ctl, int mixed) {
+                                             Ctl *ctl, int write_cross) {
   const double CCMNM = fmin(ctl->ccmnm_int, ctl->ccmnm_bc);
   const double CCMNMI = 1. / CCMNM;
   bool asym = false;
@@ -233,19 +239,16 @@ __global__ void __launch_bounds__(NT) k_scale(DevStatic S, DevState X, DevSystem
     const double fpt = X.fp[d] * CCMNMI;
     Y.ccs[d] = ccs;
     Y.ccw[d] = ccw;
-    Y.cce[d] = cce;
-    Y.ccn[d] = ccn;
     Y.ccc[d] = ccc;
     Y.fptmp[d] = fpt;
-    if (mixed) {
-      Y.ccs32[d] = float(ccs);
-      Y.ccw32[d] = float(ccw);
-      Y.cce32[d] = float(cce);
-      Y.ccn32[d] = float(ccn);
-      Y.ccc32[d] = float(ccc);
+    if (write_cross) {
+      Y.cce[d] = cce;
+      Y.ccn[d] = ccn;
     }
   }
-  if (__syncthreads_or(asym) && threadIdx.x == 0) atomicOr(&ctl->asym, 1);
+  // an unsymmetric operator without the cross coefficients written cannot be
+  // solved: flag it (status 2) so that the host reports it
+  if (__syncthreads_or(asym) && threadIdx.x == 0) atomicOr(&ctl->asym, write_cross ? 1 : 3);
 }
 
 // ---------------------------------------------------------------------------
@@ -257,10 +260,11 @@ __global__ void __launch_bounds__(NT) k_scale(DevStatic S, DevState X, DevSystem
 __global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double *P, int ntile,
                                                Ctl *ctl, double *part) {
   __shared__ double sh[32];
+  const bool asym = ctl->asym;
   double acc = 0.0;
   CG_TILE_LOOP(ntile) {
     CG_TILE_GEO(S);
-    const V4<double> r = residual_row(g, S.kind, P, Y);
+    const V4<double> r = residual_row(g, S.kind, P, Y, asym);
     const V4<double> c = ld4(Y.ccc + g.d0);
     const V4<double> z = {r.x * rcpT(c.x), r.y * rcpT(c.y), r.z * rcpT(c.z), r.w * rcpT(c.w)};
     if (valid) {
@@ -367,21 +371,22 @@ __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, DevSystem Y, const
                                                 int ntile, Ctl *ctl, double *part, double rsqm,
                                                 double rel_tol) {
   __shared__ double sh[32];
+  const bool asym = ctl->asym;
   double a1 = 0.0, a2 = 0.0;
   CG_TILE_LOOP(ntile) {
     CG_TILE_GEO(S);
-    const V4<double> r = residual_row(g, S.kind, P, Y);
-    const V4<float> c = ld4(Y.ccc32 + g.d0);
-    const V4<float> r32 = {float(r.x), float(r.y), float(r.z), float(r.w)};
-    const V4<float> z32 = {r32.x * rcpT(c.x), r32.y * rcpT(c.y), r32.z * rcpT(c.z),
-                           r32.w * rcpT(c.w)};
+    const V4<double> r = residual_row(g, S.kind, P, Y, asym);
+    const V4<double> c = ld4(Y.ccc + g.d0);
+    // scaled residual rhat = D^-1/2 r of the Jacobi-scaled inner system
+    const V4<float> r32 = {float(r.x / sqrt(c.x)), float(r.y / sqrt(c.y)), float(r.z / sqrt(c.z)),
+                           float(r.w / sqrt(c.w))};
     if (valid) {
       st4(Y.r32 + g.d0, r32);
-      st4(Y.pa32 + g.d0, z32);
+      st4(Y.pa32 + g.d0, r32);
       st4(Y.x32 + g.d0, V4<float>{0.f, 0.f, 0.f, 0.f});
       a1 += r.x * r.x + r.y * r.y + r.z * r.z + r.w * r.w;
-      a2 += double(r32.x) * double(z32.x) + double(r32.y) * double(z32.y) +
-            double(r32.z) * double(z32.z) + double(r32.w) * double(z32.w);
+      a2 += double(r32.x) * double(r32.x) + double(r32.y) * double(r32.y) +
+            double(r32.z) * double(r32.z) + double(r32.w) * double(r32.w);
     }
   }
   a1 = block_sum(a1, sh);
@@ -400,8 +405,10 @@ __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, DevSystem Y, const
       ctl->inner_iter = 0;
       ctl->idone = 0;
       ctl->outer += 1;
-      const double tgt = fmax(rsq * rel_tol * rel_tol, 0.1 * rsqm);
-      ctl->rsq_target = tgt;
+      // inner stop on the scaled residual: reduce it by the factor the FP64
+      // residual needs to reach 0.1*RSQM, and by at least rel_tol (in norm)
+      const double need = (rsq > 0.0) ? 0.1 * rsqm / rsq : 1.0;
+      ctl->rsq_target = rz * fmax(fmin(need, 1.0), rel_tol * rel_tol);
       if (!isfinite(rsq)) {
         ctl->done = 1;
         ctl->status = EFDC_XM_NONFINITE;
@@ -415,27 +422,47 @@ __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, DevSystem Y, const
   }
 }
 
-// MIXED: P += x32 (the FP32 correction).
+// MIXED: P += D^-1/2 x32 (the FP32 correction of the scaled system).
 __global__ void __launch_bounds__(NT) k_mx_apply(DevStatic S, DevSystem Y, double *P, int ntile) {
   CG_TILE_LOOP(ntile) {
     CG_TILE_GEO(S);
     if (!valid) continue;
     V4<double> x = ld4(P + g.d0);
+    const V4<double> c = ld4(Y.ccc + g.d0);
     const V4<float> d = ld4(Y.x32 + g.d0);
-    x.x = x.x + double(d.x);
-    x.y = x.y + double(d.y);
-    x.z = x.z + double(d.z);
-    x.w = x.w + double(d.w);
+    // P += D^-1/2 xhat
+    x.x = x.x + double(d.x) / sqrt(c.x);
+    x.y = x.y + double(d.y) / sqrt(c.y);
+    x.z = x.z + double(d.z) / sqrt(c.z);
+    x.w = x.w + double(d.w) / sqrt(c.w);
     st4(P + g.d0, x);
   }
 }
 
 // ---------------------------------------------------------------------------
+// MIXED: the FP32 inner operator Ahat = D^-1/2 A D^-1/2 with D = CCC (unit
+// diagonal): AS(L) = CCS(L)/sqrt(CCC(L)*CCC(LS)), AW likewise; AE, AN only
+// when the operator can be unsymmetric (else AE(L)=AW(LE), AN(L)=AS(LN)).
+__global__ void __launch_bounds__(NT) k_scale32(DevStatic S, DevSystem Y, int ntile,
+                                               int write_cross) {
+  TILE_LOOP(ntile) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    const double di = 1. / sqrt(Y.ccc[d]);
+    Y.as32[d] = float(Y.ccs[d] * di / sqrt(Y.ccc[q.s]));
+    Y.aw32[d] = float(Y.ccw[d] * di / sqrt(Y.ccc[q.w]));
+    if (write_cross) {
+      Y.ae32[d] = float(Y.cce[d] * di / sqrt(Y.ccc[q.e]));
+      Y.an32[d] = float(Y.ccn[d] * di / sqrt(Y.ccc[q.n]));
+    }
+  }
+}
+
 // Standalone CONGRAD: a caller-assembled scaled system.  Land slots are made
 // inert (CCC=1, couplings 0, b=0), FP32 copies made for MIXED, and the
 // symmetry of the given CCE/CCN against CCW(LE)/CCS(LN) is recorded.
-__global__ void __launch_bounds__(NT) k_sys_prepare(DevStatic S, DevSystem Y, int ntile, Ctl *ctl,
-                                                   int mixed) {
+__global__ void __launch_bounds__(NT) k_sys_prepare(DevStatic S, DevSystem Y, int ntile, Ctl *ctl) {
   bool asym = false;
   TILE_LOOP(ntile) {
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
@@ -443,8 +470,6 @@ __global__ void __launch_bounds__(NT) k_sys_prepare(DevStatic S, DevSystem Y, in
     if (S.kind[d] == LAND) {
       Y.ccc[d] = 1.0;
       Y.ccs[d] = Y.ccw[d] = Y.cce[d] = Y.ccn[d] = Y.fptmp[d] = 0.0;
-      Y.ccc32[d] = 1.0f;
-      Y.ccs32[d] = Y.ccw32[d] = Y.cce32[d] = Y.ccn32[d] = 0.0f;
       continue;
     }
     const double cce = Y.cce[d], ccn = Y.ccn[d];
@@ -452,13 +477,6 @@ __global__ void __launch_bounds__(NT) k_sys_prepare(DevStatic S, DevSystem Y, in
     const double ccw_e = (S.kind[q.e] == LAND) ? 0.0 : Y.ccw[q.e];
     const double ccs_n = (S.kind[q.n] == LAND) ? 0.0 : Y.ccs[q.n];
     asym |= (cce != ccw_e) || (ccn != ccs_n);
-    if (mixed) {
-      Y.ccc32[d] = float(Y.ccc[d]);
-      Y.ccs32[d] = float(Y.ccs[d]);
-      Y.ccw32[d] = float(Y.ccw[d]);
-      Y.cce32[d] = float(cce);
-      Y.ccn32[d] = float(ccn);
-    }
   }
   if (__syncthreads_or(asym) && threadIdx.x == 0) atomicOr(&ctl->asym, 1);
 }
@@ -828,7 +846,7 @@ void launch_obc(const Launch &l, const DevStatic &S, const DevState &X, const De
   if (serial)
     k_obc_serial<<<1, 1, 0, l.stream>>>(S, X, B, c, ctl);
   else
-    k_obc_parallel<<<1, NT, 0, l.stream>>>(S, X, B, c, ctl);
+    k_obc_parallel<<<(B.n + NT - 1) / NT, NT, 0, l.stream>>>(S, X, B, c, ctl);
   count_launches(1);
 }
 void launch_obc_reset(const Launch &l, const DevObc &B, const DevState &X) {
@@ -837,9 +855,13 @@ void launch_obc_reset(const Launch &l, const DevObc &B, const DevState &X) {
   count_launches(1);
 }
 void launch_scale(const Launch &l, const DevStatic &S, const DevState &X, const DevSystem &Y,
-                  Ctl *ctl, int mixed) {
-  k_scale<<<l.grid, NT, 0, l.stream>>>(S, X, Y, l.ntile, ctl, mixed);
+                  Ctl *ctl, int mixed, int write_cross) {
+  k_scale<<<l.grid, NT, 0, l.stream>>>(S, X, Y, l.ntile, ctl, write_cross);
   count_launches(1);
+  if (mixed) {
+    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, write_cross);
+    count_launches(1);
+  }
 }
 void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                     double *part) {
@@ -923,8 +945,12 @@ void launch_gather(cudaStream_t st, const CopyJob *jobs, int njob, const int *li
 
 void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                         int mixed) {
-  k_sys_prepare<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, mixed);
+  k_sys_prepare<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, ctl);
   count_launches(1);
+  if (mixed) {  // the standalone system may be unsymmetric: always the 4-array form
+    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, 1);
+    count_launches(1);
+  }
 }
 
 int occupancy_blocks_per_sm() {
