@@ -1,6 +1,7 @@
 // xm_capi.cu -- the C-ABI of libefdc_xm (include/efdc_xm.h): context set-up
-// (tile layout, device arrays), host<->device transfers, and the host-side
-// orchestration of one CALPUV2C step (calpuv2c.f90:128-1187) and of CONGRAD.
+// (tile layout of M >= 1 basins, device arrays), host<->device transfers, and
+// the host-side orchestration of one CALPUV2C step (calpuv2c.f90:128-1187) of
+// every member and of CONGRAD.
 
 #include <algorithm>
 #include <atomic>
@@ -9,9 +10,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
-#include <map>
 #include <string>
-#include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "xm_kernels.h"
@@ -42,6 +42,7 @@ std::atomic<long long> g_launches{0};
 
 using xm::CopyJob;
 using xm::Ctl;
+using xm::Glob;
 using xm::TILE;
 
 uint64_t morton2(uint32_t x, uint32_t y) {
@@ -57,6 +58,9 @@ uint64_t morton2(uint32_t x, uint32_t y) {
   return spread(x) | (spread(y) << 1);
 }
 
+constexpr int NSTAGE = 8;     // staging buffers (each holds one array of every member)
+constexpr int MAX_JOBS = 64;  // arrays moved by one upload/download call
+
 }  // namespace
 
 namespace xm {
@@ -70,44 +74,57 @@ struct DevBuf {
   size_t bytes = 0;
 };
 
+// One basin of the context.
+struct Member {
+  int la = 0, lc = 0;
+  int tile0 = 0, tile1 = 0;  // its tiles [tile0, tile1)
+  long long off = 0;         // element offset of its arrays in the staging buffers
+  int nobc = 0, b0 = 0;      // its open-boundary cells [b0, b0+nobc) of the packed list
+  int side_n[4] = {0, 0, 0, 0};
+  int mtide = 0;
+  std::vector<double> tcp;
+  bool may_asym = false;  // a radiation boundary: the operator can be unsymmetric
+  int last_iters = 8, last_inner = 8;
+  int last_n = 0, last_ntstbc = 0, last_isdry = 0;
+  std::vector<int32_t> oldmask_h;
+};
+
 struct efdc_xm_ctx {
   int device = 0;
-  int la = 0, lc = 0;
-  int ntile = 0, nslot = 0, grid = 1, grid_cg = 1, grid_mv64 = 1, grid_cg32 = 1, grid_up32 = 1, nsm = 0;
+  int M = 0;
+  std::vector<Member> mem;
+  int ntile = 0, nslot = 0, nquad = 0;
+  int grid = 1, grid_cg = 1, grid_mv64 = 1, grid_cg32 = 1, grid_up32 = 1, nsm = 0;
+  long long stage_len = 0;  // elements of one staging buffer
   cudaStream_t stream = nullptr;
   std::vector<DevBuf> bufs;
-  // host copies of the layout
-  std::vector<int> slot_of_L;  // [lc+1], slot of water cell L (0 otherwise)
-  std::vector<int> lidx_h;     // [nslot]
   // device views
   xm::DevStatic S{};
   xm::DevState X{};
   xm::DevSystem Y{};
   xm::DevObc B{};
-  Ctl *ctl = nullptr;
-  Ctl *ctl_h = nullptr;  // pinned mirror
+  Ctl *ctl = nullptr;                // [M]
+  Ctl *ctl_h = nullptr;              // [M] pinned mirror
+  Glob *glob = nullptr;
+  Glob *glob_h = nullptr;            // pinned
+  int *act = nullptr;                // [M] member takes part in the current sweep
+  int *act_h = nullptr;              // [M] pinned
+  xm::StepScalars *sc = nullptr;     // [M]
+  xm::StepScalars *sc_h = nullptr;   // [M] pinned
   double *part = nullptr;
   int *lidx = nullptr;
-  // staging: device buffers in host (L) order, one per transferable array
+  int *tile_member = nullptr;
+  long long *moff = nullptr;
+  int *mlc = nullptr;
   std::vector<double *> stage;
   CopyJob *jobs_d = nullptr;
   CopyJob *jobs_h = nullptr;  // pinned
-  int max_jobs = 0;
-  // open boundaries
   bool obc_serial = false;
-  bool may_asym = false;  // a radiation boundary exists: the operator can be unsymmetric
+  bool any_may_asym = false;
   int nobc = 0;
-  int side_n[4] = {0, 0, 0, 0};
-  std::vector<double> tcp;
-  int mtide = 0;
   double *pser_d = nullptr;
   double *pser_h = nullptr;  // pinned
   double *ptmp = nullptr;    // scratch P for kernel timing
-  // bookkeeping
-  int last_iters = 8;
-  int last_inner = 8;
-  int last_n = 0, last_ntstbc = 0, last_isdry = 0;
-  std::vector<int32_t> oldmask_h;
 
   template <class T>
   T *alloc(size_t n, bool zero = true) {
@@ -118,179 +135,194 @@ struct efdc_xm_ctx {
     bufs.push_back(b);
     return static_cast<T *>(b.p);
   }
-  xm::Launch L() const { return xm::Launch{grid, grid_cg, grid_mv64, grid_cg32, grid_up32, ntile, stream}; }
+  xm::Launch L() const {
+    return xm::Launch{grid, grid_cg, grid_mv64, grid_cg32, grid_up32, ntile, stream};
+  }
 };
 
 namespace {
 
-// Scatter host-order device staging buffers into tile-order arrays.
-int run_scatter(efdc_xm_ctx *c, const std::vector<CopyJob> &jobs) {
-  if (jobs.empty()) return EFDC_XM_OK;
-  for (size_t base = 0; base < jobs.size(); base += c->max_jobs) {
-    const int n = int(std::min<size_t>(c->max_jobs, jobs.size() - base));
-    std::memcpy(c->jobs_h, jobs.data() + base, n * sizeof(CopyJob));
-    CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, n * sizeof(CopyJob), cudaMemcpyHostToDevice, c->stream));
-    xm::launch_scatter(c->stream, c->jobs_d, n, c->lidx, c->nslot, c->lc);
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(c->stream));
-  }
-  return EFDC_XM_OK;
-}
-
-int run_gather(efdc_xm_ctx *c, const std::vector<CopyJob> &jobs) {
-  if (jobs.empty()) return EFDC_XM_OK;
-  for (size_t base = 0; base < jobs.size(); base += c->max_jobs) {
-    const int n = int(std::min<size_t>(c->max_jobs, jobs.size() - base));
-    std::memcpy(c->jobs_h, jobs.data() + base, n * sizeof(CopyJob));
-    CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, n * sizeof(CopyJob), cudaMemcpyHostToDevice, c->stream));
-    xm::launch_gather(c->stream, c->jobs_d, n, c->lidx, c->nslot);
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(c->stream));
-  }
-  return EFDC_XM_OK;
-}
-
-// Transfer plan entry: a host array (element L at [L-1], LC elements) and the
-// tile-order device array it maps to.
+// Transfer plan entry: one array of every member (host pointers, element L
+// at [L-1], LC elements) and the tile-order device array.
 struct Xfer {
-  const void *host;
+  std::vector<const void *> host;  // [M]
   void *dev;
   int kind;  // 0 double, 1 LOGICAL (normalised to 0/1), 2 raw int, 3 double water-only
 };
 
-int upload_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
-  std::vector<CopyJob> jobs;
-  size_t k = 0;
-  for (const Xfer &x : xs) {
-    if (!x.host || !x.dev) continue;
-    if (k >= c->stage.size()) {
-      set_error("internal: staging exhausted");
-      return EFDC_XM_CUDA_ERROR;
-    }
-    const size_t bytes = size_t(c->lc) * ((x.kind == 1 || x.kind == 2) ? sizeof(int32_t) : sizeof(double));
-    CK(cudaMemcpyAsync(c->stage[k], x.host, bytes, cudaMemcpyHostToDevice, c->stream));
-    jobs.push_back(CopyJob{c->stage[k], x.dev, x.kind});
-    ++k;
+size_t esize(int kind) { return (kind == 1 || kind == 2) ? sizeof(int32_t) : sizeof(double); }
+
+// A field moves when every member gives it; given for some members only, it is an error.
+int collect(efdc_xm_ctx *c, std::vector<Xfer> &out, const std::vector<const void *> &ptrs,
+            const void *dev, int kind, const char *name) {
+  int n = 0;
+  for (const void *p : ptrs) n += p ? 1 : 0;
+  if (n == 0 || !dev) return EFDC_XM_OK;
+  if (n != c->M) {
+    set_error("field %s is given for %d of %d members (all or none)", name, n, c->M);
+    return EFDC_XM_BAD_ARGUMENT;
   }
-  return run_scatter(c, jobs);
+  out.push_back(Xfer{ptrs, const_cast<void *>(dev), kind});
+  return EFDC_XM_OK;
+}
+
+int upload_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
+  if (xs.empty()) return EFDC_XM_OK;
+  if (xs.size() > size_t(MAX_JOBS)) {
+    set_error("internal: too many arrays in one transfer");
+    return EFDC_XM_CUDA_ERROR;
+  }
+  for (size_t j = 0; j < xs.size(); ++j)
+    c->jobs_h[j] = CopyJob{c->stage[j % NSTAGE], xs[j].dev, xs[j].kind};
+  CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, xs.size() * sizeof(CopyJob), cudaMemcpyHostToDevice,
+                     c->stream));
+  for (size_t g0 = 0; g0 < xs.size(); g0 += NSTAGE) {
+    const size_t g1 = std::min(xs.size(), g0 + NSTAGE);
+    for (size_t j = g0; j < g1; ++j) {
+      const size_t es = esize(xs[j].kind);
+      char *dst = reinterpret_cast<char *>(c->stage[j % NSTAGE]);
+      for (int m = 0; m < c->M; ++m)
+        CK(cudaMemcpyAsync(dst + c->mem[m].off * es, xs[j].host[m], size_t(c->mem[m].lc) * es,
+                           cudaMemcpyHostToDevice, c->stream));
+    }
+    // stream order: the next group's copies into the same staging buffers
+    // start after this scatter has read them
+    xm::launch_scatter(c->stream, c->jobs_d + g0, int(g1 - g0), c->lidx, c->tile_member, c->moff,
+                       c->mlc, c->nslot);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return EFDC_XM_OK;
 }
 
 int download_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
-  std::vector<CopyJob> jobs;
-  std::vector<std::pair<void *, size_t>> dst;
-  size_t k = 0;
-  for (const Xfer &x : xs) {
-    if (!x.host || !x.dev) continue;
-    // the gather fills elements L=2..LA (indices 1..LA-1); only that range
-    // goes back, so the caller's ghost elements 1 and LC are left alone
-    const size_t esz = ((x.kind == 1 || x.kind == 2) ? sizeof(int32_t) : sizeof(double));
-    jobs.push_back(CopyJob{c->stage[k], x.dev, x.kind});
-    dst.push_back({const_cast<void *>(x.host), esz});
-    ++k;
+  if (xs.empty()) return EFDC_XM_OK;
+  if (xs.size() > size_t(MAX_JOBS)) {
+    set_error("internal: too many arrays in one transfer");
+    return EFDC_XM_CUDA_ERROR;
   }
-  int rc = run_gather(c, jobs);
-  if (rc) return rc;
-  for (size_t i = 0; i < dst.size(); ++i) {
-    const size_t esz = dst[i].second;
-    CK(cudaMemcpyAsync(static_cast<char *>(dst[i].first) + esz,
-                       reinterpret_cast<const char *>(c->stage[i]) + esz, esz * size_t(c->la - 1),
-                       cudaMemcpyDeviceToHost, c->stream));
+  for (size_t j = 0; j < xs.size(); ++j)
+    c->jobs_h[j] = CopyJob{c->stage[j % NSTAGE], xs[j].dev, xs[j].kind};
+  CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, xs.size() * sizeof(CopyJob), cudaMemcpyHostToDevice,
+                     c->stream));
+  for (size_t g0 = 0; g0 < xs.size(); g0 += NSTAGE) {
+    const size_t g1 = std::min(xs.size(), g0 + NSTAGE);
+    xm::launch_gather(c->stream, c->jobs_d + g0, int(g1 - g0), c->lidx, c->tile_member, c->moff,
+                      c->nslot);
+    CK(cudaGetLastError());
+    // the gather fills elements L=2..LA (indices 1..LA-1) of each member; only
+    // that range goes back, so the caller's ghost elements 1 and LC stay as they are
+    for (size_t j = g0; j < g1; ++j) {
+      const size_t es = esize(xs[j].kind);
+      const char *src = reinterpret_cast<const char *>(c->stage[j % NSTAGE]);
+      for (int m = 0; m < c->M; ++m)
+        CK(cudaMemcpyAsync(static_cast<char *>(const_cast<void *>(xs[j].host[m])) + es,
+                           src + (c->mem[m].off + 1) * es, es * size_t(c->mem[m].la - 1),
+                           cudaMemcpyDeviceToHost, c->stream));
+    }
   }
   CK(cudaStreamSynchronize(c->stream));
   return EFDC_XM_OK;
 }
 
 int read_ctl(efdc_xm_ctx *c) {
-  CK(cudaMemcpyAsync(c->ctl_h, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->ctl_h, c->ctl, sizeof(Ctl) * c->M, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return EFDC_XM_OK;
 }
 
-int write_ctl(efdc_xm_ctx *c) {
-  CK(cudaMemcpyAsync(c->ctl, c->ctl_h, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+int read_glob(efdc_xm_ctx *c) {
+  CK(cudaMemcpyAsync(c->glob_h, c->glob, sizeof(Glob), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return EFDC_XM_OK;
 }
 
-// FP64 CONGRAD on the scaled system in c->Y, P = c->X.p (or `P`).
-int solve_fp64(efdc_xm_ctx *c, double *P, double rsqm, int iterm, int *iters, double *rsq,
-               int *status) {
+int write_act(efdc_xm_ctx *c) {
+  CK(cudaMemcpyAsync(c->act, c->act_h, sizeof(int) * c->M, cudaMemcpyHostToDevice, c->stream));
+  return EFDC_XM_OK;
+}
+
+// FP64 CONGRAD of every active member on the scaled system in c->Y.  The
+// members iterate in lockstep launches; a member that has stopped is skipped
+// by the kernels.  On return c->ctl_h holds each member's outcome.
+int solve_fp64(efdc_xm_ctx *c, double *P) {
   const xm::Launch l = c->L();
-  xm::launch_cg_init(l, c->S, c->Y, P, c->ctl, c->part);
+  xm::launch_solve_reset(l, c->ctl, c->glob, c->act, c->M);
+  xm::launch_cg_init(l, c->S, c->Y, P, c->ctl, c->glob, c->part);
   CK(cudaGetLastError());
+  int chunk = 1, cap = 1;
+  for (int m = 0; m < c->M; ++m)
+    if (c->act_h[m]) {
+      chunk = std::max(chunk, c->mem[m].last_iters);
+      cap = std::max(cap, c->sc_h[m].iterm);
+    }
+  chunk = std::min(chunk, cap);
   int launched = 0;
-  int chunk = std::max(1, std::min(c->last_iters, iterm));
   for (;;) {
-    for (int k = 0; k < chunk && launched < iterm; ++k, ++launched)
-      xm::launch_cg_iter(l, c->S, c->Y, P, c->ctl, c->part, rsqm, iterm);
+    for (int k = 0; k < chunk && launched < cap; ++k, ++launched)
+      xm::launch_cg_iter(l, c->S, c->Y, P, c->ctl, c->glob, c->part);
     CK(cudaGetLastError());
-    int rc = read_ctl(c);
+    int rc = read_glob(c);
     if (rc) return rc;
-    if (c->ctl_h->done || launched >= iterm) break;
+    if (c->glob_h->ndone >= c->M || launched >= cap) break;
     chunk = 4;
   }
-  *iters = c->ctl_h->iter;
-  *rsq = c->ctl_h->rsq;
-  *status = c->ctl_h->status;
-  if (!c->ctl_h->done) *status = EFDC_XM_CG_MAXITER;
-  if (*iters > 0) c->last_iters = *iters;
-  return EFDC_XM_OK;
-}
-
-// MIXED: FP64 refinement around the FP32 inner PCG.
-int solve_mixed(efdc_xm_ctx *c, double *P, double rsqm_ref, int iterm, int *iters, double *rsq,
-                int *status, int *outer, double factor) {
-  const xm::Launch l = c->L();
-  // the FP32 path stops on the FP64 residual, past the reference's RSQM
-  const double rsqm = rsqm_ref * (factor > 0 ? factor : 0.1);
-  const int total_cap = 2 * iterm + 50;
-  const int max_outer = 30;
-  const double rel_tol = 1e-6;  // inner: |r| down 1e-6 (FP32 reaches ~1e-7 here)
-  // reset the solve bookkeeping
   int rc = read_ctl(c);
   if (rc) return rc;
-  c->ctl_h->iter = 0;
-  c->ctl_h->outer = 0;
-  c->ctl_h->done = 0;
-  c->ctl_h->idone = 0;
-  c->ctl_h->status = 0;
-  c->ctl_h->counter = 0;
-  rc = write_ctl(c);
-  if (rc) return rc;
-  bool converged = false;
-  for (int o = 0; o < max_outer; ++o) {
-    xm::launch_mx_resid(l, c->S, c->Y, P, c->ctl, c->part, rsqm, rel_tol);
-    CK(cudaGetLastError());
-    rc = read_ctl(c);
-    if (rc) return rc;
-    if (c->ctl_h->done) {
-      converged = (c->ctl_h->status == 0);
-      break;
-    }
-    if (c->ctl_h->iter >= total_cap) break;
-    int chunk = std::max(1, c->last_inner);
-    for (;;) {
-      for (int k = 0; k < chunk; ++k)
-        xm::launch_mx_iter(l, c->S, c->Y, c->ctl, c->part, iterm, total_cap);
-      CK(cudaGetLastError());
-      rc = read_ctl(c);
-      if (rc) return rc;
-      if (c->ctl_h->idone || c->ctl_h->done) break;
-      chunk = 4;
-    }
-    if (c->ctl_h->inner_iter > 0) c->last_inner = c->ctl_h->inner_iter;
-    if (c->ctl_h->done) break;  // non-finite
-    xm::launch_mx_apply(l, c->S, c->Y, P);
-    CK(cudaGetLastError());
+  for (int m = 0; m < c->M; ++m) {
+    if (!c->act_h[m]) continue;
+    Ctl &k = c->ctl_h[m];
+    if (!k.done && k.status == 0) k.status = EFDC_XM_CG_MAXITER;
+    if (k.iter > 0) c->mem[m].last_iters = k.iter;
   }
-  *iters = c->ctl_h->iter;
-  *rsq = c->ctl_h->rsq64;
-  *outer = c->ctl_h->outer;
-  *status = c->ctl_h->status;
-  if (*status == 0 && !converged) *status = EFDC_XM_CG_MAXITER;
   return EFDC_XM_OK;
 }
 
-xm::StepScalars make_scalars(const efdc_xm_ctx *c, const efdc_xm_params *p) {
+// MIXED: FP64 refinement around the FP32 inner PCG, all active members in
+// lockstep outer passes.
+int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
+  const xm::Launch l = c->L();
+  const double fac = factor > 0 ? factor : 0.1;  // stop at fac*RSQM in FP64
+  const int max_outer = 30;
+  const double rel_tol = 1e-6;  // inner: |r| down 1e-6 at least (FP32 reaches ~1e-7 here)
+  xm::launch_solve_reset(l, c->ctl, c->glob, c->act, c->M);
+  int rc = 0;
+  for (int o = 0; o < max_outer; ++o) {
+    xm::launch_outer_reset(l, c->glob);
+    xm::launch_mx_resid(l, c->S, c->Y, P, c->ctl, c->glob, c->part, fac, rel_tol, 0);
+    CK(cudaGetLastError());
+    if ((rc = read_glob(c))) return rc;
+    if (c->glob_h->ndone >= c->M) break;
+    int chunk = 1;
+    for (int m = 0; m < c->M; ++m)
+      if (c->act_h[m]) chunk = std::max(chunk, c->mem[m].last_inner);
+    for (int guard = 0;; ++guard) {
+      for (int k = 0; k < chunk; ++k) xm::launch_mx_iter(l, c->S, c->Y, c->ctl, c->glob, c->part);
+      CK(cudaGetLastError());
+      if ((rc = read_glob(c))) return rc;
+      if (c->glob_h->nidone + c->glob_h->ndone >= c->M) break;
+      chunk = 4;
+      if (guard > 100000) {  // the inner stop test caps iterations; this is a backstop
+        set_error("internal: inner solve did not finish");
+        return EFDC_XM_CUDA_ERROR;
+      }
+    }
+    xm::launch_mx_apply(l, c->S, c->Y, P, c->ctl);
+    CK(cudaGetLastError());
+    if ((rc = read_ctl(c))) return rc;
+    for (int m = 0; m < c->M; ++m)
+      if (c->act_h[m] && c->ctl_h[m].inner_iter > 0) c->mem[m].last_inner = c->ctl_h[m].inner_iter;
+  }
+  if ((rc = read_ctl(c))) return rc;
+  for (int m = 0; m < c->M; ++m) {
+    if (!c->act_h[m]) continue;
+    Ctl &k = c->ctl_h[m];
+    if (!k.done && k.status == 0) k.status = EFDC_XM_CG_MAXITER;
+  }
+  return EFDC_XM_OK;
+}
+
+xm::StepScalars make_scalars(const Member &mb, const efdc_xm_params *p) {
   xm::StepScalars s{};
   s.delt = p->delt;
   s.deltd2 = 0.5 * p->delt;  // calpuv2c.f90:129-135
@@ -306,13 +338,118 @@ xm::StepScalars make_scalars(const efdc_xm_ctx *c, const efdc_xm_params *p) {
   s.isbal = p->isbal;
   s.iterm = p->iterm;
   // setopenbc.f90:24-29 on the host, libm as the reference
-  for (int m = 0; m < c->mtide && m < xm::MT_MAX; ++m) {
-    double TM = std::fmod(p->tn, c->tcp[m]);
-    TM = p->pi2 * TM / c->tcp[m];
+  for (int m = 0; m < mb.mtide && m < xm::MT_MAX; ++m) {
+    double TM = std::fmod(p->tn, mb.tcp[m]);
+    TM = p->pi2 * TM / mb.tcp[m];
     s.cosv[m] = std::cos(TM);
     s.sinv[m] = std::sin(TM);
   }
   return s;
+}
+
+// Tile layout of one member on the host.
+struct MemberLayout {
+  std::vector<std::pair<uint64_t, int>> tiles;  // (Morton key, ty*ntx+tx), Morton order
+  std::vector<int> tile_of;                     // local tile number (1-based) of (tx,ty), 0 none
+  int ntx = 0, nty = 0, imin = 0, jmin = 0;
+};
+
+// Checks one member's grid (a structured grid with the reference's
+// neighbour maps) and lays out its tiles.  Returns false with the error set.
+bool member_layout(const efdc_xm_grid *g, int mi, MemberLayout &ml) {
+  const int la = g->la, lc = g->lc;
+  if (la < 2 || lc != la + 1) {
+    set_error("efdc_xm_create: member %d: need LA >= 2 and LC == LA+1 (got LA=%d LC=%d)", mi, la,
+              lc);
+    return false;
+  }
+  if (!g->il || !g->jl || !g->lnc || !g->lsc || !g->lec || !g->lwc) {
+    set_error("efdc_xm_create: member %d: IL, JL and the four neighbour maps are required", mi);
+    return false;
+  }
+  const double *req[] = {g->dxyp, g->dxyip, g->dxiu, g->dyiu, g->dxiv, g->dyiv, g->dxyu, g->dxyv,
+                         g->hruo, g->hrvo, g->subo, g->svbo, g->sbxo, g->sbyo, g->belv};
+  for (const double *r : req)
+    if (!r) {
+      set_error("efdc_xm_create: member %d: a metric array is NULL", mi);
+      return false;
+    }
+  if (g->mtide < 0 || g->mtide > xm::MT_MAX || (g->mtide > 0 && !g->tcp)) {
+    set_error("efdc_xm_create: member %d: MTIDE must be in 0..%d with TCP given", mi, xm::MT_MAX);
+    return false;
+  }
+  int imin = INT32_MAX, imax = INT32_MIN, jmin = INT32_MAX, jmax = INT32_MIN;
+  for (int L = 2; L <= la; ++L) {
+    imin = std::min(imin, g->il[L - 1]);
+    imax = std::max(imax, g->il[L - 1]);
+    jmin = std::min(jmin, g->jl[L - 1]);
+    jmax = std::max(jmax, g->jl[L - 1]);
+  }
+  const long ni = long(imax) - imin + 1, nj = long(jmax) - jmin + 1;
+  if (ni <= 0 || nj <= 0 || ni * nj > (1L << 31) - 1) {
+    set_error("efdc_xm_create: member %d: bad IL/JL range", mi);
+    return false;
+  }
+  std::vector<int> lij(size_t(ni * nj), 0);
+  for (int L = 2; L <= la; ++L) {
+    const long k = long(g->jl[L - 1] - jmin) * ni + (g->il[L - 1] - imin);
+    if (lij[k]) {
+      set_error("efdc_xm_create: member %d: cells %d and %d share (I,J)", mi, lij[k], L);
+      return false;
+    }
+    lij[k] = L;
+  }
+  auto at = [&](long i, long j) -> int {
+    if (i < imin || i > imax || j < jmin || j > jmax) return lc;
+    const int L = lij[size_t(long(j - jmin) * ni + (i - imin))];
+    return L ? L : lc;
+  };
+  for (int L = 2; L <= la; ++L) {
+    const int i = g->il[L - 1], j = g->jl[L - 1];
+    if (g->lec[L - 1] != at(i + 1, j) || g->lwc[L - 1] != at(i - 1, j) ||
+        g->lnc[L - 1] != at(i, j + 1) || g->lsc[L - 1] != at(i, j - 1)) {
+      set_error("efdc_xm_create: member %d, cell L=%d (I=%d,J=%d): LNC/LSC/LEC/LWC are not the "
+                "maps of a structured grid (periodic ISCONNECT links are not supported)",
+                mi, L, i, j);
+      return false;
+    }
+  }
+  ml.imin = imin;
+  ml.jmin = jmin;
+  ml.ntx = int((ni + xm::TX - 1) / xm::TX);
+  ml.nty = int((nj + xm::TY - 1) / xm::TY);
+  ml.tile_of.assign(size_t(ml.ntx) * ml.nty, 0);
+  for (int L = 2; L <= la; ++L) {
+    const int tx = (g->il[L - 1] - imin) / xm::TX, ty = (g->jl[L - 1] - jmin) / xm::TY;
+    int &t = ml.tile_of[size_t(ty) * ml.ntx + tx];
+    if (!t) {
+      t = -1;
+      ml.tiles.push_back({morton2(tx, ty), ty * ml.ntx + tx});
+    }
+  }
+  std::sort(ml.tiles.begin(), ml.tiles.end());
+  for (size_t k = 0; k < ml.tiles.size(); ++k) ml.tile_of[ml.tiles[k].second] = int(k) + 1;
+  return true;
+}
+
+// The status of a batch call: the first member error, else NEG_DEPTH if any
+// member had one, else OK.
+int overall_status(const efdc_xm_stats *st, int M) {
+  int worst = EFDC_XM_OK;
+  for (int m = 0; m < M; ++m) {
+    const int s = st[m].status;
+    if (s == EFDC_XM_OK) continue;
+    if (s == EFDC_XM_NEG_DEPTH) {
+      if (worst == EFDC_XM_OK) worst = s;
+      continue;
+    }
+    if (worst == EFDC_XM_OK || worst == EFDC_XM_NEG_DEPTH) worst = s;
+  }
+  return worst;
+}
+
+void fill_status(efdc_xm_stats *st, int M, int status) {
+  for (int m = 0; m < M; ++m) st[m].status = status;
 }
 
 }  // namespace
@@ -328,95 +465,54 @@ void efdc_xm_destroy(efdc_xm_ctx *c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (auto &b : c->bufs) cudaFree(b.p);
-  if (c->ctl_h) cudaFreeHost(c->ctl_h);
-  if (c->jobs_h) cudaFreeHost(c->jobs_h);
-  if (c->pser_h) cudaFreeHost(c->pser_h);
+  void *pinned[] = {c->ctl_h, c->glob_h, c->act_h, c->sc_h, c->jobs_h, c->pser_h};
+  for (void *p : pinned)
+    if (p) cudaFreeHost(p);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
 
-efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *g, int32_t device) {
+int32_t efdc_xm_nmembers(const efdc_xm_ctx *c) { return c ? c->M : 0; }
+
+efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, int32_t device) {
   g_last_error.clear();
-  if (!g) {
-    set_error("efdc_xm_create: grid is NULL");
+  if (!grids || nmembers < 1) {
+    set_error("efdc_xm_create: need a grid for each of nmembers >= 1 members");
     return nullptr;
   }
-  const int la = g->la, lc = g->lc;
-  if (la < 2 || lc != la + 1) {
-    set_error("efdc_xm_create: need LA >= 2 and LC == LA+1 (got LA=%d LC=%d)", la, lc);
+  const int M = nmembers;
+  std::vector<MemberLayout> ml(M);
+  long long nt = 1;
+  for (int m = 0; m < M; ++m) {
+    if (!member_layout(&grids[m], m, ml[m])) return nullptr;
+    nt += (long long)ml[m].tiles.size();
+  }
+  if (nt * TILE > (long long)INT32_MAX) {
+    set_error("efdc_xm_create: %lld tiles exceed the 32-bit slot index", nt);
     return nullptr;
   }
-  if (!g->il || !g->jl || !g->lnc || !g->lsc || !g->lec || !g->lwc) {
-    set_error("efdc_xm_create: IL, JL and the four neighbour maps are required");
-    return nullptr;
-  }
-  const double *req[] = {g->dxyp, g->dxyip, g->dxiu, g->dyiu, g->dxiv, g->dyiv, g->dxyu, g->dxyv,
-                         g->hruo, g->hrvo, g->subo, g->svbo, g->sbxo, g->sbyo, g->belv};
-  for (const double *r : req)
-    if (!r) {
-      set_error("efdc_xm_create: a metric array is NULL");
-      return nullptr;
-    }
-  if (g->mtide < 0 || g->mtide > xm::MT_MAX || (g->mtide > 0 && !g->tcp)) {
-    set_error("efdc_xm_create: MTIDE must be in 0..%d with TCP given", xm::MT_MAX);
-    return nullptr;
-  }
-  // ---- structured-grid check and tile layout (host) ----
-  int imin = INT32_MAX, imax = INT32_MIN, jmin = INT32_MAX, jmax = INT32_MIN;
-  for (int L = 2; L <= la; ++L) {
-    imin = std::min(imin, g->il[L - 1]);
-    imax = std::max(imax, g->il[L - 1]);
-    jmin = std::min(jmin, g->jl[L - 1]);
-    jmax = std::max(jmax, g->jl[L - 1]);
-  }
-  const long ni = long(imax) - imin + 1, nj = long(jmax) - jmin + 1;
-  if (ni <= 0 || nj <= 0 || ni * nj > (1L << 31) - 1) {
-    set_error("efdc_xm_create: bad IL/JL range");
-    return nullptr;
-  }
-  std::vector<int> lij(size_t(ni * nj), 0);
-  for (int L = 2; L <= la; ++L) {
-    const long k = long(g->jl[L - 1] - jmin) * ni + (g->il[L - 1] - imin);
-    if (lij[k]) {
-      set_error("efdc_xm_create: cells %d and %d share (I,J)", lij[k], L);
-      return nullptr;
-    }
-    lij[k] = L;
-  }
-  auto at = [&](long i, long j) -> int {
-    if (i < imin || i > imax || j < jmin || j > jmax) return lc;
-    const int L = lij[size_t(long(j - jmin) * ni + (i - imin))];
-    return L ? L : lc;
-  };
-  for (int L = 2; L <= la; ++L) {
-    const int i = g->il[L - 1], j = g->jl[L - 1];
-    if (g->lec[L - 1] != at(i + 1, j) || g->lwc[L - 1] != at(i - 1, j) ||
-        g->lnc[L - 1] != at(i, j + 1) || g->lsc[L - 1] != at(i, j - 1)) {
-      set_error("efdc_xm_create: cell L=%d (I=%d,J=%d): LNC/LSC/LEC/LWC are not the maps of a "
-                "structured grid (periodic ISCONNECT links are not supported)", L, i, j);
-      return nullptr;
-    }
-  }
-  const int ntx = int((ni + xm::TX - 1) / xm::TX), nty = int((nj + xm::TY - 1) / xm::TY);
-  std::vector<int> tile_of(size_t(ntx) * nty, 0);
-  std::vector<std::pair<uint64_t, int>> act;
-  for (int L = 2; L <= la; ++L) {
-    const int tx = (g->il[L - 1] - imin) / xm::TX, ty = (g->jl[L - 1] - jmin) / xm::TY;
-    int &t = tile_of[size_t(ty) * ntx + tx];
-    if (!t) {
-      t = -1;
-      act.push_back({morton2(tx, ty), ty * ntx + tx});
-    }
-  }
-  std::sort(act.begin(), act.end());
-  for (size_t k = 0; k < act.size(); ++k) tile_of[act[k].second] = int(k) + 1;
 
   efdc_xm_ctx *c = new efdc_xm_ctx();
   c->device = device;
-  c->la = la;
-  c->lc = lc;
-  c->ntile = int(act.size()) + 1;
-  c->nslot = c->ntile * TILE;
+  c->M = M;
+  c->mem.resize(M);
+  int ntile = 1;  // tile 0: the ghost tile
+  long long off = 0;
+  for (int m = 0; m < M; ++m) {
+    Member &mb = c->mem[m];
+    mb.la = grids[m].la;
+    mb.lc = grids[m].lc;
+    mb.tile0 = ntile;
+    ntile += int(ml[m].tiles.size());
+    mb.tile1 = ntile;
+    mb.off = off;
+    off += mb.lc + 1;
+    mb.mtide = grids[m].mtide;
+    if (mb.mtide > 0) mb.tcp.assign(grids[m].tcp, grids[m].tcp + mb.mtide);
+  }
+  c->ntile = ntile;
+  c->nslot = ntile * TILE;
+  c->stage_len = off;
   auto bail = [&](const char *what) -> efdc_xm_ctx * {
     if (g_last_error.empty()) set_error("efdc_xm_create: %s", what);
     efdc_xm_destroy(c);
@@ -430,79 +526,137 @@ efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *g, int32_t device) {
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail("stream creation failed");
   cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
-  const int occ = xm::occupancy_blocks_per_sm();
-  const int occ_cg = xm::occupancy_blocks_per_sm_cg();
-  const int occ_cg32 = xm::occupancy_blocks_per_sm_mixed();
-  c->grid = std::max(1, std::min(c->ntile - 1, c->nsm * occ));
-  c->grid_cg = std::max(1, std::min((c->ntile - 1 + 3) / 4, c->nsm * occ_cg));
-  c->grid_cg32 = std::max(1, std::min((c->ntile - 1 + 3) / 4, c->nsm * occ_cg32));
-  c->grid_mv64 = std::max(1, std::min((c->ntile - 1 + 3) / 4, c->nsm * xm::occupancy_blocks_per_sm_mv64()));
-  c->grid_up32 = std::max(1, std::min((c->ntile - 1 + 3) / 4, c->nsm * xm::occupancy_blocks_per_sm_mixed_update()));
 
-  std::vector<int4> tnbr(c->ntile, int4{0, 0, 0, 0});
+  // ---- host layout: tiles, quads (4-tile CG units, never across members), slots ----
+  std::vector<int4> tnbr(ntile, int4{0, 0, 0, 0});
+  std::vector<int> tile_member(ntile, 0), tend(M), qstart(M + 1, 0);
+  std::vector<int2> quads;
   std::vector<uint8_t> kind(c->nslot, xm::LAND);
-  c->lidx_h.assign(c->nslot, 0);
-  c->slot_of_L.assign(size_t(lc) + 1, 0);
-  for (size_t k = 0; k < act.size(); ++k) {
-    const int id = act[k].second, tx = id % ntx, ty = id / ntx;
-    auto tl = [&](int x, int y) { return (x < 0 || y < 0 || x >= ntx || y >= nty) ? 0 : std::max(tile_of[size_t(y) * ntx + x], 0); };
-    tnbr[k + 1] = int4{tl(tx - 1, ty), tl(tx + 1, ty), tl(tx, ty - 1), tl(tx, ty + 1)};
+  std::vector<int> lidx(c->nslot, 0);
+  std::vector<std::vector<int>> slot_of(M);
+  for (int m = 0; m < M; ++m) {
+    const efdc_xm_grid *g = &grids[m];
+    const MemberLayout &ly = ml[m];
+    Member &mb = c->mem[m];
+    for (size_t k = 0; k < ly.tiles.size(); ++k) {
+      const int id = ly.tiles[k].second, tx = id % ly.ntx, ty = id / ly.ntx;
+      auto tl = [&](int x, int y) {
+        if (x < 0 || y < 0 || x >= ly.ntx || y >= ly.nty) return 0;
+        const int t = ly.tile_of[size_t(y) * ly.ntx + x];
+        return t > 0 ? mb.tile0 + t - 1 : 0;
+      };
+      const int gt = mb.tile0 + int(k);
+      tnbr[gt] = int4{tl(tx - 1, ty), tl(tx + 1, ty), tl(tx, ty - 1), tl(tx, ty + 1)};
+      tile_member[gt] = m;
+    }
+    tend[m] = mb.tile1;
+    qstart[m] = int(quads.size());
+    for (int t = mb.tile0; t < mb.tile1; t += 4) quads.push_back(int2{m, t});
+    qstart[m + 1] = int(quads.size());
+    slot_of[m].assign(size_t(mb.lc) + 1, 0);
+    for (int L = 2; L <= mb.la; ++L) {
+      const int ii = g->il[L - 1] - ly.imin, jj = g->jl[L - 1] - ly.jmin;
+      const int t = ly.tile_of[size_t(jj / xm::TY) * ly.ntx + ii / xm::TX];
+      const int d = (mb.tile0 + t - 1) * TILE + (jj % xm::TY) * xm::TX + (ii % xm::TX);
+      kind[d] = xm::WATER;
+      lidx[d] = L;
+      slot_of[m][L] = d;
+    }
   }
-  for (int L = 2; L <= la; ++L) {
-    const int ii = g->il[L - 1] - imin, jj = g->jl[L - 1] - jmin;
-    const int t = tile_of[size_t(jj / xm::TY) * ntx + ii / xm::TX];
-    const int d = t * TILE + (jj % xm::TY) * xm::TX + (ii % xm::TX);
-    kind[d] = xm::WATER;
-    c->lidx_h[d] = L;
-    c->slot_of_L[L] = d;
-  }
-  // ---- open boundaries ----
-  std::vector<int> bslot, bnbr, bside, bispb;
+  c->nquad = int(quads.size());
+
+  // ---- open boundaries, packed per member in the W, E, S, N loop order ----
+  int mtmax = 1;
+  for (int m = 0; m < M; ++m) mtmax = std::max(mtmax, grids[m].mtide);
+  std::vector<int> bslot, bnbr, bside, bispb, bmember, bstart(M + 1, 0), bmt(M);
   std::vector<double> bpcb, bpsb;
-  c->mtide = g->mtide;
-  c->tcp.assign(g->tcp, g->tcp + g->mtide);
-  for (int s = 0; s < 4; ++s) {
-    const efdc_xm_obc &o = g->obc[s];
-    if (o.n < 0 || (o.n > 0 && (!o.l || !o.ispb))) return bail("bad open-boundary arrays");
-    c->side_n[s] = o.n;
-    for (int ll = 0; ll < o.n; ++ll) {
-      const int L = o.l[ll];
-      if (L < 2 || L > la) return bail("open-boundary L out of range");
-      const int nbL = (s == 0) ? g->lec[L - 1] : (s == 1) ? g->lwc[L - 1] : (s == 2) ? g->lnc[L - 1] : g->lsc[L - 1];
-      bslot.push_back(c->slot_of_L[L]);
-      bnbr.push_back(nbL == lc ? 0 : c->slot_of_L[nbL]);  // 0 = a slot of the ghost tile
-      bside.push_back(s);
-      bispb.push_back(o.ispb[ll]);
-      for (int m = 0; m < g->mtide; ++m) {
-        bpcb.push_back(o.pcb ? o.pcb[size_t(m) * o.ld + ll] : 0.0);
-        bpsb.push_back(o.psb ? o.psb[size_t(m) * o.ld + ll] : 0.0);
+  for (int m = 0; m < M; ++m) {
+    const efdc_xm_grid *g = &grids[m];
+    Member &mb = c->mem[m];
+    mb.b0 = int(bslot.size());
+    bstart[m] = mb.b0;
+    bmt[m] = g->mtide;
+    std::unordered_set<int> bcells, targets;
+    for (int s = 0; s < 4; ++s) {
+      const efdc_xm_obc &o = g->obc[s];
+      if (o.n < 0 || (o.n > 0 && (!o.l || !o.ispb))) return bail("bad open-boundary arrays");
+      for (int ll = 0; ll < o.n; ++ll) bcells.insert(o.l[ll]);
+    }
+    for (int s = 0; s < 4; ++s) {
+      const efdc_xm_obc &o = g->obc[s];
+      mb.side_n[s] = o.n;
+      for (int ll = 0; ll < o.n; ++ll) {
+        const int L = o.l[ll];
+        if (L < 2 || L > mb.la) return bail("open-boundary L out of range");
+        const int nbL = (s == 0) ? g->lec[L - 1] : (s == 1) ? g->lwc[L - 1]
+                        : (s == 2) ? g->lnc[L - 1] : g->lsc[L - 1];
+        bslot.push_back(slot_of[m][L]);
+        bnbr.push_back(nbL == mb.lc ? 0 : slot_of[m][nbL]);  // 0 = a slot of the ghost tile
+        bside.push_back(s);
+        bispb.push_back(o.ispb[ll]);
+        bmember.push_back(m);
+        for (int t = 0; t < mtmax; ++t) {
+          const bool have = t < g->mtide;
+          bpcb.push_back(have && o.pcb ? o.pcb[size_t(t) * o.ld + ll] : 0.0);
+          bpsb.push_back(have && o.psb ? o.psb[size_t(t) * o.ld + ll] : 0.0);
+        }
+        kind[slot_of[m][L]] = xm::OPENBC;
+        if (o.ispb[ll] == 1 || o.ispb[ll] == 2) mb.may_asym = true;
+        // hazard: a ghost or boundary-cell target, or a target shared by two
+        // boundary cells, needs the reference's serial loop order
+        if (nbL == mb.lc || bcells.count(nbL) || !targets.insert(nbL).second) c->obc_serial = true;
       }
-      kind[c->slot_of_L[L]] = xm::OPENBC;
-      if (o.ispb[ll] == 1 || o.ispb[ll] == 2) c->may_asym = true;
     }
+    mb.nobc = int(bslot.size()) - mb.b0;
+    c->any_may_asym |= mb.may_asym;
   }
+  bstart[M] = int(bslot.size());
   c->nobc = int(bslot.size());
-  {  // hazard check: unique interior targets that are not boundary cells
-    std::unordered_map<int, int> seen;
-    std::vector<char> isbc(c->nslot, 0);
-    for (int d : bslot) isbc[d] = 1;
-    bool serial = false;
-    for (size_t k = 0; k < bslot.size(); ++k) {
-      const int nb = bnbr[k];
-      if (nb == 0 || isbc[nb] || seen.count(nb)) serial = true;
-      seen[nb] = 1;
-    }
-    c->obc_serial = serial;
-  }
+
+  // ---- launch geometry ----
+  const int occ = xm::occupancy_blocks_per_sm();
+  c->grid = std::max(1, std::min(c->ntile - 1, c->nsm * occ));
+  auto qgrid = [&](int per_sm) { return std::max(1, std::min(c->nquad, c->nsm * per_sm)); };
+  c->grid_cg = qgrid(xm::occupancy_blocks_per_sm_cg());
+  c->grid_mv64 = qgrid(xm::occupancy_blocks_per_sm_mv64());
+  c->grid_cg32 = qgrid(xm::occupancy_blocks_per_sm_mixed());
+  c->grid_up32 = qgrid(xm::occupancy_blocks_per_sm_mixed_update());
+
   // ---- device arrays ----
   const size_t ns = c->nslot;
   c->lidx = c->alloc<int>(ns);
-  int4 *tnbr_d = c->alloc<int4>(c->ntile);
+  c->tile_member = c->alloc<int>(ntile);
+  int4 *tnbr_d = c->alloc<int4>(ntile);
   uint8_t *kind_d = c->alloc<uint8_t>(ns);
-  if (!c->lidx || !tnbr_d || !kind_d) return bail("cudaMalloc failed");
-  cudaMemcpy(c->lidx, c->lidx_h.data(), ns * sizeof(int), cudaMemcpyHostToDevice);
+  int2 *quads_d = c->alloc<int2>(quads.size());
+  int *qstart_d = c->alloc<int>(M + 1), *tend_d = c->alloc<int>(M);
+  c->moff = c->alloc<long long>(M);
+  c->mlc = c->alloc<int>(M);
+  c->sc = c->alloc<xm::StepScalars>(M);
+  c->ctl = c->alloc<Ctl>(M);
+  c->glob = c->alloc<Glob>(1);
+  c->act = c->alloc<int>(M);
+  c->part = c->alloc<double>(2 * size_t(c->nquad) + 64);
+  if (!c->lidx || !c->tile_member || !tnbr_d || !kind_d || !quads_d || !qstart_d || !tend_d ||
+      !c->moff || !c->mlc || !c->sc || !c->ctl || !c->glob || !c->act || !c->part)
+    return bail("cudaMalloc failed");
+  {
+    std::vector<long long> moff(M);
+    std::vector<int> mlc(M);
+    for (int m = 0; m < M; ++m) {
+      moff[m] = c->mem[m].off;
+      mlc[m] = c->mem[m].lc;
+    }
+    cudaMemcpy(c->moff, moff.data(), M * sizeof(long long), cudaMemcpyHostToDevice);
+    cudaMemcpy(c->mlc, mlc.data(), M * sizeof(int), cudaMemcpyHostToDevice);
+  }
+  cudaMemcpy(c->lidx, lidx.data(), ns * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(c->tile_member, tile_member.data(), ntile * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(tnbr_d, tnbr.data(), tnbr.size() * sizeof(int4), cudaMemcpyHostToDevice);
   cudaMemcpy(kind_d, kind.data(), ns, cudaMemcpyHostToDevice);
+  cudaMemcpy(quads_d, quads.data(), quads.size() * sizeof(int2), cudaMemcpyHostToDevice);
+  cudaMemcpy(qstart_d, qstart.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(tend_d, tend.data(), M * sizeof(int), cudaMemcpyHostToDevice);
   auto D = [&]() { return c->alloc<double>(ns); };
   auto I = [&]() { return c->alloc<int>(ns); };
   auto Fl = [&]() { return c->alloc<float>(ns); };
@@ -510,6 +664,12 @@ efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *g, int32_t device) {
   S.tnbr = tnbr_d;
   S.kind = kind_d;
   S.lidx = c->lidx;
+  S.tile_member = c->tile_member;
+  S.quads = quads_d;
+  S.qstart = qstart_d;
+  S.tend = tend_d;
+  S.sc = c->sc;
+  S.nquad = c->nquad;
   double *st[18];
   for (double *&p : st) p = D();
   S.dxyp = st[0]; S.dxyip = st[1]; S.dxiu = st[2]; S.dyiu = st[3]; S.dxiv = st[4];
@@ -534,275 +694,455 @@ efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *g, int32_t device) {
   Y.as32 = Fl(); Y.aw32 = Fl(); Y.ae32 = Fl(); Y.an32 = Fl();
   Y.r32 = Fl(); Y.pa32 = Fl(); Y.pb32 = Fl(); Y.ap32 = Fl(); Y.x32 = Fl();
   c->ptmp = D();
-  c->ctl = c->alloc<Ctl>(1);
-  c->part = c->alloc<double>(size_t(2) * std::max(std::max(c->grid, c->grid_up32),
-                                                  std::max(c->grid_cg, c->grid_cg32)) + 64);
-  if (!Y.x32 || !c->ctl || !c->part) return bail("cudaMalloc failed (device memory)");
-  if (cudaHostAlloc(reinterpret_cast<void **>(&c->ctl_h), sizeof(Ctl), cudaHostAllocDefault) != cudaSuccess)
+  if (!c->ptmp || !Y.x32) return bail("cudaMalloc failed (device memory)");
+  auto pin = [](void *pp, size_t bytes) {
+    return cudaHostAlloc(static_cast<void **>(pp), std::max<size_t>(bytes, 1),
+                         cudaHostAllocDefault) == cudaSuccess;
+  };
+  if (!pin(&c->ctl_h, sizeof(Ctl) * M) || !pin(&c->glob_h, sizeof(Glob)) ||
+      !pin(&c->act_h, sizeof(int) * M) || !pin(&c->sc_h, sizeof(xm::StepScalars) * M) ||
+      !pin(&c->jobs_h, sizeof(CopyJob) * MAX_JOBS))
     return bail("cudaHostAlloc failed");
-  std::memset(c->ctl_h, 0, sizeof(Ctl));
-  // land slots of the scaled system: CCC=1 keeps them inert in the CG
-  {
-    std::vector<double> one(ns, 0.0);
+  std::memset(c->ctl_h, 0, sizeof(Ctl) * M);
+  std::memset(c->sc_h, 0, sizeof(xm::StepScalars) * M);
+  c->jobs_d = c->alloc<CopyJob>(MAX_JOBS);
+  if (!c->jobs_d) return bail("cudaMalloc failed");
+  {  // land slots of the scaled system: CCC=1 keeps them inert in the CG;
+     // RCX/RCY = 1 on water cells, 0 on the ghosts (calpuv2c.f90:97-102)
+    std::vector<double> one(ns, 0.0), rc(ns, 0.0), fu(ns, 1.0), fv(ns, 1.0);
     for (size_t d = 0; d < ns; ++d)
       if (kind[d] == xm::LAND) one[d] = 1.0;
+    for (int m = 0; m < M; ++m)
+      for (int L = 2; L <= c->mem[m].la; ++L) {
+        const int d = slot_of[m][L];
+        rc[d] = 1.0;
+        fu[d] = 0.5 / grids[m].dxyu[L - 1];  // calpuv2c.f90:111-116
+        fv[d] = 0.5 / grids[m].dxyv[L - 1];
+      }
     cudaMemcpy(Y.ccc, one.data(), ns * sizeof(double), cudaMemcpyHostToDevice);
-    // RCX/RCY: 1 on water cells, 0 on the ghosts (calpuv2c.f90:97-102)
-    std::vector<double> rc(ns, 0.0), fu(ns, 1.0), fv(ns, 1.0);
-    for (int L = 2; L <= la; ++L) {
-      const int d = c->slot_of_L[L];
-      rc[d] = 1.0;
-      fu[d] = 0.5 / g->dxyu[L - 1];  // calpuv2c.f90:111-116
-      fv[d] = 0.5 / g->dxyv[L - 1];
-    }
     cudaMemcpy(st[15], rc.data(), ns * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(st[16], fu.data(), ns * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(st[17], fv.data(), ns * sizeof(double), cudaMemcpyHostToDevice);
   }
-  // staging buffers (host order) and copy jobs
-  const int nstage = 40;
-  for (int k = 0; k < nstage; ++k) {
-    double *p = c->alloc<double>(size_t(lc) + 1, false);
+  for (int k = 0; k < NSTAGE; ++k) {
+    double *p = c->alloc<double>(size_t(c->stage_len), false);
     if (!p) return bail("cudaMalloc failed (staging)");
     c->stage.push_back(p);
   }
-  c->max_jobs = 64;
-  c->jobs_d = c->alloc<CopyJob>(c->max_jobs);
-  if (cudaHostAlloc(reinterpret_cast<void **>(&c->jobs_h), c->max_jobs * sizeof(CopyJob), cudaHostAllocDefault) != cudaSuccess)
-    return bail("cudaHostAlloc failed");
-  // open-boundary device arrays
   xm::DevObc &Bo = c->B;
   Bo.n = c->nobc;
-  Bo.mtide = g->mtide;
+  Bo.mtmax = mtmax;
+  {
+    int *bmt_d = c->alloc<int>(M), *bstart_d = c->alloc<int>(M + 1);
+    if (!bmt_d || !bstart_d) return bail("cudaMalloc failed (obc)");
+    cudaMemcpy(bmt_d, bmt.data(), M * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(bstart_d, bstart.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice);
+    Bo.mtide = bmt_d;
+    Bo.bstart = bstart_d;
+  }
   if (c->nobc > 0) {
-    int *bs = c->alloc<int>(c->nobc), *bn = c->alloc<int>(c->nobc), *bd = c->alloc<int>(c->nobc),
-        *bi = c->alloc<int>(c->nobc);
-    double *pc = c->alloc<double>(std::max<size_t>(bpcb.size(), 1)),
-           *ps = c->alloc<double>(std::max<size_t>(bpsb.size(), 1));
-    c->pser_d = c->alloc<double>(c->nobc);
-    if (!bs || !bn || !bd || !bi || !pc || !ps || !c->pser_d) return bail("cudaMalloc failed (obc)");
-    cudaMemcpy(bs, bslot.data(), c->nobc * sizeof(int), cudaMemcpyHostToDevice);
-    cudaMemcpy(bn, bnbr.data(), c->nobc * sizeof(int), cudaMemcpyHostToDevice);
-    cudaMemcpy(bd, bside.data(), c->nobc * sizeof(int), cudaMemcpyHostToDevice);
-    cudaMemcpy(bi, bispb.data(), c->nobc * sizeof(int), cudaMemcpyHostToDevice);
-    if (!bpcb.empty()) {
-      cudaMemcpy(pc, bpcb.data(), bpcb.size() * sizeof(double), cudaMemcpyHostToDevice);
-      cudaMemcpy(ps, bpsb.data(), bpsb.size() * sizeof(double), cudaMemcpyHostToDevice);
-    }
+    const int n = c->nobc;
+    int *bs = c->alloc<int>(n), *bn = c->alloc<int>(n), *bd = c->alloc<int>(n),
+        *bi = c->alloc<int>(n), *bm = c->alloc<int>(n);
+    double *pc = c->alloc<double>(bpcb.size()), *ps = c->alloc<double>(bpsb.size());
+    c->pser_d = c->alloc<double>(n);
+    if (!bs || !bn || !bd || !bi || !bm || !pc || !ps || !c->pser_d)
+      return bail("cudaMalloc failed (obc)");
+    cudaMemcpy(bs, bslot.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(bn, bnbr.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(bd, bside.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(bi, bispb.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(bm, bmember.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(pc, bpcb.data(), bpcb.size() * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(ps, bpsb.data(), bpsb.size() * sizeof(double), cudaMemcpyHostToDevice);
     Bo.slot = bs;
     Bo.nbr = bn;
     Bo.side = bd;
     Bo.ispb = bi;
+    Bo.member = bm;
     Bo.pcb = pc;
     Bo.psb = ps;
     Bo.pser = c->pser_d;
-    if (cudaHostAlloc(reinterpret_cast<void **>(&c->pser_h), c->nobc * sizeof(double), cudaHostAllocDefault) != cudaSuccess)
-      return bail("cudaHostAlloc failed");
+    if (!pin(&c->pser_h, n * sizeof(double))) return bail("cudaHostAlloc failed");
   }
   // the zero-fills above ran on the legacy stream; finish them before any
   // work on the non-blocking solver stream
   if (cudaDeviceSynchronize() != cudaSuccess) return bail("device error during allocation");
-  // static metrics into tile order (land slots take element LC)
-  std::vector<Xfer> xs = {
-      {g->dxyp, st[0], 0}, {g->dxyip, st[1], 0}, {g->dxiu, st[2], 0}, {g->dyiu, st[3], 0},
-      {g->dxiv, st[4], 0}, {g->dyiv, st[5], 0}, {g->dxyu, st[6], 0}, {g->dxyv, st[7], 0},
-      {g->hruo, st[8], 0}, {g->hrvo, st[9], 0}, {g->subo, st[10], 0}, {g->svbo, st[11], 0},
-      {g->sbxo, st[12], 0}, {g->sbyo, st[13], 0}, {g->belv, st[14], 0}};
+  // static metrics into tile order (land slots take element LC of their member)
+  auto per = [&](const double *efdc_xm_grid::*f) {
+    std::vector<const void *> v(M);
+    for (int m = 0; m < M; ++m) v[m] = grids[m].*f;
+    return v;
+  };
+  const std::pair<const double *efdc_xm_grid::*, double *> metrics[] = {
+      {&efdc_xm_grid::dxyp, st[0]},   {&efdc_xm_grid::dxyip, st[1]}, {&efdc_xm_grid::dxiu, st[2]},
+      {&efdc_xm_grid::dyiu, st[3]},   {&efdc_xm_grid::dxiv, st[4]},  {&efdc_xm_grid::dyiv, st[5]},
+      {&efdc_xm_grid::dxyu, st[6]},   {&efdc_xm_grid::dxyv, st[7]},  {&efdc_xm_grid::hruo, st[8]},
+      {&efdc_xm_grid::hrvo, st[9]},   {&efdc_xm_grid::subo, st[10]}, {&efdc_xm_grid::svbo, st[11]},
+      {&efdc_xm_grid::sbxo, st[12]},  {&efdc_xm_grid::sbyo, st[13]}, {&efdc_xm_grid::belv, st[14]}};
+  std::vector<Xfer> xs;
+  for (const auto &mt : metrics) xs.push_back(Xfer{per(mt.first), mt.second, 0});
   if (upload_arrays(c, xs) != EFDC_XM_OK) return bail("upload of the static arrays failed");
   if (cudaDeviceSynchronize() != cudaSuccess) return bail("device error during set-up");
   return c;
 }
 
-int32_t efdc_xm_upload(efdc_xm_ctx *c, const efdc_xm_fields *f) {
+efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *g, int32_t device) {
+  if (!g) {
+    g_last_error.clear();
+    set_error("efdc_xm_create: grid is NULL");
+    return nullptr;
+  }
+  return efdc_xm_create_batch(g, 1, device);
+}
+
+int32_t efdc_xm_upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f) {
   if (!c || !f) {
     set_error("efdc_xm_upload: NULL argument");
     return EFDC_XM_BAD_ARGUMENT;
   }
   CK(cudaSetDevice(c->device));
   xm::DevState &X = c->X;
-  std::vector<Xfer> xs = {
-      {f->p, X.p, 0}, {f->hp, X.hp, 0}, {f->hu, X.hu, 0}, {f->hv, X.hv, 0},
-      {f->uhdye, X.uhdye, 0}, {f->vhdxe, X.vhdxe, 0}, {f->sub, X.sub, 0}, {f->svb, X.svb, 0},
-      {f->sbx, X.sbx, 0}, {f->sby, X.sby, 0}, {f->lmaskdry, X.lmaskdry, 1},
-      {f->iscdry, X.iscdry, 2}, {f->lopenbcdry, X.lopenbcdry, 1}, {f->natdry, X.natdry, 2},
-      {f->fcaxe, const_cast<double *>(X.fcaxe), 0}, {f->fcaye, const_cast<double *>(X.fcaye), 0},
-      {f->fxe, const_cast<double *>(X.fxe), 0}, {f->fye, const_cast<double *>(X.fye), 0},
-      {f->tsx, const_cast<double *>(X.tsx), 0}, {f->tsy, const_cast<double *>(X.tsy), 0},
-      {f->tbx, const_cast<double *>(X.tbx), 0}, {f->tby, const_cast<double *>(X.tby), 0},
-      {f->qsume, const_cast<double *>(X.qsume), 0}, {f->qdwaste, X.qdwaste, 0},
-      {f->vdwaste, X.vdwaste, 0}};
-  int rc = upload_arrays(c, xs);
-  if (rc) return rc;
+  const int M = c->M;
+  std::vector<Xfer> xs;
+  int rc = 0;
+#define XM_UP(name, dev, kind)                                   \
+  {                                                              \
+    std::vector<const void *> v(M);                              \
+    for (int m = 0; m < M; ++m) v[m] = f[m].name;                \
+    if ((rc = collect(c, xs, v, dev, kind, #name))) return rc;   \
+  }
+  XM_UP(p, X.p, 0) XM_UP(hp, X.hp, 0) XM_UP(hu, X.hu, 0) XM_UP(hv, X.hv, 0)
+  XM_UP(uhdye, X.uhdye, 0) XM_UP(vhdxe, X.vhdxe, 0) XM_UP(sub, X.sub, 0) XM_UP(svb, X.svb, 0)
+  XM_UP(sbx, X.sbx, 0) XM_UP(sby, X.sby, 0) XM_UP(lmaskdry, X.lmaskdry, 1)
+  XM_UP(iscdry, X.iscdry, 2) XM_UP(lopenbcdry, X.lopenbcdry, 1) XM_UP(natdry, X.natdry, 2)
+  XM_UP(fcaxe, X.fcaxe, 0) XM_UP(fcaye, X.fcaye, 0) XM_UP(fxe, X.fxe, 0) XM_UP(fye, X.fye, 0)
+  XM_UP(tsx, X.tsx, 0) XM_UP(tsy, X.tsy, 0) XM_UP(tbx, X.tbx, 0) XM_UP(tby, X.tby, 0)
+  XM_UP(qsume, X.qsume, 0) XM_UP(qdwaste, X.qdwaste, 0) XM_UP(vdwaste, X.vdwaste, 0)
+#undef XM_UP
+  if ((rc = upload_arrays(c, xs))) return rc;
   // the second buffer of each time-level pair starts as a copy (its land
   // slots must hold the ghost values too); the H1P input is not used because
   // a step begins with H1P = HP (calpuv2c.f90:264)
   const size_t nb = size_t(c->nslot) * sizeof(double);
-  if (f->uhdye) CK(cudaMemcpyAsync(X.uhdy1e, X.uhdye, nb, cudaMemcpyDeviceToDevice, c->stream));
-  if (f->vhdxe) CK(cudaMemcpyAsync(X.vhdx1e, X.vhdxe, nb, cudaMemcpyDeviceToDevice, c->stream));
-  if (f->hp) CK(cudaMemcpyAsync(X.h1p, X.hp, nb, cudaMemcpyDeviceToDevice, c->stream));
+  if (f[0].uhdye) CK(cudaMemcpyAsync(X.uhdy1e, X.uhdye, nb, cudaMemcpyDeviceToDevice, c->stream));
+  if (f[0].vhdxe) CK(cudaMemcpyAsync(X.vhdx1e, X.vhdxe, nb, cudaMemcpyDeviceToDevice, c->stream));
+  if (f[0].hp) CK(cudaMemcpyAsync(X.h1p, X.hp, nb, cudaMemcpyDeviceToDevice, c->stream));
   if (c->nobc > 0) {
-    int k = 0;
-    for (int s = 0; s < 4; ++s)
-      for (int ll = 0; ll < c->side_n[s]; ++ll, ++k) c->pser_h[k] = f->pser[s] ? f->pser[s][ll] : 0.0;
-    CK(cudaMemcpyAsync(c->pser_d, c->pser_h, c->nobc * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    for (int m = 0; m < M; ++m) {
+      int k = c->mem[m].b0;
+      for (int s = 0; s < 4; ++s)
+        for (int ll = 0; ll < c->mem[m].side_n[s]; ++ll, ++k)
+          c->pser_h[k] = f[m].pser[s] ? f[m].pser[s][ll] : 0.0;
+    }
+    CK(cudaMemcpyAsync(c->pser_d, c->pser_h, c->nobc * sizeof(double), cudaMemcpyHostToDevice,
+                       c->stream));
   }
-  if (f->lmaskdry) c->oldmask_h.assign(f->lmaskdry, f->lmaskdry + c->lc);
+  CK(cudaStreamSynchronize(c->stream));
+  for (int m = 0; m < M; ++m)
+    if (f[m].lmaskdry) c->mem[m].oldmask_h.assign(f[m].lmaskdry, f[m].lmaskdry + c->mem[m].lc);
   return EFDC_XM_OK;
 }
 
-int32_t efdc_xm_download(efdc_xm_ctx *c, efdc_xm_fields *f) {
+int32_t efdc_xm_download_batch(efdc_xm_ctx *c, efdc_xm_fields *f) {
   if (!c || !f) {
     set_error("efdc_xm_download: NULL argument");
     return EFDC_XM_BAD_ARGUMENT;
   }
   CK(cudaSetDevice(c->device));
   xm::DevState &X = c->X;
-  std::vector<int32_t> oldmask;
-  const bool lists = f->lwet || f->ldry;
-  if (lists) oldmask.assign(c->lc, 1);
-  std::vector<Xfer> xs = {
-      {f->p, X.p, 0}, {f->hp, X.hp, 0}, {f->h1p, X.h1p, 0}, {f->hu, X.hu, 0}, {f->hv, X.hv, 0},
-      {f->uhdye, X.uhdye, 0}, {f->vhdxe, X.vhdxe, 0}, {f->sub, X.sub, 0}, {f->svb, X.svb, 0},
-      {f->sbx, X.sbx, 0}, {f->sby, X.sby, 0}, {f->lmaskdry, X.lmaskdry, 1},
-      {f->iscdry, X.iscdry, 2}, {f->lopenbcdry, X.lopenbcdry, 1}, {f->natdry, X.natdry, 2},
-      {f->uhe, X.uhe, 0}, {f->vhe, X.vhe, 0}, {f->hpi, X.hpi, 0}, {f->hui, X.hui, 0},
-      {f->hvi, X.hvi, 0}, {f->qdwaste, X.qdwaste, 0}, {f->vdwaste, X.vdwaste, 0},
-      {f->ccc, c->Y.ccc, 0}, {f->ccs, c->Y.ccs, 0}, {f->ccw, c->Y.ccw, 0}, {f->cce, c->Y.cce, 0},
-      {f->ccn, c->Y.ccn, 0}, {f->fptmp, c->Y.fptmp, 0},
-      {lists ? oldmask.data() : nullptr, X.oldmask, 2}};
-  int rc = download_arrays(c, xs);
-  if (rc) return rc;
-  if (lists) {  // calpuv2c.f90:1061-1080 (L order)
-    std::vector<int32_t> mask(c->lc, 1);
-    if (c->last_isdry > 0) {
-      std::vector<Xfer> m = {{mask.data(), X.lmaskdry, 1}};
-      if ((rc = download_arrays(c, m))) return rc;
+  const xm::DevSystem &Y = c->Y;
+  const int M = c->M;
+  std::vector<Xfer> xs;
+  int rc = 0;
+#define XM_DN(name, dev, kind)                                   \
+  {                                                              \
+    std::vector<const void *> v(M);                              \
+    for (int m = 0; m < M; ++m) v[m] = f[m].name;                \
+    if ((rc = collect(c, xs, v, dev, kind, #name))) return rc;   \
+  }
+  XM_DN(p, X.p, 0) XM_DN(hp, X.hp, 0) XM_DN(h1p, X.h1p, 0) XM_DN(hu, X.hu, 0) XM_DN(hv, X.hv, 0)
+  XM_DN(uhdye, X.uhdye, 0) XM_DN(vhdxe, X.vhdxe, 0) XM_DN(sub, X.sub, 0) XM_DN(svb, X.svb, 0)
+  XM_DN(sbx, X.sbx, 0) XM_DN(sby, X.sby, 0) XM_DN(lmaskdry, X.lmaskdry, 1)
+  XM_DN(iscdry, X.iscdry, 2) XM_DN(lopenbcdry, X.lopenbcdry, 1) XM_DN(natdry, X.natdry, 2)
+  XM_DN(uhe, X.uhe, 0) XM_DN(vhe, X.vhe, 0) XM_DN(hpi, X.hpi, 0) XM_DN(hui, X.hui, 0)
+  XM_DN(hvi, X.hvi, 0) XM_DN(qdwaste, X.qdwaste, 0) XM_DN(vdwaste, X.vdwaste, 0)
+  XM_DN(ccc, Y.ccc, 0) XM_DN(ccs, Y.ccs, 0) XM_DN(ccw, Y.ccw, 0) XM_DN(cce, Y.cce, 0)
+  XM_DN(ccn, Y.ccn, 0) XM_DN(fptmp, Y.fptmp, 0)
+#undef XM_DN
+  // the wet/dry lists need the mask at exit and at entry (OLDMASK)
+  std::vector<std::vector<int32_t>> mask(M), oldm(M);
+  bool lists = false;
+  for (int m = 0; m < M; ++m) lists |= (f[m].lwet || f[m].ldry);
+  if (lists) {
+    std::vector<const void *> pm(M), po(M);
+    for (int m = 0; m < M; ++m) {
+      mask[m].assign(c->mem[m].lc, 1);
+      oldm[m].assign(c->mem[m].lc, 1);
+      pm[m] = mask[m].data();
+      po[m] = oldm[m].data();
     }
-    int nw = 0, nd = 0;
-    for (int L = 2; L <= c->la; ++L) {
-      if (c->last_isdry == 0 || mask[L - 1]) {
-        if (f->lwet) f->lwet[nw] = L;
-        ++nw;
-      } else if (oldmask[L - 1] || c->last_n < c->last_ntstbc + 1) {
-        if (f->ldry) f->ldry[nd] = L;
-        ++nd;
+    xs.push_back(Xfer{pm, X.lmaskdry, 1});
+    xs.push_back(Xfer{po, X.oldmask, 2});
+  }
+  if ((rc = download_arrays(c, xs))) return rc;
+  if (lists) {  // calpuv2c.f90:1061-1080 (L order)
+    for (int m = 0; m < M; ++m) {
+      const Member &mb = c->mem[m];
+      int nw = 0, nd = 0;
+      for (int L = 2; L <= mb.la; ++L) {
+        if (mb.last_isdry == 0 || mask[m][L - 1]) {
+          if (f[m].lwet) f[m].lwet[nw] = L;
+          ++nw;
+        } else if (oldm[m][L - 1] || mb.last_n < mb.last_ntstbc + 1) {
+          if (f[m].ldry) f[m].ldry[nd] = L;
+          ++nd;
+        }
       }
     }
   }
   return EFDC_XM_OK;
 }
 
-int32_t efdc_xm_step_device(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats) {
-  efdc_xm_stats dummy;
-  if (!stats) stats = &dummy;
-  std::memset(stats, 0, sizeof(*stats));
-  if (!c || !prm) {
+int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
+                                  efdc_xm_stats *stats) {
+  if (!c || !prm || !stats) {
     set_error("efdc_xm_step_device: NULL argument");
-    return stats->status = EFDC_XM_BAD_ARGUMENT;
+    return EFDC_XM_BAD_ARGUMENT;
   }
-  if (!(prm->delt > 0) || prm->iterm < 1 || prm->g <= 0) {
-    set_error("efdc_xm_step_device: need DELT > 0, G > 0, ITERM >= 1");
-    return stats->status = EFDC_XM_BAD_ARGUMENT;
-  }
-  if (prm->precision != EFDC_XM_PREC_FP64 && prm->precision != EFDC_XM_PREC_MIXED) {
-    set_error("efdc_xm_step_device: unknown precision %d", prm->precision);
-    return stats->status = EFDC_XM_BAD_ARGUMENT;
+  const int M = c->M;
+  std::memset(stats, 0, sizeof(efdc_xm_stats) * M);
+  for (int m = 0; m < M; ++m) {
+    if (!(prm[m].delt > 0) || prm[m].iterm < 1 || prm[m].g <= 0) {
+      set_error("efdc_xm_step_device: member %d: need DELT > 0, G > 0, ITERM >= 1", m);
+      fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+    if ((prm[m].precision != EFDC_XM_PREC_FP64 && prm[m].precision != EFDC_XM_PREC_MIXED) ||
+        prm[m].precision != prm[0].precision) {
+      set_error("efdc_xm_step_device: member %d: unknown precision %d, or members differ", m,
+                prm[m].precision);
+      fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
   }
   CK(cudaSetDevice(c->device));
-  const xm::StepScalars s = make_scalars(c, prm);
   const xm::Launch l = c->L();
-  const bool mixed = prm->precision == EFDC_XM_PREC_MIXED;
-  const int max_sweeps = prm->max_sweeps > 0 ? prm->max_sweeps : 500;
-  c->last_n = prm->n;
-  c->last_ntstbc = prm->ntstbc;
-  c->last_isdry = prm->isdry;
-
-  // counters of this step
-  int rc = read_ctl(c);
-  if (rc) return stats->status = rc;
-  c->ctl_h->nneg = c->ctl_h->nnonfinite = c->ctl_h->nwasted = 0;
-  c->ctl_h->icordry = 0;
-  c->ctl_h->counter = 0;
-  if ((rc = write_ctl(c))) return stats->status = rc;
-
+  const bool mixed = prm[0].precision == EFDC_XM_PREC_MIXED;
+  bool any_isdry = false, any_legacy = false, any99 = false, any_waste = false;
+  std::vector<int> ncordry(M, 0), status(M, EFDC_XM_OK), max_sweeps(M);
+  for (int m = 0; m < M; ++m) {
+    Member &mb = c->mem[m];
+    c->sc_h[m] = make_scalars(mb, &prm[m]);
+    mb.last_n = prm[m].n;
+    mb.last_ntstbc = prm[m].ntstbc;
+    mb.last_isdry = prm[m].isdry;
+    max_sweeps[m] = prm[m].max_sweeps > 0 ? prm[m].max_sweeps : 500;
+    const int isd = prm[m].isdry;
+    any_isdry |= isd > 0;
+    any_legacy |= (isd > 0 && isd != 99);
+    any99 |= isd == 99;
+    any_waste |= (isd > 0 && prm[m].ndrystp < 0);
+    c->act_h[m] = 1;
+  }
+  CK(cudaMemcpyAsync(c->sc, c->sc_h, sizeof(xm::StepScalars) * M, cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaMemsetAsync(c->ctl, 0, sizeof(Ctl) * M, c->stream));  // counters of this step
+  int rc = write_act(c);
+  if (rc) return rc;
   // time levels by buffer swap: after it the *1 buffers hold the entry values
   // (UHDY1E=UHDYE, VHDX1E=VHDXE, H1P=HP, calpuv2c.f90:256-264) and the
   // others are rewritten for every water cell before they are read
   std::swap(c->X.uhdye, c->X.uhdy1e);
   std::swap(c->X.vhdxe, c->X.vhdx1e);
   std::swap(c->X.hp, c->X.h1p);
-  xm::launch_begin(c->L(), c->S, c->X, s);
-  if (prm->isdry > 0) xm::launch_obc_reset(l, c->B, c->X);
+  xm::launch_begin(l, c->S, c->X);
+  if (any_isdry) xm::launch_obc_reset(l, c->S, c->B, c->X);
   CK(cudaGetLastError());
-  int ncordry = 0, status = EFDC_XM_OK;
-  for (;;) {  // 1000 CONTINUE
-    xm::launch_assemble(l, c->S, c->X, s, c->ctl, c->part);
-    xm::launch_obc(l, c->S, c->X, c->B, s, c->ctl, c->obc_serial);
-    xm::launch_scale(l, c->S, c->X, c->Y, c->ctl, mixed ? 1 : 0, c->may_asym ? 1 : 0);
+  for (;;) {  // 1000 CONTINUE, for the members still sweeping
+    xm::launch_sweep_reset(l, c->ctl, c->act, M);
+    xm::launch_assemble(l, c->S, c->X, c->ctl, c->act);
+    xm::launch_obc(l, c->S, c->X, c->B, c->ctl, c->act, c->obc_serial);
+    xm::launch_scale(l, c->S, c->X, c->Y, c->ctl, c->act, mixed ? 1 : 0, c->any_may_asym ? 1 : 0);
     CK(cudaGetLastError());
-    int iters = 0, st = 0, outer = 0;
-    double rsq = 0;
-    rc = mixed ? solve_mixed(c, c->X.p, prm->rsqm, prm->iterm, &iters, &rsq, &st, &outer,
-                             prm->mixed_rsq_factor)
-               : solve_fp64(c, c->X.p, prm->rsqm, prm->iterm, &iters, &rsq, &st);
-    if (rc) return stats->status = rc;
-    if (c->ctl_h->asym & 2) {
-      set_error("the scaled operator is unsymmetric although the model has no radiation "
-                "boundary (check SUBO/SVBO next to the open-boundary cells)");
-      return stats->status = EFDC_XM_UNSUPPORTED;
-    }
-    stats->iters_last = iters;
-    stats->iters_total += iters;
-    stats->solves += 1;
-    stats->rsq_last = rsq;
-    stats->outer_refinements += outer;
-    stats->ccmnm_last = std::min(c->ctl_h->ccmnm_int, c->ctl_h->ccmnm_bc);
-    if (st != EFDC_XM_OK) {
-      status = st;
-      set_error("CONGRAD: %s after %d iterations (RSQ=%g, RSQM=%g)",
-                st == EFDC_XM_CG_MAXITER ? "maximum iterations exceeded" : "non-finite residual",
-                iters, rsq, prm->rsqm);
-      break;
-    }
-    xm::launch_backsub(l, c->S, c->X, s);
-    xm::launch_obc_hp(l, c->S, c->X, c->B, s);
-    if (prm->isdry > 0 && prm->isdry < 98) {
-      xm::launch_wd_legacy(l, c->S, c->X, s, c->ctl, 1);
-    } else if (prm->isdry == 99) {
-      xm::launch_wd99(l, c->S, c->X, s, c->ctl);
-    } else if (prm->isdry > 0) {
-      xm::launch_wd_legacy(l, c->S, c->X, s, c->ctl, 0);
-    }
-    CK(cudaGetLastError());
-    if (prm->isdry > 0 && prm->isdry != 98) {
-      if ((rc = read_ctl(c))) return stats->status = rc;
-      if (c->ctl_h->icordry) {
-        c->ctl_h->icordry = 0;
-        if ((rc = write_ctl(c))) return stats->status = rc;
-        ++ncordry;
-        if (ncordry < max_sweeps) continue;
-        status = EFDC_XM_WETDRY_MAXSWEEP;
-        set_error("wet/dry: NCORDRY reached %d", max_sweeps);
-        break;
+    rc = mixed ? solve_mixed(c, c->X.p, prm[0].mixed_rsq_factor) : solve_fp64(c, c->X.p);
+    if (rc) return rc;
+    // a member whose solve failed stops here, before the back-substitution
+    bool dropped = false;
+    int nact = 0;
+    for (int m = 0; m < M; ++m) {
+      if (!c->act_h[m]) continue;
+      const Ctl &k = c->ctl_h[m];
+      efdc_xm_stats &s = stats[m];
+      s.iters_last = k.iter;
+      s.iters_total += k.iter;
+      s.solves += 1;
+      s.rsq_last = mixed ? k.rsq64 : k.rsq;
+      s.outer_refinements += k.outer;
+      s.ccmnm_last = std::min(k.ccmnm_int, k.ccmnm_bc);
+      if (k.asym & 2) {
+        status[m] = EFDC_XM_UNSUPPORTED;
+        set_error("member %d: the scaled operator is unsymmetric although the model has no "
+                  "radiation boundary (check SUBO/SVBO next to the open-boundary cells)", m);
+      } else if (k.status != EFDC_XM_OK) {
+        status[m] = k.status;
+        set_error("member %d: CONGRAD: %s after %d iterations (RSQ=%g, RSQM=%g)", m,
+                  k.status == EFDC_XM_CG_MAXITER ? "maximum iterations exceeded"
+                                                 : "non-finite residual",
+                  k.iter, s.rsq_last, prm[m].rsqm);
+      }
+      if (status[m] != EFDC_XM_OK) {
+        c->act_h[m] = 0;
+        dropped = true;
+      } else {
+        ++nact;
       }
     }
-    break;
+    if (nact == 0) break;
+    if (dropped && (rc = write_act(c))) return rc;
+    xm::launch_backsub(l, c->S, c->X, c->act);
+    xm::launch_obc_hp(l, c->S, c->X, c->B, c->act);
+    bool resweep = false;
+    if (any_isdry) {
+      xm::launch_wetdry(l, c->S, c->X, c->ctl, c->act, any_legacy, any99);
+      CK(cudaGetLastError());
+      if ((rc = read_ctl(c))) return rc;
+      for (int m = 0; m < M; ++m) {
+        if (!c->act_h[m]) continue;
+        const int isd = prm[m].isdry;
+        int next = 0;
+        if (isd > 0 && isd != 98 && c->ctl_h[m].icordry) {
+          if (++ncordry[m] < max_sweeps[m]) {
+            next = 1;
+          } else {
+            status[m] = EFDC_XM_WETDRY_MAXSWEEP;
+            set_error("member %d: wet/dry: NCORDRY reached %d", m, max_sweeps[m]);
+          }
+        }
+        c->act_h[m] = next;
+        resweep |= next != 0;
+      }
+    }
+    CK(cudaGetLastError());
+    if (!resweep) break;
+    if ((rc = write_act(c))) return rc;
   }
-  if (status == EFDC_XM_OK) {
-    xm::launch_final(l, c->S, c->X, s, c->ctl);
+  // finalisation of the members whose sweeps ended normally
+  bool any_fin = false;
+  for (int m = 0; m < M; ++m) {
+    c->act_h[m] = (status[m] == EFDC_XM_OK) ? 1 : 0;
+    any_fin |= c->act_h[m] != 0;
+  }
+  if (any_fin) {
+    if ((rc = write_act(c))) return rc;
+    xm::launch_final(l, c->S, c->X, c->ctl, c->act, any_waste);
     CK(cudaGetLastError());
   }
-  if ((rc = read_ctl(c))) return stats->status = rc;
-  stats->n_negdep = c->ctl_h->nneg;
-  stats->n_wasted = c->ctl_h->nwasted;
-  if (status == EFDC_XM_OK && c->ctl_h->nnonfinite > 0) {
-    status = EFDC_XM_NONFINITE;
-    set_error("non-finite P in %d cells", c->ctl_h->nnonfinite);
+  if ((rc = read_ctl(c))) return rc;
+  for (int m = 0; m < M; ++m) {
+    efdc_xm_stats &s = stats[m];
+    const Ctl &k = c->ctl_h[m];
+    s.n_negdep = k.nneg;
+    s.n_wasted = k.nwasted;
+    if (status[m] == EFDC_XM_OK && k.nnonfinite > 0) {
+      status[m] = EFDC_XM_NONFINITE;
+      set_error("member %d: non-finite P in %d cells", m, k.nnonfinite);
+    }
+    if (status[m] == EFDC_XM_OK && k.nneg > 0) status[m] = EFDC_XM_NEG_DEPTH;
+    s.status = status[m];
   }
-  if (status == EFDC_XM_OK && c->ctl_h->nneg > 0) status = EFDC_XM_NEG_DEPTH;
-  stats->status = status;
-  return status;
+  return overall_status(stats, M);
+}
+
+int32_t efdc_xm_step_batch(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
+                           efdc_xm_stats *stats) {
+  if (!c || !prm || !f || !stats) {
+    set_error("efdc_xm_step: NULL argument");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  const int M = c->M;
+  std::memset(stats, 0, sizeof(efdc_xm_stats) * M);
+  for (int m = 0; m < M; ++m) {
+    const efdc_xm_fields &x = f[m];
+    if (!x.p || !x.hp || !x.hu || !x.hv || !x.uhdye || !x.vhdxe || !x.sub || !x.svb) {
+      set_error("efdc_xm_step: member %d: NULL argument (P, HP, HU, HV, UHDYE, VHDXE, SUB, SVB "
+                "are required)", m);
+      fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+    if (prm[m].isdry > 0 && (!x.sbx || !x.sby || !x.lmaskdry || !x.iscdry)) {
+      set_error("efdc_xm_step: member %d: ISDRY>0 needs SBX, SBY, LMASKDRY and ISCDRY", m);
+      fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+  }
+  int rc = efdc_xm_upload_batch(c, f);
+  if (rc) {
+    fill_status(stats, M, rc);
+    return rc;
+  }
+  const int st = efdc_xm_step_device_batch(c, prm, stats);
+  if (st == EFDC_XM_CUDA_ERROR || st == EFDC_XM_BAD_ARGUMENT) return st;
+  if ((rc = efdc_xm_download_batch(c, f))) {
+    fill_status(stats, M, rc);
+    return rc;
+  }
+  for (int m = 0; m < M; ++m) {
+    if (!(f[m].lwet || f[m].ldry)) continue;
+    const Member &mb = c->mem[m];
+    if (prm[m].isdry == 0) {
+      stats[m].lawet = mb.la - 1;
+      stats[m].ladry = 0;
+    } else {
+      int nw = 0, nd = 0;
+      for (int L = 2; L <= mb.la; ++L) {
+        if (f[m].lmaskdry[L - 1]) ++nw;
+        else if ((!mb.oldmask_h.empty() && mb.oldmask_h[L - 1]) || prm[m].n < prm[m].ntstbc + 1)
+          ++nd;
+      }
+      stats[m].lawet = nw;
+      stats[m].ladry = nd;
+    }
+  }
+  return st;
+}
+
+}  // extern "C"
+
+namespace {
+int single_only(const efdc_xm_ctx *c, const char *who) {
+  if (!c) {
+    set_error("%s: NULL context", who);
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  if (c->M != 1) {
+    set_error("%s: the context holds %d members; use the _batch entry point", who, c->M);
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  return EFDC_XM_OK;
+}
+}  // namespace
+
+extern "C" {
+
+// ---- single-basin entry points: the batch API with one member ----
+int32_t efdc_xm_upload(efdc_xm_ctx *c, const efdc_xm_fields *f) {
+  const int rc = single_only(c, "efdc_xm_upload");
+  return rc ? rc : efdc_xm_upload_batch(c, f);
+}
+
+int32_t efdc_xm_download(efdc_xm_ctx *c, efdc_xm_fields *f) {
+  const int rc = single_only(c, "efdc_xm_download");
+  return rc ? rc : efdc_xm_download_batch(c, f);
+}
+
+int32_t efdc_xm_step_device(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats) {
+  efdc_xm_stats dummy;
+  if (!stats) stats = &dummy;
+  std::memset(stats, 0, sizeof(*stats));
+  const int rc = single_only(c, "efdc_xm_step_device");
+  if (rc) return stats->status = rc;
+  return efdc_xm_step_device_batch(c, prm, stats);
 }
 
 int32_t efdc_xm_step(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
@@ -810,72 +1150,52 @@ int32_t efdc_xm_step(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *
   efdc_xm_stats dummy;
   if (!stats) stats = &dummy;
   std::memset(stats, 0, sizeof(*stats));
-  if (!c || !prm || !f || !f->p || !f->hp || !f->hu || !f->hv || !f->uhdye || !f->vhdxe ||
-      !f->sub || !f->svb) {
-    set_error("efdc_xm_step: NULL argument (P, HP, HU, HV, UHDYE, VHDXE, SUB, SVB are required)");
-    return stats->status = EFDC_XM_BAD_ARGUMENT;
-  }
-  if (prm->isdry > 0 && (!f->sbx || !f->sby || !f->lmaskdry || !f->iscdry)) {
-    set_error("efdc_xm_step: ISDRY>0 needs SBX, SBY, LMASKDRY and ISCDRY");
-    return stats->status = EFDC_XM_BAD_ARGUMENT;
-  }
-  int rc = efdc_xm_upload(c, f);
+  const int rc = single_only(c, "efdc_xm_step");
   if (rc) return stats->status = rc;
-  const int st = efdc_xm_step_device(c, prm, stats);
-  if (st == EFDC_XM_CUDA_ERROR || st == EFDC_XM_BAD_ARGUMENT) return st;
-  rc = efdc_xm_download(c, f);
-  if (rc) return stats->status = rc;
-  if (f->lwet || f->ldry) {
-    if (prm->isdry == 0) {
-      stats->lawet = c->la - 1;
-      stats->ladry = 0;
-    } else {
-      int nw = 0, nd = 0;
-      for (int L = 2; L <= c->la; ++L) {
-        if (f->lmaskdry[L - 1]) ++nw;
-        else if ((!c->oldmask_h.empty() && c->oldmask_h[L - 1]) || prm->n < prm->ntstbc + 1) ++nd;
-      }
-      stats->lawet = nw;
-      stats->ladry = nd;
-    }
-  }
-  return st;
+  return efdc_xm_step_batch(c, prm, f, stats);
 }
 
 int32_t efdc_xm_congrad(efdc_xm_ctx *c, const double *ccc, const double *ccs, const double *ccn,
                         const double *ccw, const double *cce, const double *ccci,
                         const double *fptmp, double *p, double rsqm, int32_t iterm,
                         int32_t precision, int32_t *iters, double *rsq) {
-  if (!c || !ccc || !ccs || !ccn || !ccw || !cce || !fptmp || !p || iterm < 1) {
+  int rc = single_only(c, "efdc_xm_congrad");
+  if (rc) return rc;
+  if (!ccc || !ccs || !ccn || !ccw || !cce || !fptmp || !p || iterm < 1) {
     set_error("efdc_xm_congrad: NULL argument or ITERM < 1");
     return EFDC_XM_BAD_ARGUMENT;
   }
   (void)ccci;  // CCCI = 1./CCC is recomputed on the device (same rounding)
   CK(cudaSetDevice(c->device));
   // the scaled system; land slots are reset to the inert CCC=1, C*=0, b=0
-  std::vector<Xfer> xs = {{ccc, c->Y.ccc, 3}, {ccs, c->Y.ccs, 3}, {ccn, c->Y.ccn, 3},
-                          {ccw, c->Y.ccw, 3}, {cce, c->Y.cce, 3}, {fptmp, c->Y.fptmp, 3},
-                          {p, c->X.p, 0}};
-  int rc = upload_arrays(c, xs);
-  if (rc) return rc;
-  CK(cudaMemsetAsync(&c->ctl->asym, 0, sizeof(int), c->stream));
-  xm::launch_sys_prepare(c->L(), c->S, c->Y, c->ctl, precision == EFDC_XM_PREC_MIXED ? 1 : 0);
+  auto one = [](const void *q) { return std::vector<const void *>{q}; };
+  std::vector<Xfer> xs = {{one(ccc), c->Y.ccc, 3}, {one(ccs), c->Y.ccs, 3},
+                          {one(ccn), c->Y.ccn, 3}, {one(ccw), c->Y.ccw, 3},
+                          {one(cce), c->Y.cce, 3}, {one(fptmp), c->Y.fptmp, 3},
+                          {one(p), c->X.p, 0}};
+  if ((rc = upload_arrays(c, xs))) return rc;
+  c->sc_h[0] = xm::StepScalars{};
+  c->sc_h[0].rsqm = rsqm;
+  c->sc_h[0].iterm = iterm;
+  CK(cudaMemcpyAsync(c->sc, c->sc_h, sizeof(xm::StepScalars), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->ctl, 0, sizeof(Ctl), c->stream));
+  c->act_h[0] = 1;
+  if ((rc = write_act(c))) return rc;
+  const bool mixed = precision == EFDC_XM_PREC_MIXED;
+  xm::launch_sys_prepare(c->L(), c->S, c->Y, c->ctl, mixed ? 1 : 0);
   CK(cudaGetLastError());
-  int it = 0, st = 0, outer = 0;
-  double r = 0;
-  rc = (precision == EFDC_XM_PREC_MIXED)
-           ? solve_mixed(c, c->X.p, rsqm, iterm, &it, &r, &st, &outer, 0.0)
-           : solve_fp64(c, c->X.p, rsqm, iterm, &it, &r, &st);
+  rc = mixed ? solve_mixed(c, c->X.p, 0.0) : solve_fp64(c, c->X.p);
   if (rc) return rc;
-  std::vector<Xfer> out = {{p, c->X.p, 0}};
-  rc = download_arrays(c, out);
-  if (rc) return rc;
-  if (iters) *iters = it;
-  if (rsq) *rsq = r;
-  if (st != EFDC_XM_OK)
+  const Ctl k = c->ctl_h[0];
+  std::vector<Xfer> out = {{one(p), c->X.p, 0}};
+  if ((rc = download_arrays(c, out))) return rc;
+  if (iters) *iters = k.iter;
+  if (rsq) *rsq = mixed ? k.rsq64 : k.rsq;
+  if (k.status != EFDC_XM_OK)
     set_error("CONGRAD: %s after %d iterations (RSQ=%g)",
-              st == EFDC_XM_CG_MAXITER ? "maximum iterations exceeded" : "non-finite residual", it, r);
-  return st;
+              k.status == EFDC_XM_CG_MAXITER ? "maximum iterations exceeded" : "non-finite residual",
+              k.iter, mixed ? k.rsq64 : k.rsq);
+  return k.status;
 }
 
 void *efdc_xm_stream(efdc_xm_ctx *c) { return c ? static_cast<void *>(c->stream) : nullptr; }
@@ -889,34 +1209,32 @@ int32_t efdc_xm_time_kernels(efdc_xm_ctx *c, int32_t precision, int32_t reps, ef
   }
   CK(cudaSetDevice(c->device));
   const xm::Launch l = c->L();
+  const bool mixed = precision == EFDC_XM_PREC_MIXED;
   cudaEvent_t ev[3];
   for (auto &e : ev) CK(cudaEventCreate(&e));
   double tm = 0, tu = 0;
-  // the iterations run on a scratch copy of P with the stop test disabled
+  // the iterations run on a scratch copy of P with the stop tests disabled
   CK(cudaMemcpyAsync(c->ptmp, c->X.p, size_t(c->nslot) * sizeof(double), cudaMemcpyDeviceToDevice,
                      c->stream));
-  if (precision == EFDC_XM_PREC_MIXED) {
-    xm::launch_mx_resid(l, c->S, c->Y, c->ptmp, c->ctl, c->part, 0.0, 0.0);
-  } else {
-    xm::launch_cg_init(l, c->S, c->Y, c->ptmp, c->ctl, c->part);
-  }
-  CK(cudaGetLastError());
-  int rc = read_ctl(c);
+  for (int m = 0; m < c->M; ++m) c->act_h[m] = 1;
+  int rc = write_act(c);
   if (rc) return rc;
-  c->ctl_h->done = 0;
-  c->ctl_h->idone = 0;
-  c->ctl_h->status = 0;
-  if ((rc = write_ctl(c))) return rc;
+  xm::launch_solve_reset(l, c->ctl, c->glob, c->act, c->M);
+  if (mixed)
+    xm::launch_mx_resid(l, c->S, c->Y, c->ptmp, c->ctl, c->glob, c->part, 1.0, 0.0, 1);
+  else
+    xm::launch_cg_init(l, c->S, c->Y, c->ptmp, c->ctl, c->glob, c->part);
+  CK(cudaGetLastError());
   for (int k = 0; k < reps; ++k) {
     CK(cudaEventRecord(ev[0], c->stream));
-    if (precision == EFDC_XM_PREC_MIXED) {
+    if (mixed) {
       xm::launch_mx_matvec(l, c->S, c->Y, c->ctl, c->part);
       CK(cudaEventRecord(ev[1], c->stream));
-      xm::launch_mx_update(l, c->S, c->Y, c->ctl, c->part, INT_MAX, INT_MAX);
+      xm::launch_mx_update(l, c->S, c->Y, c->ctl, c->glob, c->part, 1);
     } else {
       xm::launch_cg_matvec(l, c->S, c->Y, c->ctl, c->part);
       CK(cudaEventRecord(ev[1], c->stream));
-      xm::launch_cg_update(l, c->S, c->Y, c->ptmp, c->ctl, c->part, -1.0, INT_MAX);
+      xm::launch_cg_update(l, c->S, c->Y, c->ptmp, c->ctl, c->glob, c->part, 1);
     }
     CK(cudaEventRecord(ev[2], c->stream));
     CK(cudaEventSynchronize(ev[2]));
@@ -926,17 +1244,21 @@ int32_t efdc_xm_time_kernels(efdc_xm_ctx *c, int32_t precision, int32_t reps, ef
     tm += a;
     tu += b;
   }
-  if ((rc = read_ctl(c))) return rc;
   for (auto &e : ev) cudaEventDestroy(e);
+  if ((rc = read_ctl(c))) return rc;
   out->ms_matvec = tm / reps;
   out->ms_update = tu / reps;
   out->reps = reps;
-  out->ncells = c->la - 1;
+  long long ncell = 0;
+  for (const Member &mb : c->mem) ncell += mb.la - 1;
+  out->ncells = int32_t(std::min<long long>(ncell, INT32_MAX));
   out->nslots = (c->ntile - 1) * TILE;
-  if (c->ctl_h->done) {
-    set_error("efdc_xm_time_kernels: the iteration stopped early (status %d)", c->ctl_h->status);
-    return EFDC_XM_NONFINITE;
-  }
+  for (int m = 0; m < c->M; ++m)
+    if (c->ctl_h[m].done) {
+      set_error("efdc_xm_time_kernels: the iteration of member %d stopped early (status %d)", m,
+                c->ctl_h[m].status);
+      return EFDC_XM_NONFINITE;
+    }
   return EFDC_XM_OK;
 }
 

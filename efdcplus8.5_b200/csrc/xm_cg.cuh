@@ -15,18 +15,152 @@ namespace xm {
 __device__ __forceinline__ float rcpT(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double rcpT(double x) { return 1. / x; }
 
-// The CG kernels loop over the active tiles, 4 per CTA iteration; past the
-// end a thread works on tile 0 (the ghost tile, all inert) with stores off,
-// so that every lane of a row takes part in the shuffles.
-#define CG_TILE_LOOP(ntile)                                                         \
-  const int sub_ = threadIdx.x / TPT, q_ = threadIdx.x % TPT;                       \
-  for (int base_ = blockIdx.x * TILES_PER_CTA; base_ < (ntile) - 1;                 \
-       base_ += gridDim.x * TILES_PER_CTA)
+// The CG kernels loop over "quads": 4 consecutive tiles of one member, one
+// CTA pass each (a thread owns 4 cells of a row, 64 threads per tile), quads
+// dealt to the CTAs cyclically.  Past the member's last tile a thread works
+// on tile 0 (the ghost tile, all inert) with stores off, so that every lane
+// of a row takes part in the shuffles.  A quad whose member is finished (or
+// not in this sweep) is skipped by the whole CTA.
+//
+// Reductions: each pass leaves one partial per warp in shared memory (warp
+// shuffles only, no CTA barrier per quad).  Every QCAP quads, and at the end,
+// the CTA "flushes": it adds the warp partials of each quad in fixed warp
+// order into part[quad], publishes them with one fence, and counts its quads
+// into the member's arrival counter (one atomic per member it touched).  The
+// CTA that completes a member reduces the member's per-quad partials in
+// fixed quad order (reduce_partials) and runs the epilogue (thread 0 writes
+// the member's Ctl).  The sums therefore do not depend on the grid size or
+// on which other members share the context.
+constexpr int QCAP = 32;         // quads a CTA logs between two flushes
+constexpr int NWARP = NT / 32;   // warps per CTA
 
-#define CG_TILE_GEO(S)                                                              \
-  const int ti_ = base_ + sub_;                                                     \
-  const bool valid = ti_ < ntile - 1;                                               \
-  const RowGeo g = row_geo((S).tnbr, valid ? ti_ + 1 : 0, q_)
+template <int NS>
+struct QuadLog {
+  double w[NS][QCAP][NWARP];  // per-warp partials of NS sums
+  int qd[QCAP];               // quad of each entry
+  int mem[QCAP];              // its member
+  int last[QCAP];             // this CTA completed the member
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int NS, class Epi>
+__device__ __forceinline__ void quad_flush(QuadLog<NS> &L, int n, const DevStatic &S, Ctl *ctl,
+                                           double *part, double *sh, Epi &epi) {
+  __syncthreads();  // the warp partials and the entries are in shared memory
+  const int t = threadIdx.x;
+  if (t < n) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      double a = 0.0;
+#pragma unroll
+      for (int w = 0; w < NWARP; ++w) a += L.w[s][t][w];
+      part[size_t(s) * S.nquad + L.qd[t]] = a;
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (t < n) {
+    const int m = L.mem[t];
+    int last = 0;
+    if (t == 0 || L.mem[t - 1] != m) {  // head of a run of equal members
+      int cnt = 1;
+      while (t + cnt < n && L.mem[t + cnt] == m) ++cnt;
+      const unsigned total = unsigned(S.qstart[m + 1] - S.qstart[m]);
+      const unsigned prev = atomicAdd(&ctl[m].counter, unsigned(cnt));
+      if (prev + unsigned(cnt) == total) {
+        last = 1;
+        ctl[m].counter = 0u;  // every quad of m has arrived: ready for the next kernel
+      }
+    }
+    L.last[t] = last;
+  }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    if (!L.last[k]) continue;  // uniform: shared memory
+    __threadfence();
+    const int m = L.mem[k];
+    const int q0 = S.qstart[m], nq = S.qstart[m + 1] - q0;
+    double r[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) r[s] = reduce_partials(part + size_t(s) * S.nquad + q0, nq, sh);
+    epi(m, r);  // r valid in thread 0
+  }
+  __syncthreads();  // the log is reused after this
+}
+
+// One CG kernel over all quads.  setup(m) returns the member's values for the
+// body (a struct with at least `bool skip`); it runs when the member changes
+// from one quad to the next, so a CTA reads a member's Ctl once per run of
+// its quads.  body(a, g, valid, v) processes one quad row vector and adds its
+// parts of the NS sums to v[]; epi(m, r) finishes member m with its NS sums.
+template <int NS, class Setup, class Body, class Epi>
+__device__ __forceinline__ void quad_sweep(const DevStatic &S, Ctl *ctl, double *part,
+                                           Setup setup, Body body, Epi epi) {
+  __shared__ QuadLog<NS> L;
+  __shared__ double sh[32];
+  const int sub = threadIdx.x / TPT, q = threadIdx.x % TPT;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int n = 0;
+  int qd = blockIdx.x;
+  int2 cur = qd < S.nquad ? S.quads[qd] : make_int2(0, 0);
+  int mc = cur.x;
+  auto a = setup(mc);
+  int tend = S.tend[mc];
+  while (qd < S.nquad) {
+    const int qn = qd + gridDim.x;
+    const int2 nxt = qn < S.nquad ? S.quads[qn] : make_int2(0, 0);  // prefetch
+    const int m = cur.x;
+    if (m != mc) {
+      mc = m;
+      a = setup(m);
+      tend = S.tend[m];
+    }
+    if (!a.skip) {
+      const int ti = cur.y + sub;
+      const bool valid = ti < tend;
+      const RowGeo g = row_geo(S.tnbr, valid ? ti : 0, q);
+      double v[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) v[s] = 0.0;
+      body(a, g, valid, v);
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const double x = warp_sum(v[s]);
+        if (lane == 0) L.w[s][n][warp] = x;
+      }
+      if (threadIdx.x == 0) {
+        L.qd[n] = qd;
+        L.mem[n] = m;
+      }
+      if (++n == QCAP) {
+        quad_flush<NS>(L, n, S, ctl, part, sh, epi);
+        n = 0;
+      }
+    }
+    qd = qn;
+    cur = nxt;
+  }
+  if (n) quad_flush<NS>(L, n, S, ctl, part, sh, epi);
+}
+
+// The same loop without reductions (member-wise vector updates).
+template <class Skip, class Body>
+__device__ __forceinline__ void quad_apply(const DevStatic &S, Skip skip, Body body) {
+  const int sub = threadIdx.x / TPT, q = threadIdx.x % TPT;
+  for (int qd = blockIdx.x; qd < S.nquad; qd += gridDim.x) {
+    const int2 cur = S.quads[qd];
+    const int m = cur.x;
+    if (skip(m)) continue;
+    const int ti = cur.y + sub;
+    if (ti >= S.tend[m]) continue;
+    body(m, row_geo(S.tnbr, ti, q));
+  }
+}
 
 // PCG = CCCI*RCG + BETA*PCG (congrad.f90:133-159) on the cell's row vector and
 // its N/S rows and E/W neighbours, then APCG = CCC*P + CCS*PS + CCN*PN + CCW*PW

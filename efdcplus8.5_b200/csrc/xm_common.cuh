@@ -81,6 +81,12 @@ __device__ __forceinline__ double reduce_partials(const double *part, int nblk, 
   return block_sum(s, sh);
 }
 
+// atomic min of a non-negative double (its bit pattern orders like its value)
+__device__ __forceinline__ void atomic_min_nonneg(double *addr, double v) {
+  atomicMin(reinterpret_cast<unsigned long long *>(addr),
+            static_cast<unsigned long long>(__double_as_longlong(fmax(v, 0.0))));
+}
+
 // ---------------------------------------------------------------------------
 // Row-vector geometry of the CG kernels: a thread owns 4 consecutive cells of
 // one tile row (8 threads per row, 64 per tile, 4 tiles per 256-thread CTA).

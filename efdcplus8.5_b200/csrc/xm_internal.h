@@ -1,13 +1,19 @@
 // xm_internal.h -- device data layout and kernel interface of libefdc_xm.
 //
-// Layout ("bricks"): the structured grid is cut into 32x8-cell tiles.  Tiles
-// holding at least one water cell are stored contiguously, ordered along a
-// Morton (Z) curve of their tile coordinates; inside a tile a cell's slot is
-// ty*32+tx.  Slot d = tile*256 + ty*32 + tx.  Tile 0 is a ghost tile (all
-// land).  Neighbours come from the slot position plus a 4-entry tile
-// neighbour table, so no per-cell index arrays are read in the solver: E/W
-// neighbours are adjacent words and N/S neighbours are the rows above and
-// below, which keeps every warp access a contiguous 32-cell row.
+// Layout ("bricks"): each basin's structured grid is cut into 32x8-cell
+// tiles.  Tiles holding at least one water cell are stored contiguously,
+// member after member, each member's tiles ordered along a Morton (Z) curve of
+// their tile coordinates; inside a tile a cell's slot is ty*32+tx.  Slot
+// d = tile*256 + ty*32 + tx.  Tile 0 is a ghost tile (all land).  Neighbours
+// come from the slot position plus a 4-entry tile neighbour table, so no
+// per-cell index arrays are read in the solver: E/W neighbours are adjacent
+// words and N/S neighbours are the rows above and below, which keeps every
+// warp access a contiguous 32-cell row.
+//
+// A context holds M >= 1 independent basins ("members" of an ensemble); one
+// launch of each kernel covers all of them.  Everything that the reference
+// reduces over a basin (CCMNM, the CG dot products, the wet/dry re-solve flag,
+// the negative-depth count) is reduced per member.
 //
 // Land slots (padding inside a tile, and tile 0) stand for EFDC+'s ghost cell
 // LC (a missing neighbour maps to LC, EFDC/cellmap.f90:80-134): they hold the
@@ -28,11 +34,48 @@ constexpr int MT_MAX = 16;     // max harmonic constituents per call
 
 enum SlotKind : uint8_t { LAND = 0, WATER = 1, OPENBC = 2 };
 
+// Per-member scalars of one call (device memory, refreshed every step).
+struct StepScalars {
+  double delt, deltd2, delti, g, gi, hdry, rsqm, snlt, ritb1;
+  int isdry, ndrystp, isbal, iterm;
+  double cosv[MT_MAX], sinv[MT_MAX];
+};
+
+// Device-side control block of one member.  Written by the "last CTA" of a
+// member's reductions; read by the host once per solve.
+struct Ctl {
+  double rpcg, alpha, beta, rsq, papcg;
+  double rsq64, rsq_target;       // MIXED: outer residual, inner target
+  double ccmnm_int, ccmnm_bc;     // min CC over interior / open-BC cells (atomic min on bits)
+  int iter, done, status, parity; // status: enum efdc_xm_status
+  int inner_iter, outer, idone;   // MIXED bookkeeping (idone: inner solve finished)
+  int asym;                       // 1 if the scaled operator is not symmetric (2: unexpected)
+  int icordry;                    // wet/dry re-solve flag of this sweep
+  int active;                     // member takes part in the current sweep
+  int nneg, nnonfinite, nwasted;
+  unsigned int counter;           // last-CTA arrival counter
+  int pad;
+};
+
+// Counters across members, polled by the host.
+struct Glob {
+  int ndone;     // members whose solve finished
+  int nidone;    // members whose inner (FP32) solve finished
+  int nicordry;  // members that need another wet/dry sweep
+  int pad;
+};
+
 // Static per-slot model data (FP64).  Land slots hold element LC.
 struct DevStatic {
   const int4 *tnbr;       // [ntile] (w, e, s, n) neighbour tiles, 0 = ghost tile
   const uint8_t *kind;    // [nslot]
-  const int *lidx;        // [nslot] L of the slot, 0 for land
+  const int *lidx;        // [nslot] member-local L of the slot, 0 for land
+  const int *tile_member; // [ntile] member of each tile
+  const int2 *quads;      // [nquad] (member, first tile): 4-tile units of the CG kernels
+  const int *qstart;      // [M+1] first quad of each member
+  const int *tend;        // [M] one past the member's last tile
+  const StepScalars *sc;  // [M] per-member scalars of the current step
+  int nquad;
   const double *dxyp, *dxyip, *dxiu, *dyiu, *dxiv, *dyiv, *dxyu, *dxyv;
   const double *hruo, *hrvo, *subo, *svbo, *sbxo, *sbyo, *belv;
   const double *rcx;      // RCX = RCY: 1 on water, 0 on ghosts (calpuv2c.f90:97-102)
@@ -64,38 +107,19 @@ struct DevSystem {
   float *r32, *pa32, *pb32, *ap32, *x32;         // FP32 inner CG vectors (scaled)
 };
 
-// Device-side control block of one solve.  Written by the "last CTA" of each
-// reduction; read by the host once per solve.
-struct Ctl {
-  double rpcg, alpha, beta, rsq, papcg;
-  double rsq64, rsq_target;       // MIXED: outer residual, inner target
-  double ccmnm_int, ccmnm_bc;     // min CC over interior / open-BC cells
-  int iter, done, status, parity; // status: enum efdc_xm_status
-  int inner_iter, outer, idone;   // MIXED bookkeeping (idone: inner solve finished)
-  int asym;                       // 1 if the scaled operator is not symmetric
-  int icordry;                    // wet/dry re-solve flag
-  int nneg, nnonfinite, nwasted;
-  unsigned int counter;           // last-CTA arrival counter
-  unsigned int counter2;
-};
-
-// Open-boundary cells (packed W, E, S, N in the reference's loop order).
+// Open-boundary cells (packed per member: W, E, S, N in the reference's loop order).
 struct DevObc {
   int n;                 // total number of open-boundary cells
-  int mtide;
+  int mtmax;             // stride of pcb/psb (max MTIDE over members)
   const int *slot;       // [n] slot of the boundary cell
   const int *nbr;        // [n] slot of its interior neighbour (LEC/LWC/LNC/LSC)
   const int *side;       // [n] 0 W, 1 E, 2 S, 3 N
   const int *ispb;       // [n]
-  const double *pcb, *psb;  // [n*mtide], index k*mtide+m
+  const int *member;     // [n]
+  const int *mtide;      // [M] harmonic constituents of each member
+  const int *bstart;     // [M+1] first boundary cell of each member
+  const double *pcb, *psb;  // [n*mtmax], index k*mtmax+m
   const double *pser;    // [n] per-step series part
-  const int *side_start; // [5] prefix offsets of the sides
-};
-
-struct StepScalars {
-  double delt, deltd2, delti, g, gi, hdry, rsqm, snlt, ritb1;
-  int isdry, ndrystp, isbal, iterm;
-  double cosv[MT_MAX], sinv[MT_MAX];
 };
 
 }  // namespace xm

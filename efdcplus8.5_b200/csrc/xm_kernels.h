@@ -11,59 +11,62 @@ namespace xm {
 
 struct Launch {
   int grid;          // CTAs of the grid-stride cell kernels (one tile per CTA pass)
-  int grid_cg;       // CTAs of the FP64 CG kernels (four tiles per CTA pass)
+  int grid_cg;       // CTAs of the FP64 CG kernels (one quad of 4 tiles per CTA pass)
   int grid_mv64;     // CTAs of the FP64 matrix-vector kernel (register-heavy)
-  int grid_cg32;     // CTAs of the FP32 matrix-vector kernel (four tiles per CTA pass)
+  int grid_cg32;     // CTAs of the FP32 matrix-vector kernel
   int grid_up32;     // CTAs of the FP32 update kernel
   int ntile;         // tiles including the ghost tile 0
   cudaStream_t stream;
 };
 
-// One array to move between host order (element L at [L-1]) and tile order.
+// One array to move between host order and tile order (see k_scatter).
 struct CopyJob {
-  const void *host_order;  // device staging buffer in host (L) order
+  const void *host_order;  // device staging buffer: every member's array back to back
   void *dev;               // tile-order device array
   int is_int;              // 0 double, 1 LOGICAL (0/1), 2 raw int, 3 double water-only
 };
 
-void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c);
-void launch_assemble(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
-                     Ctl *ctl, double *part);
-void launch_obc(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B,
-                const StepScalars &c, Ctl *ctl, bool serial);
-void launch_obc_reset(const Launch &l, const DevObc &B, const DevState &X);
+void launch_begin(const Launch &l, const DevStatic &S, const DevState &X);
+void launch_sweep_reset(const Launch &l, Ctl *ctl, const int *act, int nmember);
+void launch_assemble(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
+                     const int *act);
+void launch_obc(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B, Ctl *ctl,
+                const int *act, bool serial);
+void launch_obc_reset(const Launch &l, const DevStatic &S, const DevObc &B, const DevState &X);
 void launch_scale(const Launch &l, const DevStatic &S, const DevState &X, const DevSystem &Y,
-                  Ctl *ctl, int mixed, int write_cross);
+                  Ctl *ctl, const int *act, int mixed, int write_cross);
+void launch_solve_reset(const Launch &l, Ctl *ctl, Glob *glob, const int *act, int nmember);
+void launch_outer_reset(const Launch &l, Glob *glob);
 void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
-                    double *part);
+                    Glob *glob, double *part);
 void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
-                    double *part, double rsqm, int iterm);
-void launch_mx_resid(const Launch &l, const DevStatic &S, const DevSystem &Y, const double *P,
-                     Ctl *ctl, double *part, double rsqm, double rel_tol);
-void launch_mx_apply(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P);
-void launch_mx_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
-                    double *part, int inner_cap, int total_cap);
+                    Glob *glob, double *part);
 void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part);
 void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
-                      double *part, double rsqm, int iterm);
+                      Glob *glob, double *part, int no_stop);
+void launch_mx_resid(const Launch &l, const DevStatic &S, const DevSystem &Y, const double *P,
+                     Ctl *ctl, Glob *glob, double *part, double rsqm_fac, double rel_tol,
+                     int no_stop);
+void launch_mx_apply(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
+                     const Ctl *ctl);
 void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part);
 void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
-                      double *part, int inner_cap, int total_cap);
-void launch_backsub(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c);
+                      Glob *glob, double *part, int no_stop);
+void launch_mx_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl, Glob *glob,
+                    double *part);
+void launch_backsub(const Launch &l, const DevStatic &S, const DevState &X, const int *act);
 void launch_obc_hp(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B,
-                   const StepScalars &c);
-void launch_wd_legacy(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
-                      Ctl *ctl, int check);
-void launch_wd99(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
-                 Ctl *ctl);
-void launch_final(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
-                  Ctl *ctl);
-void launch_scatter(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx, int nslot,
-                    int lc);
-void launch_gather(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx, int nslot);
-
+                   const int *act);
+void launch_wetdry(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
+                   const int *act, bool any_legacy, bool any99);
+void launch_final(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
+                  const int *act, bool any_waste);
+void launch_scatter(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx,
+                    const int *tile_member, const long long *moff, const int *mlc, int nslot);
+void launch_gather(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx,
+                   const int *tile_member, const long long *moff, int nslot);
 void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                         int mixed);
 

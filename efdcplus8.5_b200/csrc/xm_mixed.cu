@@ -15,87 +15,92 @@ namespace xm {
 #define TILE_LOOP(ntile)                                                      \
   for (int tile = blockIdx.x + 1; tile < (ntile); tile += gridDim.x)
 
-// p = z + beta*p_old at the cell and its neighbours, Ap, p.Ap, ALPHA.
-__global__ void __launch_bounds__(NT, 5) k_mx_matvec(DevStatic S, DevSystem Y, int ntile, Ctl *ctl,
-                                                 double *part) {
-  __shared__ double sh[32];
-  if (ctl->done | ctl->idone) return;
-  const float beta = float(ctl->beta);
-  const bool par = ctl->parity;
-  const float *pold = par ? Y.pb32 : Y.pa32;
-  float *pnew = par ? Y.pa32 : Y.pb32;
-  const bool asym = ctl->asym;
-  double acc = 0.0;
-  CG_TILE_LOOP(ntile) {
-    CG_TILE_GEO(S);
-    acc += matvec_row_scaled(g, valid, Y.r32, pold, pnew, Y.as32, Y.aw32, Y.ae32, Y.an32, Y.ap32,
-                             beta, asym);
-  }
-  acc = block_sum(acc, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = acc;
-  if (arrive_last(&ctl->counter)) {
-    const double papcg = reduce_partials(part, gridDim.x, sh);
-    if (threadIdx.x == 0) {
-      ctl->papcg = papcg;
-      ctl->alpha = ctl->rpcg / papcg;
-      ctl->counter = 0;
-    }
-  }
+// p = r + beta*p_old at the cell and its halo, Ahat*p, p.Ap, ALPHA (per member).
+__global__ void __launch_bounds__(NT, 5) k_mx_matvec(DevStatic S, DevSystem Y, Ctl *ctl,
+                                                    double *part) {
+  struct A {
+    bool skip, asym;
+    float beta;
+    const float *pold;
+    float *pnew;
+  };
+  quad_sweep<1>(
+      S, ctl, part,
+      [&](int m) {
+        const Ctl &k = ctl[m];
+        const bool par = k.parity;
+        return A{(k.done | k.idone) != 0, k.asym != 0, float(k.beta), par ? Y.pb32 : Y.pa32,
+                 par ? Y.pa32 : Y.pb32};
+      },
+      [&](const A &a, const RowGeo &g, bool valid, double *v) {
+        v[0] = matvec_row_scaled(g, valid, Y.r32, a.pold, a.pnew, Y.as32, Y.aw32, Y.ae32, Y.an32,
+                                 Y.ap32, a.beta, a.asym);
+      },
+      [&](int m, const double *sum) {
+        if (threadIdx.x != 0) return;
+        ctl[m].papcg = sum[0];
+        ctl[m].alpha = ctl[m].rpcg / sum[0];
+      });
 }
 
-// x += alpha*p, r -= alpha*Ap, r.z and r.r (FP64 sums), BETA, inner stop test.
-__global__ void __launch_bounds__(NT) k_mx_update(DevStatic S, DevSystem Y, int ntile, Ctl *ctl,
-                                                 double *part, int inner_cap, int total_cap) {
-  __shared__ double sh[32];
-  if (ctl->done | ctl->idone) return;
-  const float alpha = float(ctl->alpha);
-  const float *pnew = ctl->parity ? Y.pa32 : Y.pb32;
-  double a1 = 0.0;
-  CG_TILE_LOOP(ntile) {
-    CG_TILE_GEO(S);
-    update_row_scaled(g, valid, Y.x32, pnew, Y.r32, Y.ap32, alpha, a1);
-  }
-  a1 = block_sum(a1, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = a1;
-  if (arrive_last(&ctl->counter)) {
-    const double rz = reduce_partials(part, gridDim.x, sh);  // r.z = r.r (unit diagonal)
-    const double rr = rz;
-    if (threadIdx.x == 0) {
-      ctl->beta = rz / ctl->rpcg;
-      ctl->rpcg = rz;
-      ctl->rsq = rr;
-      const int it = ctl->inner_iter + 1;
-      ctl->inner_iter = it;
-      ctl->iter += 1;
-      if (!isfinite(rr) || !isfinite(ctl->alpha)) {
-        ctl->done = 1;
-        ctl->status = EFDC_XM_NONFINITE;
-      } else if (rr <= ctl->rsq_target || it >= inner_cap || ctl->iter >= total_cap) {
-        ctl->idone = 1;
-      } else {
-        ctl->parity ^= 1;
-      }
-      ctl->counter = 0;
-    }
-  }
+// x += alpha*p, r -= alpha*Ap, r.r (FP64 sums; = r.z on the unit-diagonal
+// system), BETA and the inner stop test.  With no_stop the inner solve runs
+// past its target (kernel timing only).
+__global__ void __launch_bounds__(NT) k_mx_update(DevStatic S, DevSystem Y, Ctl *ctl, Glob *glob,
+                                                 double *part, double total_cap_fac, int no_stop) {
+  struct A {
+    bool skip;
+    float alpha;
+    const float *pnew;
+  };
+  quad_sweep<1>(
+      S, ctl, part,
+      [&](int m) {
+        const Ctl &k = ctl[m];
+        return A{(k.done | k.idone) != 0, float(k.alpha), k.parity ? Y.pa32 : Y.pb32};
+      },
+      [&](const A &a, const RowGeo &g, bool valid, double *v) {
+        update_row_scaled(g, valid, Y.x32, a.pnew, Y.r32, Y.ap32, a.alpha, v[0]);
+      },
+      [&](int m, const double *sum) {
+        if (threadIdx.x != 0) return;
+        Ctl &k = ctl[m];
+        const double rz = sum[0];
+        const int iterm = S.sc[m].iterm;
+        k.beta = rz / k.rpcg;
+        k.rpcg = rz;
+        k.rsq = rz;
+        const int it = k.inner_iter + 1;
+        k.inner_iter = it;
+        k.iter += 1;
+        if (!isfinite(rz) || !isfinite(k.alpha)) {
+          k.status = EFDC_XM_NONFINITE;
+          k.done = 1;
+          atomicAdd(&glob->ndone, 1);
+        } else if (!no_stop && (rz <= k.rsq_target || it >= iterm ||
+                                k.iter >= int(total_cap_fac * iterm) + 50)) {
+          k.idone = 1;
+          atomicAdd(&glob->nidone, 1);
+        } else {
+          k.parity ^= 1;
+        }
+      });
 }
 
 void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {
-  k_mx_matvec<<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
+  k_mx_matvec<<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
   count_launches(1);
 }
 void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
-                      double *part, int inner_cap, int total_cap) {
-  k_mx_update<<<l.grid_up32, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part, inner_cap, total_cap);
+                      Glob *glob, double *part, int no_stop) {
+  k_mx_update<<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, glob, part, 2.0, no_stop);
   count_launches(1);
 }
-void launch_mx_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
-                    double *part, int inner_cap, int total_cap) {
-  k_mx_matvec<<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
-  count_launches(1);
-  k_mx_update<<<l.grid_up32, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part, inner_cap, total_cap);
-  count_launches(1);
+void launch_mx_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl, Glob *glob,
+                    double *part) {
+  launch_mx_matvec(l, S, Y, ctl, part);
+  launch_mx_update(l, S, Y, ctl, glob, part, 0);
 }
 
 int occupancy_blocks_per_sm_mixed_update() {

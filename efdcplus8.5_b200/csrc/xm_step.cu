@@ -4,21 +4,31 @@
 // per-cell arithmetic matches EFDC+ statement by statement; only the order of
 // the global dot products differs (fixed-order tree instead of serial).
 //
-// Each kernel is a grid-stride loop over tiles (one 256-thread CTA processes a
-// whole 32x8 tile per iteration); tile 0 is the ghost tile and is skipped.
+// The cell kernels are grid-stride loops over tiles (one 256-thread CTA
+// processes a whole 32x8 tile per pass; tile 0 is the ghost tile and is
+// skipped).  A tile belongs to one member of the ensemble; the member's
+// scalars come from S.sc[m] and its reductions go to ctl[m].  `act[m]` says
+// whether member m takes part in the current wet/dry sweep (or, for the
+// finalisation kernels, whether its step is to be finalised).
 
 #include "xm_cg.cuh"
 #include "xm_kernels.h"
 
 namespace xm {
 
-#define TILE_LOOP(ntile)                                                      \
-  for (int tile = blockIdx.x + 1; tile < (ntile); tile += gridDim.x)
+#define TILE_LOOP(ntile) for (int tile = blockIdx.x + 1; tile < (ntile); tile += gridDim.x)
+
+#define TILE_MEMBER(S)                  \
+  const int m = (S).tile_member[tile]; \
+  const StepScalars &c = (S).sc[m]
 
 // ---------------------------------------------------------------------------
-// calpuv2c.f90:164-293: switches, explicit transports, time-level advance, FP1
-__global__ void __launch_bounds__(NT) k_begin(DevStatic S, DevState X, StepScalars c, int ntile) {
+// calpuv2c.f90:164-293: switches, explicit transports, FP1.  The host swapped
+// UHDYE<->UHDY1E, VHDXE<->VHDX1E and HP<->H1P before this kernel, so the *1
+// buffers hold the values at entry (the time-level advance :256-264).
+__global__ void __launch_bounds__(NT) k_begin(DevStatic S, DevState X, int ntile) {
   TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
     if (S.kind[d] == LAND) continue;
@@ -32,8 +42,6 @@ __global__ void __launch_bounds__(NT) k_begin(DevStatic S, DevState X, StepScala
       X.wasted[d] = 0;
     }
     const double P = X.p[d];
-    // the host swapped UHDYE<->UHDY1E, VHDXE<->VHDX1E and HP<->H1P before this
-    // step: the *1 buffers hold the values at entry (calpuv2c.f90:256-264)
     const double uhdye = X.uhdy1e[d], vhdxe = X.vhdx1e[d];
     // :214-220
     X.fuhdye[d] = uhdye - c.deltd2 * sub * S.hruo[d] * X.hu[d] * (P - X.p[q.w]) +
@@ -57,58 +65,60 @@ __global__ void __launch_bounds__(NT) k_begin(DevStatic S, DevState X, StepScala
   }
 }
 
+// Start of a sweep: reset the per-member minima, symmetry and re-solve flags.
+__global__ void k_sweep_reset(Ctl *ctl, const int *act, int nmember) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < nmember; m += gridDim.x * blockDim.x) {
+    if (!act[m]) continue;
+    ctl[m].ccmnm_int = 1.e+18;
+    ctl[m].ccmnm_bc = 1.e+18;
+    ctl[m].asym = 0;
+    ctl[m].icordry = 0;
+    ctl[m].counter = 0u;
+  }
+}
+
 // ---------------------------------------------------------------------------
-// calpuv2c.f90:306-344 (FP, CS, CW, CE, CN, CC) and the minimum of CC over
-// the non-open-boundary cells (:360-368; the open-boundary cells' CC is
-// replaced by SETOPENBC and enters through k_obc).
-__global__ void __launch_bounds__(NT) k_assemble(DevStatic S, DevState X, StepScalars c, int ntile,
-                                                Ctl *ctl, double *part) {
+// calpuv2c.f90:306-344 (FP, CS, CW, CE, CN, CC) and the member's minimum of
+// CC over its non-open-boundary cells (:360-368; the open-boundary cells' CC
+// is replaced by SETOPENBC and enters through k_obc_*).  CC > 0 here.
+__global__ void __launch_bounds__(NT) k_assemble(DevStatic S, DevState X, int ntile, Ctl *ctl,
+                                                const int *act) {
   __shared__ double sh[32];
-  double mn = 1.e+18;
   TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    if (!act[m]) continue;
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
     const uint8_t kd = S.kind[d];
-    if (kd == LAND) continue;
-    double C1 = 0.5 * c.g;
-    const double sub = X.sub[d], svb = X.svb[d], sube = X.sub[q.e], svbn = X.svb[q.n];
-    X.fp[d] = X.fp1[d] - C1 * (sube * X.fuhdye[q.e] - sub * X.fuhdye[d] +
-                               svbn * X.fvhdxe[q.n] - svb * X.fvhdxe[d] - 2.0 * X.qsume[d]);
-    C1 = -0.5 * c.deltd2 * c.g;
-    const double cs = C1 * svb * S.hrvo[d] * S.rcx[d] * X.hv[d];
-    const double cw = C1 * sub * S.hruo[d] * S.rcx[d] * X.hu[d];
-    const double ce = C1 * sube * S.hruo[q.e] * S.rcx[q.e] * X.hu[q.e];
-    const double cn = C1 * svbn * S.hrvo[q.n] * S.rcx[q.n] * X.hv[q.n];
-    const double cc = c.delti * S.dxyp[d] - cs - cw - ce - cn;
-    X.cs[d] = cs;
-    X.cw[d] = cw;
-    X.ce[d] = ce;
-    X.cn[d] = cn;
-    X.cc[d] = cc;
-    if (kd == WATER) mn = fmin(mn, cc);
-  }
-  mn = block_min(mn, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = mn;
-  if (arrive_last(&ctl->counter)) {
-    double m = 1.e+18;
-    for (int i = threadIdx.x; i < gridDim.x; i += NT) m = fmin(m, __ldcg(&part[i]));
-    m = block_min(m, sh);
-    if (threadIdx.x == 0) {
-      ctl->ccmnm_int = m;
-      ctl->ccmnm_bc = 1.e+18;
-      ctl->asym = 0;
-      ctl->counter = 0;
+    double mn = 1.e+18;
+    if (kd != LAND) {
+      double C1 = 0.5 * c.g;
+      const double sub = X.sub[d], svb = X.svb[d], sube = X.sub[q.e], svbn = X.svb[q.n];
+      X.fp[d] = X.fp1[d] - C1 * (sube * X.fuhdye[q.e] - sub * X.fuhdye[d] +
+                                 svbn * X.fvhdxe[q.n] - svb * X.fvhdxe[d] - 2.0 * X.qsume[d]);
+      C1 = -0.5 * c.deltd2 * c.g;
+      const double cs = C1 * svb * S.hrvo[d] * S.rcx[d] * X.hv[d];
+      const double cw = C1 * sub * S.hruo[d] * S.rcx[d] * X.hu[d];
+      const double ce = C1 * sube * S.hruo[q.e] * S.rcx[q.e] * X.hu[q.e];
+      const double cn = C1 * svbn * S.hrvo[q.n] * S.rcx[q.n] * X.hv[q.n];
+      const double cc = c.delti * S.dxyp[d] - cs - cw - ce - cn;
+      X.cs[d] = cs;
+      X.cw[d] = cw;
+      X.ce[d] = ce;
+      X.cn[d] = cn;
+      X.cc[d] = cc;
+      if (kd == WATER) mn = cc;
     }
+    mn = block_min(mn, sh);
+    if (threadIdx.x == 0 && mn < 1.e+18) atomic_min_nonneg(&ctl[m].ccmnm_int, mn);
   }
 }
 
 // ---------------------------------------------------------------------------
 // SETOPENBC (setopenbc.f90:22-206) + SETOPENBC2 (setopenbc2.f90:17-46) for one
-// boundary cell k.  Returns CC of the cell.  `apply` updates the interior
-// neighbour's FP and coupling; the parallel kernel uses it only when the host
-// proved every target unique and not itself a boundary cell.
+// boundary cell k.  Returns CC of the cell.
 __device__ __forceinline__ double obc_cell(const DevStatic &S, const DevState &X,
-                                           const DevObc &B, const StepScalars &c, int k) {
+                                           const DevObc &B, const StepScalars &c, int k, int mt) {
   const int d = B.slot[k], nb = B.nbr[k], side = B.side[k], ispb = B.ispb[k];
   const double D = c.deltd2, G = c.g, HDRY2 = 0.2 * c.hdry;
   X.cc[d] = c.delti * S.dxyp[d];
@@ -118,9 +128,9 @@ __device__ __forceinline__ double obc_cell(const DevStatic &S, const DevState &X
   X.cn[d] = 0.;
   if (!X.lopenbcdry[d]) {
     double fp = B.pser ? B.pser[k] : 0.0;
-    for (int m = 0; m < B.mtide; ++m) {
-      const double TC = c.cosv[m], TS = c.sinv[m];
-      fp = fp + B.pcb[k * B.mtide + m] * TC + B.psb[k * B.mtide + m] * TS;
+    for (int t = 0; t < mt; ++t) {
+      const double TC = c.cosv[t], TS = c.sinv[t];
+      fp = fp + B.pcb[k * B.mtmax + t] * TC + B.psb[k * B.mtmax + t] * TS;
     }
     if (ispb == 1 || ispb == 2) {  // radiation
       if (side == 0) {  // W, face at LEC(L)
@@ -186,266 +196,77 @@ __device__ __forceinline__ void obc2_cell(const DevState &X, const DevObc &B, in
 // Boundary cells in parallel, one thread each (hazard-free layouts only: no
 // two cells share an interior target and no target is a boundary cell, so
 // SETOPENBC's and SETOPENBC2's writes to the targets commute).  The minimum
-// CC of the boundary cells goes to ctl->ccmnm_bc by an atomic min on the bit
-// pattern, which orders non-negative doubles like their values (CC >= 0 here).
-__global__ void __launch_bounds__(NT) k_obc_parallel(DevStatic S, DevState X, DevObc B,
-                                                    StepScalars c, Ctl *ctl) {
-  __shared__ double sh[32];
-  double mn = 1.e+18;
+// CC of each member's boundary cells goes to ctl[m].ccmnm_bc (atomic min).
+__global__ void __launch_bounds__(NT) k_obc_parallel(DevStatic S, DevState X, DevObc B, Ctl *ctl,
+                                                    const int *act) {
   const int k = blockIdx.x * NT + threadIdx.x;
-  if (k < B.n) {
-    mn = obc_cell(S, X, B, c, k);
-    obc2_cell(X, B, k);
-  }
-  mn = block_min(mn, sh);
-  if (threadIdx.x == 0)
-    atomicMin(reinterpret_cast<unsigned long long *>(&ctl->ccmnm_bc),
-              static_cast<unsigned long long>(__double_as_longlong(fmax(mn, 0.0))));
+  if (k >= B.n) return;
+  const int m = B.member[k];
+  if (!act[m]) return;
+  const double cc = obc_cell(S, X, B, S.sc[m], k, B.mtide[m]);
+  obc2_cell(X, B, k);
+  atomic_min_nonneg(&ctl[m].ccmnm_bc, cc);
 }
 
 // One thread, the reference's exact loop order (layouts where boundary cells
 // share or are each other's interior neighbours).
-__global__ void k_obc_serial(DevStatic S, DevState X, DevObc B, StepScalars c, Ctl *ctl) {
+__global__ void k_obc_serial(DevStatic S, DevState X, DevObc B, Ctl *ctl, const int *act) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double mn = 1.e+18;
-  for (int k = 0; k < B.n; ++k) mn = fmin(mn, obc_cell(S, X, B, c, k));
-  for (int k = 0; k < B.n; ++k) obc2_cell(X, B, k);
-  ctl->ccmnm_bc = mn;
+  for (int k = 0; k < B.n; ++k) {
+    const int m = B.member[k];
+    if (!act[m]) continue;
+    const double cc = obc_cell(S, X, B, S.sc[m], k, B.mtide[m]);
+    ctl[m].ccmnm_bc = fmin(ctl[m].ccmnm_bc, cc);
+  }
+  for (int k = 0; k < B.n; ++k)
+    if (act[B.member[k]]) obc2_cell(X, B, k);
 }
 
-// calpuv2c.f90:150-157: LOPENBCDRY=.FALSE. on the open-boundary cells
-__global__ void k_obc_reset(DevObc B, DevState X) {
+// calpuv2c.f90:150-157: LOPENBCDRY=.FALSE. on the open-boundary cells (ISDRY>0)
+__global__ void k_obc_reset(DevStatic S, DevObc B, DevState X) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B.n; k += gridDim.x * blockDim.x)
-    X.lopenbcdry[B.slot[k]] = 0;
+    if (S.sc[B.member[k]].isdry > 0) X.lopenbcdry[B.slot[k]] = 0;
 }
 
 // ---------------------------------------------------------------------------
-// calpuv2c.f90:371-399: scale by the minimum diagonal; FP32 copies for MIXED.
-// Also flags an unsymmetric operator (CE(L) /= CW(LE) or CN(L) /= CS(LN)),
-// which only a radiation boundary with a closed interior face produces.
+// calpuv2c.f90:371-399: scale by the member's minimum diagonal.  Also flags an
+// unsymmetric operator (CE(L) /= CW(LE) or CN(L) /= CS(LN)), which only a
+// radiation boundary with a closed interior face produces.
 __global__ void __launch_bounds__(NT) k_scale(DevStatic S, DevState X, DevSystem Y, int ntile,
-                                             Ctl *ctl, int write_cross) {
-  const double CCMNM = fmin(ctl->ccmnm_int, ctl->ccmnm_bc);
-  const double CCMNMI = 1. / CCMNM;
-  bool asym = false;
+                                             Ctl *ctl, const int *act, int write_cross) {
   TILE_LOOP(ntile) {
+    const int m = S.tile_member[tile];
+    if (!act[m]) continue;
+    const double CCMNM = fmin(ctl[m].ccmnm_int, ctl[m].ccmnm_bc);
+    const double CCMNMI = 1. / CCMNM;
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
-    if (S.kind[d] == LAND) continue;
-    const double cs = X.cs[d], cw = X.cw[d], ce = X.ce[d], cn = X.cn[d];
-    asym |= (ce != X.cw[q.e]) || (cn != X.cs[q.n]);
-    const double ccs = cs * CCMNMI, ccw = cw * CCMNMI, cce = ce * CCMNMI,
-                 ccn = cn * CCMNMI, ccc = X.cc[d] * CCMNMI;
-    const double fpt = X.fp[d] * CCMNMI;
-    Y.ccs[d] = ccs;
-    Y.ccw[d] = ccw;
-    Y.ccc[d] = ccc;
-    Y.fptmp[d] = fpt;
-    if (write_cross) {
-      Y.cce[d] = cce;
-      Y.ccn[d] = ccn;
-    }
-  }
-  // an unsymmetric operator without the cross coefficients written cannot be
-  // solved: flag it (status 2) so that the host reports it
-  if (__syncthreads_or(asym) && threadIdx.x == 0) atomicOr(&ctl->asym, write_cross ? 1 : 3);
-}
-
-// ---------------------------------------------------------------------------
-// CONGRAD in FP64 (congrad.f90:54-187).  Vectors: P (the state array), r,
-// p double-buffered (pa/pb, selected by ctl->parity), Ap.  z = CCCI*r with
-// CCCI = 1./CCC is recomputed where needed instead of stored.
-
-// :54-88 initial residual, z0 = CCCI*r, RPCG.
-__global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double *P, int ntile,
-                                               Ctl *ctl, double *part) {
-  __shared__ double sh[32];
-  const bool asym = ctl->asym;
-  double acc = 0.0;
-  CG_TILE_LOOP(ntile) {
-    CG_TILE_GEO(S);
-    const V4<double> r = residual_row(g, S.kind, P, Y, asym);
-    const V4<double> c = ld4(Y.ccc + g.d0);
-    const V4<double> z = {r.x * rcpT(c.x), r.y * rcpT(c.y), r.z * rcpT(c.z), r.w * rcpT(c.w)};
-    if (valid) {
-      st4(Y.r + g.d0, r);
-      st4(Y.pa + g.d0, z);
-      acc += r.x * z.x + r.y * z.y + r.z * z.z + r.w * z.w;
-    }
-  }
-  acc = block_sum(acc, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = acc;
-  if (arrive_last(&ctl->counter)) {
-    const double rpcg = reduce_partials(part, gridDim.x, sh);
-    if (threadIdx.x == 0) {
-      ctl->rpcg = rpcg;
-      ctl->beta = 0.0;
-      ctl->parity = 0;
-      ctl->iter = 0;
-      ctl->rsq = 0.0;
-      ctl->status = 0;
-      ctl->done = (rpcg == 0.0) ? 1 : 0;  // :88 RETURN
-      if (!isfinite(rpcg)) {
-        ctl->done = 1;
-        ctl->status = EFDC_XM_NONFINITE;
+    bool asym = false;
+    if (S.kind[d] != LAND) {
+      const double cs = X.cs[d], cw = X.cw[d], ce = X.ce[d], cn = X.cn[d];
+      asym = (ce != X.cw[q.e]) || (cn != X.cs[q.n]);
+      Y.ccs[d] = cs * CCMNMI;
+      Y.ccw[d] = cw * CCMNMI;
+      Y.ccc[d] = X.cc[d] * CCMNMI;
+      Y.fptmp[d] = X.fp[d] * CCMNMI;
+      if (write_cross) {
+        Y.cce[d] = ce * CCMNMI;
+        Y.ccn[d] = cn * CCMNMI;
       }
-      ctl->counter = 0;
     }
+    // unsymmetric without the cross coefficients written cannot be solved:
+    // flag it (bit 2) so that the host reports it
+    if (__syncthreads_or(asym) && threadIdx.x == 0) atomicOr(&ctl[m].asym, write_cross ? 1 : 3);
   }
 }
 
-// :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA).
-__global__ void __launch_bounds__(NT) k_cg_matvec(DevStatic S, DevSystem Y, int ntile, Ctl *ctl,
-                                                 double *part) {
-  __shared__ double sh[32];
-  if (ctl->done) return;
-  const double beta = ctl->beta;
-  const bool par = ctl->parity;
-  const double *pold = par ? Y.pb : Y.pa;
-  double *pnew = par ? Y.pa : Y.pb;
-  const bool asym = ctl->asym;
-  double acc = 0.0;
-  CG_TILE_LOOP(ntile) {
-    CG_TILE_GEO(S);
-    acc += matvec_row<double>(g, valid, Y.r, Y.ccc, pold, pnew, Y.ccs, Y.ccw, Y.cce, Y.ccn, Y.ap,
-                              beta, asym);
-  }
-  acc = block_sum(acc, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = acc;
-  if (arrive_last(&ctl->counter)) {
-    const double papcg = reduce_partials(part, gridDim.x, sh);
-    if (threadIdx.x == 0) {
-      ctl->papcg = papcg;
-      ctl->alpha = ctl->rpcg / papcg;  // :124
-      ctl->counter = 0;
-    }
-  }
-}
-
-// :127-149 (P, RCG update, RPCGN, RSQ, BETA) and the stop test :165.
-__global__ void __launch_bounds__(NT) k_cg_update(DevStatic S, DevSystem Y, double *P, int ntile,
-                                                 Ctl *ctl, double *part, double rsqm, int iterm) {
-  __shared__ double sh[32];
-  if (ctl->done) return;
-  const double alpha = ctl->alpha;
-  const double *pnew = ctl->parity ? Y.pa : Y.pb;
-  double a1 = 0.0, a2 = 0.0;
-  CG_TILE_LOOP(ntile) {
-    CG_TILE_GEO(S);
-    update_row<double>(g, valid, P, pnew, Y.r, Y.ap, Y.ccc, alpha, a1, a2);
-  }
-  a1 = block_sum(a1, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = a1;
-  a2 = block_sum(a2, sh);
-  if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = a2;
-  if (arrive_last(&ctl->counter)) {
-    const double rpcgn = reduce_partials(part, gridDim.x, sh);
-    const double rsq = reduce_partials(part + gridDim.x, gridDim.x, sh);
-    if (threadIdx.x == 0) {
-      const double beta = rpcgn / ctl->rpcg;
-      ctl->beta = beta;
-      ctl->rpcg = rpcgn;
-      ctl->rsq = rsq;
-      const int it = ctl->iter + 1;
-      ctl->iter = it;
-      if (!isfinite(rsq) || !isfinite(ctl->alpha)) {
-        ctl->done = 1;
-        ctl->status = EFDC_XM_NONFINITE;
-      } else if (rsq <= rsqm) {
-        ctl->done = 1;
-      } else if (it >= iterm) {
-        ctl->done = 1;
-        ctl->status = EFDC_XM_CG_MAXITER;
-      } else {
-        ctl->parity ^= 1;
-      }
-      ctl->counter = 0;
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// MIXED outer step: r = b - A*P in FP64 (the FP64 refinement residual),
-// RSQ in FP64, and the FP32 inner system r32, z32 = r32/CCC, x32 = 0.
-__global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, DevSystem Y, const double *P,
-                                                int ntile, Ctl *ctl, double *part, double rsqm,
-                                                double rel_tol) {
-  __shared__ double sh[32];
-  const bool asym = ctl->asym;
-  double a1 = 0.0, a2 = 0.0;
-  CG_TILE_LOOP(ntile) {
-    CG_TILE_GEO(S);
-    const V4<double> r = residual_row(g, S.kind, P, Y, asym);
-    const V4<double> c = ld4(Y.ccc + g.d0);
-    // scaled residual rhat = D^-1/2 r of the Jacobi-scaled inner system
-    const V4<float> r32 = {float(r.x / sqrt(c.x)), float(r.y / sqrt(c.y)), float(r.z / sqrt(c.z)),
-                           float(r.w / sqrt(c.w))};
-    if (valid) {
-      st4(Y.r32 + g.d0, r32);
-      st4(Y.pa32 + g.d0, r32);
-      st4(Y.x32 + g.d0, V4<float>{0.f, 0.f, 0.f, 0.f});
-      a1 += r.x * r.x + r.y * r.y + r.z * r.z + r.w * r.w;
-      a2 += double(r32.x) * double(r32.x) + double(r32.y) * double(r32.y) +
-            double(r32.z) * double(r32.z) + double(r32.w) * double(r32.w);
-    }
-  }
-  a1 = block_sum(a1, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = a1;
-  a2 = block_sum(a2, sh);
-  if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = a2;
-  if (arrive_last(&ctl->counter)) {
-    const double rsq = reduce_partials(part, gridDim.x, sh);
-    const double rz = reduce_partials(part + gridDim.x, gridDim.x, sh);
-    if (threadIdx.x == 0) {
-      ctl->rsq64 = rsq;
-      ctl->rsq = rsq;
-      ctl->rpcg = rz;
-      ctl->beta = 0.0;
-      ctl->parity = 0;
-      ctl->inner_iter = 0;
-      ctl->idone = 0;
-      ctl->outer += 1;
-      // inner stop on the scaled residual: reduce it by the factor the FP64
-      // residual needs to reach 0.1*RSQM, and by at least rel_tol (in norm)
-      const double need = (rsq > 0.0) ? 0.1 * rsqm / rsq : 1.0;
-      ctl->rsq_target = rz * fmax(fmin(need, 1.0), rel_tol * rel_tol);
-      if (!isfinite(rsq)) {
-        ctl->done = 1;
-        ctl->status = EFDC_XM_NONFINITE;
-      } else if (rsq <= rsqm || rz == 0.0) {
-        ctl->done = 1;
-      } else {
-        ctl->done = 0;
-      }
-      ctl->counter = 0;
-    }
-  }
-}
-
-// MIXED: P += D^-1/2 x32 (the FP32 correction of the scaled system).
-__global__ void __launch_bounds__(NT) k_mx_apply(DevStatic S, DevSystem Y, double *P, int ntile) {
-  CG_TILE_LOOP(ntile) {
-    CG_TILE_GEO(S);
-    if (!valid) continue;
-    V4<double> x = ld4(P + g.d0);
-    const V4<double> c = ld4(Y.ccc + g.d0);
-    const V4<float> d = ld4(Y.x32 + g.d0);
-    // P += D^-1/2 xhat
-    x.x = x.x + double(d.x) / sqrt(c.x);
-    x.y = x.y + double(d.y) / sqrt(c.y);
-    x.z = x.z + double(d.z) / sqrt(c.z);
-    x.w = x.w + double(d.w) / sqrt(c.w);
-    st4(P + g.d0, x);
-  }
-}
-
-// ---------------------------------------------------------------------------
 // MIXED: the FP32 inner operator Ahat = D^-1/2 A D^-1/2 with D = CCC (unit
 // diagonal): AS(L) = CCS(L)/sqrt(CCC(L)*CCC(LS)), AW likewise; AE, AN only
 // when the operator can be unsymmetric (else AE(L)=AW(LE), AN(L)=AS(LN)).
 __global__ void __launch_bounds__(NT) k_scale32(DevStatic S, DevSystem Y, int ntile,
-                                               int write_cross) {
+                                               const int *act, int write_cross) {
   TILE_LOOP(ntile) {
+    if (act && !act[S.tile_member[tile]]) continue;
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
     if (S.kind[d] == LAND) continue;
@@ -459,9 +280,232 @@ __global__ void __launch_bounds__(NT) k_scale32(DevStatic S, DevSystem Y, int nt
   }
 }
 
-// Standalone CONGRAD: a caller-assembled scaled system.  Land slots are made
-// inert (CCC=1, couplings 0, b=0), FP32 copies made for MIXED, and the
-// symmetry of the given CCE/CCN against CCW(LE)/CCS(LN) is recorded.
+// ---------------------------------------------------------------------------
+// Start of a solve: members not in this sweep are finished from the start.
+__global__ void k_solve_reset(Ctl *ctl, Glob *glob, const int *act, int nmember) {
+  __shared__ int ninact;
+  if (threadIdx.x == 0) ninact = 0;
+  __syncthreads();
+  for (int m = threadIdx.x; m < nmember; m += blockDim.x) {
+    Ctl &k = ctl[m];
+    k.done = act[m] ? 0 : 1;
+    if (!act[m]) atomicAdd(&ninact, 1);
+    k.idone = 0;
+    k.iter = 0;
+    k.inner_iter = 0;
+    k.outer = 0;
+    k.status = 0;
+    k.parity = 0;
+    k.beta = 0.0;
+    k.counter = 0u;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    glob->ndone = ninact;
+    glob->nidone = 0;
+  }
+}
+
+// MIXED: start of an outer pass
+__global__ void k_outer_reset(Glob *glob) { glob->nidone = 0; }
+
+// CONGRAD in FP64 (congrad.f90:54-187).  Vectors: P (the state array), r,
+// p double-buffered (pa/pb, selected by ctl[m].parity), Ap.  z = CCCI*r with
+// CCCI = 1./CCC is recomputed where needed instead of stored.
+
+// :54-88 initial residual, z0 = CCCI*r, RPCG.
+__global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double *P, Ctl *ctl,
+                                               Glob *glob, double *part) {
+  struct A {
+    bool skip, asym;
+  };
+  quad_sweep<1>(
+      S, ctl, part, [&](int m) { return A{ctl[m].done != 0, ctl[m].asym != 0}; },
+      [&](const A &a, const RowGeo &g, bool valid, double *v) {
+        const V4<double> r = residual_row(g, S.kind, P, Y, a.asym);
+        const V4<double> c = ld4(Y.ccc + g.d0);
+        const V4<double> z = {r.x * rcpT(c.x), r.y * rcpT(c.y), r.z * rcpT(c.z),
+                              r.w * rcpT(c.w)};
+        if (valid) {
+          st4(Y.r + g.d0, r);
+          st4(Y.pa + g.d0, z);
+          v[0] = r.x * z.x + r.y * z.y + r.z * z.z + r.w * z.w;
+        }
+      },
+      [&](int m, const double *sum) {
+        if (threadIdx.x != 0) return;
+        Ctl &k = ctl[m];
+        const double rpcg = sum[0];
+        k.rpcg = rpcg;
+        k.beta = 0.0;
+        k.parity = 0;
+        k.iter = 0;
+        k.rsq = 0.0;
+        k.status = 0;
+        if (rpcg == 0.0 || !isfinite(rpcg)) {  // :88 RETURN
+          if (!isfinite(rpcg)) k.status = EFDC_XM_NONFINITE;
+          k.done = 1;
+          atomicAdd(&glob->ndone, 1);
+        }
+      });
+}
+
+// :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA).
+__global__ void __launch_bounds__(NT) k_cg_matvec(DevStatic S, DevSystem Y, Ctl *ctl,
+                                                 double *part) {
+  struct A {
+    bool skip, asym;
+    double beta;
+    const double *pold;
+    double *pnew;
+  };
+  quad_sweep<1>(
+      S, ctl, part,
+      [&](int m) {
+        const Ctl &k = ctl[m];
+        const bool par = k.parity;
+        return A{k.done != 0, k.asym != 0, k.beta, par ? Y.pb : Y.pa, par ? Y.pa : Y.pb};
+      },
+      [&](const A &a, const RowGeo &g, bool valid, double *v) {
+        v[0] = matvec_row<double>(g, valid, Y.r, Y.ccc, a.pold, a.pnew, Y.ccs, Y.ccw, Y.cce, Y.ccn,
+                                  Y.ap, a.beta, a.asym);
+      },
+      [&](int m, const double *sum) {
+        if (threadIdx.x != 0) return;
+        ctl[m].papcg = sum[0];
+        ctl[m].alpha = ctl[m].rpcg / sum[0];  // :124
+      });
+}
+
+// :127-149 (P, RCG update, RPCGN, RSQ, BETA) and the stop test :165.  With
+// no_stop the iteration continues past RSQM and ITERM (kernel timing only).
+__global__ void __launch_bounds__(NT, 5) k_cg_update(DevStatic S, DevSystem Y, double *P, Ctl *ctl,
+                                                 Glob *glob, double *part, int no_stop) {
+  struct A {
+    bool skip;
+    double alpha;
+    const double *pnew;
+  };
+  quad_sweep<2>(
+      S, ctl, part,
+      [&](int m) {
+        const Ctl &k = ctl[m];
+        return A{k.done != 0, k.alpha, k.parity ? Y.pa : Y.pb};
+      },
+      [&](const A &a, const RowGeo &g, bool valid, double *v) {
+        update_row<double>(g, valid, P, a.pnew, Y.r, Y.ap, Y.ccc, a.alpha, v[0], v[1]);
+      },
+      [&](int m, const double *sum) {
+        if (threadIdx.x != 0) return;
+        Ctl &k = ctl[m];
+        const StepScalars &c = S.sc[m];
+        const double rpcgn = sum[0], rsq = sum[1];
+        k.beta = rpcgn / k.rpcg;
+        k.rpcg = rpcgn;
+        k.rsq = rsq;
+        const int it = k.iter + 1;
+        k.iter = it;
+        int fin = 0;
+        if (!isfinite(rsq) || !isfinite(k.alpha)) {
+          k.status = EFDC_XM_NONFINITE;
+          fin = 1;
+        } else if (!no_stop && rsq <= c.rsqm) {
+          fin = 1;
+        } else if (!no_stop && it >= c.iterm) {
+          k.status = EFDC_XM_CG_MAXITER;
+          fin = 1;
+        } else {
+          k.parity ^= 1;
+        }
+        if (fin) {
+          k.done = 1;
+          atomicAdd(&glob->ndone, 1);
+        }
+      });
+}
+
+// ---------------------------------------------------------------------------
+// MIXED outer step: r = b - A*P in FP64 (the FP64 refinement residual), RSQ
+// in FP64, and the FP32 scaled inner system rhat = D^-1/2 r, p0 = rhat,
+// x = 0.  rsqm_fac scales the member's RSQM (the MIXED stop, below RSQM).
+__global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, DevSystem Y, const double *P,
+                                                Ctl *ctl, Glob *glob, double *part,
+                                                double rsqm_fac, double rel_tol, int no_stop) {
+  struct A {
+    bool skip, asym;
+  };
+  quad_sweep<2>(
+      S, ctl, part, [&](int m) { return A{ctl[m].done != 0, ctl[m].asym != 0}; },
+      [&](const A &a, const RowGeo &g, bool valid, double *v) {
+        const V4<double> r = residual_row(g, S.kind, P, Y, a.asym);
+        const V4<double> c = ld4(Y.ccc + g.d0);
+        const V4<float> r32 = {float(r.x / sqrt(c.x)), float(r.y / sqrt(c.y)),
+                               float(r.z / sqrt(c.z)), float(r.w / sqrt(c.w))};
+        if (valid) {
+          st4(Y.r32 + g.d0, r32);
+          st4(Y.pa32 + g.d0, r32);
+          st4(Y.x32 + g.d0, V4<float>{0.f, 0.f, 0.f, 0.f});
+          v[0] = r.x * r.x + r.y * r.y + r.z * r.z + r.w * r.w;
+          v[1] = double(r32.x) * double(r32.x) + double(r32.y) * double(r32.y) +
+                 double(r32.z) * double(r32.z) + double(r32.w) * double(r32.w);
+        }
+      },
+      [&](int m, const double *sum) {
+        if (threadIdx.x != 0) return;
+        Ctl &k = ctl[m];
+        const double rsq = sum[0], rz = sum[1];
+        const double rsqm = S.sc[m].rsqm * rsqm_fac;
+        k.rsq64 = rsq;
+        k.rsq = rsq;
+        k.rpcg = rz;
+        k.beta = 0.0;
+        k.parity = 0;
+        k.inner_iter = 0;
+        k.idone = 0;
+        k.outer += 1;
+        // inner stop on the scaled residual: reduce it by the factor the FP64
+        // residual needs to reach 0.1*RSQM, and by at least rel_tol (in norm)
+        const double need = (rsq > 0.0) ? 0.1 * rsqm / rsq : 1.0;
+        k.rsq_target = rz * fmax(fmin(need, 1.0), rel_tol * rel_tol);
+        int fin = 0;
+        if (!isfinite(rsq)) {
+          k.status = EFDC_XM_NONFINITE;
+          fin = 1;
+        } else if (!no_stop && (rsq <= rsqm || rz == 0.0)) {
+          fin = 1;
+        } else if (!no_stop && k.iter >= 2 * S.sc[m].iterm + 50) {
+          k.status = EFDC_XM_CG_MAXITER;  // inner iterations of all passes exhausted
+          fin = 1;
+        }
+        if (fin) {
+          k.done = 1;
+          atomicAdd(&glob->ndone, 1);
+        }
+      });
+}
+
+// MIXED: P += D^-1/2 x32 (the FP32 correction of the scaled system) for the
+// members whose inner solve finished.
+__global__ void __launch_bounds__(NT) k_mx_apply(DevStatic S, DevSystem Y, double *P,
+                                                const Ctl *ctl) {
+  quad_apply(
+      S, [&](int m) { return ctl[m].done || !ctl[m].idone; },
+      [&](int, const RowGeo &g) {
+        V4<double> x = ld4(P + g.d0);
+        const V4<double> c = ld4(Y.ccc + g.d0);
+        const V4<float> d = ld4(Y.x32 + g.d0);
+        x.x = x.x + double(d.x) / sqrt(c.x);
+        x.y = x.y + double(d.y) / sqrt(c.y);
+        x.z = x.z + double(d.z) / sqrt(c.z);
+        x.w = x.w + double(d.w) / sqrt(c.w);
+        st4(P + g.d0, x);
+      });
+}
+
+// ---------------------------------------------------------------------------
+// Standalone CONGRAD: a caller-assembled scaled system (one member).  Land
+// slots are made inert (CCC=1, couplings 0, b=0), and the symmetry of the
+// given CCE/CCN against CCW(LE)/CCS(LN) is recorded.
 __global__ void __launch_bounds__(NT) k_sys_prepare(DevStatic S, DevSystem Y, int ntile, Ctl *ctl) {
   bool asym = false;
   TILE_LOOP(ntile) {
@@ -478,13 +522,16 @@ __global__ void __launch_bounds__(NT) k_sys_prepare(DevStatic S, DevSystem Y, in
     const double ccs_n = (S.kind[q.n] == LAND) ? 0.0 : Y.ccs[q.n];
     asym |= (cce != ccw_e) || (ccn != ccs_n);
   }
-  if (__syncthreads_or(asym) && threadIdx.x == 0) atomicOr(&ctl->asym, 1);
+  if (__syncthreads_or(asym) && threadIdx.x == 0) atomicOr(&ctl[0].asym, 1);
 }
 
 // ---------------------------------------------------------------------------
 // calpuv2c.f90:416-437 face discharges and unit-width discharges.
-__global__ void __launch_bounds__(NT) k_backsub(DevStatic S, DevState X, StepScalars c, int ntile) {
+__global__ void __launch_bounds__(NT) k_backsub(DevStatic S, DevState X, int ntile,
+                                               const int *act) {
   TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    if (!act[m]) continue;
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
     if (S.kind[d] == LAND) continue;
@@ -501,9 +548,11 @@ __global__ void __launch_bounds__(NT) k_backsub(DevStatic S, DevState X, StepSca
 }
 
 // calpuv2c.f90:466-486 continuity.
-__global__ void __launch_bounds__(NT) k_continuity(DevStatic S, DevState X, StepScalars c,
-                                                  int ntile) {
+__global__ void __launch_bounds__(NT) k_continuity(DevStatic S, DevState X, int ntile,
+                                                  const int *act) {
   TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    if (!act[m]) continue;
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
     if (S.kind[d] == LAND) continue;
@@ -517,8 +566,11 @@ __global__ void __launch_bounds__(NT) k_continuity(DevStatic S, DevState X, Step
 
 // calpuv2c.f90:489-535 depths of the open-boundary cells (+ drying of a
 // boundary cell).  Concurrent zero-writes to shared faces are benign.
-__global__ void k_obc_hp(DevStatic S, DevState X, DevObc B, StepScalars c) {
+__global__ void k_obc_hp(DevStatic S, DevState X, DevObc B, const int *act) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B.n; k += gridDim.x * blockDim.x) {
+    const int m = B.member[k];
+    if (!act[m]) continue;
+    const StepScalars &c = S.sc[m];
     const int d = B.slot[k];
     double hp = c.gi * X.p[d] - S.belv[d];
     if (c.isdry > 0) {
@@ -555,34 +607,38 @@ __global__ void k_obc_hp(DevStatic S, DevState X, DevObc B, StepScalars c) {
 }
 
 // ---------------------------------------------------------------------------
-// ISDRY>0: P = G*(HP+BELV) (:560-570) fused with the legacy drying check,
-// ISDRY 1..97 (:574-603).  All face writes are zeros, so the order of the
-// reference's serial loop does not matter.
-__global__ void __launch_bounds__(NT) k_wd_legacy(DevStatic S, DevState X, StepScalars c,
-                                                 int ntile, Ctl *ctl, int check) {
-  bool flag = false;
+// ISDRY>0 and /= 99: P = G*(HP+BELV) (:560-570) fused with the legacy drying
+// check of ISDRY 1..97 (:574-603).  All face writes are zeros, so the order
+// of the reference's serial loop does not matter.
+__global__ void __launch_bounds__(NT) k_wd_legacy(DevStatic S, DevState X, int ntile, Ctl *ctl,
+                                                 const int *act) {
   TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    if (!act[m] || c.isdry <= 0 || c.isdry == 99) continue;
+    const bool check = c.isdry < 98;
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
-    if (S.kind[d] == LAND) continue;
-    const double hp = X.hp[d];
-    X.p[d] = c.g * (hp + S.belv[d]);
-    if (check && hp <= c.hdry) {
-      if (X.iscdry[d] == 0) {
-        X.iscdry[d] = 1;
-        flag = true;
+    bool flag = false;
+    if (S.kind[d] != LAND) {
+      const double hp = X.hp[d];
+      X.p[d] = c.g * (hp + S.belv[d]);
+      if (check && hp <= c.hdry) {
+        if (X.iscdry[d] == 0) {
+          X.iscdry[d] = 1;
+          flag = true;
+        }
+        X.sub[d] = 0.;
+        X.svb[d] = 0.;
+        X.sub[q.e] = 0.;
+        X.svb[q.n] = 0.;
+        X.sbx[d] = 0.;
+        X.sby[d] = 0.;
+        X.sbx[q.e] = 0.;
+        X.sby[q.n] = 0.;
       }
-      X.sub[d] = 0.;
-      X.svb[d] = 0.;
-      X.sub[q.e] = 0.;
-      X.svb[q.n] = 0.;
-      X.sbx[d] = 0.;
-      X.sby[d] = 0.;
-      X.sbx[q.e] = 0.;
-      X.sby[q.n] = 0.;
     }
+    if (__syncthreads_or(flag) && threadIdx.x == 0) atomicOr(&ctl[m].icordry, 1);
   }
-  if (__syncthreads_or(flag) && threadIdx.x == 0) atomicOr(&ctl->icordry, 1);
 }
 
 // ISDRY=99 (:606-734), pass 1: P update and each cell's decision, from
@@ -591,10 +647,12 @@ __global__ void __launch_bounds__(NT) k_wd_legacy(DevStatic S, DevState X, StepS
 // branches (rising too slowly, or drying).
 enum : int { WD_ACT = 1, WD_FAST = 2, WD_RW = 4, WD_RE = 8, WD_RS = 16, WD_RN = 32, WD_SLOW = 64 };
 
-__global__ void __launch_bounds__(NT) k_wd99_decide(DevStatic S, DevState X, StepScalars c,
-                                                   int ntile) {
-  const double HDRY = c.hdry, HDRY2 = 2. * HDRY, HDRY90 = 0.9 * HDRY;
+__global__ void __launch_bounds__(NT) k_wd99_decide(DevStatic S, DevState X, int ntile,
+                                                   const int *act) {
   TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    if (!act[m] || c.isdry != 99) continue;
+    const double HDRY = c.hdry, HDRY2 = 2. * HDRY, HDRY90 = 0.9 * HDRY;
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
     if (S.kind[d] == LAND) {
@@ -603,97 +661,104 @@ __global__ void __launch_bounds__(NT) k_wd99_decide(DevStatic S, DevState X, Ste
     }
     const double hp = X.hp[d], h1p = X.h1p[d];
     X.p[d] = c.g * (hp + S.belv[d]);
-    int act = 0;
+    int a = 0;
     if (hp <= HDRY) {
       const double DHPDT = hp - h1p;
       if (DHPDT > 0.0) {
-        act = WD_ACT;
+        a = WD_ACT;
         const double DHPDT2 = (HDRY - h1p) * 0.01;
         if (DHPDT > DHPDT2) {
-          act |= WD_FAST;
-          if (S.subo[d] > 0.5 && X.uhdye[d] > 0.0 && X.hp[q.w] > HDRY2) act |= WD_RW;
-          if (S.subo[q.e] > 0.5 && X.uhdye[q.e] < 0.0 && X.hp[q.e] > HDRY2) act |= WD_RE;
-          if (S.svbo[d] > 0.5 && X.vhdxe[d] > 0.0 && X.hp[q.s] > HDRY2) act |= WD_RS;
-          if (S.svbo[q.n] > 0.5 && X.vhdxe[q.n] < 0.0 && X.hp[q.n] > HDRY2) act |= WD_RN;
+          a |= WD_FAST;
+          if (S.subo[d] > 0.5 && X.uhdye[d] > 0.0 && X.hp[q.w] > HDRY2) a |= WD_RW;
+          if (S.subo[q.e] > 0.5 && X.uhdye[q.e] < 0.0 && X.hp[q.e] > HDRY2) a |= WD_RE;
+          if (S.svbo[d] > 0.5 && X.vhdxe[d] > 0.0 && X.hp[q.s] > HDRY2) a |= WD_RS;
+          if (S.svbo[q.n] > 0.5 && X.vhdxe[q.n] < 0.0 && X.hp[q.n] > HDRY2) a |= WD_RN;
         } else {
-          act |= WD_SLOW;
+          a |= WD_SLOW;
         }
       } else if (hp < HDRY90 || h1p < HDRY) {
-        act = WD_ACT | WD_SLOW;
+        a = WD_ACT | WD_SLOW;
       }
     }
-    X.wd_act[d] = act;
+    X.wd_act[d] = a;
   }
 }
 
 // ISDRY=99 pass 2: the face values the reference's serial L-order loop
 // leaves (a face shared by cells L and LW is last written by L), the ISCDRY
 // updates and the re-solve flag, into the *_n scratch arrays.
-__global__ void __launch_bounds__(NT) k_wd99_apply(DevStatic S, DevState X, int ntile, Ctl *ctl) {
-  bool flag = false;
+__global__ void __launch_bounds__(NT) k_wd99_apply(DevStatic S, DevState X, int ntile, Ctl *ctl,
+                                                  const int *act) {
   TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    if (!act[m] || c.isdry != 99) continue;
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
-    if (S.kind[d] == LAND) continue;
-    const int a = X.wd_act[d], aw = X.wd_act[q.w], as = X.wd_act[q.s];
-    const double subo = S.subo[d], svbo = S.svbo[d];
-    // the west face SUB(L) (owners: L, then LW as its east face)
-    double sub, sbx, svb, sby;
-    if (a & WD_ACT) {
-      const bool o = a & WD_RW;
-      sub = o ? subo : 0.0;
-      sbx = o ? S.sbxo[d] : 0.0;
-    } else if (aw & WD_ACT) {
-      const bool o = aw & WD_RE;
-      sub = o ? subo : 0.0;
-      sbx = o ? S.sbxo[d] : 0.0;
-    } else {
-      sub = X.sub[d];
-      sbx = X.sbx[d];
-    }
-    if (a & WD_ACT) {
-      const bool o = a & WD_RS;
-      svb = o ? svbo : 0.0;
-      sby = o ? S.sbyo[d] : 0.0;
-    } else if (as & WD_ACT) {
-      const bool o = as & WD_RN;
-      svb = o ? svbo : 0.0;
-      sby = o ? S.sbyo[d] : 0.0;
-    } else {
-      svb = X.svb[d];
-      sby = X.sby[d];
-    }
-    X.sub_n[d] = sub;
-    X.sbx_n[d] = sbx;
-    X.svb_n[d] = svb;
-    X.sby_n[d] = sby;
-    if (a & WD_FAST) {
-      const double ww = (a & WD_RW) ? subo : 0.0;
-      const double we = (a & WD_RE) ? S.subo[q.e] : 0.0;
-      const double ws = (a & WD_RS) ? svbo : 0.0;
-      const double wn = (a & WD_RN) ? S.svbo[q.n] : 0.0;
-      const double RDRY = ww + we + ws + wn;
-      X.iscdry[d] = (RDRY < 0.5) ? 1 : 0;
-      // values seen by L before its own writes
-      const double SUBW = (aw & WD_ACT) ? ((aw & WD_RE) ? subo : 0.0) : X.sub[d];
-      const double SUBE = X.sub[q.e];
-      const double SVBS = (as & WD_ACT) ? ((as & WD_RN) ? svbo : 0.0) : X.svb[d];
-      const double SVBN = X.svb[q.n];
-      if (fabs(ww - SUBW) > 0.5 || fabs(we - SUBE) > 0.5 || fabs(ws - SVBS) > 0.5 ||
-          fabs(wn - SVBN) > 0.5)
-        flag = true;
-    } else if (a & WD_SLOW) {
-      if (X.iscdry[d] == 0) {
-        X.iscdry[d] = 1;
-        flag = true;
+    bool flag = false;
+    if (S.kind[d] != LAND) {
+      const int a = X.wd_act[d], aw = X.wd_act[q.w], as = X.wd_act[q.s];
+      const double subo = S.subo[d], svbo = S.svbo[d];
+      // the west face SUB(L) (owners: L, then LW as its east face)
+      double sub, sbx, svb, sby;
+      if (a & WD_ACT) {
+        const bool o = a & WD_RW;
+        sub = o ? subo : 0.0;
+        sbx = o ? S.sbxo[d] : 0.0;
+      } else if (aw & WD_ACT) {
+        const bool o = aw & WD_RE;
+        sub = o ? subo : 0.0;
+        sbx = o ? S.sbxo[d] : 0.0;
+      } else {
+        sub = X.sub[d];
+        sbx = X.sbx[d];
+      }
+      if (a & WD_ACT) {
+        const bool o = a & WD_RS;
+        svb = o ? svbo : 0.0;
+        sby = o ? S.sbyo[d] : 0.0;
+      } else if (as & WD_ACT) {
+        const bool o = as & WD_RN;
+        svb = o ? svbo : 0.0;
+        sby = o ? S.sbyo[d] : 0.0;
+      } else {
+        svb = X.svb[d];
+        sby = X.sby[d];
+      }
+      X.sub_n[d] = sub;
+      X.sbx_n[d] = sbx;
+      X.svb_n[d] = svb;
+      X.sby_n[d] = sby;
+      if (a & WD_FAST) {
+        const double ww = (a & WD_RW) ? subo : 0.0;
+        const double we = (a & WD_RE) ? S.subo[q.e] : 0.0;
+        const double ws = (a & WD_RS) ? svbo : 0.0;
+        const double wn = (a & WD_RN) ? S.svbo[q.n] : 0.0;
+        const double RDRY = ww + we + ws + wn;
+        X.iscdry[d] = (RDRY < 0.5) ? 1 : 0;
+        // values seen by L before its own writes
+        const double SUBW = (aw & WD_ACT) ? ((aw & WD_RE) ? subo : 0.0) : X.sub[d];
+        const double SUBE = X.sub[q.e];
+        const double SVBS = (as & WD_ACT) ? ((as & WD_RN) ? svbo : 0.0) : X.svb[d];
+        const double SVBN = X.svb[q.n];
+        if (fabs(ww - SUBW) > 0.5 || fabs(we - SUBE) > 0.5 || fabs(ws - SVBS) > 0.5 ||
+            fabs(wn - SVBN) > 0.5)
+          flag = true;
+      } else if (a & WD_SLOW) {
+        if (X.iscdry[d] == 0) {
+          X.iscdry[d] = 1;
+          flag = true;
+        }
       }
     }
+    if (__syncthreads_or(flag) && threadIdx.x == 0) atomicOr(&ctl[m].icordry, 1);
   }
-  if (__syncthreads_or(flag) && threadIdx.x == 0) atomicOr(&ctl->icordry, 1);
 }
 
-__global__ void __launch_bounds__(NT) k_wd99_commit(DevStatic S, DevState X, int ntile) {
+__global__ void __launch_bounds__(NT) k_wd99_commit(DevStatic S, DevState X, int ntile,
+                                                   const int *act) {
   TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    if (!act[m] || c.isdry != 99) continue;
     const int d = tile * TILE + threadIdx.x;
     if (S.kind[d] == LAND) continue;
     X.sub[d] = X.sub_n[d];
@@ -703,108 +768,113 @@ __global__ void __launch_bounds__(NT) k_wd99_commit(DevStatic S, DevState X, int
   }
 }
 
-// ISDRY>0 without a drying check (ISDRY=98): only the P update.
-// (k_wd_legacy with check=0.)
-
 // ---------------------------------------------------------------------------
-// :838-889 volume wasting of isolated wet cells (NDRYSTP<0) and the later
-// H1P/QDWASTE fix-up of the wasted cells (:1003-1025).
-__global__ void __launch_bounds__(NT) k_fin_waste(DevStatic S, DevState X, StepScalars c,
-                                                 int ntile, Ctl *ctl) {
-  const int NTMP = abs(c.ndrystp);
-  int nw = 0;
+// :838-889 volume wasting of isolated wet cells (ISDRY>0, NDRYSTP<0) and the
+// later H1P/QDWASTE fix-up of the wasted cells (:1003-1025).
+__global__ void __launch_bounds__(NT) k_fin_waste(DevStatic S, DevState X, int ntile, Ctl *ctl,
+                                                 const int *act) {
   TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    if (!act[m] || c.isdry <= 0 || c.ndrystp >= 0) continue;
+    const int NTMP = abs(c.ndrystp);
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
-    if (S.kind[d] == LAND) continue;
-    const double hp = X.hp[d];
-    if (hp >= c.hdry) {
-      const double RDRY = X.sub[d] + X.sub[q.e] + X.svb[d] + X.svb[q.n];
-      if (RDRY > 0.5) {
-        X.natdry[d] = 0;
-      } else {
-        const int nat = X.natdry[d] + 1;
-        X.natdry[d] = nat;
-        if (nat > NTMP) {
-          const double bl = S.belv[d];
-          double RVAL = 0.0;
-          if (S.subo[q.e] > 0.5 && S.belv[q.e] < bl) RVAL = RVAL + 1.;
-          if (S.subo[d] > 0.5 && S.belv[q.w] < bl) RVAL = RVAL + 1.;
-          if (S.svbo[q.n] > 0.5 && S.belv[q.n] < bl) RVAL = RVAL + 1.;
-          if (S.svbo[d] > 0.5 && S.belv[q.s] < bl) RVAL = RVAL + 1.;
-          if (RVAL > 0. || hp < c.hdry * 2.) {
-            const double HOLDTMP = hp;
-            const double hnew = 0.90 * c.hdry;
-            X.hp[d] = hnew;
-            X.h1p[d] = 0.90 * c.hdry;
-            X.natdry[d] = 0;
-            X.qdwaste[d] = (c.isbal == 0) ? 0.0 : c.delti * S.dxyp[d] * (HOLDTMP - hnew);
-            X.vdwaste[d] = X.vdwaste[d] + S.dxyp[d] * (HOLDTMP - hnew);
-            X.wasted[d] = 1;
-            ++nw;
+    int nw = 0;
+    if (S.kind[d] != LAND) {
+      const double hp = X.hp[d];
+      if (hp >= c.hdry) {
+        const double RDRY = X.sub[d] + X.sub[q.e] + X.svb[d] + X.svb[q.n];
+        if (RDRY > 0.5) {
+          X.natdry[d] = 0;
+        } else {
+          const int nat = X.natdry[d] + 1;
+          X.natdry[d] = nat;
+          if (nat > NTMP) {
+            const double bl = S.belv[d];
+            double RVAL = 0.0;
+            if (S.subo[q.e] > 0.5 && S.belv[q.e] < bl) RVAL = RVAL + 1.;
+            if (S.subo[d] > 0.5 && S.belv[q.w] < bl) RVAL = RVAL + 1.;
+            if (S.svbo[q.n] > 0.5 && S.belv[q.n] < bl) RVAL = RVAL + 1.;
+            if (S.svbo[d] > 0.5 && S.belv[q.s] < bl) RVAL = RVAL + 1.;
+            if (RVAL > 0. || hp < c.hdry * 2.) {
+              const double HOLDTMP = hp;
+              const double hnew = 0.90 * c.hdry;
+              X.hp[d] = hnew;
+              X.h1p[d] = 0.90 * c.hdry;
+              X.natdry[d] = 0;
+              X.qdwaste[d] = (c.isbal == 0) ? 0.0 : c.delti * S.dxyp[d] * (HOLDTMP - hnew);
+              X.vdwaste[d] = X.vdwaste[d] + S.dxyp[d] * (HOLDTMP - hnew);
+              X.wasted[d] = 1;
+              nw = 1;
+            }
           }
         }
       }
     }
+    nw = __syncthreads_count(nw);
+    if (threadIdx.x == 0 && nw) atomicAdd(&ctl[m].nwasted, nw);
   }
-  for (int o = 16; o > 0; o >>= 1) nw += __shfl_down_sync(0xffffffffu, nw, o);
-  if ((threadIdx.x & 31) == 0 && nw) atomicAdd(&ctl->nwasted, nw);
 }
 
 // :893-931 final P (ISDRY=0), HU, HV, reciprocals, LMASKDRY; NEGDEP count.
-__global__ void __launch_bounds__(NT) k_fin(DevStatic S, DevState X, StepScalars c, int ntile,
-                                           Ctl *ctl) {
-  int nneg = 0, nbad = 0;
+__global__ void __launch_bounds__(NT) k_fin(DevStatic S, DevState X, int ntile, Ctl *ctl,
+                                           const int *act) {
   TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    if (!act[m]) continue;
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
-    if (S.kind[d] == LAND) continue;
-    const double hp = X.hp[d];
-    if (c.isdry == 0) X.p[d] = c.g * (hp + S.belv[d]);
-    const double dxyp = S.dxyp[d];
-    const double hu = (dxyp * hp + S.dxyp[q.w] * X.hp[q.w]) * S.fsgzu[d];
-    const double hv = (dxyp * hp + S.dxyp[q.s] * X.hp[q.s]) * S.fsgzv[d];
-    X.hu[d] = hu;
-    X.hv[d] = hv;
-    X.hpi[d] = 1. / hp;
-    X.hui[d] = 1. / hu;
-    X.hvi[d] = 1. / hv;
-    if (c.isdry > 0) {
-      int mask = 1;
-      if (hp < c.hdry) {
-        int IUW = 0, IUE = 0, IVS = 0, IVN = 0;
-        if (X.sub1[d] < 0.5 && X.sub[d] < 0.5) IUE = 1;
-        if (X.sub1[q.e] < 0.5 && X.sub[q.e] < 0.5) IUW = 1;
-        if (X.svb1[d] < 0.5 && X.svb[d] < 0.5) IVS = 1;
-        if (X.svb1[q.n] < 0.5 && X.svb[q.n] < 0.5) IVN = 1;
-        if (IUW + IUE + IVS + IVN == 4) mask = 0;
+    int neg = 0, bad = 0;
+    if (S.kind[d] != LAND) {
+      const double hp = X.hp[d];
+      if (c.isdry == 0) X.p[d] = c.g * (hp + S.belv[d]);
+      const double dxyp = S.dxyp[d];
+      const double hu = (dxyp * hp + S.dxyp[q.w] * X.hp[q.w]) * S.fsgzu[d];
+      const double hv = (dxyp * hp + S.dxyp[q.s] * X.hp[q.s]) * S.fsgzv[d];
+      X.hu[d] = hu;
+      X.hv[d] = hv;
+      X.hpi[d] = 1. / hp;
+      X.hui[d] = 1. / hu;
+      X.hvi[d] = 1. / hv;
+      if (c.isdry > 0) {
+        int mask = 1;
+        if (hp < c.hdry) {
+          int IUW = 0, IUE = 0, IVS = 0, IVN = 0;
+          if (X.sub1[d] < 0.5 && X.sub[d] < 0.5) IUE = 1;
+          if (X.sub1[q.e] < 0.5 && X.sub[q.e] < 0.5) IUW = 1;
+          if (X.svb1[d] < 0.5 && X.svb[d] < 0.5) IVS = 1;
+          if (X.svb1[q.n] < 0.5 && X.svb[q.n] < 0.5) IVN = 1;
+          if (IUW + IUE + IVS + IVN == 4) mask = 0;
+        }
+        X.lmaskdry[d] = mask;
       }
-      X.lmaskdry[d] = mask;
+      neg = (hp <= 0.) ? 1 : 0;
+      bad = isfinite(X.p[d]) ? 0 : 1;
     }
-    if (hp <= 0.) ++nneg;
-    if (!isfinite(X.p[d])) ++nbad;
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    nneg += __shfl_down_sync(0xffffffffu, nneg, o);
-    nbad += __shfl_down_sync(0xffffffffu, nbad, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    if (nneg) atomicAdd(&ctl->nneg, nneg);
-    if (nbad) atomicAdd(&ctl->nnonfinite, nbad);
+    neg = __syncthreads_count(neg);
+    bad = __syncthreads_count(bad);
+    if (threadIdx.x == 0) {
+      if (neg) atomicAdd(&ctl[m].nneg, neg);
+      if (bad) atomicAdd(&ctl[m].nnonfinite, bad);
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
-// Host order <-> tile order.  A land slot receives element LC of the host
-// array (the ghost value); gathers write water slots only.
-__global__ void k_scatter(const CopyJob *jobs, int njob, const int *lidx, int nslot, int lc) {
+// Host order <-> tile order.  A staging buffer holds every member's host array
+// back to back (member m at element offset moff[m], LC = mlc[m] elements).  A
+// land slot receives element LC of its member's array (the ghost value);
+// gathers write water slots only.
+__global__ void k_scatter(const CopyJob *jobs, int njob, const int *lidx, const int *tile_member,
+                          const long long *moff, const int *mlc, int nslot) {
   const int j = blockIdx.y;
   if (j >= njob) return;
   const CopyJob J = jobs[j];
   for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nslot; d += gridDim.x * blockDim.x) {
     const int L = lidx[d];
     if (L < 2 && J.is_int == 3) continue;  // water-only: leave land slots as they are
-    const int src = (L >= 2 ? L : lc) - 1;
+    const int m = tile_member[d / TILE];
+    const long long src = moff[m] + (L >= 2 ? L : mlc[m]) - 1;
     if (J.is_int == 1 || J.is_int == 2)
       static_cast<int *>(J.dev)[d] = (J.is_int == 1)
                                          ? (static_cast<const int *>(J.host_order)[src] != 0 ? 1 : 0)
@@ -814,141 +884,158 @@ __global__ void k_scatter(const CopyJob *jobs, int njob, const int *lidx, int ns
   }
 }
 
-__global__ void k_gather(const CopyJob *jobs, int njob, const int *lidx, int nslot) {
+__global__ void k_gather(const CopyJob *jobs, int njob, const int *lidx, const int *tile_member,
+                         const long long *moff, int nslot) {
   const int j = blockIdx.y;
   if (j >= njob) return;
   const CopyJob J = jobs[j];
   for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nslot; d += gridDim.x * blockDim.x) {
     const int L = lidx[d];
     if (L < 2) continue;
+    const long long dst = moff[tile_member[d / TILE]] + L - 1;
     if (J.is_int == 1 || J.is_int == 2)
-      static_cast<int *>(const_cast<void *>(J.host_order))[L - 1] = static_cast<const int *>(J.dev)[d];
+      static_cast<int *>(const_cast<void *>(J.host_order))[dst] = static_cast<const int *>(J.dev)[d];
     else
-      static_cast<double *>(const_cast<void *>(J.host_order))[L - 1] =
+      static_cast<double *>(const_cast<void *>(J.host_order))[dst] =
           static_cast<const double *>(J.dev)[d];
   }
 }
 
 // ---------------------------------------------------------------------------
 // launch wrappers
-void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c) {
-  k_begin<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile);
+void launch_begin(const Launch &l, const DevStatic &S, const DevState &X) {
+  k_begin<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
   count_launches(1);
 }
-void launch_assemble(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
-                     Ctl *ctl, double *part) {
-  k_assemble<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile, ctl, part);
+void launch_sweep_reset(const Launch &l, Ctl *ctl, const int *act, int nmember) {
+  k_sweep_reset<<<(nmember + 255) / 256, 256, 0, l.stream>>>(ctl, act, nmember);
   count_launches(1);
 }
-void launch_obc(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B,
-                const StepScalars &c, Ctl *ctl, bool serial) {
+void launch_assemble(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
+                     const int *act) {
+  k_assemble<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, ctl, act);
+  count_launches(1);
+}
+void launch_obc(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B, Ctl *ctl,
+                const int *act, bool serial) {
   if (B.n == 0) return;
   if (serial)
-    k_obc_serial<<<1, 1, 0, l.stream>>>(S, X, B, c, ctl);
+    k_obc_serial<<<1, 1, 0, l.stream>>>(S, X, B, ctl, act);
   else
-    k_obc_parallel<<<(B.n + NT - 1) / NT, NT, 0, l.stream>>>(S, X, B, c, ctl);
+    k_obc_parallel<<<(B.n + NT - 1) / NT, NT, 0, l.stream>>>(S, X, B, ctl, act);
   count_launches(1);
 }
-void launch_obc_reset(const Launch &l, const DevObc &B, const DevState &X) {
+void launch_obc_reset(const Launch &l, const DevStatic &S, const DevObc &B, const DevState &X) {
   if (B.n == 0) return;
-  k_obc_reset<<<(B.n + 255) / 256, 256, 0, l.stream>>>(B, X);
+  k_obc_reset<<<(B.n + 255) / 256, 256, 0, l.stream>>>(S, B, X);
   count_launches(1);
 }
 void launch_scale(const Launch &l, const DevStatic &S, const DevState &X, const DevSystem &Y,
-                  Ctl *ctl, int mixed, int write_cross) {
-  k_scale<<<l.grid, NT, 0, l.stream>>>(S, X, Y, l.ntile, ctl, write_cross);
+                  Ctl *ctl, const int *act, int mixed, int write_cross) {
+  k_scale<<<l.grid, NT, 0, l.stream>>>(S, X, Y, l.ntile, ctl, act, write_cross);
   count_launches(1);
   if (mixed) {
-    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, write_cross);
+    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, act, write_cross);
     count_launches(1);
   }
 }
+void launch_solve_reset(const Launch &l, Ctl *ctl, Glob *glob, const int *act, int nmember) {
+  k_solve_reset<<<1, 256, 0, l.stream>>>(ctl, glob, act, nmember);
+  count_launches(1);
+}
+void launch_outer_reset(const Launch &l, Glob *glob) {
+  k_outer_reset<<<1, 1, 0, l.stream>>>(glob);
+  count_launches(1);
+}
 void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
-                    double *part) {
-  k_cg_init<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part);
+                    Glob *glob, double *part) {
+  k_cg_init<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, glob, part);
   count_launches(1);
 }
 void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
-                    double *part, double rsqm, int iterm) {
-  k_cg_matvec<<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
+                    Glob *glob, double *part) {
+  k_cg_matvec<<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, ctl, part);
   count_launches(1);
-  k_cg_update<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part, rsqm, iterm);
+  k_cg_update<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, glob, part, 0);
   count_launches(1);
 }
 void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {
-  k_cg_matvec<<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, l.ntile, ctl, part);
+  k_cg_matvec<<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, ctl, part);
   count_launches(1);
 }
 void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
-                      double *part, double rsqm, int iterm) {
-  k_cg_update<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part, rsqm, iterm);
+                      Glob *glob, double *part, int no_stop) {
+  k_cg_update<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, glob, part, no_stop);
   count_launches(1);
 }
 void launch_mx_resid(const Launch &l, const DevStatic &S, const DevSystem &Y, const double *P,
-                     Ctl *ctl, double *part, double rsqm, double rel_tol) {
-  k_mx_resid<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, l.ntile, ctl, part, rsqm, rel_tol);
+                     Ctl *ctl, Glob *glob, double *part, double rsqm_fac, double rel_tol,
+                     int no_stop) {
+  k_mx_resid<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, glob, part, rsqm_fac, rel_tol, no_stop);
   count_launches(1);
 }
-void launch_mx_apply(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P) {
-  k_mx_apply<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, l.ntile);
+void launch_mx_apply(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
+                     const Ctl *ctl) {
+  k_mx_apply<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl);
   count_launches(1);
 }
-void launch_backsub(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c) {
-  k_backsub<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile);
+void launch_backsub(const Launch &l, const DevStatic &S, const DevState &X, const int *act) {
+  k_backsub<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
   count_launches(1);
-  k_continuity<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile);
+  k_continuity<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
   count_launches(1);
 }
 void launch_obc_hp(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B,
-                   const StepScalars &c) {
+                   const int *act) {
   if (B.n == 0) return;
-  k_obc_hp<<<(B.n + 255) / 256, 256, 0, l.stream>>>(S, X, B, c);
+  k_obc_hp<<<(B.n + 255) / 256, 256, 0, l.stream>>>(S, X, B, act);
   count_launches(1);
 }
-void launch_wd_legacy(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
-                      Ctl *ctl, int check) {
-  k_wd_legacy<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile, ctl, check);
-  count_launches(1);
-}
-void launch_wd99(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
-                 Ctl *ctl) {
-  k_wd99_decide<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile);
-  count_launches(1);
-  k_wd99_apply<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, ctl);
-  count_launches(1);
-  k_wd99_commit<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
-  count_launches(1);
-}
-void launch_final(const Launch &l, const DevStatic &S, const DevState &X, const StepScalars &c,
-                  Ctl *ctl) {
-  if (c.isdry > 0 && c.ndrystp < 0) {
-    k_fin_waste<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile, ctl);
+void launch_wetdry(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
+                   const int *act, bool any_legacy, bool any99) {
+  if (any_legacy) {
+    k_wd_legacy<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, ctl, act);
     count_launches(1);
   }
-  k_fin<<<l.grid, NT, 0, l.stream>>>(S, X, c, l.ntile, ctl);
+  if (any99) {
+    k_wd99_decide<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
+    count_launches(1);
+    k_wd99_apply<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, ctl, act);
+    count_launches(1);
+    k_wd99_commit<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
+    count_launches(1);
+  }
+}
+void launch_final(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
+                  const int *act, bool any_waste) {
+  if (any_waste) {
+    k_fin_waste<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, ctl, act);
+    count_launches(1);
+  }
+  k_fin<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, ctl, act);
   count_launches(1);
 }
-void launch_scatter(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx, int nslot,
-                    int lc) {
+void launch_scatter(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx,
+                    const int *tile_member, const long long *moff, const int *mlc, int nslot) {
   if (njob == 0) return;
   dim3 g(std::min((nslot + 255) / 256, 2048), njob);
-  k_scatter<<<g, 256, 0, st>>>(jobs, njob, lidx, nslot, lc);
+  k_scatter<<<g, 256, 0, st>>>(jobs, njob, lidx, tile_member, moff, mlc, nslot);
   count_launches(1);
 }
-void launch_gather(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx, int nslot) {
+void launch_gather(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx,
+                   const int *tile_member, const long long *moff, int nslot) {
   if (njob == 0) return;
   dim3 g(std::min((nslot + 255) / 256, 2048), njob);
-  k_gather<<<g, 256, 0, st>>>(jobs, njob, lidx, nslot);
+  k_gather<<<g, 256, 0, st>>>(jobs, njob, lidx, tile_member, moff, nslot);
   count_launches(1);
 }
-
 void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                         int mixed) {
   k_sys_prepare<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, ctl);
   count_launches(1);
   if (mixed) {  // the standalone system may be unsymmetric: always the 4-array form
-    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, 1);
+    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, nullptr, 1);
     count_launches(1);
   }
 }

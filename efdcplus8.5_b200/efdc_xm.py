@@ -242,6 +242,19 @@ def load(path: str | os.PathLike | None = None):
     lib.efdc_xm_congrad.restype = C.c_int32
     lib.efdc_xm_congrad.argtypes = [C.c_void_p] + [_pd] * 8 + [C.c_double, C.c_int32,
                                                                 C.c_int32, _pi, _pd]
+    lib.efdc_xm_create_batch.restype = C.c_void_p
+    lib.efdc_xm_create_batch.argtypes = [C.POINTER(Grid), C.c_int32, C.c_int32]
+    lib.efdc_xm_nmembers.restype = C.c_int32
+    lib.efdc_xm_nmembers.argtypes = [C.c_void_p]
+    lib.efdc_xm_step_batch.restype = C.c_int32
+    lib.efdc_xm_step_batch.argtypes = [C.c_void_p, C.POINTER(Params), C.POINTER(Fields),
+                                       C.POINTER(Stats)]
+    lib.efdc_xm_upload_batch.restype = C.c_int32
+    lib.efdc_xm_upload_batch.argtypes = [C.c_void_p, C.POINTER(Fields)]
+    lib.efdc_xm_download_batch.restype = C.c_int32
+    lib.efdc_xm_download_batch.argtypes = [C.c_void_p, C.POINTER(Fields)]
+    lib.efdc_xm_step_device_batch.restype = C.c_int32
+    lib.efdc_xm_step_device_batch.argtypes = [C.c_void_p, C.POINTER(Params), C.POINTER(Stats)]
     if path is None:
         _lib = lib
     return lib
@@ -321,3 +334,87 @@ class Solver:
                                       float(rsqm), int(iterm), int(precision),
                                       C.byref(it), C.byref(rsq))
         return rc, it.value, rsq.value
+
+
+class BatchSolver:
+    """Host-side handle over one efdc_xm batch context: M independent basins
+    (ensemble members) advanced together, one launch sequence per step."""
+
+    def __init__(self, grids: list, device: int = 0, lib=None):
+        self.lib = lib or load()
+        self.m = len(grids)
+        if self.m < 1:
+            raise ValueError("BatchSolver needs at least one grid")
+        built = [make_grid(g) for g in grids]
+        self._keep = [k for _, k in built]
+        self._grids = (Grid * self.m)(*[s for s, _ in built])
+        self.ctx = self.lib.efdc_xm_create_batch(self._grids, self.m, device)
+        if not self.ctx:
+            raise RuntimeError("efdc_xm_create_batch failed: " + self.last_error())
+        self.la = [int(g["la"]) for g in grids]
+
+    def last_error(self) -> str:
+        return self.lib.efdc_xm_last_error().decode()
+
+    def close(self):
+        if self.ctx:
+            self.lib.efdc_xm_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):  # pragma: no cover - best effort
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _fields(self, states, **kw):
+        if len(states) != self.m:
+            raise ValueError(f"need {self.m} member states, got {len(states)}")
+        fs = [make_fields(st, **kw) for st in states]
+        return (Fields * self.m)(*[f for f, _ in fs]), fs
+
+    def _params(self, params):
+        if len(params) != self.m:
+            raise ValueError(f"need {self.m} member parameter sets, got {len(params)}")
+        return (Params * self.m)(*params)
+
+    def _check(self, name, rc):
+        if rc in (CUDA_ERROR, BAD_ARGUMENT, UNSUPPORTED, DEVICE_TIMEOUT):
+            raise RuntimeError(f"{name}: {STATUS_NAMES.get(rc, rc)}: {self.last_error()}")
+
+    def step(self, params: list, states: list, *, diag=False, lists=False) -> list:
+        fa, _k = self._fields(states, diag=diag, lists=lists)
+        pa = self._params(params)
+        sa = (Stats * self.m)()
+        rc = self.lib.efdc_xm_step_batch(self.ctx, pa, fa, sa)
+        self._check("efdc_xm_step_batch", rc)
+        return list(sa)
+
+    def upload(self, states: list):
+        fa, _k = self._fields(states)
+        rc = self.lib.efdc_xm_upload_batch(self.ctx, fa)
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_upload_batch: {self.last_error()}")
+
+    def download(self, states: list, *, diag=False, lists=False):
+        fa, _k = self._fields(states, diag=diag, lists=lists)
+        rc = self.lib.efdc_xm_download_batch(self.ctx, fa)
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_download_batch: {self.last_error()}")
+
+    def step_device(self, params: list) -> list:
+        pa = self._params(params)
+        sa = (Stats * self.m)()
+        rc = self.lib.efdc_xm_step_device_batch(self.ctx, pa, sa)
+        self._check("efdc_xm_step_device_batch", rc)
+        return list(sa)
+
+    def stream(self) -> int:
+        return int(self.lib.efdc_xm_stream(self.ctx) or 0)
+
+    def time_kernels(self, precision: int, reps: int = 20) -> KTime:
+        kt = KTime()
+        rc = self.lib.efdc_xm_time_kernels(self.ctx, precision, reps, C.byref(kt))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_time_kernels: {self.last_error()}")
+        return kt

@@ -188,6 +188,32 @@ int32_t efdc_xm_congrad(efdc_xm_ctx *ctx, const double *ccc, const double *ccs,
                         double rsqm, int32_t iterm, int32_t precision,
                         int32_t *iters, double *rsq);
 
+/* ---- Ensembles: several independent basins in one context ----
+ *
+ * No counterpart in the reference, which runs one basin per process.  A
+ * batch context holds `nmembers` basins ("members": ensemble runs,
+ * calibration perturbations, or unrelated grids of any sizes) and advances
+ * all of them with one launch sequence per step, each member exactly as
+ * efdc_xm_step would advance it alone: every reduction (CCMNM, the PCG dot
+ * products, the wet/dry re-solve flag, the negative-depth count) is taken per
+ * member, each member stops its PCG at its own RSQM/ITERM and sweeps wet/dry
+ * its own number of times.  All members must use the same `precision`.
+ * Arrays of structures are indexed by member (grids[m], prm[m], f[m],
+ * stats[m]); a field pointer is either given for every member or for none.
+ * The return value is the first member error, else EFDC_XM_NEG_DEPTH if any
+ * member had negative depths, else EFDC_XM_OK; stats[m].status is per member.
+ * The single-basin functions above are the same code with one member and
+ * refuse a context that holds more than one. */
+efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers,
+                                  int32_t device);
+int32_t efdc_xm_nmembers(const efdc_xm_ctx *ctx);
+int32_t efdc_xm_step_batch(efdc_xm_ctx *ctx, const efdc_xm_params *prm,
+                           efdc_xm_fields *f, efdc_xm_stats *stats);
+int32_t efdc_xm_upload_batch(efdc_xm_ctx *ctx, const efdc_xm_fields *f);
+int32_t efdc_xm_step_device_batch(efdc_xm_ctx *ctx, const efdc_xm_params *prm,
+                                  efdc_xm_stats *stats);
+int32_t efdc_xm_download_batch(efdc_xm_ctx *ctx, efdc_xm_fields *f);
+
 /* ---- Extensions with no counterpart in the reference (measurement hooks) ---- */
 
 /* The CUDA stream (cudaStream_t) every call of this context runs on, so a
@@ -205,7 +231,7 @@ typedef struct efdc_xm_ktime {
   double ms_matvec;     /* per launch */
   double ms_update;     /* per launch */
   int32_t reps;
-  int32_t ncells;       /* water cells, LA-1 */
+  int32_t ncells;       /* water cells, LA-1 summed over members */
   int32_t nslots;       /* tile slots processed per launch (incl. land padding) */
 } efdc_xm_ktime;
 int32_t efdc_xm_time_kernels(efdc_xm_ctx *ctx, int32_t precision, int32_t reps,
