@@ -1,29 +1,38 @@
 #!/usr/bin/env python
 """External-mode throughput on one B200: cell-iterations per second.
 
-Workload: the single-domain 2048x2048 curvilinear basin (~3.4M wet cells,
-DXP/DYP 50-200 m, depth 1-60 m, west tidal boundary 0.2-1.5 m, dt=5 s),
-seeded and synthetic.  A "step" is one CALPUV2C call (assembly, open
-boundaries, scaling, PCG, back-substitution, continuity, finalisation).
+Headline workload (default, ``--workload ensemble``): a batched ensemble of
+256 independent basins with wet-cell counts drawn log-uniformly from 10k to
+400k (26.3M cells in total), each with its own seeded bathymetry (1-40 m),
+Manning n (0.015-0.04) and M2 amplitude (0.1-1.0 m), dt=10 s, RSQM=1e-10.
+Synthetic and seeded.  A "step" is one CALPUV2C call for every member
+(assembly, open boundaries, scaling, PCG, back-substitution, continuity,
+finalisation), all members in one launch sequence.
 
-* value: the MIXED solver (FP32 inner PCG, FP64 refinement and dot products),
-  state resident in HBM.  cell-iterations = wet cells x CG iterations of the
-  FP64 solve of the same step (the FP64 drop-in is run first over the same
-  steps; its iteration counts are the credit), so extra inner iterations of
-  the mixed solver earn nothing.
-* fp64_value: the plain FP64 drop-in on the same steps.
-* e2e: the same metric through efdc_xm_step with pinned host arrays: every
-  step uploads the caller's fields and downloads the outputs.
-* roofline: the dominant kernel (FP32 CG matrix-vector kernel) timed live with
-  CUDA events on the library's stream, against MEASURED_PEAKS.json.
+* value: the batched MIXED solver (FP32 inner PCG, FP64 refinement and dot
+  products), state resident in HBM.  cell-iterations = wet cells x CG
+  iterations of the FP64 solve of the same step and member (the batched FP64
+  run over the same steps gives the credit; it is bit-identical to the
+  single-basin drop-in), so extra inner iterations of the mixed solver earn
+  nothing.
+* fp64_dropin_value: the plain FP64 drop-in, efdc_xm_step_device once per
+  member per step (one context per basin, as a host that calls CALPUV2C per
+  basin would run it).
+* fp64_batched_value: FP64, all members in one context.
+* e2e: the same metric through efdc_xm_step_batch with pinned host arrays:
+  every step uploads every member's fields and downloads the outputs.
+* roofline: the dominant kernel (FP32 CG matrix-vector kernel over all
+  members) timed live with CUDA events on the library's stream, against
+  MEASURED_PEAKS.json.
 * cpu_baseline: the FP64 C++ restatement of the reference (OpenMP, NOPTIMAL
-  range split, serial dot products) on a bounded sample of the same workload.
+  range split, serial dot products) on a bounded sample of members.
+* single_domain: the same three figures on the 2048x2048 curvilinear basin
+  (3.4M cells, dt=5 s); ``--workload basin`` makes it the headline.
 
 --impl reference times that CPU restatement alone (the reference itself is
-Intel Fortran and cannot be built here).  With --gpus N>1 every rank solves its
-own replica of the basin (the external mode of one domain does not shard;
-members of an ensemble would), and value is the sum over ranks divided by the
-slowest rank's time.
+Intel Fortran and cannot be built here).  With --gpus N>1 every rank advances
+its own ensemble (distinct seeds; the members shard with no exchange), and
+value is the sum over ranks divided by the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -35,6 +44,7 @@ import subprocess
 import sys
 import tempfile
 import time
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 import numpy as np
@@ -55,8 +65,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--size", type=int, default=2048)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--workload", choices=("ensemble", "basin"), default="ensemble")
+    ap.add_argument("--members", type=int, default=256)
+    ap.add_argument("--size", type=int, default=2048, help="basin workload: grid size")
+    ap.add_argument("--dropin-steps", type=int, default=10)
+    ap.add_argument("--basin-steps", type=int, default=50,
+                    help="single-domain side measurement (0: skip)")
+    ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -67,20 +82,37 @@ def dist_env():
             int(os.environ.get("WORLD_SIZE", 1)))
 
 
-def workload_config(scn, size):
-    return {"workload": f"single-domain basin {size}x{size} curvilinear, west M2 boundary 0.2-1.5 m, "
-                        f"dt=5 s, RSQM=1e-10, FP64-iteration credit",
-            "cells": int(scn.ncell), "grid": f"{size}x{size}", "tiles_32x8": None,
-            "l2": "flushed between timed steps (256 MiB write); working set > L2",
-            "parallelism": "replicas"}
-
-
 def measured_peaks():
     p = REPO / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def ensemble(members, seed):
+    """The seeded ensemble (threaded: numpy releases the GIL)."""
+    sizes = S.config3_sizes(seed=seed, members=members)
+    with ThreadPoolExecutor(os.cpu_count() or 4) as ex:
+        return list(ex.map(lambda kn: S.config3_member(kn[0], int(kn[1]), seed=seed),
+                           enumerate(sizes)))
+
+
+def ensemble_config(scns, seed):
+    cells = [s.ncell for s in scns]
+    return {"workload": f"batched ensemble of {len(scns)} basins, wet cells log-uniform "
+                        f"10k-400k, depth 1-40 m, Manning 0.015-0.04, M2 0.1-1.0 m, dt=10 s, "
+                        f"RSQM=1e-10, FP64-iteration credit",
+            "members": len(scns), "cells": int(sum(cells)), "min_cells": int(min(cells)),
+            "max_cells": int(max(cells)), "seed": seed,
+            "l2": "inputs larger than L2 (all members resident, >10 GB)"}
+
+
+def basin_config(scn, size):
+    return {"workload": f"single-domain basin {size}x{size} curvilinear, west M2 boundary "
+                        f"0.2-1.5 m, dt=5 s, RSQM=1e-10, FP64-iteration credit",
+            "cells": int(scn.ncell), "grid": f"{size}x{size}",
+            "l2": "flushed between timed steps (256 MiB write); working set > L2"}
 
 
 # ------------------------------------------------------------------ clocks
@@ -125,44 +157,70 @@ class Clocks:
 
 
 # --------------------------------------------------------------- CPU runs
-def cpu_run(scn, seconds, max_steps, warmup=0):
-    """The oracle port (FP64, OpenMP over all host threads) on the workload."""
+def cpu_run(scns, seconds, max_steps, warmup=0):
+    """The oracle port (FP64, OpenMP over all host threads): steps of the
+    given basins, all basins per step, until `seconds` or `max_steps`."""
     sys.path.insert(0, str(REPO / "oracle"))
     import oracle as O
     cores = os.cpu_count() or 1
-    orc = O.Oracle(scn.grid, nthreads=cores, noptimal_cap=cores)
-    st = scn.copy_state()
+    orcs = [O.Oracle(s.grid, nthreads=cores, noptimal_cap=cores) for s in scns]
+    sts = [s.copy_state() for s in scns]
     n = 0
     for _ in range(warmup):
         n += 1
-        orc.step(X.make_params(scn.params, n=n, tn=scn.tn(n)), st)
+        for s, o, st in zip(scns, orcs, sts):
+            o.step(X.make_params(s.params, n=n, tn=s.tn(n)), st)
     cell_iters = 0
     t0 = time.perf_counter()
     k = 0
     while k < max_steps:
         n += 1
-        s = orc.step(X.make_params(scn.params, n=n, tn=scn.tn(n)), st)
-        cell_iters += scn.ncell * s.iters_total
+        for s, o, st in zip(scns, orcs, sts):
+            r = o.step(X.make_params(s.params, n=n, tn=s.tn(n)), st)
+            cell_iters += s.ncell * r.iters_total
         k += 1
         if time.perf_counter() - t0 > seconds:
             break
     dt = time.perf_counter() - t0
-    return cell_iters / dt, k, dt, orc.noptimal
+    nopt = orcs[0].noptimal
+    for o in orcs:
+        o.close()
+    return cell_iters / dt, k, dt, nopt
+
+
+def cpu_sample(scns):
+    """A bounded, size-spread sample of the ensemble for the CPU port: every
+    32nd member in size order (8 of 256)."""
+    order = sorted(range(len(scns)), key=lambda k: scns[k].ncell)
+    pick = order[::max(1, len(order) // 8)][:8]
+    return [scns[k] for k in pick]
 
 
 def reference_arm(args):
     rank, _, world = dist_env()
     if rank != 0:
         return
-    scn = S.config2(n=args.size)
-    v, k, dt, nopt = cpu_run(scn, seconds=max(5.0, 6.0 * args.steps), max_steps=args.steps,
+    if args.workload == "ensemble":
+        seed = 3
+        scns = ensemble(args.members, seed)
+        cfg = ensemble_config(scns, seed)
+        samp = cpu_sample(scns)
+        what = (f"{len(samp)} members spread over the size range "
+                f"({sum(s.ncell for s in samp)} cells)")
+    else:
+        scn = S.config2(n=args.size)
+        cfg = basin_config(scn, args.size)
+        samp = [scn]
+        what = f"the {args.size}x{args.size} basin ({scn.ncell} cells)"
+    v, k, dt, nopt = cpu_run(samp, seconds=min(120.0, max(5.0, 1.0 * args.steps)),
+                             max_steps=args.steps,
                              warmup=min(args.warmup, 1))
-    sample = (f"{k} CALPUV2C steps of the {args.size}x{args.size} basin ({scn.ncell} cells) "
-              f"after {min(args.warmup, 1)} warm-up, FP64 C++ restatement, {nopt} OpenMP threads")
+    sample = (f"{k} CALPUV2C steps of {what} after {min(args.warmup, 1)} warm-up, FP64 C++ "
+              f"restatement, {nopt} OpenMP threads")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": k, "warmup": min(args.warmup, 1), "ms_per_step": 1000 * dt / max(k, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded)", "config": workload_config(scn, args.size),
+            "data": "synthetic (seeded)", "config": cfg,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": nopt, "kind": "port",
                              "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -172,20 +230,63 @@ def reference_arm(args):
 
 
 # --------------------------------------------------------------- GPU runs
-def transfer_bytes(state, lc, la, isdry):
+DBL_IN = ("p", "hp", "hu", "hv", "uhdye", "vhdxe", "sub", "svb", "sbx", "sby", "fcaxe", "fcaye",
+          "fxe", "fye", "tsx", "tsy", "tbx", "tby", "qsume", "qdwaste", "vdwaste")
+INT_IO = ("lmaskdry", "iscdry", "lopenbcdry", "natdry")
+DBL_OUT = ("p", "hp", "h1p", "hu", "hv", "uhdye", "vhdxe", "sub", "svb", "sbx", "sby", "uhe",
+           "vhe", "hpi", "hui", "hvi", "qdwaste", "vdwaste")
+
+
+def transfer_bytes(state, lc, la):
     """Bytes efdc_xm_step moves per call for a Fortran-shim-like field set:
     uploads LC elements of every input/in-out array, downloads LA-1 elements of
     every output/in-out array (mirrors efdc_xm_upload/efdc_xm_download)."""
-    dbl_in = ["p", "hp", "hu", "hv", "uhdye", "vhdxe", "sub", "svb", "sbx", "sby",
-              "fcaxe", "fcaye", "fxe", "fye", "tsx", "tsy", "tbx", "tby", "qsume", "qdwaste",
-              "vdwaste"]
-    int_in = ["lmaskdry", "iscdry", "lopenbcdry", "natdry"]
-    dbl_out = ["p", "hp", "h1p", "hu", "hv", "uhdye", "vhdxe", "sub", "svb", "sbx", "sby",
-               "uhe", "vhe", "hpi", "hui", "hvi", "qdwaste", "vdwaste"]
     nb = sum(len(v) for v in state["pser"].values())
-    h2d = lc * (8 * len(dbl_in) + 4 * len(int_in)) + 8 * nb
-    d2h = (la - 1) * (8 * len(dbl_out) + 4 * len(int_in))
+    h2d = lc * (8 * len(DBL_IN) + 4 * len(INT_IO)) + 8 * nb
+    d2h = (la - 1) * (8 * len(DBL_OUT) + 4 * len(INT_IO))
     return h2d, d2h
+
+
+def pinned_states(torch, scns):
+    """Copies of the members' states in one pinned host allocation."""
+    items = []
+    for s in scns:
+        for k, v in s.state.items():
+            if isinstance(v, np.ndarray):
+                items.append(v)
+    total = sum((v.nbytes + 63) // 64 * 64 for v in items)
+    buf = torch.empty(total, dtype=torch.uint8, pin_memory=True).numpy()
+    off = 0
+    out = []
+    for s in scns:
+        st = {}
+        for k, v in s.state.items():
+            if isinstance(v, np.ndarray):
+                a = buf[off:off + v.nbytes].view(v.dtype).reshape(v.shape)
+                a[...] = v
+                st[k] = a
+                off += (v.nbytes + 63) // 64 * 64
+        st["pser"] = {q: a.copy() for q, a in s.state["pser"].items()}
+        out.append(st)
+    return out, buf
+
+
+class Timer:
+    """CUDA events on the solver's stream around one region."""
+
+    def __init__(self, torch, stream):
+        self.torch, self.stream = torch, stream
+
+    def __enter__(self):
+        self.e0 = self.torch.cuda.Event(enable_timing=True)
+        self.e1 = self.torch.cuda.Event(enable_timing=True)
+        self.e0.record(self.stream)
+        return self
+
+    def __exit__(self, *a):
+        self.e1.record(self.stream)
+        self.e1.synchronize()
+        self.ms = self.e0.elapsed_time(self.e1)
 
 
 def ours(args):
@@ -193,7 +294,7 @@ def ours(args):
     import torch.distributed as dist
     rank, local, world = dist_env()
     if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=900))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
@@ -201,68 +302,196 @@ def ours(args):
         if world > 1:
             dist.barrier()
 
-    scn = S.config2(n=args.size)
-    sol = X.Solver(scn.grid, device=local)
-    stream = torch.cuda.ExternalStream(sol.stream(), device=dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    lib = sol.lib
+    def max_over_ranks(*vals):
+        if world == 1:
+            return vals
+        t = torch.tensor(vals, dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return tuple(float(x) for x in t)
+
+    def sum_over_ranks(*vals):
+        if world == 1:
+            return vals
+        t = torch.tensor(vals, dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return tuple(float(x) for x in t)
+
+    lib = X.load()
+    peak, peak_kind = measured_peaks()
+    ck = Clocks(local)
+
+    # ---------------- the headline ensemble (or the basin) ----------------
+    if args.workload == "ensemble":
+        seed = 3 + 1000 * rank
+        scns = ensemble(args.members, seed)
+        cfg = ensemble_config(scns, seed)
+    else:
+        scns = [S.config2(n=args.size)]
+        cfg = basin_config(scns[0], args.size)
+    cells = np.array([s.ncell for s in scns], dtype=np.int64)
+    M = len(scns)
+    bs = X.BatchSolver([s.grid for s in scns], device=local)
+    stream = torch.cuda.ExternalStream(bs.stream(), device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if M == 1 else None
 
     def params(n, prec):
-        return X.make_params(scn.params, n=n, tn=scn.tn(n), precision=prec)
+        return [X.make_params(s.params, n=n, tn=s.tn(n), precision=prec) for s in scns]
 
-    def run(prec, steps, warmup):
-        st = scn.copy_state()
-        sol.upload(st)
+    def run_batch(prec, steps, warmup):
+        bs.upload([s.state for s in scns])
         n = 0
         for _ in range(warmup):
             n += 1
-            s = sol.step_device(params(n, prec))
-            assert s.status in (X.OK, X.NEG_DEPTH), s.as_dict()
+            for st in bs.step_device(params(n, prec)):
+                assert st.status in (X.OK, X.NEG_DEPTH), st.as_dict()
         barrier()
         torch.cuda.synchronize()
         l0 = lib.efdc_xm_kernel_launches()
-        times, iters, outer = [], [], []
+        times, iters, outer = [], np.zeros(M, np.int64), 0
+        per_step_iters = []
         for _ in range(steps):
             n += 1
-            with torch.cuda.stream(stream):
-                flush.zero_()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            s = sol.step_device(params(n, prec))
-            e1.record(stream)
-            e1.synchronize()
-            assert s.status in (X.OK, X.NEG_DEPTH), s.as_dict()
-            times.append(e0.elapsed_time(e1))
-            iters.append(s.iters_total)
-            outer.append(s.outer_refinements)
+            if flush is not None:
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+            prm = params(n, prec)
+            with Timer(torch, stream) as tm:
+                sts = bs.step_device(prm)
+            for m, st in enumerate(sts):
+                assert st.status in (X.OK, X.NEG_DEPTH), (m, st.as_dict())
+            it = np.array([st.iters_total for st in sts], dtype=np.int64)
+            iters += it
+            per_step_iters.append(it)
+            outer += sum(st.outer_refinements for st in sts)
+            times.append(tm.ms)
         torch.cuda.synchronize()
         barrier()
         launches = lib.efdc_xm_kernel_launches() - l0
-        out = scn.copy_state()
-        sol.download(out)
-        return dict(times=times, iters=iters, outer=outer, launches=launches, state=out)
+        out = [{"p": np.zeros(s.lc)} for s in scns]
+        bs.download(out)
+        return dict(times=times, iters=iters, per_step=per_step_iters, outer=outer,
+                    launches=launches, p=[o["p"] for o in out])
 
-    ck = Clocks(local)
-    r64 = run(X.PREC_FP64, args.steps, args.warmup)
-    rmx = run(X.PREC_MIXED, args.steps, args.warmup)
-    clocks = ck.stop()
-    cells = scn.ncell
-    credit = cells * sum(r64["iters"])  # FP64 iterations of the same steps
-    t_mx = sum(rmx["times"]) / 1000.0
-    t_64 = sum(r64["times"]) / 1000.0
-    if world > 1:
-        tt = torch.tensor([t_mx, t_64], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_mx, t_64 = float(tt[0]), float(tt[1])
-    value = world * credit / t_mx
-    fp64_value = world * credit / t_64
-    eta_err = float(np.abs(rmx["state"]["p"][1:scn.la] - r64["state"]["p"][1:scn.la]).max() / S.G)
+    r64 = run_batch(X.PREC_FP64, args.steps, args.warmup)
+    rmx = run_batch(X.PREC_MIXED, args.steps, args.warmup)
 
-    # roofline of the dominant kernel on the last assembled (mixed) system
-    kt = sol.time_kernels(X.PREC_MIXED, reps=20)
-    kt64 = sol.time_kernels(X.PREC_FP64, reps=20)
-    peak, peak_kind = measured_peaks()
+    # elevation error of the MIXED solver against the FP64 solve of the same
+    # input: one step from the FP64 run's final state in each precision
+    def one_step(prec, state_src, n, rsqm_scale=1.0):
+        bs.upload(state_src)
+        prm = params(n, prec)
+        for pp in prm:
+            pp.rsqm *= rsqm_scale
+        bs.step_device(prm)
+        out = [{"p": np.zeros(s.lc)} for s in scns]
+        bs.download(out)
+        return [o["p"] for o in out]
+
+    full = [s.copy_state() for s in scns]
+    bs.upload([s.state for s in scns])
+    n_end = args.warmup + args.steps
+    for k in range(n_end):  # FP64 trajectory to the end of the timed run
+        bs.step_device(params(k + 1, X.PREC_FP64))
+    bs.download(full)
+    p64 = one_step(X.PREC_FP64, full, n_end + 1)
+    pmx = one_step(X.PREC_MIXED, full, n_end + 1)
+    step_err = max(float(np.abs(a[1:s.la] - b[1:s.la]).max()) for a, b, s in
+                   zip(pmx, p64, scns)) / S.G
+    # the FP64 solver's own sensitivity to its stop: RSQM/10 over the timed run
+    bs.upload([s.state for s in scns])
+    for k in range(n_end):
+        prm = params(k + 1, X.PREC_FP64)
+        for pp in prm:
+            pp.rsqm *= 0.1
+        bs.step_device(prm)
+    tight = [{"p": np.zeros(s.lc)} for s in scns]
+    bs.download(tight)
+    drift64 = max(float(np.abs(a["p"][1:s.la] - b[1:s.la]).max()) for a, b, s in
+                  zip(tight, r64["p"], scns)) / S.G
+    credit = float((cells * r64["iters"]).sum())
+    t_mx, t_64 = max_over_ranks(sum(rmx["times"]) / 1e3, sum(r64["times"]) / 1e3)
+    credit_all, = sum_over_ranks(credit)
+    value = credit_all / t_mx
+    fp64_batched = credit_all / t_64
+    eta_err = max(float(np.abs(a[1:s.la] - b[1:s.la]).max()) for a, b, s in
+                  zip(rmx["p"], r64["p"], scns)) / S.G
+    # dominant kernel, live: on the last (mixed) system of every member
+    kt = bs.time_kernels(X.PREC_MIXED, reps=20)
+    kt64 = bs.time_kernels(X.PREC_FP64, reps=20)
+
+    # ---------------- plain FP64 drop-in: one context per basin ----------------
+    dropin = None
+    if args.dropin_steps > 0 and M > 1:
+        sols = [X.Solver(s.grid, device=local) for s in scns]
+        for sol, s in zip(sols, scns):
+            sol.upload(s.state)
+        n = 0
+        for _ in range(args.warmup):
+            n += 1
+            for sol, s in zip(sols, scns):
+                sol.step_device(X.make_params(s.params, n=n, tn=s.tn(n)))
+        torch.cuda.synchronize()
+        barrier()
+        s_first = torch.cuda.ExternalStream(sols[0].stream(), device=dev)
+        s_last = torch.cuda.ExternalStream(sols[-1].stream(), device=dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        d_credit = 0.0
+        mismatch = 0
+        e0.record(s_first)
+        for k in range(args.dropin_steps):
+            n += 1
+            for m, (sol, s) in enumerate(zip(sols, scns)):
+                st = sol.step_device(X.make_params(s.params, n=n, tn=s.tn(n)))
+                d_credit += s.ncell * st.iters_total
+                if k < len(r64["per_step"]):
+                    mismatch += int(st.iters_total != r64["per_step"][k][m])
+        e1.record(s_last)
+        e1.synchronize()
+        t_d, = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        d_credit_all, = sum_over_ranks(d_credit)
+        dropin = {"value": d_credit_all / t_d, "steps": args.dropin_steps,
+                  "ms_per_step": 1000 * t_d / args.dropin_steps,
+                  "iteration_count_mismatches_vs_batched_fp64": mismatch,
+                  "how": "efdc_xm_step_device per member per step, one context per basin, "
+                         "state resident, the same steps as the first timed batched steps"}
+        for sol in sols:
+            sol.close()
+        del sols
+
+    # ---------------- e2e through efdc_xm_step_batch with pinned host arrays ----------------
+    e2e = None
+    if args.e2e_steps > 0:
+        pst, _buf = pinned_states(torch, scns)
+        h2d = d2h = 0
+        for st, s in zip(pst, scns):
+            a, b = transfer_bytes(st, s.lc, s.la)
+            h2d += a
+            d2h += b
+        # the same warm-up as the device-resident runs, so that timed e2e step
+        # k is timed FP64 step k (whose iteration counts are the credit)
+        n = 0
+        for _ in range(max(1, args.warmup)):
+            n += 1
+            bs.step(params(n, X.PREC_MIXED), pst)
+        torch.cuda.synchronize()
+        barrier()
+        tms, cred = [], 0.0
+        for k in range(args.e2e_steps):
+            n += 1
+            with Timer(torch, stream) as tm:
+                bs.step(params(n, X.PREC_MIXED), pst)
+            tms.append(tm.ms)
+            cred += float((cells * r64["per_step"][min(k, len(r64["per_step"]) - 1)]).sum())
+        t_e, = max_over_ranks(sum(tms) / 1e3)
+        cred_all, = sum_over_ranks(cred)
+        e2e = {"value": cred_all / t_e, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": 1000 * t_e / len(tms),
+               "steps": len(tms), "host_buffers": "pinned (one torch pin_memory block)",
+               "api": "efdc_xm_step_batch"}
+        del pst, _buf
+
+    # ---------------- roofline of the dominant kernel ----------------
     # algorithmic bytes per water cell: the FP32 matvec of the Jacobi-scaled
     # system reads r, p_old, AS, AW and writes p_new, Ap (6 x 4 B); the FP64
     # drop-in's reads r, CCC, p_old, CCS, CCW and writes p_new, Ap (7 x 8 B)
@@ -275,85 +504,103 @@ def ours(args):
         t = tj.get("k_mx_matvec")
         if t and "k_mx_matvec" not in tj.get("stale_for", []):
             traffic = float(t["dram_bytes_per_cell"]) * kt.ncells
-    roof = {"bound": "hbm", "kernel": "k_mx_matvec (FP32 p-update + Ahat*p + p.Ap)",
+    roof = {"bound": "hbm", "kernel": "k_mx_matvec (FP32 p-update + Ahat*p + p.Ap, all members)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_kind": peak_kind, "traffic": traffic,
             "ms_per_launch": kt.ms_matvec, "bytes_per_launch": bytes_mv,
+            "cells_per_launch": kt.ncells, "slots_per_launch": kt.nslots,
             "update_kernel": {"ms_per_launch": kt.ms_update, "bytes_per_launch": 24.0 * kt.ncells,
                               "achieved": 24.0 * kt.ncells / (kt.ms_update * 1e-3) / 1e9},
             "fp64_matvec": {"ms_per_launch": kt64.ms_matvec, "bytes_per_launch": 56.0 * kt.ncells,
                             "achieved": 56.0 * kt.ncells / (kt64.ms_matvec * 1e-3) / 1e9}}
+    bs.close()
+    del bs
 
-    # e2e: efdc_xm_step with pinned host arrays, mixed precision
-    e2e = None
-    if args.e2e_steps > 0:
-        st = scn.copy_state()
-        pinned = {}
-        for k, v in st.items():
-            if isinstance(v, np.ndarray):
-                t = torch.empty(v.shape, dtype=torch.float64 if v.dtype == np.float64 else torch.int32,
-                                pin_memory=True)
-                a = t.numpy()
-                a[...] = v
-                pinned[k] = (t, a)
-        pst = {k: a for k, (t, a) in pinned.items()}
-        pst["pser"] = st["pser"]
-        h2d, d2h = transfer_bytes(pst, scn.lc, scn.la, scn.params["isdry"])
-        n = 0
-        for _ in range(1):
-            n += 1
-            sol.step(params(n, X.PREC_MIXED), pst)
-        torch.cuda.synchronize()
-        barrier()
-        tms = []
-        its = []
-        for k in range(args.e2e_steps):
-            n += 1
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            s = sol.step(params(n, X.PREC_MIXED), pst)
-            e1.record(stream)
-            e1.synchronize()
-            tms.append(e0.elapsed_time(e1))
-            its.append(r64["iters"][min(k, len(r64["iters"]) - 1)])
-        t_e = sum(tms) / 1000.0
-        if world > 1:
-            tt = torch.tensor([t_e], dtype=torch.float64, device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t_e = float(tt[0])
-        e2e = {"value": world * cells * sum(its) / t_e, "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "ms_per_step": 1000 * t_e / len(tms),
-               "steps": len(tms), "host_buffers": "pinned (torch pin_memory)"}
+    # ---------------- single-domain side measurement ----------------
+    single = None
+    if args.workload == "ensemble" and args.basin_steps > 0:
+        scn = S.config2(n=2048)
+        sol = X.Solver(scn.grid, device=local)
+        sstream = torch.cuda.ExternalStream(sol.stream(), device=dev)
+        fl = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
+        def run1(prec):
+            sol.upload(scn.state)
+            n = 0
+            for _ in range(args.warmup):
+                n += 1
+                sol.step_device(X.make_params(scn.params, n=n, tn=scn.tn(n), precision=prec))
+            torch.cuda.synchronize()
+            ts, its = [], []
+            for _ in range(args.basin_steps):
+                n += 1
+                with torch.cuda.stream(sstream):
+                    fl.zero_()
+                with Timer(torch, sstream) as tm:
+                    st = sol.step_device(X.make_params(scn.params, n=n, tn=scn.tn(n),
+                                                       precision=prec))
+                ts.append(tm.ms)
+                its.append(st.iters_total)
+            return sum(ts) / 1e3, its
+
+        t64b, it64 = run1(X.PREC_FP64)
+        tmxb, _ = run1(X.PREC_MIXED)
+        kb = sol.time_kernels(X.PREC_MIXED, reps=20)
+        t64b, tmxb = max_over_ranks(t64b, tmxb)
+        cb, = sum_over_ranks(float(scn.ncell * sum(it64)))
+        single = {"config": basin_config(scn, 2048), "steps": args.basin_steps,
+                  "value": cb / tmxb, "fp64_value": cb / t64b, "speedup_vs_fp64": t64b / tmxb,
+                  "ms_per_step": 1000 * tmxb / args.basin_steps,
+                  "fp64_ms_per_step": 1000 * t64b / args.basin_steps,
+                  "k_mx_matvec_ms": kb.ms_matvec,
+                  "k_mx_matvec_frac": 24.0 * kb.ncells / (kb.ms_matvec * 1e-3) / 1e9 / peak}
+        sol.close()
+        del fl
+    clocks = ck.stop()
+
+    # ---------------- CPU baseline (rank 0, N=1) ----------------
     cpu = None
-    if rank == 0 and not args.no_cpu:
-        v, k, dt, nopt = cpu_run(scn, seconds=args.cpu_seconds, max_steps=50)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        samp = cpu_sample(scns) if M > 1 else scns
+        v, k, dt, nopt = cpu_run(samp, seconds=args.cpu_seconds, max_steps=50)
         cpu = {"value": v, "unit": UNIT, "cores": nopt, "kind": "port",
-               "sample": f"{k} CALPUV2C steps of the same basin ({cells} cells), FP64 C++ "
-                         f"restatement of CALPUV2C/CONGRAD, {nopt} OpenMP threads, {dt:.1f} s"}
+               "sample": f"{k} CALPUV2C steps of {len(samp)} basins "
+                         f"({sum(s.ncell for s in samp)} cells), FP64 C++ restatement of "
+                         f"CALPUV2C/CONGRAD, {nopt} OpenMP threads, {dt:.1f} s"}
 
     if rank == 0:
-        cfg = workload_config(scn, args.size)
+        cfg["parallelism"] = (f"{world} GPUs, each its own ensemble (members shard, no exchange)"
+                              if world > 1 else "single GPU")
         cfg["tiles_32x8"] = kt.nslots // 256
-        cfg["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000 * t_mx / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement",
             "data": "synthetic (seeded)", "config": cfg,
-            "fp64_value": fp64_value, "speedup_vs_fp64": value / fp64_value,
-            "fp64_ms_per_step": 1000 * t_64 / args.steps,
-            "iters_fp64_total": int(sum(r64["iters"])), "iters_mixed_inner_total": int(sum(rmx["iters"])),
-            "outer_refinements_per_step": float(np.mean(rmx["outer"])),
-            "max_eta_diff_mixed_vs_fp64_m": eta_err,
-            "solves_per_s": world * args.steps / t_mx, "cell_steps_per_s": world * cells * args.steps / t_mx,
+            "fp64_batched_value": fp64_batched,
+            "fp64_dropin_value": dropin["value"] if dropin else None,
+            "speedup_vs_fp64_dropin": value / dropin["value"] if dropin else None,
+            "speedup_vs_fp64_batched": value / fp64_batched,
+            "fp64_batched_ms_per_step": 1000 * t_64 / args.steps,
+            "fp64_dropin": dropin,
+            "iters_fp64_total": int(r64["iters"].sum()),
+            "iters_mixed_inner_total": int(rmx["iters"].sum()),
+            "outer_refinements_per_member_step": rmx["outer"] / (args.steps * M),
+            "eta_err_per_step_mixed_vs_fp64_m": step_err,
+            "eta_drift_after_run_mixed_vs_fp64_m": eta_err,
+            "eta_drift_after_run_fp64_rsqm_div10_vs_fp64_m": drift64,
+            "eta_note": "per step: one step from the same FP64 state in each precision "
+                        "(the 1e-6 m bar); after run: free-running trajectories, MIXED stops "
+                        "at 0.1*RSQM and FP64 at RSQM, so the drift is FP64's own truncation, "
+                        "of the size FP64 drifts from itself when RSQM is divided by 10",
+            "solves_per_s": world * M * args.steps / t_mx,
+            "cell_steps_per_s": world * float(cells.sum()) * args.steps / t_mx,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(rmx["launches"]), "clocks": clocks,
+            "single_domain": single,
         }
         print(json.dumps(line), flush=True)
-    sol.close()
     if world > 1:
         dist.destroy_process_group()
 

@@ -670,6 +670,7 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   S.tend = tend_d;
   S.sc = c->sc;
   S.nquad = c->nquad;
+  S.nmember = M;
   double *st[18];
   for (double *&p : st) p = D();
   S.dxyp = st[0]; S.dxyip = st[1]; S.dxiu = st[2]; S.dyiu = st[3]; S.dxiv = st[4];
@@ -1210,10 +1211,9 @@ int32_t efdc_xm_time_kernels(efdc_xm_ctx *c, int32_t precision, int32_t reps, ef
   CK(cudaSetDevice(c->device));
   const xm::Launch l = c->L();
   const bool mixed = precision == EFDC_XM_PREC_MIXED;
-  cudaEvent_t ev[3];
-  for (auto &e : ev) CK(cudaEventCreate(&e));
-  double tm = 0, tu = 0;
-  // the iterations run on a scratch copy of P with the stop tests disabled
+  // the iterations run on a scratch copy of P with the stop tests disabled;
+  // all launches are queued back to back (one untimed warm-up pair first),
+  // so the events bracket device execution only, not host launch latency
   CK(cudaMemcpyAsync(c->ptmp, c->X.p, size_t(c->nslot) * sizeof(double), cudaMemcpyDeviceToDevice,
                      c->stream));
   for (int m = 0; m < c->M; ++m) c->act_h[m] = 1;
@@ -1225,22 +1225,30 @@ int32_t efdc_xm_time_kernels(efdc_xm_ctx *c, int32_t precision, int32_t reps, ef
   else
     xm::launch_cg_init(l, c->S, c->Y, c->ptmp, c->ctl, c->glob, c->part);
   CK(cudaGetLastError());
-  for (int k = 0; k < reps; ++k) {
-    CK(cudaEventRecord(ev[0], c->stream));
+  std::vector<cudaEvent_t> ev(2 * reps + 1);
+  for (auto &e : ev) CK(cudaEventCreate(&e));
+  auto pair = [&](int k) {
     if (mixed) {
       xm::launch_mx_matvec(l, c->S, c->Y, c->ctl, c->part);
-      CK(cudaEventRecord(ev[1], c->stream));
+      if (k >= 0) cudaEventRecord(ev[2 * k + 1], c->stream);
       xm::launch_mx_update(l, c->S, c->Y, c->ctl, c->glob, c->part, 1);
     } else {
       xm::launch_cg_matvec(l, c->S, c->Y, c->ctl, c->part);
-      CK(cudaEventRecord(ev[1], c->stream));
+      if (k >= 0) cudaEventRecord(ev[2 * k + 1], c->stream);
       xm::launch_cg_update(l, c->S, c->Y, c->ptmp, c->ctl, c->glob, c->part, 1);
     }
-    CK(cudaEventRecord(ev[2], c->stream));
-    CK(cudaEventSynchronize(ev[2]));
+    if (k >= 0) cudaEventRecord(ev[2 * k + 2], c->stream);
+  };
+  pair(-1);
+  CK(cudaEventRecord(ev[0], c->stream));
+  for (int k = 0; k < reps; ++k) pair(k);
+  CK(cudaGetLastError());
+  CK(cudaEventSynchronize(ev[2 * reps]));
+  double tm = 0, tu = 0;
+  for (int k = 0; k < reps; ++k) {
     float a = 0, b = 0;
-    CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
-    CK(cudaEventElapsedTime(&b, ev[1], ev[2]));
+    CK(cudaEventElapsedTime(&a, ev[2 * k], ev[2 * k + 1]));
+    CK(cudaEventElapsedTime(&b, ev[2 * k + 1], ev[2 * k + 2]));
     tm += a;
     tu += b;
   }

@@ -22,24 +22,21 @@ __device__ __forceinline__ double rcpT(double x) { return 1. / x; }
 // of a row takes part in the shuffles.  A quad whose member is finished (or
 // not in this sweep) is skipped by the whole CTA.
 //
-// Reductions: each pass leaves one partial per warp in shared memory (warp
-// shuffles only, no CTA barrier per quad).  Every QCAP quads, and at the end,
-// the CTA "flushes": it adds the warp partials of each quad in fixed warp
-// order into part[quad], publishes them with one fence, and counts its quads
-// into the member's arrival counter (one atomic per member it touched).  The
-// CTA that completes a member reduces the member's per-quad partials in
-// fixed quad order (reduce_partials) and runs the epilogue (thread 0 writes
-// the member's Ctl).  The sums therefore do not depend on the grid size or
-// on which other members share the context.
-constexpr int QCAP = 32;         // quads a CTA logs between two flushes
+// Reductions in two kernels: the CG kernel leaves one partial per warp in
+// shared memory (warp shuffles only, no CTA barrier per quad) and, every
+// QCAP quads and at its end, adds the warp partials of each quad in fixed
+// warp order into part[quad] (plain stores).  A member-reduce kernel then
+// reduces each member's per-quad partials in fixed quad order (one CTA per
+// member) and finishes the member (its Ctl).  No fences, atomics or
+// "last CTA" in the CG kernels, and sums that depend neither on the grid size
+// nor on which other members share the context.
+constexpr int QCAP = 32;         // quads a CTA logs between two stores
 constexpr int NWARP = NT / 32;   // warps per CTA
 
 template <int NS>
 struct QuadLog {
   double w[NS][QCAP][NWARP];  // per-warp partials of NS sums
   int qd[QCAP];               // quad of each entry
-  int mem[QCAP];              // its member
-  int last[QCAP];             // this CTA completed the member
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -48,9 +45,9 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-template <int NS, class Epi>
-__device__ __forceinline__ void quad_flush(QuadLog<NS> &L, int n, const DevStatic &S, Ctl *ctl,
-                                           double *part, double *sh, Epi &epi) {
+template <int NS>
+__device__ __forceinline__ void quad_store(QuadLog<NS> &L, int n, const DevStatic &S,
+                                           double *part) {
   __syncthreads();  // the warp partials and the entries are in shared memory
   const int t = threadIdx.x;
   if (t < n) {
@@ -62,68 +59,50 @@ __device__ __forceinline__ void quad_flush(QuadLog<NS> &L, int n, const DevStati
       part[size_t(s) * S.nquad + L.qd[t]] = a;
     }
   }
-  __threadfence();
-  __syncthreads();
-  if (t < n) {
-    const int m = L.mem[t];
-    int last = 0;
-    if (t == 0 || L.mem[t - 1] != m) {  // head of a run of equal members
-      int cnt = 1;
-      while (t + cnt < n && L.mem[t + cnt] == m) ++cnt;
-      const unsigned total = unsigned(S.qstart[m + 1] - S.qstart[m]);
-      const unsigned prev = atomicAdd(&ctl[m].counter, unsigned(cnt));
-      if (prev + unsigned(cnt) == total) {
-        last = 1;
-        ctl[m].counter = 0u;  // every quad of m has arrived: ready for the next kernel
-      }
-    }
-    L.last[t] = last;
-  }
-  __syncthreads();
-  for (int k = 0; k < n; ++k) {
-    if (!L.last[k]) continue;  // uniform: shared memory
-    __threadfence();
-    const int m = L.mem[k];
-    const int q0 = S.qstart[m], nq = S.qstart[m + 1] - q0;
-    double r[NS];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) r[s] = reduce_partials(part + size_t(s) * S.nquad + q0, nq, sh);
-    epi(m, r);  // r valid in thread 0
-  }
   __syncthreads();  // the log is reused after this
 }
 
 // One CG kernel over all quads.  setup(m) returns the member's values for the
-// body (a struct with at least `bool skip`); it runs when the member changes
-// from one quad to the next, so a CTA reads a member's Ctl once per run of
-// its quads.  body(a, g, valid, v) processes one quad row vector and adds its
-// parts of the NS sums to v[]; epi(m, r) finishes member m with its NS sums.
-template <int NS, class Setup, class Body, class Epi>
-__device__ __forceinline__ void quad_sweep(const DevStatic &S, Ctl *ctl, double *part,
-                                           Setup setup, Body body, Epi epi) {
+// body (a struct with at least `bool skip`).  body(a, g, valid, v) processes
+// one quad row vector and adds its parts of the NS sums to v[].
+//
+// Everything a quad's loads depend on (its table entry, its member's values
+// from setup(), the member's last tile and the thread's tile-neighbour entry)
+// is fetched one quad ahead, so that those small dependent loads overlap the
+// current quad's memory traffic instead of preceding the next one's.  In an
+// ensemble nearly every quad of a CTA belongs to another member.
+template <int NS, class Setup, class Body>
+__device__ __forceinline__ void quad_sweep(const DevStatic &S, double *part, Setup setup,
+                                           Body body) {
   __shared__ QuadLog<NS> L;
-  __shared__ double sh[32];
   const int sub = threadIdx.x / TPT, q = threadIdx.x % TPT;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int n = 0;
+  const int G = gridDim.x, NQ = S.nquad;
   int qd = blockIdx.x;
-  int2 cur = qd < S.nquad ? S.quads[qd] : make_int2(0, 0);
-  int mc = cur.x;
-  auto a = setup(mc);
-  int tend = S.tend[mc];
-  while (qd < S.nquad) {
-    const int qn = qd + gridDim.x;
-    const int2 nxt = qn < S.nquad ? S.quads[qn] : make_int2(0, 0);  // prefetch
-    const int m = cur.x;
-    if (m != mc) {
-      mc = m;
-      a = setup(m);
-      tend = S.tend[m];
+  if (qd >= NQ) return;
+  int2 cur = S.quads[qd];
+  auto a = setup(cur.x);
+  int tend = S.tend[cur.x];
+  int4 nb = __ldg(&S.tnbr[cur.y + sub < tend ? cur.y + sub : 0]);
+  int2 nxt = (qd + G < NQ) ? S.quads[qd + G] : cur;
+  int n = 0;
+  for (;;) {
+    const int qn = qd + G;
+    const bool more = qn < NQ;
+    // the next quad's descriptors
+    auto an = a;
+    int tendn = tend;
+    if (more && nxt.x != cur.x) {
+      an = setup(nxt.x);
+      tendn = S.tend[nxt.x];
     }
+    const int tin = nxt.y + sub;
+    const int4 nbn = __ldg(&S.tnbr[(more && tin < tendn) ? tin : 0]);
+    const int2 nn = (qn + G < NQ) ? S.quads[qn + G] : nxt;
     if (!a.skip) {
       const int ti = cur.y + sub;
       const bool valid = ti < tend;
-      const RowGeo g = row_geo(S.tnbr, valid ? ti : 0, q);
+      const RowGeo g = row_geo_nb(nb, valid ? ti : 0, q);
       double v[NS];
 #pragma unroll
       for (int s = 0; s < NS; ++s) v[s] = 0.0;
@@ -133,19 +112,38 @@ __device__ __forceinline__ void quad_sweep(const DevStatic &S, Ctl *ctl, double 
         const double x = warp_sum(v[s]);
         if (lane == 0) L.w[s][n][warp] = x;
       }
-      if (threadIdx.x == 0) {
-        L.qd[n] = qd;
-        L.mem[n] = m;
-      }
+      if (threadIdx.x == 0) L.qd[n] = qd;
       if (++n == QCAP) {
-        quad_flush<NS>(L, n, S, ctl, part, sh, epi);
+        quad_store<NS>(L, n, S, part);
         n = 0;
       }
     }
+    if (!more) break;
     qd = qn;
     cur = nxt;
+    a = an;
+    tend = tendn;
+    nb = nbn;
+    nxt = nn;
   }
-  if (n) quad_flush<NS>(L, n, S, ctl, part, sh, epi);
+  if (n) quad_store<NS>(L, n, S, part);
+}
+
+// The member-reduce kernels: member m (one CTA per member, grid-stride) sums
+// its quads' partials of each of the NS sums in fixed order and, unless
+// skip(m), epi(m, r) finishes it (r valid in thread 0).
+template <int NS, class Skip, class Epi>
+__device__ __forceinline__ void member_reduce(const DevStatic &S, const double *part, Skip skip,
+                                              Epi epi) {
+  __shared__ double sh[32];
+  for (int m = blockIdx.x; m < S.nmember; m += gridDim.x) {
+    if (skip(m)) continue;  // uniform
+    const int q0 = S.qstart[m], nq = S.qstart[m + 1] - q0;
+    double r[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) r[s] = reduce_partials(part + size_t(s) * S.nquad + q0, nq, sh);
+    epi(m, r);
+  }
 }
 
 // The same loop without reductions (member-wise vector updates).

@@ -73,11 +73,20 @@ __device__ __forceinline__ bool arrive_last(unsigned int *counter) {
   return last;
 }
 
-// Fixed-order sum of nblk partials by the last CTA: thread i adds partials
+// Fixed-order sum of nblk partials by one CTA: thread i adds partials
 // i, i+NT, ... in order, then the fixed block tree.  Deterministic.
 __device__ __forceinline__ double reduce_partials(const double *part, int nblk, double *sh) {
   double s = 0.0;
-  for (int i = threadIdx.x; i < nblk; i += NT) s += __ldcg(&part[i]);
+  for (int base = 0; base < nblk; base += 8 * NT) {
+    double v[8];  // a pass's loads are all issued before the (ordered) adds
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int i = base + j * NT + int(threadIdx.x);
+      v[j] = (i < nblk) ? __ldcg(&part[i]) : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s += v[j];
+  }
   return block_sum(s, sh);
 }
 
@@ -106,9 +115,9 @@ struct RowGeo {
   int cx;      // column group 0..7
 };
 
-__device__ __forceinline__ RowGeo row_geo(const int4 *__restrict__ tnbr, int tile, int q) {
+// nb = tnbr[tile], the (w, e, s, n) neighbour tiles
+__device__ __forceinline__ RowGeo row_geo_nb(const int4 nb, int tile, int q) {
   const int cx = q & (ROWT - 1), ty = q / ROWT;
-  const int4 nb = __ldg(&tnbr[tile]);  // (w, e, s, n)
   RowGeo g;
   g.cx = cx;
   g.d0 = tile * TILE + ty * TX + cx * CPT;
@@ -117,6 +126,10 @@ __device__ __forceinline__ RowGeo row_geo(const int4 *__restrict__ tnbr, int til
   g.dwe = nb.x * TILE + ty * TX + (TX - 1);
   g.dee = nb.y * TILE + ty * TX;
   return g;
+}
+
+__device__ __forceinline__ RowGeo row_geo(const int4 *__restrict__ tnbr, int tile, int q) {
+  return row_geo_nb(__ldg(&tnbr[tile]), tile, q);
 }
 
 template <class T>

@@ -76,6 +76,7 @@ struct DevStatic {
   const int *tend;        // [M] one past the member's last tile
   const StepScalars *sc;  // [M] per-member scalars of the current step
   int nquad;
+  int nmember;
   const double *dxyp, *dxyip, *dxiu, *dyiu, *dxiv, *dyiv, *dxyu, *dxyv;
   const double *hruo, *hrvo, *subo, *svbo, *sbxo, *sbyo, *belv;
   const double *rcx;      // RCX = RCY: 1 on water, 0 on ghosts (calpuv2c.f90:97-102)

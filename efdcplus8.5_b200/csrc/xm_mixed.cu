@@ -15,8 +15,8 @@ namespace xm {
 #define TILE_LOOP(ntile)                                                      \
   for (int tile = blockIdx.x + 1; tile < (ntile); tile += gridDim.x)
 
-// p = r + beta*p_old at the cell and its halo, Ahat*p, p.Ap, ALPHA (per member).
-__global__ void __launch_bounds__(NT, 5) k_mx_matvec(DevStatic S, DevSystem Y, Ctl *ctl,
+// p = r + beta*p_old at the cell and its halo, Ahat*p, p.Ap (per member).
+__global__ void __launch_bounds__(NT, 5) k_mx_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
                                                     double *part) {
   struct A {
     bool skip, asym;
@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(NT, 5) k_mx_matvec(DevStatic S, DevSystem Y, C
     float *pnew;
   };
   quad_sweep<1>(
-      S, ctl, part,
+      S, part,
       [&](int m) {
         const Ctl &k = ctl[m];
         const bool par = k.parity;
@@ -35,7 +35,12 @@ __global__ void __launch_bounds__(NT, 5) k_mx_matvec(DevStatic S, DevSystem Y, C
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         v[0] = matvec_row_scaled(g, valid, Y.r32, a.pold, a.pnew, Y.as32, Y.aw32, Y.ae32, Y.an32,
                                  Y.ap32, a.beta, a.asym);
-      },
+      });
+}
+// ALPHA = RPCG / p.Ap
+__global__ void __launch_bounds__(NT) k_red_mx_matvec(DevStatic S, Ctl *ctl, const double *part) {
+  member_reduce<1>(
+      S, part, [&](int m) { return (ctl[m].done | ctl[m].idone) != 0; },
       [&](int m, const double *sum) {
         if (threadIdx.x != 0) return;
         ctl[m].papcg = sum[0];
@@ -44,24 +49,31 @@ __global__ void __launch_bounds__(NT, 5) k_mx_matvec(DevStatic S, DevSystem Y, C
 }
 
 // x += alpha*p, r -= alpha*Ap, r.r (FP64 sums; = r.z on the unit-diagonal
-// system), BETA and the inner stop test.  With no_stop the inner solve runs
-// past its target (kernel timing only).
-__global__ void __launch_bounds__(NT) k_mx_update(DevStatic S, DevSystem Y, Ctl *ctl, Glob *glob,
-                                                 double *part, double total_cap_fac, int no_stop) {
+// system).
+__global__ void __launch_bounds__(NT) k_mx_update(DevStatic S, DevSystem Y, const Ctl *ctl,
+                                                 double *part) {
   struct A {
     bool skip;
     float alpha;
     const float *pnew;
   };
   quad_sweep<1>(
-      S, ctl, part,
+      S, part,
       [&](int m) {
         const Ctl &k = ctl[m];
         return A{(k.done | k.idone) != 0, float(k.alpha), k.parity ? Y.pa32 : Y.pb32};
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         update_row_scaled(g, valid, Y.x32, a.pnew, Y.r32, Y.ap32, a.alpha, v[0]);
-      },
+      });
+}
+// BETA and the inner stop test.  With no_stop the inner solve runs past its
+// target (kernel timing only).
+__global__ void __launch_bounds__(NT) k_red_mx_update(DevStatic S, Ctl *ctl, Glob *glob,
+                                                     const double *part, double total_cap_fac,
+                                                     int no_stop) {
+  member_reduce<1>(
+      S, part, [&](int m) { return (ctl[m].done | ctl[m].idone) != 0; },
       [&](int m, const double *sum) {
         if (threadIdx.x != 0) return;
         Ctl &k = ctl[m];
@@ -87,15 +99,19 @@ __global__ void __launch_bounds__(NT) k_mx_update(DevStatic S, DevSystem Y, Ctl 
       });
 }
 
+static int reduce_grid(const DevStatic &S) { return std::min(S.nmember, 1024); }
+
 void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {
   k_mx_matvec<<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
-  count_launches(1);
+  k_red_mx_matvec<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part);
+  count_launches(2);
 }
 void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       Glob *glob, double *part, int no_stop) {
-  k_mx_update<<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, glob, part, 2.0, no_stop);
-  count_launches(1);
+  k_mx_update<<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part);
+  k_red_mx_update<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, 2.0, no_stop);
+  count_launches(2);
 }
 void launch_mx_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl, Glob *glob,
                     double *part) {

@@ -315,12 +315,12 @@ __global__ void k_outer_reset(Glob *glob) { glob->nidone = 0; }
 
 // :54-88 initial residual, z0 = CCCI*r, RPCG.
 __global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double *P, Ctl *ctl,
-                                               Glob *glob, double *part) {
+                                               double *part) {
   struct A {
     bool skip, asym;
   };
   quad_sweep<1>(
-      S, ctl, part, [&](int m) { return A{ctl[m].done != 0, ctl[m].asym != 0}; },
+      S, part, [&](int m) { return A{ctl[m].done != 0, ctl[m].asym != 0}; },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         const V4<double> r = residual_row(g, S.kind, P, Y, a.asym);
         const V4<double> c = ld4(Y.ccc + g.d0);
@@ -331,7 +331,12 @@ __global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double
           st4(Y.pa + g.d0, z);
           v[0] = r.x * z.x + r.y * z.y + r.z * z.z + r.w * z.w;
         }
-      },
+      });
+}
+__global__ void __launch_bounds__(NT) k_red_cg_init(DevStatic S, Ctl *ctl, Glob *glob,
+                                                   const double *part) {
+  member_reduce<1>(
+      S, part, [&](int m) { return ctl[m].done != 0; },
       [&](int m, const double *sum) {
         if (threadIdx.x != 0) return;
         Ctl &k = ctl[m];
@@ -351,7 +356,7 @@ __global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double
 }
 
 // :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA).
-__global__ void __launch_bounds__(NT) k_cg_matvec(DevStatic S, DevSystem Y, Ctl *ctl,
+__global__ void __launch_bounds__(NT) k_cg_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
                                                  double *part) {
   struct A {
     bool skip, asym;
@@ -360,7 +365,7 @@ __global__ void __launch_bounds__(NT) k_cg_matvec(DevStatic S, DevSystem Y, Ctl 
     double *pnew;
   };
   quad_sweep<1>(
-      S, ctl, part,
+      S, part,
       [&](int m) {
         const Ctl &k = ctl[m];
         const bool par = k.parity;
@@ -369,7 +374,11 @@ __global__ void __launch_bounds__(NT) k_cg_matvec(DevStatic S, DevSystem Y, Ctl 
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         v[0] = matvec_row<double>(g, valid, Y.r, Y.ccc, a.pold, a.pnew, Y.ccs, Y.ccw, Y.cce, Y.ccn,
                                   Y.ap, a.beta, a.asym);
-      },
+      });
+}
+__global__ void __launch_bounds__(NT) k_red_cg_matvec(DevStatic S, Ctl *ctl, const double *part) {
+  member_reduce<1>(
+      S, part, [&](int m) { return ctl[m].done != 0; },
       [&](int m, const double *sum) {
         if (threadIdx.x != 0) return;
         ctl[m].papcg = sum[0];
@@ -379,22 +388,27 @@ __global__ void __launch_bounds__(NT) k_cg_matvec(DevStatic S, DevSystem Y, Ctl 
 
 // :127-149 (P, RCG update, RPCGN, RSQ, BETA) and the stop test :165.  With
 // no_stop the iteration continues past RSQM and ITERM (kernel timing only).
-__global__ void __launch_bounds__(NT, 5) k_cg_update(DevStatic S, DevSystem Y, double *P, Ctl *ctl,
-                                                 Glob *glob, double *part, int no_stop) {
+__global__ void __launch_bounds__(NT, 5) k_cg_update(DevStatic S, DevSystem Y, double *P,
+                                                    const Ctl *ctl, double *part) {
   struct A {
     bool skip;
     double alpha;
     const double *pnew;
   };
   quad_sweep<2>(
-      S, ctl, part,
+      S, part,
       [&](int m) {
         const Ctl &k = ctl[m];
         return A{k.done != 0, k.alpha, k.parity ? Y.pa : Y.pb};
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         update_row<double>(g, valid, P, a.pnew, Y.r, Y.ap, Y.ccc, a.alpha, v[0], v[1]);
-      },
+      });
+}
+__global__ void __launch_bounds__(NT) k_red_cg_update(DevStatic S, Ctl *ctl, Glob *glob,
+                                                     const double *part, int no_stop) {
+  member_reduce<2>(
+      S, part, [&](int m) { return ctl[m].done != 0; },
       [&](int m, const double *sum) {
         if (threadIdx.x != 0) return;
         Ctl &k = ctl[m];
@@ -429,13 +443,12 @@ __global__ void __launch_bounds__(NT, 5) k_cg_update(DevStatic S, DevSystem Y, d
 // in FP64, and the FP32 scaled inner system rhat = D^-1/2 r, p0 = rhat,
 // x = 0.  rsqm_fac scales the member's RSQM (the MIXED stop, below RSQM).
 __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, DevSystem Y, const double *P,
-                                                Ctl *ctl, Glob *glob, double *part,
-                                                double rsqm_fac, double rel_tol, int no_stop) {
+                                                const Ctl *ctl, double *part) {
   struct A {
     bool skip, asym;
   };
   quad_sweep<2>(
-      S, ctl, part, [&](int m) { return A{ctl[m].done != 0, ctl[m].asym != 0}; },
+      S, part, [&](int m) { return A{ctl[m].done != 0, ctl[m].asym != 0}; },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         const V4<double> r = residual_row(g, S.kind, P, Y, a.asym);
         const V4<double> c = ld4(Y.ccc + g.d0);
@@ -449,7 +462,13 @@ __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, DevSystem Y, const
           v[1] = double(r32.x) * double(r32.x) + double(r32.y) * double(r32.y) +
                  double(r32.z) * double(r32.z) + double(r32.w) * double(r32.w);
         }
-      },
+      });
+}
+__global__ void __launch_bounds__(NT) k_red_mx_resid(DevStatic S, Ctl *ctl, Glob *glob,
+                                                    const double *part, double rsqm_fac,
+                                                    double rel_tol, int no_stop) {
+  member_reduce<2>(
+      S, part, [&](int m) { return ctl[m].done != 0; },
       [&](int m, const double *sum) {
         if (threadIdx.x != 0) return;
         Ctl &k = ctl[m];
@@ -947,33 +966,39 @@ void launch_outer_reset(const Launch &l, Glob *glob) {
   k_outer_reset<<<1, 1, 0, l.stream>>>(glob);
   count_launches(1);
 }
+// one CTA per member (grid-stride past 1024 members)
+static int reduce_grid(const DevStatic &S) { return std::min(S.nmember, 1024); }
+
 void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                     Glob *glob, double *part) {
-  k_cg_init<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, glob, part);
-  count_launches(1);
-}
-void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
-                    Glob *glob, double *part) {
-  k_cg_matvec<<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, ctl, part);
-  count_launches(1);
-  k_cg_update<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, glob, part, 0);
-  count_launches(1);
+  k_cg_init<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, part);
+  k_red_cg_init<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part);
+  count_launches(2);
 }
 void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {
   k_cg_matvec<<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, ctl, part);
-  count_launches(1);
+  k_red_cg_matvec<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part);
+  count_launches(2);
 }
 void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                       Glob *glob, double *part, int no_stop) {
-  k_cg_update<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, glob, part, no_stop);
-  count_launches(1);
+  k_cg_update<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, part);
+  k_red_cg_update<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, no_stop);
+  count_launches(2);
+}
+void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
+                    Glob *glob, double *part) {
+  launch_cg_matvec(l, S, Y, ctl, part);
+  launch_cg_update(l, S, Y, P, ctl, glob, part, 0);
 }
 void launch_mx_resid(const Launch &l, const DevStatic &S, const DevSystem &Y, const double *P,
                      Ctl *ctl, Glob *glob, double *part, double rsqm_fac, double rel_tol,
                      int no_stop) {
-  k_mx_resid<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, glob, part, rsqm_fac, rel_tol, no_stop);
-  count_launches(1);
+  k_mx_resid<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, part);
+  k_red_mx_resid<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, rsqm_fac, rel_tol,
+                                                      no_stop);
+  count_launches(2);
 }
 void launch_mx_apply(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
                      const Ctl *ctl) {

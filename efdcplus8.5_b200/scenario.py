@@ -306,7 +306,7 @@ def make_scenario(nx=100, ny=60, *, seed=1, dx=100.0, dy=100.0, land_frac=0.07,
                   mtide=1, tcp=(M2_PERIOD,), manning=0.025, u0=0.1, dt=10.0,
                   rsqm=1e-10, iterm=200, isdry=0, hdry=0.05, ndrystp=0, isbal=1,
                   datum=0.0, eta0=0.0, belv2d=None, land_mask=None, kc=4,
-                  explicit_noise=0.0, snlt=0.0, ntstbc=0):
+                  explicit_noise=0.0, snlt=0.0, ntstbc=0, fill_dead_ends=False):
     """A basin of nx*ny candidate cells inside a closed land ring.
 
     The land mask is seeded Bernoulli(land_frac) (the open-boundary column or
@@ -331,6 +331,17 @@ def make_scenario(nx=100, ny=60, *, seed=1, dx=100.0, dy=100.0, land_frac=0.07,
     if "N" in obc_sides:
         keep[-2:, :] = True
     inner |= keep
+    if fill_dead_ends:
+        # water cells with three or four land neighbours (single-cell inlets
+        # and lakes) become land, repeatedly, as grid generators do
+        while True:
+            pad = np.pad(inner, 1, constant_values=False)
+            nwet = (pad[:-2, 1:-1].astype(np.int8) + pad[2:, 1:-1] + pad[1:-1, :-2] +
+                    pad[1:-1, 2:])
+            dead = inner & (nwet <= 1) & ~keep
+            if not dead.any():
+                break
+            inner &= ~dead
     ijct[1:-1, 1:-1] = np.where(inner, WATER, LAND)
 
     if curvilinear is not None:
@@ -472,7 +483,13 @@ def config3_sizes(seed=3, members=256, lo=10_000, hi=400_000):
 
 def config3_member(k, ncell, seed=3):
     """Member k of the batched ensemble: a square-ish basin of ~ncell wet
-    cells, depth 1-40 m, Manning 0.015-0.04, M2 amplitude 0.1-1.0 m."""
+    cells, depth 1-40 m, Manning 0.015-0.04, M2 amplitude 0.1-1.0 m.
+
+    The members run without wetting/drying (ISDRY=0), where the reference
+    STOPs at the first non-positive depth.  So that the seeded members stay
+    wet, the shallowest water of a member is 3x its tidal amplitude (at least
+    1 m) and dead-end cells (single-cell inlets, in which the tidal standing
+    wave amplifies) are land."""
     rng = np.random.default_rng(seed * 100_003 + k)
     n_man = rng.uniform(0.015, 0.04)
     amp = rng.uniform(0.1, 1.0)
@@ -480,9 +497,10 @@ def config3_member(k, ncell, seed=3):
     ny = max(8, side)
     nx = max(8, int(math.ceil(ncell / 0.93 / ny)))
     return make_scenario(nx, ny, seed=seed * 7919 + k, dx=100.0, dy=100.0,
-                         land_frac=0.07, depth=(1.0, 40.0), corr_len_m=1500.0,
-                         obc_sides=("W",), amp=amp, manning=n_man, dt=10.0,
-                         rsqm=1e-10, iterm=500, isdry=0, kc=4)
+                         land_frac=0.07, depth=(max(1.0, 3.0 * amp), 40.0),
+                         corr_len_m=1500.0, obc_sides=("W",), amp=amp, manning=n_man,
+                         dt=10.0, rsqm=1e-10, iterm=500, isdry=0, kc=4,
+                         fill_dead_ends=True)
 
 
 def tidal_flat(n=1024, *, seed=5, hdry=0.05, amp=2.0, ramp=(-2.0, 15.0 / 4.0),
