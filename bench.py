@@ -30,9 +30,10 @@ finalisation), all members in one launch sequence.
   (3.4M cells, dt=5 s); ``--workload basin`` makes it the headline.
 
 --impl reference times that CPU restatement alone (the reference itself is
-Intel Fortran and cannot be built here).  With --gpus N>1 every rank advances
-its own ensemble (distinct seeds; the members shard with no exchange), and
-value is the sum over ranks divided by the slowest rank's time.
+Intel Fortran and cannot be built here).  With --gpus N>1 the ensemble has
+N x 256 members, partitioned over the ranks by wet cells (ensemble.partition;
+the members shard with no exchange), and value is the sum over ranks divided
+by the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -53,6 +54,7 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO / "efdcplus8.5_b200"))
 
 import efdc_xm as X  # noqa: E402
+import ensemble as E  # noqa: E402
 import scenario as S  # noqa: E402
 
 METRIC = "external-mode cell-iter/s on 1 B200: mixed/batched vs plain FP64 at 1e-6 m err"
@@ -90,12 +92,13 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ensemble(members, seed):
-    """The seeded ensemble (threaded: numpy releases the GIL)."""
+def ensemble(members, seed, pick=None):
+    """The seeded ensemble, or the members `pick` of it (threaded: numpy
+    releases the GIL)."""
     sizes = S.config3_sizes(seed=seed, members=members)
+    ks = range(members) if pick is None else pick
     with ThreadPoolExecutor(os.cpu_count() or 4) as ex:
-        return list(ex.map(lambda kn: S.config3_member(kn[0], int(kn[1]), seed=seed),
-                           enumerate(sizes)))
+        return list(ex.map(lambda k: S.config3_member(k, int(sizes[k]), seed=seed), ks))
 
 
 def ensemble_config(scns, seed):
@@ -303,18 +306,10 @@ def ours(args):
             dist.barrier()
 
     def max_over_ranks(*vals):
-        if world == 1:
-            return vals
-        t = torch.tensor(vals, dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return tuple(float(x) for x in t)
+        return E.max_over_ranks(vals, device=dev)
 
     def sum_over_ranks(*vals):
-        if world == 1:
-            return vals
-        t = torch.tensor(vals, dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return tuple(float(x) for x in t)
+        return E.sum_over_ranks(vals, device=dev)
 
     lib = X.load()
     peak, peak_kind = measured_peaks()
@@ -322,9 +317,13 @@ def ours(args):
 
     # ---------------- the headline ensemble (or the basin) ----------------
     if args.workload == "ensemble":
-        seed = 3 + 1000 * rank
-        scns = ensemble(args.members, seed)
+        # N GPUs: an ensemble of N x members, partitioned by wet cells
+        seed = 3
+        total = args.members * world
+        mine = E.partition(S.config3_sizes(seed=seed, members=total), world)[rank]
+        scns = ensemble(total, seed, pick=mine)
         cfg = ensemble_config(scns, seed)
+        cfg["members_all_ranks"] = total
     else:
         scns = [S.config2(n=args.size)]
         cfg = basin_config(scns[0], args.size)
@@ -569,7 +568,7 @@ def ours(args):
                          f"CALPUV2C/CONGRAD, {nopt} OpenMP threads, {dt:.1f} s"}
 
     if rank == 0:
-        cfg["parallelism"] = (f"{world} GPUs, each its own ensemble (members shard, no exchange)"
+        cfg["parallelism"] = (f"{world} GPUs, members partitioned by wet cells (no exchange)"
                               if world > 1 else "single GPU")
         cfg["tiles_32x8"] = kt.nslots // 256
         line = {

@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(NT) k_red_cg_init(DevStatic S, Ctl *ctl, Glob 
 }
 
 // :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA).
-__global__ void __launch_bounds__(NT) k_cg_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
+__global__ void __launch_bounds__(NT, 3) k_cg_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
                                                  double *part) {
   struct A {
     bool skip, asym;
