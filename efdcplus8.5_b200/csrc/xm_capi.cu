@@ -60,6 +60,8 @@ uint64_t morton2(uint32_t x, uint32_t y) {
 
 constexpr int NSTAGE = 8;     // staging buffers (each holds one array of every member)
 constexpr int MAX_JOBS = 64;  // arrays moved by one upload/download call
+constexpr int GRAPH_ITERS = 4;  // CG iterations per graph launch
+constexpr int KERNELS_PER_ITER = 4;  // matvec, its reduce, update, its reduce
 
 }  // namespace
 
@@ -125,6 +127,10 @@ struct efdc_xm_ctx {
   double *pser_d = nullptr;
   double *pser_h = nullptr;  // pinned
   double *ptmp = nullptr;    // scratch P for kernel timing
+  // CUDA graphs of GRAPH_ITERS consecutive CG iterations on X.p (FP64) and
+  // of the FP32 inner iteration, captured on first use
+  cudaGraphExec_t graph_cg = nullptr, graph_mx = nullptr;
+  bool graph_cg_failed = false, graph_mx_failed = false;
 
   template <class T>
   T *alloc(size_t n, bool zero = true) {
@@ -242,6 +248,59 @@ int write_act(efdc_xm_ctx *c) {
   return EFDC_XM_OK;
 }
 
+// Captures `body` (GRAPH_ITERS iterations launched on c->stream) into a
+// graph.  A failed capture leaves plain launches in use (same kernels).
+template <class Body>
+cudaGraphExec_t capture_graph(efdc_xm_ctx *c, Body body) {
+  const long long before = g_launches.load();
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  for (int k = 0; k < GRAPH_ITERS; ++k) body();
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  g_launches.fetch_sub(g_launches.load() - before);  // captured, not launched
+  if (e != cudaSuccess || !g) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) {
+    cudaGetLastError();
+    exec = nullptr;
+  }
+  cudaGraphDestroy(g);
+  return exec;
+}
+
+// `n` CG iterations: whole graphs where they fit, single launches for the rest.
+int run_iters(efdc_xm_ctx *c, bool mixed, double *P, int n) {
+  const xm::Launch l = c->L();
+  cudaGraphExec_t &gr = mixed ? c->graph_mx : c->graph_cg;
+  bool &failed = mixed ? c->graph_mx_failed : c->graph_cg_failed;
+  auto one = [&]() {
+    if (mixed)
+      xm::launch_mx_iter(l, c->S, c->Y, c->ctl, c->glob, c->part);
+    else
+      xm::launch_cg_iter(l, c->S, c->Y, P, c->ctl, c->glob, c->part);
+  };
+  if (!gr && !failed && n >= GRAPH_ITERS && P == c->X.p) {
+    gr = capture_graph(c, one);
+    failed = (gr == nullptr);
+  }
+  int k = 0;
+  if (gr && P == c->X.p) {
+    for (; k + GRAPH_ITERS <= n; k += GRAPH_ITERS) {
+      CK(cudaGraphLaunch(gr, c->stream));
+      xm::count_launches(GRAPH_ITERS * KERNELS_PER_ITER);
+    }
+  }
+  for (; k < n; ++k) one();
+  CK(cudaGetLastError());
+  return EFDC_XM_OK;
+}
+
 // FP64 CONGRAD of every active member on the scaled system in c->Y.  The
 // members iterate in lockstep launches; a member that has stopped is skipped
 // by the kernels.  On return c->ctl_h holds each member's outcome.
@@ -259,10 +318,11 @@ int solve_fp64(efdc_xm_ctx *c, double *P) {
   chunk = std::min(chunk, cap);
   int launched = 0;
   for (;;) {
-    for (int k = 0; k < chunk && launched < cap; ++k, ++launched)
-      xm::launch_cg_iter(l, c->S, c->Y, P, c->ctl, c->glob, c->part);
-    CK(cudaGetLastError());
-    int rc = read_glob(c);
+    const int n = std::min(chunk, cap - launched);
+    int rc = run_iters(c, false, P, n);
+    if (rc) return rc;
+    launched += n;
+    rc = read_glob(c);
     if (rc) return rc;
     if (c->glob_h->ndone >= c->M || launched >= cap) break;
     chunk = 4;
@@ -297,8 +357,7 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
     for (int m = 0; m < c->M; ++m)
       if (c->act_h[m]) chunk = std::max(chunk, c->mem[m].last_inner);
     for (int guard = 0;; ++guard) {
-      for (int k = 0; k < chunk; ++k) xm::launch_mx_iter(l, c->S, c->Y, c->ctl, c->glob, c->part);
-      CK(cudaGetLastError());
+      if ((rc = run_iters(c, true, P, chunk))) return rc;
       if ((rc = read_glob(c))) return rc;
       if (c->glob_h->nidone + c->glob_h->ndone >= c->M) break;
       chunk = 4;
@@ -468,6 +527,8 @@ void efdc_xm_destroy(efdc_xm_ctx *c) {
   void *pinned[] = {c->ctl_h, c->glob_h, c->act_h, c->sc_h, c->jobs_h, c->pser_h};
   for (void *p : pinned)
     if (p) cudaFreeHost(p);
+  if (c->graph_cg) cudaGraphExecDestroy(c->graph_cg);
+  if (c->graph_mx) cudaGraphExecDestroy(c->graph_mx);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
