@@ -24,6 +24,7 @@ SOURCES = {
     "xm_mixed.cu": [],
     "xm_capi.cu": [],
     "xm_noalloc.cu": ["-fmad=false"],
+    "xm_adjoint.cu": [],
 }
 
 

@@ -4,6 +4,7 @@
 // every member and of CONGRAD.
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <climits>
 #include <cmath>
@@ -89,6 +90,7 @@ struct Member {
   int last_iters = 8, last_inner = 8;
   int last_n = 0, last_ntstbc = 0, last_isdry = 0;
   std::vector<int32_t> oldmask_h;
+  std::vector<int> slot_of;  // slot of cell L (0 for L outside 2..LA)
 };
 
 struct efdc_xm_ctx {
@@ -131,6 +133,16 @@ struct efdc_xm_ctx {
   // of the FP32 inner iteration, captured on first use
   cudaGraphExec_t graph_cg = nullptr, graph_mx = nullptr;
   bool graph_cg_failed = false, graph_mx_failed = false;
+  // calibration (efdc_xm_calib_*): adjoint state, step-start snapshots,
+  // the CG solution of the last step, gauge gathers
+  bool calib = false;
+  xm::DevCalib A{};
+  std::vector<std::array<double *, 6>> snap;  // P, HP, HU, HV, UHDYE, VHDXE
+  double *psol = nullptr;
+  double *bsq = nullptr;
+  int *gslot = nullptr;   // [gcap] gauge slots
+  double *gbuf = nullptr; // [gcap] gauge values / adjoint weights
+  int gcap = 0;
 
   template <class T>
   T *alloc(size_t n, bool zero = true) {
@@ -527,6 +539,8 @@ void efdc_xm_destroy(efdc_xm_ctx *c) {
   void *pinned[] = {c->ctl_h, c->glob_h, c->act_h, c->sc_h, c->jobs_h, c->pser_h};
   for (void *p : pinned)
     if (p) cudaFreeHost(p);
+  if (c->gslot) cudaFree(c->gslot);
+  if (c->gbuf) cudaFree(c->gbuf);
   if (c->graph_cg) cudaGraphExecDestroy(c->graph_cg);
   if (c->graph_mx) cudaGraphExecDestroy(c->graph_mx);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -846,6 +860,7 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   for (const auto &mt : metrics) xs.push_back(Xfer{per(mt.first), mt.second, 0});
   if (upload_arrays(c, xs) != EFDC_XM_OK) return bail("upload of the static arrays failed");
   if (cudaDeviceSynchronize() != cudaSuccess) return bail("device error during set-up");
+  for (int m = 0; m < M; ++m) c->mem[m].slot_of = std::move(slot_of[m]);
   return c;
 }
 
@@ -1029,6 +1044,9 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
     CK(cudaGetLastError());
     rc = mixed ? solve_mixed(c, c->X.p, prm[0].mixed_rsq_factor) : solve_fp64(c, c->X.p);
     if (rc) return rc;
+    if (c->psol)  // calibration: the adjoint needs P' before P is refreshed from HP
+      CK(cudaMemcpyAsync(c->psol, c->X.p, size_t(c->nslot) * sizeof(double),
+                         cudaMemcpyDeviceToDevice, c->stream));
     // a member whose solve failed stops here, before the back-substitution
     bool dropped = false;
     int nact = 0;
@@ -1328,6 +1346,313 @@ int32_t efdc_xm_time_kernels(efdc_xm_ctx *c, int32_t precision, int32_t reps, ef
                 c->ctl_h[m].status);
       return EFDC_XM_NONFINITE;
     }
+  return EFDC_XM_OK;
+}
+
+
+// ---- calibration (adjoint) entry points: single-basin contexts ----
+
+static int calib_ready(efdc_xm_ctx *c, const char *who) {
+  if (!c) {
+    set_error("%s: NULL context", who);
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  if (!c->calib) {
+    set_error("%s: call efdc_xm_calib_enable first", who);
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  return EFDC_XM_OK;
+}
+
+static int gauge_slots(efdc_xm_ctx *c, int32_t n, const int32_t *L) {
+  if (n < 0 || (n > 0 && !L)) {
+    set_error("gauge list: bad arguments");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  if (n > c->gcap) {
+    if (c->gslot) cudaFree(c->gslot);
+    if (c->gbuf) cudaFree(c->gbuf);
+    c->gslot = nullptr;
+    c->gbuf = nullptr;
+    c->gcap = 0;
+    CK(cudaMalloc(&c->gslot, size_t(n) * sizeof(int)));
+    CK(cudaMalloc(&c->gbuf, size_t(n) * sizeof(double)));
+    c->gcap = n;
+  }
+  std::vector<int> sl(n);
+  const Member &mb = c->mem[0];
+  for (int i = 0; i < n; ++i) {
+    if (L[i] < 2 || L[i] > mb.la) {
+      set_error("gauge list: L=%d outside 2..LA", L[i]);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+    sl[i] = mb.slot_of[L[i]];
+  }
+  if (n > 0)
+    CK(cudaMemcpyAsync(c->gslot, sl.data(), size_t(n) * sizeof(int), cudaMemcpyHostToDevice,
+                       c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return EFDC_XM_OK;
+}
+
+int32_t efdc_xm_calib_enable(efdc_xm_ctx *c, int32_t nsnap) {
+  int rc = single_only(c, "efdc_xm_calib_enable");
+  if (rc) return rc;
+  if (nsnap < 1) {
+    set_error("efdc_xm_calib_enable: need at least one snapshot slot");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  if (c->any_may_asym) {
+    set_error("efdc_xm_calib_enable: the adjoint covers clamped open boundaries (ISPB=0) only");
+    return EFDC_XM_UNSUPPORTED;
+  }
+  if (c->calib) {
+    set_error("efdc_xm_calib_enable: already enabled");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  CK(cudaSetDevice(c->device));
+  const size_t ns = c->nslot;
+  xm::DevCalib &A = c->A;
+  double **arrs[] = {&A.kappa, &A.ap_in, &A.ahp_in, &A.ahu_in, &A.ahv_in, &A.au_in, &A.av_in,
+                     &A.ap_out, &A.ahp_out, &A.ahu_out, &A.ahv_out, &A.au_out, &A.av_out,
+                     &A.ahpe, &A.rhs, &A.lam, &A.afp, &A.afu, &A.afv, &A.atbx, &A.atby,
+                     &A.nbu, &A.nbv, &A.vub, &A.uvb, &A.akappa, &A.abelv};
+  for (double **a : arrs)
+    if (!(*a = c->alloc<double>(ns))) {
+      set_error("efdc_xm_calib_enable: cudaMalloc failed");
+      return EFDC_XM_CUDA_ERROR;
+    }
+  const size_t nb = size_t(std::max(1, c->nobc)) * std::max(1, c->B.mtmax);
+  A.apcb = c->alloc<double>(nb);
+  A.apsb = c->alloc<double>(nb);
+  A.nflag = c->alloc<int>(1);
+  c->psol = c->alloc<double>(ns);
+  c->bsq = c->alloc<double>(1);
+  if (!A.apcb || !A.apsb || !A.nflag || !c->psol || !c->bsq) {
+    set_error("efdc_xm_calib_enable: cudaMalloc failed");
+    return EFDC_XM_CUDA_ERROR;
+  }
+  for (int k = 0; k < nsnap; ++k) {
+    std::array<double *, 6> a{};
+    for (double *&x : a)
+      if (!(x = c->alloc<double>(ns))) {
+        set_error("efdc_xm_calib_enable: cudaMalloc failed (snapshots)");
+        return EFDC_XM_CUDA_ERROR;
+      }
+    c->snap.push_back(a);
+  }
+  A.tbx = const_cast<double *>(c->X.tbx);
+  A.tby = const_cast<double *>(c->X.tby);
+  CK(cudaDeviceSynchronize());  // the zero-fills of the legacy stream
+  c->calib = true;
+  return EFDC_XM_OK;
+}
+
+int32_t efdc_xm_calib_set_roughness(efdc_xm_ctx *c, const double *log_n) {
+  int rc = calib_ready(c, "efdc_xm_calib_set_roughness");
+  if (rc) return rc;
+  if (!log_n) {
+    set_error("efdc_xm_calib_set_roughness: NULL argument");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  CK(cudaSetDevice(c->device));
+  std::vector<Xfer> xs = {{{log_n}, c->A.kappa, 0}};
+  return upload_arrays(c, xs);
+}
+
+int32_t efdc_xm_calib_set_harmonics(efdc_xm_ctx *c, const double *pcb, const double *psb) {
+  int rc = calib_ready(c, "efdc_xm_calib_set_harmonics");
+  if (rc) return rc;
+  if (c->nobc == 0) return EFDC_XM_OK;
+  if (!pcb || !psb) {
+    set_error("efdc_xm_calib_set_harmonics: NULL argument");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  CK(cudaSetDevice(c->device));
+  const size_t n = size_t(c->nobc) * c->B.mtmax * sizeof(double);
+  CK(cudaMemcpyAsync(const_cast<double *>(c->B.pcb), pcb, n, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(const_cast<double *>(c->B.psb), psb, n, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return EFDC_XM_OK;
+}
+
+static int snap_copy(efdc_xm_ctx *c, int32_t slot, bool save) {
+  if (slot < 0 || slot >= int(c->snap.size())) {
+    set_error("snapshot slot %d outside 0..%d", slot, int(c->snap.size()) - 1);
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  CK(cudaSetDevice(c->device));
+  double *live[6] = {c->X.p, c->X.hp, c->X.hu, c->X.hv, c->X.uhdye, c->X.vhdxe};
+  const size_t nb = size_t(c->nslot) * sizeof(double);
+  for (int k = 0; k < 6; ++k)
+    CK(cudaMemcpyAsync(save ? c->snap[slot][k] : live[k], save ? live[k] : c->snap[slot][k], nb,
+                       cudaMemcpyDeviceToDevice, c->stream));
+  return EFDC_XM_OK;
+}
+
+int32_t efdc_xm_calib_snapshot(efdc_xm_ctx *c, int32_t slot) {
+  const int rc = calib_ready(c, "efdc_xm_calib_snapshot");
+  return rc ? rc : snap_copy(c, slot, true);
+}
+
+int32_t efdc_xm_calib_restore(efdc_xm_ctx *c, int32_t slot) {
+  const int rc = calib_ready(c, "efdc_xm_calib_restore");
+  return rc ? rc : snap_copy(c, slot, false);
+}
+
+int32_t efdc_xm_calib_step(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats) {
+  efdc_xm_stats dummy;
+  if (!stats) stats = &dummy;
+  std::memset(stats, 0, sizeof(*stats));
+  int rc = calib_ready(c, "efdc_xm_calib_step");
+  if (rc) return stats->status = rc;
+  if (!prm || prm->isdry != 0 || prm->precision != EFDC_XM_PREC_FP64) {
+    set_error("efdc_xm_calib_step: the calibration model runs FP64 with ISDRY=0");
+    return stats->status = EFDC_XM_BAD_ARGUMENT;
+  }
+  CK(cudaSetDevice(c->device));
+  // the drag of this step from the state at its start (the scalars first)
+  c->sc_h[0] = make_scalars(c->mem[0], prm);
+  CK(cudaMemcpyAsync(c->sc, c->sc_h, sizeof(xm::StepScalars), cudaMemcpyHostToDevice, c->stream));
+  xm::DevCalib A = c->A;
+  A.u0 = c->X.uhdye;
+  A.v0 = c->X.vhdxe;
+  A.hu0 = c->X.hu;
+  A.hv0 = c->X.hv;
+  xm::launch_cal_tbxy(c->L(), c->S, c->X, A);
+  CK(cudaGetLastError());
+  return efdc_xm_step_device_batch(c, prm, stats);
+}
+
+int32_t efdc_xm_calib_gauges(efdc_xm_ctx *c, int32_t n, const int32_t *L, double *p_out) {
+  int rc = calib_ready(c, "efdc_xm_calib_gauges");
+  if (rc) return rc;
+  if (n == 0) return EFDC_XM_OK;
+  if (!p_out) {
+    set_error("efdc_xm_calib_gauges: NULL output");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  if ((rc = gauge_slots(c, n, L))) return rc;
+  xm::launch_gather_slots(c->stream, c->X.p, c->gslot, n, c->gbuf);
+  CK(cudaMemcpyAsync(p_out, c->gbuf, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return EFDC_XM_OK;
+}
+
+int32_t efdc_xm_calib_adjoint_reset(efdc_xm_ctx *c) {
+  int rc = calib_ready(c, "efdc_xm_calib_adjoint_reset");
+  if (rc) return rc;
+  CK(cudaSetDevice(c->device));
+  xm::DevCalib &A = c->A;
+  const size_t nb = size_t(c->nslot) * sizeof(double);
+  double *z[] = {A.ap_in, A.ahp_in, A.ahu_in, A.ahv_in, A.au_in, A.av_in, A.ap_out, A.ahp_out,
+                 A.ahu_out, A.ahv_out, A.au_out, A.av_out, A.akappa, A.abelv};
+  for (double *a : z) CK(cudaMemsetAsync(a, 0, nb, c->stream));
+  const size_t np = size_t(std::max(1, c->nobc)) * std::max(1, c->B.mtmax) * sizeof(double);
+  CK(cudaMemsetAsync(A.apcb, 0, np, c->stream));
+  CK(cudaMemsetAsync(A.apsb, 0, np, c->stream));
+  CK(cudaMemsetAsync(A.nflag, 0, sizeof(int), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return EFDC_XM_OK;
+}
+
+int32_t efdc_xm_calib_add_p_adjoint(efdc_xm_ctx *c, int32_t n, const int32_t *L, const double *w) {
+  int rc = calib_ready(c, "efdc_xm_calib_add_p_adjoint");
+  if (rc) return rc;
+  if (n == 0) return EFDC_XM_OK;
+  if (!w) {
+    set_error("efdc_xm_calib_add_p_adjoint: NULL weights");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  if ((rc = gauge_slots(c, n, L))) return rc;
+  CK(cudaMemcpyAsync(c->gbuf, w, size_t(n) * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  xm::launch_adj_gauge(c->L(), c->gslot, c->gbuf, n, c->A.ap_in);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return EFDC_XM_OK;
+}
+
+int32_t efdc_xm_calib_adjoint_step(efdc_xm_ctx *c, const efdc_xm_params *prm, int32_t slot,
+                                   double rel_tol, int32_t *cg_iters) {
+  int rc = calib_ready(c, "efdc_xm_calib_adjoint_step");
+  if (rc) return rc;
+  if (!(rel_tol > 0.0)) {
+    set_error("efdc_xm_calib_adjoint_step: rel_tol must be > 0");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  // the step again, from its start state: its operator, CG solution and drag
+  if ((rc = efdc_xm_calib_restore(c, slot))) return rc;
+  efdc_xm_stats st;
+  rc = efdc_xm_calib_step(c, prm, &st);
+  if (rc != EFDC_XM_OK) return rc;
+  const xm::Launch l = c->L();
+  xm::DevCalib &A = c->A;
+  A.p0 = c->snap[slot][0];
+  A.hp0 = c->snap[slot][1];
+  A.hu0 = c->snap[slot][2];
+  A.hv0 = c->snap[slot][3];
+  A.u0 = c->snap[slot][4];
+  A.v0 = c->snap[slot][5];
+  A.psol = c->psol;
+  xm::launch_adj_pre(l, c->S, c->X, c->B, A);
+  CK(cudaMemsetAsync(c->bsq, 0, sizeof(double), c->stream));
+  xm::launch_adj_rhs(l, c->S, c->Y, c->ctl, A, c->bsq);
+  CK(cudaGetLastError());
+  double bsq = 0.0;
+  CK(cudaMemcpyAsync(&bsq, c->bsq, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  int iters = 0;
+  if (bsq > 0.0) {  // A lam = rhs, the step's operator (symmetric), relative stop
+    c->sc_h[0].rsqm = rel_tol * rel_tol * bsq;
+    CK(cudaMemcpyAsync(c->sc, c->sc_h, sizeof(xm::StepScalars), cudaMemcpyHostToDevice,
+                       c->stream));
+    c->act_h[0] = 1;
+    if ((rc = write_act(c))) return rc;
+    if ((rc = solve_fp64(c, A.lam))) return rc;
+    const Ctl &k = c->ctl_h[0];
+    iters = k.iter;
+    if (k.status != EFDC_XM_OK) {
+      set_error("adjoint CONGRAD: %s after %d iterations",
+                k.status == EFDC_XM_CG_MAXITER ? "maximum iterations exceeded"
+                                               : "non-finite residual", k.iter);
+      return k.status;
+    }
+  }
+  if (cg_iters) *cg_iters = iters;
+  xm::launch_adj_post(l, c->S, c->X, c->B, A);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  // the adjoints of this step's inputs are those of the previous step's outputs
+  std::swap(A.ap_in, A.ap_out);
+  std::swap(A.ahp_in, A.ahp_out);
+  std::swap(A.ahu_in, A.ahu_out);
+  std::swap(A.ahv_in, A.ahv_out);
+  std::swap(A.au_in, A.au_out);
+  std::swap(A.av_in, A.av_out);
+  return EFDC_XM_OK;
+}
+
+int32_t efdc_xm_calib_gradients(efdc_xm_ctx *c, double *dlog_n, double *dbelv, double *dpcb,
+                                double *dpsb, double *const state[6], int32_t *n_clamped) {
+  int rc = calib_ready(c, "efdc_xm_calib_gradients");
+  if (rc) return rc;
+  CK(cudaSetDevice(c->device));
+  const xm::DevCalib &A = c->A;
+  auto one = [](const void *q) { return std::vector<const void *>{q}; };
+  std::vector<Xfer> xs;
+  if (dlog_n) xs.push_back({one(dlog_n), A.akappa, 0});
+  if (dbelv) xs.push_back({one(dbelv), A.abelv, 0});
+  if (state) {
+    double *src[6] = {A.ap_in, A.ahp_in, A.ahu_in, A.ahv_in, A.au_in, A.av_in};
+    for (int k = 0; k < 6; ++k)
+      if (state[k]) xs.push_back({one(state[k]), src[k], 0});
+  }
+  if ((rc = download_arrays(c, xs))) return rc;
+  const size_t np = size_t(c->nobc) * c->B.mtmax * sizeof(double);
+  if (np && dpcb) CK(cudaMemcpy(dpcb, A.apcb, np, cudaMemcpyDeviceToHost));
+  if (np && dpsb) CK(cudaMemcpy(dpsb, A.apsb, np, cudaMemcpyDeviceToHost));
+  if (n_clamped) CK(cudaMemcpy(n_clamped, A.nflag, sizeof(int), cudaMemcpyDeviceToHost));
   return EFDC_XM_OK;
 }
 

@@ -123,4 +123,26 @@ struct DevObc {
   const double *pser;    // [n] per-step series part
 };
 
+// Calibration (adjoint) state of a single-member context, tile layout.
+// "0" arrays are the step-start state (a snapshot), `psol` the step's CG
+// solution P'; the adjoint arrays hold d(loss)/d(x).  in: adjoints of the
+// step's outputs; out: of its inputs.
+struct DevCalib {
+  double *kappa;                                   // log Manning n per slot
+  double *tbx, *tby;                               // the drag written for the step
+  const double *p0, *hp0, *hu0, *hv0, *u0, *v0;    // P, HP, HU, HV, UHDYE, VHDXE at step start
+  const double *psol;                              // P' (CG solution of the step)
+  double *ap_in, *ahp_in, *ahu_in, *ahv_in, *au_in, *av_in;
+  double *ap_out, *ahp_out, *ahu_out, *ahv_out, *au_out, *av_out;
+  double *ahpe;            // adjoint of HP' (continuity output) after the face-depth terms
+  double *rhs, *lam;       // adjoint solve: A lam = rhs
+  double *afp, *afu, *afv; // adjoints of FP, FUHDYE, FVHDXE
+  double *atbx, *atby;     // adjoints of TBX, TBY
+  double *nbu, *nbv;       // adjoints of the face Manning n (u, v faces)
+  double *vub, *uvb;       // adjoints of VU (at u faces) and UV (at v faces)
+  double *akappa, *abelv;  // accumulated gradients w.r.t. log n and BELV
+  double *apcb, *apsb;     // accumulated gradients w.r.t. PCB, PSB ([n_obc * mtmax])
+  int *nflag;              // [1] boundary cells whose dry-clamp branch fired (not differentiated)
+};
+
 }  // namespace xm

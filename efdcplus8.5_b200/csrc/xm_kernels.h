@@ -70,6 +70,17 @@ void launch_gather(cudaStream_t st, const CopyJob *jobs, int njob, const int *li
 void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                         int mixed);
 
+// calibration: drag from log n, and the reverse of one step (xm_adjoint.cu)
+void launch_cal_tbxy(const Launch &l, const DevStatic &S, const DevState &X, const DevCalib &A);
+void launch_adj_gauge(const Launch &l, const int *slots, const double *w, int n, double *ap);
+void launch_adj_pre(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B,
+                    const DevCalib &A);
+void launch_adj_rhs(const Launch &l, const DevStatic &S, const DevSystem &Y, const Ctl *ctl,
+                    const DevCalib &A, double *bsq);
+void launch_adj_post(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B,
+                     const DevCalib &A);
+void launch_gather_slots(cudaStream_t st, const double *src, const int *slots, int n, double *out);
+
 // sets the message returned by efdc_xm_last_error() for this thread
 void set_last_error_str(const char *msg);
 

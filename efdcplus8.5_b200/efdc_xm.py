@@ -242,6 +242,22 @@ def load(path: str | os.PathLike | None = None):
     lib.efdc_xm_congrad.restype = C.c_int32
     lib.efdc_xm_congrad.argtypes = [C.c_void_p] + [_pd] * 8 + [C.c_double, C.c_int32,
                                                                 C.c_int32, _pi, _pd]
+    for name, args in (
+            ("efdc_xm_calib_enable", [C.c_void_p, C.c_int32]),
+            ("efdc_xm_calib_set_roughness", [C.c_void_p, _pd]),
+            ("efdc_xm_calib_set_harmonics", [C.c_void_p, _pd, _pd]),
+            ("efdc_xm_calib_snapshot", [C.c_void_p, C.c_int32]),
+            ("efdc_xm_calib_restore", [C.c_void_p, C.c_int32]),
+            ("efdc_xm_calib_step", [C.c_void_p, C.POINTER(Params), C.POINTER(Stats)]),
+            ("efdc_xm_calib_gauges", [C.c_void_p, C.c_int32, _pi, _pd]),
+            ("efdc_xm_calib_adjoint_reset", [C.c_void_p]),
+            ("efdc_xm_calib_add_p_adjoint", [C.c_void_p, C.c_int32, _pi, _pd]),
+            ("efdc_xm_calib_adjoint_step", [C.c_void_p, C.POINTER(Params), C.c_int32, C.c_double,
+                                            _pi]),
+            ("efdc_xm_calib_gradients", [C.c_void_p, _pd, _pd, _pd, _pd, C.POINTER(_pd), _pi])):
+        fn = getattr(lib, name)
+        fn.restype = C.c_int32
+        fn.argtypes = args
     lib.efdc_xm_create_batch.restype = C.c_void_p
     lib.efdc_xm_create_batch.argtypes = [C.POINTER(Grid), C.c_int32, C.c_int32]
     lib.efdc_xm_nmembers.restype = C.c_int32
@@ -324,6 +340,75 @@ class Solver:
         if rc != OK:
             raise RuntimeError(f"efdc_xm_time_kernels: {self.last_error()}")
         return kt
+
+    # ---- calibration (adjoint) ----
+    def _ok(self, name, rc):
+        if rc != OK:
+            raise RuntimeError(f"{name}: {STATUS_NAMES.get(rc, rc)}: {self.last_error()}")
+
+    def calib_enable(self, nsnap: int):
+        self._ok("efdc_xm_calib_enable", self.lib.efdc_xm_calib_enable(self.ctx, int(nsnap)))
+
+    def calib_set_roughness(self, log_n):
+        a = np.ascontiguousarray(log_n, dtype=np.float64)
+        self._ok("efdc_xm_calib_set_roughness", self.lib.efdc_xm_calib_set_roughness(self.ctx, _dp(a)))
+
+    def calib_set_harmonics(self, pcb, psb):
+        a = np.ascontiguousarray(pcb, dtype=np.float64)
+        b = np.ascontiguousarray(psb, dtype=np.float64)
+        self._ok("efdc_xm_calib_set_harmonics",
+                 self.lib.efdc_xm_calib_set_harmonics(self.ctx, _dp(a), _dp(b)))
+
+    def calib_snapshot(self, slot: int):
+        self._ok("efdc_xm_calib_snapshot", self.lib.efdc_xm_calib_snapshot(self.ctx, int(slot)))
+
+    def calib_restore(self, slot: int):
+        self._ok("efdc_xm_calib_restore", self.lib.efdc_xm_calib_restore(self.ctx, int(slot)))
+
+    def calib_step(self, params: Params) -> Stats:
+        st = Stats()
+        rc = self.lib.efdc_xm_calib_step(self.ctx, C.byref(params), C.byref(st))
+        if rc not in (OK, NEG_DEPTH):
+            raise RuntimeError(f"efdc_xm_calib_step: {STATUS_NAMES.get(rc, rc)}: {self.last_error()}")
+        return st
+
+    def calib_gauges(self, cells) -> np.ndarray:
+        L = np.ascontiguousarray(cells, dtype=np.int32)
+        out = np.zeros(L.size)
+        self._ok("efdc_xm_calib_gauges",
+                 self.lib.efdc_xm_calib_gauges(self.ctx, L.size, _ip(L), _dp(out)))
+        return out
+
+    def calib_adjoint_reset(self):
+        self._ok("efdc_xm_calib_adjoint_reset", self.lib.efdc_xm_calib_adjoint_reset(self.ctx))
+
+    def calib_add_p_adjoint(self, cells, w):
+        L = np.ascontiguousarray(cells, dtype=np.int32)
+        a = np.ascontiguousarray(w, dtype=np.float64)
+        self._ok("efdc_xm_calib_add_p_adjoint",
+                 self.lib.efdc_xm_calib_add_p_adjoint(self.ctx, L.size, _ip(L), _dp(a)))
+
+    def calib_adjoint_step(self, params: Params, slot: int, rel_tol: float = 1e-12) -> int:
+        it = C.c_int32(0)
+        self._ok("efdc_xm_calib_adjoint_step",
+                 self.lib.efdc_xm_calib_adjoint_step(self.ctx, C.byref(params), int(slot),
+                                                     float(rel_tol), C.byref(it)))
+        return it.value
+
+    def calib_gradients(self, nobc_mt: int):
+        """(d/dlog n, d/dBELV, d/dPCB, d/dPSB, state adjoints dict, n_clamped);
+        per-cell arrays have the LCM = LC+1 length of the model's arrays."""
+        lc = self.lc + 1
+        dk, db = np.zeros(lc), np.zeros(lc)
+        dpc, dps = np.zeros(max(nobc_mt, 1)), np.zeros(max(nobc_mt, 1))
+        names = ("p", "hp", "hu", "hv", "uhdye", "vhdxe")
+        st = {k: np.zeros(lc) for k in names}
+        arr = (_pd * 6)(*[_dp(st[k]) for k in names])
+        ncl = C.c_int32(0)
+        self._ok("efdc_xm_calib_gradients",
+                 self.lib.efdc_xm_calib_gradients(self.ctx, _dp(dk), _dp(db), _dp(dpc), _dp(dps),
+                                                  arr, C.byref(ncl)))
+        return dk, db, dpc[:nobc_mt], dps[:nobc_mt], st, ncl.value
 
     def congrad(self, ccc, ccs, ccn, ccw, cce, ccci, fptmp, p, rsqm, iterm,
                 precision=PREC_FP64):

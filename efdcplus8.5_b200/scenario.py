@@ -503,6 +503,27 @@ def config3_member(k, ncell, seed=3):
                          fill_dead_ends=True)
 
 
+def config4(seed=4, n=512, nsteps=200, ngauges=20):
+    """Adjoint calibration basin: n x n cells (~240k wet at n=512), 7% land,
+    depth 2-30 m, west M2 boundary 0.5 m, dt=10 s, ISDRY=0, RSQM=1e-10.
+    Returns (scenario, gauges, true log n, true boundary amplitudes): the
+    per-cell log Manning n ~ N(log 0.025, 0.2), four amplitudes, and 20
+    seeded interior gauge cells (1-based L)."""
+    scn = make_scenario(n, n, seed=seed, dx=100.0, dy=100.0, land_frac=0.07,
+                        depth=(2.0, 30.0), corr_len_m=1000.0, obc_sides=("W",), amp=0.5,
+                        manning=0.0, dt=10.0, rsqm=1e-10, iterm=500, isdry=0, kc=4,
+                        fill_dead_ends=True)
+    rng = np.random.default_rng(seed + 4000)
+    log_n = np.full(scn.lc + 1, math.log(0.025))
+    log_n[1:scn.la] = rng.normal(math.log(0.025), 0.2, scn.la - 1)
+    amps = np.array([0.45, 0.55, 0.5, 0.6])
+    bc = set(int(x) for s in SIDES for x in scn.grid["obc"][s]["l"])
+    il = scn.grid["il"]
+    cand = [L for L in range(2, scn.la + 1) if L not in bc and il[L - 1] > 4]
+    gauges = np.sort(rng.choice(cand, size=ngauges, replace=False)).astype(np.int32)
+    return scn, gauges, log_n, amps
+
+
 def tidal_flat(n=1024, *, seed=5, hdry=0.05, amp=2.0, ramp=(-2.0, 15.0 / 4.0),
                noise=0.3, dt=5.0):
     """Wetting/drying tidal flat: bed elevation ramps west->east across the

@@ -214,6 +214,50 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *ctx, const efdc_xm_params *prm,
                                   efdc_xm_stats *stats);
 int32_t efdc_xm_download_batch(efdc_xm_ctx *ctx, efdc_xm_fields *f);
 
+/* ---- Calibration: the reverse (adjoint) of the external mode ----
+ *
+ * No counterpart in the reference.  For single-basin contexts with clamped
+ * open boundaries (ISPB=0), ISDRY=0, FP64.  The calibration model is
+ * CALPUV2C preceded by a bottom drag written from a per-cell Manning n:
+ * TBX = STBX*SQRT(VU^2+U^2)*U with STBX = G*n_u^2/HU^(1/3) (the form of
+ * hdmt2t.f90:682 with AVCON1=0; U the depth-averaged u-face velocity, VU the
+ * mean of the four v-face velocities around it, n_u the mean n of the face's
+ * two cells), and TBY alike.  The adjoint of a step runs the step again from
+ * a snapshot of its start state, then the reverse kernels, whose implicit
+ * solve is a CG solve with the step's own (symmetric) operator.
+ *
+ * Typical use (N steps, a snapshot every K steps):
+ *   forward:  snapshot(n/K) every K steps; calib_step(n); calib_gauges()
+ *   backward: adjoint_reset(); for each K-step segment, last first: restore
+ *             the segment's snapshot, rerun its steps taking one snapshot per
+ *             step, then for each step n of the segment, last first:
+ *             add_p_adjoint(d loss / d P after step n); adjoint_step(n)
+ *   result:   calib_gradients()                                          */
+int32_t efdc_xm_calib_enable(efdc_xm_ctx *ctx, int32_t nsnap); /* nsnap snapshot slots */
+int32_t efdc_xm_calib_set_roughness(efdc_xm_ctx *ctx, const double *log_n); /* 1..LC */
+/* harmonic amplitudes PCB/PSB of every open-boundary cell, packed in the
+ * W, E, S, N order of the grid's lists: [cell*mtmax + m], mtmax = MTIDE */
+int32_t efdc_xm_calib_set_harmonics(efdc_xm_ctx *ctx, const double *pcb, const double *psb);
+int32_t efdc_xm_calib_snapshot(efdc_xm_ctx *ctx, int32_t slot); /* P, HP, HU, HV, UHDYE, VHDXE */
+int32_t efdc_xm_calib_restore(efdc_xm_ctx *ctx, int32_t slot);
+int32_t efdc_xm_calib_step(efdc_xm_ctx *ctx, const efdc_xm_params *prm, efdc_xm_stats *stats);
+int32_t efdc_xm_calib_gauges(efdc_xm_ctx *ctx, int32_t n, const int32_t *l, double *p_out);
+int32_t efdc_xm_calib_adjoint_reset(efdc_xm_ctx *ctx);
+/* d(loss)/dP += w at cells l (P after the step whose adjoint runs next) */
+int32_t efdc_xm_calib_add_p_adjoint(efdc_xm_ctx *ctx, int32_t n, const int32_t *l,
+                                    const double *w);
+/* the reverse of the step that starts at snapshot `slot`; the adjoint solve
+ * stops at |r| <= rel_tol*|b| */
+int32_t efdc_xm_calib_adjoint_step(efdc_xm_ctx *ctx, const efdc_xm_params *prm, int32_t slot,
+                                   double rel_tol, int32_t *cg_iters);
+/* accumulated d(loss)/d(log n) and d(loss)/d(BELV) (1..LC, elements 2..LA
+ * written), d(loss)/d(PCB), d(loss)/d(PSB) (packed as above), and the
+ * adjoint of the state at the start of the last reversed step (P, HP, HU,
+ * HV, UHDYE, VHDXE; any may be NULL); *n_clamped counts boundary targets
+ * that were dry-clamped (not differentiated) */
+int32_t efdc_xm_calib_gradients(efdc_xm_ctx *ctx, double *dlog_n, double *dbelv, double *dpcb,
+                                double *dpsb, double *const state[6], int32_t *n_clamped);
+
 /* ---- Extensions with no counterpart in the reference (measurement hooks) ---- */
 
 /* The CUDA stream (cudaStream_t) every call of this context runs on, so a
