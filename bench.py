@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--basin-steps", type=int, default=50,
                     help="single-domain side measurement (0: skip)")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--calib-steps", type=int, default=200,
+                    help="adjoint calibration side measurement, 512x512 basin (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -197,6 +199,46 @@ def cpu_sample(scns):
     order = sorted(range(len(scns)), key=lambda k: scns[k].ncell)
     pick = order[::max(1, len(order) // 8)][:8]
     return [scns[k] for k in pick]
+
+
+def calibration(args, torch):
+    """Config-4 adjoint: gradient of a 20-gauge elevation misfit over
+    `calib_steps` steps w.r.t. per-cell log Manning n and four boundary
+    amplitudes on the 512x512 basin, checked by central differences."""
+    from calib import CalibProblem
+    import math
+    scn, gauges, log_true, a_true = S.config4()
+    pb = CalibProblem(scn, gauges, args.calib_steps, every=20, adj_rel_tol=1e-12, rsqm=1e-18)
+    pb.obs = pb.forward(log_true, a_true, keep=False)
+    log0 = np.full(scn.lc + 1, math.log(0.025))
+    a0 = np.full(4, 0.5)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss = pb.loss(log0, a0)
+    t1 = time.perf_counter()
+    dk, da, db, iters = pb.backward()
+    t2 = time.perf_counter()
+    rng = np.random.default_rng(44)
+    h = 1e-4
+    v = np.zeros_like(log0)
+    v[1:scn.la] = rng.standard_normal(scn.la - 1)
+    fd = (pb.loss(log0 + h * v, a0) - pb.loss(log0 - h * v, a0)) / (2 * h)
+    an = float((dk * v).sum())
+    errs = {"log_n_direction": abs(fd - an) / abs(an)}
+    for j in range(4):
+        e = np.zeros(4)
+        e[j] = 1.0
+        fdj = (pb.loss(log0, a0 + h * e) - pb.loss(log0, a0 - h * e)) / (2 * h)
+        errs[f"amplitude_{j}"] = abs(fdj - da[j]) / abs(da[j])
+    pb.close()
+    return {"config": {"workload": "adjoint calibration, 512x512 basin, 20 gauges, per-cell log "
+                                   "Manning n ~ N(log 0.025, 0.2) and 4 boundary amplitudes, "
+                                   "checkpoints every 20 steps, FP64",
+                       "cells": int(scn.ncell), "steps": args.calib_steps},
+            "loss": loss, "forward_s": t1 - t0, "gradient_s": t2 - t1,
+            "gradient_over_forward": (t2 - t1) / (t1 - t0), "adjoint_cg_iterations": int(iters),
+            "fd_h": h, "fd_rel_err": errs, "fd_rel_err_max": max(errs.values()),
+            "grad_norm_log_n": float(np.linalg.norm(dk)), "grad_amplitudes": da.tolist()}
 
 
 def reference_arm(args):
@@ -555,6 +597,9 @@ def ours(args):
                   "k_mx_matvec_frac": 24.0 * kb.ncells / (kb.ms_matvec * 1e-3) / 1e9 / peak}
         sol.close()
         del fl
+    calib_res = None
+    if rank == 0 and world == 1 and args.calib_steps > 0:
+        calib_res = calibration(args, torch)
     clocks = ck.stop()
 
     # ---------------- CPU baseline (rank 0, N=1) ----------------
@@ -598,6 +643,7 @@ def ours(args):
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(rmx["launches"]), "clocks": clocks,
             "single_domain": single,
+            "calibration": calib_res,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
