@@ -74,6 +74,9 @@ def parse():
     ap.add_argument("--basin-steps", type=int, default=50,
                     help="single-domain side measurement (0: skip)")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--wetdry-members", type=int, default=64)
+    ap.add_argument("--wetdry-steps", type=int, default=20,
+                    help="wetting/drying batch side measurement, 1024x1024 flats (0: skip)")
     ap.add_argument("--calib-steps", type=int, default=200,
                     help="adjoint calibration side measurement, 512x512 basin (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -199,6 +202,112 @@ def cpu_sample(scns):
     order = sorted(range(len(scns)), key=lambda k: scns[k].ncell)
     pick = order[::max(1, len(order) // 8)][:8]
     return [scns[k] for k in pick]
+
+
+def volume_residual(scn, before, after):
+    """|dV - (boundary inflow + sources - wasted volume)| / V over the
+    non-boundary cells for one step (calpuv2c.f90:466-486 summed: interior
+    faces cancel; the faces next to open-boundary cells carry the inflow)."""
+    g = scn.grid
+    la = scn.la
+    bc = np.zeros(scn.lc + 1, bool)
+    for s_ in ("W", "E", "S", "N"):
+        bc[np.asarray(g["obc"][s_]["l"], dtype=np.int64) - 1] = True
+    ii = np.arange(1, la)
+    ii = ii[~bc[ii]]
+    dxyp = g["dxyp"]
+    v0 = float(np.sum(dxyp[ii] * before["hp"][ii]))
+    v1 = float(np.sum(dxyp[ii] * after["hp"][ii]))
+    d2 = 0.5 * float(scn.params["dt"])
+    flow = 0.0
+    for s_, key, nbk, sign in (("W", "uhdye", "lec", 1.0), ("E", "uhdye", None, -1.0),
+                               ("S", "vhdxe", "lnc", 1.0), ("N", "vhdxe", None, -1.0)):
+        for L in np.asarray(g["obc"][s_]["l"], dtype=np.int64):
+            f = (g[nbk][L - 1] - 1) if nbk else (L - 1)  # the face between the cell and its target
+            flow += sign * d2 * (after[key][f] + before[key][f])
+    src = 2.0 * d2 * float(np.sum(after["qsume"][ii]))
+    waste = float(np.sum(after["vdwaste"][ii]) - np.sum(before["vdwaste"][ii]))
+    return abs((v1 - v0) - (flow + src - waste)) / v0
+
+
+def wetdry(args, torch, dev, rank):
+    """Config-5 style batch: tidal flats (1024x1024, bed ramp -2..15 m +
+    N(0, 0.3 m), 2 m M2, ISDRY=99, NDRYSTP=-10), FP64 and MIXED batched
+    runs, the MIXED masks checked against FP64 from the same inputs and the
+    volume budget, on the first two members."""
+    from concurrent.futures import ThreadPoolExecutor as TPE
+    K = args.wetdry_steps
+    with TPE(os.cpu_count() or 4) as ex:
+        scns = list(ex.map(lambda k: S.tidal_flat(n=1024, seed=5 + 97 * k + 1000 * rank),
+                           range(args.wetdry_members)))
+    cells = np.array([sc.ncell for sc in scns], dtype=np.int64)
+    bs = X.BatchSolver([sc.grid for sc in scns], device=dev.index)
+    stream = torch.cuda.ExternalStream(bs.stream(), device=dev)
+    tmul = 60.0  # a tidal phase in which the flat wets and dries within the run
+
+    def prm(n, prec):
+        return [X.make_params(sc.params, n=n, tn=sc.tn(n) * tmul, precision=prec) for sc in scns]
+
+    def run(prec):
+        bs.upload([sc.state for sc in scns])
+        bs.step_device(prm(1, prec))
+        its = np.zeros(len(scns), np.int64)
+        sweeps = 0
+        t = 0.0
+        for n in range(2, K + 2):
+            with Timer(torch, stream) as tm:
+                sts = bs.step_device(prm(n, prec))
+            t += tm.ms / 1e3
+            for m, st in enumerate(sts):
+                assert st.status in (X.OK, X.NEG_DEPTH), (m, st.as_dict())
+            its += np.array([st.iters_total for st in sts])
+            sweeps += sum(st.solves for st in sts)
+        out = [{"lmaskdry": np.zeros(sc.lc + 1, np.int32), "sub": np.zeros(sc.lc + 1),
+                "svb": np.zeros(sc.lc + 1)} for sc in scns]
+        bs.download(out)
+        return t, its, sweeps, out
+
+    t64, it64, sw64, m64 = run(X.PREC_FP64)
+    tmx, _itmx, swmx, mmx = run(X.PREC_MIXED)
+    credit = float((cells * it64).sum())
+    free_diff = sum(int(np.sum(a[k][1:sc.la] != b[k][1:sc.la])) for a, b, sc in
+                    zip(m64, mmx, scns) for k in ("lmaskdry", "sub", "svb"))
+    bs.close()
+    # same-input check, member by member, and the volume budget
+    step_diff, vres, toggled = 0, 0.0, 0
+    for sc in scns[:2]:
+        s64, smx = X.Solver(sc.grid, device=dev.index), X.Solver(sc.grid, device=dev.index)
+        st = sc.copy_state()
+        wet0 = st["lmaskdry"][1:sc.la].copy()
+        for n in range(1, K + 2):
+            a, b = {k: (v.copy() if isinstance(v, np.ndarray) else
+                        {q: w.copy() for q, w in v.items()} if isinstance(v, dict) else v)
+                    for k, v in st.items()}, None
+            b = {k: (v.copy() if isinstance(v, np.ndarray) else
+                     {q: w.copy() for q, w in v.items()} if isinstance(v, dict) else v)
+                 for k, v in st.items()}
+            p = X.make_params(sc.params, n=n, tn=sc.tn(n) * tmul)
+            s64.step(p, a)
+            pm = X.make_params(sc.params, n=n, tn=sc.tn(n) * tmul, precision=X.PREC_MIXED)
+            smx.step(pm, b)
+            for k in ("lmaskdry", "sub", "svb", "iscdry"):
+                step_diff += int(np.sum(a[k][1:sc.la] != b[k][1:sc.la]))
+            vres = max(vres, volume_residual(sc, st, b))
+            st = a
+        toggled += int(np.sum(st["lmaskdry"][1:sc.la] != wet0))
+        s64.close()
+        smx.close()
+    return {"config": {"workload": f"{len(scns)} wetting/drying tidal flats 1024x1024 (bed ramp "
+                                   f"-2..15 m + N(0, 0.3 m), 2 m M2, ISDRY=99, NDRYSTP=-10), "
+                                   f"{K} timed steps after 1, batched",
+                       "members": len(scns), "cells": int(cells.sum())},
+            "value": credit / tmx, "fp64_value": credit / t64, "speedup_vs_fp64": t64 / tmx,
+            "ms_per_step": 1000 * tmx / K, "fp64_ms_per_step": 1000 * t64 / K,
+            "solves_per_member_step": sw64 / (K * len(scns)),
+            "mask_diff_cells_free_run": free_diff,
+            "mask_diff_cells_same_input_2_members": step_diff,
+            "cells_toggled_2_members": toggled,
+            "volume_residual_max_2_members": vres}
 
 
 def calibration(args, torch):
@@ -597,6 +706,9 @@ def ours(args):
                   "k_mx_matvec_frac": 24.0 * kb.ncells / (kb.ms_matvec * 1e-3) / 1e9 / peak}
         sol.close()
         del fl
+    wd_res = None
+    if args.wetdry_steps > 0 and args.workload == "ensemble":
+        wd_res = wetdry(args, torch, dev, rank)
     calib_res = None
     if rank == 0 and world == 1 and args.calib_steps > 0:
         calib_res = calibration(args, torch)
@@ -643,6 +755,7 @@ def ours(args):
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(rmx["launches"]), "clocks": clocks,
             "single_domain": single,
+            "wetdry": wd_res,
             "calibration": calib_res,
         }
         print(json.dumps(line), flush=True)
