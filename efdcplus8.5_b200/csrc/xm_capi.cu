@@ -88,6 +88,7 @@ struct Member {
   std::vector<double> tcp;
   bool may_asym = false;  // a radiation boundary: the operator can be unsymmetric
   int last_iters = 8, last_inner = 8;
+  float jac_est = 20.f;  // Jacobi-equivalent inner iterations per outer pass (MIXED)
   int last_n = 0, last_ntstbc = 0, last_isdry = 0;
   std::vector<int32_t> oldmask_h;
   std::vector<int> slot_of;  // slot of cell L (0 for L outside 2..LA)
@@ -112,6 +113,8 @@ struct efdc_xm_ctx {
   Glob *glob = nullptr;
   Glob *glob_h = nullptr;            // pinned
   int *act = nullptr;                // [M] member takes part in the current sweep
+  int *mpoly = nullptr;              // [M] MIXED inner preconditioner of the member
+  int *mpoly_h = nullptr;            // [M] pinned
   int *act_h = nullptr;              // [M] pinned
   xm::StepScalars *sc = nullptr;     // [M]
   xm::StepScalars *sc_h = nullptr;   // [M] pinned
@@ -131,8 +134,9 @@ struct efdc_xm_ctx {
   double *ptmp = nullptr;    // scratch P for kernel timing
   // CUDA graphs of GRAPH_ITERS consecutive CG iterations on X.p (FP64) and
   // of the FP32 inner iteration, captured on first use
-  cudaGraphExec_t graph_cg = nullptr, graph_mx = nullptr;
-  bool graph_cg_failed = false, graph_mx_failed = false;
+  cudaGraphExec_t graph_cg = nullptr, graph_mx[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool graph_cg_failed = false, graph_mx_failed[4] = {false, false, false, false};
+  bool mx_jac = true, mx_poly = false;  // kinds of MIXED inner solve in use
   // calibration (efdc_xm_calib_*): adjoint state, step-start snapshots,
   // the CG solution of the last step, gauge gathers
   bool calib = false;
@@ -154,7 +158,8 @@ struct efdc_xm_ctx {
     return static_cast<T *>(b.p);
   }
   xm::Launch L() const {
-    return xm::Launch{grid, grid_cg, grid_mv64, grid_cg32, grid_up32, ntile, stream};
+    return xm::Launch{grid, grid_cg, grid_mv64, grid_cg32, grid_up32, ntile, stream, mx_jac,
+                      mx_poly};
   }
 };
 
@@ -289,8 +294,9 @@ cudaGraphExec_t capture_graph(efdc_xm_ctx *c, Body body) {
 // `n` CG iterations: whole graphs where they fit, single launches for the rest.
 int run_iters(efdc_xm_ctx *c, bool mixed, double *P, int n) {
   const xm::Launch l = c->L();
-  cudaGraphExec_t &gr = mixed ? c->graph_mx : c->graph_cg;
-  bool &failed = mixed ? c->graph_mx_failed : c->graph_cg_failed;
+  const int kind = (c->mx_jac ? 1 : 0) | (c->mx_poly ? 2 : 0);  // the kernels the graph holds
+  cudaGraphExec_t &gr = mixed ? c->graph_mx[kind] : c->graph_cg;
+  bool &failed = mixed ? c->graph_mx_failed[kind] : c->graph_cg_failed;
   auto one = [&]() {
     if (mixed)
       xm::launch_mx_iter(l, c->S, c->Y, c->ctl, c->glob, c->part);
@@ -358,10 +364,20 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
   const int max_outer = 30;
   const double rel_tol = 1e-6;  // inner: |r| down 1e-6 at least (FP32 reaches ~1e-7 here)
   xm::launch_solve_reset(l, c->ctl, c->glob, c->act, c->M);
+  // inner preconditioner per member: the Neumann polynomial halves the
+  // iterations at ~1.3x the cost of one; members whose Jacobi solve takes
+  // few iterations keep Jacobi
+  c->mx_jac = c->mx_poly = false;
+  for (int m = 0; m < c->M; ++m) {
+    c->mpoly_h[m] = c->mem[m].jac_est > 10.f ? 1 : 0;
+    if (c->act_h[m]) (c->mpoly_h[m] ? c->mx_poly : c->mx_jac) = true;
+  }
+  CK(cudaMemcpyAsync(c->mpoly, c->mpoly_h, sizeof(int) * c->M, cudaMemcpyHostToDevice, c->stream));
+  const xm::Launch lk = c->L();  // with the kinds in use
   int rc = 0;
   for (int o = 0; o < max_outer; ++o) {
-    xm::launch_outer_reset(l, c->glob);
-    xm::launch_mx_resid(l, c->S, c->Y, P, c->ctl, c->glob, c->part, fac, rel_tol, 0);
+    xm::launch_outer_reset(lk, c->glob);
+    xm::launch_mx_resid(lk, c->S, c->Y, P, c->ctl, c->glob, c->part, fac, rel_tol, 0);
     CK(cudaGetLastError());
     if ((rc = read_glob(c))) return rc;
     if (c->glob_h->ndone >= c->M) break;
@@ -378,11 +394,15 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
         return EFDC_XM_CUDA_ERROR;
       }
     }
-    xm::launch_mx_apply(l, c->S, c->Y, P, c->ctl);
+    xm::launch_mx_apply(lk, c->S, c->Y, P, c->ctl);
     CK(cudaGetLastError());
     if ((rc = read_ctl(c))) return rc;
     for (int m = 0; m < c->M; ++m)
-      if (c->act_h[m] && c->ctl_h[m].inner_iter > 0) c->mem[m].last_inner = c->ctl_h[m].inner_iter;
+      if (c->act_h[m] && c->ctl_h[m].inner_iter > 0) {
+        c->mem[m].last_inner = c->ctl_h[m].inner_iter;
+        if (o == 0)  // the first pass carries the solve
+          c->mem[m].jac_est = float(c->ctl_h[m].inner_iter) * (c->mpoly_h[m] ? 1.9f : 1.0f);
+      }
   }
   if ((rc = read_ctl(c))) return rc;
   for (int m = 0; m < c->M; ++m) {
@@ -536,13 +556,14 @@ void efdc_xm_destroy(efdc_xm_ctx *c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (auto &b : c->bufs) cudaFree(b.p);
-  void *pinned[] = {c->ctl_h, c->glob_h, c->act_h, c->sc_h, c->jobs_h, c->pser_h};
+  void *pinned[] = {c->ctl_h, c->glob_h, c->act_h, c->mpoly_h, c->sc_h, c->jobs_h, c->pser_h};
   for (void *p : pinned)
     if (p) cudaFreeHost(p);
   if (c->gslot) cudaFree(c->gslot);
   if (c->gbuf) cudaFree(c->gbuf);
   if (c->graph_cg) cudaGraphExecDestroy(c->graph_cg);
-  if (c->graph_mx) cudaGraphExecDestroy(c->graph_mx);
+  for (cudaGraphExec_t g : c->graph_mx)
+    if (g) cudaGraphExecDestroy(g);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -711,9 +732,10 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   c->ctl = c->alloc<Ctl>(M);
   c->glob = c->alloc<Glob>(1);
   c->act = c->alloc<int>(M);
+  c->mpoly = c->alloc<int>(M);
   c->part = c->alloc<double>(2 * size_t(c->nquad) + 64);
   if (!c->lidx || !c->tile_member || !tnbr_d || !kind_d || !quads_d || !qstart_d || !tend_d ||
-      !c->moff || !c->mlc || !c->sc || !c->ctl || !c->glob || !c->act || !c->part)
+      !c->moff || !c->mlc || !c->sc || !c->ctl || !c->glob || !c->act || !c->mpoly || !c->part)
     return bail("cudaMalloc failed");
   {
     std::vector<long long> moff(M);
@@ -768,15 +790,18 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   Y.ccc = D(); Y.ccs = D(); Y.ccw = D(); Y.cce = D(); Y.ccn = D(); Y.fptmp = D();
   Y.r = D(); Y.pa = D(); Y.pb = D(); Y.ap = D();
   Y.as32 = Fl(); Y.aw32 = Fl(); Y.ae32 = Fl(); Y.an32 = Fl();
-  Y.r32 = Fl(); Y.pa32 = Fl(); Y.pb32 = Fl(); Y.ap32 = Fl(); Y.x32 = Fl();
+  Y.r32 = Fl(); Y.pa32 = Fl(); Y.pb32 = Fl(); Y.ap32 = Fl(); Y.x32 = Fl(); Y.z32 = Fl();
+  Y.r32b = Fl();
+  Y.mpoly = c->mpoly;
   c->ptmp = D();
-  if (!c->ptmp || !Y.x32) return bail("cudaMalloc failed (device memory)");
+  if (!c->ptmp || !Y.x32 || !Y.z32 || !Y.r32b) return bail("cudaMalloc failed (device memory)");
   auto pin = [](void *pp, size_t bytes) {
     return cudaHostAlloc(static_cast<void **>(pp), std::max<size_t>(bytes, 1),
                          cudaHostAllocDefault) == cudaSuccess;
   };
   if (!pin(&c->ctl_h, sizeof(Ctl) * M) || !pin(&c->glob_h, sizeof(Glob)) ||
-      !pin(&c->act_h, sizeof(int) * M) || !pin(&c->sc_h, sizeof(xm::StepScalars) * M) ||
+      !pin(&c->act_h, sizeof(int) * M) || !pin(&c->mpoly_h, sizeof(int) * M) ||
+      !pin(&c->sc_h, sizeof(xm::StepScalars) * M) ||
       !pin(&c->jobs_h, sizeof(CopyJob) * MAX_JOBS))
     return bail("cudaHostAlloc failed");
   std::memset(c->ctl_h, 0, sizeof(Ctl) * M);

@@ -254,6 +254,118 @@ __device__ __forceinline__ double matvec_row_scaled(const RowGeo &g, bool valid,
          double(a.w) * double(p.w);
 }
 
+// MIXED, polynomial-preconditioned: x += alpha*p, r -= alpha*Ap at the cell
+// and (recomputed from r and Ap) at its four neighbours, then
+// z = (2I - Ahat) r = r - N r (N: the couplings AS, AW, AN = AS(LN),
+// AE = AW(LE)) -- the two-term Neumann series of Ahat^-1, symmetric positive
+// definite for a symmetric unit-diagonal Ahat with eigenvalues in (0, 2).
+// With poly == false z = r (Jacobi; unsymmetric operators).  Stores x, the
+// new r (into the other residual buffer: neighbours still read the old r for
+// their own halo) and z; adds r.z and r.r.
+__device__ __forceinline__ void update_row_poly(const RowGeo &g, bool valid,
+                                                float *__restrict__ x,
+                                                const float *__restrict__ pnew,
+                                                const float *__restrict__ r,
+                                                float *__restrict__ rnew,
+                                                const float *__restrict__ ap,
+                                                const float *__restrict__ as,
+                                                const float *__restrict__ aw,
+                                                float *__restrict__ z, float alpha, bool poly,
+                                                double &rz, double &rr) {
+  const V4<float> r0 = ld4(r + g.d0), a0 = ld4(ap + g.d0);
+  const V4<float> rn0 = {fmaf(-alpha, a0.x, r0.x), fmaf(-alpha, a0.y, r0.y),
+                         fmaf(-alpha, a0.z, r0.z), fmaf(-alpha, a0.w, r0.w)};
+  V4<float> zv = rn0;
+  if (poly) {
+    const V4<float> rN = ld4(r + g.dn), aN = ld4(ap + g.dn);
+    const V4<float> rS = ld4(r + g.ds), aS = ld4(ap + g.ds);
+    const V4<float> nN = {fmaf(-alpha, aN.x, rN.x), fmaf(-alpha, aN.y, rN.y),
+                          fmaf(-alpha, aN.z, rN.z), fmaf(-alpha, aN.w, rN.w)};
+    const V4<float> nS = {fmaf(-alpha, aS.x, rS.x), fmaf(-alpha, aS.y, rS.y),
+                          fmaf(-alpha, aS.z, rS.z), fmaf(-alpha, aS.w, rS.w)};
+    float nw = from_west(rn0), ne = from_east(rn0);
+    if (g.cx == 0) nw = fmaf(-alpha, ap[g.dwe], r[g.dwe]);
+    if (g.cx == ROWT - 1) ne = fmaf(-alpha, ap[g.dee], r[g.dee]);
+    const V4<float> ks = ld4(as + g.d0), kw = ld4(aw + g.d0), kn = ld4(as + g.dn);
+    float kwe = from_east(kw);
+    if (g.cx == ROWT - 1) kwe = aw[g.dee];
+    const V4<float> ke = {kw.y, kw.z, kw.w, kwe};
+    zv.x = rn0.x - (ks.x * nS.x + kn.x * nN.x + kw.x * nw + ke.x * rn0.y);
+    zv.y = rn0.y - (ks.y * nS.y + kn.y * nN.y + kw.y * rn0.x + ke.y * rn0.z);
+    zv.z = rn0.z - (ks.z * nS.z + kn.z * nN.z + kw.z * rn0.y + ke.z * rn0.w);
+    zv.w = rn0.w - (ks.w * nS.w + kn.w * nN.w + kw.w * rn0.z + ke.w * ne);
+  }
+  if (!valid) return;
+  V4<float> xv = ld4(x + g.d0);
+  const V4<float> pv = ld4(pnew + g.d0);
+  xv.x = fmaf(alpha, pv.x, xv.x);
+  xv.y = fmaf(alpha, pv.y, xv.y);
+  xv.z = fmaf(alpha, pv.z, xv.z);
+  xv.w = fmaf(alpha, pv.w, xv.w);
+  st4(x + g.d0, xv);
+  st4(rnew + g.d0, rn0);
+  st4(z + g.d0, zv);
+  rz += double(rn0.x) * double(zv.x) + double(rn0.y) * double(zv.y) +
+        double(rn0.z) * double(zv.z) + double(rn0.w) * double(zv.w);
+  rr += double(rn0.x) * double(rn0.x) + double(rn0.y) * double(rn0.y) +
+        double(rn0.z) * double(rn0.z) + double(rn0.w) * double(rn0.w);
+}
+
+// MIXED: z0 = (2I - Ahat) r (or r) for the first inner iteration, p_old = 0,
+// and the part of r.z.
+__device__ __forceinline__ double zinit_row(const RowGeo &g, bool valid,
+                                           const float *__restrict__ r,
+                                           const float *__restrict__ as,
+                                           const float *__restrict__ aw, float *__restrict__ z,
+                                           float *__restrict__ pold, bool poly) {
+  const V4<float> r0 = ld4(r + g.d0);
+  V4<float> zv = r0;
+  if (poly) {
+    const V4<float> rN = ld4(r + g.dn), rS = ld4(r + g.ds);
+    float rw = from_west(r0), re = from_east(r0);
+    if (g.cx == 0) rw = r[g.dwe];
+    if (g.cx == ROWT - 1) re = r[g.dee];
+    const V4<float> ks = ld4(as + g.d0), kw = ld4(aw + g.d0), kn = ld4(as + g.dn);
+    float kwe = from_east(kw);
+    if (g.cx == ROWT - 1) kwe = aw[g.dee];
+    const V4<float> ke = {kw.y, kw.z, kw.w, kwe};
+    zv.x = r0.x - (ks.x * rS.x + kn.x * rN.x + kw.x * rw + ke.x * r0.y);
+    zv.y = r0.y - (ks.y * rS.y + kn.y * rN.y + kw.y * r0.x + ke.y * r0.z);
+    zv.z = r0.z - (ks.z * rS.z + kn.z * rN.z + kw.z * r0.y + ke.z * r0.w);
+    zv.w = r0.w - (ks.w * rS.w + kn.w * rN.w + kw.w * r0.z + ke.w * re);
+  }
+  if (!valid) return 0.0;
+  st4(z + g.d0, zv);
+  st4(pold + g.d0, V4<float>{0.f, 0.f, 0.f, 0.f});
+  return double(r0.x) * double(zv.x) + double(r0.y) * double(zv.y) + double(r0.z) * double(zv.z) +
+         double(r0.w) * double(zv.w);
+}
+
+// MIXED, Jacobi: x += alpha*p, r -= alpha*Ap (into the other residual buffer)
+// and the part of r.r (= r.z on the unit-diagonal system).
+__device__ __forceinline__ void update_row_jac(const RowGeo &g, bool valid, float *__restrict__ x,
+                                               const float *__restrict__ pnew,
+                                               const float *__restrict__ r,
+                                               float *__restrict__ rnew,
+                                               const float *__restrict__ ap, float alpha,
+                                               double &rr) {
+  if (!valid) return;
+  V4<float> xv = ld4(x + g.d0), rv = ld4(r + g.d0);
+  const V4<float> pv = ld4(pnew + g.d0), av = ld4(ap + g.d0);
+  xv.x = fmaf(alpha, pv.x, xv.x);
+  xv.y = fmaf(alpha, pv.y, xv.y);
+  xv.z = fmaf(alpha, pv.z, xv.z);
+  xv.w = fmaf(alpha, pv.w, xv.w);
+  rv.x = fmaf(-alpha, av.x, rv.x);
+  rv.y = fmaf(-alpha, av.y, rv.y);
+  rv.z = fmaf(-alpha, av.z, rv.z);
+  rv.w = fmaf(-alpha, av.w, rv.w);
+  st4(x + g.d0, xv);
+  st4(rnew + g.d0, rv);
+  rr += double(rv.x) * double(rv.x) + double(rv.y) * double(rv.y) + double(rv.z) * double(rv.z) +
+        double(rv.w) * double(rv.w);
+}
+
 // MIXED: x += alpha*p, r -= alpha*Ap and the part of r.r (= r.z, unit diagonal).
 __device__ __forceinline__ void update_row_scaled(const RowGeo &g, bool valid, float *__restrict__ x,
                                                   const float *__restrict__ pnew,

@@ -106,6 +106,9 @@ struct DevSystem {
   // Jacobi-PCG on A and needs no diagonal array:
   float *as32, *aw32, *ae32, *an32;              // off-diagonals of Ahat (E/N only if unsymmetric)
   float *r32, *pa32, *pb32, *ap32, *x32;         // FP32 inner CG vectors (scaled)
+  float *z32;                                    // preconditioned residual z = M^-1 r
+  float *r32b;                                   // second residual buffer (r32 / r32b by parity)
+  const int *mpoly;                              // [M] 1: Neumann polynomial, 0: Jacobi (per solve)
 };
 
 // Open-boundary cells (packed per member: W, E, S, N in the reference's loop order).

@@ -17,6 +17,8 @@ struct Launch {
   int grid_up32;     // CTAs of the FP32 update kernel
   int ntile;         // tiles including the ghost tile 0
   cudaStream_t stream;
+  bool mx_jac = true;    // MIXED: some member runs the Jacobi inner solve
+  bool mx_poly = false;  // MIXED: some member runs the polynomial-preconditioned one
 };
 
 // One array to move between host order and tile order (see k_scatter).
@@ -54,6 +56,8 @@ void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, C
                       double *part);
 void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       Glob *glob, double *part, int no_stop);
+void launch_mx_zinit(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
+                     double *part);
 void launch_mx_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl, Glob *glob,
                     double *part);
 void launch_backsub(const Launch &l, const DevStatic &S, const DevState &X, const int *act);

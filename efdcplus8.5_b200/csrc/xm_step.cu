@@ -440,8 +440,10 @@ __global__ void __launch_bounds__(NT) k_red_cg_update(DevStatic S, Ctl *ctl, Glo
 
 // ---------------------------------------------------------------------------
 // MIXED outer step: r = b - A*P in FP64 (the FP64 refinement residual), RSQ
-// in FP64, and the FP32 scaled inner system rhat = D^-1/2 r, p0 = rhat,
-// x = 0.  rsqm_fac scales the member's RSQM (the MIXED stop, below RSQM).
+// in FP64, and the FP32 scaled inner system's rhs rhat = D^-1/2 r with
+// x = 0 and p0 = rhat (k_mx_zinit then forms z0 = M^-1 rhat and p_old = 0 for
+// the polynomial members).  rsqm_fac scales the member's RSQM (the MIXED stop,
+// below RSQM).
 __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, DevSystem Y, const double *P,
                                                 const Ctl *ctl, double *part) {
   struct A {
@@ -999,6 +1001,7 @@ void launch_mx_resid(const Launch &l, const DevStatic &S, const DevSystem &Y, co
   k_red_mx_resid<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, rsqm_fac, rel_tol,
                                                       no_stop);
   count_launches(2);
+  launch_mx_zinit(l, S, Y, ctl, part);  // z0 = M^-1 r0 of the inner solve
 }
 void launch_mx_apply(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
                      const Ctl *ctl) {
