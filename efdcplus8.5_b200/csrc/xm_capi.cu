@@ -137,6 +137,8 @@ struct efdc_xm_ctx {
   cudaGraphExec_t graph_cg = nullptr, graph_mx[4] = {nullptr, nullptr, nullptr, nullptr};
   bool graph_cg_failed = false, graph_mx_failed[4] = {false, false, false, false};
   bool mx_jac = true, mx_poly = false;  // kinds of MIXED inner solve in use
+  xm::SysView mxview{};  // the system the MIXED solve refines (the step's assembly, or CONGRAD's)
+  bool last_mixed = false;  // the last step ran MIXED: the scaled FP64 system is formed on request
   // calibration (efdc_xm_calib_*): adjoint state, step-start snapshots,
   // the CG solution of the last step, gauge gathers
   bool calib = false;
@@ -319,6 +321,18 @@ int run_iters(efdc_xm_ctx *c, bool mixed, double *P, int n) {
   return EFDC_XM_OK;
 }
 
+// The scaled FP64 system of the last step (calpuv2c.f90:371-399), which a
+// MIXED step does not form itself; for downloads and FP64 kernel timing.
+int scaled_system(efdc_xm_ctx *c) {
+  for (int m = 0; m < c->M; ++m) c->act_h[m] = 1;
+  int rc = write_act(c);
+  if (rc) return rc;
+  xm::launch_scale(c->L(), c->S, c->X, c->Y, c->ctl, c->act, 0, 1);
+  CK(cudaGetLastError());
+  c->last_mixed = false;
+  return EFDC_XM_OK;
+}
+
 // FP64 CONGRAD of every active member on the scaled system in c->Y.  The
 // members iterate in lockstep launches; a member that has stopped is skipped
 // by the kernels.  On return c->ctl_h holds each member's outcome.
@@ -377,7 +391,7 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
   int rc = 0;
   for (int o = 0; o < max_outer; ++o) {
     xm::launch_outer_reset(lk, c->glob);
-    xm::launch_mx_resid(lk, c->S, c->Y, P, c->ctl, c->glob, c->part, fac, rel_tol, 0);
+    xm::launch_mx_resid(lk, c->S, c->mxview, c->Y, P, c->ctl, c->glob, c->part, fac, rel_tol, 0);
     CK(cudaGetLastError());
     if ((rc = read_glob(c))) return rc;
     if (c->glob_h->ndone >= c->M) break;
@@ -394,7 +408,7 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
         return EFDC_XM_CUDA_ERROR;
       }
     }
-    xm::launch_mx_apply(lk, c->S, c->Y, P, c->ctl);
+    xm::launch_mx_apply(lk, c->S, c->mxview, c->Y, P, c->ctl);
     CK(cudaGetLastError());
     if ((rc = read_ctl(c))) return rc;
     for (int m = 0; m < c->M; ++m)
@@ -794,6 +808,7 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   Y.r32b = Fl();
   Y.mpoly = c->mpoly;
   c->ptmp = D();
+  c->mxview = xm::SysView{X.fp, X.cc, X.cs, X.cw, X.ce, X.cn, 1};
   if (!c->ptmp || !Y.x32 || !Y.z32 || !Y.r32b) return bail("cudaMalloc failed (device memory)");
   auto pin = [](void *pp, size_t bytes) {
     return cudaHostAlloc(static_cast<void **>(pp), std::max<size_t>(bytes, 1),
@@ -972,6 +987,15 @@ int32_t efdc_xm_download_batch(efdc_xm_ctx *c, efdc_xm_fields *f) {
   XM_DN(ccc, Y.ccc, 0) XM_DN(ccs, Y.ccs, 0) XM_DN(ccw, Y.ccw, 0) XM_DN(cce, Y.cce, 0)
   XM_DN(ccn, Y.ccn, 0) XM_DN(fptmp, Y.fptmp, 0)
 #undef XM_DN
+  if (c->last_mixed && (f[0].ccc || f[0].ccs || f[0].ccw || f[0].cce || f[0].ccn || f[0].fptmp)) {
+    // a MIXED step solves from the unscaled assembly: the scaled system
+    // (calpuv2c.f90:371-399) is formed when it is asked for
+    if ((rc = scaled_system(c))) return rc;
+  }
+  if (f[0].hpi || f[0].hui || f[0].hvi) {  // 1/HP, 1/HU, 1/HV are formed on request
+    xm::launch_reciprocals(c->L(), c->S, c->X);
+    CK(cudaGetLastError());
+  }
   // the wet/dry lists need the mask at exit and at entry (OLDMASK)
   std::vector<std::vector<int32_t>> mask(M), oldm(M);
   bool lists = false;
@@ -1031,6 +1055,8 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
   CK(cudaSetDevice(c->device));
   const xm::Launch l = c->L();
   const bool mixed = prm[0].precision == EFDC_XM_PREC_MIXED;
+  c->mxview = xm::SysView{c->X.fp, c->X.cc, c->X.cs, c->X.cw, c->X.ce, c->X.cn, 1};
+  c->last_mixed = mixed;
   bool any_isdry = false, any_legacy = false, any99 = false, any_waste = false;
   std::vector<int> ncordry(M, 0), status(M, EFDC_XM_OK), max_sweeps(M);
   for (int m = 0; m < M; ++m) {
@@ -1287,6 +1313,8 @@ int32_t efdc_xm_congrad(efdc_xm_ctx *c, const double *ccc, const double *ccs, co
   c->act_h[0] = 1;
   if ((rc = write_act(c))) return rc;
   const bool mixed = precision == EFDC_XM_PREC_MIXED;
+  c->mxview = xm::SysView{c->Y.fptmp, c->Y.ccc, c->Y.ccs, c->Y.ccw, c->Y.cce, c->Y.ccn, 0};
+  c->last_mixed = false;
   xm::launch_sys_prepare(c->L(), c->S, c->Y, c->ctl, mixed ? 1 : 0);
   CK(cudaGetLastError());
   rc = mixed ? solve_mixed(c, c->X.p, 0.0) : solve_fp64(c, c->X.p);
@@ -1315,6 +1343,10 @@ int32_t efdc_xm_time_kernels(efdc_xm_ctx *c, int32_t precision, int32_t reps, ef
   CK(cudaSetDevice(c->device));
   const xm::Launch l = c->L();
   const bool mixed = precision == EFDC_XM_PREC_MIXED;
+  if (!mixed && c->last_mixed) {
+    const int rc0 = scaled_system(c);
+    if (rc0) return rc0;
+  }
   // the iterations run on a scratch copy of P with the stop tests disabled;
   // all launches are queued back to back (one untimed warm-up pair first),
   // so the events bracket device execution only, not host launch latency
@@ -1325,7 +1357,8 @@ int32_t efdc_xm_time_kernels(efdc_xm_ctx *c, int32_t precision, int32_t reps, ef
   if (rc) return rc;
   xm::launch_solve_reset(l, c->ctl, c->glob, c->act, c->M);
   if (mixed)
-    xm::launch_mx_resid(l, c->S, c->Y, c->ptmp, c->ctl, c->glob, c->part, 1.0, 0.0, 1);
+    xm::launch_mx_resid(l, c->S, c->mxview, c->Y, c->ptmp, c->ctl, c->glob, c->part, 1.0, 0.0,
+                        1);
   else
     xm::launch_cg_init(l, c->S, c->Y, c->ptmp, c->ctl, c->glob, c->part);
   CK(cudaGetLastError());

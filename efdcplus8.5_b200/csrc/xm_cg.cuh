@@ -418,24 +418,24 @@ __device__ __forceinline__ void update_row(const RowGeo &g, bool valid, T *__res
 }
 
 // RCG = FPTMP - CCC*P - CCN*PN - CCS*PS - CCW*PW - CCE*PE (congrad.f90:72) in
-// FP64 on a row vector; land slots give 0.
+// FP64 on a row vector of the system V; land slots give 0.
 __device__ __forceinline__ V4<double> residual_row(const RowGeo &g, const uint8_t *kind,
                                                    const double *__restrict__ P,
-                                                   const DevSystem &Y, bool asym) {
+                                                   const SysView &V, bool asym) {
   const V4<double> x = ld4(P + g.d0), xn = ld4(P + g.dn), xs = ld4(P + g.ds);
   double xw = from_west(x), xe = from_east(x);
   if (g.cx == 0) xw = P[g.dwe];
   if (g.cx == ROWT - 1) xe = P[g.dee];
-  const V4<double> b = ld4(Y.fptmp + g.d0), c = ld4(Y.ccc + g.d0), ks = ld4(Y.ccs + g.d0),
-                   kw = ld4(Y.ccw + g.d0);
+  const V4<double> b = ld4(V.fp + g.d0), c = ld4(V.cc + g.d0), ks = ld4(V.cs + g.d0),
+                   kw = ld4(V.cw + g.d0);
   V4<double> kn, ke;
   if (asym) {
-    kn = ld4(Y.ccn + g.d0);
-    ke = ld4(Y.cce + g.d0);
+    kn = ld4(V.cn + g.d0);
+    ke = ld4(V.ce + g.d0);
   } else {  // CCN(L) = CCS(LN), CCE(L) = CCW(LE)
-    kn = ld4(Y.ccs + g.dn);
+    kn = ld4(V.cs + g.dn);
     double kwe = from_east(kw);
-    if (g.cx == ROWT - 1) kwe = Y.ccw[g.dee];
+    if (g.cx == ROWT - 1) kwe = V.cw[g.dee];
     ke = {kw.y, kw.z, kw.w, kwe};
   }
   const uchar4 kd = *reinterpret_cast<const uchar4 *>(kind + g.d0);
@@ -449,6 +449,17 @@ __device__ __forceinline__ V4<double> residual_row(const RowGeo &g, const uint8_
   if (kd.z == LAND) r.z = 0.;
   if (kd.w == LAND) r.w = 0.;
   return r;
+}
+
+__device__ __forceinline__ V4<double> residual_row(const RowGeo &g, const uint8_t *kind,
+                                                   const double *__restrict__ P,
+                                                   const DevSystem &Y, bool asym) {
+  return residual_row(g, kind, P, SysView{Y.fptmp, Y.ccc, Y.ccs, Y.ccw, Y.cce, Y.ccn, 0}, asym);
+}
+
+// x / sqrt(c), 0 where c == 0 (land slots of an unscaled system)
+__device__ __forceinline__ double div_sqrt(double x, double c) {
+  return c > 0.0 ? x / sqrt(c) : 0.0;
 }
 
 }  // namespace xm

@@ -111,6 +111,15 @@ struct DevSystem {
   const int *mpoly;                              // [M] 1: Neumann polynomial, 0: Jacobi (per solve)
 };
 
+// The system a MIXED solve refines: a step's unscaled assembly (FP, CC, CS,
+// CW, CE, CN), or a caller's scaled system (standalone CONGRAD).  The inner
+// operator D^-1/2 A D^-1/2 and the correction D^-1/2 x do not depend on the
+// scaling; only RSQ (taken on the scaled system, as CONGRAD's) does.
+struct SysView {
+  const double *fp, *cc, *cs, *cw, *ce, *cn;
+  int unscaled;  // 1: RSQ = sum(r^2) / CCMNM^2
+};
+
 // Open-boundary cells (packed per member: W, E, S, N in the reference's loop order).
 struct DevObc {
   int n;                 // total number of open-boundary cells

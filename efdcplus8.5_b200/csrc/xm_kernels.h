@@ -47,11 +47,11 @@ void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, C
                       double *part);
 void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                       Glob *glob, double *part, int no_stop);
-void launch_mx_resid(const Launch &l, const DevStatic &S, const DevSystem &Y, const double *P,
-                     Ctl *ctl, Glob *glob, double *part, double rsqm_fac, double rel_tol,
-                     int no_stop);
-void launch_mx_apply(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
-                     const Ctl *ctl);
+void launch_mx_resid(const Launch &l, const DevStatic &S, const SysView &V, const DevSystem &Y,
+                     const double *P, Ctl *ctl, Glob *glob, double *part, double rsqm_fac,
+                     double rel_tol, int no_stop);
+void launch_mx_apply(const Launch &l, const DevStatic &S, const SysView &V, const DevSystem &Y,
+                     double *P, const Ctl *ctl);
 void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part);
 void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
@@ -67,6 +67,7 @@ void launch_wetdry(const Launch &l, const DevStatic &S, const DevState &X, Ctl *
                    const int *act, bool any_legacy, bool any99);
 void launch_final(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
                   const int *act, bool any_waste);
+void launch_reciprocals(const Launch &l, const DevStatic &S, const DevState &X);
 void launch_scatter(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx,
                     const int *tile_member, const long long *moff, const int *mlc, int nslot);
 void launch_gather(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx,

@@ -260,23 +260,37 @@ __global__ void __launch_bounds__(NT) k_scale(DevStatic S, DevState X, DevSystem
   }
 }
 
-// MIXED: the FP32 inner operator Ahat = D^-1/2 A D^-1/2 with D = CCC (unit
-// diagonal): AS(L) = CCS(L)/sqrt(CCC(L)*CCC(LS)), AW likewise; AE, AN only
-// when the operator can be unsymmetric (else AE(L)=AW(LE), AN(L)=AS(LN)).
-__global__ void __launch_bounds__(NT) k_scale32(DevStatic S, DevSystem Y, int ntile,
-                                               const int *act, int write_cross) {
+// MIXED: the FP32 inner operator Ahat = D^-1/2 A D^-1/2 with D = the diagonal
+// of the system V (unit diagonal): AS(L) = CS(L)/sqrt(CC(L)*CC(LS)), AW alike;
+// AE, AN only when the operator can be unsymmetric (else AE(L)=AW(LE),
+// AN(L)=AS(LN)).  Ahat does not depend on V's scaling, so a step's MIXED solve
+// uses the unscaled assembly directly.  With detect_asym the member's
+// asymmetry flag is set here (CE(L) /= CW(LE) or CN(L) /= CS(LN)).
+__global__ void __launch_bounds__(NT) k_scale32(DevStatic S, SysView V, DevSystem Y, int ntile,
+                                               Ctl *ctl, const int *act, int write_cross,
+                                               int detect_asym) {
   TILE_LOOP(ntile) {
-    if (act && !act[S.tile_member[tile]]) continue;
+    const int m = S.tile_member[tile];
+    if (act && !act[m]) continue;
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
-    if (S.kind[d] == LAND) continue;
-    const double di = 1. / sqrt(Y.ccc[d]);
-    Y.as32[d] = float(Y.ccs[d] * di / sqrt(Y.ccc[q.s]));
-    Y.aw32[d] = float(Y.ccw[d] * di / sqrt(Y.ccc[q.w]));
-    if (write_cross) {
-      Y.ae32[d] = float(Y.cce[d] * di / sqrt(Y.ccc[q.e]));
-      Y.an32[d] = float(Y.ccn[d] * di / sqrt(Y.ccc[q.n]));
+    bool asym = false;
+    if (S.kind[d] != LAND) {
+      const double di = 1. / sqrt(V.cc[d]);
+      auto off = [&](double cnb, int x) {
+        return S.kind[x] == LAND ? 0.f : float(cnb * di / sqrt(V.cc[x]));
+      };
+      Y.as32[d] = off(V.cs[d], q.s);
+      Y.aw32[d] = off(V.cw[d], q.w);
+      if (write_cross) {
+        Y.ae32[d] = off(V.ce[d], q.e);
+        Y.an32[d] = off(V.cn[d], q.n);
+      }
+      if (detect_asym) asym = (V.ce[d] != V.cw[q.e]) || (V.cn[d] != V.cs[q.n]);
     }
+    // unsymmetric without the cross coefficients written: bit 2, as k_scale
+    if (detect_asym && __syncthreads_or(asym) && threadIdx.x == 0)
+      atomicOr(&ctl[m].asym, write_cross ? 1 : 3);
   }
 }
 
@@ -444,18 +458,18 @@ __global__ void __launch_bounds__(NT) k_red_cg_update(DevStatic S, Ctl *ctl, Glo
 // x = 0 and p0 = rhat (k_mx_zinit then forms z0 = M^-1 rhat and p_old = 0 for
 // the polynomial members).  rsqm_fac scales the member's RSQM (the MIXED stop,
 // below RSQM).
-__global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, DevSystem Y, const double *P,
-                                                const Ctl *ctl, double *part) {
+__global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, SysView V, DevSystem Y,
+                                                const double *P, const Ctl *ctl, double *part) {
   struct A {
     bool skip, asym;
   };
   quad_sweep<2>(
       S, part, [&](int m) { return A{ctl[m].done != 0, ctl[m].asym != 0}; },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
-        const V4<double> r = residual_row(g, S.kind, P, Y, a.asym);
-        const V4<double> c = ld4(Y.ccc + g.d0);
-        const V4<float> r32 = {float(r.x / sqrt(c.x)), float(r.y / sqrt(c.y)),
-                               float(r.z / sqrt(c.z)), float(r.w / sqrt(c.w))};
+        const V4<double> r = residual_row(g, S.kind, P, V, a.asym);
+        const V4<double> c = ld4(V.cc + g.d0);
+        const V4<float> r32 = {float(div_sqrt(r.x, c.x)), float(div_sqrt(r.y, c.y)),
+                               float(div_sqrt(r.z, c.z)), float(div_sqrt(r.w, c.w))};
         if (valid) {
           st4(Y.r32 + g.d0, r32);
           st4(Y.pa32 + g.d0, r32);
@@ -468,13 +482,18 @@ __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, DevSystem Y, const
 }
 __global__ void __launch_bounds__(NT) k_red_mx_resid(DevStatic S, Ctl *ctl, Glob *glob,
                                                     const double *part, double rsqm_fac,
-                                                    double rel_tol, int no_stop) {
+                                                    double rel_tol, int no_stop, int unscaled) {
   member_reduce<2>(
       S, part, [&](int m) { return ctl[m].done != 0; },
       [&](int m, const double *sum) {
         if (threadIdx.x != 0) return;
         Ctl &k = ctl[m];
-        const double rsq = sum[0], rz = sum[1];
+        double rsq = sum[0];
+        if (unscaled) {  // RSQ of the scaled system, as CONGRAD measures it
+          const double ccmnm = fmin(k.ccmnm_int, k.ccmnm_bc);
+          rsq = rsq / (ccmnm * ccmnm);
+        }
+        const double rz = sum[1];
         const double rsqm = S.sc[m].rsqm * rsqm_fac;
         k.rsq64 = rsq;
         k.rsq = rsq;
@@ -507,18 +526,18 @@ __global__ void __launch_bounds__(NT) k_red_mx_resid(DevStatic S, Ctl *ctl, Glob
 
 // MIXED: P += D^-1/2 x32 (the FP32 correction of the scaled system) for the
 // members whose inner solve finished.
-__global__ void __launch_bounds__(NT) k_mx_apply(DevStatic S, DevSystem Y, double *P,
+__global__ void __launch_bounds__(NT) k_mx_apply(DevStatic S, SysView V, DevSystem Y, double *P,
                                                 const Ctl *ctl) {
   quad_apply(
       S, [&](int m) { return ctl[m].done || !ctl[m].idone; },
       [&](int, const RowGeo &g) {
         V4<double> x = ld4(P + g.d0);
-        const V4<double> c = ld4(Y.ccc + g.d0);
+        const V4<double> c = ld4(V.cc + g.d0);
         const V4<float> d = ld4(Y.x32 + g.d0);
-        x.x = x.x + double(d.x) / sqrt(c.x);
-        x.y = x.y + double(d.y) / sqrt(c.y);
-        x.z = x.z + double(d.z) / sqrt(c.z);
-        x.w = x.w + double(d.w) / sqrt(c.w);
+        x.x = x.x + div_sqrt(double(d.x), c.x);
+        x.y = x.y + div_sqrt(double(d.y), c.y);
+        x.z = x.z + div_sqrt(double(d.z), c.z);
+        x.w = x.w + div_sqrt(double(d.w), c.w);
         st4(P + g.d0, x);
       });
 }
@@ -837,7 +856,8 @@ __global__ void __launch_bounds__(NT) k_fin_waste(DevStatic S, DevState X, int n
   }
 }
 
-// :893-931 final P (ISDRY=0), HU, HV, reciprocals, LMASKDRY; NEGDEP count.
+// :893-931 final P (ISDRY=0), HU, HV, LMASKDRY; NEGDEP count (the reciprocals
+// HPI, HUI, HVI are formed when downloaded: k_reciprocals).
 __global__ void __launch_bounds__(NT) k_fin(DevStatic S, DevState X, int ntile, Ctl *ctl,
                                            const int *act) {
   TILE_LOOP(ntile) {
@@ -854,9 +874,6 @@ __global__ void __launch_bounds__(NT) k_fin(DevStatic S, DevState X, int ntile, 
       const double hv = (dxyp * hp + S.dxyp[q.s] * X.hp[q.s]) * S.fsgzv[d];
       X.hu[d] = hu;
       X.hv[d] = hv;
-      X.hpi[d] = 1. / hp;
-      X.hui[d] = 1. / hu;
-      X.hvi[d] = 1. / hv;
       if (c.isdry > 0) {
         int mask = 1;
         if (hp < c.hdry) {
@@ -953,12 +970,13 @@ void launch_obc_reset(const Launch &l, const DevStatic &S, const DevObc &B, cons
 }
 void launch_scale(const Launch &l, const DevStatic &S, const DevState &X, const DevSystem &Y,
                   Ctl *ctl, const int *act, int mixed, int write_cross) {
-  k_scale<<<l.grid, NT, 0, l.stream>>>(S, X, Y, l.ntile, ctl, act, write_cross);
-  count_launches(1);
-  if (mixed) {
-    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, act, write_cross);
-    count_launches(1);
+  if (mixed) {  // the FP32 operator straight from the unscaled assembly
+    const SysView V{X.fp, X.cc, X.cs, X.cw, X.ce, X.cn, 1};
+    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, V, Y, l.ntile, ctl, act, write_cross, 1);
+  } else {
+    k_scale<<<l.grid, NT, 0, l.stream>>>(S, X, Y, l.ntile, ctl, act, write_cross);
   }
+  count_launches(1);
 }
 void launch_solve_reset(const Launch &l, Ctl *ctl, Glob *glob, const int *act, int nmember) {
   k_solve_reset<<<1, 256, 0, l.stream>>>(ctl, glob, act, nmember);
@@ -994,18 +1012,18 @@ void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, dou
   launch_cg_matvec(l, S, Y, ctl, part);
   launch_cg_update(l, S, Y, P, ctl, glob, part, 0);
 }
-void launch_mx_resid(const Launch &l, const DevStatic &S, const DevSystem &Y, const double *P,
-                     Ctl *ctl, Glob *glob, double *part, double rsqm_fac, double rel_tol,
-                     int no_stop) {
-  k_mx_resid<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, part);
+void launch_mx_resid(const Launch &l, const DevStatic &S, const SysView &V, const DevSystem &Y,
+                     const double *P, Ctl *ctl, Glob *glob, double *part, double rsqm_fac,
+                     double rel_tol, int no_stop) {
+  k_mx_resid<<<l.grid_cg, NT, 0, l.stream>>>(S, V, Y, P, ctl, part);
   k_red_mx_resid<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, rsqm_fac, rel_tol,
-                                                      no_stop);
+                                                      no_stop, V.unscaled);
   count_launches(2);
   launch_mx_zinit(l, S, Y, ctl, part);  // z0 = M^-1 r0 of the inner solve
 }
-void launch_mx_apply(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
-                     const Ctl *ctl) {
-  k_mx_apply<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl);
+void launch_mx_apply(const Launch &l, const DevStatic &S, const SysView &V, const DevSystem &Y,
+                     double *P, const Ctl *ctl) {
+  k_mx_apply<<<l.grid_cg, NT, 0, l.stream>>>(S, V, Y, P, ctl);
   count_launches(1);
 }
 void launch_backsub(const Launch &l, const DevStatic &S, const DevState &X, const int *act) {
@@ -1044,6 +1062,22 @@ void launch_final(const Launch &l, const DevStatic &S, const DevState &X, Ctl *c
   k_fin<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, ctl, act);
   count_launches(1);
 }
+// HPI, HUI, HVI (calpuv2c.f90:896-906) from the final HP, HU, HV: outputs
+// only (nothing on the device reads them), formed when they are downloaded.
+__global__ void __launch_bounds__(NT) k_reciprocals(DevStatic S, DevState X, int ntile) {
+  TILE_LOOP(ntile) {
+    const int d = tile * TILE + threadIdx.x;
+    if (S.kind[d] == LAND) continue;
+    X.hpi[d] = 1. / X.hp[d];
+    X.hui[d] = 1. / X.hu[d];
+    X.hvi[d] = 1. / X.hv[d];
+  }
+}
+void launch_reciprocals(const Launch &l, const DevStatic &S, const DevState &X) {
+  k_reciprocals<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+  count_launches(1);
+}
+
 void launch_scatter(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx,
                     const int *tile_member, const long long *moff, const int *mlc, int nslot) {
   if (njob == 0) return;
@@ -1063,7 +1097,8 @@ void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y,
   k_sys_prepare<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, ctl);
   count_launches(1);
   if (mixed) {  // the standalone system may be unsymmetric: always the 4-array form
-    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, Y, l.ntile, nullptr, 1);
+    const SysView V{Y.fptmp, Y.ccc, Y.ccs, Y.ccw, Y.cce, Y.ccn, 0};
+    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, V, Y, l.ntile, ctl, nullptr, 1, 0);
     count_launches(1);
   }
 }
