@@ -499,6 +499,9 @@ def ours(args):
         l0 = lib.efdc_xm_kernel_launches()
         times, iters, outer = [], np.zeros(M, np.int64), 0
         per_step_iters = []
+        # the timed MIXED steps are the profiler range (ncu --profile-from-start off)
+        if prec == X.PREC_MIXED:
+            torch.cuda.profiler.start()
         for _ in range(steps):
             n += 1
             if flush is not None:
@@ -515,6 +518,8 @@ def ours(args):
             outer += sum(st.outer_refinements for st in sts)
             times.append(tm.ms)
         torch.cuda.synchronize()
+        if prec == X.PREC_MIXED:
+            torch.cuda.profiler.stop()
         barrier()
         launches = lib.efdc_xm_kernel_launches() - l0
         out = [{"p": np.zeros(s.lc)} for s in scns]

@@ -139,6 +139,7 @@ struct efdc_xm_ctx {
   bool mx_jac = true, mx_poly = false;  // kinds of MIXED inner solve in use
   xm::SysView mxview{};  // the system the MIXED solve refines (the step's assembly, or CONGRAD's)
   bool last_mixed = false;  // the last step ran MIXED: the scaled FP64 system is formed on request
+  bool sys_external = false;  // the system being solved is a caller's (efdc_xm_congrad)
   // calibration (efdc_xm_calib_*): adjoint state, step-start snapshots,
   // the CG solution of the last step, gauge gathers
   bool calib = false;
@@ -380,11 +381,20 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
   xm::launch_solve_reset(l, c->ctl, c->glob, c->act, c->M);
   // inner preconditioner per member: the Neumann polynomial halves the
   // iterations at ~1.3x the cost of one; members whose Jacobi solve takes
-  // few iterations keep Jacobi
+  // few iterations keep Jacobi.  A member whose operator turns out
+  // unsymmetric (its flag is set on the device) runs Jacobi whatever the
+  // choice, so the Jacobi kernels are launched too wherever that can happen:
+  // a radiation boundary, or a caller's standalone system.
   c->mx_jac = c->mx_poly = false;
   for (int m = 0; m < c->M; ++m) {
     c->mpoly_h[m] = c->mem[m].jac_est > 10.f ? 1 : 0;
-    if (c->act_h[m]) (c->mpoly_h[m] ? c->mx_poly : c->mx_jac) = true;
+    if (!c->act_h[m]) continue;
+    if (!c->mpoly_h[m]) {
+      c->mx_jac = true;
+    } else {
+      c->mx_poly = true;
+      if (c->mem[m].may_asym || c->sys_external) c->mx_jac = true;
+    }
   }
   CK(cudaMemcpyAsync(c->mpoly, c->mpoly_h, sizeof(int) * c->M, cudaMemcpyHostToDevice, c->stream));
   const xm::Launch lk = c->L();  // with the kinds in use
@@ -414,8 +424,10 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
     for (int m = 0; m < c->M; ++m)
       if (c->act_h[m] && c->ctl_h[m].inner_iter > 0) {
         c->mem[m].last_inner = c->ctl_h[m].inner_iter;
-        if (o == 0)  // the first pass carries the solve
-          c->mem[m].jac_est = float(c->ctl_h[m].inner_iter) * (c->mpoly_h[m] ? 1.9f : 1.0f);
+        if (o == 0) {  // the first pass carries the solve
+          const bool poly = c->mpoly_h[m] && !c->ctl_h[m].asym;
+          c->mem[m].jac_est = float(c->ctl_h[m].inner_iter) * (poly ? 1.9f : 1.0f);
+        }
       }
   }
   if ((rc = read_ctl(c))) return rc;
@@ -1057,6 +1069,7 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
   const bool mixed = prm[0].precision == EFDC_XM_PREC_MIXED;
   c->mxview = xm::SysView{c->X.fp, c->X.cc, c->X.cs, c->X.cw, c->X.ce, c->X.cn, 1};
   c->last_mixed = mixed;
+  c->sys_external = false;
   bool any_isdry = false, any_legacy = false, any99 = false, any_waste = false;
   std::vector<int> ncordry(M, 0), status(M, EFDC_XM_OK), max_sweeps(M);
   for (int m = 0; m < M; ++m) {
@@ -1090,7 +1103,7 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
   for (;;) {  // 1000 CONTINUE, for the members still sweeping
     xm::launch_sweep_reset(l, c->ctl, c->act, M);
     xm::launch_assemble(l, c->S, c->X, c->ctl, c->act);
-    xm::launch_obc(l, c->S, c->X, c->B, c->ctl, c->act, c->obc_serial);
+    xm::launch_obc(l, c->S, c->X, c->B, c->ctl, c->act, c->obc_serial, c->any_may_asym ? 1 : 0);
     xm::launch_scale(l, c->S, c->X, c->Y, c->ctl, c->act, mixed ? 1 : 0, c->any_may_asym ? 1 : 0);
     CK(cudaGetLastError());
     rc = mixed ? solve_mixed(c, c->X.p, prm[0].mixed_rsq_factor) : solve_fp64(c, c->X.p);
@@ -1315,6 +1328,7 @@ int32_t efdc_xm_congrad(efdc_xm_ctx *c, const double *ccc, const double *ccs, co
   const bool mixed = precision == EFDC_XM_PREC_MIXED;
   c->mxview = xm::SysView{c->Y.fptmp, c->Y.ccc, c->Y.ccs, c->Y.ccw, c->Y.cce, c->Y.ccn, 0};
   c->last_mixed = false;
+  c->sys_external = true;
   xm::launch_sys_prepare(c->L(), c->S, c->Y, c->ctl, mixed ? 1 : 0);
   CK(cudaGetLastError());
   rc = mixed ? solve_mixed(c, c->X.p, 0.0) : solve_fp64(c, c->X.p);

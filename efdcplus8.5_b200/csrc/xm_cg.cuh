@@ -457,9 +457,17 @@ __device__ __forceinline__ V4<double> residual_row(const RowGeo &g, const uint8_
   return residual_row(g, kind, P, SysView{Y.fptmp, Y.ccc, Y.ccs, Y.ccw, Y.cce, Y.ccn, 0}, asym);
 }
 
-// x / sqrt(c), 0 where c == 0 (land slots of an unscaled system)
-__device__ __forceinline__ double div_sqrt(double x, double c) {
-  return c > 0.0 ? x / sqrt(c) : 0.0;
+// The Jacobi scaling of the MIXED inner system, 1/sqrt(c) for a diagonal c
+// (0 where c <= 0: land slots of an unscaled system): the FP32 hardware
+// estimate refined by one Newton-Raphson step y(3 - c y^2)/2 in FP64
+// (relative error ~1e-13).  Explicitly rounded operations, so every kernel
+// (whatever its contraction flags) gets the same value for the same c: the
+// operator, the scaled residual and the correction all use one D.
+__device__ __forceinline__ double inv_sqrt_diag(double c) {
+  if (!(c > 0.0)) return 0.0;
+  const double y = double(rsqrtf(float(c)));
+  const double t = __dmul_rn(__dmul_rn(c, y), y);
+  return __dmul_rn(y, __fma_rn(-0.5, t, 1.5));
 }
 
 }  // namespace xm

@@ -33,7 +33,7 @@ void launch_sweep_reset(const Launch &l, Ctl *ctl, const int *act, int nmember);
 void launch_assemble(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
                      const int *act);
 void launch_obc(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B, Ctl *ctl,
-                const int *act, bool serial);
+                const int *act, bool serial, int write_cross);
 void launch_obc_reset(const Launch &l, const DevStatic &S, const DevObc &B, const DevState &X);
 void launch_scale(const Launch &l, const DevStatic &S, const DevState &X, const DevSystem &Y,
                   Ctl *ctl, const int *act, int mixed, int write_cross);

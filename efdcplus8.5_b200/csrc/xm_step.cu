@@ -229,9 +229,9 @@ __global__ void k_obc_reset(DevStatic S, DevObc B, DevState X) {
 }
 
 // ---------------------------------------------------------------------------
-// calpuv2c.f90:371-399: scale by the member's minimum diagonal.  Also flags an
-// unsymmetric operator (CE(L) /= CW(LE) or CN(L) /= CS(LN)), which only a
-// radiation boundary with a closed interior face produces.
+// calpuv2c.f90:371-399: scale by the member's minimum diagonal.  CE and CN
+// are scaled only when the batch holds a possibly unsymmetric member
+// (write_cross); otherwise the CG reads CCE(L) = CCW(LE), CCN(L) = CCS(LN).
 __global__ void __launch_bounds__(NT) k_scale(DevStatic S, DevState X, DevSystem Y, int ntile,
                                              Ctl *ctl, const int *act, int write_cross) {
   TILE_LOOP(ntile) {
@@ -239,58 +239,65 @@ __global__ void __launch_bounds__(NT) k_scale(DevStatic S, DevState X, DevSystem
     if (!act[m]) continue;
     const double CCMNM = fmin(ctl[m].ccmnm_int, ctl[m].ccmnm_bc);
     const double CCMNMI = 1. / CCMNM;
-    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
-    const int d = q.d;
-    bool asym = false;
-    if (S.kind[d] != LAND) {
-      const double cs = X.cs[d], cw = X.cw[d], ce = X.ce[d], cn = X.cn[d];
-      asym = (ce != X.cw[q.e]) || (cn != X.cs[q.n]);
-      Y.ccs[d] = cs * CCMNMI;
-      Y.ccw[d] = cw * CCMNMI;
-      Y.ccc[d] = X.cc[d] * CCMNMI;
-      Y.fptmp[d] = X.fp[d] * CCMNMI;
-      if (write_cross) {
-        Y.cce[d] = ce * CCMNMI;
-        Y.ccn[d] = cn * CCMNMI;
-      }
+    const int d = tile * TILE + threadIdx.x;
+    if (S.kind[d] == LAND) continue;
+    Y.ccs[d] = X.cs[d] * CCMNMI;
+    Y.ccw[d] = X.cw[d] * CCMNMI;
+    Y.ccc[d] = X.cc[d] * CCMNMI;
+    Y.fptmp[d] = X.fp[d] * CCMNMI;
+    if (write_cross) {
+      Y.cce[d] = X.ce[d] * CCMNMI;
+      Y.ccn[d] = X.cn[d] * CCMNMI;
     }
-    // unsymmetric without the cross coefficients written cannot be solved:
-    // flag it (bit 2) so that the host reports it
-    if (__syncthreads_or(asym) && threadIdx.x == 0) atomicOr(&ctl[m].asym, write_cross ? 1 : 3);
   }
 }
 
-// MIXED: the FP32 inner operator Ahat = D^-1/2 A D^-1/2 with D = the diagonal
-// of the system V (unit diagonal): AS(L) = CS(L)/sqrt(CC(L)*CC(LS)), AW alike;
-// AE, AN only when the operator can be unsymmetric (else AE(L)=AW(LE),
-// AN(L)=AS(LN)).  Ahat does not depend on V's scaling, so a step's MIXED solve
-// uses the unscaled assembly directly.  With detect_asym the member's
-// asymmetry flag is set here (CE(L) /= CW(LE) or CN(L) /= CS(LN)).
+// MIXED: the FP32 inner operator Ahat = D A D with D = diag(inv_sqrt_diag(CC))
+// (unit diagonal): AS(L) = CS(L)*D(L)*D(LS), AW alike; AE, AN only when the
+// operator can be unsymmetric (else AE(L)=AW(LE), AN(L)=AS(LN)).  Ahat does
+// not depend on the system's scaling, so a step's MIXED solve uses the
+// unscaled assembly directly.
 __global__ void __launch_bounds__(NT) k_scale32(DevStatic S, SysView V, DevSystem Y, int ntile,
-                                               Ctl *ctl, const int *act, int write_cross,
-                                               int detect_asym) {
+                                               const int *act, int write_cross) {
   TILE_LOOP(ntile) {
     const int m = S.tile_member[tile];
     if (act && !act[m]) continue;
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
-    bool asym = false;
-    if (S.kind[d] != LAND) {
-      const double di = 1. / sqrt(V.cc[d]);
-      auto off = [&](double cnb, int x) {
-        return S.kind[x] == LAND ? 0.f : float(cnb * di / sqrt(V.cc[x]));
-      };
-      Y.as32[d] = off(V.cs[d], q.s);
-      Y.aw32[d] = off(V.cw[d], q.w);
-      if (write_cross) {
-        Y.ae32[d] = off(V.ce[d], q.e);
-        Y.an32[d] = off(V.cn[d], q.n);
-      }
-      if (detect_asym) asym = (V.ce[d] != V.cw[q.e]) || (V.cn[d] != V.cs[q.n]);
+    if (S.kind[d] == LAND) continue;
+    const double di = inv_sqrt_diag(V.cc[d]);
+    auto off = [&](double cnb, int x) {
+      return S.kind[x] == LAND ? 0.f : float(cnb * di * inv_sqrt_diag(V.cc[x]));
+    };
+    Y.as32[d] = off(V.cs[d], q.s);
+    Y.aw32[d] = off(V.cw[d], q.w);
+    if (write_cross) {
+      Y.ae32[d] = off(V.ce[d], q.e);
+      Y.an32[d] = off(V.cn[d], q.n);
     }
-    // unsymmetric without the cross coefficients written: bit 2, as k_scale
-    if (detect_asym && __syncthreads_or(asym) && threadIdx.x == 0)
-      atomicOr(&ctl[m].asym, write_cross ? 1 : 3);
+  }
+}
+
+// Symmetry of the assembled operator.  The interior assembly gives CE(L) =
+// CW(LE) and CN(L) = CS(LN) bit for bit (both are built from the same face's
+// values in the same order), so only SETOPENBC/SETOPENBC2 can break it, at an
+// open-boundary cell's four faces.  One thread per boundary cell compares
+// both coefficients of each face with a water neighbour and flags the member
+// (bit 1 unsymmetric; bit 2 as well when the cross coefficients are not
+// scaled, which the host reports as an error).
+__global__ void k_obc_asym(DevStatic S, DevState X, DevObc B, Ctl *ctl, const int *act,
+                           int write_cross) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B.n; k += gridDim.x * blockDim.x) {
+    const int m = B.member[k];
+    if (!act[m]) continue;
+    const int d = B.slot[k];
+    const Nb q = neighbours_of_slot(S.tnbr, d);
+    bool a = false;
+    if (S.kind[q.e] != LAND) a |= X.ce[d] != X.cw[q.e];
+    if (S.kind[q.w] != LAND) a |= X.cw[d] != X.ce[q.w];
+    if (S.kind[q.n] != LAND) a |= X.cn[d] != X.cs[q.n];
+    if (S.kind[q.s] != LAND) a |= X.cs[d] != X.cn[q.s];
+    if (a) atomicOr(&ctl[m].asym, write_cross ? 1 : 3);
   }
 }
 
@@ -468,8 +475,8 @@ __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, SysView V, DevSyst
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         const V4<double> r = residual_row(g, S.kind, P, V, a.asym);
         const V4<double> c = ld4(V.cc + g.d0);
-        const V4<float> r32 = {float(div_sqrt(r.x, c.x)), float(div_sqrt(r.y, c.y)),
-                               float(div_sqrt(r.z, c.z)), float(div_sqrt(r.w, c.w))};
+        const V4<float> r32 = {float(r.x * inv_sqrt_diag(c.x)), float(r.y * inv_sqrt_diag(c.y)),
+                               float(r.z * inv_sqrt_diag(c.z)), float(r.w * inv_sqrt_diag(c.w))};
         if (valid) {
           st4(Y.r32 + g.d0, r32);
           st4(Y.pa32 + g.d0, r32);
@@ -534,10 +541,10 @@ __global__ void __launch_bounds__(NT) k_mx_apply(DevStatic S, SysView V, DevSyst
         V4<double> x = ld4(P + g.d0);
         const V4<double> c = ld4(V.cc + g.d0);
         const V4<float> d = ld4(Y.x32 + g.d0);
-        x.x = x.x + div_sqrt(double(d.x), c.x);
-        x.y = x.y + div_sqrt(double(d.y), c.y);
-        x.z = x.z + div_sqrt(double(d.z), c.z);
-        x.w = x.w + div_sqrt(double(d.w), c.w);
+        x.x = x.x + double(d.x) * inv_sqrt_diag(c.x);
+        x.y = x.y + double(d.y) * inv_sqrt_diag(c.y);
+        x.z = x.z + double(d.z) * inv_sqrt_diag(c.z);
+        x.w = x.w + double(d.w) * inv_sqrt_diag(c.w);
         st4(P + g.d0, x);
       });
 }
@@ -955,13 +962,14 @@ void launch_assemble(const Launch &l, const DevStatic &S, const DevState &X, Ctl
   count_launches(1);
 }
 void launch_obc(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B, Ctl *ctl,
-                const int *act, bool serial) {
+                const int *act, bool serial, int write_cross) {
   if (B.n == 0) return;
   if (serial)
     k_obc_serial<<<1, 1, 0, l.stream>>>(S, X, B, ctl, act);
   else
     k_obc_parallel<<<(B.n + NT - 1) / NT, NT, 0, l.stream>>>(S, X, B, ctl, act);
-  count_launches(1);
+  k_obc_asym<<<(B.n + NT - 1) / NT, NT, 0, l.stream>>>(S, X, B, ctl, act, write_cross);
+  count_launches(2);
 }
 void launch_obc_reset(const Launch &l, const DevStatic &S, const DevObc &B, const DevState &X) {
   if (B.n == 0) return;
@@ -972,7 +980,7 @@ void launch_scale(const Launch &l, const DevStatic &S, const DevState &X, const 
                   Ctl *ctl, const int *act, int mixed, int write_cross) {
   if (mixed) {  // the FP32 operator straight from the unscaled assembly
     const SysView V{X.fp, X.cc, X.cs, X.cw, X.ce, X.cn, 1};
-    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, V, Y, l.ntile, ctl, act, write_cross, 1);
+    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, V, Y, l.ntile, act, write_cross);
   } else {
     k_scale<<<l.grid, NT, 0, l.stream>>>(S, X, Y, l.ntile, ctl, act, write_cross);
   }
@@ -1098,7 +1106,7 @@ void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y,
   count_launches(1);
   if (mixed) {  // the standalone system may be unsymmetric: always the 4-array form
     const SysView V{Y.fptmp, Y.ccc, Y.ccs, Y.ccw, Y.cce, Y.ccn, 0};
-    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, V, Y, l.ntile, ctl, nullptr, 1, 0);
+    k_scale32<<<l.grid, NT, 0, l.stream>>>(S, V, Y, l.ntile, nullptr, 1);
     count_launches(1);
   }
 }

@@ -27,7 +27,24 @@ def build(name):
         scn = S.make_scenario(60, 40, seed=15, obc_sides=("W",), amp=0.4, dt=10.0,
                               explicit_noise=3e-4, datum=35.0, snlt=1.0)
         return scn, 10, 10.0
+    if name == "radiation_closed_face":  # unsymmetric operator, see unsymmetric()
+        return unsymmetric(), 6, 20.0
     raise KeyError(name)
+
+
+def unsymmetric():
+    """A radiation-boundary basin whose operator is unsymmetric: the interior
+    faces behind three west boundary cells are closed in the state (SUB = 0,
+    as drying leaves them while the static HRUO stays open).  CALPUV2C then
+    gives CW(LE) = 0 while SETOPENBC's radiation row keeps CE(L) = -CET
+    (setopenbc.f90:67-80), so CE(L) /= CW(LE) at those three faces."""
+    scn = S.make_scenario(40, 30, seed=16, obc_sides=("W", "E"), ispb=1, amp=0.3, dt=20.0,
+                          land_frac=0.03, explicit_noise=1e-4)
+    lw = scn.grid["obc"]["W"]["l"]
+    lec = scn.grid["lec"]
+    for L in lw[5:8]:
+        scn.state["sub"][lec[L - 1] - 1] = 0.0
+    return scn
 
 
 def state_err(a, b, la, key="p", g=S.G):
