@@ -652,7 +652,7 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   // ---- host layout: tiles, quads (4-tile CG units, never across members), slots ----
   std::vector<int4> tnbr(ntile, int4{0, 0, 0, 0});
   std::vector<int> tile_member(ntile, 0), tend(M), qstart(M + 1, 0);
-  std::vector<int2> quads;
+  std::vector<int4> quads;
   std::vector<uint8_t> kind(c->nslot, xm::LAND);
   std::vector<int> lidx(c->nslot, 0);
   std::vector<std::vector<int>> slot_of(M);
@@ -673,7 +673,8 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
     }
     tend[m] = mb.tile1;
     qstart[m] = int(quads.size());
-    for (int t = mb.tile0; t < mb.tile1; t += 4) quads.push_back(int2{m, t});
+    for (int t = mb.tile0; t < mb.tile1; t += 4)
+      quads.push_back(int4{m, t, std::min(4, mb.tile1 - t), 0});
     qstart[m + 1] = int(quads.size());
     slot_of[m].assign(size_t(mb.lc) + 1, 0);
     for (int L = 2; L <= mb.la; ++L) {
@@ -750,7 +751,7 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   c->tile_member = c->alloc<int>(ntile);
   int4 *tnbr_d = c->alloc<int4>(ntile);
   uint8_t *kind_d = c->alloc<uint8_t>(ns);
-  int2 *quads_d = c->alloc<int2>(quads.size());
+  int4 *quads_d = c->alloc<int4>(quads.size());
   int *qstart_d = c->alloc<int>(M + 1), *tend_d = c->alloc<int>(M);
   c->moff = c->alloc<long long>(M);
   c->mlc = c->alloc<int>(M);
@@ -777,7 +778,7 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   cudaMemcpy(c->tile_member, tile_member.data(), ntile * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(tnbr_d, tnbr.data(), tnbr.size() * sizeof(int4), cudaMemcpyHostToDevice);
   cudaMemcpy(kind_d, kind.data(), ns, cudaMemcpyHostToDevice);
-  cudaMemcpy(quads_d, quads.data(), quads.size() * sizeof(int2), cudaMemcpyHostToDevice);
+  cudaMemcpy(quads_d, quads.data(), quads.size() * sizeof(int4), cudaMemcpyHostToDevice);
   cudaMemcpy(qstart_d, qstart.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(tend_d, tend.data(), M * sizeof(int), cudaMemcpyHostToDevice);
   auto D = [&]() { return c->alloc<double>(ns); };

@@ -67,7 +67,7 @@ __device__ __forceinline__ void quad_store(QuadLog<NS> &L, int n, const DevStati
 // one quad row vector and adds its parts of the NS sums to v[].
 //
 // Everything a quad's loads depend on (its table entry, its member's values
-// from setup(), the member's last tile and the thread's tile-neighbour entry)
+// from setup() and the thread's tile-neighbour entry)
 // is fetched one quad ahead, so that those small dependent loads overlap the
 // current quad's memory traffic instead of preceding the next one's.  In an
 // ensemble nearly every quad of a CTA belongs to another member.
@@ -80,28 +80,22 @@ __device__ __forceinline__ void quad_sweep(const DevStatic &S, double *part, Set
   const int G = gridDim.x, NQ = S.nquad;
   int qd = blockIdx.x;
   if (qd >= NQ) return;
-  int2 cur = S.quads[qd];
+  int4 cur = S.quads[qd];
   auto a = setup(cur.x);
-  int tend = S.tend[cur.x];
-  int4 nb = __ldg(&S.tnbr[cur.y + sub < tend ? cur.y + sub : 0]);
-  int2 nxt = (qd + G < NQ) ? S.quads[qd + G] : cur;
+  int4 nb = __ldg(&S.tnbr[sub < cur.z ? cur.y + sub : 0]);
+  int4 nxt = (qd + G < NQ) ? S.quads[qd + G] : cur;
   int n = 0;
   for (;;) {
     const int qn = qd + G;
     const bool more = qn < NQ;
-    // the next quad's descriptors
+    // the next quad's descriptors (one load level after its table entry)
     auto an = a;
-    int tendn = tend;
-    if (more && nxt.x != cur.x) {
-      an = setup(nxt.x);
-      tendn = S.tend[nxt.x];
-    }
-    const int tin = nxt.y + sub;
-    const int4 nbn = __ldg(&S.tnbr[(more && tin < tendn) ? tin : 0]);
-    const int2 nn = (qn + G < NQ) ? S.quads[qn + G] : nxt;
+    if (more && nxt.x != cur.x) an = setup(nxt.x);
+    const int4 nbn = __ldg(&S.tnbr[(more && sub < nxt.z) ? nxt.y + sub : 0]);
+    const int4 nn = (qn + G < NQ) ? S.quads[qn + G] : nxt;
     if (!a.skip) {
       const int ti = cur.y + sub;
-      const bool valid = ti < tend;
+      const bool valid = sub < cur.z;
       const RowGeo g = row_geo_nb(nb, valid ? ti : 0, q);
       double v[NS];
 #pragma unroll
@@ -122,7 +116,6 @@ __device__ __forceinline__ void quad_sweep(const DevStatic &S, double *part, Set
     qd = qn;
     cur = nxt;
     a = an;
-    tend = tendn;
     nb = nbn;
     nxt = nn;
   }
@@ -151,12 +144,11 @@ template <class Skip, class Body>
 __device__ __forceinline__ void quad_apply(const DevStatic &S, Skip skip, Body body) {
   const int sub = threadIdx.x / TPT, q = threadIdx.x % TPT;
   for (int qd = blockIdx.x; qd < S.nquad; qd += gridDim.x) {
-    const int2 cur = S.quads[qd];
+    const int4 cur = S.quads[qd];
     const int m = cur.x;
     if (skip(m)) continue;
-    const int ti = cur.y + sub;
-    if (ti >= S.tend[m]) continue;
-    body(m, row_geo(S.tnbr, ti, q));
+    if (sub >= cur.z) continue;
+    body(m, row_geo(S.tnbr, cur.y + sub, q));
   }
 }
 

@@ -71,7 +71,8 @@ struct DevStatic {
   const uint8_t *kind;    // [nslot]
   const int *lidx;        // [nslot] member-local L of the slot, 0 for land
   const int *tile_member; // [ntile] member of each tile
-  const int2 *quads;      // [nquad] (member, first tile): 4-tile units of the CG kernels
+  const int4 *quads;      // [nquad] (member, first tile, tiles of the member in it (1..4), 0):
+                          // the 4-tile units of the CG kernels
   const int *qstart;      // [M+1] first quad of each member
   const int *tend;        // [M] one past the member's last tile
   const StepScalars *sc;  // [M] per-member scalars of the current step
