@@ -134,8 +134,9 @@ struct efdc_xm_ctx {
   double *ptmp = nullptr;    // scratch P for kernel timing
   // CUDA graphs of GRAPH_ITERS consecutive CG iterations on X.p (FP64) and
   // of the FP32 inner iteration, captured on first use
-  cudaGraphExec_t graph_cg = nullptr, graph_mx[4] = {nullptr, nullptr, nullptr, nullptr};
-  bool graph_cg_failed = false, graph_mx_failed[4] = {false, false, false, false};
+  // CG iteration graphs: [may_asym] (FP64), [kinds | may_asym << 2] (MIXED)
+  cudaGraphExec_t graph_cg[2] = {}, graph_mx[8] = {};
+  bool graph_cg_failed[2] = {}, graph_mx_failed[8] = {};
   bool mx_jac = true, mx_poly = false;  // kinds of MIXED inner solve in use
   xm::SysView mxview{};  // the system the MIXED solve refines (the step's assembly, or CONGRAD's)
   bool last_mixed = false;  // the last step ran MIXED: the scaled FP64 system is formed on request
@@ -161,8 +162,9 @@ struct efdc_xm_ctx {
     return static_cast<T *>(b.p);
   }
   xm::Launch L() const {
-    return xm::Launch{grid, grid_cg, grid_mv64, grid_cg32, grid_up32, ntile, stream, mx_jac,
-                      mx_poly};
+    return xm::Launch{grid,   grid_cg, grid_mv64, grid_cg32,
+                      grid_up32, ntile,  stream,    mx_jac,
+                      mx_poly, any_may_asym || sys_external};
   }
 };
 
@@ -297,9 +299,11 @@ cudaGraphExec_t capture_graph(efdc_xm_ctx *c, Body body) {
 // `n` CG iterations: whole graphs where they fit, single launches for the rest.
 int run_iters(efdc_xm_ctx *c, bool mixed, double *P, int n) {
   const xm::Launch l = c->L();
-  const int kind = (c->mx_jac ? 1 : 0) | (c->mx_poly ? 2 : 0);  // the kernels the graph holds
-  cudaGraphExec_t &gr = mixed ? c->graph_mx[kind] : c->graph_cg;
-  bool &failed = mixed ? c->graph_mx_failed[kind] : c->graph_cg_failed;
+  // the kernels the graph holds
+  const int ma = l.may_asym ? 1 : 0;
+  const int kind = (c->mx_jac ? 1 : 0) | (c->mx_poly ? 2 : 0) | (ma << 2);
+  cudaGraphExec_t &gr = mixed ? c->graph_mx[kind] : c->graph_cg[ma];
+  bool &failed = mixed ? c->graph_mx_failed[kind] : c->graph_cg_failed[ma];
   auto one = [&]() {
     if (mixed)
       xm::launch_mx_iter(l, c->S, c->Y, c->ctl, c->glob, c->part);
@@ -425,7 +429,7 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
       if (c->act_h[m] && c->ctl_h[m].inner_iter > 0) {
         c->mem[m].last_inner = c->ctl_h[m].inner_iter;
         if (o == 0) {  // the first pass carries the solve
-          const bool poly = c->mpoly_h[m] && !c->ctl_h[m].asym;
+          const bool poly = c->mpoly_h[m] && !(c->ctl_h[m].asym & 1);
           c->mem[m].jac_est = float(c->ctl_h[m].inner_iter) * (poly ? 1.9f : 1.0f);
         }
       }
@@ -587,7 +591,8 @@ void efdc_xm_destroy(efdc_xm_ctx *c) {
     if (p) cudaFreeHost(p);
   if (c->gslot) cudaFree(c->gslot);
   if (c->gbuf) cudaFree(c->gbuf);
-  if (c->graph_cg) cudaGraphExecDestroy(c->graph_cg);
+  for (cudaGraphExec_t g : c->graph_cg)
+    if (g) cudaGraphExecDestroy(g);
   for (cudaGraphExec_t g : c->graph_mx)
     if (g) cudaGraphExecDestroy(g);
   if (c->stream) cudaStreamDestroy(c->stream);

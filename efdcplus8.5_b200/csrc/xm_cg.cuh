@@ -30,6 +30,14 @@ __device__ __forceinline__ double rcpT(double x) { return 1. / x; }
 // member) and finishes the member (its Ctl).  No fences, atomics or
 // "last CTA" in the CG kernels, and sums that depend neither on the grid size
 // nor on which other members share the context.
+// A member's operator is handled as unsymmetric (the four-array form) when
+// its flag's bit 1 is set; MA = false compiles the symmetric form only, for
+// batches in which no member can be unsymmetric (no radiation boundary).
+template <bool MA>
+__device__ __forceinline__ bool unsym(const Ctl &k) {
+  return MA && (k.asym & 1) != 0;
+}
+
 constexpr int QCAP = 32;         // quads a CTA logs between two stores
 constexpr int NWARP = NT / 32;   // warps per CTA
 

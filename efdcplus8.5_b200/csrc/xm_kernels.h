@@ -19,6 +19,7 @@ struct Launch {
   cudaStream_t stream;
   bool mx_jac = true;    // MIXED: some member runs the Jacobi inner solve
   bool mx_poly = false;  // MIXED: some member runs the polynomial-preconditioned one
+  bool may_asym = true;  // some member's operator can be unsymmetric (else symmetric kernels)
 };
 
 // One array to move between host order and tile order (see k_scatter).

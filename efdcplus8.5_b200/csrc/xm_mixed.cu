@@ -22,6 +22,7 @@ namespace xm {
 
 // p = z + beta*p_old at the cell and its halo (z = r for Jacobi members),
 // Ahat*p, p.Ap (per member).
+template <bool MA>
 __global__ void __launch_bounds__(NT, 5) k_mx_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
                                                     double *part) {
   struct A {
@@ -36,8 +37,9 @@ __global__ void __launch_bounds__(NT, 5) k_mx_matvec(DevStatic S, DevSystem Y, c
       [&](int m) {
         const Ctl &k = ctl[m];
         const bool par = k.parity;
-        const bool poly = Y.mpoly[m] && !k.asym;
-        return A{(k.done | k.idone) != 0, k.asym != 0, float(k.beta), par ? Y.pb32 : Y.pa32,
+        const bool asym = unsym<MA>(k);
+        const bool poly = Y.mpoly[m] && !asym;
+        return A{(k.done | k.idone) != 0, asym, float(k.beta), par ? Y.pb32 : Y.pa32,
                  par ? Y.pa32 : Y.pb32, poly ? Y.z32 : (par ? Y.r32b : Y.r32)};
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
@@ -72,7 +74,7 @@ __global__ void __launch_bounds__(NT, 5) k_mx_update_poly(DevStatic S, DevSystem
       [&](int m) {
         const Ctl &k = ctl[m];
         const bool par = k.parity;
-        const bool poly = Y.mpoly[m] && !k.asym;
+        const bool poly = Y.mpoly[m] && !unsym<true>(k);
         return A{(k.done | k.idone) != 0 || !poly, float(k.alpha), par ? Y.pa32 : Y.pb32,
                  par ? Y.r32b : Y.r32, par ? Y.r32 : Y.r32b};
       },
@@ -96,7 +98,7 @@ __global__ void __launch_bounds__(NT) k_mx_update_jac(DevStatic S, DevSystem Y, 
       [&](int m) {
         const Ctl &k = ctl[m];
         const bool par = k.parity;
-        const bool poly = Y.mpoly[m] && !k.asym;
+        const bool poly = Y.mpoly[m] && !unsym<true>(k);
         return A{(k.done | k.idone) != 0 || poly, float(k.alpha), par ? Y.pa32 : Y.pb32,
                  par ? Y.r32b : Y.r32, par ? Y.r32 : Y.r32b};
       },
@@ -148,7 +150,7 @@ __global__ void __launch_bounds__(NT) k_mx_zinit(DevStatic S, DevSystem Y, const
   };
   quad_sweep<1>(
       S, part,
-      [&](int m) { return A{ctl[m].done != 0 || !Y.mpoly[m] || ctl[m].asym != 0, false}; },
+      [&](int m) { return A{ctl[m].done != 0 || !Y.mpoly[m] || unsym<true>(ctl[m]), false}; },
       [&](const A &, const RowGeo &g, bool valid, double *v) {
         v[0] = zinit_row(g, valid, Y.r32, Y.as32, Y.aw32, Y.z32, Y.pa32, true);
       });
@@ -156,7 +158,7 @@ __global__ void __launch_bounds__(NT) k_mx_zinit(DevStatic S, DevSystem Y, const
 __global__ void __launch_bounds__(NT) k_red_mx_zinit(DevStatic S, DevSystem Y, Ctl *ctl,
                                                      const double *part) {
   member_reduce<1>(
-      S, part, [&](int m) { return ctl[m].done != 0 || !Y.mpoly[m] || ctl[m].asym != 0; },
+      S, part, [&](int m) { return ctl[m].done != 0 || !Y.mpoly[m] || unsym<true>(ctl[m]); },
       [&](int m, const double *sum) {
         if (threadIdx.x == 0) ctl[m].rpcg = sum[0];
       });
@@ -166,7 +168,10 @@ static int reduce_grid(const DevStatic &S) { return std::min(S.nmember, 1024); }
 
 void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {
-  k_mx_matvec<<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
+  if (l.may_asym)
+    k_mx_matvec<true><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
+  else
+    k_mx_matvec<false><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
   k_red_mx_matvec<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part);
   count_launches(2);
 }
@@ -204,7 +209,7 @@ int occupancy_blocks_per_sm_mixed_update() {
 
 int occupancy_blocks_per_sm_mixed() {
   int a = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_mx_matvec, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_mx_matvec<true>, NT, 0);
   return a > 0 ? a : 1;
 }
 

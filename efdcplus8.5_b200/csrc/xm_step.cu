@@ -282,9 +282,9 @@ __global__ void __launch_bounds__(NT) k_scale32(DevStatic S, SysView V, DevSyste
 // CW(LE) and CN(L) = CS(LN) bit for bit (both are built from the same face's
 // values in the same order), so only SETOPENBC/SETOPENBC2 can break it, at an
 // open-boundary cell's four faces.  One thread per boundary cell compares
-// both coefficients of each face with a water neighbour and flags the member
-// (bit 1 unsymmetric; bit 2 as well when the cross coefficients are not
-// scaled, which the host reports as an error).
+// both coefficients of each face with a water neighbour and flags the member:
+// bit 1 (the CG kernels use the four-array form) when the batch's cross
+// coefficients are formed, else bit 2, which the host reports as an error.
 __global__ void k_obc_asym(DevStatic S, DevState X, DevObc B, Ctl *ctl, const int *act,
                            int write_cross) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B.n; k += gridDim.x * blockDim.x) {
@@ -297,7 +297,7 @@ __global__ void k_obc_asym(DevStatic S, DevState X, DevObc B, Ctl *ctl, const in
     if (S.kind[q.w] != LAND) a |= X.cw[d] != X.ce[q.w];
     if (S.kind[q.n] != LAND) a |= X.cn[d] != X.cs[q.n];
     if (S.kind[q.s] != LAND) a |= X.cs[d] != X.cn[q.s];
-    if (a) atomicOr(&ctl[m].asym, write_cross ? 1 : 3);
+    if (a) atomicOr(&ctl[m].asym, write_cross ? 1 : 2);
   }
 }
 
@@ -335,13 +335,14 @@ __global__ void k_outer_reset(Glob *glob) { glob->nidone = 0; }
 // CCCI = 1./CCC is recomputed where needed instead of stored.
 
 // :54-88 initial residual, z0 = CCCI*r, RPCG.
+template <bool MA>
 __global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double *P, Ctl *ctl,
                                                double *part) {
   struct A {
     bool skip, asym;
   };
   quad_sweep<1>(
-      S, part, [&](int m) { return A{ctl[m].done != 0, ctl[m].asym != 0}; },
+      S, part, [&](int m) { return A{ctl[m].done != 0, unsym<MA>(ctl[m])}; },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         const V4<double> r = residual_row(g, S.kind, P, Y, a.asym);
         const V4<double> c = ld4(Y.ccc + g.d0);
@@ -377,6 +378,7 @@ __global__ void __launch_bounds__(NT) k_red_cg_init(DevStatic S, Ctl *ctl, Glob 
 }
 
 // :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA).
+template <bool MA>
 __global__ void __launch_bounds__(NT, 3) k_cg_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
                                                  double *part) {
   struct A {
@@ -390,7 +392,7 @@ __global__ void __launch_bounds__(NT, 3) k_cg_matvec(DevStatic S, DevSystem Y, c
       [&](int m) {
         const Ctl &k = ctl[m];
         const bool par = k.parity;
-        return A{k.done != 0, k.asym != 0, k.beta, par ? Y.pb : Y.pa, par ? Y.pa : Y.pb};
+        return A{k.done != 0, unsym<MA>(k), k.beta, par ? Y.pb : Y.pa, par ? Y.pa : Y.pb};
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         v[0] = matvec_row<double>(g, valid, Y.r, Y.ccc, a.pold, a.pnew, Y.ccs, Y.ccw, Y.cce, Y.ccn,
@@ -465,13 +467,14 @@ __global__ void __launch_bounds__(NT) k_red_cg_update(DevStatic S, Ctl *ctl, Glo
 // x = 0 and p0 = rhat (k_mx_zinit then forms z0 = M^-1 rhat and p_old = 0 for
 // the polynomial members).  rsqm_fac scales the member's RSQM (the MIXED stop,
 // below RSQM).
+template <bool MA>
 __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, SysView V, DevSystem Y,
                                                 const double *P, const Ctl *ctl, double *part) {
   struct A {
     bool skip, asym;
   };
   quad_sweep<2>(
-      S, part, [&](int m) { return A{ctl[m].done != 0, ctl[m].asym != 0}; },
+      S, part, [&](int m) { return A{ctl[m].done != 0, unsym<MA>(ctl[m])}; },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         const V4<double> r = residual_row(g, S.kind, P, V, a.asym);
         const V4<double> c = ld4(V.cc + g.d0);
@@ -999,13 +1002,19 @@ static int reduce_grid(const DevStatic &S) { return std::min(S.nmember, 1024); }
 
 void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                     Glob *glob, double *part) {
-  k_cg_init<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, part);
+  if (l.may_asym)
+    k_cg_init<true><<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, part);
+  else
+    k_cg_init<false><<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, part);
   k_red_cg_init<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part);
   count_launches(2);
 }
 void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {
-  k_cg_matvec<<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, ctl, part);
+  if (l.may_asym)
+    k_cg_matvec<true><<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, ctl, part);
+  else
+    k_cg_matvec<false><<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, ctl, part);
   k_red_cg_matvec<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part);
   count_launches(2);
 }
@@ -1023,7 +1032,10 @@ void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, dou
 void launch_mx_resid(const Launch &l, const DevStatic &S, const SysView &V, const DevSystem &Y,
                      const double *P, Ctl *ctl, Glob *glob, double *part, double rsqm_fac,
                      double rel_tol, int no_stop) {
-  k_mx_resid<<<l.grid_cg, NT, 0, l.stream>>>(S, V, Y, P, ctl, part);
+  if (l.may_asym)
+    k_mx_resid<true><<<l.grid_cg, NT, 0, l.stream>>>(S, V, Y, P, ctl, part);
+  else
+    k_mx_resid<false><<<l.grid_cg, NT, 0, l.stream>>>(S, V, Y, P, ctl, part);
   k_red_mx_resid<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, rsqm_fac, rel_tol,
                                                       no_stop, V.unscaled);
   count_launches(2);
@@ -1122,7 +1134,7 @@ int occupancy_blocks_per_sm() {
 
 int occupancy_blocks_per_sm_mv64() {
   int a = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_matvec, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_matvec<true>, NT, 0);
   return a > 0 ? a : 1;
 }
 
@@ -1130,8 +1142,8 @@ int occupancy_blocks_per_sm_cg() {
   int a = 0, b = 0, c = 0, d = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_mx_apply, NT, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cg_update, NT, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_cg_init, NT, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_mx_resid, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_cg_init<true>, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_mx_resid<true>, NT, 0);
   const int m = std::min(std::min(a, b), std::min(c, d));
   return m > 0 ? m : 1;
 }
