@@ -162,9 +162,9 @@ struct efdc_xm_ctx {
     return static_cast<T *>(b.p);
   }
   xm::Launch L() const {
-    return xm::Launch{grid,   grid_cg, grid_mv64, grid_cg32,
-                      grid_up32, ntile,  stream,    mx_jac,
-                      mx_poly, any_may_asym || sys_external};
+    return xm::Launch{grid,   grid_cg, grid_mv64, grid_cg32, grid_up32,
+                      ntile,  nsm,     stream,    mx_jac,    mx_poly,
+                      any_may_asym || sys_external};
   }
 };
 

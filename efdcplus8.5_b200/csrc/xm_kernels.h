@@ -16,6 +16,7 @@ struct Launch {
   int grid_cg32;     // CTAs of the FP32 matrix-vector kernel
   int grid_up32;     // CTAs of the FP32 update kernel
   int ntile;         // tiles including the ghost tile 0
+  int nsm;           // SMs of the device
   cudaStream_t stream;
   bool mx_jac = true;    // MIXED: some member runs the Jacobi inner solve
   bool mx_poly = false;  // MIXED: some member runs the polynomial-preconditioned one

@@ -11,6 +11,9 @@
 // whether member m takes part in the current wet/dry sweep (or, for the
 // finalisation kernels, whether its step is to be finalised).
 
+#include <map>
+#include <mutex>
+
 #include "xm_cg.cuh"
 #include "xm_kernels.h"
 
@@ -21,6 +24,56 @@ namespace xm {
 #define TILE_MEMBER(S)                  \
   const int m = (S).tile_member[tile]; \
   const StepScalars &c = (S).sc[m]
+
+// ---------------------------------------------------------------------------
+// calpuv2c.f90:214-220: the explicit transports FUHDYE (face between cell d
+// and its west neighbour, elevations P and PW) and FVHDXE (south face).
+__device__ __forceinline__ double fuh_face(const DevStatic &S, const DevState &X,
+                                           const StepScalars &c, int d, double P, double PW,
+                                           double sub) {
+  return X.uhdy1e[d] - c.deltd2 * sub * S.hruo[d] * X.hu[d] * (P - PW) +
+         sub * c.delt * S.dxiu[d] *
+             (S.dxyu[d] * (X.tsx[d] - c.ritb1 * X.tbx[d]) + X.fcaxe[d] + 0.0 - c.snlt * X.fxe[d]);
+}
+__device__ __forceinline__ double fvh_face(const DevStatic &S, const DevState &X,
+                                           const StepScalars &c, int d, double P, double PS,
+                                           double svb) {
+  return X.vhdx1e[d] - c.deltd2 * svb * S.hrvo[d] * X.hv[d] * (P - PS) +
+         svb * c.delt * S.dyiv[d] *
+             (S.dxyv[d] * (X.tsy[d] - c.ritb1 * X.tby[d]) - X.fcaye[d] + 0.0 - c.snlt * X.fye[d]);
+}
+
+// calpuv2c.f90:282-290
+__device__ __forceinline__ double fp1_cell(const DevStatic &S, const DevState &X,
+                                           const StepScalars &c, const Nb &q, double P) {
+  const double C1 = 0.5 * c.g;
+  return c.delti * S.dxyp[q.d] * P -
+         C1 * (X.uhdy1e[q.e] - X.uhdy1e[q.d] + X.vhdx1e[q.n] - X.vhdx1e[q.d]);
+}
+
+// calpuv2c.f90:306-344 for cell q.d from its faces' transports: FP, CS, CW,
+// CE, CN, CC.  Returns CC.
+__device__ __forceinline__ double assemble_cell(const DevStatic &S, const DevState &X,
+                                                const StepScalars &c, const Nb &q, double fp1,
+                                                double fuh, double fuhe, double fvh,
+                                                double fvhn) {
+  const int d = q.d;
+  double C1 = 0.5 * c.g;
+  const double sub = X.sub[d], svb = X.svb[d], sube = X.sub[q.e], svbn = X.svb[q.n];
+  X.fp[d] = fp1 - C1 * (sube * fuhe - sub * fuh + svbn * fvhn - svb * fvh - 2.0 * X.qsume[d]);
+  C1 = -0.5 * c.deltd2 * c.g;
+  const double cs = C1 * svb * S.hrvo[d] * S.rcx[d] * X.hv[d];
+  const double cw = C1 * sub * S.hruo[d] * S.rcx[d] * X.hu[d];
+  const double ce = C1 * sube * S.hruo[q.e] * S.rcx[q.e] * X.hu[q.e];
+  const double cn = C1 * svbn * S.hrvo[q.n] * S.rcx[q.n] * X.hv[q.n];
+  const double cc = c.delti * S.dxyp[d] - cs - cw - ce - cn;
+  X.cs[d] = cs;
+  X.cw[d] = cw;
+  X.ce[d] = ce;
+  X.cn[d] = cn;
+  X.cc[d] = cc;
+  return cc;
+}
 
 // ---------------------------------------------------------------------------
 // calpuv2c.f90:164-293: switches, explicit transports, FP1.  The host swapped
@@ -42,26 +95,15 @@ __global__ void __launch_bounds__(NT) k_begin(DevStatic S, DevState X, int ntile
       X.wasted[d] = 0;
     }
     const double P = X.p[d];
-    const double uhdye = X.uhdy1e[d], vhdxe = X.vhdx1e[d];
-    // :214-220
-    X.fuhdye[d] = uhdye - c.deltd2 * sub * S.hruo[d] * X.hu[d] * (P - X.p[q.w]) +
-                  sub * c.delt * S.dxiu[d] *
-                      (S.dxyu[d] * (X.tsx[d] - c.ritb1 * X.tbx[d]) + X.fcaxe[d] + 0.0 -
-                       c.snlt * X.fxe[d]);
-    X.fvhdxe[d] = vhdxe - c.deltd2 * svb * S.hrvo[d] * X.hv[d] * (P - X.p[q.s]) +
-                  svb * c.delt * S.dyiv[d] *
-                      (S.dxyv[d] * (X.tsy[d] - c.ritb1 * X.tby[d]) - X.fcaye[d] + 0.0 -
-                       c.snlt * X.fye[d]);
+    X.fuhdye[d] = fuh_face(S, X, c, d, P, X.p[q.w], sub);
+    X.fvhdxe[d] = fvh_face(S, X, c, d, P, X.p[q.s], svb);
     if (c.isdry > 0) {  // :246-253
       X.sub[d] = S.subo[d];
       X.svb[d] = S.svbo[d];
       X.sbx[d] = S.sbxo[d];
       X.sby[d] = S.sbyo[d];
     }
-    // :282-290
-    const double C1 = 0.5 * c.g;
-    X.fp1[d] = c.delti * S.dxyp[d] * P -
-               C1 * (X.uhdy1e[q.e] - uhdye + X.vhdx1e[q.n] - vhdxe);
+    X.fp1[d] = fp1_cell(S, X, c, q, P);
   }
 }
 
@@ -92,21 +134,8 @@ __global__ void __launch_bounds__(NT) k_assemble(DevStatic S, DevState X, int nt
     const uint8_t kd = S.kind[d];
     double mn = 1.e+18;
     if (kd != LAND) {
-      double C1 = 0.5 * c.g;
-      const double sub = X.sub[d], svb = X.svb[d], sube = X.sub[q.e], svbn = X.svb[q.n];
-      X.fp[d] = X.fp1[d] - C1 * (sube * X.fuhdye[q.e] - sub * X.fuhdye[d] +
-                                 svbn * X.fvhdxe[q.n] - svb * X.fvhdxe[d] - 2.0 * X.qsume[d]);
-      C1 = -0.5 * c.deltd2 * c.g;
-      const double cs = C1 * svb * S.hrvo[d] * S.rcx[d] * X.hv[d];
-      const double cw = C1 * sub * S.hruo[d] * S.rcx[d] * X.hu[d];
-      const double ce = C1 * sube * S.hruo[q.e] * S.rcx[q.e] * X.hu[q.e];
-      const double cn = C1 * svbn * S.hrvo[q.n] * S.rcx[q.n] * X.hv[q.n];
-      const double cc = c.delti * S.dxyp[d] - cs - cw - ce - cn;
-      X.cs[d] = cs;
-      X.cw[d] = cw;
-      X.ce[d] = ce;
-      X.cn[d] = cn;
-      X.cc[d] = cc;
+      const double cc = assemble_cell(S, X, c, q, X.fp1[d], X.fuhdye[d], X.fuhdye[q.e],
+                                      X.fvhdxe[d], X.fvhdxe[q.n]);
       if (kd == WATER) mn = cc;
     }
     mn = block_min(mn, sh);
@@ -379,7 +408,7 @@ __global__ void __launch_bounds__(NT) k_red_cg_init(DevStatic S, Ctl *ctl, Glob 
 
 // :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA).
 template <bool MA>
-__global__ void __launch_bounds__(NT, 3) k_cg_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
+__global__ void __launch_bounds__(NT, 2) k_cg_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
                                                  double *part) {
   struct A {
     bool skip, asym;
@@ -1000,12 +1029,34 @@ void launch_outer_reset(const Launch &l, Glob *glob) {
 // one CTA per member (grid-stride past 1024 members)
 static int reduce_grid(const DevStatic &S) { return std::min(S.nmember, 1024); }
 
+// Resident CTAs per SM of a kernel, looked up once per process and kernel.
+static int blocks_per_sm(const void *kernel) {
+  static std::mutex mu;
+  static std::map<const void *, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto it = cache.find(kernel);
+  if (it != cache.end()) return it->second;
+  int a = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, kernel, NT, 0);
+  a = a > 0 ? a : 1;
+  cache[kernel] = a;
+  return a;
+}
+
+// One wave of a quad kernel: its own resident CTAs per SM times the SMs, at
+// most one CTA per quad.
+template <class K>
+static int quad_grid(const Launch &l, const DevStatic &S, K kernel) {
+  const int per_sm = blocks_per_sm(reinterpret_cast<const void *>(kernel));
+  return std::max(1, std::min(S.nquad, l.nsm * per_sm));
+}
+
 void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                     Glob *glob, double *part) {
   if (l.may_asym)
-    k_cg_init<true><<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, part);
+    k_cg_init<true><<<quad_grid(l, S, k_cg_init<true>), NT, 0, l.stream>>>(S, Y, P, ctl, part);
   else
-    k_cg_init<false><<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, part);
+    k_cg_init<false><<<quad_grid(l, S, k_cg_init<false>), NT, 0, l.stream>>>(S, Y, P, ctl, part);
   k_red_cg_init<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part);
   count_launches(2);
 }
@@ -1020,7 +1071,7 @@ void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, C
 }
 void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                       Glob *glob, double *part, int no_stop) {
-  k_cg_update<<<l.grid_cg, NT, 0, l.stream>>>(S, Y, P, ctl, part);
+  k_cg_update<<<quad_grid(l, S, k_cg_update), NT, 0, l.stream>>>(S, Y, P, ctl, part);
   k_red_cg_update<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, no_stop);
   count_launches(2);
 }
@@ -1033,9 +1084,10 @@ void launch_mx_resid(const Launch &l, const DevStatic &S, const SysView &V, cons
                      const double *P, Ctl *ctl, Glob *glob, double *part, double rsqm_fac,
                      double rel_tol, int no_stop) {
   if (l.may_asym)
-    k_mx_resid<true><<<l.grid_cg, NT, 0, l.stream>>>(S, V, Y, P, ctl, part);
+    k_mx_resid<true><<<quad_grid(l, S, k_mx_resid<true>), NT, 0, l.stream>>>(S, V, Y, P, ctl, part);
   else
-    k_mx_resid<false><<<l.grid_cg, NT, 0, l.stream>>>(S, V, Y, P, ctl, part);
+    k_mx_resid<false><<<quad_grid(l, S, k_mx_resid<false>), NT, 0, l.stream>>>(S, V, Y, P, ctl,
+                                                                             part);
   k_red_mx_resid<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, rsqm_fac, rel_tol,
                                                       no_stop, V.unscaled);
   count_launches(2);
@@ -1043,7 +1095,7 @@ void launch_mx_resid(const Launch &l, const DevStatic &S, const SysView &V, cons
 }
 void launch_mx_apply(const Launch &l, const DevStatic &S, const SysView &V, const DevSystem &Y,
                      double *P, const Ctl *ctl) {
-  k_mx_apply<<<l.grid_cg, NT, 0, l.stream>>>(S, V, Y, P, ctl);
+  k_mx_apply<<<quad_grid(l, S, k_mx_apply), NT, 0, l.stream>>>(S, V, Y, P, ctl);
   count_launches(1);
 }
 void launch_backsub(const Launch &l, const DevStatic &S, const DevState &X, const int *act) {
