@@ -384,44 +384,24 @@ def reference_arm(args):
 
 
 # --------------------------------------------------------------- GPU runs
-DBL_IN = ("p", "hp", "hu", "hv", "uhdye", "vhdxe", "sub", "svb", "sbx", "sby", "fcaxe", "fcaye",
-          "fxe", "fye", "tsx", "tsy", "tbx", "tby", "qsume", "qdwaste", "vdwaste")
-INT_IO = ("lmaskdry", "iscdry", "lopenbcdry", "natdry")
-DBL_OUT = ("p", "hp", "h1p", "hu", "hv", "uhdye", "vhdxe", "sub", "svb", "sbx", "sby", "uhe",
-           "vhe", "hpi", "hui", "hvi", "qdwaste", "vdwaste")
-
-
-def transfer_bytes(state, lc, la):
-    """Bytes efdc_xm_step moves per call for a Fortran-shim-like field set:
-    uploads LC elements of every input/in-out array, downloads LA-1 elements of
-    every output/in-out array (mirrors efdc_xm_upload/efdc_xm_download)."""
-    nb = sum(len(v) for v in state["pser"].values())
-    h2d = lc * (8 * len(DBL_IN) + 4 * len(INT_IO)) + 8 * nb
-    d2h = (la - 1) * (8 * len(DBL_OUT) + 4 * len(INT_IO))
-    return h2d, d2h
-
-
 def pinned_states(torch, scns):
-    """Copies of the members' states in one pinned host allocation."""
-    items = []
-    for s in scns:
-        for k, v in s.state.items():
-            if isinstance(v, np.ndarray):
-                items.append(v)
-    total = sum((v.nbytes + 63) // 64 * 64 for v in items)
+    """Copies of the members' states in one pinned host allocation, field by
+    field: each field's member arrays back to back, as an ensemble driver
+    holds one (LCM, members) array per field."""
+    keys = [k for k, v in scns[0].state.items() if isinstance(v, np.ndarray)]
+    total = sum(s.state[k].nbytes for s in scns for k in keys)
     buf = torch.empty(total, dtype=torch.uint8, pin_memory=True).numpy()
+    out = [dict() for _ in scns]
     off = 0
-    out = []
-    for s in scns:
-        st = {}
-        for k, v in s.state.items():
-            if isinstance(v, np.ndarray):
-                a = buf[off:off + v.nbytes].view(v.dtype).reshape(v.shape)
-                a[...] = v
-                st[k] = a
-                off += (v.nbytes + 63) // 64 * 64
+    for k in keys:
+        for st, s in zip(out, scns):
+            v = s.state[k]
+            a = buf[off:off + v.nbytes].view(v.dtype).reshape(v.shape)
+            a[...] = v
+            st[k] = a
+            off += v.nbytes
+    for st, s in zip(out, scns):
         st["pser"] = {q: a.copy() for q, a in s.state["pser"].items()}
-        out.append(st)
     return out, buf
 
 
@@ -618,11 +598,6 @@ def ours(args):
     e2e = None
     if args.e2e_steps > 0:
         pst, _buf = pinned_states(torch, scns)
-        h2d = d2h = 0
-        for st, s in zip(pst, scns):
-            a, b = transfer_bytes(st, s.lc, s.la)
-            h2d += a
-            d2h += b
         # the same warm-up as the device-resident runs, so that timed e2e step
         # k is timed FP64 step k (whose iteration counts are the credit)
         n = 0
@@ -632,17 +607,21 @@ def ours(args):
         torch.cuda.synchronize()
         barrier()
         tms, cred = [], 0.0
+        b0 = X.transfer_bytes()  # the library's count of the arrays it copies
         for k in range(args.e2e_steps):
             n += 1
             with Timer(torch, stream) as tm:
                 bs.step(params(n, X.PREC_MIXED), pst)
             tms.append(tm.ms)
             cred += float((cells * r64["per_step"][min(k, len(r64["per_step"]) - 1)]).sum())
+        b1 = X.transfer_bytes()
+        h2d = (b1[0] - b0[0]) // len(tms)
+        d2h = (b1[1] - b0[1]) // len(tms)
         t_e, = max_over_ranks(sum(tms) / 1e3)
         cred_all, = sum_over_ranks(cred)
         e2e = {"value": cred_all / t_e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": 1000 * t_e / len(tms),
-               "steps": len(tms), "host_buffers": "pinned (one torch pin_memory block)",
+               "steps": len(tms), "host_buffers": "pinned, one (LCM, members) block per field",
                "api": "efdc_xm_step_batch"}
         del pst, _buf
 

@@ -40,6 +40,7 @@ void set_error(const char *fmt, ...) {
   } while (0)
 
 std::atomic<long long> g_launches{0};
+std::atomic<long long> g_h2d{0}, g_d2h{0};  // bytes of the callers' arrays copied
 
 using xm::CopyJob;
 using xm::Ctl;
@@ -60,6 +61,7 @@ uint64_t morton2(uint32_t x, uint32_t y) {
 }
 
 constexpr int NSTAGE = 8;     // staging buffers (each holds one array of every member)
+constexpr int NCOPY = 4;      // streams for host<->device copies
 constexpr int MAX_JOBS = 64;  // arrays moved by one upload/download call
 constexpr int GRAPH_ITERS = 4;  // CG iterations per graph launch
 constexpr int KERNELS_PER_ITER = 4;  // matvec, its reduce, update, its reduce
@@ -102,6 +104,11 @@ struct efdc_xm_ctx {
   int grid = 1, grid_cg = 1, grid_mv64 = 1, grid_cg32 = 1, grid_up32 = 1, nsm = 0;
   long long stage_len = 0;  // elements of one staging buffer
   cudaStream_t stream = nullptr;
+  // host<->device copies: many per-member copies of small arrays run
+  // concurrently on NCOPY streams (each ordered after the kernels that
+  // filled or before the kernels that read the staging buffers, by events)
+  cudaStream_t copy_stream[NCOPY] = {};
+  cudaEvent_t copy_event[NCOPY + 1] = {};
   std::vector<DevBuf> bufs;
   // device views
   xm::DevStatic S{};
@@ -194,6 +201,21 @@ int collect(efdc_xm_ctx *c, std::vector<Xfer> &out, const std::vector<const void
   return EFDC_XM_OK;
 }
 
+// The copy streams wait for the compute stream's work so far, and the compute
+// stream then waits for the copies issued on them.
+int copies_after_compute(efdc_xm_ctx *c) {
+  CK(cudaEventRecord(c->copy_event[NCOPY], c->stream));
+  for (cudaStream_t s : c->copy_stream) CK(cudaStreamWaitEvent(s, c->copy_event[NCOPY], 0));
+  return EFDC_XM_OK;
+}
+int compute_after_copies(efdc_xm_ctx *c) {
+  for (int k = 0; k < NCOPY; ++k) {
+    CK(cudaEventRecord(c->copy_event[k], c->copy_stream[k]));
+    CK(cudaStreamWaitEvent(c->stream, c->copy_event[k], 0));
+  }
+  return EFDC_XM_OK;
+}
+
 int upload_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
   if (xs.empty()) return EFDC_XM_OK;
   if (xs.size() > size_t(MAX_JOBS)) {
@@ -204,17 +226,32 @@ int upload_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
     c->jobs_h[j] = CopyJob{c->stage[j % NSTAGE], xs[j].dev, xs[j].kind};
   CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, xs.size() * sizeof(CopyJob), cudaMemcpyHostToDevice,
                      c->stream));
+  int rc = 0, k = 0;
   for (size_t g0 = 0; g0 < xs.size(); g0 += NSTAGE) {
     const size_t g1 = std::min(xs.size(), g0 + NSTAGE);
+    // the previous group's scatter has read the staging buffers
+    if ((rc = copies_after_compute(c))) return rc;
     for (size_t j = g0; j < g1; ++j) {
       const size_t es = esize(xs[j].kind);
       char *dst = reinterpret_cast<char *>(c->stage[j % NSTAGE]);
-      for (int m = 0; m < c->M; ++m)
-        CK(cudaMemcpyAsync(dst + c->mem[m].off * es, xs[j].host[m], size_t(c->mem[m].lc) * es,
-                           cudaMemcpyHostToDevice, c->stream));
+      // members whose host arrays lie back to back at the staging stride (LC+1
+      // elements: an ensemble held as one (LCM, members) array per field) go
+      // in one copy
+      for (int m = 0; m < c->M;) {
+        const char *h0 = static_cast<const char *>(xs[j].host[m]);
+        int e = m + 1;
+        while (e < c->M && static_cast<const char *>(xs[j].host[e]) ==
+                               static_cast<const char *>(xs[j].host[e - 1]) +
+                                   size_t(c->mem[e - 1].lc + 1) * es)
+          ++e;
+        const size_t n = size_t(c->mem[e - 1].off - c->mem[m].off + c->mem[e - 1].lc);
+        CK(cudaMemcpyAsync(dst + c->mem[m].off * es, h0, n * es, cudaMemcpyHostToDevice,
+                           c->copy_stream[k++ % NCOPY]));
+        g_h2d.fetch_add(static_cast<long long>(n * es), std::memory_order_relaxed);
+        m = e;
+      }
     }
-    // stream order: the next group's copies into the same staging buffers
-    // start after this scatter has read them
+    if ((rc = compute_after_copies(c))) return rc;
     xm::launch_scatter(c->stream, c->jobs_d + g0, int(g1 - g0), c->lidx, c->tile_member, c->moff,
                        c->mlc, c->nslot);
     CK(cudaGetLastError());
@@ -233,22 +270,29 @@ int download_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
     c->jobs_h[j] = CopyJob{c->stage[j % NSTAGE], xs[j].dev, xs[j].kind};
   CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, xs.size() * sizeof(CopyJob), cudaMemcpyHostToDevice,
                      c->stream));
+  int rc = 0, k = 0;
   for (size_t g0 = 0; g0 < xs.size(); g0 += NSTAGE) {
     const size_t g1 = std::min(xs.size(), g0 + NSTAGE);
+    if (g0 > 0 && (rc = compute_after_copies(c))) return rc;  // the buffers were copied out
     xm::launch_gather(c->stream, c->jobs_d + g0, int(g1 - g0), c->lidx, c->tile_member, c->moff,
                       c->nslot);
     CK(cudaGetLastError());
+    if ((rc = copies_after_compute(c))) return rc;
     // the gather fills elements L=2..LA (indices 1..LA-1) of each member; only
     // that range goes back, so the caller's ghost elements 1 and LC stay as they are
     for (size_t j = g0; j < g1; ++j) {
       const size_t es = esize(xs[j].kind);
       const char *src = reinterpret_cast<const char *>(c->stage[j % NSTAGE]);
-      for (int m = 0; m < c->M; ++m)
+      for (int m = 0; m < c->M; ++m) {
+        const size_t n = es * size_t(c->mem[m].la - 1);
         CK(cudaMemcpyAsync(static_cast<char *>(const_cast<void *>(xs[j].host[m])) + es,
-                           src + (c->mem[m].off + 1) * es, es * size_t(c->mem[m].la - 1),
-                           cudaMemcpyDeviceToHost, c->stream));
+                           src + (c->mem[m].off + 1) * es, n, cudaMemcpyDeviceToHost,
+                           c->copy_stream[k++ % NCOPY]));
+        g_d2h.fetch_add(static_cast<long long>(n), std::memory_order_relaxed);
+      }
     }
   }
+  for (cudaStream_t s : c->copy_stream) CK(cudaStreamSynchronize(s));
   CK(cudaStreamSynchronize(c->stream));
   return EFDC_XM_OK;
 }
@@ -595,6 +639,10 @@ void efdc_xm_destroy(efdc_xm_ctx *c) {
     if (g) cudaGraphExecDestroy(g);
   for (cudaGraphExec_t g : c->graph_mx)
     if (g) cudaGraphExecDestroy(g);
+  for (cudaStream_t s : c->copy_stream)
+    if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t e : c->copy_event)
+    if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -652,6 +700,12 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   }
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail("stream creation failed");
+  for (cudaStream_t &s : c->copy_stream)
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+      return bail("stream creation failed");
+  for (cudaEvent_t &e : c->copy_event)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+      return bail("event creation failed");
   cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
 
   // ---- host layout: tiles, quads (4-tile CG units, never across members), slots ----
@@ -979,7 +1033,20 @@ int32_t efdc_xm_upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f) {
   return EFDC_XM_OK;
 }
 
+namespace {
+int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged);
+}
+
 int32_t efdc_xm_download_batch(efdc_xm_ctx *c, efdc_xm_fields *f) {
+  return download_batch(c, f, false);
+}
+
+namespace {
+// skip_unchanged: leave out the fields that a step with ISDRY = 0 in every
+// member does not write (the face switches SUB, SVB, SBX, SBY, LMASKDRY,
+// ISCDRY, NATDRY, QDWASTE, VDWASTE): within efdc_xm_step_batch their device
+// values are the host values uploaded by the same call.
+int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged) {
   if (!c || !f) {
     set_error("efdc_xm_download: NULL argument");
     return EFDC_XM_BAD_ARGUMENT;
@@ -997,11 +1064,14 @@ int32_t efdc_xm_download_batch(efdc_xm_ctx *c, efdc_xm_fields *f) {
     if ((rc = collect(c, xs, v, dev, kind, #name))) return rc;   \
   }
   XM_DN(p, X.p, 0) XM_DN(hp, X.hp, 0) XM_DN(h1p, X.h1p, 0) XM_DN(hu, X.hu, 0) XM_DN(hv, X.hv, 0)
-  XM_DN(uhdye, X.uhdye, 0) XM_DN(vhdxe, X.vhdxe, 0) XM_DN(sub, X.sub, 0) XM_DN(svb, X.svb, 0)
-  XM_DN(sbx, X.sbx, 0) XM_DN(sby, X.sby, 0) XM_DN(lmaskdry, X.lmaskdry, 1)
-  XM_DN(iscdry, X.iscdry, 2) XM_DN(lopenbcdry, X.lopenbcdry, 1) XM_DN(natdry, X.natdry, 2)
+  XM_DN(uhdye, X.uhdye, 0) XM_DN(vhdxe, X.vhdxe, 0) XM_DN(lopenbcdry, X.lopenbcdry, 1)
   XM_DN(uhe, X.uhe, 0) XM_DN(vhe, X.vhe, 0) XM_DN(hpi, X.hpi, 0) XM_DN(hui, X.hui, 0)
-  XM_DN(hvi, X.hvi, 0) XM_DN(qdwaste, X.qdwaste, 0) XM_DN(vdwaste, X.vdwaste, 0)
+  XM_DN(hvi, X.hvi, 0)
+  if (!skip_unchanged) {
+    XM_DN(sub, X.sub, 0) XM_DN(svb, X.svb, 0) XM_DN(sbx, X.sbx, 0) XM_DN(sby, X.sby, 0)
+    XM_DN(lmaskdry, X.lmaskdry, 1) XM_DN(iscdry, X.iscdry, 2) XM_DN(natdry, X.natdry, 2)
+    XM_DN(qdwaste, X.qdwaste, 0) XM_DN(vdwaste, X.vdwaste, 0)
+  }
   XM_DN(ccc, Y.ccc, 0) XM_DN(ccs, Y.ccs, 0) XM_DN(ccw, Y.ccw, 0) XM_DN(cce, Y.cce, 0)
   XM_DN(ccn, Y.ccn, 0) XM_DN(fptmp, Y.fptmp, 0)
 #undef XM_DN
@@ -1047,6 +1117,7 @@ int32_t efdc_xm_download_batch(efdc_xm_ctx *c, efdc_xm_fields *f) {
   }
   return EFDC_XM_OK;
 }
+}  // namespace
 
 int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
                                   efdc_xm_stats *stats) {
@@ -1233,7 +1304,9 @@ int32_t efdc_xm_step_batch(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fi
   }
   const int st = efdc_xm_step_device_batch(c, prm, stats);
   if (st == EFDC_XM_CUDA_ERROR || st == EFDC_XM_BAD_ARGUMENT) return st;
-  if ((rc = efdc_xm_download_batch(c, f))) {
+  bool no_wetdry = true;
+  for (int m = 0; m < M; ++m) no_wetdry &= prm[m].isdry == 0;
+  if ((rc = download_batch(c, f, no_wetdry))) {
     fill_status(stats, M, rc);
     return rc;
   }
@@ -1354,6 +1427,11 @@ int32_t efdc_xm_congrad(efdc_xm_ctx *c, const double *ccc, const double *ccs, co
 void *efdc_xm_stream(efdc_xm_ctx *c) { return c ? static_cast<void *>(c->stream) : nullptr; }
 
 int64_t efdc_xm_kernel_launches(void) { return g_launches.load(); }
+
+void efdc_xm_transfer_bytes(int64_t *h2d, int64_t *d2h) {
+  if (h2d) *h2d = g_h2d.load();
+  if (d2h) *d2h = g_d2h.load();
+}
 
 int32_t efdc_xm_time_kernels(efdc_xm_ctx *c, int32_t precision, int32_t reps, efdc_xm_ktime *out) {
   if (!c || !out || reps < 1 || reps > 40) {

@@ -204,6 +204,15 @@ class CudaLibraryMissing(RuntimeError):
 _lib = None
 
 
+def transfer_bytes() -> tuple[int, int]:
+    """Bytes of callers' arrays copied (host->device, device->host) by the
+    library in this process so far."""
+    lib = load()
+    h, d = C.c_int64(0), C.c_int64(0)
+    lib.efdc_xm_transfer_bytes(C.byref(h), C.byref(d))
+    return h.value, d.value
+
+
 def load(path: str | os.PathLike | None = None):
     """Load libefdc_xm.so (built in-tree by build.py).  Fails loudly when it is
     missing: there is no CPU fallback."""
@@ -234,6 +243,8 @@ def load(path: str | os.PathLike | None = None):
     lib.efdc_xm_stream.restype = C.c_void_p
     lib.efdc_xm_stream.argtypes = [C.c_void_p]
     lib.efdc_xm_kernel_launches.restype = C.c_int64
+    lib.efdc_xm_transfer_bytes.restype = None
+    lib.efdc_xm_transfer_bytes.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.efdc_xm_time_kernels.restype = C.c_int32
     lib.efdc_xm_time_kernels.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(KTime)]
     lib.efdc_xm_congrad_noalloc.restype = C.c_int32

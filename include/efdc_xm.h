@@ -267,6 +267,11 @@ void *efdc_xm_stream(efdc_xm_ctx *ctx);
 /* Number of kernels this library has launched in the process so far. */
 int64_t efdc_xm_kernel_launches(void);
 
+/* Bytes copied host->device (*h2d) and device->host (*d2h) by the upload,
+ * download and step calls of every context since the library was loaded
+ * (the caller's arrays only: no small control transfers). */
+void efdc_xm_transfer_bytes(int64_t *h2d, int64_t *d2h);
+
 /* Average device time (CUDA events on the context's stream) of the CG
  * iteration kernels on the system currently assembled in the context:
  * `reps` matrix-vector (p update + A*p + p.Ap) and update (x, r, r.z, r.r)
