@@ -79,7 +79,8 @@ def parse():
                     help="wetting/drying batch side measurement, 1024x1024 flats (0: skip)")
     ap.add_argument("--calib-steps", type=int, default=200,
                     help="adjoint calibration side measurement, 512x512 basin (0: skip)")
-    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="CPU baseline: seconds per thread setting (two settings)")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
@@ -165,13 +166,14 @@ class Clocks:
 
 
 # --------------------------------------------------------------- CPU runs
-def cpu_run(scns, seconds, max_steps, warmup=0):
-    """The oracle port (FP64, OpenMP over all host threads): steps of the
-    given basins, all basins per step, until `seconds` or `max_steps`."""
+def cpu_run(scns, seconds, max_steps, warmup=0, threads=None, cap=None):
+    """The oracle port (FP64, OpenMP): steps of the given basins, all basins
+    per step, until `seconds` or `max_steps`.  threads defaults to all host
+    threads; cap is the NOPTIMAL thread cap (the reference's is 8)."""
     sys.path.insert(0, str(REPO / "oracle"))
     import oracle as O
-    cores = os.cpu_count() or 1
-    orcs = [O.Oracle(s.grid, nthreads=cores, noptimal_cap=cores) for s in scns]
+    cores = threads or os.cpu_count() or 1
+    orcs = [O.Oracle(s.grid, nthreads=cores, noptimal_cap=cap or cores) for s in scns]
     sts = [s.copy_state() for s in scns]
     n = 0
     for _ in range(warmup):
@@ -707,6 +709,12 @@ def ours(args):
                "sample": f"{k} CALPUV2C steps of {len(samp)} basins "
                          f"({sum(s.ncell for s in samp)} cells), FP64 C++ restatement of "
                          f"CALPUV2C/CONGRAD, {nopt} OpenMP threads, {dt:.1f} s"}
+        # the reference's own thread cap, NOPTIMAL = MIN(NTHREADS, 8, LA/100)
+        t8 = min(os.cpu_count() or 1, 8)
+        v8, k8, dt8, nopt8 = cpu_run(samp, seconds=args.cpu_seconds, max_steps=50, threads=t8,
+                                     cap=8)
+        cpu["noptimal_cap_8"] = {"value": v8, "cores": nopt8, "steps": k8,
+                                 "seconds": round(dt8, 2)}
 
     if rank == 0:
         cfg["parallelism"] = (f"{world} GPUs, members partitioned by wet cells (no exchange)"
