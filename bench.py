@@ -632,6 +632,9 @@ def ours(args):
     # system reads r, p_old, AS, AW and writes p_new, Ap (6 x 4 B); the FP64
     # drop-in's reads r, CCC, p_old, CCS, CCW and writes p_new, Ap (7 x 8 B)
     bytes_mv = 24.0 * kt.ncells
+    # the update: 24 B per cell (x, p, r, Ap in; x, r out) for a Jacobi member,
+    # 36 B for a polynomial one (+ AS, AW in, z out)
+    bytes_up = 24.0 * kt.ncells + 12.0 * kt.ncells_poly
     achieved = bytes_mv / (kt.ms_matvec * 1e-3) / 1e9
     traffic = None
     tf = REPO / "profiles" / "traffic.json"
@@ -645,8 +648,9 @@ def ours(args):
             "peak_kind": peak_kind, "traffic": traffic,
             "ms_per_launch": kt.ms_matvec, "bytes_per_launch": bytes_mv,
             "cells_per_launch": kt.ncells, "slots_per_launch": kt.nslots,
-            "update_kernel": {"ms_per_launch": kt.ms_update, "bytes_per_launch": 24.0 * kt.ncells,
-                              "achieved": 24.0 * kt.ncells / (kt.ms_update * 1e-3) / 1e9},
+            "update_kernel": {"ms_per_launch": kt.ms_update, "bytes_per_launch": bytes_up,
+                              "achieved": bytes_up / (kt.ms_update * 1e-3) / 1e9,
+                              "cells_polynomial": kt.ncells_poly},
             "fp64_matvec": {"ms_per_launch": kt64.ms_matvec, "bytes_per_launch": 56.0 * kt.ncells,
                             "achieved": 56.0 * kt.ncells / (kt64.ms_matvec * 1e-3) / 1e9}}
     bs.close()

@@ -1496,6 +1496,10 @@ int32_t efdc_xm_time_kernels(efdc_xm_ctx *c, int32_t precision, int32_t reps, ef
   for (const Member &mb : c->mem) ncell += mb.la - 1;
   out->ncells = int32_t(std::min<long long>(ncell, INT32_MAX));
   out->nslots = (c->ntile - 1) * TILE;
+  long long npoly = 0;
+  for (int m = 0; m < c->M; ++m)
+    if (mixed && c->mpoly_h[m] && !(c->ctl_h[m].asym & 1)) npoly += c->mem[m].la - 1;
+  out->ncells_poly = int32_t(std::min<long long>(npoly, INT32_MAX));
   for (int m = 0; m < c->M; ++m)
     if (c->ctl_h[m].done) {
       set_error("efdc_xm_time_kernels: the iteration of member %d stopped early (status %d)", m,

@@ -80,7 +80,7 @@ class Stats(C.Structure):
 
 class KTime(C.Structure):
     _fields_ = [("ms_matvec", C.c_double), ("ms_update", C.c_double), ("reps", C.c_int32),
-                ("ncells", C.c_int32), ("nslots", C.c_int32)]
+                ("ncells", C.c_int32), ("nslots", C.c_int32), ("ncells_poly", C.c_int32)]
 
 
 FIELD_DOUBLE_INOUT = ("p", "hp", "h1p", "hu", "hv", "uhdye", "vhdxe", "sub", "svb",

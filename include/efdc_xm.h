@@ -282,6 +282,9 @@ typedef struct efdc_xm_ktime {
   int32_t reps;
   int32_t ncells;       /* water cells, LA-1 summed over members */
   int32_t nslots;       /* tile slots processed per launch (incl. land padding) */
+  int32_t ncells_poly;  /* MIXED: water cells of the members whose inner solve uses the
+                         * polynomial preconditioner (their update moves 36 B per cell,
+                         * the others' 24 B) */
 } efdc_xm_ktime;
 int32_t efdc_xm_time_kernels(efdc_xm_ctx *ctx, int32_t precision, int32_t reps,
                              efdc_xm_ktime *out);
