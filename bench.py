@@ -708,14 +708,14 @@ def ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         samp = cpu_sample(scns) if M > 1 else scns
-        v, k, dt, nopt = cpu_run(samp, seconds=args.cpu_seconds, max_steps=50)
+        v, k, dt, nopt = cpu_run(samp, seconds=args.cpu_seconds, max_steps=2000)
         cpu = {"value": v, "unit": UNIT, "cores": nopt, "kind": "port",
                "sample": f"{k} CALPUV2C steps of {len(samp)} basins "
                          f"({sum(s.ncell for s in samp)} cells), FP64 C++ restatement of "
                          f"CALPUV2C/CONGRAD, {nopt} OpenMP threads, {dt:.1f} s"}
         # the reference's own thread cap, NOPTIMAL = MIN(NTHREADS, 8, LA/100)
         t8 = min(os.cpu_count() or 1, 8)
-        v8, k8, dt8, nopt8 = cpu_run(samp, seconds=args.cpu_seconds, max_steps=50, threads=t8,
+        v8, k8, dt8, nopt8 = cpu_run(samp, seconds=args.cpu_seconds, max_steps=2000, threads=t8,
                                      cap=8)
         cpu["noptimal_cap_8"] = {"value": v8, "cores": nopt8, "steps": k8,
                                  "seconds": round(dt8, 2)}
