@@ -25,6 +25,7 @@ SOURCES = {
     "xm_capi.cu": [],
     "xm_noalloc.cu": ["-fmad=false"],
     "xm_adjoint.cu": [],
+    "xm_chan.cu": ["-fmad=false"],
 }
 
 

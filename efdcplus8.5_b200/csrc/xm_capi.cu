@@ -96,6 +96,13 @@ struct Member {
   std::vector<int> slot_of;  // slot of cell L (0 for L outside 2..LA)
 };
 
+// One sub-grid channel of a member, as efdc_xm_set_channels received it.
+struct ChanSpec {
+  int type, lh, lu, lv;  // MDCHTYP, LMDCHH, LMDCHU, LMDCHV
+  double len, fric;      // CHANLEN, CHANFRIC
+  double gw, gl;         // guest's WCHAN and cross length (DXP/DYP of LMDCHU or LMDCHV)
+};
+
 struct efdc_xm_ctx {
   int device = 0;
   int M = 0;
@@ -141,9 +148,10 @@ struct efdc_xm_ctx {
   double *ptmp = nullptr;    // scratch P for kernel timing
   // CUDA graphs of GRAPH_ITERS consecutive CG iterations on X.p (FP64) and
   // of the FP32 inner iteration, captured on first use
-  // CG iteration graphs: [may_asym] (FP64), [kinds | may_asym << 2] (MIXED)
-  cudaGraphExec_t graph_cg[2] = {}, graph_mx[8] = {};
-  bool graph_cg_failed[2] = {}, graph_mx_failed[8] = {};
+  // CG iteration graphs: [may_asym | chan << 1] (FP64),
+  // [kinds | may_asym << 2 | chan << 3] (MIXED)
+  cudaGraphExec_t graph_cg[4] = {}, graph_mx[16] = {};
+  bool graph_cg_failed[4] = {}, graph_mx_failed[16] = {};
   bool mx_jac = true, mx_poly = false;  // kinds of MIXED inner solve in use
   xm::SysView mxview{};  // the system the MIXED solve refines (the step's assembly, or CONGRAD's)
   bool last_mixed = false;  // the last step ran MIXED: the scaled FP64 system is formed on request
@@ -158,6 +166,15 @@ struct efdc_xm_ctx {
   int *gslot = nullptr;   // [gcap] gauge slots
   double *gbuf = nullptr; // [gcap] gauge values / adjoint weights
   int gcap = 0;
+  // sub-grid channels: each member's list, the slot kinds as created, and
+  // the device arrays behind S.ch (rebuilt by efdc_xm_set_channels)
+  std::vector<std::vector<ChanSpec>> chans;
+  std::vector<uint8_t> kind_h;
+  std::vector<void *> chan_bufs;
+  std::vector<double> hp1_h;  // [M] HP(1) at the last upload
+  std::vector<int> chan_start;  // [M+1] first channel of each member in S.ch
+  std::vector<int> qstart_h;    // [M+1] first quad of each member
+  double *chan_hp1 = nullptr;   // S.ch.hp1
 
   template <class T>
   T *alloc(size_t n, bool zero = true) {
@@ -169,9 +186,10 @@ struct efdc_xm_ctx {
     return static_cast<T *>(b.p);
   }
   xm::Launch L() const {
-    return xm::Launch{grid,   grid_cg, grid_mv64, grid_cg32, grid_up32,
-                      ntile,  nsm,     stream,    mx_jac,    mx_poly,
-                      any_may_asym || sys_external};
+    return xm::Launch{grid,    grid_cg, grid_mv64, grid_cg32,
+                      grid_up32, ntile, nsm,       stream,
+                      mx_jac,  mx_poly, any_may_asym || sys_external,
+                      S.ch.n > 0 && !sys_external};
   }
 };
 
@@ -344,10 +362,10 @@ cudaGraphExec_t capture_graph(efdc_xm_ctx *c, Body body) {
 int run_iters(efdc_xm_ctx *c, bool mixed, double *P, int n) {
   const xm::Launch l = c->L();
   // the kernels the graph holds
-  const int ma = l.may_asym ? 1 : 0;
-  const int kind = (c->mx_jac ? 1 : 0) | (c->mx_poly ? 2 : 0) | (ma << 2);
-  cudaGraphExec_t &gr = mixed ? c->graph_mx[kind] : c->graph_cg[ma];
-  bool &failed = mixed ? c->graph_mx_failed[kind] : c->graph_cg_failed[ma];
+  const int ma = l.may_asym ? 1 : 0, ch = l.chan ? 1 : 0;
+  const int kind = (c->mx_jac ? 1 : 0) | (c->mx_poly ? 2 : 0) | (ma << 2) | (ch << 3);
+  cudaGraphExec_t &gr = mixed ? c->graph_mx[kind] : c->graph_cg[ma | (ch << 1)];
+  bool &failed = mixed ? c->graph_mx_failed[kind] : c->graph_cg_failed[ma | (ch << 1)];
   auto one = [&]() {
     if (mixed)
       xm::launch_mx_iter(l, c->S, c->Y, c->ctl, c->glob, c->part);
@@ -435,7 +453,8 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
   // a radiation boundary, or a caller's standalone system.
   c->mx_jac = c->mx_poly = false;
   for (int m = 0; m < c->M; ++m) {
-    c->mpoly_h[m] = c->mem[m].jac_est > 10.f ? 1 : 0;
+    // a member with sub-grid channels keeps Jacobi (the couplings enter A*p only)
+    c->mpoly_h[m] = (c->mem[m].jac_est > 10.f && !(l.chan && !c->chans[m].empty())) ? 1 : 0;
     if (!c->act_h[m]) continue;
     if (!c->mpoly_h[m]) {
       c->mx_jac = true;
@@ -446,6 +465,7 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
   }
   CK(cudaMemcpyAsync(c->mpoly, c->mpoly_h, sizeof(int) * c->M, cudaMemcpyHostToDevice, c->stream));
   const xm::Launch lk = c->L();  // with the kinds in use
+  xm::launch_chan_p0(lk, c->S, c->mxview, P, c->act);
   int rc = 0;
   for (int o = 0; o < max_outer; ++o) {
     xm::launch_outer_reset(lk, c->glob);
@@ -502,6 +522,8 @@ xm::StepScalars make_scalars(const Member &mb, const efdc_xm_params *p) {
   s.ndrystp = p->ndrystp;
   s.isbal = p->isbal;
   s.iterm = p->iterm;
+  s.rlamn = p->qcherr;  // calpuv2c.f90:353 (RLAMN = QCHERR)
+  s.chan_consistent = p->chan_consistent != 0 ? 1 : 0;
   // setopenbc.f90:24-29 on the host, libm as the reference
   for (int m = 0; m < mb.mtide && m < xm::MT_MAX; ++m) {
     double TM = std::fmod(p->tn, mb.tcp[m]);
@@ -639,6 +661,7 @@ void efdc_xm_destroy(efdc_xm_ctx *c) {
     if (g) cudaGraphExecDestroy(g);
   for (cudaGraphExec_t g : c->graph_mx)
     if (g) cudaGraphExecDestroy(g);
+  for (void *b : c->chan_bufs) cudaFree(b);
   for (cudaStream_t s : c->copy_stream)
     if (s) cudaStreamDestroy(s);
   for (cudaEvent_t e : c->copy_event)
@@ -837,6 +860,11 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   cudaMemcpy(c->tile_member, tile_member.data(), ntile * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(tnbr_d, tnbr.data(), tnbr.size() * sizeof(int4), cudaMemcpyHostToDevice);
   cudaMemcpy(kind_d, kind.data(), ns, cudaMemcpyHostToDevice);
+  c->kind_h = kind;
+  c->chans.assign(M, {});
+  c->hp1_h.assign(M, 1.0);
+  c->chan_start.assign(M + 1, 0);
+  c->qstart_h = qstart;
   cudaMemcpy(quads_d, quads.data(), quads.size() * sizeof(int4), cudaMemcpyHostToDevice);
   cudaMemcpy(qstart_d, qstart.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(tend_d, tend.data(), M * sizeof(int), cudaMemcpyHostToDevice);
@@ -993,6 +1021,12 @@ int32_t efdc_xm_upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f) {
   CK(cudaSetDevice(c->device));
   xm::DevState &X = c->X;
   const int M = c->M;
+  for (int m = 0; m < M; ++m)
+    if (!c->chans[m].empty() && (!f[m].qchanu || !f[m].qchanv || !f[m].qchanun || !f[m].qchanvn)) {
+      set_error("efdc_xm_upload: member %d has sub-grid channels: QCHANU, QCHANV, QCHANUN and "
+                "QCHANVN are required", m);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
   std::vector<Xfer> xs;
   int rc = 0;
 #define XM_UP(name, dev, kind)                                   \
@@ -1026,6 +1060,21 @@ int32_t efdc_xm_upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f) {
     }
     CK(cudaMemcpyAsync(c->pser_d, c->pser_h, c->nobc * sizeof(double), cudaMemcpyHostToDevice,
                        c->stream));
+  }
+  if (c->S.ch.n > 0) {  // the channels' flows and HP(1) (subchan.f90:84)
+    const xm::DevChan &C = c->S.ch;
+    for (int m = 0; m < M; ++m) {
+      const int k0 = c->chan_start[m], n = c->chan_start[m + 1] - k0;
+      if (f[m].hp) c->hp1_h[m] = f[m].hp[0];
+      if (n == 0) continue;
+      const size_t b = sizeof(double) * size_t(n);
+      CK(cudaMemcpyAsync(C.qu + k0, f[m].qchanu, b, cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpyAsync(C.qv + k0, f[m].qchanv, b, cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpyAsync(C.qun + k0, f[m].qchanun, b, cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpyAsync(C.qvn + k0, f[m].qchanvn, b, cudaMemcpyHostToDevice, c->stream));
+    }
+    CK(cudaMemcpyAsync(c->chan_hp1, c->hp1_h.data(), sizeof(double) * M,
+                       cudaMemcpyHostToDevice, c->stream));
   }
   CK(cudaStreamSynchronize(c->stream));
   for (int m = 0; m < M; ++m)
@@ -1100,6 +1149,21 @@ int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged) {
     xs.push_back(Xfer{po, X.oldmask, 2});
   }
   if ((rc = download_arrays(c, xs))) return rc;
+  if (c->S.ch.n > 0) {  // the channels' flows
+    const xm::DevChan &C = c->S.ch;
+    for (int m = 0; m < M; ++m) {
+      const int k0 = c->chan_start[m], n = c->chan_start[m + 1] - k0;
+      if (n == 0) continue;
+      const size_t b = sizeof(double) * size_t(n);
+      if (f[m].qchanu) CK(cudaMemcpyAsync(f[m].qchanu, C.qu + k0, b, cudaMemcpyDeviceToHost, c->stream));
+      if (f[m].qchanv) CK(cudaMemcpyAsync(f[m].qchanv, C.qv + k0, b, cudaMemcpyDeviceToHost, c->stream));
+      if (f[m].qchanun)
+        CK(cudaMemcpyAsync(f[m].qchanun, C.qun + k0, b, cudaMemcpyDeviceToHost, c->stream));
+      if (f[m].qchanvn)
+        CK(cudaMemcpyAsync(f[m].qchanvn, C.qvn + k0, b, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+  }
   if (lists) {  // calpuv2c.f90:1061-1080 (L order)
     for (int m = 0; m < M; ++m) {
       const Member &mb = c->mem[m];
@@ -1142,11 +1206,11 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
     }
   }
   CK(cudaSetDevice(c->device));
-  const xm::Launch l = c->L();
   const bool mixed = prm[0].precision == EFDC_XM_PREC_MIXED;
   c->mxview = xm::SysView{c->X.fp, c->X.cc, c->X.cs, c->X.cw, c->X.ce, c->X.cn, 1};
   c->last_mixed = mixed;
   c->sys_external = false;
+  const xm::Launch l = c->L();
   bool any_isdry = false, any_legacy = false, any99 = false, any_waste = false;
   std::vector<int> ncordry(M, 0), status(M, EFDC_XM_OK), max_sweeps(M);
   for (int m = 0; m < M; ++m) {
@@ -1174,13 +1238,15 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
   std::swap(c->X.uhdye, c->X.uhdy1e);
   std::swap(c->X.vhdxe, c->X.vhdx1e);
   std::swap(c->X.hp, c->X.h1p);
+  xm::launch_chan_entry(l, c->S, c->X);
   xm::launch_begin(l, c->S, c->X);
   if (any_isdry) xm::launch_obc_reset(l, c->S, c->B, c->X);
   CK(cudaGetLastError());
-  for (;;) {  // 1000 CONTINUE, for the members still sweeping
+  for (int sweep = 0;; ++sweep) {  // 1000 CONTINUE, for the members still sweeping
     xm::launch_sweep_reset(l, c->ctl, c->act, M);
     xm::launch_assemble(l, c->S, c->X, c->ctl, c->act);
     xm::launch_obc(l, c->S, c->X, c->B, c->ctl, c->act, c->obc_serial, c->any_may_asym ? 1 : 0);
+    xm::launch_chan_sub(l, c->S, c->X, c->ctl, c->act, sweep == 0 ? 1 : 0);
     xm::launch_scale(l, c->S, c->X, c->Y, c->ctl, c->act, mixed ? 1 : 0, c->any_may_asym ? 1 : 0);
     CK(cudaGetLastError());
     rc = mixed ? solve_mixed(c, c->X.p, prm[0].mixed_rsq_factor) : solve_fp64(c, c->X.p);
@@ -1221,8 +1287,10 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
     }
     if (nact == 0) break;
     if (dropped && (rc = write_act(c))) return rc;
+    xm::launch_chan_flow(l, c->S, c->X, c->act);
     xm::launch_backsub(l, c->S, c->X, c->act);
     xm::launch_obc_hp(l, c->S, c->X, c->B, c->act);
+    xm::launch_chan_exch(l, c->S, c->X, c->act);
     bool resweep = false;
     if (any_isdry) {
       xm::launch_wetdry(l, c->S, c->X, c->ctl, c->act, any_legacy, any99);
@@ -1376,6 +1444,164 @@ int32_t efdc_xm_step(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *
   const int rc = single_only(c, "efdc_xm_step");
   if (rc) return stats->status = rc;
   return efdc_xm_step_batch(c, prm, f, stats);
+}
+
+namespace {
+// CUDA graphs hold the kernels' arguments; a change of the channel arrays
+// drops them (they are captured again on next use).
+void drop_graphs(efdc_xm_ctx *c) {
+  for (cudaGraphExec_t &g : c->graph_cg)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  for (cudaGraphExec_t &g : c->graph_mx)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  for (bool &f : c->graph_cg_failed) f = false;
+  for (bool &f : c->graph_mx_failed) f = false;
+}
+
+// S.ch from every member's channel list, and the slot kinds (channel cells
+// are CHAN).  Channels are few: plain host-side packing and small copies.
+int rebuild_channels(efdc_xm_ctx *c) {
+  CK(cudaStreamSynchronize(c->stream));
+  for (void *b : c->chan_bufs) cudaFree(b);
+  c->chan_bufs.clear();
+  xm::DevChan &C = c->S.ch;
+  C = xm::DevChan{};
+  c->chan_hp1 = nullptr;
+  const int M = c->M;
+  std::vector<uint8_t> kind = c->kind_h;
+  std::vector<int> cstart(M + 1, 0), type, host, guest, gu, qh, qg, fh, fg;
+  std::vector<double> len, fric, gw, gl;
+  for (int m = 0; m < M; ++m) {
+    cstart[m] = int(type.size());
+    const Member &mb = c->mem[m];
+    std::vector<int> seen;
+    auto first = [&](int d) {
+      if (std::find(seen.begin(), seen.end(), d) != seen.end()) return 0;
+      seen.push_back(d);
+      return 1;
+    };
+    auto quad = [&](int d) { return c->qstart_h[m] + (d / xm::TILE - mb.tile0) / 4; };
+    for (const ChanSpec &k : c->chans[m]) {
+      const int dh = mb.slot_of[k.lh], dg = mb.slot_of[k.type == 1 ? k.lu : k.lv];
+      type.push_back(k.type);
+      host.push_back(dh);
+      guest.push_back(dg);
+      gu.push_back(k.type == 2 && k.lu >= 2 ? mb.slot_of[k.lu] : -1);
+      qh.push_back(quad(dh));
+      qg.push_back(quad(dg));
+      fg.push_back(first(dg));
+      fh.push_back(first(dh));
+      len.push_back(k.len);
+      fric.push_back(k.fric);
+      gw.push_back(k.gw);
+      gl.push_back(k.gl);
+      kind[dh] = kind[dg] = xm::CHAN;
+    }
+  }
+  const int n = int(type.size());
+  cstart[M] = n;
+  c->chan_start = cstart;
+  CK(cudaMemcpy(const_cast<uint8_t *>(c->S.kind), kind.data(), kind.size(), cudaMemcpyHostToDevice));
+  drop_graphs(c);
+  if (n == 0) return EFDC_XM_OK;
+  auto dev = [&](const void *src, size_t bytes) -> void * {
+    void *p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(bytes, 1)) != cudaSuccess) return nullptr;
+    c->chan_bufs.push_back(p);
+    if (src)
+      cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
+    else
+      cudaMemset(p, 0, bytes);
+    return p;
+  };
+  const size_t ni = sizeof(int) * size_t(n), nd = sizeof(double) * size_t(n);
+  C.cstart = static_cast<const int *>(dev(cstart.data(), sizeof(int) * (M + 1)));
+  C.type = static_cast<const int *>(dev(type.data(), ni));
+  C.host = static_cast<const int *>(dev(host.data(), ni));
+  C.guest = static_cast<const int *>(dev(guest.data(), ni));
+  C.gu = static_cast<const int *>(dev(gu.data(), ni));
+  C.qhost = static_cast<const int *>(dev(qh.data(), ni));
+  C.qguest = static_cast<const int *>(dev(qg.data(), ni));
+  C.first_host = static_cast<const int *>(dev(fh.data(), ni));
+  C.first_guest = static_cast<const int *>(dev(fg.data(), ni));
+  C.len = static_cast<const double *>(dev(len.data(), nd));
+  C.fric = static_cast<const double *>(dev(fric.data(), nd));
+  C.gw = static_cast<const double *>(dev(gw.data(), nd));
+  C.gl = static_cast<const double *>(dev(gl.data(), nd));
+  c->chan_hp1 = static_cast<double *>(dev(c->hp1_h.data(), sizeof(double) * M));
+  C.hp1 = c->chan_hp1;
+  double **st[] = {&C.qu, &C.qv, &C.qun, &C.qvn, &C.qut, &C.qvt, &C.cu,
+                   &C.cv, &C.chh, &C.p1h, &C.p1g, &C.p0h, &C.p0g};
+  for (double **q : st) *q = static_cast<double *>(dev(nullptr, nd));
+  C.hh32 = static_cast<float *>(dev(nullptr, sizeof(float) * size_t(n)));
+  C.iact = static_cast<int *>(dev(nullptr, ni));
+  for (void *b : c->chan_bufs)
+    if (!b) {
+      set_error("efdc_xm_set_channels: device allocation failed");
+      return EFDC_XM_CUDA_ERROR;
+    }
+  if (c->chan_bufs.size() != 29) {
+    set_error("internal: channel arrays");
+    return EFDC_XM_CUDA_ERROR;
+  }
+  C.n = n;
+  return EFDC_XM_OK;
+}
+}  // namespace
+
+int32_t efdc_xm_set_channels(efdc_xm_ctx *c, int32_t member, const efdc_xm_channels *ch) {
+  if (!c || !ch || member < 0 || member >= (c ? c->M : 0) || ch->n < 0) {
+    set_error("efdc_xm_set_channels: need a context, a member index and a channel struct");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  if (c->calib) {
+    set_error("efdc_xm_set_channels: the adjoint does not cover sub-grid channels");
+    return EFDC_XM_UNSUPPORTED;
+  }
+  const Member &mb = c->mem[member];
+  std::vector<ChanSpec> list;
+  if (ch->n > 0) {
+    if (!ch->type || !ch->lhost || !ch->lu || !ch->lv || !ch->chanlen || !ch->chanfric ||
+        !ch->dxp || !ch->dyp) {
+      set_error("efdc_xm_set_channels: NULL channel array");
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+    auto water = [&](int L) {
+      return L >= 2 && L <= mb.la && c->kind_h[mb.slot_of[L]] == xm::WATER;
+    };
+    for (int k = 0; k < ch->n; ++k) {
+      ChanSpec s{ch->type[k], ch->lhost[k], ch->lu[k], ch->lv[k], ch->chanlen[k], ch->chanfric[k],
+                 0.0, 0.0};
+      const int lg = s.type == 1 ? s.lu : s.lv;
+      if (s.type != 1 && s.type != 2) {
+        set_error("efdc_xm_set_channels: channel %d: MDCHTYP %d (only 1 and 2 enter CALPUV2C)",
+                  k + 1, s.type);
+        return EFDC_XM_UNSUPPORTED;
+      }
+      if (!water(s.lh) || !water(lg) || s.lh == lg) {
+        set_error("efdc_xm_set_channels: channel %d: host %d and guest %d must be distinct "
+                  "water cells (2..LA) that are not open-boundary cells", k + 1, s.lh, lg);
+        return EFDC_XM_BAD_ARGUMENT;
+      }
+      if (s.type == 2 && s.lu != 1 && !(s.lu >= 2 && s.lu <= mb.la)) {
+        set_error("efdc_xm_set_channels: channel %d: LMDCHU %d (1 or a cell 2..LA)", k + 1, s.lu);
+        return EFDC_XM_BAD_ARGUMENT;
+      }
+      // subchan.f90:51-52 (x) and :90-91 (y)
+      s.gw = s.type == 1 ? ch->dxp[lg - 1] : ch->dyp[lg - 1];
+      s.gl = s.type == 1 ? ch->dyp[lg - 1] : ch->dxp[lg - 1];
+      list.push_back(s);
+    }
+  }
+  CK(cudaSetDevice(c->device));
+  c->chans[member] = std::move(list);
+  return rebuild_channels(c);
 }
 
 int32_t efdc_xm_congrad(efdc_xm_ctx *c, const double *ccc, const double *ccs, const double *ccn,
@@ -1564,6 +1790,10 @@ int32_t efdc_xm_calib_enable(efdc_xm_ctx *c, int32_t nsnap) {
   }
   if (c->any_may_asym) {
     set_error("efdc_xm_calib_enable: the adjoint covers clamped open boundaries (ISPB=0) only");
+    return EFDC_XM_UNSUPPORTED;
+  }
+  if (c->S.ch.n > 0) {
+    set_error("efdc_xm_calib_enable: the adjoint does not cover sub-grid channels");
     return EFDC_XM_UNSUPPORTED;
   }
   if (c->calib) {

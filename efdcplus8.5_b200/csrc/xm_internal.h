@@ -32,12 +32,16 @@ constexpr int TILE = TX * TY;  // 256 slots per tile
 constexpr int NT = TILE;       // threads per CTA in the cell kernels
 constexpr int MT_MAX = 16;     // max harmonic constituents per call
 
-enum SlotKind : uint8_t { LAND = 0, WATER = 1, OPENBC = 2 };
+// CHAN: a water cell that is the host or guest of a sub-grid channel (its CC
+// enters the minimum diagonal after the channel terms, not in the assembly)
+enum SlotKind : uint8_t { LAND = 0, WATER = 1, OPENBC = 2, CHAN = 3 };
 
 // Per-member scalars of one call (device memory, refreshed every step).
 struct StepScalars {
   double delt, deltd2, delti, g, gi, hdry, rsqm, snlt, ritb1;
   int isdry, ndrystp, isbal, iterm;
+  double rlamn;         // QCHERR: implicit weight of the channel flows
+  int chan_consistent;  // channels: 1 = A*p with -CCCCHH (else as congradc.f90 writes it)
   double cosv[MT_MAX], sinv[MT_MAX];
 };
 
@@ -66,6 +70,28 @@ struct Glob {
 };
 
 // Static per-slot model data (FP64).  Land slots hold element LC.
+// Sub-grid channels of all members, packed member after member (channel NMD
+// of member m at cstart[m] + NMD - 1).  Slots are tile-order cells.
+struct DevChan {
+  int n;                     // channels of all members (0: none)
+  const int *cstart;         // [M+1]
+  const int *type;           // MDCHTYP: 1 x-direction, 2 y-direction
+  const int *host, *guest;   // slots of LMDCHH and of LMDCHU (x) / LMDCHV (y)
+  const int *gu;             // slot of LMDCHU for the y-direction HP test; -1: L = 1
+  const int *qhost, *qguest; // quads holding the host / guest slot
+  const int *first_host, *first_guest;  // 1: first endpoint of the member on its cell
+  const double *len, *fric;  // CHANLEN, CHANFRIC
+  const double *gw, *gl;     // guest's WCHAN (DXP x, DYP y) and cross length (DYP x, DXP y)
+  const double *hp1;         // [M] HP(1) of each member (its value at upload)
+  double *qu, *qv, *qun, *qvn;  // QCHANU, QCHANV, QCHANUN, QCHANVN
+  double *qut, *qvt;         // QCHANUT, QCHANVT: the flows at step entry
+  double *cu, *cv, *chh;     // CCCCHU, CCCCHV, CCCCHH (unscaled)
+  double *p1h, *p1g;         // P1 at host and guest (P at step entry)
+  double *p0h, *p0g;         // P at the entry of a MIXED solve
+  float *hh32;               // MIXED: coupling of the Jacobi-scaled FP32 operator
+  int *iact;                 // IACTIVE
+};
+
 struct DevStatic {
   const int4 *tnbr;       // [ntile] (w, e, s, n) neighbour tiles, 0 = ghost tile
   const uint8_t *kind;    // [nslot]
@@ -82,6 +108,7 @@ struct DevStatic {
   const double *hruo, *hrvo, *subo, *svbo, *sbxo, *sbyo, *belv;
   const double *rcx;      // RCX = RCY: 1 on water, 0 on ghosts (calpuv2c.f90:97-102)
   const double *fsgzu, *fsgzv;  // 0.5/DXYU, 0.5/DXYV (calpuv2c.f90:111-116)
+  DevChan ch;                   // sub-grid channels (ch.n == 0: none)
 };
 
 // Per-step state and work arrays (tile layout).

@@ -21,6 +21,7 @@ struct Launch {
   bool mx_jac = true;    // MIXED: some member runs the Jacobi inner solve
   bool mx_poly = false;  // MIXED: some member runs the polynomial-preconditioned one
   bool may_asym = true;  // some member's operator can be unsymmetric (else symmetric kernels)
+  bool chan = false;     // sub-grid channel terms (a step of a context with channels)
 };
 
 // One array to move between host order and tile order (see k_scatter).
@@ -31,6 +32,22 @@ struct CopyJob {
 };
 
 void launch_begin(const Launch &l, const DevStatic &S, const DevState &X);
+// sub-grid channels (xm_chan.cu); each does nothing unless l.chan
+void launch_chan_entry(const Launch &l, const DevStatic &S, const DevState &X);
+void launch_chan_sub(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
+                     const int *act, int first_sweep);
+void launch_chan_res64(const Launch &l, const DevStatic &S, const DevSystem &Y, const double *P,
+                       const Ctl *ctl, double *part);
+void launch_chan_mv64(const Launch &l, const DevStatic &S, const DevSystem &Y, const Ctl *ctl,
+                      double *part);
+void launch_chan_flow(const Launch &l, const DevStatic &S, const DevState &X, const int *act);
+void launch_chan_exch(const Launch &l, const DevStatic &S, const DevState &X, const int *act);
+void launch_chan_p0(const Launch &l, const DevStatic &S, const SysView &V, const double *P,
+                    const int *act);
+void launch_chan_resmx(const Launch &l, const DevStatic &S, const SysView &V, const DevSystem &Y,
+                       const double *P, const Ctl *ctl, double *part);
+void launch_chan_mvmx(const Launch &l, const DevStatic &S, const DevSystem &Y, const Ctl *ctl,
+                      double *part);
 void launch_sweep_reset(const Launch &l, Ctl *ctl, const int *act, int nmember);
 void launch_assemble(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
                      const int *act);

@@ -172,6 +172,7 @@ void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, C
     k_mx_matvec<true><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
   else
     k_mx_matvec<false><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
+  launch_chan_mvmx(l, S, Y, ctl, part);
   k_red_mx_matvec<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part);
   count_launches(2);
 }

@@ -1057,6 +1057,7 @@ void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, dou
     k_cg_init<true><<<quad_grid(l, S, k_cg_init<true>), NT, 0, l.stream>>>(S, Y, P, ctl, part);
   else
     k_cg_init<false><<<quad_grid(l, S, k_cg_init<false>), NT, 0, l.stream>>>(S, Y, P, ctl, part);
+  launch_chan_res64(l, S, Y, P, ctl, part);
   k_red_cg_init<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part);
   count_launches(2);
 }
@@ -1066,6 +1067,7 @@ void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, C
     k_cg_matvec<true><<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, ctl, part);
   else
     k_cg_matvec<false><<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, ctl, part);
+  launch_chan_mv64(l, S, Y, ctl, part);
   k_red_cg_matvec<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part);
   count_launches(2);
 }
@@ -1088,6 +1090,7 @@ void launch_mx_resid(const Launch &l, const DevStatic &S, const SysView &V, cons
   else
     k_mx_resid<false><<<quad_grid(l, S, k_mx_resid<false>), NT, 0, l.stream>>>(S, V, Y, P, ctl,
                                                                              part);
+  launch_chan_resmx(l, S, V, Y, P, ctl, part);
   k_red_mx_resid<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, rsqm_fac, rel_tol,
                                                       no_stop, V.unscaled);
   count_launches(2);

@@ -51,7 +51,8 @@ class Params(C.Structure):
                 ("snlt", C.c_double), ("ritb1", C.c_double), ("iterm", C.c_int32),
                 ("isdry", C.c_int32), ("ndrystp", C.c_int32), ("isbal", C.c_int32),
                 ("n", C.c_int32), ("ntstbc", C.c_int32), ("max_sweeps", C.c_int32),
-                ("precision", C.c_int32), ("mixed_rsq_factor", C.c_double)]
+                ("precision", C.c_int32), ("mixed_rsq_factor", C.c_double),
+                ("qcherr", C.c_double), ("chan_consistent", C.c_int32), ("pad_", C.c_int32)]
 
 
 class Fields(C.Structure):
@@ -64,7 +65,13 @@ class Fields(C.Structure):
                 ("vhe", _pd), ("hpi", _pd), ("hui", _pd), ("hvi", _pd),
                 ("qdwaste", _pd), ("vdwaste", _pd), ("lwet", _pi), ("ldry", _pi),
                 ("ccc", _pd), ("ccs", _pd), ("ccw", _pd), ("cce", _pd), ("ccn", _pd),
-                ("fptmp", _pd)]
+                ("fptmp", _pd), ("qchanu", _pd), ("qchanv", _pd), ("qchanun", _pd),
+                ("qchanvn", _pd)]
+
+
+class Channels(C.Structure):
+    _fields_ = [("n", C.c_int32), ("type", _pi), ("lhost", _pi), ("lu", _pi), ("lv", _pi),
+                ("chanlen", _pd), ("chanfric", _pd), ("dxp", _pd), ("dyp", _pd)]
 
 
 class Stats(C.Structure):
@@ -88,6 +95,7 @@ FIELD_DOUBLE_INOUT = ("p", "hp", "h1p", "hu", "hv", "uhdye", "vhdxe", "sub", "sv
 FIELD_INT_INOUT = ("lmaskdry", "iscdry", "lopenbcdry", "natdry")
 FIELD_IN = ("fcaxe", "fcaye", "fxe", "fye", "tsx", "tsy", "tbx", "tby", "qsume")
 FIELD_OUT = ("uhe", "vhe", "hpi", "hui", "hvi", "qdwaste", "vdwaste")
+FIELD_CHAN = ("qchanu", "qchanv", "qchanun", "qchanvn")  # per channel, in/out
 FIELD_DIAG = ("ccc", "ccs", "ccw", "cce", "ccn", "fptmp")
 
 
@@ -163,14 +171,33 @@ def make_params(p: dict, *, n: int, tn: float, precision: int = PREC_FP64):
     s.max_sweeps = p.get("max_sweeps", 500)
     s.precision = precision
     s.mixed_rsq_factor = p.get("mixed_rsq_factor", 0.0)
+    s.qcherr = p.get("qcherr", 1.0)
+    s.chan_consistent = int(p.get("chan_consistent", 0))
     return s
+
+
+def make_channels(ch: dict | None):
+    """A Channels struct over a dict of numpy arrays (type, lhost, lu, lv:
+    int32; chanlen, chanfric: float64 per channel; dxp, dyp: float64 over
+    1..LC), or an empty one for None.  Returns (struct, kept arrays)."""
+    s = Channels()
+    if not ch:
+        s.n = 0
+        return s, []
+    keep = [np.ascontiguousarray(ch[k], dtype=np.int32) for k in ("type", "lhost", "lu", "lv")]
+    keep += [np.ascontiguousarray(ch[k], dtype=np.float64)
+             for k in ("chanlen", "chanfric", "dxp", "dyp")]
+    s.n = int(keep[0].size)
+    s.type, s.lhost, s.lu, s.lv = (_ip(a) for a in keep[:4])
+    s.chanlen, s.chanfric, s.dxp, s.dyp = (_dp(a) for a in keep[4:])
+    return s, keep
 
 
 def make_fields(st: dict, *, diag: bool = False, lists: bool = False):
     """Build a Fields struct over the numpy arrays of a state dict (in place)."""
     s = Fields()
     keep = []
-    for k in FIELD_DOUBLE_INOUT + FIELD_IN + FIELD_OUT:
+    for k in FIELD_DOUBLE_INOUT + FIELD_IN + FIELD_OUT + FIELD_CHAN:
         a = st.get(k)
         if a is not None:
             setattr(s, k, _dp(a))
@@ -243,6 +270,8 @@ def load(path: str | os.PathLike | None = None):
     lib.efdc_xm_stream.restype = C.c_void_p
     lib.efdc_xm_stream.argtypes = [C.c_void_p]
     lib.efdc_xm_kernel_launches.restype = C.c_int64
+    lib.efdc_xm_set_channels.restype = C.c_int32
+    lib.efdc_xm_set_channels.argtypes = [C.c_void_p, C.c_int32, C.POINTER(Channels)]
     lib.efdc_xm_transfer_bytes.restype = None
     lib.efdc_xm_transfer_bytes.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.efdc_xm_time_kernels.restype = C.c_int32
@@ -344,6 +373,13 @@ class Solver:
 
     def stream(self) -> int:
         return int(self.lib.efdc_xm_stream(self.ctx) or 0)
+
+    def set_channels(self, ch: dict | None, member: int = 0):
+        s, _keep = make_channels(ch)
+        rc = self.lib.efdc_xm_set_channels(self.ctx, member, C.byref(s))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_set_channels: {STATUS_NAMES.get(rc, rc)}: "
+                               f"{self.last_error()}")
 
     def time_kernels(self, precision: int, reps: int = 20) -> KTime:
         kt = KTime()
@@ -462,6 +498,13 @@ class BatchSolver:
             self.close()
         except Exception:
             pass
+
+    def set_channels(self, ch: dict | None, member: int):
+        s, _keep = make_channels(ch)
+        rc = self.lib.efdc_xm_set_channels(self.ctx, member, C.byref(s))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_set_channels: {STATUS_NAMES.get(rc, rc)}: "
+                               f"{self.last_error()}")
 
     def _fields(self, states, **kw):
         if len(states) != self.m:

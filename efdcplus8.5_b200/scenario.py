@@ -69,6 +69,7 @@ class Scenario:
     state: dict
     params: dict
     ijct: np.ndarray = field(repr=False, default=None)
+    channels: dict = field(repr=False, default=None)  # sub-grid channels (add_channels)
 
     @property
     def ncell(self) -> int:
@@ -271,7 +272,7 @@ def build_grid(ijct, dxp2d, dyp2d, belv2d, *, obc=None, mtide=1, tcp=(M2_PERIOD,
                 dxyu=dxyu, dxyv=dxyv, hruo=hruo, hrvo=hrvo, subo=subo, svbo=svbo,
                 sbxo=sbxo, sbyo=sbyo, belv=belv, mtide=mtide,
                 tcp=np.asarray(tcp, dtype=np.float64)[:mtide], obc=sides,
-                dxu=dxu, dyu=dyu, dxv=dxv, dyv=dyv)
+                dxu=dxu, dyu=dyu, dxv=dxv, dyv=dyv, dxp=dxp, dyp=dyp)
     init = dict(sub=sub, svb=svb, sbx=sbx, sby=sby)
     return la, lc, grid, lij, init
 
@@ -539,3 +540,53 @@ def tidal_flat(n=1024, *, seed=5, hdry=0.05, amp=2.0, ramp=(-2.0, 15.0 / 4.0),
     return make_scenario(n, n, seed=seed, land_frac=0.0, belv2d=belv, dx=50.0, dy=50.0,
                          obc_sides=("W",), amp=amp, dt=dt, isdry=99, hdry=hdry,
                          ndrystp=-10, rsqm=1e-10, iterm=500, kc=4)
+
+
+def add_channels(scn: Scenario, n: int = 6, *, seed: int = 0, types=(1, 2), qcherr: float = 1.0,
+                 chanlen=(20.0, 80.0), chanfric=(0.5, 5.0), reach: int = 3,
+                 hmin: float = 0.1) -> Scenario:
+    """Sub-grid channels (the MDCHH host-guest pairs of subchan.f90) between
+    seeded pairs of distinct water cells that are not open-boundary cells, the
+    guest within `reach` cells of its host.  Channel k has type
+    types[k % len(types)]: 1 = x-direction (guest in LMDCHU, LMDCHV = 1),
+    2 = y-direction (guest in LMDCHV, LMDCHU = 1), as input.f90:2576-2588 sets
+    them.  Adds the per-channel flows QCHANU, QCHANV, QCHANUN, QCHANVN (zero,
+    as input.f90 starts them) to the state, QCHERR to the parameters, and
+    HP(1) = HMIN (ainit.f90:91; SUBCHAN's y-direction test reads HP(LMDCHU))."""
+    rng = np.random.default_rng(seed)
+    g = scn.grid
+    bc = set(int(x) for s_ in SIDES for x in g["obc"][s_]["l"])
+    lij = {(int(g["il"][L - 1]), int(g["jl"][L - 1])): L for L in range(2, scn.la + 1)}
+    used = set(bc)
+    host, guest = [], []
+    for L in rng.permutation(np.arange(2, scn.la + 1)):
+        if len(host) == n:
+            break
+        L = int(L)
+        if L in used:
+            continue
+        i, j = int(g["il"][L - 1]), int(g["jl"][L - 1])
+        near = [lij[(i + di, j + dj)] for di in range(-reach, reach + 1)
+                for dj in range(-reach, reach + 1)
+                if (di or dj) and (i + di, j + dj) in lij and lij[(i + di, j + dj)] not in used]
+        if not near:
+            continue
+        G_ = int(near[rng.integers(len(near))])
+        host.append(L)
+        guest.append(G_)
+        used.update((L, G_))
+    host = np.array(host, dtype=np.int32)
+    guest = np.array(guest, dtype=np.int32)
+    n = host.size
+    typ = np.array([types[k % len(types)] for k in range(n)], dtype=np.int32)
+    lu = np.where(typ == 1, guest, 1).astype(np.int32)
+    lv = np.where(typ == 2, guest, 1).astype(np.int32)
+    scn.channels = dict(type=typ, lhost=host, lu=lu, lv=lv,
+                        chanlen=rng.uniform(*chanlen, n), chanfric=rng.uniform(*chanfric, n),
+                        dxp=np.asarray(g["dxp"], dtype=np.float64),
+                        dyp=np.asarray(g["dyp"], dtype=np.float64))
+    for k in ("qchanu", "qchanv", "qchanun", "qchanvn"):
+        scn.state[k] = np.zeros(n)
+    scn.state["hp"][0] = hmin
+    scn.params["qcherr"] = qcherr
+    return scn

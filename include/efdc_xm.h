@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define EFDC_XM_ABI_VERSION 1
+#define EFDC_XM_ABI_VERSION 2
 
 /* Status codes.  The reference STOPs where these are returned. */
 enum efdc_xm_status {
@@ -105,6 +105,15 @@ typedef struct efdc_xm_params {
                               the default 0.1 (the FP32 path converges a little past
                               RSQM so that its per-step surface error against the FP64
                               solve stays well inside 1e-6 m)                         */
+  double qcherr;     /* QCHERR: implicit weight RLAMN of the sub-grid channel flows
+                        (calpuv2c.f90:353-354); used only where channels are set      */
+  int32_t chan_consistent; /* channels only.  0: CONGRADC as written, which adds the
+                        coupling CCCCHH with the same sign to the initial residual
+                        (congradc.f90:59-77) and to A*p (:99-116), so that its CG
+                        solves (A+C)P = b + 2C*P0 rather than (A-C)P = b (P0: P at
+                        entry); the flows it gives can grow without bound.  1: the
+                        conductance operator (A-C)P = b, i.e. A*p with -CCCCHH     */
+  int32_t pad_;
 } efdc_xm_params;
 
 /* Per-call arrays.  "in/out" arrays are read and overwritten.  Optional outputs
@@ -134,6 +143,12 @@ typedef struct efdc_xm_fields {
   int32_t *lwet, *ldry;               /* LWET(1..LAWET), LDRY(1..LADRY), optional    */
   /* optional diagnostics: the scaled system of the last sweep, as CONGRAD saw it */
   double *ccc, *ccs, *ccw, *cce, *ccn, *fptmp;
+  /* sub-grid channels (efdc_xm_set_channels), one element per channel NMD,
+   * in/out: QCHANU, QCHANV (the flows of the previous step in, the new ones
+   * out, calpuv2c.f90:440-460) and QCHANUN, QCHANVN (set to zero where a
+   * channel is inactive, else left as they are).  Required where channels
+   * are set, ignored elsewhere. */
+  double *qchanu, *qchanv, *qchanun, *qchanvn;
 } efdc_xm_fields;
 
 typedef struct efdc_xm_stats {
@@ -150,6 +165,22 @@ typedef struct efdc_xm_stats {
 } efdc_xm_stats;
 
 typedef struct efdc_xm_ctx efdc_xm_ctx;
+
+/* Sub-grid channels: MDCHH host-guest pairs whose exchange flow enters the
+ * external solve implicitly (subchan.f90:1-124; calpuv2c.f90:139-145,
+ * 352-356, 401-410, 440-460, 538-556) and the operator CONGRADC solves
+ * (congradc.f90:1-207).  Arrays of n elements, channel NMD at [NMD-1]. */
+typedef struct efdc_xm_channels {
+  int32_t n;               /* MDCHH (0: no channels)                                  */
+  const int32_t *type;     /* MDCHTYP: 1 x-direction (guest LMDCHU), 2 y-direction
+                              (guest LMDCHV); other types are not supported          */
+  const int32_t *lhost;    /* LMDCHH                                                  */
+  const int32_t *lu, *lv;  /* LMDCHU, LMDCHV (1 where unused, as input.f90 sets them) */
+  const double *chanlen;   /* CHANLEN as ainit.f90:286-316 leaves it                 */
+  const double *chanfric;  /* CHANFRIC                                                */
+  const double *dxp, *dyp; /* DXP, DYP of the model (1-based, LC elements): the
+                              guest cells' widths and lengths                         */
+} efdc_xm_channels;
 
 /* Version of this header the library was built with. */
 int32_t efdc_xm_abi_version(void);
@@ -177,6 +208,14 @@ int32_t efdc_xm_upload(efdc_xm_ctx *ctx, const efdc_xm_fields *f);
 int32_t efdc_xm_step_device(efdc_xm_ctx *ctx, const efdc_xm_params *prm,
                             efdc_xm_stats *stats);
 int32_t efdc_xm_download(efdc_xm_ctx *ctx, efdc_xm_fields *f);
+
+/* Sets (n > 0) or removes (n == 0) the sub-grid channels of member `member`
+ * of the context (0 for a single-basin context): the input of
+ * calpuv2c.f90:139-145 and subchan.f90.  The host and guest cells must be
+ * water cells (2..LA) that are not open-boundary cells, and differ.  A step
+ * of a member with channels solves CONGRADC's system in place of CONGRAD's
+ * (calpuv2c.f90:409-410) and needs the QCHANU..QCHANVN fields. */
+int32_t efdc_xm_set_channels(efdc_xm_ctx *ctx, int32_t member, const efdc_xm_channels *ch);
 
 /* Standalone replacement of CONGRAD (congrad.f90:1-191) for callers that
  * assemble the scaled system themselves (e.g. calpuv9c.f90:446).  Arrays are

@@ -1,5 +1,6 @@
 // efdc_oracle.cpp -- TEST INFRASTRUCTURE ONLY: CPU FP64 restatement of EFDC+
-// 8.5 CALPUV2C / CONGRAD / SETOPENBC / SETOPENBC2 / NEGDEP (check part).
+// 8.5 CALPUV2C / CONGRAD / CONGRADC / SUBCHAN / SETOPENBC / SETOPENBC2 /
+// NEGDEP (check part).
 // Parity against the reference is UNPINNED (no compiler, no reference tests);
 // see efdc_oracle.h.  Each block cites the Fortran it restates.
 //
@@ -32,6 +33,16 @@ struct Side {
   std::vector<double> pcb, psb;    // [(m-1)*n + (ll-1)]
 };
 
+// Sub-grid channels (GLOBAL's MDCHH arrays), channel NMD at [NMD-1].
+struct Channels {
+  int n = 0;
+  std::vector<int> typ, lh, lu, lv;
+  std::vector<double> len, fric, dxp, dyp;  // dxp/dyp 1-based over 1..LC
+  // SUBCHAN's per-step outputs and the step-start copies of CALPUV2C
+  std::vector<double> cu, cv, chh, qut, qvt;
+  std::vector<int> iact;
+};
+
 }  // namespace
 
 struct oracle_ctx {
@@ -50,6 +61,8 @@ struct oracle_ctx {
       vhdx1e;
   std::vector<double> pcg, pnv, pev, pwv, psv, rcg, apcg, tmpcg;
   std::vector<int> oldmask;
+  Channels ch;
+  std::vector<double> p1;  // P at entry (P1, calpuv2c.f90:259)
 };
 
 namespace {
@@ -73,10 +86,14 @@ void copy1(std::vector<T> &dst, const T *src, int lc) {
     for (int L = 1; L <= lc; ++L) dst[L] = src[L - 1];
 }
 
-// CONGRAD body (congrad.f90:54-187) on the context's scaled system.
-// p is the caller's 1-based P. Returns 0 or EFDC_XM_CG_MAXITER / NONFINITE.
+// CONGRAD body (congrad.f90:54-187) on the context's scaled system.  With
+// channels (chan = true) it is CONGRADC (congradc.f90:1-207): the same
+// iteration plus the host-guest couplings CCCCHH, added as written to the
+// initial residual (:59-77) and to A*p (:99-116); with `consistent` A*p takes
+// -CCCCHH instead (the operator of the residual).  p is the caller's 1-based
+// P. Returns 0 or EFDC_XM_CG_MAXITER / NONFINITE.
 int congrad(oracle_ctx *c, F<double> P, double rsqm, int iterm, int *iters_out,
-            double *rsq_out) {
+            double *rsq_out, bool chan = false, bool consistent = false) {
   const int la = c->la;
   const int *LNC = c->lnc.data(), *LSC = c->lsc.data(), *LEC = c->lec.data(),
             *LWC = c->lwc.data();
@@ -98,6 +115,21 @@ int congrad(oracle_ctx *c, F<double> P, double rsqm, int iterm, int *iters_out,
     RCG[L] = FPTMP[L] - CCC[L] * P[L] - CCN[L] * PN[L] - CCS[L] * PS[L] -
              CCW[L] * PW[L] - CCE[L] * PE[L];
   });
+  const Channels &ch = c->ch;
+  if (chan)  // congradc.f90:59-77
+    for (int k = 0; k < ch.n; ++k) {
+      const int LH = ch.lh[k];
+      if (ch.typ[k] == 1) {
+        const int LU = ch.lu[k];
+        RCG[LU] = RCG[LU] + ch.chh[k] * P[LH];
+        RCG[LH] = RCG[LH] + ch.chh[k] * P[LU];
+      }
+      if (ch.typ[k] == 2) {
+        const int LV = ch.lv[k];
+        RCG[LV] = RCG[LV] + ch.chh[k] * P[LH];
+        RCG[LH] = RCG[LH] + ch.chh[k] * P[LV];
+      }
+    }
   // :79-88
   for (int L = 2; L <= la; ++L) PCG[L] = RCG[L] * CCCI[L];
   double RPCG = 0.;
@@ -134,6 +166,21 @@ int congrad(oracle_ctx *c, F<double> P, double rsqm, int iterm, int *iters_out,
       }
 #pragma omp single
       {  // :118-125 serial dot "to prevent roundoff error"
+        if (chan)  // congradc.f90:99-116
+          for (int k = 0; k < ch.n; ++k) {
+            const int LH = ch.lh[k];
+            const double h = consistent ? -ch.chh[k] : ch.chh[k];
+            if (ch.typ[k] == 1) {
+              const int LU = ch.lu[k];
+              APCG[LU] = APCG[LU] + h * PCG[LH];
+              APCG[LH] = APCG[LH] + h * PCG[LU];
+            }
+            if (ch.typ[k] == 2) {
+              const int LV = ch.lv[k];
+              APCG[LV] = APCG[LV] + h * PCG[LH];
+              APCG[LH] = APCG[LH] + h * PCG[LV];
+            }
+          }
         PAPCG = 0.;
         for (int L = 2; L <= la; ++L) PAPCG = PAPCG + APCG[L] * PCG[L];
         ALPHA = RPCG / PAPCG;
@@ -180,6 +227,96 @@ int congrad(oracle_ctx *c, F<double> P, double rsqm, int iterm, int *iters_out,
   }
   *iters_out = iter;  // IDRYTBP = ITER (:187)
   return EFDC_XM_OK;
+}
+
+// SUBCHAN (subchan.f90:1-124): per channel NMD in order, the activity test,
+// the implicit coefficients CCCCHU, CCCCHV, CCCCHH, and their entries in CC
+// and FP of the host and guest cells.  RLAMN = QCHERR, DE_T = DELT.
+void subchan(oracle_ctx *c, double G, double DE_T, double HDRY, double RLAMN,
+             F<const double> H1P, F<const double> HP, double *CC, double *FP) {
+  Channels &ch = c->ch;
+  const double RLAMO = 1. - RLAMN;
+  const double *BELV = c->belv.data(), *P1 = c->p1.data();
+  for (int k = 0; k < ch.n; ++k) {
+    ch.cu[k] = 0.0;
+    ch.cv[k] = 0.0;
+    ch.chh[k] = 0.0;
+    const int LHOST = ch.lh[k], LCHNU = ch.lu[k], LCHNV = ch.lv[k];
+    if (ch.typ[k] == 1) {  // :29-62 x-direction channel
+      ch.iact[k] = 0;
+      const double SRFHOST = H1P[LHOST] + BELV[LHOST];
+      const double SRFCHAN = H1P[LCHNU] + BELV[LCHNU];
+      if (SRFCHAN > SRFHOST)
+        if (H1P[LCHNU] > HDRY) ch.iact[k] = 1;
+      if (SRFHOST > SRFCHAN)
+        if (H1P[LHOST] > HDRY) ch.iact[k] = 1;
+      if (HP[LHOST] <= 0.0 || HP[LCHNU] <= 0.0)
+        if (ch.iact[k] == 1) ch.iact[k] = 0;
+      if (ch.iact[k] == 1) {
+        const double WCHAN = ch.dxp[LCHNU];
+        const double RLCHN = 0.5 * ch.dyp[LCHNU] + ch.len[k];
+        double HCHAN = 0.5 * ch.dyp[LCHNU] * H1P[LCHNU] + ch.len[k] * H1P[LHOST];
+        HCHAN = HCHAN / RLCHN;
+        if (HCHAN > 0.) {
+          const double TMPVAL = ch.fric[k] * DE_T / (HCHAN * HCHAN * WCHAN);
+          ch.cu[k] = 1. / (1. + TMPVAL * std::fabs(ch.qut[k]));
+          ch.cv[k] = DE_T * HCHAN * WCHAN / RLCHN;
+        }
+      }
+    }
+    if (ch.typ[k] == 2) {  // :64-101 y-direction channel
+      int IHCHMX = 0, IHCHMN = 0;
+      double HCHNMX = 0., HCHNMN = 0.;
+      ch.iact[k] = 0;
+      const double SRFHOST = H1P[LHOST] + BELV[LHOST];
+      const double SRFCHAN = H1P[LCHNV] + BELV[LCHNV];
+      if (SRFCHAN > SRFHOST)
+        if (H1P[LCHNV] > HDRY) {
+          HCHNMX = -H1P[LCHNV];
+          IHCHMX = 1;
+          ch.iact[k] = 1;
+        }
+      if (SRFHOST > SRFCHAN)
+        if (H1P[LHOST] > HDRY) {
+          HCHNMN = H1P[LHOST];
+          IHCHMN = 1;
+          ch.iact[k] = 1;
+        }
+      // :84 tests HP(LCHNU) for the y-direction channel too, as written
+      if (HP[LHOST] <= 0.0 || HP[LCHNU] <= 0.0)
+        if (ch.iact[k] == 1) ch.iact[k] = 0;
+      if (ch.iact[k] == 1) {
+        const double WCHAN = ch.dyp[LCHNV];
+        const double RLCHN = 0.5 * ch.dxp[LCHNV] + ch.len[k];
+        double HCHAN = 0.5 * ch.dxp[LCHNV] * H1P[LCHNV] + ch.len[k] * H1P[LHOST];
+        HCHAN = HCHAN / RLCHN;
+        if (IHCHMX == 1) HCHAN = std::max(HCHAN, HCHNMX);
+        if (IHCHMN == 1) HCHAN = std::min(HCHAN, HCHNMN);
+        if (HCHAN > 0.) {
+          const double TMPVAL = ch.fric[k] * DE_T / (HCHAN * HCHAN * WCHAN);
+          ch.cu[k] = 1. / (1. + TMPVAL * std::fabs(ch.qvt[k]));
+          ch.cv[k] = DE_T * HCHAN * WCHAN / RLCHN;
+        }
+      }
+    }
+    // :104-119
+    CC[LHOST] = CC[LHOST] + G * RLAMN * RLAMN * ch.cu[k] * ch.cv[k];
+    ch.chh[k] = G * RLAMN * RLAMN * ch.cu[k] * ch.cv[k];
+    if (ch.typ[k] == 1) {
+      CC[LCHNU] = CC[LCHNU] + G * RLAMN * RLAMN * ch.cu[k] * ch.cv[k];
+      const double TMPVAL = G * (RLAMO + RLAMN * ch.cu[k]) * ch.qut[k] -
+                            G * RLAMN * RLAMO * ch.cu[k] * ch.cv[k] * (P1[LHOST] - P1[LCHNU]);
+      FP[LHOST] = FP[LHOST] + TMPVAL;
+      FP[LCHNU] = FP[LCHNU] - TMPVAL;
+    }
+    if (ch.typ[k] == 2) {
+      CC[LCHNV] = CC[LCHNV] + G * RLAMN * RLAMN * ch.cu[k] * ch.cv[k];
+      const double TMPVAL = G * (RLAMO + RLAMN * ch.cu[k]) * ch.qvt[k] -
+                            G * RLAMN * RLAMO * ch.cu[k] * ch.cv[k] * (P1[LHOST] - P1[LCHNV]);
+      FP[LHOST] = FP[LHOST] + TMPVAL;
+      FP[LCHNV] = FP[LCHNV] - TMPVAL;
+    }
+  }
 }
 
 }  // namespace
@@ -326,6 +463,20 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
   const int max_sweeps = prm->max_sweeps > 0 ? prm->max_sweeps : 500;
 
   int NCORDRY = 0;
+  Channels &ch = c->ch;
+  const bool chans = ch.n > 0;
+  const double RLAMN = prm->qcherr, RLAMO = 1. - RLAMN;  // :353-354
+  if (chans) {
+    if (!f->qchanu || !f->qchanv || !f->qchanun || !f->qchanvn) {
+      st->status = EFDC_XM_BAD_ARGUMENT;
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+    for (int k = 0; k < ch.n; ++k) {  // :139-145
+      ch.qut[k] = f->qchanu[k];
+      ch.qvt[k] = f->qchanv[k];
+    }
+    for (int L = 1; L <= lc; ++L) c->p1[L] = P[L];  // P1 = P (:259)
+  }
   // :150-157
   if (ISDRY > 0)
     for (int L : c->lobcs) LOPENBCDRY[L] = 0;
@@ -534,6 +685,10 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
       }
     }
 
+    // :352-356 implicit sub-grid channel interactions
+    if (chans) subchan(c, G, DELT, HDRY, RLAMN, F<const double>{H1P.b}, F<const double>{HP.b},
+                       CC, FP);
+
     // :360-377 minimum diagonal (order-free), FPTMP=FP
     double CCMNM = 1.e+18;
     for (int L = 2; L <= la; ++L) {
@@ -565,10 +720,14 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
       CCCI[L] = 1. / CCC[L];
     });
 
-    // :409 CONGRAD
+    // :401-405 channel coefficients scaled like the system
+    for (int k = 0; k < ch.n; ++k) ch.chh[k] = ch.chh[k] * CCMNMI;
+
+    // :409-410 CONGRAD, or CONGRADC with channels
     int iters = 0;
     double rsq = 0.;
-    const int cg = congrad(c, P, prm->rsqm, prm->iterm, &iters, &rsq);
+    const int cg =
+        congrad(c, P, prm->rsqm, prm->iterm, &iters, &rsq, chans, prm->chan_consistent != 0);
     iters_total += iters;
     last_iters = iters;
     last_rsq = rsq;
@@ -589,6 +748,30 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
       UHE[L] = UHDYE[L] * DYIU[L];
       VHE[L] = VHDXE[L] * DXIV[L];
     });
+    // :440-460 new channel exchange flows
+    for (int k = 0; k < ch.n; ++k) {
+      const double *P1 = c->p1.data();
+      if (ch.iact[k] > 0) {
+        const int LHOST = ch.lh[k], LCHNU = ch.lu[k], LCHNV = ch.lv[k];
+        if (ch.typ[k] == 1) {
+          f->qchanu[k] = ch.cu[k] * ch.qut[k] -
+                         RLAMN * ch.cu[k] * ch.cv[k] * (P[LHOST] - P[LCHNU]) -
+                         RLAMO * ch.cu[k] * ch.cv[k] * (P1[LHOST] - P1[LCHNU]);
+          f->qchanv[k] = 0.;
+        }
+        if (ch.typ[k] == 2) {
+          f->qchanu[k] = 0.;
+          f->qchanv[k] = ch.cu[k] * ch.qvt[k] -
+                         RLAMN * ch.cu[k] * ch.cv[k] * (P[LHOST] - P[LCHNV]) -
+                         RLAMO * ch.cu[k] * ch.cv[k] * (P1[LHOST] - P1[LCHNV]);
+        }
+      } else {
+        f->qchanv[k] = 0.;
+        f->qchanvn[k] = 0.;
+        f->qchanu[k] = 0.;
+        f->qchanun[k] = 0.;
+      }
+    }
     // :466-486 continuity
     for_domains(c, [&](int L) {
       const int LE = LEC[L], LN = LNC[L];
@@ -616,6 +799,22 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
           CC[L] = DELTI * DXYP[L];
           P[L] = (HP[L] + BELV[L]) * G;
           FP1[L] = DELTI * DXYP[L] * P[L];
+        }
+      }
+    }
+    // :538-556 channel exchanges
+    for (int k = 0; k < ch.n; ++k) {
+      if (ch.iact[k] > 0) {
+        const int LHOST = ch.lh[k], LCHNU = ch.lu[k], LCHNV = ch.lv[k];
+        if (ch.typ[k] == 1) {
+          const double TMPVAL = DELT * (RLAMN * f->qchanu[k] + RLAMO * ch.qut[k]);
+          HP[LHOST] = HP[LHOST] + TMPVAL * DXYIP[LHOST];
+          HP[LCHNU] = HP[LCHNU] - TMPVAL * DXYIP[LCHNU];
+        }
+        if (ch.typ[k] == 2) {
+          const double TMPVAL = DELT * (RLAMN * f->qchanv[k] + RLAMO * ch.qvt[k]);
+          HP[LHOST] = HP[LHOST] + TMPVAL * DXYIP[LHOST];
+          HP[LCHNV] = HP[LCHNV] - TMPVAL * DXYIP[LCHNV];
         }
       }
     }
@@ -821,6 +1020,29 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
   if (f->fptmp) for (int L = 1; L <= lc; ++L) f->fptmp[L - 1] = FPTMP[L];
   st->status = status;
   return status;
+}
+
+int oracle_set_channels(oracle_ctx *c, const efdc_xm_channels *in) {
+  Channels &ch = c->ch;
+  ch = Channels{};
+  if (!in || in->n <= 0) return EFDC_XM_OK;
+  const int n = in->n;
+  if (!in->type || !in->lhost || !in->lu || !in->lv || !in->chanlen || !in->chanfric ||
+      !in->dxp || !in->dyp)
+    return EFDC_XM_BAD_ARGUMENT;
+  ch.n = n;
+  ch.typ.assign(in->type, in->type + n);
+  ch.lh.assign(in->lhost, in->lhost + n);
+  ch.lu.assign(in->lu, in->lu + n);
+  ch.lv.assign(in->lv, in->lv + n);
+  ch.len.assign(in->chanlen, in->chanlen + n);
+  ch.fric.assign(in->chanfric, in->chanfric + n);
+  copy1(ch.dxp, in->dxp, c->lc);
+  copy1(ch.dyp, in->dyp, c->lc);
+  for (auto *v : {&ch.cu, &ch.cv, &ch.chh, &ch.qut, &ch.qvt}) v->assign(n, 0.0);
+  ch.iact.assign(n, 0);
+  c->p1.assign(size_t(c->lc) + 2, 0.0);
+  return EFDC_XM_OK;
 }
 
 int oracle_congrad(oracle_ctx *c, const double *ccc, const double *ccs,

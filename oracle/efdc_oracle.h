@@ -44,6 +44,10 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
                 efdc_xm_stats *st);
 
 /* CONGRAD on a caller-assembled scaled system (congrad.f90:54-187). */
+/* Sub-grid channels of the basin (efdc_xm_set_channels' contract); n = 0
+ * removes them.  Returns 0, or EFDC_XM_BAD_ARGUMENT. */
+int oracle_set_channels(oracle_ctx *c, const efdc_xm_channels *ch);
+
 int oracle_congrad(oracle_ctx *c, const double *ccc, const double *ccs,
                    const double *ccn, const double *ccw, const double *cce,
                    const double *ccci, const double *fptmp, double *p,

@@ -42,6 +42,8 @@ def load():
         lib.oracle_step.argtypes = [C.c_void_p, C.POINTER(X.Params), C.POINTER(X.Fields),
                                     C.POINTER(X.Stats)]
         pd = C.POINTER(C.c_double)
+        lib.oracle_set_channels.restype = C.c_int
+        lib.oracle_set_channels.argtypes = [C.c_void_p, C.POINTER(X.Channels)]
         lib.oracle_congrad.restype = C.c_int
         lib.oracle_congrad.argtypes = [C.c_void_p] + [pd] * 8 + [
             C.c_double, C.c_int, C.POINTER(C.c_int), pd]
@@ -76,6 +78,12 @@ class Oracle:
         st = X.Stats()
         self.lib.oracle_step(self.ctx, C.byref(params), C.byref(f), C.byref(st))
         return st
+
+    def set_channels(self, ch: dict | None):
+        s, _keep = X.make_channels(ch)
+        rc = self.lib.oracle_set_channels(self.ctx, C.byref(s))
+        if rc != 0:
+            raise RuntimeError("oracle_set_channels: bad channel arrays")
 
     def congrad(self, ccc, ccs, ccn, ccw, cce, ccci, fptmp, p, rsqm, iterm):
         it = C.c_int(0)

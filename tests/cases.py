@@ -47,6 +47,18 @@ def unsymmetric():
     return scn
 
 
+def channels(consistent=0, *, closed=False, qcherr=1.0, n=10, seed=21):
+    """A basin with `n` sub-grid channels (x- and y-direction, guests within
+    3 cells of their hosts).  With closed=True it has no open boundary and is
+    driven by its explicit terms only (its volume is constant).
+    `consistent` selects the channel operator (chan_consistent)."""
+    scn = S.make_scenario(60, 40, seed=seed, obc_sides=() if closed else ("W",), amp=0.5,
+                          dt=10.0, explicit_noise=3e-4)
+    S.add_channels(scn, n, seed=3, qcherr=qcherr)
+    scn.params["chan_consistent"] = consistent
+    return scn
+
+
 def state_err(a, b, la, key="p", g=S.G):
     d = np.abs(a[key][1:la] - b[key][1:la])
     return float(d.max() / (g if key == "p" else 1.0))
