@@ -62,7 +62,7 @@ uint64_t morton2(uint32_t x, uint32_t y) {
 
 constexpr int NSTAGE = 8;     // staging buffers (each holds one array of every member)
 constexpr int NCOPY = 4;      // streams for host<->device copies
-constexpr int MAX_JOBS = 64;  // arrays moved by one upload/download call
+constexpr int MAX_JOBS = 128;  // arrays moved by one upload/download call
 constexpr int GRAPH_ITERS = 4;  // CG iterations per graph launch
 constexpr int KERNELS_PER_ITER = 4;  // matvec, its reduce, update, its reduce
 
@@ -175,6 +175,11 @@ struct efdc_xm_ctx {
   std::vector<int> chan_start;  // [M+1] first channel of each member in S.ch
   std::vector<int> qstart_h;    // [M+1] first quad of each member
   double *chan_hp1 = nullptr;   // S.ch.hp1
+  // baroclinic terms: layers set by efdc_xm_set_layers (S.baro), and whether
+  // the current step has a member with them
+  std::vector<char> has_layers;  // [M]
+  bool step_baro = false;
+  std::vector<double> zeros_h;   // LC zeros: B of a member without it
 
   template <class T>
   T *alloc(size_t n, bool zero = true) {
@@ -189,7 +194,7 @@ struct efdc_xm_ctx {
     return xm::Launch{grid,    grid_cg, grid_mv64, grid_cg32,
                       grid_up32, ntile, nsm,       stream,
                       mx_jac,  mx_poly, any_may_asym || sys_external,
-                      S.ch.n > 0 && !sys_external};
+                      S.ch.n > 0 && !sys_external, step_baro && !sys_external};
   }
 };
 
@@ -523,6 +528,8 @@ xm::StepScalars make_scalars(const Member &mb, const efdc_xm_params *p) {
   s.isbal = p->isbal;
   s.iterm = p->iterm;
   s.rlamn = p->qcherr;  // calpuv2c.f90:353 (RLAMN = QCHERR)
+  s.baro = p->bsc > 1.E-6 ? 1 : 0;  // calpuv2c.f90:161, 192
+  s.gp = p->gp;
   s.chan_consistent = p->chan_consistent != 0 ? 1 : 0;
   // setopenbc.f90:24-29 on the host, libm as the reference
   for (int m = 0; m < mb.mtide && m < xm::MT_MAX; ++m) {
@@ -865,6 +872,7 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   c->hp1_h.assign(M, 1.0);
   c->chan_start.assign(M + 1, 0);
   c->qstart_h = qstart;
+  c->has_layers.assign(M, 0);
   cudaMemcpy(quads_d, quads.data(), quads.size() * sizeof(int4), cudaMemcpyHostToDevice);
   cudaMemcpy(qstart_d, qstart.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(tend_d, tend.data(), M * sizeof(int), cudaMemcpyHostToDevice);
@@ -1043,6 +1051,23 @@ int32_t efdc_xm_upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f) {
   XM_UP(tsx, X.tsx, 0) XM_UP(tsy, X.tsy, 0) XM_UP(tbx, X.tbx, 0) XM_UP(tby, X.tby, 0)
   XM_UP(qsume, X.qsume, 0) XM_UP(qdwaste, X.qdwaste, 0) XM_UP(vdwaste, X.vdwaste, 0)
 #undef XM_UP
+  // B(L,K), one staging job per layer; a member without B gets zeros
+  bool anyb = false;
+  for (int m = 0; m < M; ++m) anyb |= f[m].b != nullptr;
+  if (anyb && c->S.baro.kc > 0) {
+    for (int m = 0; m < M; ++m)
+      if (f[m].b && f[m].b_ld < c->mem[m].lc) {
+        set_error("efdc_xm_upload: member %d: b_ld %d < LC", m, f[m].b_ld);
+        return EFDC_XM_BAD_ARGUMENT;
+      }
+    for (int k = 0; k < c->S.baro.kc; ++k) {
+      std::vector<const void *> v(M);
+      for (int m = 0; m < M; ++m)
+        v[m] = f[m].b ? static_cast<const void *>(f[m].b + size_t(k) * f[m].b_ld)
+                      : static_cast<const void *>(c->zeros_h.data());
+      xs.push_back(Xfer{v, c->S.baro.b + size_t(k) * c->S.baro.stride, 0});
+    }
+  }
   if ((rc = upload_arrays(c, xs))) return rc;
   // the second buffer of each time-level pair starts as a copy (its land
   // slots must hold the ghost values too); the H1P input is not used because
@@ -1210,6 +1235,16 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
   c->mxview = xm::SysView{c->X.fp, c->X.cc, c->X.cs, c->X.cw, c->X.ce, c->X.cn, 1};
   c->last_mixed = mixed;
   c->sys_external = false;
+  c->step_baro = false;
+  for (int m = 0; m < M; ++m) {
+    if (!(prm[m].bsc > 1.E-6)) continue;
+    if (!c->has_layers[m]) {
+      set_error("efdc_xm_step: member %d: BSC > 1E-6 needs the layers (efdc_xm_set_layers)", m);
+      fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+    c->step_baro = true;
+  }
   const xm::Launch l = c->L();
   bool any_isdry = false, any_legacy = false, any99 = false, any_waste = false;
   std::vector<int> ncordry(M, 0), status(M, EFDC_XM_OK), max_sweeps(M);
@@ -1356,6 +1391,11 @@ int32_t efdc_xm_step_batch(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fi
     if (!x.p || !x.hp || !x.hu || !x.hv || !x.uhdye || !x.vhdxe || !x.sub || !x.svb) {
       set_error("efdc_xm_step: member %d: NULL argument (P, HP, HU, HV, UHDYE, VHDXE, SUB, SVB "
                 "are required)", m);
+      fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+    if (prm[m].bsc > 1.E-6 && !x.b) {
+      set_error("efdc_xm_step: member %d: BSC > 1E-6 needs B", m);
       fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
       return EFDC_XM_BAD_ARGUMENT;
     }
@@ -1509,7 +1549,10 @@ int rebuild_channels(efdc_xm_ctx *c) {
   c->chan_start = cstart;
   CK(cudaMemcpy(const_cast<uint8_t *>(c->S.kind), kind.data(), kind.size(), cudaMemcpyHostToDevice));
   drop_graphs(c);
-  if (n == 0) return EFDC_XM_OK;
+  if (n == 0) {
+    CK(cudaDeviceSynchronize());  // the kinds are in place before the next launch
+    return EFDC_XM_OK;
+  }
   auto dev = [&](const void *src, size_t bytes) -> void * {
     void *p = nullptr;
     if (cudaMalloc(&p, std::max<size_t>(bytes, 1)) != cudaSuccess) return nullptr;
@@ -1550,10 +1593,96 @@ int rebuild_channels(efdc_xm_ctx *c) {
     set_error("internal: channel arrays");
     return EFDC_XM_CUDA_ERROR;
   }
+  // copies and zeroing ran on the legacy stream, which the context's stream
+  // does not wait for
+  CK(cudaDeviceSynchronize());
   C.n = n;
   return EFDC_XM_OK;
 }
 }  // namespace
+
+int32_t efdc_xm_set_layers(efdc_xm_ctx *c, int32_t member, const efdc_xm_layers *ly) {
+  if (!c || !ly || member < 0 || member >= c->M || ly->kc < 1 || ly->kc > 64 || !ly->dzc ||
+      !ly->zz || ly->ld < c->mem[member].lc) {
+    set_error("efdc_xm_set_layers: need a context, a member, 1 <= kc <= 64, ld >= LC and the "
+              "DZC, ZZ arrays");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  xm::DevBaro &Bc = c->S.baro;
+  if (Bc.kc != 0 && Bc.kc != ly->kc) {
+    set_error("efdc_xm_set_layers: the members of a context share KC (%d, not %d)", Bc.kc,
+              ly->kc);
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  CK(cudaSetDevice(c->device));
+  const size_t ns = c->nslot;
+  if (Bc.kc == 0) {  // the planes, once (zeroed: land slots stay 0)
+    double *dzc = c->alloc<double>(ns * ly->kc), *zz = c->alloc<double>(ns * ly->kc);
+    double *b = c->alloc<double>(ns * ly->kc);
+    double *bi1 = c->alloc<double>(ns), *bi2 = c->alloc<double>(ns), *be = c->alloc<double>(ns);
+    if (!dzc || !zz || !b || !bi1 || !bi2 || !be) {
+      set_error("efdc_xm_set_layers: device allocation failed");
+      return EFDC_XM_CUDA_ERROR;
+    }
+    Bc.dzc = dzc;
+    Bc.zz = zz;
+    Bc.b = b;
+    Bc.bi1 = bi1;
+    Bc.bi2 = bi2;
+    Bc.be = be;
+    Bc.stride = (long long)ns;
+    Bc.kc = ly->kc;
+    int lcmax = 0;
+    for (const Member &mb : c->mem) lcmax = std::max(lcmax, mb.lc);
+    c->zeros_h.assign(size_t(lcmax) + 1, 0.0);
+  }
+  // the member's cells of each layer, host order -> tile order
+  const Member &mb = c->mem[member];
+  const int n = mb.la - 1;
+  std::vector<int> idx(n);
+  for (int L = 2; L <= mb.la; ++L) idx[L - 2] = mb.slot_of[L];
+  std::vector<double> val(size_t(n) * 2 * ly->kc);
+  for (int k = 0; k < ly->kc; ++k)
+    for (int L = 2; L <= mb.la; ++L) {
+      val[(size_t(2 * k)) * n + (L - 2)] = ly->dzc[size_t(k) * ly->ld + (L - 1)];
+      val[(size_t(2 * k + 1)) * n + (L - 2)] = ly->zz[size_t(k) * ly->ld + (L - 1)];
+    }
+  int *idx_d = nullptr;
+  double *val_d = nullptr;
+  if (cudaMalloc(&idx_d, sizeof(int) * std::max(n, 1)) != cudaSuccess ||
+      cudaMalloc(&val_d, sizeof(double) * std::max<size_t>(val.size(), 1)) != cudaSuccess) {
+    cudaFree(idx_d);
+    set_error("efdc_xm_set_layers: device allocation failed");
+    return EFDC_XM_CUDA_ERROR;
+  }
+  // the context's stream does not wait for the legacy stream: the zeroing of
+  // new planes and these copies must be complete before the scatter runs
+  if (cudaDeviceSynchronize() != cudaSuccess ||
+      cudaMemcpyAsync(idx_d, idx.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(val_d, val.data(), sizeof(double) * val.size(), cudaMemcpyHostToDevice,
+                      c->stream) != cudaSuccess) {
+    cudaFree(idx_d);
+    cudaFree(val_d);
+    set_error("efdc_xm_set_layers: copy failed");
+    return EFDC_XM_CUDA_ERROR;
+  }
+  for (int k = 0; k < ly->kc; ++k) {
+    xm::launch_put(c->stream, idx_d, val_d + size_t(2 * k) * n, n,
+                   const_cast<double *>(Bc.dzc) + size_t(k) * ns);
+    xm::launch_put(c->stream, idx_d, val_d + size_t(2 * k + 1) * n, n,
+                   const_cast<double *>(Bc.zz) + size_t(k) * ns);
+  }
+  const cudaError_t e = cudaStreamSynchronize(c->stream);
+  cudaFree(idx_d);
+  cudaFree(val_d);
+  if (e != cudaSuccess) {
+    set_error("efdc_xm_set_layers: %s", cudaGetErrorString(e));
+    return EFDC_XM_CUDA_ERROR;
+  }
+  c->has_layers[member] = 1;
+  return EFDC_XM_OK;
+}
 
 int32_t efdc_xm_set_channels(efdc_xm_ctx *c, int32_t member, const efdc_xm_channels *ch) {
   if (!c || !ch || member < 0 || member >= (c ? c->M : 0) || ch->n < 0) {
@@ -1896,8 +2025,8 @@ int32_t efdc_xm_calib_step(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_st
   std::memset(stats, 0, sizeof(*stats));
   int rc = calib_ready(c, "efdc_xm_calib_step");
   if (rc) return stats->status = rc;
-  if (!prm || prm->isdry != 0 || prm->precision != EFDC_XM_PREC_FP64) {
-    set_error("efdc_xm_calib_step: the calibration model runs FP64 with ISDRY=0");
+  if (!prm || prm->isdry != 0 || prm->precision != EFDC_XM_PREC_FP64 || prm->bsc > 1.E-6) {
+    set_error("efdc_xm_calib_step: the calibration model runs FP64 with ISDRY=0 and BSC=0");
     return stats->status = EFDC_XM_BAD_ARGUMENT;
   }
   CK(cudaSetDevice(c->device));
@@ -2039,6 +2168,7 @@ int32_t efdc_xm_calib_gradients(efdc_xm_ctx *c, double *dlog_n, double *dbelv, d
       if (state[k]) xs.push_back({one(state[k]), src[k], 0});
   }
   if ((rc = download_arrays(c, xs))) return rc;
+  CK(cudaStreamSynchronize(c->stream));  // the copies below run on the legacy stream
   const size_t np = size_t(c->nobc) * c->B.mtmax * sizeof(double);
   if (np && dpcb) CK(cudaMemcpy(dpcb, A.apcb, np, cudaMemcpyDeviceToHost));
   if (np && dpsb) CK(cudaMemcpy(dpsb, A.apsb, np, cudaMemcpyDeviceToHost));

@@ -42,6 +42,8 @@ struct StepScalars {
   int isdry, ndrystp, isbal, iterm;
   double rlamn;         // QCHERR: implicit weight of the channel flows
   int chan_consistent;  // channels: 1 = A*p with -CCCCHH (else as congradc.f90 writes it)
+  int baro;             // BSC > 1e-6: the baroclinic terms FPGXE, FPGYE enter
+  double gp;            // GP
   double cosv[MT_MAX], sinv[MT_MAX];
 };
 
@@ -92,6 +94,16 @@ struct DevChan {
   int *iact;                 // IACTIVE
 };
 
+// Baroclinic terms (CALEBI, standard sigma grid): layer planes of `stride`
+// elements (layer K at [(K-1)*stride]) in tile order.
+struct DevBaro {
+  int kc;                  // layers (0: not set)
+  long long stride;        // elements per plane (the slot count)
+  const double *dzc, *zz;  // DZC(L,K), ZZ(L,K)
+  double *b;               // B(L,K), uploaded with the fields
+  double *bi1, *bi2, *be;  // BI1W=BI1S, BI2W=BI2S, BEW=BES: kept between steps
+};
+
 struct DevStatic {
   const int4 *tnbr;       // [ntile] (w, e, s, n) neighbour tiles, 0 = ghost tile
   const uint8_t *kind;    // [nslot]
@@ -109,6 +121,7 @@ struct DevStatic {
   const double *rcx;      // RCX = RCY: 1 on water, 0 on ghosts (calpuv2c.f90:97-102)
   const double *fsgzu, *fsgzv;  // 0.5/DXYU, 0.5/DXYV (calpuv2c.f90:111-116)
   DevChan ch;                   // sub-grid channels (ch.n == 0: none)
+  DevBaro baro;                 // layers and buoyancy integrals (baro.kc == 0: none)
 };
 
 // Per-step state and work arrays (tile layout).

@@ -22,6 +22,7 @@ struct Launch {
   bool mx_poly = false;  // MIXED: some member runs the polynomial-preconditioned one
   bool may_asym = true;  // some member's operator can be unsymmetric (else symmetric kernels)
   bool chan = false;     // sub-grid channel terms (a step of a context with channels)
+  bool baro = false;     // some member of the step has the baroclinic terms (CALEBI)
 };
 
 // One array to move between host order and tile order (see k_scatter).
@@ -32,6 +33,7 @@ struct CopyJob {
 };
 
 void launch_begin(const Launch &l, const DevStatic &S, const DevState &X);
+void launch_put(cudaStream_t st, const int *idx, const double *val, int n, double *dst);
 // sub-grid channels (xm_chan.cu); each does nothing unless l.chan
 void launch_chan_entry(const Launch &l, const DevStatic &S, const DevState &X);
 void launch_chan_sub(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,

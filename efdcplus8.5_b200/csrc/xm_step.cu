@@ -28,19 +28,53 @@ namespace xm {
 // ---------------------------------------------------------------------------
 // calpuv2c.f90:214-220: the explicit transports FUHDYE (face between cell d
 // and its west neighbour, elevations P and PW) and FVHDXE (south face).
+// FPGXE / FPGYE: the baroclinic terms, 0.0 without them.
 __device__ __forceinline__ double fuh_face(const DevStatic &S, const DevState &X,
                                            const StepScalars &c, int d, double P, double PW,
-                                           double sub) {
+                                           double sub, double FPGXE) {
   return X.uhdy1e[d] - c.deltd2 * sub * S.hruo[d] * X.hu[d] * (P - PW) +
          sub * c.delt * S.dxiu[d] *
-             (S.dxyu[d] * (X.tsx[d] - c.ritb1 * X.tbx[d]) + X.fcaxe[d] + 0.0 - c.snlt * X.fxe[d]);
+             (S.dxyu[d] * (X.tsx[d] - c.ritb1 * X.tbx[d]) + X.fcaxe[d] + FPGXE -
+              c.snlt * X.fxe[d]);
 }
 __device__ __forceinline__ double fvh_face(const DevStatic &S, const DevState &X,
                                            const StepScalars &c, int d, double P, double PS,
-                                           double svb) {
+                                           double svb, double FPGYE) {
   return X.vhdx1e[d] - c.deltd2 * svb * S.hrvo[d] * X.hv[d] * (P - PS) +
          svb * c.delt * S.dyiv[d] *
-             (S.dxyv[d] * (X.tsy[d] - c.ritb1 * X.tby[d]) - X.fcaye[d] + 0.0 - c.snlt * X.fye[d]);
+             (S.dxyv[d] * (X.tsy[d] - c.ritb1 * X.tby[d]) - X.fcaye[d] + FPGYE -
+              c.snlt * X.fye[d]);
+}
+
+// CALEBI (calebi.f90:73-120) for the standard sigma grid (KSZ = 1): the
+// external buoyancy integrals of each wet cell (LWET of the last step: every
+// cell with ISDRY = 0, else the cells with LMASKDRY).  The reference's two
+// loops from the top layer down are one here (the same additions in the same
+// order).
+__global__ void __launch_bounds__(NT) k_calebi(DevStatic S, DevState X, int ntile) {
+  const DevBaro &Bc = S.baro;
+  TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    if (!c.baro) continue;
+    const int d = tile * TILE + threadIdx.x;
+    if (S.kind[d] == LAND) continue;
+    if (c.isdry > 0 && !X.lmaskdry[d]) continue;
+    double DBK = 0., BEC = 0., BI1C = 0., BI2C = 0.;
+    for (int k = Bc.kc - 1; k >= 0; --k) {
+      const size_t o = size_t(k) * size_t(Bc.stride) + d;
+      const double DZCC = Bc.dzc[o];
+      const double DZCB = DZCC * Bc.b[o];
+      DBK = DBK + DZCB;
+      const double BK = DBK - 0.5 * DZCB;
+      BEC = BEC + DZCB;
+      const double DZCBK = DZCC * BK;
+      BI1C = BI1C + DZCBK;
+      BI2C = BI2C + DZCBK + Bc.zz[o] * DZCB;
+    }
+    Bc.bi1[d] = BI1C;
+    Bc.bi2[d] = BI2C;
+    Bc.be[d] = BEC;
+  }
 }
 
 // calpuv2c.f90:282-290
@@ -95,8 +129,21 @@ __global__ void __launch_bounds__(NT) k_begin(DevStatic S, DevState X, int ntile
       X.wasted[d] = 0;
     }
     const double P = X.p[d];
-    X.fuhdye[d] = fuh_face(S, X, c, d, P, X.p[q.w], sub);
-    X.fvhdxe[d] = fvh_face(S, X, c, d, P, X.p[q.s], svb);
+    double FPGXE = 0., FPGYE = 0.;
+    if (c.baro) {  // :192-201 external density gradients (entry HP, HU, HV, SBX, SBY)
+      const DevBaro &Bc = S.baro;
+      const double *HP = X.h1p;
+      FPGXE = -X.sbx[d] * X.hu[d] * c.gp *
+              ((Bc.bi2[d] + Bc.bi2[q.w]) * (HP[d] - HP[q.w]) +
+               2.0 * X.hu[d] * (Bc.bi1[d] - Bc.bi1[q.w]) +
+               (Bc.be[d] + Bc.be[q.w]) * (S.belv[d] - S.belv[q.w]));
+      FPGYE = -X.sby[d] * X.hv[d] * c.gp *
+              ((Bc.bi2[d] + Bc.bi2[q.s]) * (HP[d] - HP[q.s]) +
+               2.0 * X.hv[d] * (Bc.bi1[d] - Bc.bi1[q.s]) +
+               (Bc.be[d] + Bc.be[q.s]) * (S.belv[d] - S.belv[q.s]));
+    }
+    X.fuhdye[d] = fuh_face(S, X, c, d, P, X.p[q.w], sub, FPGXE);
+    X.fvhdxe[d] = fvh_face(S, X, c, d, P, X.p[q.s], svb, FPGYE);
     if (c.isdry > 0) {  // :246-253
       X.sub[d] = S.subo[d];
       X.svb[d] = S.svbo[d];
@@ -980,7 +1027,22 @@ __global__ void k_gather(const CopyJob *jobs, int njob, const int *lidx, const i
 
 // ---------------------------------------------------------------------------
 // launch wrappers
+// dst[idx[i]] = val[i]: a member's values into tile order (set-up only).
+__global__ void k_put(const int *idx, const double *val, int n, double *dst) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    dst[idx[i]] = val[i];
+}
+void launch_put(cudaStream_t st, const int *idx, const double *val, int n, double *dst) {
+  if (n <= 0) return;
+  k_put<<<std::min((n + 255) / 256, 4096), 256, 0, st>>>(idx, val, n, dst);
+  count_launches(1);
+}
+
 void launch_begin(const Launch &l, const DevStatic &S, const DevState &X) {
+  if (l.baro) {
+    k_calebi<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+    count_launches(1);
+  }
   k_begin<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
   count_launches(1);
 }

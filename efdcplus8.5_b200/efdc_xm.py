@@ -52,7 +52,8 @@ class Params(C.Structure):
                 ("isdry", C.c_int32), ("ndrystp", C.c_int32), ("isbal", C.c_int32),
                 ("n", C.c_int32), ("ntstbc", C.c_int32), ("max_sweeps", C.c_int32),
                 ("precision", C.c_int32), ("mixed_rsq_factor", C.c_double),
-                ("qcherr", C.c_double), ("chan_consistent", C.c_int32), ("pad_", C.c_int32)]
+                ("qcherr", C.c_double), ("chan_consistent", C.c_int32), ("pad_", C.c_int32),
+                ("bsc", C.c_double), ("gp", C.c_double)]
 
 
 class Fields(C.Structure):
@@ -66,7 +67,11 @@ class Fields(C.Structure):
                 ("qdwaste", _pd), ("vdwaste", _pd), ("lwet", _pi), ("ldry", _pi),
                 ("ccc", _pd), ("ccs", _pd), ("ccw", _pd), ("cce", _pd), ("ccn", _pd),
                 ("fptmp", _pd), ("qchanu", _pd), ("qchanv", _pd), ("qchanun", _pd),
-                ("qchanvn", _pd)]
+                ("qchanvn", _pd), ("b", _pd), ("b_ld", C.c_int32), ("pad_b_", C.c_int32)]
+
+
+class Layers(C.Structure):
+    _fields_ = [("kc", C.c_int32), ("ld", C.c_int32), ("dzc", _pd), ("zz", _pd)]
 
 
 class Channels(C.Structure):
@@ -173,7 +178,21 @@ def make_params(p: dict, *, n: int, tn: float, precision: int = PREC_FP64):
     s.mixed_rsq_factor = p.get("mixed_rsq_factor", 0.0)
     s.qcherr = p.get("qcherr", 1.0)
     s.chan_consistent = int(p.get("chan_consistent", 0))
+    s.bsc = p.get("bsc", 0.0)
+    s.gp = p.get("gp", p["g"])
     return s
+
+
+def make_layers(ly: dict | None):
+    """A Layers struct over {"dzc", "zz"}: (KC, LCM) float64 arrays, layer K
+    at row K-1.  Returns (struct, kept arrays)."""
+    s = Layers()
+    if not ly:
+        return s, []
+    keep = [np.ascontiguousarray(ly[k], dtype=np.float64) for k in ("dzc", "zz")]
+    s.kc, s.ld = int(keep[0].shape[0]), int(keep[0].shape[1])
+    s.dzc, s.zz = _dp(keep[0]), _dp(keep[1])
+    return s, keep
 
 
 def make_channels(ch: dict | None):
@@ -221,6 +240,10 @@ def make_fields(st: dict, *, diag: bool = False, lists: bool = False):
             if k not in st:
                 st[k] = np.zeros(n)
             setattr(s, k, _dp(st[k]))
+    b = st.get("b")
+    if b is not None:  # B(L,K) as a (KC, LCM) array: layer K at row K-1
+        s.b = _dp(b)
+        s.b_ld = int(b.shape[-1])
     return s, keep
 
 
@@ -270,6 +293,8 @@ def load(path: str | os.PathLike | None = None):
     lib.efdc_xm_stream.restype = C.c_void_p
     lib.efdc_xm_stream.argtypes = [C.c_void_p]
     lib.efdc_xm_kernel_launches.restype = C.c_int64
+    lib.efdc_xm_set_layers.restype = C.c_int32
+    lib.efdc_xm_set_layers.argtypes = [C.c_void_p, C.c_int32, C.POINTER(Layers)]
     lib.efdc_xm_set_channels.restype = C.c_int32
     lib.efdc_xm_set_channels.argtypes = [C.c_void_p, C.c_int32, C.POINTER(Channels)]
     lib.efdc_xm_transfer_bytes.restype = None
@@ -373,6 +398,13 @@ class Solver:
 
     def stream(self) -> int:
         return int(self.lib.efdc_xm_stream(self.ctx) or 0)
+
+    def set_layers(self, ly: dict, member: int = 0):
+        s, _keep = make_layers(ly)
+        rc = self.lib.efdc_xm_set_layers(self.ctx, member, C.byref(s))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_set_layers: {STATUS_NAMES.get(rc, rc)}: "
+                               f"{self.last_error()}")
 
     def set_channels(self, ch: dict | None, member: int = 0):
         s, _keep = make_channels(ch)
@@ -498,6 +530,13 @@ class BatchSolver:
             self.close()
         except Exception:
             pass
+
+    def set_layers(self, ly: dict, member: int):
+        s, _keep = make_layers(ly)
+        rc = self.lib.efdc_xm_set_layers(self.ctx, member, C.byref(s))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_set_layers: {STATUS_NAMES.get(rc, rc)}: "
+                               f"{self.last_error()}")
 
     def set_channels(self, ch: dict | None, member: int):
         s, _keep = make_channels(ch)

@@ -11,9 +11,9 @@
 !     status code the library returns (congrad.f90:171-184,
 !     calpuv2c.f90:726-749, negdep.f90:47-167).
 ! Restrictions (the library returns EFDC_XM_UNSUPPORTED or this shim stops):
-! BSC<=1E-6, ISITB=0, ISVEG=0, ISGWIE=0, IGRIDV=0, no periodic (ISCONNECT)
-! links; sub-grid channels (MDCHH>=1) of MDCHTYP 1 and 2, whose cells are not
-! open-boundary cells.
+! ISITB=0, ISVEG=0, ISGWIE=0, IGRIDV=0 (the baroclinic terms of BSC>1E-6 on
+! the standard sigma grid), no periodic (ISCONNECT) links; sub-grid channels
+! (MDCHH>=1) of MDCHTYP 1 and 2, whose cells are not open-boundary cells.
 SUBROUTINE CALPUV2C
   USE GLOBAL
   USE EFDCOUT
@@ -26,13 +26,14 @@ SUBROUTINE CALPUV2C
   TYPE(EFDC_XM_FIELDS_T) :: FLD
   TYPE(EFDC_XM_STATS_T) :: ST
   TYPE(EFDC_XM_CHANNELS_T) :: CHN
+  TYPE(EFDC_XM_LAYERS_T) :: LYR
   REAL(C_DOUBLE), SAVE, ALLOCATABLE, TARGET :: PSERW(:), PSERE(:), PSERS(:), PSERN(:)
   INTEGER(C_INT32_T), SAVE, ALLOCATABLE, TARGET :: LMASKI(:), ISCDRYI(:), LOBCDRYI(:)
   INTEGER :: L, K, LL, ND, LF, LP, LN, IRC
   REAL(RKD), SAVE :: DAYOLD
 
-  IF( BSC > 1.E-6 .OR. ISITB > 0 .OR. ISVEG > 0 .OR. ISGWIE > 0 .OR. IGRIDV > 0 )THEN
-    STOP '*** CALPUV2C (GPU): BSC, ISITB, ISVEG, ISGWIE, IGRIDV options are not supported'
+  IF( ISITB > 0 .OR. ISVEG > 0 .OR. ISGWIE > 0 .OR. IGRIDV > 0 )THEN
+    STOP '*** CALPUV2C (GPU): ISITB, ISVEG, ISGWIE, IGRIDV options are not supported'
   ENDIF
 
   IF( .NOT. C_ASSOCIATED(CTX) )THEN
@@ -60,6 +61,17 @@ SUBROUTINE CALPUV2C
     IF( .NOT. C_ASSOCIATED(CTX) )THEN
       WRITE(6,'(A,A)') ' CALPUV2C (GPU): ', TRIM(EFDC_XM_ERRMSG())
       STOP '*** CALPUV2C (GPU): context creation failed'
+    ENDIF
+    IF( BSC > 1.E-6 )THEN
+      ! *** layers of the sigma grid for CALEBI (aaefdc.f90:1090-1237)
+      LYR%KC = KC
+      LYR%LD = LCM
+      LYR%DZC = C_LOC(DZC(1,1))
+      LYR%ZZ = C_LOC(ZZ(1,1))
+      IF( EFDC_XM_SET_LAYERS(CTX, 0_C_INT32_T, LYR) /= EFDC_XM_OK )THEN
+        WRITE(6,'(A,A)') ' CALPUV2C (GPU): ', TRIM(EFDC_XM_ERRMSG())
+        STOP '*** CALPUV2C (GPU): layers not accepted'
+      ENDIF
     ENDIF
     IF( MDCHH >= 1 )THEN
       ! *** sub-grid channels (input.f90:2563-2590, ainit.f90:286-316)
@@ -108,6 +120,8 @@ SUBROUTINE CALPUV2C
   PRM%QCHERR = QCHERR
   PRM%CHAN_CONSISTENT = 0     ! CONGRADC as the reference writes it
   PRM%PAD_ = 0
+  PRM%BSC = BSC
+  PRM%GP = GP
 
   ! *** time series part of the open-boundary targets (setopenbc.f90:41-46)
   DO LL=1,NPBW
@@ -171,6 +185,14 @@ SUBROUTINE CALPUV2C
   FLD%LWET = C_LOC(LWET(1));   FLD%LDRY = C_LOC(LDRY(1))
   FLD%CCC = C_NULL_PTR; FLD%CCS = C_NULL_PTR; FLD%CCW = C_NULL_PTR
   FLD%CCE = C_NULL_PTR; FLD%CCN = C_NULL_PTR; FLD%FPTMP = C_NULL_PTR
+  IF( BSC > 1.E-6 )THEN
+    FLD%B = C_LOC(B(1,1))
+    FLD%B_LD = LCM
+  ELSE
+    FLD%B = C_NULL_PTR
+    FLD%B_LD = 0
+  ENDIF
+  FLD%PAD_B_ = 0
   IF( MDCHH >= 1 )THEN
     FLD%QCHANU = C_LOC(QCHANU(1));   FLD%QCHANV = C_LOC(QCHANV(1))
     FLD%QCHANUN = C_LOC(QCHANUN(1)); FLD%QCHANVN = C_LOC(QCHANVN(1))

@@ -70,6 +70,7 @@ class Scenario:
     params: dict
     ijct: np.ndarray = field(repr=False, default=None)
     channels: dict = field(repr=False, default=None)  # sub-grid channels (add_channels)
+    layers: dict = field(repr=False, default=None)  # sigma layers (add_baroclinic)
 
     @property
     def ncell(self) -> int:
@@ -589,4 +590,31 @@ def add_channels(scn: Scenario, n: int = 6, *, seed: int = 0, types=(1, 2), qche
         scn.state[k] = np.zeros(n)
     scn.state["hp"][0] = hmin
     scn.params["qcherr"] = qcherr
+    return scn
+
+
+def add_baroclinic(scn: Scenario, kc: int = 4, *, seed: int = 0, front: float = 2e-3,
+                   strat: float = 5e-4, bsc: float = 1.0) -> Scenario:
+    """Baroclinic terms on a uniform sigma grid of `kc` layers: DZC = 1/KC and
+    ZZ = the layer mid-points (aaefdc.f90:1090, 1237), and a seeded buoyancy
+    B(L,K) (a horizontal front of amplitude `front` across the basin plus a
+    stable vertical stratification `strat` and small noise).  Adds the
+    layers as scn.layers ({"dzc", "zz"}: (KC, LCM)), B to the state
+    ((KC, LCM)), and BSC, GP = G to the parameters."""
+    rng = np.random.default_rng(seed)
+    lcm = scn.lc + 1
+    g = scn.grid
+    dzc = np.full((kc, lcm), 1.0 / kc)
+    zz = np.repeat(((np.arange(kc) + 0.5) / kc)[:, None], lcm, axis=1)
+    il = np.zeros(lcm)
+    il[1:scn.la] = g["il"][1:scn.la]
+    x = (il - il[1:scn.la].min()) / max(1.0, float(np.ptp(il[1:scn.la])))
+    b = np.zeros((kc, lcm))
+    for k in range(kc):
+        b[k, 1:scn.la] = (front * x[1:scn.la] - strat * (kc - 1 - k) / max(kc - 1, 1) +
+                          1e-5 * rng.standard_normal(scn.la - 1))
+    scn.layers = dict(dzc=dzc, zz=zz)
+    scn.state["b"] = b
+    scn.params["bsc"] = bsc
+    scn.params["gp"] = G
     return scn

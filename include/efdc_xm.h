@@ -114,6 +114,9 @@ typedef struct efdc_xm_params {
                         entry); the flows it gives can grow without bound.  1: the
                         conductance operator (A-C)P = b, i.e. A*p with -CCCCHH     */
   int32_t pad_;
+  double bsc;        /* BSC: the baroclinic terms FPGXE, FPGYE enter when > 1e-6
+                        (calpuv2c.f90:161, 192-211); needs efdc_xm_set_layers and B */
+  double gp;         /* GP (hdmt2t.f90:459-463)                                       */
 } efdc_xm_params;
 
 /* Per-call arrays.  "in/out" arrays are read and overwritten.  Optional outputs
@@ -149,6 +152,11 @@ typedef struct efdc_xm_fields {
    * channel is inactive, else left as they are).  Required where channels
    * are set, ignored elsewhere. */
   double *qchanu, *qchanv, *qchanun, *qchanvn;
+  /* buoyancy B(L,K), in, K = 1..KC of efdc_xm_set_layers, at b[(K-1)*b_ld + L-1]
+   * (a Fortran B(LCM,KCM) has b_ld = LCM).  Required where BSC > 1e-6. */
+  const double *b;
+  int32_t b_ld;
+  int32_t pad_b_;
 } efdc_xm_fields;
 
 typedef struct efdc_xm_stats {
@@ -216,6 +224,18 @@ int32_t efdc_xm_download(efdc_xm_ctx *ctx, efdc_xm_fields *f);
  * of a member with channels solves CONGRADC's system in place of CONGRAD's
  * (calpuv2c.f90:409-410) and needs the QCHANU..QCHANVN fields. */
 int32_t efdc_xm_set_channels(efdc_xm_ctx *ctx, int32_t member, const efdc_xm_channels *ch);
+
+/* Layer geometry of the standard sigma grid (IGRIDV = 0, KSZ = 1) for the
+ * external buoyancy integrals of CALEBI (calebi.f90:82-120): DZC(L,K) and
+ * ZZ(L,K), K = 1..kc, at [(K-1)*ld + L-1] (ld = LCM for Fortran arrays;
+ * ZZ from its layer 1, i.e. C_LOC(ZZ(1,1))).  kc is shared by the members
+ * of a batch (1..64). */
+typedef struct efdc_xm_layers {
+  int32_t kc;
+  int32_t ld;
+  const double *dzc, *zz;
+} efdc_xm_layers;
+int32_t efdc_xm_set_layers(efdc_xm_ctx *ctx, int32_t member, const efdc_xm_layers *ly);
 
 /* Standalone replacement of CONGRAD (congrad.f90:1-191) for callers that
  * assemble the scaled system themselves (e.g. calpuv9c.f90:446).  Arrays are

@@ -1,6 +1,6 @@
 // efdc_oracle.cpp -- TEST INFRASTRUCTURE ONLY: CPU FP64 restatement of EFDC+
-// 8.5 CALPUV2C / CONGRAD / CONGRADC / SUBCHAN / SETOPENBC / SETOPENBC2 /
-// NEGDEP (check part).
+// 8.5 CALPUV2C / CONGRAD / CONGRADC / SUBCHAN / CALEBI (standard sigma) /
+// SETOPENBC / SETOPENBC2 / NEGDEP (check part).
 // Parity against the reference is UNPINNED (no compiler, no reference tests);
 // see efdc_oracle.h.  Each block cites the Fortran it restates.
 //
@@ -63,6 +63,10 @@ struct oracle_ctx {
   std::vector<int> oldmask;
   Channels ch;
   std::vector<double> p1;  // P at entry (P1, calpuv2c.f90:259)
+  // CALEBI: layers (DZCC, ZZC of the first call, layer k at [k*(lc+2) + L])
+  // and the buoyancy integrals, kept between calls like the module arrays
+  int kc = 0;
+  std::vector<double> dzc, zz, bi1, bi2, be;
 };
 
 namespace {
@@ -459,7 +463,33 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
   const double HDRY = prm->hdry;
   const int ISDRY = prm->isdry, NDRYSTP = prm->ndrystp;
   const double RITB1 = prm->ritb1, SNLT = prm->snlt;
-  const double FPGXE = 0., FPGYE = 0.;  // BSC <= 1e-6: no baroclinic term
+  const bool baro = prm->bsc > 1.E-6;
+  if (baro && (c->kc < 1 || !f->b)) {
+    st->status = EFDC_XM_BAD_ARGUMENT;
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  if (baro) {  // :161 CALL CALEBI (calebi.f90:73-120, standard sigma, KSZ = 1)
+    const size_t ldb = size_t(f->b_ld), ldl = size_t(lc) + 2;
+    for (int L = 2; L <= la; ++L) {
+      if (ISDRY > 0 && !f->lmaskdry[L - 1]) continue;  // LWET of the last step
+      double DBK = 0., BEC = 0., BI1C = 0., BI2C = 0.;
+      for (int K = c->kc; K >= 1; --K) {
+        const double DZCC = c->dzc[size_t(K - 1) * ldl + L];
+        const double DZCB = DZCC * f->b[size_t(K - 1) * ldb + (L - 1)];
+        DBK = DBK + DZCB;  // :94-98
+        const double BK = DBK - 0.5 * DZCB;
+        BEC = BEC + DZCB;  // :100-108
+        const double DZCBK = DZCC * BK;
+        BI1C = BI1C + DZCBK;
+        BI2C = BI2C + DZCBK + c->zz[size_t(K - 1) * ldl + L] * DZCB;
+      }
+      c->bi1[L] = BI1C;  // BI1W = BI1S (:110-118)
+      c->bi2[L] = BI2C;
+      c->be[L] = BEC;
+    }
+  }
+  const double GP = prm->gp;
+  const double *BI1 = c->bi1.data(), *BI2 = c->bi2.data(), *BE = c->be.data();
   const int max_sweeps = prm->max_sweeps > 0 ? prm->max_sweeps : 500;
 
   int NCORDRY = 0;
@@ -494,6 +524,15 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
     }
     {  // :214-220 explicit external transports
       const int LS = LSC[L], LW = LWC[L];
+      double FPGXE = 0., FPGYE = 0.;
+      if (baro) {  // :192-201 external density gradients (IGRIDV = 0)
+        FPGXE = -SBX[L] * HU[L] * GP *
+                ((BI2[L] + BI2[LW]) * (HP[L] - HP[LW]) + 2.0 * HU[L] * (BI1[L] - BI1[LW]) +
+                 (BE[L] + BE[LW]) * (BELV[L] - BELV[LW]));
+        FPGYE = -SBY[L] * HV[L] * GP *
+                ((BI2[L] + BI2[LS]) * (HP[L] - HP[LS]) + 2.0 * HV[L] * (BI1[L] - BI1[LS]) +
+                 (BE[L] + BE[LS]) * (BELV[L] - BELV[LS]));
+      }
       FUHDYE[L] = UHDYE[L] - DELTD2 * SUB[L] * HRUO[L] * HU[L] * (P[L] - P[LW]) +
                   SUB[L] * DELT * DXIU[L] *
                       (DXYU[L] * (TSX[L] - RITB1 * TBX[L]) + FCAXE[L] + FPGXE -
@@ -1020,6 +1059,24 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
   if (f->fptmp) for (int L = 1; L <= lc; ++L) f->fptmp[L - 1] = FPTMP[L];
   st->status = status;
   return status;
+}
+
+int oracle_set_layers(oracle_ctx *c, const efdc_xm_layers *ly) {
+  if (!ly || ly->kc < 1 || ly->kc > 64 || ly->ld < c->lc || !ly->dzc || !ly->zz)
+    return EFDC_XM_BAD_ARGUMENT;
+  const size_t ldl = size_t(c->lc) + 2;
+  c->kc = ly->kc;
+  c->dzc.assign(ldl * ly->kc, 0.0);
+  c->zz.assign(ldl * ly->kc, 0.0);
+  for (int k = 0; k < ly->kc; ++k)
+    for (int L = 1; L <= c->lc; ++L) {
+      c->dzc[k * ldl + L] = ly->dzc[size_t(k) * ly->ld + (L - 1)];
+      c->zz[k * ldl + L] = ly->zz[size_t(k) * ly->ld + (L - 1)];
+    }
+  c->bi1.assign(ldl, 0.0);
+  c->bi2.assign(ldl, 0.0);
+  c->be.assign(ldl, 0.0);
+  return EFDC_XM_OK;
 }
 
 int oracle_set_channels(oracle_ctx *c, const efdc_xm_channels *in) {

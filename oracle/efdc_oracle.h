@@ -48,6 +48,9 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
  * removes them.  Returns 0, or EFDC_XM_BAD_ARGUMENT. */
 int oracle_set_channels(oracle_ctx *c, const efdc_xm_channels *ch);
 
+/* Layers of the standard sigma grid for CALEBI (efdc_xm_set_layers' contract). */
+int oracle_set_layers(oracle_ctx *c, const efdc_xm_layers *ly);
+
 int oracle_congrad(oracle_ctx *c, const double *ccc, const double *ccs,
                    const double *ccn, const double *ccw, const double *cce,
                    const double *ccci, const double *fptmp, double *p,

@@ -42,6 +42,8 @@ def load():
         lib.oracle_step.argtypes = [C.c_void_p, C.POINTER(X.Params), C.POINTER(X.Fields),
                                     C.POINTER(X.Stats)]
         pd = C.POINTER(C.c_double)
+        lib.oracle_set_layers.restype = C.c_int
+        lib.oracle_set_layers.argtypes = [C.c_void_p, C.POINTER(X.Layers)]
         lib.oracle_set_channels.restype = C.c_int
         lib.oracle_set_channels.argtypes = [C.c_void_p, C.POINTER(X.Channels)]
         lib.oracle_congrad.restype = C.c_int
@@ -78,6 +80,11 @@ class Oracle:
         st = X.Stats()
         self.lib.oracle_step(self.ctx, C.byref(params), C.byref(f), C.byref(st))
         return st
+
+    def set_layers(self, ly: dict):
+        s, _keep = X.make_layers(ly)
+        if self.lib.oracle_set_layers(self.ctx, C.byref(s)) != 0:
+            raise RuntimeError("oracle_set_layers: bad layer arrays")
 
     def set_channels(self, ch: dict | None):
         s, _keep = X.make_channels(ch)

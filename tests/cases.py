@@ -59,6 +59,19 @@ def channels(consistent=0, *, closed=False, qcherr=1.0, n=10, seed=21):
     return scn
 
 
+def baroclinic(wetdry=False, *, closed=False, kc=4):
+    """A basin with the baroclinic terms (BSC = 1, KC sigma layers, a seeded
+    buoyancy front).  wetdry=True: the ISDRY=99 tidal flat instead, so that
+    the buoyancy integrals skip the cells that were dry at the last step."""
+    if wetdry:
+        scn = S.tidal_flat(n=48, seed=13, dt=5.0)
+    else:
+        scn = S.make_scenario(60, 40, seed=31, obc_sides=() if closed else ("W",), amp=0.3,
+                              dt=10.0, explicit_noise=1e-4)
+    S.add_baroclinic(scn, kc, seed=2)
+    return scn
+
+
 def state_err(a, b, la, key="p", g=S.G):
     d = np.abs(a[key][1:la] - b[key][1:la])
     return float(d.max() / (g if key == "p" else 1.0))
