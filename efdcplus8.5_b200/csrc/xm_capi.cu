@@ -180,6 +180,11 @@ struct efdc_xm_ctx {
   std::vector<char> has_layers;  // [M]
   bool step_baro = false;
   std::vector<double> zeros_h;   // LC zeros: B of a member without it
+  // the device copies of LMASKDRY, ISCDRY, NATDRY, QDWASTE, VDWASTE (wd_stale)
+  // and of SBX, SBY (sbxy_stale) are out of date: the last efdc_xm_step_batch
+  // ran without wetting and drying (and without baroclinic terms) and did
+  // not upload them; the host holds them
+  bool wd_stale = false, sbxy_stale = false;
 
   template <class T>
   T *alloc(size_t n, bool zero = true) {
@@ -1021,7 +1026,20 @@ efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *g, int32_t device) {
   return efdc_xm_create_batch(g, 1, device);
 }
 
+namespace {
+int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool skip_sbxy);
+}
+
 int32_t efdc_xm_upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f) {
+  return upload_batch(c, f, false, false);
+}
+
+namespace {
+// skip_wetdry: leave out the fields that only wetting and drying reads
+// (LMASKDRY, ISCDRY, NATDRY, QDWASTE, VDWASTE), for a step in which no member
+// has it; skip_sbxy: SBX, SBY as well (read also by the baroclinic terms).
+// Their device copies are then marked out of date.
+int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool skip_sbxy) {
   if (!c || !f) {
     set_error("efdc_xm_upload: NULL argument");
     return EFDC_XM_BAD_ARGUMENT;
@@ -1045,11 +1063,17 @@ int32_t efdc_xm_upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f) {
   }
   XM_UP(p, X.p, 0) XM_UP(hp, X.hp, 0) XM_UP(hu, X.hu, 0) XM_UP(hv, X.hv, 0)
   XM_UP(uhdye, X.uhdye, 0) XM_UP(vhdxe, X.vhdxe, 0) XM_UP(sub, X.sub, 0) XM_UP(svb, X.svb, 0)
-  XM_UP(sbx, X.sbx, 0) XM_UP(sby, X.sby, 0) XM_UP(lmaskdry, X.lmaskdry, 1)
-  XM_UP(iscdry, X.iscdry, 2) XM_UP(lopenbcdry, X.lopenbcdry, 1) XM_UP(natdry, X.natdry, 2)
+  XM_UP(lopenbcdry, X.lopenbcdry, 1)
   XM_UP(fcaxe, X.fcaxe, 0) XM_UP(fcaye, X.fcaye, 0) XM_UP(fxe, X.fxe, 0) XM_UP(fye, X.fye, 0)
   XM_UP(tsx, X.tsx, 0) XM_UP(tsy, X.tsy, 0) XM_UP(tbx, X.tbx, 0) XM_UP(tby, X.tby, 0)
-  XM_UP(qsume, X.qsume, 0) XM_UP(qdwaste, X.qdwaste, 0) XM_UP(vdwaste, X.vdwaste, 0)
+  XM_UP(qsume, X.qsume, 0)
+  if (!skip_sbxy) {
+    XM_UP(sbx, X.sbx, 0) XM_UP(sby, X.sby, 0)
+  }
+  if (!skip_wetdry) {
+    XM_UP(lmaskdry, X.lmaskdry, 1) XM_UP(iscdry, X.iscdry, 2) XM_UP(natdry, X.natdry, 2)
+    XM_UP(qdwaste, X.qdwaste, 0) XM_UP(vdwaste, X.vdwaste, 0)
+  }
 #undef XM_UP
   // B(L,K), one staging job per layer; a member without B gets zeros
   bool anyb = false;
@@ -1102,10 +1126,15 @@ int32_t efdc_xm_upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f) {
                        cudaMemcpyHostToDevice, c->stream));
   }
   CK(cudaStreamSynchronize(c->stream));
-  for (int m = 0; m < M; ++m)
-    if (f[m].lmaskdry) c->mem[m].oldmask_h.assign(f[m].lmaskdry, f[m].lmaskdry + c->mem[m].lc);
+  c->wd_stale = skip_wetdry;
+  c->sbxy_stale = skip_sbxy;
+  if (!skip_wetdry)
+    for (int m = 0; m < M; ++m)
+      if (f[m].lmaskdry)
+        c->mem[m].oldmask_h.assign(f[m].lmaskdry, f[m].lmaskdry + c->mem[m].lc);
   return EFDC_XM_OK;
 }
+}  // namespace
 
 namespace {
 int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged);
@@ -1142,9 +1171,14 @@ int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged) {
   XM_DN(uhe, X.uhe, 0) XM_DN(vhe, X.vhe, 0) XM_DN(hpi, X.hpi, 0) XM_DN(hui, X.hui, 0)
   XM_DN(hvi, X.hvi, 0)
   if (!skip_unchanged) {
-    XM_DN(sub, X.sub, 0) XM_DN(svb, X.svb, 0) XM_DN(sbx, X.sbx, 0) XM_DN(sby, X.sby, 0)
-    XM_DN(lmaskdry, X.lmaskdry, 1) XM_DN(iscdry, X.iscdry, 2) XM_DN(natdry, X.natdry, 2)
-    XM_DN(qdwaste, X.qdwaste, 0) XM_DN(vdwaste, X.vdwaste, 0)
+    XM_DN(sub, X.sub, 0) XM_DN(svb, X.svb, 0)
+    if (!c->sbxy_stale) {  // else the host holds them (see sbxy_stale)
+      XM_DN(sbx, X.sbx, 0) XM_DN(sby, X.sby, 0)
+    }
+    if (!c->wd_stale) {
+      XM_DN(lmaskdry, X.lmaskdry, 1) XM_DN(iscdry, X.iscdry, 2) XM_DN(natdry, X.natdry, 2)
+      XM_DN(qdwaste, X.qdwaste, 0) XM_DN(vdwaste, X.vdwaste, 0)
+    }
   }
   XM_DN(ccc, Y.ccc, 0) XM_DN(ccs, Y.ccs, 0) XM_DN(ccw, Y.ccw, 0) XM_DN(cce, Y.cce, 0)
   XM_DN(ccn, Y.ccn, 0) XM_DN(fptmp, Y.fptmp, 0)
@@ -1236,6 +1270,15 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
   c->last_mixed = mixed;
   c->sys_external = false;
   c->step_baro = false;
+  for (int m = 0; m < M; ++m)
+    if ((prm[m].isdry > 0 && (c->wd_stale || c->sbxy_stale)) ||
+        (prm[m].bsc > 1.E-6 && c->sbxy_stale)) {
+      set_error("efdc_xm_step_device: member %d has ISDRY > 0 or BSC > 0, but fields it reads "
+                "(of SBX, SBY, LMASKDRY, ISCDRY, NATDRY, QDWASTE, VDWASTE) were last left on "
+                "the host by a step without them: upload them first", m);
+      fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
   for (int m = 0; m < M; ++m) {
     if (!(prm[m].bsc > 1.E-6)) continue;
     if (!c->has_layers[m]) {
@@ -1405,15 +1448,18 @@ int32_t efdc_xm_step_batch(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fi
       return EFDC_XM_BAD_ARGUMENT;
     }
   }
-  int rc = efdc_xm_upload_batch(c, f);
+  bool no_wetdry = true, no_baro = true;
+  for (int m = 0; m < M; ++m) {
+    no_wetdry &= prm[m].isdry == 0;
+    no_baro &= !(prm[m].bsc > 1.E-6);
+  }
+  int rc = upload_batch(c, f, no_wetdry, no_wetdry && no_baro);
   if (rc) {
     fill_status(stats, M, rc);
     return rc;
   }
   const int st = efdc_xm_step_device_batch(c, prm, stats);
   if (st == EFDC_XM_CUDA_ERROR || st == EFDC_XM_BAD_ARGUMENT) return st;
-  bool no_wetdry = true;
-  for (int m = 0; m < M; ++m) no_wetdry &= prm[m].isdry == 0;
   if ((rc = download_batch(c, f, no_wetdry))) {
     fill_status(stats, M, rc);
     return rc;

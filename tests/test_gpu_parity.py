@@ -247,3 +247,32 @@ def test_large_basin_mixed_vs_fp64():
         out[prec] = st
         sol.close()
     assert eta_err(out[X.PREC_MIXED], out[X.PREC_FP64], scn.la) <= 1e-6
+
+
+def test_wetdry_fields_left_on_host_by_dry_free_step():
+    """efdc_xm_step without wetting and drying neither uploads nor returns the
+    fields only wetting and drying reads; a device-resident ISDRY > 0 step is
+    then refused until they are uploaded, and gives the oracle's result after."""
+    scn, steps, tm = cases.build("tidal_flat_99")
+    st = scn.copy_state()
+    sol = X.Solver(scn.grid)
+    dry_free = X.make_params(dict(scn.params, isdry=0), n=1, tn=scn.tn(1) * tm)
+    before = {k: st[k].copy() for k in ("sbx", "sby", "lmaskdry", "iscdry", "natdry")}
+    assert sol.step(dry_free, st).status in (X.OK, X.NEG_DEPTH)
+    for k, v in before.items():  # untouched on the host
+        assert np.array_equal(st[k], v), k
+    prm = X.make_params(scn.params, n=2, tn=scn.tn(2) * tm)
+    with pytest.raises(RuntimeError, match="upload them first"):
+        sol.step_device(prm)
+    sol.upload(st)
+    a = sol.step_device(prm)
+    so = {k: (v.copy() if isinstance(v, np.ndarray) else
+              {s: x.copy() for s, x in v.items()} if isinstance(v, dict) else v)
+          for k, v in st.items()}
+    b = O.Oracle(scn.grid).step(X.make_params(scn.params, n=2, tn=scn.tn(2) * tm), so)
+    assert a.iters_total == b.iters_total
+    out = {k: np.zeros_like(st[k]) for k in ("p", "lmaskdry")}
+    sol.download(out)
+    assert float(np.abs(out["p"][1:scn.la] - so["p"][1:scn.la]).max()) / S.G < 1e-9
+    assert np.array_equal(out["lmaskdry"][1:scn.la], so["lmaskdry"][1:scn.la])
+    sol.close()
