@@ -298,6 +298,22 @@ int download_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
     c->jobs_h[j] = CopyJob{c->stage[j % NSTAGE], xs[j].dev, xs[j].kind};
   CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, xs.size() * sizeof(CopyJob), cudaMemcpyHostToDevice,
                      c->stream));
+  // Members whose host arrays lie back to back at the staging stride go back
+  // in one copy of the whole run; that copy also covers each member's ghost
+  // elements (L = 1 and LC) and the element between two members, which must
+  // stay as the caller has them: their host values are kept here and written
+  // back once the copies are done (the caller waits inside this call).
+  struct Keep {
+    char *at;
+    char val[8];
+    size_t n;
+  };
+  std::vector<Keep> keep;
+  auto save = [&](char *at, size_t es) {
+    Keep k{at, {}, es};
+    std::memcpy(k.val, at, es);
+    keep.push_back(k);
+  };
   int rc = 0, k = 0;
   for (size_t g0 = 0; g0 < xs.size(); g0 += NSTAGE) {
     const size_t g1 = std::min(xs.size(), g0 + NSTAGE);
@@ -306,22 +322,40 @@ int download_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
                       c->nslot);
     CK(cudaGetLastError());
     if ((rc = copies_after_compute(c))) return rc;
-    // the gather fills elements L=2..LA (indices 1..LA-1) of each member; only
-    // that range goes back, so the caller's ghost elements 1 and LC stay as they are
     for (size_t j = g0; j < g1; ++j) {
       const size_t es = esize(xs[j].kind);
       const char *src = reinterpret_cast<const char *>(c->stage[j % NSTAGE]);
-      for (int m = 0; m < c->M; ++m) {
-        const size_t n = es * size_t(c->mem[m].la - 1);
-        CK(cudaMemcpyAsync(static_cast<char *>(const_cast<void *>(xs[j].host[m])) + es,
-                           src + (c->mem[m].off + 1) * es, n, cudaMemcpyDeviceToHost,
-                           c->copy_stream[k++ % NCOPY]));
-        g_d2h.fetch_add(static_cast<long long>(n), std::memory_order_relaxed);
+      for (int m = 0; m < c->M;) {
+        char *h0 = static_cast<char *>(const_cast<void *>(xs[j].host[m]));
+        int e = m + 1;
+        while (e < c->M && static_cast<const char *>(xs[j].host[e]) ==
+                               static_cast<const char *>(xs[j].host[e - 1]) +
+                                   size_t(c->mem[e - 1].lc + 1) * es)
+          ++e;
+        if (e == m + 1) {  // one member: its water elements L = 2..LA only
+          const size_t n = es * size_t(c->mem[m].la - 1);
+          CK(cudaMemcpyAsync(h0 + es, src + (c->mem[m].off + 1) * es, n, cudaMemcpyDeviceToHost,
+                             c->copy_stream[k++ % NCOPY]));
+          g_d2h.fetch_add(static_cast<long long>(n), std::memory_order_relaxed);
+        } else {
+          for (int q = m; q < e; ++q) {
+            char *hq = static_cast<char *>(const_cast<void *>(xs[j].host[q]));
+            save(hq, es);                                        // L = 1
+            save(hq + size_t(c->mem[q].lc - 1) * es, es);        // L = LC
+            if (q + 1 < e) save(hq + size_t(c->mem[q].lc) * es, es);  // between members
+          }
+          const size_t n = es * size_t(c->mem[e - 1].off - c->mem[m].off + c->mem[e - 1].lc);
+          CK(cudaMemcpyAsync(h0, src + c->mem[m].off * es, n, cudaMemcpyDeviceToHost,
+                             c->copy_stream[k++ % NCOPY]));
+          g_d2h.fetch_add(static_cast<long long>(n), std::memory_order_relaxed);
+        }
+        m = e;
       }
     }
   }
   for (cudaStream_t s : c->copy_stream) CK(cudaStreamSynchronize(s));
   CK(cudaStreamSynchronize(c->stream));
+  for (const Keep &kp : keep) std::memcpy(kp.at, kp.val, kp.n);
   return EFDC_XM_OK;
 }
 

@@ -172,12 +172,20 @@ def test_field_major_host_layout(precision):
     bf = X.BatchSolver([scn.grid for scn, _, _ in ms])
     sa = [scn.copy_state() for scn, _, _ in ms]
     sf = field_major([scn.copy_state() for scn, _, _ in ms])
+    def edges(st, scn):  # L = 1, L = LC and the element after LC
+        return {k: (st[k][0], st[k][scn.lc - 1], st[k][-1]) for k in STATE_F + MASK_F
+                if k in st and isinstance(st[k], np.ndarray)}
     for n in range(1, 4):
         prm = params_at(ms, n, precision)
+        before = [edges(sf[m], scn) for m, (scn, _, _) in enumerate(ms)]
         sta = ba.step(prm, sa)
         stf = bf.step(prm, sf)
         for m, (scn, _, _) in enumerate(ms):
             assert sta[m].iters_total == stf[m].iters_total, (m, n)
             assert_same(sa[m], sf[m], scn.la, f"member {m} step {n}")
+            # whole-run copies leave the caller's ghost and padding elements alone
+            after = edges(sf[m], scn)
+            for k, v in before[m].items():
+                assert np.array_equal(np.array(v), np.array(after[k])), (m, n, k)
     ba.close()
     bf.close()
