@@ -113,6 +113,9 @@ __device__ __forceinline__ double assemble_cell(const DevStatic &S, const DevSta
 // calpuv2c.f90:164-293: switches, explicit transports, FP1.  The host swapped
 // UHDYE<->UHDY1E, VHDXE<->VHDX1E and HP<->H1P before this kernel, so the *1
 // buffers hold the values at entry (the time-level advance :256-264).
+// BARO: a member of the batch has baroclinic terms; the instance without them
+// keeps the register count (and so the grid of every cell kernel) low.
+template <bool BARO>
 __global__ void __launch_bounds__(NT) k_begin(DevStatic S, DevState X, int ntile) {
   TILE_LOOP(ntile) {
     TILE_MEMBER(S);
@@ -130,7 +133,7 @@ __global__ void __launch_bounds__(NT) k_begin(DevStatic S, DevState X, int ntile
     }
     const double P = X.p[d];
     double FPGXE = 0., FPGYE = 0.;
-    if (c.baro) {  // :192-201 external density gradients (entry HP, HU, HV, SBX, SBY)
+    if (BARO && c.baro) {  // :192-201 external density gradients (entry HP, HU, HV, SBX, SBY)
       const DevBaro &Bc = S.baro;
       const double *HP = X.h1p;
       FPGXE = -X.sbx[d] * X.hu[d] * c.gp *
@@ -1043,7 +1046,10 @@ void launch_begin(const Launch &l, const DevStatic &S, const DevState &X) {
     k_calebi<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
     count_launches(1);
   }
-  k_begin<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+  if (l.baro)
+    k_begin<true><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+  else
+    k_begin<false><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
   count_launches(1);
 }
 void launch_sweep_reset(const Launch &l, Ctl *ctl, const int *act, int nmember) {
@@ -1243,7 +1249,7 @@ void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y,
 int occupancy_blocks_per_sm() {
   int a = 0, b = 0, c = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_assemble, NT, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_begin, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_begin<false>, NT, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_fin, NT, 0);
   const int m = std::min(a, std::min(b, c));
   return m > 0 ? m : 1;
