@@ -185,6 +185,10 @@ struct efdc_xm_ctx {
   // ran without wetting and drying (and without baroclinic terms) and did
   // not upload them; the host holds them
   bool wd_stale = false, sbxy_stale = false;
+  // three time levels (CALPUV9C): their buffers are allocated by the first
+  // upload that carries them (tl3_alloc); tl3_ready: the device holds a
+  // consistent set of levels (uploaded, or advanced by CALPUV9C steps)
+  bool tl3_alloc = false, tl3_ready = false;
 
   template <class T>
   T *alloc(size_t n, bool zero = true) {
@@ -570,6 +574,10 @@ xm::StepScalars make_scalars(const Member &mb, const efdc_xm_params *p) {
   s.baro = p->bsc > 1.E-6 ? 1 : 0;  // calpuv2c.f90:161, 192
   s.gp = p->gp;
   s.chan_consistent = p->chan_consistent != 0 ? 1 : 0;
+  s.istl = p->tl3_istl;
+  s.nctbc = p->nctbc;
+  s.rold = p->rold;
+  s.rnew = p->rnew;
   // setopenbc.f90:24-29 on the host, libm as the reference
   for (int m = 0; m < mb.mtide && m < xm::MT_MAX; ++m) {
     double TM = std::fmod(p->tn, mb.tcp[m]);
@@ -947,6 +955,8 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   X.uhdy1e = D(); X.vhdx1e = D(); X.sub1 = D(); X.svb1 = D(); X.fp1 = D(); X.fuhdye = D();
   X.fvhdxe = D(); X.fp = D(); X.cc = D(); X.cs = D(); X.cw = D(); X.ce = D(); X.cn = D();
   X.wd_act = I(); X.sub_n = D(); X.svb_n = D(); X.sbx_n = D(); X.sby_n = D(); X.wasted = I();
+  // the views of a CALPUV2C step (reset by every step after its swaps)
+  X.huc = X.hu; X.hvc = X.hv; X.hb = X.h1p; X.ub = X.uhdy1e; X.vb = X.vhdx1e; X.hp0 = X.h1p;
   xm::DevSystem &Y = c->Y;
   Y.ccc = D(); Y.ccs = D(); Y.ccw = D(); Y.cce = D(); Y.ccn = D(); Y.fptmp = D();
   Y.r = D(); Y.pa = D(); Y.pb = D(); Y.ap = D();
@@ -1061,19 +1071,57 @@ efdc_xm_ctx *efdc_xm_create(const efdc_xm_grid *g, int32_t device) {
 }
 
 namespace {
-int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool skip_sbxy);
+int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool skip_sbxy,
+                 bool levels);
 }
 
 int32_t efdc_xm_upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f) {
-  return upload_batch(c, f, false, false);
+  return upload_batch(c, f, false, false, f && f[0].p1);
 }
+
+namespace {
+// The buffers of the three time levels, on first use.
+int ensure_levels(efdc_xm_ctx *c) {
+  if (c->tl3_alloc) return EFDC_XM_OK;
+  xm::DevState &X = c->X;
+  double *b[14];
+  for (double *&p : b) {
+    p = c->alloc<double>(size_t(c->nslot));  // zeroed: HUTMP, HVTMP stay 0 on land slots
+    if (!p) {
+      set_error("cudaMalloc failed (device memory for the three time levels)");
+      return EFDC_XM_CUDA_ERROR;
+    }
+  }
+  X.p1 = b[0]; X.h2p = b[1]; X.uhdy2e = b[2]; X.vhdx2e = b[3]; X.h1u = b[4]; X.h1v = b[5];
+  X.hutmp = b[6]; X.hvtmp = b[7]; X.fpgxe = b[8]; X.fpgye = b[9];
+  X.tsx1 = b[10]; X.tsy1 = b[11]; X.tbx1 = b[12]; X.tby1 = b[13];
+  CK(cudaDeviceSynchronize());  // the zeroing ran on the legacy stream
+  c->tl3_alloc = true;
+  return EFDC_XM_OK;
+}
+
+// The views of the step about to run (DevState::huc ... hp0), after its
+// time-level swaps.
+void set_views(efdc_xm_ctx *c, int istl) {
+  xm::DevState &X = c->X;
+  const bool corr = istl == 2, leap = istl == 3;
+  X.huc = corr ? X.hutmp : X.hu;
+  X.hvc = corr ? X.hvtmp : X.hv;
+  X.hb = leap ? X.h2p : X.h1p;
+  X.ub = leap ? X.uhdy2e : X.uhdy1e;
+  X.vb = leap ? X.vhdx2e : X.vhdx1e;
+  X.hp0 = corr ? X.hp : X.h1p;
+}
+}  // namespace
 
 namespace {
 // skip_wetdry: leave out the fields that only wetting and drying reads
 // (LMASKDRY, ISCDRY, NATDRY, QDWASTE, VDWASTE), for a step in which no member
 // has it; skip_sbxy: SBX, SBY as well (read also by the baroclinic terms).
-// Their device copies are then marked out of date.
-int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool skip_sbxy) {
+// Their device copies are then marked out of date.  levels: upload the three
+// time levels of CALPUV9C (P1, H2P, H1P, UHDY1E ... FPGYE) as well.
+int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool skip_sbxy,
+                 bool levels) {
   if (!c || !f) {
     set_error("efdc_xm_upload: NULL argument");
     return EFDC_XM_BAD_ARGUMENT;
@@ -1108,6 +1156,24 @@ int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool
     XM_UP(lmaskdry, X.lmaskdry, 1) XM_UP(iscdry, X.iscdry, 2) XM_UP(natdry, X.natdry, 2)
     XM_UP(qdwaste, X.qdwaste, 0) XM_UP(vdwaste, X.vdwaste, 0)
   }
+  if (levels) {
+    for (int m = 0; m < M; ++m) {
+      const efdc_xm_fields &x = f[m];
+      if (!x.p1 || !x.h2p || !x.h1p || !x.uhdy1e || !x.vhdx1e || !x.uhdy2e || !x.vhdx2e ||
+          !x.h1u || !x.h1v) {
+        set_error("member %d: the three time levels need P1, H2P, H1P, UHDY1E, VHDX1E, UHDY2E, "
+                  "VHDX2E, H1U and H1V", m);
+        return EFDC_XM_BAD_ARGUMENT;
+      }
+    }
+    if ((rc = ensure_levels(c))) return rc;
+    XM_UP(p1, X.p1, 0) XM_UP(h2p, X.h2p, 0) XM_UP(h1p, X.h1p, 0)
+    XM_UP(uhdy1e, X.uhdy1e, 0) XM_UP(vhdx1e, X.vhdx1e, 0)
+    XM_UP(uhdy2e, X.uhdy2e, 0) XM_UP(vhdx2e, X.vhdx2e, 0)
+    XM_UP(h1u, X.h1u, 0) XM_UP(h1v, X.h1v, 0)
+    XM_UP(tsx1, X.tsx1, 0) XM_UP(tsy1, X.tsy1, 0) XM_UP(tbx1, X.tbx1, 0) XM_UP(tby1, X.tby1, 0)
+    XM_UP(fpgxe, X.fpgxe, 0) XM_UP(fpgye, X.fpgye, 0)
+  }
 #undef XM_UP
   // B(L,K), one staging job per layer; a member without B gets zeros
   bool anyb = false;
@@ -1127,13 +1193,15 @@ int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool
     }
   }
   if ((rc = upload_arrays(c, xs))) return rc;
-  // the second buffer of each time-level pair starts as a copy (its land
-  // slots must hold the ghost values too); the H1P input is not used because
-  // a step begins with H1P = HP (calpuv2c.f90:264)
+  // two time levels: the second buffer of each time-level pair starts as a
+  // copy (its land slots must hold the ghost values too); the H1P input is
+  // not used because a CALPUV2C step begins with H1P = HP (calpuv2c.f90:264)
   const size_t nb = size_t(c->nslot) * sizeof(double);
-  if (f[0].uhdye) CK(cudaMemcpyAsync(X.uhdy1e, X.uhdye, nb, cudaMemcpyDeviceToDevice, c->stream));
-  if (f[0].vhdxe) CK(cudaMemcpyAsync(X.vhdx1e, X.vhdxe, nb, cudaMemcpyDeviceToDevice, c->stream));
-  if (f[0].hp) CK(cudaMemcpyAsync(X.h1p, X.hp, nb, cudaMemcpyDeviceToDevice, c->stream));
+  if (!levels) {
+    if (f[0].uhdye) CK(cudaMemcpyAsync(X.uhdy1e, X.uhdye, nb, cudaMemcpyDeviceToDevice, c->stream));
+    if (f[0].vhdxe) CK(cudaMemcpyAsync(X.vhdx1e, X.vhdxe, nb, cudaMemcpyDeviceToDevice, c->stream));
+    if (f[0].hp) CK(cudaMemcpyAsync(X.h1p, X.hp, nb, cudaMemcpyDeviceToDevice, c->stream));
+  }
   if (c->nobc > 0) {
     for (int m = 0; m < M; ++m) {
       int k = c->mem[m].b0;
@@ -1162,6 +1230,7 @@ int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool
   CK(cudaStreamSynchronize(c->stream));
   c->wd_stale = skip_wetdry;
   c->sbxy_stale = skip_sbxy;
+  c->tl3_ready = levels;
   if (!skip_wetdry)
     for (int m = 0; m < M; ++m)
       if (f[m].lmaskdry)
@@ -1171,19 +1240,21 @@ int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool
 }  // namespace
 
 namespace {
-int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged);
+int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int levels);
 }
 
 int32_t efdc_xm_download_batch(efdc_xm_ctx *c, efdc_xm_fields *f) {
-  return download_batch(c, f, false);
+  return download_batch(c, f, false, c && c->tl3_ready ? 3 : 0);
 }
 
 namespace {
 // skip_unchanged: leave out the fields that a step with ISDRY = 0 in every
 // member does not write (the face switches SUB, SVB, SBX, SBY, LMASKDRY,
 // ISCDRY, NATDRY, QDWASTE, VDWASTE): within efdc_xm_step_batch their device
-// values are the host values uploaded by the same call.
-int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged) {
+// values are the host values uploaded by the same call.  levels: the three
+// time levels to return (0 none; 2 FPGXE, FPGYE, which a CALPUV9C(2) step
+// changes; 3 all of them, after CALPUV9C(3)).
+int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int levels) {
   if (!c || !f) {
     set_error("efdc_xm_download: NULL argument");
     return EFDC_XM_BAD_ARGUMENT;
@@ -1216,6 +1287,14 @@ int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged) {
   }
   XM_DN(ccc, Y.ccc, 0) XM_DN(ccs, Y.ccs, 0) XM_DN(ccw, Y.ccw, 0) XM_DN(cce, Y.cce, 0)
   XM_DN(ccn, Y.ccn, 0) XM_DN(fptmp, Y.fptmp, 0)
+  if (levels && c->tl3_alloc) {
+    XM_DN(fpgxe, X.fpgxe, 0) XM_DN(fpgye, X.fpgye, 0)
+    if (levels == 3) {
+      XM_DN(p1, X.p1, 0) XM_DN(h2p, X.h2p, 0) XM_DN(uhdy1e, X.uhdy1e, 0)
+      XM_DN(vhdx1e, X.vhdx1e, 0) XM_DN(uhdy2e, X.uhdy2e, 0) XM_DN(vhdx2e, X.vhdx2e, 0)
+      XM_DN(h1u, X.h1u, 0) XM_DN(h1v, X.h1v, 0)
+    }
+  }
 #undef XM_DN
   if (c->last_mixed && (f[0].ccc || f[0].ccs || f[0].ccw || f[0].cce || f[0].ccn || f[0].fptmp)) {
     // a MIXED step solves from the unscaled assembly: the scaled system
@@ -1298,6 +1377,21 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
       return EFDC_XM_BAD_ARGUMENT;
     }
   }
+  const int istl = prm[0].tl3_istl;  // 0: CALPUV2C; 3, 2: CALPUV9C(ISTL_)
+  for (int m = 0; m < M; ++m)
+    if (prm[m].tl3_istl != istl || (istl != 0 && istl != 2 && istl != 3)) {
+      set_error("efdc_xm_step_device: member %d: tl3_istl %d: need 0, 2 or 3, the same for "
+                "every member of a batch", m, prm[m].tl3_istl);
+      fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+  if (istl != 0 && (!c->tl3_ready || c->calib)) {
+    set_error(c->calib ? "efdc_xm_step_device: the calibration covers CALPUV2C only"
+                       : "efdc_xm_step_device: CALPUV9C needs the three time levels on the "
+                         "device: upload them (P1, H2P, H1P, UHDY1E, ..., H1V) first");
+    fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
+    return EFDC_XM_BAD_ARGUMENT;
+  }
   CK(cudaSetDevice(c->device));
   const bool mixed = prm[0].precision == EFDC_XM_PREC_MIXED;
   c->mxview = xm::SysView{c->X.fp, c->X.cc, c->X.cs, c->X.cw, c->X.ce, c->X.cn, 1};
@@ -1344,14 +1438,34 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
   CK(cudaMemsetAsync(c->ctl, 0, sizeof(Ctl) * M, c->stream));  // counters of this step
   int rc = write_act(c);
   if (rc) return rc;
-  // time levels by buffer swap: after it the *1 buffers hold the entry values
-  // (UHDY1E=UHDYE, VHDX1E=VHDXE, H1P=HP, calpuv2c.f90:256-264) and the
-  // others are rewritten for every water cell before they are read
-  std::swap(c->X.uhdye, c->X.uhdy1e);
-  std::swap(c->X.vhdxe, c->X.vhdx1e);
-  std::swap(c->X.hp, c->X.h1p);
-  xm::launch_chan_entry(l, c->S, c->X);
-  xm::launch_begin(l, c->S, c->X);
+  if (istl == 0) {
+    // time levels by buffer swap: after it the *1 buffers hold the entry values
+    // (UHDY1E=UHDYE, VHDX1E=VHDXE, H1P=HP, calpuv2c.f90:256-264) and the
+    // others are rewritten for every water cell before they are read
+    std::swap(c->X.uhdye, c->X.uhdy1e);
+    std::swap(c->X.vhdxe, c->X.vhdx1e);
+    std::swap(c->X.hp, c->X.h1p);
+    set_views(c, 0);
+    xm::launch_chan_entry(l, c->S, c->X);
+    xm::launch_begin(l, c->S, c->X);
+  } else {
+    xm::launch_chan_entry(l, c->S, c->X);
+    xm::launch_begin3(l, c->S, c->X);
+    if (istl == 3) {
+      // calpuv9c.f90:282-311 by buffer rotation, UHDY2E <- UHDY1E <- UHDYE and
+      // H2P <- H1P <- HP (UHDYE and HP are rewritten for every water cell
+      // before they are read), and the copies P1 = P, H1U = HU, H1V = HV
+      xm::DevState &X = c->X;
+      double *t = X.uhdy2e;
+      X.uhdy2e = X.uhdy1e; X.uhdy1e = X.uhdye; X.uhdye = t;
+      t = X.vhdx2e;
+      X.vhdx2e = X.vhdx1e; X.vhdx1e = X.vhdxe; X.vhdxe = t;
+      t = X.h2p;
+      X.h2p = X.h1p; X.h1p = X.hp; X.hp = t;
+      xm::launch_advance3(l, c->S, c->X);
+    }
+    set_views(c, istl);
+  }
   if (any_isdry) xm::launch_obc_reset(l, c->S, c->B, c->X);
   CK(cudaGetLastError());
   for (int sweep = 0;; ++sweep) {  // 1000 CONTINUE, for the members still sweeping
@@ -1440,6 +1554,7 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
     CK(cudaGetLastError());
   }
   if ((rc = read_ctl(c))) return rc;
+  if (istl == 0) c->tl3_ready = false;  // CALPUV2C does not keep the three levels
   for (int m = 0; m < M; ++m) {
     efdc_xm_stats &s = stats[m];
     const Ctl &k = c->ctl_h[m];
@@ -1481,20 +1596,26 @@ int32_t efdc_xm_step_batch(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fi
       fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
       return EFDC_XM_BAD_ARGUMENT;
     }
+    if (prm[m].tl3_istl != 0 && prm[m].bsc > 1.E-6 && (!x.fpgxe || !x.fpgye)) {
+      set_error("efdc_xm_step: member %d: CALPUV9C with BSC > 1E-6 needs FPGXE and FPGYE", m);
+      fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
   }
+  const int istl = prm[0].tl3_istl;
   bool no_wetdry = true, no_baro = true;
   for (int m = 0; m < M; ++m) {
     no_wetdry &= prm[m].isdry == 0;
     no_baro &= !(prm[m].bsc > 1.E-6);
   }
-  int rc = upload_batch(c, f, no_wetdry, no_wetdry && no_baro);
+  int rc = upload_batch(c, f, no_wetdry, no_wetdry && no_baro, istl != 0);
   if (rc) {
     fill_status(stats, M, rc);
     return rc;
   }
   const int st = efdc_xm_step_device_batch(c, prm, stats);
   if (st == EFDC_XM_CUDA_ERROR || st == EFDC_XM_BAD_ARGUMENT) return st;
-  if ((rc = download_batch(c, f, no_wetdry))) {
+  if ((rc = download_batch(c, f, no_wetdry, istl))) {
     fill_status(stats, M, rc);
     return rc;
   }

@@ -29,15 +29,29 @@ namespace xm {
 
 constexpr int CH_NT = 128;  // threads per CTA of the member kernels
 
-// calpuv2c.f90:139-145 (QCHANUT = QCHANU) and :259 (P1 = P) at the channels
+// calpuv2c.f90:139-145 (QCHANUT = QCHANU) and :259 (P1 = P) at the channels.
+// CALPUV9C (calpuv9c.f90:128-141): QCHANUT = QCHANUN, and for ISTL_ = 3
+// QCHANUN = QCHANU; its P1 is P at entry after the advance of ISTL_ = 3, the
+// caller's P1 for ISTL_ = 2.
 __global__ void k_chan_entry(DevStatic S, DevState X) {
   const DevChan &C = S.ch;
   MEMBER_LOOP {
+    const int istl = S.sc[m].istl;
+    const double *P1 = istl == 2 ? X.p1 : X.p;
     for (int k = C.cstart[m]; k < C.cstart[m + 1]; ++k) {
-      C.qut[k] = C.qu[k];
-      C.qvt[k] = C.qv[k];
-      C.p1h[k] = X.p[C.host[k]];
-      C.p1g[k] = X.p[C.guest[k]];
+      if (istl == 0) {
+        C.qut[k] = C.qu[k];
+        C.qvt[k] = C.qv[k];
+      } else {
+        C.qut[k] = C.qun[k];
+        C.qvt[k] = C.qvn[k];
+        if (istl == 3) {
+          C.qun[k] = C.qu[k];
+          C.qvn[k] = C.qv[k];
+        }
+      }
+      C.p1h[k] = P1[C.host[k]];
+      C.p1g[k] = P1[C.guest[k]];
     }
   }
 }
@@ -46,7 +60,7 @@ __global__ void k_chan_entry(DevStatic S, DevState X) {
 // CCCCHU, CCCCHV, CCCCHH and their entries in CC and FP of the host and guest
 // cells (after SETOPENBC, calpuv2c.f90:349-356); then the final CC of the
 // channels' cells into the member's minimum diagonal.  In the first sweep HP
-// is still the entry value (held in the H1P buffer).
+// is still the entry value (the view hp0).
 __global__ void k_chan_sub(DevStatic S, DevState X, Ctl *ctl, const int *act, int first_sweep) {
   const DevChan &C = S.ch;
   MEMBER_LOOP {
@@ -56,7 +70,7 @@ __global__ void k_chan_sub(DevStatic S, DevState X, Ctl *ctl, const int *act, in
     const double G = c.g, DE_T = c.delt, HDRY = c.hdry, RLAMN = c.rlamn;
     const double RLAMO = 1. - RLAMN;
     const double *H1P = X.h1p;
-    const double *HP = first_sweep ? X.h1p : X.hp;
+    const double *HP = first_sweep ? X.hp0 : X.hp;
     for (int k = k0; k < k1; ++k) {
       const int lh = C.host[k], lg = C.guest[k];
       double cu = 0.0, cv = 0.0;

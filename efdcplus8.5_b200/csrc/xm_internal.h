@@ -44,6 +44,9 @@ struct StepScalars {
   int chan_consistent;  // channels: 1 = A*p with -CCCCHH (else as congradc.f90 writes it)
   int baro;             // BSC > 1e-6: the baroclinic terms FPGXE, FPGYE enter
   double gp;            // GP
+  int istl;             // 0: CALPUV2C; 3 or 2: CALPUV9C(ISTL_) (the same for every member)
+  int nctbc;            // NCTBC (CALPUV9C, ISTL_ = 3: 1 halves UHDYE, VHDXE on advancing)
+  double rold, rnew;    // ROLD, RNEW: blend of FPGXE, FPGYE (CALPUV9C)
   double cosv[MT_MAX], sinv[MT_MAX];
 };
 
@@ -136,6 +139,19 @@ struct DevState {
   int *wd_act;
   double *sub_n, *svb_n, *sbx_n, *sby_n;
   int *wasted;  // 1 where NDRYSTP volume wasting fired this step
+  // three time levels (CALPUV9C), allocated on first use: P1, H2P, UHDY2E,
+  // VHDX2E, H1U, H1V, HUTMP, HVTMP, FPGXE, FPGYE and the level n-1 stresses
+  double *p1, *h2p, *uhdy2e, *vhdx2e, *h1u, *h1v, *hutmp, *hvtmp, *fpgxe, *fpgye;
+  const double *tsx1, *tsy1, *tbx1, *tby1;
+  // views of the step being taken, set by the host before its first kernel:
+  // huc, hvc: the face depths of the coefficients (HU, HV; HUTMP, HVTMP in
+  //   CALPUV9C(2));
+  // hb, ub, vb: the level the continuity starts from and its transports
+  //   (H1P, UHDY1E, VHDX1E; H2P, UHDY2E, VHDX2E in CALPUV9C(3)); hb is also
+  //   HPPMC of the drying checks;
+  // hp0: HP at entry (the H1P buffer after the time-level advance; HP in
+  //   CALPUV9C(2), which does not advance).
+  const double *huc, *hvc, *hb, *ub, *vb, *hp0;
 };
 
 // Scaled system and CG vectors.

@@ -33,6 +33,9 @@ struct CopyJob {
 };
 
 void launch_begin(const Launch &l, const DevStatic &S, const DevState &X);
+// CALPUV9C: the kernels up to the time-level advance, and the copies of the advance
+void launch_begin3(const Launch &l, const DevStatic &S, const DevState &X);
+void launch_advance3(const Launch &l, const DevStatic &S, const DevState &X);
 void launch_put(cudaStream_t st, const int *idx, const double *val, int n, double *dst);
 // sub-grid channels (xm_chan.cu); each does nothing unless l.chan
 void launch_chan_entry(const Launch &l, const DevStatic &S, const DevState &X);

@@ -28,22 +28,41 @@ namespace xm {
 // ---------------------------------------------------------------------------
 // calpuv2c.f90:214-220: the explicit transports FUHDYE (face between cell d
 // and its west neighbour, elevations P and PW) and FVHDXE (south face).
+// UH1: UHDYE at entry (UHDY1E in CALPUV9C), HC: the face depth (HUTMP in
+// CALPUV9C), TS, TB: the stresses (TSX1, TBX1 in CALPUV9C, calpuv9c.f90:216-217);
 // FPGXE / FPGYE: the baroclinic terms, 0.0 without them.
 __device__ __forceinline__ double fuh_face(const DevStatic &S, const DevState &X,
-                                           const StepScalars &c, int d, double P, double PW,
-                                           double sub, double FPGXE) {
-  return X.uhdy1e[d] - c.deltd2 * sub * S.hruo[d] * X.hu[d] * (P - PW) +
+                                           const StepScalars &c, int d, double UH1, double HC,
+                                           double P, double PW, double sub, double FPGXE,
+                                           double TS, double TB) {
+  return UH1 - c.deltd2 * sub * S.hruo[d] * HC * (P - PW) +
          sub * c.delt * S.dxiu[d] *
-             (S.dxyu[d] * (X.tsx[d] - c.ritb1 * X.tbx[d]) + X.fcaxe[d] + FPGXE -
-              c.snlt * X.fxe[d]);
+             (S.dxyu[d] * (TS - c.ritb1 * TB) + X.fcaxe[d] + FPGXE - c.snlt * X.fxe[d]);
 }
 __device__ __forceinline__ double fvh_face(const DevStatic &S, const DevState &X,
-                                           const StepScalars &c, int d, double P, double PS,
-                                           double svb, double FPGYE) {
-  return X.vhdx1e[d] - c.deltd2 * svb * S.hrvo[d] * X.hv[d] * (P - PS) +
+                                           const StepScalars &c, int d, double VH1, double HC,
+                                           double P, double PS, double svb, double FPGYE,
+                                           double TS, double TB) {
+  return VH1 - c.deltd2 * svb * S.hrvo[d] * HC * (P - PS) +
          svb * c.delt * S.dyiv[d] *
-             (S.dxyv[d] * (X.tsy[d] - c.ritb1 * X.tby[d]) - X.fcaye[d] + FPGYE -
-              c.snlt * X.fye[d]);
+             (S.dxyv[d] * (TS - c.ritb1 * TB) - X.fcaye[d] + FPGYE - c.snlt * X.fye[d]);
+}
+
+// calpuv2c.f90:192-201 (calpuv9c.f90:175-181): the external density
+// gradients of the west and south faces of cell q.d from HP, HU, HV, SBX, SBY.
+__device__ __forceinline__ void baro_faces(const DevStatic &S, const DevState &X,
+                                           const StepScalars &c, const Nb &q, const double *HP,
+                                           double &FPGXE, double &FPGYE) {
+  const DevBaro &Bc = S.baro;
+  const int d = q.d;
+  FPGXE = -X.sbx[d] * X.hu[d] * c.gp *
+          ((Bc.bi2[d] + Bc.bi2[q.w]) * (HP[d] - HP[q.w]) +
+           2.0 * X.hu[d] * (Bc.bi1[d] - Bc.bi1[q.w]) +
+           (Bc.be[d] + Bc.be[q.w]) * (S.belv[d] - S.belv[q.w]));
+  FPGYE = -X.sby[d] * X.hv[d] * c.gp *
+          ((Bc.bi2[d] + Bc.bi2[q.s]) * (HP[d] - HP[q.s]) +
+           2.0 * X.hv[d] * (Bc.bi1[d] - Bc.bi1[q.s]) +
+           (Bc.be[d] + Bc.be[q.s]) * (S.belv[d] - S.belv[q.s]));
 }
 
 // CALEBI (calebi.f90:73-120) for the standard sigma grid (KSZ = 1): the
@@ -77,12 +96,13 @@ __global__ void __launch_bounds__(NT) k_calebi(DevStatic S, DevState X, int ntil
   }
 }
 
-// calpuv2c.f90:282-290
-__device__ __forceinline__ double fp1_cell(const DevStatic &S, const DevState &X,
-                                           const StepScalars &c, const Nb &q, double P) {
+// calpuv2c.f90:282-290 (calpuv9c.f90:277, from P1, UHDY1E, VHDX1E); U, V: the
+// transports at entry
+__device__ __forceinline__ double fp1_cell(const DevStatic &S, const StepScalars &c,
+                                           const Nb &q, double P, const double *U,
+                                           const double *V) {
   const double C1 = 0.5 * c.g;
-  return c.delti * S.dxyp[q.d] * P -
-         C1 * (X.uhdy1e[q.e] - X.uhdy1e[q.d] + X.vhdx1e[q.n] - X.vhdx1e[q.d]);
+  return c.delti * S.dxyp[q.d] * P - C1 * (U[q.e] - U[q.d] + V[q.n] - V[q.d]);
 }
 
 // calpuv2c.f90:306-344 for cell q.d from its faces' transports: FP, CS, CW,
@@ -96,10 +116,10 @@ __device__ __forceinline__ double assemble_cell(const DevStatic &S, const DevSta
   const double sub = X.sub[d], svb = X.svb[d], sube = X.sub[q.e], svbn = X.svb[q.n];
   X.fp[d] = fp1 - C1 * (sube * fuhe - sub * fuh + svbn * fvhn - svb * fvh - 2.0 * X.qsume[d]);
   C1 = -0.5 * c.deltd2 * c.g;
-  const double cs = C1 * svb * S.hrvo[d] * S.rcx[d] * X.hv[d];
-  const double cw = C1 * sub * S.hruo[d] * S.rcx[d] * X.hu[d];
-  const double ce = C1 * sube * S.hruo[q.e] * S.rcx[q.e] * X.hu[q.e];
-  const double cn = C1 * svbn * S.hrvo[q.n] * S.rcx[q.n] * X.hv[q.n];
+  const double cs = C1 * svb * S.hrvo[d] * S.rcx[d] * X.hvc[d];
+  const double cw = C1 * sub * S.hruo[d] * S.rcx[d] * X.huc[d];
+  const double ce = C1 * sube * S.hruo[q.e] * S.rcx[q.e] * X.huc[q.e];
+  const double cn = C1 * svbn * S.hrvo[q.n] * S.rcx[q.n] * X.hvc[q.n];
   const double cc = c.delti * S.dxyp[d] - cs - cw - ce - cn;
   X.cs[d] = cs;
   X.cw[d] = cw;
@@ -114,9 +134,10 @@ __device__ __forceinline__ double assemble_cell(const DevStatic &S, const DevSta
 // UHDYE<->UHDY1E, VHDXE<->VHDX1E and HP<->H1P before this kernel, so the *1
 // buffers hold the values at entry (the time-level advance :256-264).
 // BARO: a member of the batch has baroclinic terms; the instance without them
-// keeps the register count (and so the grid of every cell kernel) low.
+// is held to 32 registers (8 CTAs per SM), which sizes the grid of every cell
+// kernel (occupancy_blocks_per_sm).
 template <bool BARO>
-__global__ void __launch_bounds__(NT) k_begin(DevStatic S, DevState X, int ntile) {
+__global__ void __launch_bounds__(NT, BARO ? 4 : 8) k_begin(DevStatic S, DevState X, int ntile) {
   TILE_LOOP(ntile) {
     TILE_MEMBER(S);
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
@@ -133,27 +154,91 @@ __global__ void __launch_bounds__(NT) k_begin(DevStatic S, DevState X, int ntile
     }
     const double P = X.p[d];
     double FPGXE = 0., FPGYE = 0.;
-    if (BARO && c.baro) {  // :192-201 external density gradients (entry HP, HU, HV, SBX, SBY)
-      const DevBaro &Bc = S.baro;
-      const double *HP = X.h1p;
-      FPGXE = -X.sbx[d] * X.hu[d] * c.gp *
-              ((Bc.bi2[d] + Bc.bi2[q.w]) * (HP[d] - HP[q.w]) +
-               2.0 * X.hu[d] * (Bc.bi1[d] - Bc.bi1[q.w]) +
-               (Bc.be[d] + Bc.be[q.w]) * (S.belv[d] - S.belv[q.w]));
-      FPGYE = -X.sby[d] * X.hv[d] * c.gp *
-              ((Bc.bi2[d] + Bc.bi2[q.s]) * (HP[d] - HP[q.s]) +
-               2.0 * X.hv[d] * (Bc.bi1[d] - Bc.bi1[q.s]) +
-               (Bc.be[d] + Bc.be[q.s]) * (S.belv[d] - S.belv[q.s]));
-    }
-    X.fuhdye[d] = fuh_face(S, X, c, d, P, X.p[q.w], sub, FPGXE);
-    X.fvhdxe[d] = fvh_face(S, X, c, d, P, X.p[q.s], svb, FPGYE);
+    if (BARO && c.baro)  // :192-201 (entry HP in the H1P buffer, HU, HV, SBX, SBY)
+      baro_faces(S, X, c, q, X.h1p, FPGXE, FPGYE);
+    X.fuhdye[d] = fuh_face(S, X, c, d, X.uhdy1e[d], X.hu[d], P, X.p[q.w], sub, FPGXE,
+                           X.tsx[d], X.tbx[d]);
+    X.fvhdxe[d] = fvh_face(S, X, c, d, X.vhdx1e[d], X.hv[d], P, X.p[q.s], svb, FPGYE,
+                           X.tsy[d], X.tby[d]);
     if (c.isdry > 0) {  // :246-253
       X.sub[d] = S.subo[d];
       X.svb[d] = S.svbo[d];
       X.sbx[d] = S.sbxo[d];
       X.sby[d] = S.sbyo[d];
     }
-    X.fp1[d] = fp1_cell(S, X, c, q, P);
+    X.fp1[d] = fp1_cell(S, c, q, P, X.uhdy1e, X.vhdx1e);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CALPUV9C(ISTL_) up to its time-level advance (calpuv9c.f90:154-280): the
+// QDWASTE reset, the blended density gradients FPGXE/FPGYE, HUTMP/HVTMP, the
+// explicit transports from level n-1 (UHDY1E, P1, TSX1, TBX1), the switch
+// reset of wetting and drying, FP1.  No swap precedes it: the buffers hold
+// the caller's levels.
+template <bool BARO>
+__global__ void __launch_bounds__(NT) k_begin3(DevStatic S, DevState X, int ntile) {
+  TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    if (c.isdry > 0 && c.ndrystp < 0) X.qdwaste[d] = 0.;  // :154-160
+    double FPGXE = 0., FPGYE = 0.;
+    if (BARO && c.baro) {  // :164-190
+      double gx, gy;
+      baro_faces(S, X, c, q, X.hp, gx, gy);
+      FPGXE = c.rold * X.fpgxe[d] + c.rnew * gx;
+      FPGYE = c.rold * X.fpgye[d] + c.rnew * gy;
+      X.fpgxe[d] = FPGXE;
+      X.fpgye[d] = FPGYE;
+    }
+    double hut, hvt;  // :192-204
+    if (c.istl == 2) {
+      hut = 0.5 * (X.hu[d] + X.h1u[d]);
+      hvt = 0.5 * (X.hv[d] + X.h1v[d]);
+      X.hutmp[d] = hut;
+      X.hvtmp[d] = hvt;
+    } else {
+      hut = X.hu[d];
+      hvt = X.hv[d];
+    }
+    const double sub = X.sub[d], svb = X.svb[d];
+    const double P1 = X.p1[d];
+    X.fuhdye[d] = fuh_face(S, X, c, d, X.uhdy1e[d], hut, P1, X.p1[q.w], sub, FPGXE,
+                           X.tsx1[d], X.tbx1[d]);  // :206-222
+    X.fvhdxe[d] = fvh_face(S, X, c, d, X.vhdx1e[d], hvt, P1, X.p1[q.s], svb, FPGYE,
+                           X.tsy1[d], X.tby1[d]);
+    if (c.isdry > 0) {  // :246-262
+      X.iscdry[d] = 0;
+      X.sub1[d] = sub;
+      X.svb1[d] = svb;
+      X.sub[d] = S.subo[d];
+      X.svb[d] = S.svbo[d];
+      X.sbx[d] = S.sbxo[d];
+      X.sby[d] = S.sbyo[d];
+      X.oldmask[d] = X.lmaskdry[d];
+      X.wasted[d] = 0;
+    }
+    X.fp1[d] = fp1_cell(S, c, q, P1, X.uhdy1e, X.vhdx1e);  // :268-280
+  }
+}
+
+// CALPUV9C(3), the copies of the time-level advance (calpuv9c.f90:282-311);
+// the host has rotated the buffers UHDY2E <- UHDY1E <- UHDYE and
+// H2P <- H1P <- HP before it.  NCTBC = 1 halves UHDYE on the way (:289-294).
+__global__ void __launch_bounds__(NT) k_advance3(DevStatic S, DevState X, int ntile) {
+  TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    const int d = tile * TILE + threadIdx.x;
+    if (S.kind[d] == LAND) continue;
+    if (c.nctbc == 1) {
+      X.uhdy1e[d] = 0.5 * X.uhdy1e[d];
+      X.vhdx1e[d] = 0.5 * X.vhdx1e[d];
+    }
+    X.p1[d] = X.p[d];
+    X.h1u[d] = X.hu[d];
+    X.h1v[d] = X.hv[d];
   }
 }
 
@@ -213,29 +298,29 @@ __device__ __forceinline__ double obc_cell(const DevStatic &S, const DevState &X
     }
     if (ispb == 1 || ispb == 2) {  // radiation
       if (side == 0) {  // W, face at LEC(L)
-        const double CET = 0.5 * D * G * S.hruo[nb] * S.rcx[nb] * X.hu[nb];
-        const double TMP = D * sqrt(G * X.hu[nb]) * S.dxiu[nb];
+        const double CET = 0.5 * D * G * S.hruo[nb] * S.rcx[nb] * X.huc[nb];
+        const double TMP = D * sqrt(G * X.huc[nb]) * S.dxiu[nb];
         X.cc[d] = CET * (1. + TMP) / TMP;
         X.ce[d] = -CET;
-        fp = CET * (2. * fp - sqrt(G * X.hu[nb]) * X.fuhdye[nb] * S.dyiu[nb] / X.hu[nb]) / TMP;
+        fp = CET * (2. * fp - sqrt(G * X.huc[nb]) * X.fuhdye[nb] * S.dyiu[nb] / X.huc[nb]) / TMP;
       } else if (side == 1) {  // E, own west face
-        const double CWT = 0.5 * D * G * S.hruo[d] * S.rcx[d] * X.hu[d];
-        const double TMP = D * sqrt(G * X.hu[d]) * S.dxiu[d];
+        const double CWT = 0.5 * D * G * S.hruo[d] * S.rcx[d] * X.huc[d];
+        const double TMP = D * sqrt(G * X.huc[d]) * S.dxiu[d];
         X.cc[d] = CWT * (1. + TMP) / TMP;
         X.cw[d] = -CWT;
-        fp = CWT * (2. * fp + sqrt(G * X.hu[d]) * X.fuhdye[d] * S.dyiu[d] / X.hu[d]) / TMP;
+        fp = CWT * (2. * fp + sqrt(G * X.huc[d]) * X.fuhdye[d] * S.dyiu[d] / X.huc[d]) / TMP;
       } else if (side == 2) {  // S, face at LNC(L)
-        const double CNT = 0.5 * D * G * S.hrvo[nb] * S.rcx[nb] * X.hv[nb];
-        const double TMP = D * sqrt(G * X.hv[nb]) * S.dyiv[nb];
+        const double CNT = 0.5 * D * G * S.hrvo[nb] * S.rcx[nb] * X.hvc[nb];
+        const double TMP = D * sqrt(G * X.hvc[nb]) * S.dyiv[nb];
         X.cc[d] = CNT * (1. + TMP) / TMP;
         X.cn[d] = -CNT;
-        fp = CNT * (2. * fp - sqrt(G * X.hv[nb]) * X.fvhdxe[nb] * S.dxiv[nb] / X.hv[nb]) / TMP;
+        fp = CNT * (2. * fp - sqrt(G * X.hvc[nb]) * X.fvhdxe[nb] * S.dxiv[nb] / X.hvc[nb]) / TMP;
       } else {  // N, own south face
-        const double CST = 0.5 * D * G * S.hrvo[d] * S.rcx[d] * X.hv[d];
-        const double TMP = D * sqrt(G * X.hv[d]) * S.dyiv[d];
+        const double CST = 0.5 * D * G * S.hrvo[d] * S.rcx[d] * X.hvc[d];
+        const double TMP = D * sqrt(G * X.hvc[d]) * S.dyiv[d];
         X.cc[d] = CST * (1. + TMP) / TMP;
         X.cs[d] = -CST;
-        fp = CST * (2. * fp + sqrt(G * X.hv[d]) * X.fvhdxe[d] * S.dxiv[d] / X.hv[d]) / TMP;
+        fp = CST * (2. * fp + sqrt(G * X.hvc[d]) * X.fvhdxe[d] * S.dxiv[d] / X.hvc[d]) / TMP;
       }
     } else {  // clamped elevation
       const double FP1G = fp / G - HDRY2;
@@ -245,13 +330,13 @@ __device__ __forceinline__ double obc_cell(const DevStatic &S, const DevState &X
         CT = 0.;
         X.lopenbcdry[d] = 1;
       } else if (side == 0) {
-        CT = 0.5 * D * G * S.hruo[nb] * S.rcx[nb] * X.hu[nb];
+        CT = 0.5 * D * G * S.hruo[nb] * S.rcx[nb] * X.huc[nb];
       } else if (side == 1) {
-        CT = 0.5 * D * G * S.hruo[d] * S.rcx[d] * X.hu[d];
+        CT = 0.5 * D * G * S.hruo[d] * S.rcx[d] * X.huc[d];
       } else if (side == 2) {
-        CT = 0.5 * D * G * S.hrvo[nb] * S.rcx[nb] * X.hv[nb];
+        CT = 0.5 * D * G * S.hrvo[nb] * S.rcx[nb] * X.hvc[nb];
       } else {
-        CT = 0.5 * D * G * S.hrvo[d] * S.rcx[d] * X.hv[d];
+        CT = 0.5 * D * G * S.hrvo[d] * S.rcx[d] * X.hvc[d];
       }
       X.fp[nb] = X.fp[nb] + CT * fp;
       fp = c.delti * S.dxyp[d] * fp;
@@ -666,9 +751,9 @@ __global__ void __launch_bounds__(NT) k_backsub(DevStatic S, DevState X, int nti
     if (S.kind[d] == LAND) continue;
     const double P = X.p[d];
     const double u = X.sub[d] *
-                     (X.fuhdye[d] - c.deltd2 * S.hruo[d] * S.rcx[d] * X.hu[d] * (P - X.p[q.w]));
+                     (X.fuhdye[d] - c.deltd2 * S.hruo[d] * S.rcx[d] * X.huc[d] * (P - X.p[q.w]));
     const double v = X.svb[d] *
-                     (X.fvhdxe[d] - c.deltd2 * S.hrvo[d] * S.rcx[d] * X.hv[d] * (P - X.p[q.s]));
+                     (X.fvhdxe[d] - c.deltd2 * S.hrvo[d] * S.rcx[d] * X.hvc[d] * (P - X.p[q.s]));
     X.uhdye[d] = u;
     X.vhdxe[d] = v;
     X.uhe[d] = u * S.dyiu[d];
@@ -676,7 +761,9 @@ __global__ void __launch_bounds__(NT) k_backsub(DevStatic S, DevState X, int nti
   }
 }
 
-// calpuv2c.f90:466-486 continuity.
+// calpuv2c.f90:466-486 continuity from H1P, UHDY1E, VHDX1E; CALPUV9C's
+// (calpuv9c.f90:500-525) is written DELT*(Q - S/2), from H2P, UHDY2E, VHDX2E
+// for ISTL_ = 3 (the views hb, ub, vb).
 __global__ void __launch_bounds__(NT) k_continuity(DevStatic S, DevState X, int ntile,
                                                   const int *act) {
   TILE_LOOP(ntile) {
@@ -685,11 +772,15 @@ __global__ void __launch_bounds__(NT) k_continuity(DevStatic S, DevState X, int 
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
     if (S.kind[d] == LAND) continue;
-    X.hp[d] = X.h1p[d] +
-              c.deltd2 * S.dxyip[d] *
-                  (2. * X.qsume[d] -
-                   (X.uhdye[q.e] + X.uhdy1e[q.e] - X.uhdye[d] - X.uhdy1e[d] + X.vhdxe[q.n] +
-                    X.vhdx1e[q.n] - X.vhdxe[d] - X.vhdx1e[d]));
+    const double *U = X.ub, *V = X.vb;
+    if (c.istl == 0)
+      X.hp[d] = X.hb[d] + c.deltd2 * S.dxyip[d] *
+                              (2. * X.qsume[d] - (X.uhdye[q.e] + U[q.e] - X.uhdye[d] - U[d] +
+                                                  X.vhdxe[q.n] + V[q.n] - X.vhdxe[d] - V[d]));
+    else
+      X.hp[d] = X.hb[d] + c.delt * S.dxyip[d] *
+                              (X.qsume[d] - 0.5 * (X.uhdye[q.e] + U[q.e] - X.uhdye[d] - U[d] +
+                                                   X.vhdxe[q.n] + V[q.n] - X.vhdxe[d] - V[d]));
   }
 }
 
@@ -751,7 +842,12 @@ __global__ void __launch_bounds__(NT) k_wd_legacy(DevStatic S, DevState X, int n
     if (S.kind[d] != LAND) {
       const double hp = X.hp[d];
       X.p[d] = c.g * (hp + S.belv[d]);
-      if (check && hp <= c.hdry) {
+      bool dry = hp <= c.hdry;
+      if (c.istl != 0) {  // calpuv9c.f90:628-662: below HDRY and not rising fast (HPPMC)
+        const double HPPMC = X.hb[d];
+        dry = hp < c.hdry && (hp < 0.9 * c.hdry || HPPMC < c.hdry) && hp < (HPPMC + 0.1 * c.hdry);
+      }
+      if (check && dry) {
         if (X.iscdry[d] == 0) {
           X.iscdry[d] = 1;
           flag = true;
@@ -788,7 +884,7 @@ __global__ void __launch_bounds__(NT) k_wd99_decide(DevStatic S, DevState X, int
       X.wd_act[d] = 0;
       continue;
     }
-    const double hp = X.hp[d], h1p = X.h1p[d];
+    const double hp = X.hp[d], h1p = X.hb[d];  // HPPMC: H1P, or H2P in CALPUV9C(3)
     X.p[d] = c.g * (hp + S.belv[d]);
     int a = 0;
     if (hp <= HDRY) {
@@ -931,7 +1027,9 @@ __global__ void __launch_bounds__(NT) k_fin_waste(DevStatic S, DevState X, int n
               X.hp[d] = hnew;
               X.h1p[d] = 0.90 * c.hdry;
               X.natdry[d] = 0;
-              X.qdwaste[d] = (c.isbal == 0) ? 0.0 : c.delti * S.dxyp[d] * (HOLDTMP - hnew);
+              // CALPUV9C adds to the QDWASTE zeroed at entry (calpuv9c.f90:919) and keeps it
+              X.qdwaste[d] = (c.istl != 0) ? X.qdwaste[d] + c.delti * S.dxyp[d] * (HOLDTMP - hnew)
+                             : (c.isbal == 0) ? 0.0 : c.delti * S.dxyp[d] * (HOLDTMP - hnew);
               X.vdwaste[d] = X.vdwaste[d] + S.dxyp[d] * (HOLDTMP - hnew);
               X.wasted[d] = 1;
               nw = 1;
@@ -1050,6 +1148,20 @@ void launch_begin(const Launch &l, const DevStatic &S, const DevState &X) {
     k_begin<true><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
   else
     k_begin<false><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+  count_launches(1);
+}
+void launch_begin3(const Launch &l, const DevStatic &S, const DevState &X) {
+  if (l.baro) {
+    k_calebi<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);  // calpuv9c.f90:145
+    count_launches(1);
+    k_begin3<true><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+  } else {
+    k_begin3<false><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+  }
+  count_launches(1);
+}
+void launch_advance3(const Launch &l, const DevStatic &S, const DevState &X) {
+  k_advance3<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
   count_launches(1);
 }
 void launch_sweep_reset(const Launch &l, Ctl *ctl, const int *act, int nmember) {

@@ -53,7 +53,8 @@ class Params(C.Structure):
                 ("n", C.c_int32), ("ntstbc", C.c_int32), ("max_sweeps", C.c_int32),
                 ("precision", C.c_int32), ("mixed_rsq_factor", C.c_double),
                 ("qcherr", C.c_double), ("chan_consistent", C.c_int32), ("pad_", C.c_int32),
-                ("bsc", C.c_double), ("gp", C.c_double)]
+                ("bsc", C.c_double), ("gp", C.c_double), ("tl3_istl", C.c_int32),
+                ("nctbc", C.c_int32), ("rold", C.c_double), ("rnew", C.c_double)]
 
 
 class Fields(C.Structure):
@@ -67,7 +68,10 @@ class Fields(C.Structure):
                 ("qdwaste", _pd), ("vdwaste", _pd), ("lwet", _pi), ("ldry", _pi),
                 ("ccc", _pd), ("ccs", _pd), ("ccw", _pd), ("cce", _pd), ("ccn", _pd),
                 ("fptmp", _pd), ("qchanu", _pd), ("qchanv", _pd), ("qchanun", _pd),
-                ("qchanvn", _pd), ("b", _pd), ("b_ld", C.c_int32), ("pad_b_", C.c_int32)]
+                ("qchanvn", _pd), ("b", _pd), ("b_ld", C.c_int32), ("pad_b_", C.c_int32),
+                ("p1", _pd), ("h2p", _pd), ("uhdy1e", _pd), ("vhdx1e", _pd), ("uhdy2e", _pd),
+                ("vhdx2e", _pd), ("h1u", _pd), ("h1v", _pd), ("tsx1", _pd), ("tsy1", _pd),
+                ("tbx1", _pd), ("tby1", _pd), ("fpgxe", _pd), ("fpgye", _pd)]
 
 
 class Layers(C.Structure):
@@ -102,6 +106,9 @@ FIELD_IN = ("fcaxe", "fcaye", "fxe", "fye", "tsx", "tsy", "tbx", "tby", "qsume")
 FIELD_OUT = ("uhe", "vhe", "hpi", "hui", "hvi", "qdwaste", "vdwaste")
 FIELD_CHAN = ("qchanu", "qchanv", "qchanun", "qchanvn")  # per channel, in/out
 FIELD_DIAG = ("ccc", "ccs", "ccw", "cce", "ccn", "fptmp")
+# three time levels (CALPUV9C): in/out, and the in-only wind and bed stresses
+FIELD_TL3 = ("p1", "h2p", "uhdy1e", "vhdx1e", "uhdy2e", "vhdx2e", "h1u", "h1v", "tsx1",
+             "tsy1", "tbx1", "tby1", "fpgxe", "fpgye")
 
 
 def _dp(a):
@@ -159,7 +166,8 @@ def make_grid(g: dict):
 
 def make_params(p: dict, *, n: int, tn: float, precision: int = PREC_FP64):
     s = Params()
-    s.delt = p["dt"]
+    # CALPUV9C(3), the leapfrog step, advances over DT2 = 2*DT (calpuv9c.f90:105-106)
+    s.delt = p["dt"] * (2.0 if int(p.get("tl3_istl", 0)) == 3 else 1.0)
     s.g = p["g"]
     s.hdry = p["hdry"]
     s.rsqm = p["rsqm"]
@@ -180,6 +188,10 @@ def make_params(p: dict, *, n: int, tn: float, precision: int = PREC_FP64):
     s.chan_consistent = int(p.get("chan_consistent", 0))
     s.bsc = p.get("bsc", 0.0)
     s.gp = p.get("gp", p["g"])
+    s.tl3_istl = int(p.get("tl3_istl", 0))
+    s.nctbc = int(p.get("nctbc", 0))
+    s.rold = p.get("rold", 0.0)
+    s.rnew = p.get("rnew", 1.0)
     return s
 
 
@@ -216,7 +228,7 @@ def make_fields(st: dict, *, diag: bool = False, lists: bool = False):
     """Build a Fields struct over the numpy arrays of a state dict (in place)."""
     s = Fields()
     keep = []
-    for k in FIELD_DOUBLE_INOUT + FIELD_IN + FIELD_OUT + FIELD_CHAN:
+    for k in FIELD_DOUBLE_INOUT + FIELD_IN + FIELD_OUT + FIELD_CHAN + FIELD_TL3:
         a = st.get(k)
         if a is not None:
             setattr(s, k, _dp(a))

@@ -618,3 +618,42 @@ def add_baroclinic(scn: Scenario, kc: int = 4, *, seed: int = 0, front: float = 
     scn.params["bsc"] = bsc
     scn.params["gp"] = G
     return scn
+
+
+def add_three_levels(scn: Scenario) -> Scenario:
+    """The state of the three-time-level scheme (CALPUV9C) at its start, with
+    level n-1 equal to level n: P1 = P, H2P = H1P = HP, UHDY1E = UHDY2E =
+    UHDYE, VHDX1E = VHDX2E = VHDXE, H1U = HU, H1V = HV, and the level n-1
+    stresses TSX1, TSY1, TBX1, TBY1 equal to TSX, TSY, TBX, TBY.  With
+    baroclinic terms FPGXE = FPGYE = 0 (their blend starts from zero)."""
+    st = scn.state
+    for dst, src in (("p1", "p"), ("h2p", "hp"), ("h1p", "hp"), ("uhdy1e", "uhdye"),
+                     ("uhdy2e", "uhdye"), ("vhdx1e", "vhdxe"), ("vhdx2e", "vhdxe"),
+                     ("h1u", "hu"), ("h1v", "hv"), ("tsx1", "tsx"), ("tsy1", "tsy"),
+                     ("tbx1", "tbx"), ("tby1", "tby")):
+        st[dst] = st[src].copy() if src in st else np.zeros_like(st["p"])
+    if scn.params.get("bsc", 0.0) > 1e-6:
+        st["fpgxe"] = np.zeros_like(st["p"])
+        st["fpgye"] = np.zeros_like(st["p"])
+    return scn
+
+
+def three_level_schedule(nsteps: int, ntstbc: int):
+    """The CALPUV9C calls of HDMT's time loop for steps 1..nsteps, as
+    (N, ISTL, NCTBC, ROLD, RNEW): leapfrog steps (ISTL = 3, ROLD = 0, RNEW = 1)
+    and, after the step on which NCTBC reaches NTSTBC, the trapezoidal
+    correction of the same step (ISTL = 2, NCTBC = 0, ROLD = RNEW = 0.5)
+    (hdmt.f90:299-305, 1009-1029; NCTBC starts at 1, aaefdc.f90:354)."""
+    out, n, istl, nctbc = [], 1, 3, 1
+    while n <= nsteps:
+        out.append((n, istl, nctbc, 0.0 if istl == 3 else 0.5, 1.0 if istl == 3 else 0.5))
+        if istl == 3 and nctbc == ntstbc:
+            nctbc, istl = 0, 2
+        else:
+            nctbc, istl, n = nctbc + 1, 3, n + 1
+    return out
+
+
+def three_level_params(params: dict, istl: int, nctbc: int, rold: float, rnew: float) -> dict:
+    """The parameters of one CALPUV9C(ISTL) call (DELT = 2*DT for ISTL = 3)."""
+    return dict(params, tl3_istl=istl, nctbc=nctbc, rold=rold, rnew=rnew)

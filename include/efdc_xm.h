@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define EFDC_XM_ABI_VERSION 2
+#define EFDC_XM_ABI_VERSION 3
 
 /* Status codes.  The reference STOPs where these are returned. */
 enum efdc_xm_status {
@@ -117,6 +117,17 @@ typedef struct efdc_xm_params {
   double bsc;        /* BSC: the baroclinic terms FPGXE, FPGYE enter when > 1e-6
                         (calpuv2c.f90:161, 192-211); needs efdc_xm_set_layers and B */
   double gp;         /* GP (hdmt2t.f90:459-463)                                       */
+  int32_t tl3_istl;  /* 0: CALPUV2C, the two-time-level step (hdmt2t.f90:509).  3 or 2:
+                        CALPUV9C(ISTL_) of the three-time-level scheme (hdmt.f90:415):
+                        3 the leapfrog step, 2 its trapezoidal correction.  delt is then
+                        the DELT of that call (calpuv9c.f90:105-111: DT2 = 2*DT for 3,
+                        DT for 2), and the fields' three-time-level arrays are used.
+                        All members of a batch take the same value                    */
+  int32_t nctbc;     /* NCTBC (CALPUV9C, ISTL_ = 3): 1 halves UHDYE, VHDXE before they
+                        become UHDY1E, VHDX1E (calpuv9c.f90:289-294)                   */
+  double rold, rnew; /* ROLD, RNEW (CALPUV9C, BSC > 1e-6): FPGXE = ROLD*FPGXE +
+                        RNEW*(new gradient) (calpuv9c.f90:157-163; hdmt.f90:304-305,
+                        1018-1028: 0 and 1 for ISTL_ = 3, 0.5 and 0.5 for 2)          */
 } efdc_xm_params;
 
 /* Per-call arrays.  "in/out" arrays are read and overwritten.  Optional outputs
@@ -157,6 +168,17 @@ typedef struct efdc_xm_fields {
   const double *b;
   int32_t b_ld;
   int32_t pad_b_;
+  /* three time levels (tl3_istl = 2 or 3), required there and ignored by CALPUV2C
+   * steps.  in/out: ISTL_ = 3 advances them (calpuv9c.f90:288-311: UHDY2E <-
+   * UHDY1E <- UHDYE, P1 <- P, H1U <- HU, H1V <- HV, H2P <- H1P <- HP); H1P is then
+   * an input as well.  The layer copies (H1PK, UHDY1EK, ...), U1V, V1U, H1UI and
+   * H1VI stay with the caller. */
+  double *p1, *h2p;                   /* P1, H2P                                      */
+  double *uhdy1e, *vhdx1e;            /* UHDY1E, VHDX1E                               */
+  double *uhdy2e, *vhdx2e;            /* UHDY2E, VHDX2E                               */
+  double *h1u, *h1v;                  /* H1U, H1V                                     */
+  const double *tsx1, *tsy1, *tbx1, *tby1;  /* TSX1, TSY1, TBX1, TBY1, in            */
+  double *fpgxe, *fpgye;              /* FPGXE, FPGYE, in/out; required where BSC > 1e-6 */
 } efdc_xm_fields;
 
 typedef struct efdc_xm_stats {

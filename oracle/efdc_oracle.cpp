@@ -1,5 +1,5 @@
 // efdc_oracle.cpp -- TEST INFRASTRUCTURE ONLY: CPU FP64 restatement of EFDC+
-// 8.5 CALPUV2C / CONGRAD / CONGRADC / SUBCHAN / CALEBI (standard sigma) /
+// 8.5 CALPUV2C / CALPUV9C / CONGRAD / CONGRADC / SUBCHAN / CALEBI (standard sigma) /
 // SETOPENBC / SETOPENBC2 / NEGDEP (check part).
 // Parity against the reference is UNPINNED (no compiler, no reference tests);
 // see efdc_oracle.h.  Each block cites the Fortran it restates.
@@ -456,7 +456,16 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
 
   const double G = prm->g;
   const double GI = 1. / G;  // aaefdc.f90:648
-  // calpuv2c.f90:128-136
+  // CALPUV2C (ISTL = 0 here), or CALPUV9C(ISTL_) of the three-time-level scheme
+  const int ISTL = prm->tl3_istl;
+  const bool tl3 = ISTL != 0;
+  if (tl3 && ((ISTL != 2 && ISTL != 3) || !f->p1 || !f->h2p || !f->uhdy1e || !f->vhdx1e ||
+              !f->uhdy2e || !f->vhdx2e || !f->h1u || !f->h1v)) {
+    st->status = EFDC_XM_BAD_ARGUMENT;
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  // calpuv2c.f90:128-136; calpuv9c.f90:105-111 (DELT = DT2 or DT as passed:
+  // DELTD2 = DT = DT2/2, or DT/2)
   const double DELT = prm->delt;
   const double DELTD2 = 0.5 * DELT;
   const double DELTI = 1. / DELT;
@@ -464,7 +473,7 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
   const int ISDRY = prm->isdry, NDRYSTP = prm->ndrystp;
   const double RITB1 = prm->ritb1, SNLT = prm->snlt;
   const bool baro = prm->bsc > 1.E-6;
-  if (baro && (c->kc < 1 || !f->b)) {
+  if (baro && (c->kc < 1 || !f->b || (tl3 && (!f->fpgxe || !f->fpgye)))) {
     st->status = EFDC_XM_BAD_ARGUMENT;
     return EFDC_XM_BAD_ARGUMENT;
   }
@@ -501,11 +510,22 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
       st->status = EFDC_XM_BAD_ARGUMENT;
       return EFDC_XM_BAD_ARGUMENT;
     }
-    for (int k = 0; k < ch.n; ++k) {  // :139-145
-      ch.qut[k] = f->qchanu[k];
-      ch.qvt[k] = f->qchanv[k];
+    for (int k = 0; k < ch.n; ++k) {
+      if (!tl3) {  // :139-145
+        ch.qut[k] = f->qchanu[k];
+        ch.qvt[k] = f->qchanv[k];
+      } else {  // calpuv9c.f90:128-141
+        ch.qut[k] = f->qchanun[k];
+        ch.qvt[k] = f->qchanvn[k];
+        if (ISTL == 3) {
+          f->qchanun[k] = f->qchanu[k];
+          f->qchanvn[k] = f->qchanv[k];
+        }
+      }
     }
-    for (int L = 1; L <= lc; ++L) c->p1[L] = P[L];  // P1 = P (:259)
+    // P1 as SUBCHAN and the exchange read it: P at entry (:259, and
+    // calpuv9c.f90:302 for ISTL_ = 3), the caller's P1 for ISTL_ = 2
+    for (int L = 1; L <= lc; ++L) c->p1[L] = (ISTL == 2) ? f->p1[L - 1] : P[L];
   }
   // :150-157
   if (ISDRY > 0)
@@ -513,7 +533,87 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
 
   std::vector<int> nnatdry_flag(size_t(lc) + 1, 0);
 
-  // ---- first domain loop (:164-293) ----
+  // Three time levels: the caller's arrays, and HUTMP/HVTMP, the face depths
+  // of the coefficients (HU, HV in CALPUV2C; HUTMP(1), HUTMP(LC) stay 0,
+  // varzeroreal.f90:249)
+  std::vector<double> hutmp(size_t(lc), 0.0), hvtmp(size_t(lc), 0.0);
+  F<double> HUT{hutmp.data()}, HVT{hvtmp.data()};
+  F<double> P1T{f->p1}, H2P{f->h2p}, U1{f->uhdy1e}, V1{f->vhdx1e}, U2{f->uhdy2e},
+      V2{f->vhdx2e}, H1U{f->h1u}, H1V{f->h1v}, FPGX{f->fpgxe}, FPGY{f->fpgye};
+  F<const double> TSX1 = cin(f->tsx1), TSY1 = cin(f->tsy1), TBX1 = cin(f->tbx1),
+                  TBY1 = cin(f->tby1);
+  const F<const double> HUc{tl3 ? HUT.b : HU.b}, HVc{tl3 ? HVT.b : HV.b};
+
+  if (tl3) {  // ---- CALPUV9C up to 1000 CONTINUE (calpuv9c.f90:128-311) ----
+    if (ISDRY > 0 && NDRYSTP < 0)  // :154-160
+      for (int L = 2; L <= la; ++L) QDWASTE[L] = 0.;
+    for_domains(c, [&](int L) {  // :164-204
+      if (baro) {  // external density gradients, blended with the last ones
+        const int LW = LWC[L], LS = LSC[L];
+        FPGX[L] = prm->rold * FPGX[L] +
+                  prm->rnew * (-SBX[L] * HU[L] * GP *
+                               ((BI2[L] + BI2[LW]) * (HP[L] - HP[LW]) +
+                                2.0 * HU[L] * (BI1[L] - BI1[LW]) +
+                                (BE[L] + BE[LW]) * (BELV[L] - BELV[LW])));
+        FPGY[L] = prm->rold * FPGY[L] +
+                  prm->rnew * (-SBY[L] * HV[L] * GP *
+                               ((BI2[L] + BI2[LS]) * (HP[L] - HP[LS]) +
+                                2.0 * HV[L] * (BI1[L] - BI1[LS]) +
+                                (BE[L] + BE[LS]) * (BELV[L] - BELV[LS])));
+      }
+      if (ISTL == 2) {
+        HUT[L] = 0.5 * (HU[L] + H1U[L]);
+        HVT[L] = 0.5 * (HV[L] + H1V[L]);
+      } else {
+        HUT[L] = HU[L];
+        HVT[L] = HV[L];
+      }
+    });
+    for_domains(c, [&](int L) {  // :206-222 explicit transports from level n-1
+      const int LS = LSC[L], LW = LWC[L];
+      const double FPGXE = baro ? FPGX[L] : 0., FPGYE = baro ? FPGY[L] : 0.;
+      FUHDYE[L] = U1[L] - DELTD2 * SUB[L] * HRUO[L] * HUT[L] * (P1T[L] - P1T[LW]) +
+                  SUB[L] * DELT * DXIU[L] *
+                      (DXYU[L] * (TSX1[L] - RITB1 * TBX1[L]) + FCAXE[L] + FPGXE -
+                       SNLT * FXE[L]);
+      FVHDXE[L] = V1[L] - DELTD2 * SVB[L] * HRVO[L] * HVT[L] * (P1T[L] - P1T[LS]) +
+                  SVB[L] * DELT * DYIV[L] *
+                      (DXYV[L] * (TSY1[L] - RITB1 * TBY1[L]) - FCAYE[L] + FPGYE -
+                       SNLT * FYE[L]);
+    });
+    if (ISDRY > 0)  // :246-262
+      for_domains(c, [&](int L) {
+        ISCDRY[L] = 0;
+        SUB1[L] = SUB[L];
+        SVB1[L] = SVB[L];
+        SUB[L] = SUBO[L];
+        SVB[L] = SVBO[L];
+        SBX[L] = SBXO[L];
+        SBY[L] = SBYO[L];
+        OLDMASK[L] = LMASKDRY[L];
+      });
+    for_domains(c, [&](int L) {  // :268-280
+      const double C1 = 0.5 * G;
+      const int LE = LEC[L], LN = LNC[L];
+      FP1[L] = DELTI * DXYP[L] * P1T[L] - C1 * (U1[LE] - U1[L] + V1[LN] - V1[L]);
+    });
+    if (ISTL == 3)  // :282-311 advance the time levels (the 2D ones)
+      for_domains(c, [&](int L) {
+        if (prm->nctbc == 1) {
+          UHDYE[L] = 0.5 * UHDYE[L];
+          VHDXE[L] = 0.5 * VHDXE[L];
+        }
+        U2[L] = U1[L];
+        V2[L] = V1[L];
+        U1[L] = UHDYE[L];
+        V1[L] = VHDXE[L];
+        P1T[L] = P[L];
+        H1U[L] = HU[L];
+        H1V[L] = HV[L];
+        H2P[L] = H1P[L];
+        H1P[L] = HP[L];
+      });
+  } else  // ---- first domain loop (:164-293) ----
   for_domains(c, [&](int L) {
     if (ISDRY > 0) {  // :172-190
       ISCDRY[L] = 0;
@@ -572,14 +672,15 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
                              SVB[LN] * FVHDXE[LN] - SVB[L] * FVHDXE[L] -
                              2.0 * QSUME[L]);
       C1 = -0.5 * DELTD2 * G;
-      CS[L] = C1 * SVB[L] * HRVO[L] * RCY[L] * HV[L];
-      CW[L] = C1 * SUB[L] * HRUO[L] * RCX[L] * HU[L];
-      CE[L] = C1 * SUB[LE] * HRUO[LE] * RCX[LE] * HU[LE];
-      CN[L] = C1 * SVB[LN] * HRVO[LN] * RCY[LN] * HV[LN];
+      CS[L] = C1 * SVB[L] * HRVO[L] * RCY[L] * HVc[L];  // HVTMP in CALPUV9C (calpuv9c.f90:369-379)
+      CW[L] = C1 * SUB[L] * HRUO[L] * RCX[L] * HUc[L];
+      CE[L] = C1 * SUB[LE] * HRUO[LE] * RCX[LE] * HUc[LE];
+      CN[L] = C1 * SVB[LN] * HRVO[LN] * RCY[LN] * HVc[LN];
       CC[L] = DELTI * DXYP[L] - CS[L] - CW[L] - CE[L] - CN[L];
     });
 
-    // :349 SETOPENBC(DELTD2,DELTI,HU,HV)  (setopenbc.f90:1-206)
+    // :349 SETOPENBC(DELTD2,DELTI,HU,HV)  (setopenbc.f90:1-206); CALPUV9C passes
+    // HUTMP, HVTMP (calpuv9c.f90:389)
     if (!c->lobcs.empty()) {
       const double D_LTD2 = DELTD2, DE_TI = DELTI;
       const double HDRY2 = 0.2 * HDRY;
@@ -612,11 +713,11 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
           FP[L] = target(s, f->pser[EFDC_XM_OBC_W], ll, L);
           const int LE = LEC[L];
           if (s.ispb[ll] == 1 || s.ispb[ll] == 2) {
-            const double CET = 0.5 * D_LTD2 * G * HRUO[LE] * RCX[LE] * HU[LE];
-            const double TMP = D_LTD2 * std::sqrt(G * HU[LE]) * DXIU[LE];
+            const double CET = 0.5 * D_LTD2 * G * HRUO[LE] * RCX[LE] * HUc[LE];
+            const double TMP = D_LTD2 * std::sqrt(G * HUc[LE]) * DXIU[LE];
             CC[L] = CET * (1. + TMP) / TMP;
             CE[L] = -CET;
-            FP[L] = CET * (2. * FP[L] - std::sqrt(G * HU[LE]) * FUHDYE[LE] * DYIU[LE] / HU[LE]) / TMP;
+            FP[L] = CET * (2. * FP[L] - std::sqrt(G * HUc[LE]) * FUHDYE[LE] * DYIU[LE] / HUc[LE]) / TMP;
           } else {
             const double FP1G = FP[L] / G - HDRY2;
             double CET;
@@ -625,7 +726,7 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
               CET = 0.;
               LOPENBCDRY[L] = 1;
             } else {
-              CET = 0.5 * D_LTD2 * G * HRUO[LE] * RCX[LE] * HU[LE];
+              CET = 0.5 * D_LTD2 * G * HRUO[LE] * RCX[LE] * HUc[LE];
             }
             FP[LE] = FP[LE] + CET * FP[L];
             FP[L] = DE_TI * DXYP[L] * FP[L];
@@ -641,11 +742,11 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
           if (LOPENBCDRY[L]) continue;
           FP[L] = target(s, f->pser[EFDC_XM_OBC_E], ll, L);
           if (s.ispb[ll] == 1 || s.ispb[ll] == 2) {
-            const double CWT = 0.5 * D_LTD2 * G * HRUO[L] * RCX[L] * HU[L];
-            const double TMP = D_LTD2 * std::sqrt(G * HU[L]) * DXIU[L];
+            const double CWT = 0.5 * D_LTD2 * G * HRUO[L] * RCX[L] * HUc[L];
+            const double TMP = D_LTD2 * std::sqrt(G * HUc[L]) * DXIU[L];
             CC[L] = CWT * (1. + TMP) / TMP;
             CW[L] = -CWT;
-            FP[L] = CWT * (2. * FP[L] + std::sqrt(G * HU[L]) * FUHDYE[L] * DYIU[L] / HU[L]) / TMP;
+            FP[L] = CWT * (2. * FP[L] + std::sqrt(G * HUc[L]) * FUHDYE[L] * DYIU[L] / HUc[L]) / TMP;
           } else {
             const int LW = LWC[L];
             const double FP1G = FP[L] / G - HDRY2;
@@ -655,7 +756,7 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
               CWT = 0.;
               LOPENBCDRY[L] = 1;
             } else {
-              CWT = 0.5 * D_LTD2 * G * HRUO[L] * RCX[L] * HU[L];
+              CWT = 0.5 * D_LTD2 * G * HRUO[L] * RCX[L] * HUc[L];
             }
             FP[LW] = FP[LW] + CWT * FP[L];
             FP[L] = DE_TI * DXYP[L] * FP[L];
@@ -672,11 +773,11 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
           if (LOPENBCDRY[L]) continue;
           FP[L] = target(s, f->pser[EFDC_XM_OBC_S], ll, L);
           if (s.ispb[ll] == 1 || s.ispb[ll] == 2) {
-            const double CNT = 0.5 * D_LTD2 * G * HRVO[LN] * RCY[LN] * HV[LN];
-            const double TMP = D_LTD2 * std::sqrt(G * HV[LN]) * DYIV[LN];
+            const double CNT = 0.5 * D_LTD2 * G * HRVO[LN] * RCY[LN] * HVc[LN];
+            const double TMP = D_LTD2 * std::sqrt(G * HVc[LN]) * DYIV[LN];
             CC[L] = CNT * (1. + TMP) / TMP;
             CN[L] = -CNT;
-            FP[L] = CNT * (2. * FP[L] - std::sqrt(G * HV[LN]) * FVHDXE[LN] * DXIV[LN] / HV[LN]) / TMP;
+            FP[L] = CNT * (2. * FP[L] - std::sqrt(G * HVc[LN]) * FVHDXE[LN] * DXIV[LN] / HVc[LN]) / TMP;
           } else {
             const double FP1G = FP[L] / G - HDRY2;
             double CNT;
@@ -685,7 +786,7 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
               CNT = 0.;
               LOPENBCDRY[L] = 1;
             } else {
-              CNT = 0.5 * D_LTD2 * G * HRVO[LN] * RCY[LN] * HV[LN];
+              CNT = 0.5 * D_LTD2 * G * HRVO[LN] * RCY[LN] * HVc[LN];
             }
             FP[LN] = FP[LN] + CNT * FP[L];
             FP[L] = DE_TI * DXYP[L] * FP[L];
@@ -702,11 +803,11 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
           if (LOPENBCDRY[L]) continue;
           FP[L] = target(s, f->pser[EFDC_XM_OBC_N], ll, L);
           if (s.ispb[ll] == 1 || s.ispb[ll] == 2) {
-            const double CST = 0.5 * D_LTD2 * G * HRVO[L] * RCY[L] * HV[L];
-            const double TMP = D_LTD2 * std::sqrt(G * HV[L]) * DYIV[L];
+            const double CST = 0.5 * D_LTD2 * G * HRVO[L] * RCY[L] * HVc[L];
+            const double TMP = D_LTD2 * std::sqrt(G * HVc[L]) * DYIV[L];
             CC[L] = CST * (1. + TMP) / TMP;
             CS[L] = -CST;
-            FP[L] = CST * (2. * FP[L] + std::sqrt(G * HV[L]) * FVHDXE[L] * DXIV[L] / HV[L]) / TMP;
+            FP[L] = CST * (2. * FP[L] + std::sqrt(G * HVc[L]) * FVHDXE[L] * DXIV[L] / HVc[L]) / TMP;
           } else {
             const double FP1G = FP[L] / G - HDRY2;
             double CST;
@@ -715,7 +816,7 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
               CST = 0.;
               LOPENBCDRY[L] = 1;
             } else {
-              CST = 0.5 * D_LTD2 * G * HRVO[L] * RCY[L] * HV[L];
+              CST = 0.5 * D_LTD2 * G * HRVO[L] * RCY[L] * HVc[L];
             }
             FP[LS] = FP[LS] + CST * FP[L];
             FP[L] = DE_TI * DXYP[L] * FP[L];
@@ -780,8 +881,8 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
     // :416-437 face discharges
     for_domains(c, [&](int L) {
       const int LS = LSC[L], LW = LWC[L];
-      UHDYE[L] = SUB[L] * (FUHDYE[L] - DELTD2 * HRUO[L] * RCX[L] * HU[L] * (P[L] - P[LW]));
-      VHDXE[L] = SVB[L] * (FVHDXE[L] - DELTD2 * HRVO[L] * RCY[L] * HV[L] * (P[L] - P[LS]));
+      UHDYE[L] = SUB[L] * (FUHDYE[L] - DELTD2 * HRUO[L] * RCX[L] * HUc[L] * (P[L] - P[LW]));
+      VHDXE[L] = SVB[L] * (FVHDXE[L] - DELTD2 * HRVO[L] * RCY[L] * HVc[L] * (P[L] - P[LS]));
     });
     for_domains(c, [&](int L) {
       UHE[L] = UHDYE[L] * DYIU[L];
@@ -812,12 +913,23 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
       }
     }
     // :466-486 continuity
-    for_domains(c, [&](int L) {
-      const int LE = LEC[L], LN = LNC[L];
-      HP[L] = H1P[L] + DELTD2 * DXYIP[L] *
-                           (2. * QSUME[L] - (UHDYE[LE] + UHDY1E[LE] - UHDYE[L] - UHDY1E[L] +
-                                             VHDXE[LN] + VHDX1E[LN] - VHDXE[L] - VHDX1E[L]));
-    });
+    if (!tl3) {
+      for_domains(c, [&](int L) {
+        const int LE = LEC[L], LN = LNC[L];
+        HP[L] = H1P[L] + DELTD2 * DXYIP[L] *
+                             (2. * QSUME[L] - (UHDYE[LE] + UHDY1E[LE] - UHDYE[L] - UHDY1E[L] +
+                                               VHDXE[LN] + VHDX1E[LN] - VHDXE[L] - VHDX1E[L]));
+      });
+    } else {  // calpuv9c.f90:500-525: from level n-1 (ISTL_ = 3) or n (ISTL_ = 2)
+      const F<double> HB = (ISTL == 3) ? H2P : H1P, UB = (ISTL == 3) ? U2 : U1,
+                      VB = (ISTL == 3) ? V2 : V1;
+      for_domains(c, [&](int L) {
+        const int LE = LEC[L], LN = LNC[L];
+        HP[L] = HB[L] + DELT * DXYIP[L] *
+                            (QSUME[L] - 0.5 * (UHDYE[LE] + UB[LE] - UHDYE[L] - UB[L] +
+                                               VHDXE[LN] + VB[LN] - VHDXE[L] - VB[L]));
+      });
+    }
     // :489-535 open boundaries
     for (int L : c->lobcs) {
       HP[L] = GI * P[L] - BELV[L];
@@ -863,9 +975,15 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
     // :574-603 legacy drying check, ISDRY 1..97 (serial in the reference)
     if (ISDRY > 0 && ISDRY < 98) {
       int ICORDRY = 0;
+      const double HDRY90 = 0.9 * HDRY, HDRY10 = 0.1 * HDRY;
       for (int L = 2; L <= la; ++L) {
         const int LE = LEC[L], LN = LNC[L];
-        if (HP[L] <= HDRY) {
+        bool dry = HP[L] <= HDRY;
+        if (tl3) {  // calpuv9c.f90:628-662: only a cell below HDRY that is not rising fast
+          const double HPPMC = (ISTL == 3) ? H2P[L] : H1P[L];
+          dry = HP[L] < HDRY && (HP[L] < HDRY90 || HPPMC < HDRY) && HP[L] < (HPPMC + HDRY10);
+        }
+        if (dry) {
           if (ISCDRY[L] == 0) {
             ISCDRY[L] = 1;
             ICORDRY = 1;
@@ -893,11 +1011,13 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
         const int LW = LWC[L], LE = LEC[L], LS = LSC[L], LN = LNC[L];
         if (HP[L] <= HDRY) {
           const double SUBW = SUB[L], SUBE = SUB[LE], SVBS = SVB[L], SVBN = SVB[LN];
-          const double DHPDT = (HP[L] - H1P[L]);
+          // HPPMC: H2P in CALPUV9C(3) (calpuv9c.f90:679-686), else H1P
+          const double HPPMC = (ISTL == 3) ? H2P[L] : H1P[L];
+          const double DHPDT = (HP[L] - HPPMC);
           if (DHPDT > 0.0) {
             SUB[L] = 0.0; SUB[LE] = 0.0; SVB[L] = 0.0; SVB[LN] = 0.0;
             SBX[L] = 0.0; SBX[LE] = 0.0; SBY[L] = 0.0; SBY[LN] = 0.0;
-            const double DHPDT2 = (HDRY - H1P[L]) * 0.01;
+            const double DHPDT2 = (HDRY - HPPMC) * 0.01;
             if (DHPDT > DHPDT2) {
               if (SUBO[L] > 0.5)
                 if (UHDYE[L] > 0.0 && HP[LW] > HDRY2) { SUB[L] = SUBO[L]; SBX[L] = SBXO[L]; }
@@ -919,7 +1039,7 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
                 ICORDRY = 1;
               }
             }
-          } else if (HP[L] < HDRY90 || H1P[L] < HDRY) {
+          } else if (HP[L] < HDRY90 || HPPMC < HDRY) {
             SUB[L] = 0.0; SUB[LE] = 0.0; SVB[L] = 0.0; SVB[LN] = 0.0;
             SBX[L] = 0.0; SBX[LE] = 0.0; SBY[L] = 0.0; SBY[LN] = 0.0;
             if (ISCDRY[L] == 0) {
@@ -974,7 +1094,9 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
               H1P[L] = HP[L];
               HP[L] = 0.90 * HDRY;
               NATDRY[L] = 0;
-              QDWASTE[L] = DELTI * DXYP[L] * (HOLDTMP - HP[L]);
+              // CALPUV9C adds to the QDWASTE it zeroed at entry (calpuv9c.f90:919)
+              QDWASTE[L] = tl3 ? QDWASTE[L] + DELTI * DXYP[L] * (HOLDTMP - HP[L])
+                               : DELTI * DXYP[L] * (HOLDTMP - HP[L]);
               VDWASTE[L] = VDWASTE[L] + DXYP[L] * (HOLDTMP - HP[L]);
               nnatdry_flag[L] = 1;
               ++n_wasted;
@@ -1012,11 +1134,12 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
     });
   }
   // :1003-1025 wasted cells: H1P reset, QDWASTE kept only with ISBAL>0
+  // (CALPUV9C resets H1P only, calpuv9c.f90:1047-1058)
   if (n_wasted > 0) {
     for (int L = 2; L <= la; ++L)
       if (nnatdry_flag[L]) {
         H1P[L] = 0.90 * HDRY;
-        if (prm->isbal == 0) QDWASTE[L] = 0.0;
+        if (prm->isbal == 0 && !tl3) QDWASTE[L] = 0.0;
       }
   }
   // NEGDEP check (negdep.f90:34-45)
