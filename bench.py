@@ -77,6 +77,9 @@ def parse():
     ap.add_argument("--wetdry-members", type=int, default=64)
     ap.add_argument("--wetdry-steps", type=int, default=20,
                     help="wetting/drying batch side measurement, 1024x1024 flats (0: skip)")
+    ap.add_argument("--tl3-calls", type=int, default=40,
+                    help="three-time-level (CALPUV9C) side measurement on the ensemble: timed "
+                         "calls of the leapfrog/correction schedule (0: skip)")
     ap.add_argument("--calib-steps", type=int, default=200,
                     help="adjoint calibration side measurement, 512x512 basin (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
@@ -653,6 +656,48 @@ def ours(args):
                               "cells_polynomial": kt.ncells_poly},
             "fp64_matvec": {"ms_per_launch": kt64.ms_matvec, "bytes_per_launch": 56.0 * kt.ncells,
                             "achieved": 56.0 * kt.ncells / (kt64.ms_matvec * 1e-3) / 1e9}}
+    # ---------------- three time levels (CALPUV9C) on the same ensemble ----------------
+    tl3_res = None
+    if args.tl3_calls > 0 and args.workload == "ensemble":
+        warm3 = 3
+        sched = S.three_level_schedule(10 * (args.tl3_calls + warm3), 4)[:warm3 + args.tl3_calls]
+        lv = (("p1", "p"), ("h2p", "hp"), ("h1p", "hp"), ("uhdy1e", "uhdye"), ("uhdy2e", "uhdye"),
+              ("vhdx1e", "vhdxe"), ("vhdx2e", "vhdxe"), ("h1u", "hu"), ("h1v", "hv"),
+              ("tsx1", "tsx"), ("tsy1", "tsy"), ("tbx1", "tbx"), ("tby1", "tby"))
+
+        def run3(prec):
+            st3 = []
+            for s in scns:  # level n-1 = level n at the start (scenario.add_three_levels)
+                d = dict(s.state)
+                for dst, src in lv:
+                    d[dst] = s.state[src].copy()
+                st3.append(d)
+            bs.upload(st3)
+            del st3
+            ms, it = [], np.zeros(M, np.int64)
+            for i, (n, istl, nctbc, rold, rnew) in enumerate(sched):
+                prm = [X.make_params(S.three_level_params(s.params, istl, nctbc, rold, rnew),
+                                     n=n, tn=s.tn(n), precision=prec) for s in scns]
+                with Timer(torch, stream) as tm:
+                    sts = bs.step_device(prm)
+                for st in sts:
+                    assert st.status in (X.OK, X.NEG_DEPTH), st.as_dict()
+                if i >= warm3:
+                    ms.append(tm.ms)
+                    it += np.array([st.iters_total for st in sts], dtype=np.int64)
+            return ms, it
+
+        ms64, it64_3 = run3(X.PREC_FP64)
+        msmx, _ = run3(X.PREC_MIXED)
+        t64_3, tmx_3 = max_over_ranks(sum(ms64) / 1e3, sum(msmx) / 1e3)
+        c3, = sum_over_ranks(float(np.dot(cells, it64_3)))
+        tl3_res = {"calls": args.tl3_calls,
+                   "schedule": "HDMT order: ISTL=3 leapfrog over 2*DT, ISTL=2 correction after "
+                               "every 4th, NCTBC/ROLD/RNEW as HDMT sets them",
+                   "value": c3 / tmx_3, "fp64_value": c3 / t64_3,
+                   "ms_per_call": 1000 * tmx_3 / args.tl3_calls,
+                   "fp64_ms_per_call": 1000 * t64_3 / args.tl3_calls,
+                   "speedup_vs_fp64": t64_3 / tmx_3}
     bs.close()
     del bs
 
@@ -751,6 +796,7 @@ def ours(args):
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(rmx["launches"]), "clocks": clocks,
             "single_domain": single,
+            "three_level": tl3_res,
             "wetdry": wd_res,
             "calibration": calib_res,
         }
