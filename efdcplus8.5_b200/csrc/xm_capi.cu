@@ -285,7 +285,7 @@ int upload_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
     }
     if ((rc = compute_after_copies(c))) return rc;
     xm::launch_scatter(c->stream, c->jobs_d + g0, int(g1 - g0), c->lidx, c->tile_member, c->moff,
-                       c->mlc, c->nslot);
+                       c->mlc, 0, c->nslot);
     CK(cudaGetLastError());
   }
   CK(cudaStreamSynchronize(c->stream));
@@ -323,7 +323,7 @@ int download_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
     const size_t g1 = std::min(xs.size(), g0 + NSTAGE);
     if (g0 > 0 && (rc = compute_after_copies(c))) return rc;  // the buffers were copied out
     xm::launch_gather(c->stream, c->jobs_d + g0, int(g1 - g0), c->lidx, c->tile_member, c->moff,
-                      c->nslot);
+                      0, c->nslot);
     CK(cudaGetLastError());
     if ((rc = copies_after_compute(c))) return rc;
     for (size_t j = g0; j < g1; ++j) {
@@ -1302,7 +1302,7 @@ int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int l
     if ((rc = scaled_system(c))) return rc;
   }
   if (f[0].hpi || f[0].hui || f[0].hvi) {  // 1/HP, 1/HU, 1/HV are formed on request
-    xm::launch_reciprocals(c->L(), c->S, c->X);
+    xm::launch_reciprocals(c->L(), c->S, c->X, 1, c->ntile);
     CK(cudaGetLastError());
   }
   // the wet/dry lists need the mask at exit and at entry (OLDMASK)
@@ -1355,14 +1355,13 @@ int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int l
 }
 }  // namespace
 
-int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
-                                  efdc_xm_stats *stats) {
-  if (!c || !prm || !stats) {
-    set_error("efdc_xm_step_device: NULL argument");
-    return EFDC_XM_BAD_ARGUMENT;
-  }
+}  // extern "C"
+
+namespace {
+// The argument checks of a device-resident step of every member (the stats
+// are filled with the status on failure).
+int validate_step(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats) {
   const int M = c->M;
-  std::memset(stats, 0, sizeof(efdc_xm_stats) * M);
   for (int m = 0; m < M; ++m) {
     if (!(prm[m].delt > 0) || prm[m].iterm < 1 || prm[m].g <= 0) {
       set_error("efdc_xm_step_device: member %d: need DELT > 0, G > 0, ITERM >= 1", m);
@@ -1392,12 +1391,6 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
     fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
     return EFDC_XM_BAD_ARGUMENT;
   }
-  CK(cudaSetDevice(c->device));
-  const bool mixed = prm[0].precision == EFDC_XM_PREC_MIXED;
-  c->mxview = xm::SysView{c->X.fp, c->X.cc, c->X.cs, c->X.cw, c->X.ce, c->X.cn, 1};
-  c->last_mixed = mixed;
-  c->sys_external = false;
-  c->step_baro = false;
   for (int m = 0; m < M; ++m)
     if ((prm[m].isdry > 0 && (c->wd_stale || c->sbxy_stale)) ||
         (prm[m].bsc > 1.E-6 && c->sbxy_stale)) {
@@ -1414,12 +1407,27 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
       fill_status(stats, M, EFDC_XM_BAD_ARGUMENT);
       return EFDC_XM_BAD_ARGUMENT;
     }
-    c->step_baro = true;
   }
+  return EFDC_XM_OK;
+}
+
+// One device-resident step of the members [m0, m1); the others take no part
+// (every kernel skips them) and keep their state and stats.
+int step_range(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats, int m0, int m1) {
+  const int M = c->M;
+  const int istl = prm[m0].tl3_istl;  // 0: CALPUV2C; 3, 2: CALPUV9C(ISTL_)
+  CK(cudaSetDevice(c->device));
+  const bool mixed = prm[0].precision == EFDC_XM_PREC_MIXED;
+  c->mxview = xm::SysView{c->X.fp, c->X.cc, c->X.cs, c->X.cw, c->X.ce, c->X.cn, 1};
+  c->last_mixed = mixed;
+  c->sys_external = false;
+  c->step_baro = false;
+  for (int m = m0; m < m1; ++m) c->step_baro |= prm[m].bsc > 1.E-6;
   const xm::Launch l = c->L();
   bool any_isdry = false, any_legacy = false, any99 = false, any_waste = false;
-  std::vector<int> ncordry(M, 0), status(M, EFDC_XM_OK), max_sweeps(M);
-  for (int m = 0; m < M; ++m) {
+  std::vector<int> ncordry(M, 0), status(M, EFDC_XM_OK), max_sweeps(M, 500);
+  for (int m = 0; m < M; ++m) c->act_h[m] = 0;
+  for (int m = m0; m < m1; ++m) {
     Member &mb = c->mem[m];
     c->sc_h[m] = make_scalars(mb, &prm[m]);
     mb.last_n = prm[m].n;
@@ -1439,18 +1447,14 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
   int rc = write_act(c);
   if (rc) return rc;
   if (istl == 0) {
-    // time levels by buffer swap: after it the *1 buffers hold the entry values
-    // (UHDY1E=UHDYE, VHDX1E=VHDXE, H1P=HP, calpuv2c.f90:256-264) and the
-    // others are rewritten for every water cell before they are read
-    std::swap(c->X.uhdye, c->X.uhdy1e);
-    std::swap(c->X.vhdxe, c->X.vhdx1e);
-    std::swap(c->X.hp, c->X.h1p);
+    // k_begin copies UHDY1E=UHDYE, VHDX1E=VHDXE, H1P=HP (calpuv2c.f90:256-264)
+    // cell by cell
     set_views(c, 0);
-    xm::launch_chan_entry(l, c->S, c->X);
-    xm::launch_begin(l, c->S, c->X);
+    xm::launch_chan_entry(l, c->S, c->X, c->act);
+    xm::launch_begin(l, c->S, c->X, c->act);
   } else {
-    xm::launch_chan_entry(l, c->S, c->X);
-    xm::launch_begin3(l, c->S, c->X);
+    xm::launch_chan_entry(l, c->S, c->X, c->act);
+    xm::launch_begin3(l, c->S, c->X, c->act);
     if (istl == 3) {
       // calpuv9c.f90:282-311 by buffer rotation, UHDY2E <- UHDY1E <- UHDYE and
       // H2P <- H1P <- HP (UHDYE and HP are rewritten for every water cell
@@ -1466,7 +1470,7 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
     }
     set_views(c, istl);
   }
-  if (any_isdry) xm::launch_obc_reset(l, c->S, c->B, c->X);
+  if (any_isdry) xm::launch_obc_reset(l, c->S, c->B, c->X, c->act);
   CK(cudaGetLastError());
   for (int sweep = 0;; ++sweep) {  // 1000 CONTINUE, for the members still sweeping
     xm::launch_sweep_reset(l, c->ctl, c->act, M);
@@ -1483,7 +1487,7 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
     // a member whose solve failed stops here, before the back-substitution
     bool dropped = false;
     int nact = 0;
-    for (int m = 0; m < M; ++m) {
+    for (int m = m0; m < m1; ++m) {
       if (!c->act_h[m]) continue;
       const Ctl &k = c->ctl_h[m];
       efdc_xm_stats &s = stats[m];
@@ -1522,7 +1526,7 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
       xm::launch_wetdry(l, c->S, c->X, c->ctl, c->act, any_legacy, any99);
       CK(cudaGetLastError());
       if ((rc = read_ctl(c))) return rc;
-      for (int m = 0; m < M; ++m) {
+      for (int m = m0; m < m1; ++m) {
         if (!c->act_h[m]) continue;
         const int isd = prm[m].isdry;
         int next = 0;
@@ -1544,7 +1548,7 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
   }
   // finalisation of the members whose sweeps ended normally
   bool any_fin = false;
-  for (int m = 0; m < M; ++m) {
+  for (int m = m0; m < m1; ++m) {
     c->act_h[m] = (status[m] == EFDC_XM_OK) ? 1 : 0;
     any_fin |= c->act_h[m] != 0;
   }
@@ -1555,7 +1559,7 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
   }
   if ((rc = read_ctl(c))) return rc;
   if (istl == 0) c->tl3_ready = false;  // CALPUV2C does not keep the three levels
-  for (int m = 0; m < M; ++m) {
+  for (int m = m0; m < m1; ++m) {
     efdc_xm_stats &s = stats[m];
     const Ctl &k = c->ctl_h[m];
     s.n_negdep = k.nneg;
@@ -1567,8 +1571,24 @@ int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
     if (status[m] == EFDC_XM_OK && k.nneg > 0) status[m] = EFDC_XM_NEG_DEPTH;
     s.status = status[m];
   }
-  return overall_status(stats, M);
+  return overall_status(stats + m0, m1 - m0);
 }
+}  // namespace
+
+extern "C" {
+
+int32_t efdc_xm_step_device_batch(efdc_xm_ctx *c, const efdc_xm_params *prm,
+                                  efdc_xm_stats *stats) {
+  if (!c || !prm || !stats) {
+    set_error("efdc_xm_step_device: NULL argument");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  std::memset(stats, 0, sizeof(efdc_xm_stats) * c->M);
+  const int rc = validate_step(c, prm, stats);
+  if (rc) return rc;
+  return step_range(c, prm, stats, 0, c->M);
+}
+
 
 int32_t efdc_xm_step_batch(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
                            efdc_xm_stats *stats) {

@@ -33,9 +33,10 @@ constexpr int CH_NT = 128;  // threads per CTA of the member kernels
 // CALPUV9C (calpuv9c.f90:128-141): QCHANUT = QCHANUN, and for ISTL_ = 3
 // QCHANUN = QCHANU; its P1 is P at entry after the advance of ISTL_ = 3, the
 // caller's P1 for ISTL_ = 2.
-__global__ void k_chan_entry(DevStatic S, DevState X) {
+__global__ void k_chan_entry(DevStatic S, DevState X, const int *act) {
   const DevChan &C = S.ch;
   MEMBER_LOOP {
+    if (!act[m]) continue;
     const int istl = S.sc[m].istl;
     const double *P1 = istl == 2 ? X.p1 : X.p;
     for (int k = C.cstart[m]; k < C.cstart[m + 1]; ++k) {
@@ -345,9 +346,9 @@ __global__ void k_chan_mvmx(DevStatic S, DevSystem Y, const Ctl *ctl, double *pa
 
 static int member_grid(const DevStatic &S) { return (S.nmember + CH_NT - 1) / CH_NT; }
 
-void launch_chan_entry(const Launch &l, const DevStatic &S, const DevState &X) {
+void launch_chan_entry(const Launch &l, const DevStatic &S, const DevState &X, const int *act) {
   if (!l.chan) return;
-  k_chan_entry<<<member_grid(S), CH_NT, 0, l.stream>>>(S, X);
+  k_chan_entry<<<member_grid(S), CH_NT, 0, l.stream>>>(S, X, act);
   count_launches(1);
 }
 void launch_chan_sub(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,

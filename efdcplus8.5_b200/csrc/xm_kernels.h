@@ -32,13 +32,13 @@ struct CopyJob {
   int is_int;              // 0 double, 1 LOGICAL (0/1), 2 raw int, 3 double water-only
 };
 
-void launch_begin(const Launch &l, const DevStatic &S, const DevState &X);
+void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const int *act);
 // CALPUV9C: the kernels up to the time-level advance, and the copies of the advance
-void launch_begin3(const Launch &l, const DevStatic &S, const DevState &X);
+void launch_begin3(const Launch &l, const DevStatic &S, const DevState &X, const int *act);
 void launch_advance3(const Launch &l, const DevStatic &S, const DevState &X);
 void launch_put(cudaStream_t st, const int *idx, const double *val, int n, double *dst);
 // sub-grid channels (xm_chan.cu); each does nothing unless l.chan
-void launch_chan_entry(const Launch &l, const DevStatic &S, const DevState &X);
+void launch_chan_entry(const Launch &l, const DevStatic &S, const DevState &X, const int *act);
 void launch_chan_sub(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
                      const int *act, int first_sweep);
 void launch_chan_res64(const Launch &l, const DevStatic &S, const DevSystem &Y, const double *P,
@@ -58,7 +58,8 @@ void launch_assemble(const Launch &l, const DevStatic &S, const DevState &X, Ctl
                      const int *act);
 void launch_obc(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B, Ctl *ctl,
                 const int *act, bool serial, int write_cross);
-void launch_obc_reset(const Launch &l, const DevStatic &S, const DevObc &B, const DevState &X);
+void launch_obc_reset(const Launch &l, const DevStatic &S, const DevObc &B, const DevState &X,
+                      const int *act);
 void launch_scale(const Launch &l, const DevStatic &S, const DevState &X, const DevSystem &Y,
                   Ctl *ctl, const int *act, int mixed, int write_cross);
 void launch_solve_reset(const Launch &l, Ctl *ctl, Glob *glob, const int *act, int nmember);
@@ -91,11 +92,13 @@ void launch_wetdry(const Launch &l, const DevStatic &S, const DevState &X, Ctl *
                    const int *act, bool any_legacy, bool any99);
 void launch_final(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
                   const int *act, bool any_waste);
-void launch_reciprocals(const Launch &l, const DevStatic &S, const DevState &X);
+void launch_reciprocals(const Launch &l, const DevStatic &S, const DevState &X, int t0, int t1);
+// slots [d0, d1)
 void launch_scatter(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx,
-                    const int *tile_member, const long long *moff, const int *mlc, int nslot);
+                    const int *tile_member, const long long *moff, const int *mlc, int d0,
+                    int d1);
 void launch_gather(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx,
-                   const int *tile_member, const long long *moff, int nslot);
+                   const int *tile_member, const long long *moff, int d0, int d1);
 void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                         int mixed);
 

@@ -70,11 +70,12 @@ __device__ __forceinline__ void baro_faces(const DevStatic &S, const DevState &X
 // cell with ISDRY = 0, else the cells with LMASKDRY).  The reference's two
 // loops from the top layer down are one here (the same additions in the same
 // order).
-__global__ void __launch_bounds__(NT) k_calebi(DevStatic S, DevState X, int ntile) {
+__global__ void __launch_bounds__(NT) k_calebi(DevStatic S, DevState X, int ntile,
+                                              const int *act) {
   const DevBaro &Bc = S.baro;
   TILE_LOOP(ntile) {
     TILE_MEMBER(S);
-    if (!c.baro) continue;
+    if (!c.baro || !act[m]) continue;
     const int d = tile * TILE + threadIdx.x;
     if (S.kind[d] == LAND) continue;
     if (c.isdry > 0 && !X.lmaskdry[d]) continue;
@@ -130,16 +131,19 @@ __device__ __forceinline__ double assemble_cell(const DevStatic &S, const DevSta
 }
 
 // ---------------------------------------------------------------------------
-// calpuv2c.f90:164-293: switches, explicit transports, FP1.  The host swapped
-// UHDYE<->UHDY1E, VHDXE<->VHDX1E and HP<->H1P before this kernel, so the *1
-// buffers hold the values at entry (the time-level advance :256-264).
+// calpuv2c.f90:164-293: switches, explicit transports, FP1, and the time-level
+// advance of the 2D arrays this library owns (UHDY1E=UHDYE, VHDX1E=VHDXE,
+// H1P=HP, :256-264) as per-cell copies, so that any subset of the members
+// can step (act).
 // BARO: a member of the batch has baroclinic terms; the instance without them
 // is held to 32 registers (8 CTAs per SM), which sizes the grid of every cell
 // kernel (occupancy_blocks_per_sm).
 template <bool BARO>
-__global__ void __launch_bounds__(NT, BARO ? 4 : 8) k_begin(DevStatic S, DevState X, int ntile) {
+__global__ void __launch_bounds__(NT, BARO ? 4 : 8) k_begin(DevStatic S, DevState X, int ntile,
+                                                           const int *act) {
   TILE_LOOP(ntile) {
     TILE_MEMBER(S);
+    if (!act[m]) continue;
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
     if (S.kind[d] == LAND) continue;
@@ -154,19 +158,21 @@ __global__ void __launch_bounds__(NT, BARO ? 4 : 8) k_begin(DevStatic S, DevStat
     }
     const double P = X.p[d];
     double FPGXE = 0., FPGYE = 0.;
-    if (BARO && c.baro)  // :192-201 (entry HP in the H1P buffer, HU, HV, SBX, SBY)
-      baro_faces(S, X, c, q, X.h1p, FPGXE, FPGYE);
-    X.fuhdye[d] = fuh_face(S, X, c, d, X.uhdy1e[d], X.hu[d], P, X.p[q.w], sub, FPGXE,
-                           X.tsx[d], X.tbx[d]);
-    X.fvhdxe[d] = fvh_face(S, X, c, d, X.vhdx1e[d], X.hv[d], P, X.p[q.s], svb, FPGYE,
-                           X.tsy[d], X.tby[d]);
+    if (BARO && c.baro)  // :192-201 (entry HP, HU, HV, SBX, SBY)
+      baro_faces(S, X, c, q, X.hp, FPGXE, FPGYE);
+    const double uh = X.uhdye[d], vh = X.vhdxe[d];
+    X.fuhdye[d] = fuh_face(S, X, c, d, uh, X.hu[d], P, X.p[q.w], sub, FPGXE, X.tsx[d], X.tbx[d]);
+    X.fvhdxe[d] = fvh_face(S, X, c, d, vh, X.hv[d], P, X.p[q.s], svb, FPGYE, X.tsy[d], X.tby[d]);
+    X.uhdy1e[d] = uh;
+    X.vhdx1e[d] = vh;
+    X.h1p[d] = X.hp[d];
     if (c.isdry > 0) {  // :246-253
       X.sub[d] = S.subo[d];
       X.svb[d] = S.svbo[d];
       X.sbx[d] = S.sbxo[d];
       X.sby[d] = S.sbyo[d];
     }
-    X.fp1[d] = fp1_cell(S, c, q, P, X.uhdy1e, X.vhdx1e);
+    X.fp1[d] = fp1_cell(S, c, q, P, X.uhdye, X.vhdxe);
   }
 }
 
@@ -387,9 +393,9 @@ __global__ void k_obc_serial(DevStatic S, DevState X, DevObc B, Ctl *ctl, const 
 }
 
 // calpuv2c.f90:150-157: LOPENBCDRY=.FALSE. on the open-boundary cells (ISDRY>0)
-__global__ void k_obc_reset(DevStatic S, DevObc B, DevState X) {
+__global__ void k_obc_reset(DevStatic S, DevObc B, DevState X, const int *act) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B.n; k += gridDim.x * blockDim.x)
-    if (S.sc[B.member[k]].isdry > 0) X.lopenbcdry[B.slot[k]] = 0;
+    if (act[B.member[k]] && S.sc[B.member[k]].isdry > 0) X.lopenbcdry[B.slot[k]] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1089,13 +1095,13 @@ __global__ void __launch_bounds__(NT) k_fin(DevStatic S, DevState X, int ntile, 
 // Host order <-> tile order.  A staging buffer holds every member's host array
 // back to back (member m at element offset moff[m], LC = mlc[m] elements).  A
 // land slot receives element LC of its member's array (the ghost value);
-// gathers write water slots only.
+// gathers write water slots only.  Both cover the slots [d0, d1).
 __global__ void k_scatter(const CopyJob *jobs, int njob, const int *lidx, const int *tile_member,
-                          const long long *moff, const int *mlc, int nslot) {
+                          const long long *moff, const int *mlc, int d0, int d1) {
   const int j = blockIdx.y;
   if (j >= njob) return;
   const CopyJob J = jobs[j];
-  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nslot; d += gridDim.x * blockDim.x) {
+  for (int d = d0 + blockIdx.x * blockDim.x + threadIdx.x; d < d1; d += gridDim.x * blockDim.x) {
     const int L = lidx[d];
     if (L < 2 && J.is_int == 3) continue;  // water-only: leave land slots as they are
     const int m = tile_member[d / TILE];
@@ -1110,11 +1116,11 @@ __global__ void k_scatter(const CopyJob *jobs, int njob, const int *lidx, const 
 }
 
 __global__ void k_gather(const CopyJob *jobs, int njob, const int *lidx, const int *tile_member,
-                         const long long *moff, int nslot) {
+                         const long long *moff, int d0, int d1) {
   const int j = blockIdx.y;
   if (j >= njob) return;
   const CopyJob J = jobs[j];
-  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nslot; d += gridDim.x * blockDim.x) {
+  for (int d = d0 + blockIdx.x * blockDim.x + threadIdx.x; d < d1; d += gridDim.x * blockDim.x) {
     const int L = lidx[d];
     if (L < 2) continue;
     const long long dst = moff[tile_member[d / TILE]] + L - 1;
@@ -1139,20 +1145,20 @@ void launch_put(cudaStream_t st, const int *idx, const double *val, int n, doubl
   count_launches(1);
 }
 
-void launch_begin(const Launch &l, const DevStatic &S, const DevState &X) {
+void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const int *act) {
   if (l.baro) {
-    k_calebi<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+    k_calebi<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
     count_launches(1);
   }
   if (l.baro)
-    k_begin<true><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+    k_begin<true><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
   else
-    k_begin<false><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+    k_begin<false><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
   count_launches(1);
 }
-void launch_begin3(const Launch &l, const DevStatic &S, const DevState &X) {
+void launch_begin3(const Launch &l, const DevStatic &S, const DevState &X, const int *act) {
   if (l.baro) {
-    k_calebi<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);  // calpuv9c.f90:145
+    k_calebi<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);  // calpuv9c.f90:145
     count_launches(1);
     k_begin3<true><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
   } else {
@@ -1183,9 +1189,10 @@ void launch_obc(const Launch &l, const DevStatic &S, const DevState &X, const De
   k_obc_asym<<<(B.n + NT - 1) / NT, NT, 0, l.stream>>>(S, X, B, ctl, act, write_cross);
   count_launches(2);
 }
-void launch_obc_reset(const Launch &l, const DevStatic &S, const DevObc &B, const DevState &X) {
+void launch_obc_reset(const Launch &l, const DevStatic &S, const DevObc &B, const DevState &X,
+                      const int *act) {
   if (B.n == 0) return;
-  k_obc_reset<<<(B.n + 255) / 256, 256, 0, l.stream>>>(S, B, X);
+  k_obc_reset<<<(B.n + 255) / 256, 256, 0, l.stream>>>(S, B, X, act);
   count_launches(1);
 }
 void launch_scale(const Launch &l, const DevStatic &S, const DevState &X, const DevSystem &Y,
@@ -1318,9 +1325,10 @@ void launch_final(const Launch &l, const DevStatic &S, const DevState &X, Ctl *c
   count_launches(1);
 }
 // HPI, HUI, HVI (calpuv2c.f90:896-906) from the final HP, HU, HV: outputs
-// only (nothing on the device reads them), formed when they are downloaded.
-__global__ void __launch_bounds__(NT) k_reciprocals(DevStatic S, DevState X, int ntile) {
-  TILE_LOOP(ntile) {
+// only (nothing on the device reads them), formed when they are downloaded;
+// tiles [t0, t1).
+__global__ void __launch_bounds__(NT) k_reciprocals(DevStatic S, DevState X, int t0, int t1) {
+  for (int tile = t0 + blockIdx.x; tile < t1; tile += gridDim.x) {
     const int d = tile * TILE + threadIdx.x;
     if (S.kind[d] == LAND) continue;
     X.hpi[d] = 1. / X.hp[d];
@@ -1328,23 +1336,25 @@ __global__ void __launch_bounds__(NT) k_reciprocals(DevStatic S, DevState X, int
     X.hvi[d] = 1. / X.hv[d];
   }
 }
-void launch_reciprocals(const Launch &l, const DevStatic &S, const DevState &X) {
-  k_reciprocals<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+void launch_reciprocals(const Launch &l, const DevStatic &S, const DevState &X, int t0, int t1) {
+  if (t1 <= t0) return;
+  k_reciprocals<<<std::min(l.grid, t1 - t0), NT, 0, l.stream>>>(S, X, t0, t1);
   count_launches(1);
 }
 
 void launch_scatter(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx,
-                    const int *tile_member, const long long *moff, const int *mlc, int nslot) {
-  if (njob == 0) return;
-  dim3 g(std::min((nslot + 255) / 256, 2048), njob);
-  k_scatter<<<g, 256, 0, st>>>(jobs, njob, lidx, tile_member, moff, mlc, nslot);
+                    const int *tile_member, const long long *moff, const int *mlc, int d0,
+                    int d1) {
+  if (njob == 0 || d1 <= d0) return;
+  dim3 g(std::min((d1 - d0 + 255) / 256, 2048), njob);
+  k_scatter<<<g, 256, 0, st>>>(jobs, njob, lidx, tile_member, moff, mlc, d0, d1);
   count_launches(1);
 }
 void launch_gather(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx,
-                   const int *tile_member, const long long *moff, int nslot) {
-  if (njob == 0) return;
-  dim3 g(std::min((nslot + 255) / 256, 2048), njob);
-  k_gather<<<g, 256, 0, st>>>(jobs, njob, lidx, tile_member, moff, nslot);
+                   const int *tile_member, const long long *moff, int d0, int d1) {
+  if (njob == 0 || d1 <= d0) return;
+  dim3 g(std::min((d1 - d0 + 255) / 256, 2048), njob);
+  k_gather<<<g, 256, 0, st>>>(jobs, njob, lidx, tile_member, moff, d0, d1);
   count_launches(1);
 }
 void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
