@@ -61,6 +61,7 @@ uint64_t morton2(uint32_t x, uint32_t y) {
 }
 
 constexpr int NSTAGE = 8;     // staging buffers (each holds one array of every member)
+constexpr int NCHUNK = 8;     // member chunks of a pipelined efdc_xm_step_batch
 constexpr int NCOPY = 4;      // streams for host<->device copies
 constexpr int MAX_JOBS = 128;  // arrays moved by one upload/download call
 constexpr int GRAPH_ITERS = 4;  // CG iterations per graph launch
@@ -80,6 +81,11 @@ struct DevBuf {
 };
 
 // One basin of the context.
+// the control blocks move as 4-byte words (launch_words)
+static_assert(sizeof(Ctl) % 4 == 0 && sizeof(Glob) % 4 == 0 &&
+                  sizeof(xm::StepScalars) % 4 == 0,
+              "control blocks must be whole 4-byte words");
+
 struct Member {
   int la = 0, lc = 0;
   int tile0 = 0, tile1 = 0;  // its tiles [tile0, tile1)
@@ -116,6 +122,13 @@ struct efdc_xm_ctx {
   // filled or before the kernels that read the staging buffers, by events)
   cudaStream_t copy_stream[NCOPY] = {};
   cudaEvent_t copy_event[NCOPY + 1] = {};
+  // pipelined efdc_xm_step_batch (member chunks: the upload of one, the step
+  // of another and the download of a third overlap): the download copy
+  // streams, the scatter and gather streams, and events per chunk
+  cudaStream_t dn_stream[NCOPY] = {};
+  cudaStream_t up_x = nullptr, dn_x = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_up[NCHUNK] = {}, ev_step[NCHUNK] = {}, ev_g[NCHUNK] = {};
+  cudaEvent_t ev_j[NCHUNK][NCOPY] = {};
   std::vector<DevBuf> bufs;
   // device views
   xm::DevStatic S{};
@@ -132,6 +145,9 @@ struct efdc_xm_ctx {
   int *act_h = nullptr;              // [M] pinned
   xm::StepScalars *sc = nullptr;     // [M]
   xm::StepScalars *sc_h = nullptr;   // [M] pinned
+  // device addresses of the mapped pinned mirrors (null: copied by the copy engines)
+  void *ctl_hd = nullptr, *glob_hd = nullptr, *act_hd = nullptr, *mpoly_hd = nullptr,
+       *sc_hd = nullptr;
   double *part = nullptr;
   int *lidx = nullptr;
   int *tile_member = nullptr;
@@ -248,6 +264,79 @@ int compute_after_copies(efdc_xm_ctx *c) {
   return EFDC_XM_OK;
 }
 
+// Host -> staging copies of the members [m0, m1) of one array (members whose
+// host arrays lie back to back at the staging stride, LC+1 elements -- an
+// ensemble held as one (LCM, members) array per field -- go in one copy),
+// spread over the streams st[k++ % NCOPY].
+int h2d_range(efdc_xm_ctx *c, const Xfer &x, char *stage, int m0, int m1, cudaStream_t *st,
+              int &k, int ns = NCOPY) {
+  const size_t es = esize(x.kind);
+  for (int m = m0; m < m1;) {
+    const char *h0 = static_cast<const char *>(x.host[m]);
+    int e = m + 1;
+    while (e < m1 && static_cast<const char *>(x.host[e]) ==
+                         static_cast<const char *>(x.host[e - 1]) +
+                             size_t(c->mem[e - 1].lc + 1) * es)
+      ++e;
+    const size_t n = size_t(c->mem[e - 1].off - c->mem[m].off + c->mem[e - 1].lc);
+    CK(cudaMemcpyAsync(stage + c->mem[m].off * es, h0, n * es, cudaMemcpyHostToDevice,
+                       st[k++ % ns]));
+    g_h2d.fetch_add(static_cast<long long>(n * es), std::memory_order_relaxed);
+    m = e;
+  }
+  return EFDC_XM_OK;
+}
+
+// A caller's host element that a staging -> host copy overwrites and that is
+// put back once the copy is done.
+struct Keep {
+  char *at;
+  char val[8];
+  size_t n;
+};
+
+// Staging -> host copies of the members [m0, m1) of one array.  A member
+// alone sends its water elements L = 2..LA; members back to back at the
+// staging stride go in one copy of the whole run, which also covers each
+// member's ghost elements (L = 1 and LC) and the element between two members:
+// those must stay as the caller has them, so their values go to `keep`.
+int d2h_range(efdc_xm_ctx *c, const Xfer &x, const char *stage, int m0, int m1, cudaStream_t *st,
+              int &k, std::vector<Keep> &keep, int ns = NCOPY) {
+  const size_t es = esize(x.kind);
+  auto save = [&](char *at) {
+    Keep kp{at, {}, es};
+    std::memcpy(kp.val, at, es);
+    keep.push_back(kp);
+  };
+  for (int m = m0; m < m1;) {
+    char *h0 = static_cast<char *>(const_cast<void *>(x.host[m]));
+    int e = m + 1;
+    while (e < m1 && static_cast<const char *>(x.host[e]) ==
+                         static_cast<const char *>(x.host[e - 1]) +
+                             size_t(c->mem[e - 1].lc + 1) * es)
+      ++e;
+    if (e == m + 1) {
+      const size_t n = es * size_t(c->mem[m].la - 1);
+      CK(cudaMemcpyAsync(h0 + es, stage + (c->mem[m].off + 1) * es, n, cudaMemcpyDeviceToHost,
+                         st[k++ % ns]));
+      g_d2h.fetch_add(static_cast<long long>(n), std::memory_order_relaxed);
+    } else {
+      for (int q = m; q < e; ++q) {
+        char *hq = static_cast<char *>(const_cast<void *>(x.host[q]));
+        save(hq);                                              // L = 1
+        save(hq + size_t(c->mem[q].lc - 1) * es);              // L = LC
+        if (q + 1 < e) save(hq + size_t(c->mem[q].lc) * es);   // between members
+      }
+      const size_t n = es * size_t(c->mem[e - 1].off - c->mem[m].off + c->mem[e - 1].lc);
+      CK(cudaMemcpyAsync(h0, stage + c->mem[m].off * es, n, cudaMemcpyDeviceToHost,
+                         st[k++ % ns]));
+      g_d2h.fetch_add(static_cast<long long>(n), std::memory_order_relaxed);
+    }
+    m = e;
+  }
+  return EFDC_XM_OK;
+}
+
 int upload_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
   if (xs.empty()) return EFDC_XM_OK;
   if (xs.size() > size_t(MAX_JOBS)) {
@@ -263,26 +352,10 @@ int upload_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
     const size_t g1 = std::min(xs.size(), g0 + NSTAGE);
     // the previous group's scatter has read the staging buffers
     if ((rc = copies_after_compute(c))) return rc;
-    for (size_t j = g0; j < g1; ++j) {
-      const size_t es = esize(xs[j].kind);
-      char *dst = reinterpret_cast<char *>(c->stage[j % NSTAGE]);
-      // members whose host arrays lie back to back at the staging stride (LC+1
-      // elements: an ensemble held as one (LCM, members) array per field) go
-      // in one copy
-      for (int m = 0; m < c->M;) {
-        const char *h0 = static_cast<const char *>(xs[j].host[m]);
-        int e = m + 1;
-        while (e < c->M && static_cast<const char *>(xs[j].host[e]) ==
-                               static_cast<const char *>(xs[j].host[e - 1]) +
-                                   size_t(c->mem[e - 1].lc + 1) * es)
-          ++e;
-        const size_t n = size_t(c->mem[e - 1].off - c->mem[m].off + c->mem[e - 1].lc);
-        CK(cudaMemcpyAsync(dst + c->mem[m].off * es, h0, n * es, cudaMemcpyHostToDevice,
-                           c->copy_stream[k++ % NCOPY]));
-        g_h2d.fetch_add(static_cast<long long>(n * es), std::memory_order_relaxed);
-        m = e;
-      }
-    }
+    for (size_t j = g0; j < g1; ++j)
+      if ((rc = h2d_range(c, xs[j], reinterpret_cast<char *>(c->stage[j % NSTAGE]), 0, c->M,
+                          c->copy_stream, k)))
+        return rc;
     if ((rc = compute_after_copies(c))) return rc;
     xm::launch_scatter(c->stream, c->jobs_d + g0, int(g1 - g0), c->lidx, c->tile_member, c->moff,
                        c->mlc, 0, c->nslot);
@@ -302,22 +375,7 @@ int download_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
     c->jobs_h[j] = CopyJob{c->stage[j % NSTAGE], xs[j].dev, xs[j].kind};
   CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, xs.size() * sizeof(CopyJob), cudaMemcpyHostToDevice,
                      c->stream));
-  // Members whose host arrays lie back to back at the staging stride go back
-  // in one copy of the whole run; that copy also covers each member's ghost
-  // elements (L = 1 and LC) and the element between two members, which must
-  // stay as the caller has them: their host values are kept here and written
-  // back once the copies are done (the caller waits inside this call).
-  struct Keep {
-    char *at;
-    char val[8];
-    size_t n;
-  };
-  std::vector<Keep> keep;
-  auto save = [&](char *at, size_t es) {
-    Keep k{at, {}, es};
-    std::memcpy(k.val, at, es);
-    keep.push_back(k);
-  };
+  std::vector<Keep> keep;  // put back once the copies are done (the caller waits here)
   int rc = 0, k = 0;
   for (size_t g0 = 0; g0 < xs.size(); g0 += NSTAGE) {
     const size_t g1 = std::min(xs.size(), g0 + NSTAGE);
@@ -326,36 +384,10 @@ int download_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
                       0, c->nslot);
     CK(cudaGetLastError());
     if ((rc = copies_after_compute(c))) return rc;
-    for (size_t j = g0; j < g1; ++j) {
-      const size_t es = esize(xs[j].kind);
-      const char *src = reinterpret_cast<const char *>(c->stage[j % NSTAGE]);
-      for (int m = 0; m < c->M;) {
-        char *h0 = static_cast<char *>(const_cast<void *>(xs[j].host[m]));
-        int e = m + 1;
-        while (e < c->M && static_cast<const char *>(xs[j].host[e]) ==
-                               static_cast<const char *>(xs[j].host[e - 1]) +
-                                   size_t(c->mem[e - 1].lc + 1) * es)
-          ++e;
-        if (e == m + 1) {  // one member: its water elements L = 2..LA only
-          const size_t n = es * size_t(c->mem[m].la - 1);
-          CK(cudaMemcpyAsync(h0 + es, src + (c->mem[m].off + 1) * es, n, cudaMemcpyDeviceToHost,
-                             c->copy_stream[k++ % NCOPY]));
-          g_d2h.fetch_add(static_cast<long long>(n), std::memory_order_relaxed);
-        } else {
-          for (int q = m; q < e; ++q) {
-            char *hq = static_cast<char *>(const_cast<void *>(xs[j].host[q]));
-            save(hq, es);                                        // L = 1
-            save(hq + size_t(c->mem[q].lc - 1) * es, es);        // L = LC
-            if (q + 1 < e) save(hq + size_t(c->mem[q].lc) * es, es);  // between members
-          }
-          const size_t n = es * size_t(c->mem[e - 1].off - c->mem[m].off + c->mem[e - 1].lc);
-          CK(cudaMemcpyAsync(h0, src + c->mem[m].off * es, n, cudaMemcpyDeviceToHost,
-                             c->copy_stream[k++ % NCOPY]));
-          g_d2h.fetch_add(static_cast<long long>(n), std::memory_order_relaxed);
-        }
-        m = e;
-      }
-    }
+    for (size_t j = g0; j < g1; ++j)
+      if ((rc = d2h_range(c, xs[j], reinterpret_cast<const char *>(c->stage[j % NSTAGE]), 0,
+                          c->M, c->copy_stream, k, keep)))
+        return rc;
   }
   for (cudaStream_t s : c->copy_stream) CK(cudaStreamSynchronize(s));
   CK(cudaStreamSynchronize(c->stream));
@@ -363,21 +395,40 @@ int download_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
   return EFDC_XM_OK;
 }
 
-int read_ctl(efdc_xm_ctx *c) {
-  CK(cudaMemcpyAsync(c->ctl_h, c->ctl, sizeof(Ctl) * c->M, cudaMemcpyDeviceToHost, c->stream));
+// Control blocks between the device and their pinned host mirrors, on the
+// solver stream.  Where the mirror is mapped (dev_h: its device address) a
+// kernel moves them, so that a step's polls do not queue behind the bulk
+// copies of a chunked efdc_xm_step_batch in flight on the copy engines.
+int to_device(efdc_xm_ctx *c, void *dev, const void *host, const void *dev_h, size_t bytes) {
+  if (dev_h) {
+    xm::launch_words(c->stream, dev, dev_h, bytes);
+    CK(cudaGetLastError());
+  } else {
+    CK(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, c->stream));
+  }
+  return EFDC_XM_OK;
+}
+int to_host(efdc_xm_ctx *c, void *host, void *dev_h, const void *dev, size_t bytes) {
+  if (dev_h) {
+    xm::launch_words(c->stream, dev_h, dev, bytes);
+    CK(cudaGetLastError());
+  } else {
+    CK(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c->stream));
+  }
   CK(cudaStreamSynchronize(c->stream));
   return EFDC_XM_OK;
+}
+
+int read_ctl(efdc_xm_ctx *c) {
+  return to_host(c, c->ctl_h, c->ctl_hd, c->ctl, sizeof(Ctl) * c->M);
 }
 
 int read_glob(efdc_xm_ctx *c) {
-  CK(cudaMemcpyAsync(c->glob_h, c->glob, sizeof(Glob), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  return EFDC_XM_OK;
+  return to_host(c, c->glob_h, c->glob_hd, c->glob, sizeof(Glob));
 }
 
 int write_act(efdc_xm_ctx *c) {
-  CK(cudaMemcpyAsync(c->act, c->act_h, sizeof(int) * c->M, cudaMemcpyHostToDevice, c->stream));
-  return EFDC_XM_OK;
+  return to_device(c, c->act, c->act_h, c->act_hd, sizeof(int) * c->M);
 }
 
 // Captures `body` (GRAPH_ITERS iterations launched on c->stream) into a
@@ -511,7 +562,7 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
       if (c->mem[m].may_asym || c->sys_external) c->mx_jac = true;
     }
   }
-  CK(cudaMemcpyAsync(c->mpoly, c->mpoly_h, sizeof(int) * c->M, cudaMemcpyHostToDevice, c->stream));
+  if (int rc0 = to_device(c, c->mpoly, c->mpoly_h, c->mpoly_hd, sizeof(int) * c->M)) return rc0;
   const xm::Launch lk = c->L();  // with the kinds in use
   xm::launch_chan_p0(lk, c->S, c->mxview, P, c->act);
   int rc = 0;
@@ -720,6 +771,17 @@ void efdc_xm_destroy(efdc_xm_ctx *c) {
     if (s) cudaStreamDestroy(s);
   for (cudaEvent_t e : c->copy_event)
     if (e) cudaEventDestroy(e);
+  for (cudaStream_t s : c->dn_stream)
+    if (s) cudaStreamDestroy(s);
+  for (cudaStream_t s : {c->up_x, c->dn_x})
+    if (s) cudaStreamDestroy(s);
+  for (int k = 0; k < NCHUNK; ++k) {
+    for (cudaEvent_t e : {c->ev_up[k], c->ev_step[k], c->ev_g[k]})
+      if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->ev_j[k])
+      if (e) cudaEventDestroy(e);
+  }
+  if (c->ev_start) cudaEventDestroy(c->ev_start);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -783,6 +845,20 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   for (cudaEvent_t &e : c->copy_event)
     if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
       return bail("event creation failed");
+  {
+    bool ok = cudaStreamCreateWithFlags(&c->up_x, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&c->dn_x, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->ev_start, cudaEventDisableTiming) == cudaSuccess;
+    for (cudaStream_t &s : c->dn_stream)
+      ok = ok && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
+    for (int k = 0; k < NCHUNK; ++k) {
+      for (cudaEvent_t *e : {&c->ev_up[k], &c->ev_step[k], &c->ev_g[k]})
+        ok = ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
+      for (cudaEvent_t &e : c->ev_j[k])
+        ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
+    }
+    if (!ok) return bail("stream or event creation failed");
+  }
   cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
 
   // ---- host layout: tiles, quads (4-tile CG units, never across members), slots ----
@@ -969,7 +1045,7 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   if (!c->ptmp || !Y.x32 || !Y.z32 || !Y.r32b) return bail("cudaMalloc failed (device memory)");
   auto pin = [](void *pp, size_t bytes) {
     return cudaHostAlloc(static_cast<void **>(pp), std::max<size_t>(bytes, 1),
-                         cudaHostAllocDefault) == cudaSuccess;
+                         cudaHostAllocMapped) == cudaSuccess;
   };
   if (!pin(&c->ctl_h, sizeof(Ctl) * M) || !pin(&c->glob_h, sizeof(Glob)) ||
       !pin(&c->act_h, sizeof(int) * M) || !pin(&c->mpoly_h, sizeof(int) * M) ||
@@ -978,6 +1054,16 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
     return bail("cudaHostAlloc failed");
   std::memset(c->ctl_h, 0, sizeof(Ctl) * M);
   std::memset(c->sc_h, 0, sizeof(xm::StepScalars) * M);
+  {  // the control mirrors' device addresses (pinned memory is mapped under UVA)
+    void *h[] = {c->ctl_h, c->glob_h, c->act_h, c->mpoly_h, c->sc_h};
+    void **d[] = {&c->ctl_hd, &c->glob_hd, &c->act_hd, &c->mpoly_hd, &c->sc_hd};
+    bool ok = true;
+    for (int k = 0; k < 5; ++k) ok = ok && cudaHostGetDevicePointer(d[k], h[k], 0) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      for (void **p : d) *p = nullptr;
+    }
+  }
   c->jobs_d = c->alloc<CopyJob>(MAX_JOBS);
   if (!c->jobs_d) return bail("cudaMalloc failed");
   {  // land slots of the scaled system: CCC=1 keeps them inert in the CG;
@@ -1120,13 +1206,9 @@ namespace {
 // has it; skip_sbxy: SBX, SBY as well (read also by the baroclinic terms).
 // Their device copies are then marked out of date.  levels: upload the three
 // time levels of CALPUV9C (P1, H2P, H1P, UHDY1E ... FPGYE) as well.
-int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool skip_sbxy,
-                 bool levels) {
-  if (!c || !f) {
-    set_error("efdc_xm_upload: NULL argument");
-    return EFDC_XM_BAD_ARGUMENT;
-  }
-  CK(cudaSetDevice(c->device));
+// The arrays of an upload, with its argument checks.
+int plan_upload(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool skip_sbxy,
+                bool levels, std::vector<Xfer> &xs) {
   xm::DevState &X = c->X;
   const int M = c->M;
   for (int m = 0; m < M; ++m)
@@ -1135,7 +1217,6 @@ int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool
                 "QCHANVN are required", m);
       return EFDC_XM_BAD_ARGUMENT;
     }
-  std::vector<Xfer> xs;
   int rc = 0;
 #define XM_UP(name, dev, kind)                                   \
   {                                                              \
@@ -1192,16 +1273,28 @@ int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool
       xs.push_back(Xfer{v, c->S.baro.b + size_t(k) * c->S.baro.stride, 0});
     }
   }
-  if ((rc = upload_arrays(c, xs))) return rc;
-  // two time levels: the second buffer of each time-level pair starts as a
-  // copy (its land slots must hold the ghost values too); the H1P input is
-  // not used because a CALPUV2C step begins with H1P = HP (calpuv2c.f90:264)
-  const size_t nb = size_t(c->nslot) * sizeof(double);
-  if (!levels) {
-    if (f[0].uhdye) CK(cudaMemcpyAsync(X.uhdy1e, X.uhdye, nb, cudaMemcpyDeviceToDevice, c->stream));
-    if (f[0].vhdxe) CK(cudaMemcpyAsync(X.vhdx1e, X.vhdxe, nb, cudaMemcpyDeviceToDevice, c->stream));
-    if (f[0].hp) CK(cudaMemcpyAsync(X.h1p, X.hp, nb, cudaMemcpyDeviceToDevice, c->stream));
-  }
+  return EFDC_XM_OK;
+}
+
+// Two time levels: the second buffer of each time-level pair starts as a copy
+// of the slots [d0, d1) (its land slots must hold the ghost values too; the
+// H1P input is not used because a CALPUV2C step begins with H1P = HP,
+// calpuv2c.f90:264).
+// Copied by a kernel (no copy engine: see to_device).
+int copy_levels(efdc_xm_ctx *c, const efdc_xm_fields *f, size_t d0, size_t d1, cudaStream_t st) {
+  const xm::DevState &X = c->X;
+  const size_t nb = (d1 - d0) * sizeof(double);
+  if (f[0].uhdye) xm::launch_words(st, X.uhdy1e + d0, X.uhdye + d0, nb);
+  if (f[0].vhdxe) xm::launch_words(st, X.vhdx1e + d0, X.vhdxe + d0, nb);
+  if (f[0].hp) xm::launch_words(st, X.h1p + d0, X.hp + d0, nb);
+  CK(cudaGetLastError());
+  return EFDC_XM_OK;
+}
+
+// The small per-member uploads: open-boundary series, channel flows, HP(1).
+// Waits for them (and for the solver stream's earlier work).
+int upload_small(efdc_xm_ctx *c, const efdc_xm_fields *f) {
+  const int M = c->M;
   if (c->nobc > 0) {
     for (int m = 0; m < M; ++m) {
       int k = c->mem[m].b0;
@@ -1228,13 +1321,36 @@ int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool
                        cudaMemcpyHostToDevice, c->stream));
   }
   CK(cudaStreamSynchronize(c->stream));
+  return EFDC_XM_OK;
+}
+
+// What the context records of an upload: which device copies are out of
+// date, whether it holds the three time levels, the entry masks (OLDMASK).
+void upload_done(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool skip_sbxy,
+                 bool levels) {
   c->wd_stale = skip_wetdry;
   c->sbxy_stale = skip_sbxy;
   c->tl3_ready = levels;
   if (!skip_wetdry)
-    for (int m = 0; m < M; ++m)
+    for (int m = 0; m < c->M; ++m)
       if (f[m].lmaskdry)
         c->mem[m].oldmask_h.assign(f[m].lmaskdry, f[m].lmaskdry + c->mem[m].lc);
+}
+
+int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool skip_sbxy,
+                 bool levels) {
+  if (!c || !f) {
+    set_error("efdc_xm_upload: NULL argument");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  CK(cudaSetDevice(c->device));
+  std::vector<Xfer> xs;
+  int rc = plan_upload(c, f, skip_wetdry, skip_sbxy, levels, xs);
+  if (!rc) rc = upload_arrays(c, xs);
+  if (!rc && !levels) rc = copy_levels(c, f, 0, size_t(c->nslot), c->stream);
+  if (!rc) rc = upload_small(c, f);
+  if (rc) return rc;
+  upload_done(c, f, skip_wetdry, skip_sbxy, levels);
   return EFDC_XM_OK;
 }
 }  // namespace
@@ -1254,16 +1370,19 @@ namespace {
 // values are the host values uploaded by the same call.  levels: the three
 // time levels to return (0 none; 2 FPGXE, FPGYE, which a CALPUV9C(2) step
 // changes; 3 all of them, after CALPUV9C(3)).
-int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int levels) {
-  if (!c || !f) {
-    set_error("efdc_xm_download: NULL argument");
-    return EFDC_XM_BAD_ARGUMENT;
-  }
-  CK(cudaSetDevice(c->device));
+// The wet/dry lists of a download: the mask at exit and at entry (OLDMASK)
+// of every member, gathered into these host copies.
+struct Lists {
+  bool on = false;
+  std::vector<std::vector<int32_t>> mask, oldm;
+};
+
+// The arrays of a download.
+int plan_download(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int levels,
+                  std::vector<Xfer> &xs, Lists &ls) {
   xm::DevState &X = c->X;
   const xm::DevSystem &Y = c->Y;
   const int M = c->M;
-  std::vector<Xfer> xs;
   int rc = 0;
 #define XM_DN(name, dev, kind)                                   \
   {                                                              \
@@ -1296,32 +1415,30 @@ int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int l
     }
   }
 #undef XM_DN
-  if (c->last_mixed && (f[0].ccc || f[0].ccs || f[0].ccw || f[0].cce || f[0].ccn || f[0].fptmp)) {
-    // a MIXED step solves from the unscaled assembly: the scaled system
-    // (calpuv2c.f90:371-399) is formed when it is asked for
-    if ((rc = scaled_system(c))) return rc;
-  }
-  if (f[0].hpi || f[0].hui || f[0].hvi) {  // 1/HP, 1/HU, 1/HV are formed on request
-    xm::launch_reciprocals(c->L(), c->S, c->X, 1, c->ntile);
-    CK(cudaGetLastError());
-  }
   // the wet/dry lists need the mask at exit and at entry (OLDMASK)
-  std::vector<std::vector<int32_t>> mask(M), oldm(M);
-  bool lists = false;
-  for (int m = 0; m < M; ++m) lists |= (f[m].lwet || f[m].ldry);
-  if (lists) {
+  ls.mask.assign(M, {});
+  ls.oldm.assign(M, {});
+  ls.on = false;
+  for (int m = 0; m < M; ++m) ls.on |= (f[m].lwet || f[m].ldry);
+  if (ls.on) {
     std::vector<const void *> pm(M), po(M);
     for (int m = 0; m < M; ++m) {
-      mask[m].assign(c->mem[m].lc, 1);
-      oldm[m].assign(c->mem[m].lc, 1);
-      pm[m] = mask[m].data();
-      po[m] = oldm[m].data();
+      ls.mask[m].assign(c->mem[m].lc, 1);
+      ls.oldm[m].assign(c->mem[m].lc, 1);
+      pm[m] = ls.mask[m].data();
+      po[m] = ls.oldm[m].data();
     }
     xs.push_back(Xfer{pm, X.lmaskdry, 1});
     xs.push_back(Xfer{po, X.oldmask, 2});
   }
-  if ((rc = download_arrays(c, xs))) return rc;
-  if (c->S.ch.n > 0) {  // the channels' flows
+  return EFDC_XM_OK;
+}
+
+// After the arrays of a download: the channels' flows, and the wet/dry lists
+// from the gathered masks (calpuv2c.f90:1061-1080, L order).
+int download_finish(efdc_xm_ctx *c, efdc_xm_fields *f, const Lists &ls) {
+  const int M = c->M;
+  if (c->S.ch.n > 0) {
     const xm::DevChan &C = c->S.ch;
     for (int m = 0; m < M; ++m) {
       const int k0 = c->chan_start[m], n = c->chan_start[m + 1] - k0;
@@ -1336,15 +1453,15 @@ int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int l
     }
     CK(cudaStreamSynchronize(c->stream));
   }
-  if (lists) {  // calpuv2c.f90:1061-1080 (L order)
+  if (ls.on) {
     for (int m = 0; m < M; ++m) {
       const Member &mb = c->mem[m];
       int nw = 0, nd = 0;
       for (int L = 2; L <= mb.la; ++L) {
-        if (mb.last_isdry == 0 || mask[m][L - 1]) {
+        if (mb.last_isdry == 0 || ls.mask[m][L - 1]) {
           if (f[m].lwet) f[m].lwet[nw] = L;
           ++nw;
-        } else if (oldm[m][L - 1] || mb.last_n < mb.last_ntstbc + 1) {
+        } else if (ls.oldm[m][L - 1] || mb.last_n < mb.last_ntstbc + 1) {
           if (f[m].ldry) f[m].ldry[nd] = L;
           ++nd;
         }
@@ -1352,6 +1469,33 @@ int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int l
     }
   }
   return EFDC_XM_OK;
+}
+
+bool wants_system(const efdc_xm_fields *f) {
+  return f[0].ccc || f[0].ccs || f[0].ccw || f[0].cce || f[0].ccn || f[0].fptmp;
+}
+
+int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int levels) {
+  if (!c || !f) {
+    set_error("efdc_xm_download: NULL argument");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  CK(cudaSetDevice(c->device));
+  std::vector<Xfer> xs;
+  Lists ls;
+  int rc = plan_download(c, f, skip_unchanged, levels, xs, ls);
+  if (rc) return rc;
+  if (c->last_mixed && wants_system(f)) {
+    // a MIXED step solves from the unscaled assembly: the scaled system
+    // (calpuv2c.f90:371-399) is formed when it is asked for
+    if ((rc = scaled_system(c))) return rc;
+  }
+  if (f[0].hpi || f[0].hui || f[0].hvi) {  // 1/HP, 1/HU, 1/HV are formed on request
+    xm::launch_reciprocals(c->L(), c->S, c->X, 1, c->ntile);
+    CK(cudaGetLastError());
+  }
+  if ((rc = download_arrays(c, xs))) return rc;
+  return download_finish(c, f, ls);
 }
 }  // namespace
 
@@ -1441,10 +1585,10 @@ int step_range(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats, 
     any_waste |= (isd > 0 && prm[m].ndrystp < 0);
     c->act_h[m] = 1;
   }
-  CK(cudaMemcpyAsync(c->sc, c->sc_h, sizeof(xm::StepScalars) * M, cudaMemcpyHostToDevice,
-                     c->stream));
-  CK(cudaMemsetAsync(c->ctl, 0, sizeof(Ctl) * M, c->stream));  // counters of this step
-  int rc = write_act(c);
+  int rc = to_device(c, c->sc, c->sc_h, c->sc_hd, sizeof(xm::StepScalars) * M);
+  if (rc) return rc;
+  xm::launch_words(c->stream, c->ctl, nullptr, sizeof(Ctl) * M);  // counters of this step
+  rc = write_act(c);
   if (rc) return rc;
   if (istl == 0) {
     // k_begin copies UHDY1E=UHDYE, VHDX1E=VHDXE, H1P=HP (calpuv2c.f90:256-264)
@@ -1573,6 +1717,179 @@ int step_range(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats, 
   }
   return overall_status(stats + m0, m1 - m0);
 }
+
+// More staging buffers, for transfers in which every array takes its own.
+int ensure_stages(efdc_xm_ctx *c, size_t n) {
+  while (c->stage.size() < n) {
+    double *p = c->alloc<double>(size_t(c->stage_len), false);
+    if (!p) {
+      set_error("cudaMalloc failed (staging)");
+      return EFDC_XM_CUDA_ERROR;
+    }
+    c->stage.push_back(p);
+  }
+  return EFDC_XM_OK;
+}
+
+// Waits for every stream of the context.
+void drain(efdc_xm_ctx *c) {
+  for (cudaStream_t s : c->copy_stream) cudaStreamSynchronize(s);
+  for (cudaStream_t s : c->dn_stream) cudaStreamSynchronize(s);
+  cudaStreamSynchronize(c->up_x);
+  cudaStreamSynchronize(c->dn_x);
+  cudaStreamSynchronize(c->stream);
+}
+
+// Copy streams per direction of a chunked step: each long copy runs at the
+// link's speed on one stream, and the copy engines left free serve the other
+// direction at the same time.
+constexpr int NPIPE = 1;
+
+// efdc_xm_step_batch of a CALPUV2C step in NCHUNK member chunks of about
+// equal cell counts, so that the upload of one chunk, the step of an earlier
+// one and the download of a still earlier one overlap (the link carries both
+// directions at once).  Every array of the two transfers has its own staging
+// buffer, in which each member has its own range, so no chunk waits for the
+// buffers of another: a chunk's upload (copies on copy_stream, scatter on
+// up_x) -> its step (stream) -> its download (gather on dn_x, copies on
+// dn_stream), ordered by events.  Results are those of the unchunked call
+// bit for bit: every member steps exactly as in a step of all members.
+int step_batch_chunks(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
+                      efdc_xm_stats *stats, bool skip_wetdry, bool skip_sbxy) {
+  const int M = c->M;
+  std::vector<Xfer> up, dn;
+  Lists ls;
+  int rc = plan_upload(c, f, skip_wetdry, skip_sbxy, false, up);
+  if (rc) {
+    fill_status(stats, M, rc);
+    return rc;
+  }
+  upload_done(c, f, skip_wetdry, skip_sbxy, false);  // the state the step and download see
+  if ((rc = validate_step(c, prm, stats))) return rc;
+  if ((rc = plan_download(c, f, skip_wetdry, 0, dn, ls))) {
+    fill_status(stats, M, rc);
+    return rc;
+  }
+  const size_t nu = up.size(), nd = dn.size();
+  if (nu + nd > size_t(MAX_JOBS)) {
+    set_error("internal: too many arrays in one transfer");
+    fill_status(stats, M, EFDC_XM_CUDA_ERROR);
+    return EFDC_XM_CUDA_ERROR;
+  }
+  if ((rc = ensure_stages(c, std::max(nu, nd)))) {
+    fill_status(stats, M, rc);
+    return rc;
+  }
+  for (size_t j = 0; j < nu; ++j) c->jobs_h[j] = CopyJob{c->stage[j], up[j].dev, up[j].kind};
+  for (size_t j = 0; j < nd; ++j) c->jobs_h[nu + j] = CopyJob{c->stage[j], dn[j].dev, dn[j].kind};
+  CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, (nu + nd) * sizeof(CopyJob), cudaMemcpyHostToDevice,
+                     c->stream));
+  if ((rc = upload_small(c, f))) {  // waits for the solver stream: the job table is in place
+    fill_status(stats, M, rc);
+    return rc;
+  }
+  // chunk k holds the members [mb[k], mb[k+1]), about equal cell counts
+  const int K = std::min(NCHUNK, M);
+  std::vector<int> mb(K + 1, M);
+  mb[0] = 0;
+  {
+    long long tot = 0, acc = 0;
+    for (int m = 0; m < M; ++m) tot += c->mem[m].la - 1;
+    for (int m = 0, k = 1; m < M && k < K; ++m) {
+      acc += c->mem[m].la - 1;
+      if (acc * K >= tot * k) mb[k++] = m + 1;
+    }
+  }
+  auto slots = [&](int k, int &d0, int &d1) {  // chunk 0 covers the ghost tile too
+    d0 = mb[k] == 0 ? 0 : c->mem[mb[k]].tile0 * xm::TILE;
+    d1 = c->mem[mb[k + 1] - 1].tile1 * xm::TILE;
+  };
+  // the transfer streams start after the solver stream's earlier work
+  CK(cudaEventRecord(c->ev_start, c->stream));
+  for (cudaStream_t s : c->copy_stream) CK(cudaStreamWaitEvent(s, c->ev_start, 0));
+  for (cudaStream_t s : c->dn_stream) CK(cudaStreamWaitEvent(s, c->ev_start, 0));
+  CK(cudaStreamWaitEvent(c->up_x, c->ev_start, 0));
+  CK(cudaStreamWaitEvent(c->dn_x, c->ev_start, 0));
+  int q = 0, d0 = 0, d1 = 0;
+  for (int k = 0; k < K; ++k) {  // all uploads, queued
+    if (mb[k] == mb[k + 1]) continue;
+    for (size_t j = 0; j < nu; ++j)
+      if ((rc = h2d_range(c, up[j], reinterpret_cast<char *>(c->stage[j]), mb[k], mb[k + 1],
+                          c->copy_stream, q, NPIPE))) {
+        drain(c);
+        return rc;
+      }
+    for (int s = 0; s < NPIPE; ++s) {
+      CK(cudaEventRecord(c->ev_j[k][s], c->copy_stream[s]));
+      CK(cudaStreamWaitEvent(c->up_x, c->ev_j[k][s], 0));
+    }
+    slots(k, d0, d1);
+    xm::launch_scatter(c->up_x, c->jobs_d, int(nu), c->lidx, c->tile_member, c->moff, c->mlc, d0,
+                       d1);
+    CK(cudaGetLastError());
+    if ((rc = copy_levels(c, f, size_t(d0), size_t(d1), c->up_x))) {
+      drain(c);
+      return rc;
+    }
+    CK(cudaEventRecord(c->ev_up[k], c->up_x));
+  }
+  std::vector<Keep> keep;
+  const bool recip = f[0].hpi || f[0].hui || f[0].hvi;
+  q = 0;
+  for (int k = 0; k < K; ++k) {  // steps, each followed by its download, queued
+    if (mb[k] == mb[k + 1]) continue;
+    CK(cudaStreamWaitEvent(c->stream, c->ev_up[k], 0));
+    rc = step_range(c, prm, stats, mb[k], mb[k + 1]);
+    if (rc == EFDC_XM_CUDA_ERROR || rc == EFDC_XM_BAD_ARGUMENT) {
+      drain(c);
+      return rc;
+    }
+    if (recip)  // 1/HP, 1/HU, 1/HV are formed on request
+      xm::launch_reciprocals(c->L(), c->S, c->X, c->mem[mb[k]].tile0,
+                             c->mem[mb[k + 1] - 1].tile1);
+    CK(cudaEventRecord(c->ev_step[k], c->stream));
+    CK(cudaStreamWaitEvent(c->dn_x, c->ev_step[k], 0));
+    slots(k, d0, d1);
+    xm::launch_gather(c->dn_x, c->jobs_d + nu, int(nd), c->lidx, c->tile_member, c->moff, d0, d1);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev_g[k], c->dn_x));
+    for (int s = 0; s < NPIPE; ++s) CK(cudaStreamWaitEvent(c->dn_stream[s], c->ev_g[k], 0));
+    for (size_t j = 0; j < nd; ++j)
+      if ((rc = d2h_range(c, dn[j], reinterpret_cast<const char *>(c->stage[j]), mb[k],
+                          mb[k + 1], c->dn_stream, q, keep, NPIPE))) {
+        drain(c);
+        return rc;
+      }
+  }
+  drain(c);
+  CK(cudaGetLastError());
+  for (const Keep &kp : keep) std::memcpy(kp.at, kp.val, kp.n);
+  if ((rc = download_finish(c, f, ls))) return rc;
+  return overall_status(stats, M);
+}
+
+// LAWET, LADRY of the members whose lists were asked for (calpuv2c.f90:1061-1080).
+int batch_lists_stats(const efdc_xm_ctx *c, const efdc_xm_params *prm, const efdc_xm_fields *f,
+                      efdc_xm_stats *stats, int st) {
+  for (int m = 0; m < c->M; ++m) {
+    if (!(f[m].lwet || f[m].ldry)) continue;
+    const Member &mb = c->mem[m];
+    if (prm[m].isdry == 0) {
+      stats[m].lawet = mb.la - 1;
+      stats[m].ladry = 0;
+    } else {
+      int nw = 0, nd = 0;
+      for (int L = 2; L <= mb.la; ++L) {
+        if (f[m].lmaskdry[L - 1]) ++nw;
+        else if ((!mb.oldmask_h.empty() && mb.oldmask_h[L - 1]) || prm[m].n < prm[m].ntstbc + 1)
+          ++nd;
+      }
+      stats[m].lawet = nw;
+      stats[m].ladry = nd;
+    }
+  }
+  return st;
+}
 }  // namespace
 
 extern "C" {
@@ -1628,6 +1945,11 @@ int32_t efdc_xm_step_batch(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fi
     no_wetdry &= prm[m].isdry == 0;
     no_baro &= !(prm[m].bsc > 1.E-6);
   }
+  if (istl == 0 && M >= 2 && !wants_system(f) && !c->calib) {
+    const int st = step_batch_chunks(c, prm, f, stats, no_wetdry, no_wetdry && no_baro);
+    if (st == EFDC_XM_CUDA_ERROR || st == EFDC_XM_BAD_ARGUMENT) return st;
+    return batch_lists_stats(c, prm, f, stats, st);
+  }
   int rc = upload_batch(c, f, no_wetdry, no_wetdry && no_baro, istl != 0);
   if (rc) {
     fill_status(stats, M, rc);
@@ -1639,24 +1961,7 @@ int32_t efdc_xm_step_batch(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fi
     fill_status(stats, M, rc);
     return rc;
   }
-  for (int m = 0; m < M; ++m) {
-    if (!(f[m].lwet || f[m].ldry)) continue;
-    const Member &mb = c->mem[m];
-    if (prm[m].isdry == 0) {
-      stats[m].lawet = mb.la - 1;
-      stats[m].ladry = 0;
-    } else {
-      int nw = 0, nd = 0;
-      for (int L = 2; L <= mb.la; ++L) {
-        if (f[m].lmaskdry[L - 1]) ++nw;
-        else if ((!mb.oldmask_h.empty() && mb.oldmask_h[L - 1]) || prm[m].n < prm[m].ntstbc + 1)
-          ++nd;
-      }
-      stats[m].lawet = nw;
-      stats[m].ladry = nd;
-    }
-  }
-  return st;
+  return batch_lists_stats(c, prm, f, stats, st);
 }
 
 }  // extern "C"

@@ -93,6 +93,9 @@ void launch_wetdry(const Launch &l, const DevStatic &S, const DevState &X, Ctl *
 void launch_final(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
                   const int *act, bool any_waste);
 void launch_reciprocals(const Launch &l, const DevStatic &S, const DevState &X, int t0, int t1);
+// copies `bytes` (a multiple of 4) from src to dst, or zeros dst when src is
+// null, with a kernel (either side may be mapped pinned host memory)
+void launch_words(cudaStream_t st, void *dst, const void *src, size_t bytes);
 // slots [d0, d1)
 void launch_scatter(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx,
                     const int *tile_member, const long long *moff, const int *mlc, int d0,

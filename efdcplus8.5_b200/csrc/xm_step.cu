@@ -1342,6 +1342,21 @@ void launch_reciprocals(const Launch &l, const DevStatic &S, const DevState &X, 
   count_launches(1);
 }
 
+// Small control blocks between device memory and mapped pinned host memory,
+// copied by a kernel: loads and stores over the link use no copy engine, so
+// they do not queue behind bulk copies in flight on other streams.
+__global__ void k_words(const unsigned *src, unsigned *dst, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    dst[i] = src ? src[i] : 0u;
+}
+void launch_words(cudaStream_t st, void *dst, const void *src, size_t bytes) {
+  const int n = int(bytes / sizeof(unsigned));
+  if (n <= 0) return;
+  k_words<<<std::min((n + 255) / 256, 1184), 256, 0, st>>>(static_cast<const unsigned *>(src),
+                                                           static_cast<unsigned *>(dst), n);
+  count_launches(1);
+}
+
 void launch_scatter(cudaStream_t st, const CopyJob *jobs, int njob, const int *lidx,
                     const int *tile_member, const long long *moff, const int *mlc, int d0,
                     int d1) {

@@ -189,3 +189,35 @@ def test_field_major_host_layout(precision):
                 assert np.array_equal(np.array(v), np.array(after[k])), (m, n, k)
     ba.close()
     bf.close()
+
+
+def test_chunked_step_equals_device_resident():
+    """efdc_xm_step_batch runs a batch in member chunks whose transfers and
+    steps overlap: with several members per chunk, back to back in host
+    memory, it gives what the unchunked upload / step_device / download gives,
+    bit for bit, and leaves the caller's ghost and padding elements alone."""
+    ms = members() + [(S.config3_member(k, 600 + 700 * k, seed=41), STEPS, 1.0)
+                      for k in range(16)]
+    ba = X.BatchSolver([scn.grid for scn, _, _ in ms])
+    bd = X.BatchSolver([scn.grid for scn, _, _ in ms])
+    sa = field_major([scn.copy_state() for scn, _, _ in ms])
+    sd = [scn.copy_state() for scn, _, _ in ms]
+    def edges(st, scn):
+        return {k: (st[k][0], st[k][scn.lc - 1], st[k][-1]) for k in STATE_F + MASK_F
+                if k in st and isinstance(st[k], np.ndarray)}
+    for n in range(1, 4):
+        prm = params_at(ms, n, X.PREC_MIXED)
+        before = [edges(sa[m], scn) for m, (scn, _, _) in enumerate(ms)]
+        sta = ba.step(prm, sa, lists=True)
+        bd.upload(sd)
+        std = bd.step_device(prm)
+        bd.download(sd, lists=True)
+        for m, (scn, _, _) in enumerate(ms):
+            assert sta[m].status == std[m].status, (m, n)
+            assert sta[m].iters_total == std[m].iters_total, (m, n)
+            assert_same(sa[m], sd[m], scn.la, f"member {m} step {n}")
+            after = edges(sa[m], scn)
+            for k, v in before[m].items():
+                assert np.array_equal(np.array(v), np.array(after[k])), (m, n, k)
+    ba.close()
+    bd.close()
