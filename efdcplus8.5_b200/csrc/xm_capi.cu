@@ -205,6 +205,12 @@ struct efdc_xm_ctx {
   // upload that carries them (tl3_alloc); tl3_ready: the device holds a
   // consistent set of levels (uploaded, or advanced by CALPUV9C steps)
   bool tl3_alloc = false, tl3_ready = false;
+  // bottom-stress producer (efdc_xm_set_bed, efdc_xm_bottom_stress_batch)
+  xm::DevBed bed{};
+  bool bed_alloc = false;
+  std::vector<char> has_bed;         // [M]
+  std::vector<xm::DragScalars> bed_sc;  // [M] the bed's scalars (delt ... filled per call)
+  xm::DragScalars *ds = nullptr;     // [M] device
 
   template <class T>
   T *alloc(size_t n, bool zero = true) {
@@ -2208,6 +2214,147 @@ int32_t efdc_xm_set_layers(efdc_xm_ctx *c, int32_t member, const efdc_xm_layers 
   }
   c->has_layers[member] = 1;
   return EFDC_XM_OK;
+}
+
+int32_t efdc_xm_set_bed(efdc_xm_ctx *c, int32_t member, const efdc_xm_bed *bed) {
+  if (!c || !bed || member < 0 || member >= c->M || !bed->zbr || !bed->stbxo || !bed->stbyo ||
+      !bed->dxp || !bed->dyp || !bed->dzc1 || !bed->sgzu1 || !bed->sgzv1 || bed->kc < 1) {
+    set_error("efdc_xm_set_bed: need a context, a member, KC >= 1 and the ZBR, STBXO, STBYO, "
+              "DXP, DYP, DZC1, SGZU1, SGZV1 arrays");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  CK(cudaSetDevice(c->device));
+  xm::DevBed &Bd = c->bed;
+  if (!c->bed_alloc) {  // zeroed: STBX, STBY start at 0 (caltbxy.f90:112-116)
+    double *b[15];
+    for (double *&p : b)
+      if (!(p = c->alloc<double>(size_t(c->nslot)))) {
+        set_error("efdc_xm_set_bed: device allocation failed");
+        return EFDC_XM_CUDA_ERROR;
+      }
+    c->ds = c->alloc<xm::DragScalars>(size_t(c->M));
+    if (!c->ds) {
+      set_error("efdc_xm_set_bed: device allocation failed");
+      return EFDC_XM_CUDA_ERROR;
+    }
+    Bd.zbr = b[0]; Bd.zbratu = b[1]; Bd.zbratv = b[2]; Bd.sgzuu = b[3]; Bd.sgzvv = b[4];
+    Bd.stbxo = b[5]; Bd.stbyo = b[6]; Bd.stbx = b[7]; Bd.stby = b[8];
+    Bd.ub = b[9]; Bd.vb = b[10]; Bd.vu = b[11]; Bd.uv = b[12]; Bd.h1u = b[13]; Bd.h1v = b[14];
+    c->has_bed.assign(c->M, 0);
+    c->bed_sc.assign(c->M, xm::DragScalars{});
+    CK(cudaDeviceSynchronize());  // the zeroing ran on the legacy stream
+    c->bed_alloc = true;
+  }
+  // the member's arrays into tile order (its slots; tile 0, the ghost tile,
+  // with member 0); DXP, DYP, DZC1, SGZU1, SGZV1 pass through the per-call
+  // input buffers, free here
+  const int M = c->M;
+  auto one = [&](const double *a) {
+    std::vector<const void *> v(M, nullptr);
+    v[member] = a;
+    return v;
+  };
+  const std::vector<Xfer> xs = {
+      Xfer{one(bed->zbr), const_cast<double *>(Bd.zbr), 0},
+      Xfer{one(bed->stbxo), const_cast<double *>(Bd.stbxo), 0},
+      Xfer{one(bed->stbyo), const_cast<double *>(Bd.stbyo), 0},
+      Xfer{one(bed->dxp), Bd.ub, 0},   Xfer{one(bed->dyp), Bd.vb, 0},
+      Xfer{one(bed->dzc1), Bd.vu, 0},  Xfer{one(bed->sgzu1), Bd.uv, 0},
+      Xfer{one(bed->sgzv1), Bd.h1u, 0}};
+  if (xs.size() > size_t(NSTAGE)) {
+    set_error("internal: too many bed arrays");
+    return EFDC_XM_CUDA_ERROR;
+  }
+  for (size_t j = 0; j < xs.size(); ++j)
+    c->jobs_h[j] = CopyJob{c->stage[j], xs[j].dev, xs[j].kind};
+  CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, xs.size() * sizeof(CopyJob), cudaMemcpyHostToDevice,
+                     c->stream));
+  int rc = copies_after_compute(c), k = 0;
+  for (size_t j = 0; !rc && j < xs.size(); ++j)
+    rc = h2d_range(c, xs[j], reinterpret_cast<char *>(c->stage[j]), member, member + 1,
+                   c->copy_stream, k);
+  if (!rc) rc = compute_after_copies(c);
+  if (rc) return rc;
+  const Member &mb = c->mem[member];
+  const int d0 = member == 0 ? 0 : mb.tile0 * xm::TILE, d1 = mb.tile1 * xm::TILE;
+  xm::launch_scatter(c->stream, c->jobs_d, int(xs.size()), c->lidx, c->tile_member, c->moff,
+                     c->mlc, d0, d1);
+  const size_t g = size_t(mb.lc) - 1;  // the ghost cell LC
+  xm::launch_bed(c->stream, c->S, Bd, Bd.ub, Bd.vb, Bd.vu, Bd.uv, Bd.h1u,
+                 bed->dxp[g] * bed->zbr[g], bed->dyp[g] * bed->zbr[g], mb.tile0, mb.tile1);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  xm::DragScalars &q = c->bed_sc[member];
+  q.avcon = bed->avcon;
+  q.vismud = bed->vismud;
+  q.visfac = 0.0258 * std::pow(bed->coeftsbl, 2. / 7.);  // caltbxy.f90:210-211
+  q.kc1 = bed->kc == 1 ? 1 : 0;
+  c->has_bed[member] = 1;
+  return EFDC_XM_OK;
+}
+
+int32_t efdc_xm_bottom_stress_batch(efdc_xm_ctx *c, const efdc_xm_drag_params *prm,
+                                    efdc_xm_drag_fields *f) {
+  if (!c || !prm || !f) {
+    set_error("efdc_xm_bottom_stress: NULL argument");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  const int M = c->M;
+  for (int m = 0; m < M; ++m) {
+    const efdc_xm_drag_fields &x = f[m];
+    if (!c->bed_alloc || !c->has_bed[m] || !(prm[m].delt > 0) || !x.ub || !x.vb || !x.vu ||
+        !x.uv || !x.h1u || !x.h1v) {
+      set_error("efdc_xm_bottom_stress: member %d: needs its bed (efdc_xm_set_bed), DELT > 0 "
+                "and the UB, VB, VU, UV, H1U, H1V arrays", m);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+    if (prm[m].isdry > 0 && c->wd_stale) {
+      set_error("efdc_xm_bottom_stress: member %d has ISDRY > 0 but the device's LMASKDRY was "
+                "left on the host by a step without wetting and drying: upload it first", m);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+  }
+  CK(cudaSetDevice(c->device));
+  xm::DevBed &Bd = c->bed;
+  std::vector<Xfer> up, dn;
+  auto per = [&](const double *efdc_xm_drag_fields::*a) {
+    std::vector<const void *> v(M);
+    for (int m = 0; m < M; ++m) v[m] = f[m].*a;
+    return v;
+  };
+  up.push_back(Xfer{per(&efdc_xm_drag_fields::ub), Bd.ub, 0});
+  up.push_back(Xfer{per(&efdc_xm_drag_fields::vb), Bd.vb, 0});
+  up.push_back(Xfer{per(&efdc_xm_drag_fields::vu), Bd.vu, 0});
+  up.push_back(Xfer{per(&efdc_xm_drag_fields::uv), Bd.uv, 0});
+  up.push_back(Xfer{per(&efdc_xm_drag_fields::h1u), Bd.h1u, 0});
+  up.push_back(Xfer{per(&efdc_xm_drag_fields::h1v), Bd.h1v, 0});
+  int rc = upload_arrays(c, up);
+  if (rc) return rc;
+  for (int m = 0; m < M; ++m) {
+    xm::DragScalars q = c->bed_sc[m];
+    q.delt = prm[m].delt;
+    q.avcon1 = prm[m].avcon1;
+    q.isdry = prm[m].isdry;
+    q.n = prm[m].n;
+    q.ntstbc = prm[m].ntstbc;
+    q.on = 1;
+    c->bed_sc[m] = q;
+  }
+  CK(cudaMemcpyAsync(c->ds, c->bed_sc.data(), sizeof(xm::DragScalars) * M,
+                     cudaMemcpyHostToDevice, c->stream));
+  xm::launch_tbxy(c->L(), c->S, c->X, Bd, c->ds);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));  // the host copy of the scalars may change after this
+  rc = 0;
+#define XM_DN(name, dev)                                                        \
+  {                                                                             \
+    std::vector<const void *> v(M);                                             \
+    for (int m = 0; m < M; ++m) v[m] = f[m].name;                               \
+    if ((rc = collect(c, dn, v, dev, 0, #name))) return rc;                     \
+  }
+  XM_DN(stbx, Bd.stbx) XM_DN(stby, Bd.stby) XM_DN(tbx, c->X.tbx) XM_DN(tby, c->X.tby)
+#undef XM_DN
+  return download_arrays(c, dn);
 }
 
 int32_t efdc_xm_set_channels(efdc_xm_ctx *c, int32_t member, const efdc_xm_channels *ch) {

@@ -177,6 +177,25 @@ struct SysView {
   int unscaled;  // 1: RSQ = sum(r^2) / CCMNM^2
 };
 
+// Bottom-stress producer (CALTBXY's drag coefficients and the bottom stresses
+// TBX, TBY): the static bed of the members that have one, the drag
+// coefficients kept between calls, and each call's internal-mode inputs, in
+// tile order.
+struct DevBed {
+  const double *zbr, *zbratu, *zbratv, *sgzuu, *sgzvv, *stbxo, *stbyo;
+  double *stbx, *stby;                      // STBX, STBY (0 before the first call)
+  double *ub, *vb, *vu, *uv, *h1u, *h1v;    // U, V of the bottom layer, VU, UV, H1U, H1V
+};
+
+// Per-member scalars of one bottom-stress call.
+struct DragScalars {
+  double delt, avcon1, avcon, vismud, visfac;
+  int isdry, n, ntstbc;
+  int kc1;  // KC = 1: the single-layer form of the rough drag
+  int on;   // the member takes part (it has a bed)
+  int pad;
+};
+
 // Open-boundary cells (packed per member: W, E, S, N in the reference's loop order).
 struct DevObc {
   int n;                 // total number of open-boundary cells

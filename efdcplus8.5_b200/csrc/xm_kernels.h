@@ -93,6 +93,13 @@ void launch_wetdry(const Launch &l, const DevStatic &S, const DevState &X, Ctl *
 void launch_final(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
                   const int *act, bool any_waste);
 void launch_reciprocals(const Launch &l, const DevStatic &S, const DevState &X, int t0, int t1);
+// the bed's derived arrays (ZBRATU, ZBRATV, SGZUU, SGZVV) of the tiles [t0, t1)
+void launch_bed(cudaStream_t st, const DevStatic &S, const DevBed &Bd, const double *dxp,
+                const double *dyp, const double *dzc1, const double *sgzu1, const double *sgzv1,
+                double gu, double gv, int t0, int t1);
+// the bottom-stress producer (CALTBXY + TBX/TBY) of the members with ds[m].on
+void launch_tbxy(const Launch &l, const DevStatic &S, const DevState &X, const DevBed &Bd,
+                 const DragScalars *ds);
 // copies `bytes` (a multiple of 4) from src to dst, or zeros dst when src is
 // null, with a kernel (either side may be mapped pinned host memory)
 void launch_words(cudaStream_t st, void *dst, const void *src, size_t bytes);

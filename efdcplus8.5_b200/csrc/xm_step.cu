@@ -1342,6 +1342,112 @@ void launch_reciprocals(const Launch &l, const DevStatic &S, const DevState &X, 
   count_launches(1);
 }
 
+// ---------------------------------------------------------------------------
+// Bottom-stress producer: CALTBXY's drag coefficients (caltbxy.f90:476-539,
+// ISWAVE = ISVEG = ISMUD = ISITB = 0: CDLIMIT = 0.5) and the bottom stresses of
+// hdmt2t.f90:670-684, over the wet cells (LWET: every cell with ISDRY = 0,
+// else the cells with LMASKDRY); the faces of the cells of LDRY (not wet, and
+// dry at entry or N < NTSTBC+1) get TBX = TBY = 0 (caltbxy.f90:213-229), the
+// others keep theirs.  HU, HV, LMASKDRY and the entry mask are the state the
+// last step left on the device.
+__global__ void __launch_bounds__(NT) k_tbxy(DevStatic S, DevState X, DevBed Bd,
+                                            const DragScalars *ds, int ntile) {
+  TILE_LOOP(ntile) {
+    const DragScalars &q = ds[S.tile_member[tile]];
+    if (!q.on) continue;
+    const Nb nb = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = nb.d;
+    if (S.kind[d] == LAND) continue;
+    if (!(q.isdry == 0 || X.lmaskdry[d] != 0)) {
+      auto ldry = [&](int s) {
+        return S.kind[s] != LAND && X.lmaskdry[s] == 0 &&
+               (X.oldmask[s] != 0 || q.n < q.ntstbc + 1);
+      };
+      const bool dd = ldry(d);  // TBX(L), TBX(LEC(L)) of the cells L of LDRY
+      double *TBX = const_cast<double *>(X.tbx), *TBY = const_cast<double *>(X.tby);
+      if (dd || ldry(nb.w)) TBX[d] = 0.;
+      if (dd || ldry(nb.s)) TBY[d] = 0.;
+      continue;
+    }
+    const double U = Bd.ub[d], V = Bd.vb[d], VU = Bd.vu[d], UV = Bd.uv[d];
+    const double hu = X.hu[d], hv = X.hv[d];
+    const double stbxo = Bd.stbxo[d], stbyo = Bd.stbyo[d];
+    double stbx, stby;
+    if (Bd.zbr[d] <= 1.E-6) {  // :480-502 smooth (viscous) drag
+      const double UMAG = sqrt(U * U + VU * VU + 1.E-12);
+      const double VMAG = sqrt(UV * UV + V * V + 1.E-12);
+      const double CDMAXU = 0.5 * stbxo * hu / (q.delt * UMAG);
+      const double CDMAXV = 0.5 * stbyo * hv / (q.delt * VMAG);
+      double VISDHU = 0.0, VISDHV = 0.0;
+      if (UMAG > 0.0) VISDHU = (q.vismud * (1. / hu) / UMAG) * (2. / 7.);
+      if (VMAG > 0.0) VISDHV = (q.vismud * (1. / hv) / VMAG) * (2. / 7.);
+      stbx = fmin(CDMAXU, q.visfac * q.avcon * stbxo * VISDHU);
+      stby = fmin(CDMAXV, q.visfac * q.avcon * stbyo * VISDHV);
+    } else {  // :504-537 rough (log-law) drag
+      const double UMAG = sqrt(VU * VU + U * U + 1.E-12);
+      const double VMAG = sqrt(UV * UV + V * V + 1.E-12);
+      const double CDMAXU = 0.5 * stbxo * hu / (q.delt * UMAG);
+      const double CDMAXV = 0.5 * stbyo * hv / (q.delt * VMAG);
+      const double zu = Bd.zbratu[d], zv = Bd.zbratv[d];
+      const double HURTMP = fmax(zu, Bd.h1u[d]);
+      const double HVRTMP = fmax(zv, Bd.h1v[d]);
+      if (q.kc1) {
+        const double lu = log(fmax(0.5 * HURTMP / zu, 7.5)) - 1.;
+        const double lv = log(fmax(0.5 * HVRTMP / zv, 7.5)) - 1.;
+        stbx = stbxo * .16 / (lu * lu);
+        stby = stbyo * .16 / (lv * lv);
+      } else {
+        const double lu = log(fmax(1. + Bd.sgzuu[d] * HURTMP / zu, 7.5));
+        const double lv = log(fmax(1. + Bd.sgzvv[d] * HVRTMP / zv, 7.5));
+        stbx = q.avcon * stbxo * .16 / (lu * lu);
+        stby = q.avcon * stbyo * .16 / (lv * lv);
+      }
+      stbx = fmin(CDMAXU, stbx);
+      stby = fmin(CDMAXV, stby);
+    }
+    Bd.stbx[d] = stbx;
+    Bd.stby[d] = stby;
+    // hdmt2t.f90:682-683 (TBX, TBY are inputs of the step: written here only)
+    const_cast<double *>(X.tbx)[d] = (q.avcon1 * (1. / hu) + stbx * sqrt(VU * VU + U * U)) * U;
+    const_cast<double *>(X.tby)[d] = (q.avcon1 * (1. / hv) + stby * sqrt(UV * UV + V * V)) * V;
+  }
+}
+// The bed's derived arrays of member m's slots (caltbxy.f90:81-90, layer 1):
+// ZBRATU from the west neighbour's DXP*ZBR (a land neighbour is the ghost
+// cell LC, LWC(L) = LC: gu = DXP(LC)*ZBR(LC), gv = DYP(LC)*ZBR(LC) of the
+// member), SGZUU = 0.5*MAX(DZC, SGZU).
+__global__ void __launch_bounds__(NT) k_bed(DevStatic S, DevBed Bd, const double *dxp,
+                                           const double *dyp, const double *dzc1,
+                                           const double *sgzu1, const double *sgzv1, double gu,
+                                           double gv, int t0, int t1) {
+  for (int tile = t0 + blockIdx.x; tile < t1; tile += gridDim.x) {
+    const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
+    const int d = q.d;
+    if (S.kind[d] == LAND) continue;
+    const double *Z = Bd.zbr;
+    const double wu = S.kind[q.w] == LAND ? gu : dxp[q.w] * Z[q.w];
+    const double wv = S.kind[q.s] == LAND ? gv : dyp[q.s] * Z[q.s];
+    const_cast<double *>(Bd.zbratu)[d] = 0.5 * (wu + dxp[d] * Z[d]) * S.dxiu[d];
+    const_cast<double *>(Bd.zbratv)[d] = 0.5 * (wv + dyp[d] * Z[d]) * S.dyiv[d];
+    const_cast<double *>(Bd.sgzuu)[d] = 0.5 * fmax(dzc1[d], sgzu1[d]);
+    const_cast<double *>(Bd.sgzvv)[d] = 0.5 * fmax(dzc1[d], sgzv1[d]);
+  }
+}
+void launch_bed(cudaStream_t st, const DevStatic &S, const DevBed &Bd, const double *dxp,
+                const double *dyp, const double *dzc1, const double *sgzu1, const double *sgzv1,
+                double gu, double gv, int t0, int t1) {
+  if (t1 <= t0) return;
+  k_bed<<<std::min(t1 - t0, 4096), NT, 0, st>>>(S, Bd, dxp, dyp, dzc1, sgzu1, sgzv1, gu, gv, t0,
+                                                t1);
+  count_launches(1);
+}
+
+void launch_tbxy(const Launch &l, const DevStatic &S, const DevState &X, const DevBed &Bd,
+                 const DragScalars *ds) {
+  k_tbxy<<<l.grid, NT, 0, l.stream>>>(S, X, Bd, ds, l.ntile);
+  count_launches(1);
+}
+
 // Small control blocks between device memory and mapped pinned host memory,
 // copied by a kernel: loads and stores over the link use no copy engine, so
 // they do not queue behind bulk copies in flight on other streams.

@@ -78,6 +78,27 @@ class Layers(C.Structure):
     _fields_ = [("kc", C.c_int32), ("ld", C.c_int32), ("dzc", _pd), ("zz", _pd)]
 
 
+class Bed(C.Structure):
+    _fields_ = [("zbr", _pd), ("stbxo", _pd), ("stbyo", _pd), ("dxp", _pd), ("dyp", _pd),
+                ("dzc1", _pd), ("sgzu1", _pd), ("sgzv1", _pd), ("kc", C.c_int32),
+                ("pad_", C.c_int32), ("avcon", C.c_double), ("vismud", C.c_double),
+                ("coeftsbl", C.c_double)]
+
+
+class DragParams(C.Structure):
+    _fields_ = [("delt", C.c_double), ("avcon1", C.c_double), ("isdry", C.c_int32),
+                ("n", C.c_int32), ("ntstbc", C.c_int32), ("pad_", C.c_int32)]
+
+
+class DragFields(C.Structure):
+    _fields_ = [("ub", _pd), ("vb", _pd), ("vu", _pd), ("uv", _pd), ("h1u", _pd), ("h1v", _pd),
+                ("stbx", _pd), ("stby", _pd), ("tbx", _pd), ("tby", _pd)]
+
+
+DRAG_IN = ("ub", "vb", "vu", "uv", "h1u", "h1v")
+DRAG_OUT = ("stbx", "stby", "tbx", "tby")
+
+
 class Channels(C.Structure):
     _fields_ = [("n", C.c_int32), ("type", _pi), ("lhost", _pi), ("lu", _pi), ("lv", _pi),
                 ("chanlen", _pd), ("chanfric", _pd), ("dxp", _pd), ("dyp", _pd)]
@@ -205,6 +226,42 @@ def make_layers(ly: dict | None):
     s.kc, s.ld = int(keep[0].shape[0]), int(keep[0].shape[1])
     s.dzc, s.zz = _dp(keep[0]), _dp(keep[1])
     return s, keep
+
+
+def make_bed(bed: dict):
+    """A Bed struct over {"zbr", "stbxo", "stbyo", "dxp", "dyp", "dzc1", "sgzu1",
+    "sgzv1"} (float64 over 1..LC) and the scalars kc, avcon, vismud, coeftsbl.
+    Returns (struct, kept arrays)."""
+    keys = ("zbr", "stbxo", "stbyo", "dxp", "dyp", "dzc1", "sgzu1", "sgzv1")
+    keep = [np.ascontiguousarray(bed[k], dtype=np.float64) for k in keys]
+    s = Bed()
+    for k, a in zip(keys, keep):
+        setattr(s, k, _dp(a))
+    s.kc = int(bed.get("kc", 1))
+    s.avcon = float(bed.get("avcon", 1.0))
+    s.vismud = float(bed.get("vismud", 1e-6))
+    s.coeftsbl = float(bed.get("coeftsbl", 4.0))
+    return s, keep
+
+
+def make_drag_params(p: dict, *, n: int):
+    s = DragParams()
+    s.delt = float(p["dt"])
+    s.avcon1 = float(p.get("avcon1", 0.0))
+    s.isdry = int(p["isdry"])
+    s.n = n
+    s.ntstbc = int(p.get("ntstbc", 0))
+    return s
+
+
+def make_drag_fields(d: dict):
+    """A DragFields struct over the arrays of d (DRAG_IN in, DRAG_OUT out)."""
+    s = DragFields()
+    for k in DRAG_IN + DRAG_OUT:
+        a = d.get(k)
+        if a is not None:
+            setattr(s, k, _dp(a))
+    return s
 
 
 def make_channels(ch: dict | None):
@@ -348,6 +405,11 @@ def load(path: str | os.PathLike | None = None):
     lib.efdc_xm_download_batch.argtypes = [C.c_void_p, C.POINTER(Fields)]
     lib.efdc_xm_step_device_batch.restype = C.c_int32
     lib.efdc_xm_step_device_batch.argtypes = [C.c_void_p, C.POINTER(Params), C.POINTER(Stats)]
+    lib.efdc_xm_set_bed.restype = C.c_int32
+    lib.efdc_xm_set_bed.argtypes = [C.c_void_p, C.c_int32, C.POINTER(Bed)]
+    lib.efdc_xm_bottom_stress_batch.restype = C.c_int32
+    lib.efdc_xm_bottom_stress_batch.argtypes = [C.c_void_p, C.POINTER(DragParams),
+                                                C.POINTER(DragFields)]
     if path is None:
         _lib = lib
     return lib
@@ -416,6 +478,21 @@ class Solver:
         rc = self.lib.efdc_xm_set_layers(self.ctx, member, C.byref(s))
         if rc != OK:
             raise RuntimeError(f"efdc_xm_set_layers: {STATUS_NAMES.get(rc, rc)}: "
+                               f"{self.last_error()}")
+
+    def set_bed(self, bed: dict, member: int = 0):
+        s, _keep = make_bed(bed)
+        rc = self.lib.efdc_xm_set_bed(self.ctx, member, C.byref(s))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_set_bed: {STATUS_NAMES.get(rc, rc)}: {self.last_error()}")
+
+    def bottom_stress(self, params: DragParams, drag: dict):
+        """CALTBXY + TBX/TBY on the device (efdc_xm_bottom_stress_batch); the
+        outputs present in `drag` are written."""
+        f = make_drag_fields(drag)
+        rc = self.lib.efdc_xm_bottom_stress_batch(self.ctx, C.byref(params), C.byref(f))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_bottom_stress_batch: {STATUS_NAMES.get(rc, rc)}: "
                                f"{self.last_error()}")
 
     def set_channels(self, ch: dict | None, member: int = 0):
@@ -548,6 +625,20 @@ class BatchSolver:
         rc = self.lib.efdc_xm_set_layers(self.ctx, member, C.byref(s))
         if rc != OK:
             raise RuntimeError(f"efdc_xm_set_layers: {STATUS_NAMES.get(rc, rc)}: "
+                               f"{self.last_error()}")
+
+    def set_bed(self, bed: dict, member: int):
+        s, _keep = make_bed(bed)
+        rc = self.lib.efdc_xm_set_bed(self.ctx, member, C.byref(s))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_set_bed: {STATUS_NAMES.get(rc, rc)}: {self.last_error()}")
+
+    def bottom_stress(self, params: list, drags: list):
+        fa = (DragFields * self.m)(*[make_drag_fields(d) for d in drags])
+        pa = (DragParams * self.m)(*params)
+        rc = self.lib.efdc_xm_bottom_stress_batch(self.ctx, pa, fa)
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_bottom_stress_batch: {STATUS_NAMES.get(rc, rc)}: "
                                f"{self.last_error()}")
 
     def set_channels(self, ch: dict | None, member: int):

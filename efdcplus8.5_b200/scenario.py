@@ -657,3 +657,34 @@ def three_level_schedule(nsteps: int, ntstbc: int):
 def three_level_params(params: dict, istl: int, nctbc: int, rold: float, rnew: float) -> dict:
     """The parameters of one CALPUV9C(ISTL) call (DELT = 2*DT for ISTL = 3)."""
     return dict(params, tl3_istl=istl, nctbc=nctbc, rold=rold, rnew=rnew)
+
+
+def make_bed(scn: Scenario, *, seed: int = 0, kc: int = 1, smooth_frac: float = 0.1,
+             zbr=(0.002, 0.05)) -> dict:
+    """A seeded bed for the bottom-stress producer (efdc_xm_bed): roughness
+    heights ZBR log-uniform in `zbr` with a fraction `smooth_frac` of smooth
+    cells (ZBR = 0: the viscous form), drag multipliers STBXO = STBYO = 1,
+    DXP/DYP of the grid, and uniform sigma layers (DZC = SGZU = SGZV = 1/KC)."""
+    rng = np.random.default_rng(seed)
+    lcm = scn.lc + 1
+    z = np.exp(rng.uniform(np.log(zbr[0]), np.log(zbr[1]), lcm))
+    z[rng.random(lcm) < smooth_frac] = 0.0
+    one = np.ones(lcm)
+    return dict(zbr=z, stbxo=one.copy(), stbyo=one.copy(), dxp=scn.grid["dxp"].copy(),
+                dyp=scn.grid["dyp"].copy(), dzc1=one / kc, sgzu1=one / kc, sgzv1=one / kc,
+                kc=kc, avcon=1.0, vismud=1e-6, coeftsbl=4.0)
+
+
+def drag_inputs(scn: Scenario, st: dict, h1u, h1v, *, seed: int = 0) -> dict:
+    """Internal-mode inputs of the bottom-stress producer for the state `st`:
+    the depth-averaged face velocities UHDYE/(HU*DYU) as the bottom-layer U, V
+    (one layer), and seeded cross-face velocities VU, UV of the same size."""
+    rng = np.random.default_rng(seed)
+    g = scn.grid
+    with np.errstate(all="ignore"):  # ghost elements: HU = 0
+        ub = np.nan_to_num(st["uhdye"] * g["dyiu"] / st["hu"], nan=0.0, posinf=0.0, neginf=0.0)
+        vb = np.nan_to_num(st["vhdxe"] * g["dxiv"] / st["hv"], nan=0.0, posinf=0.0, neginf=0.0)
+    s = max(1e-3, float(np.abs(ub).max()))
+    return dict(ub=ub, vb=vb, vu=0.5 * s * rng.standard_normal(ub.size),
+                uv=0.5 * s * rng.standard_normal(ub.size), h1u=np.asarray(h1u, float).copy(),
+                h1v=np.asarray(h1v, float).copy())

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define EFDC_XM_ABI_VERSION 3
+#define EFDC_XM_ABI_VERSION 4
 
 /* Status codes.  The reference STOPs where these are returned. */
 enum efdc_xm_status {
@@ -258,6 +258,46 @@ typedef struct efdc_xm_layers {
   const double *dzc, *zz;
 } efdc_xm_layers;
 int32_t efdc_xm_set_layers(efdc_xm_ctx *ctx, int32_t member, const efdc_xm_layers *ly);
+
+/* Bottom stress producer: CALTBXY's bed drag coefficients STBX, STBY
+ * (caltbxy.f90:455-537 for ISWAVE = 0, ISVEG = 0, ISMUD = 0, ISITB = 0: the
+ * rough log-law form where ZBR > 1e-6, the smooth viscous form elsewhere)
+ * and the bottom stresses TBX, TBY of hdmt2t.f90:670-684, computed on the
+ * device from the state the last step left there (HU, HV, LMASKDRY and the
+ * entry mask) and the bottom-layer velocities of the internal mode.  The
+ * stresses stay on the device for the next step: a step given TBX, TBY = NULL
+ * then uses them without an upload.  No reference counterpart as a separate
+ * call: it replaces CALL CALTBXY(ISTL,IS2TL) and the TBX/TBY loop at
+ * hdmt2t.f90:669-684 when the external mode runs on the GPU. */
+typedef struct efdc_xm_bed {        /* static, per member (efdc_xm_set_bed)        */
+  const double *zbr;                /* ZBR(L), bed roughness height                */
+  const double *stbxo, *stbyo;      /* STBX, STBY as read (the multipliers STBXO,
+                                       STBYO of caltbxy.f90:84-87)                 */
+  const double *dxp, *dyp;          /* DXP, DYP                                    */
+  const double *dzc1;               /* DZC(L,1): thickness fraction of layer 1     */
+  const double *sgzu1, *sgzv1;      /* SGZU(L,1), SGZV(L,1) (caltbxy.f90:71-76)    */
+  int32_t kc;                       /* KC (1: the single-layer form, :518-526)     */
+  int32_t pad_;
+  double avcon;                     /* AVCON                                       */
+  double vismud, coeftsbl;          /* VISMUD, COEFTSBL (the smooth form)          */
+} efdc_xm_bed;
+int32_t efdc_xm_set_bed(efdc_xm_ctx *ctx, int32_t member, const efdc_xm_bed *bed);
+
+typedef struct efdc_xm_drag_params { /* per member and call                       */
+  double delt;                      /* DELT of CALTBXY (caltbxy.f90:30-42)        */
+  double avcon1;                    /* AVCON1 (hdmt2t.f90:682)                     */
+  int32_t isdry, n, ntstbc, pad_;   /* ISDRY, N, NTSTBC: the dry-cell list LDRY   */
+} efdc_xm_drag_params;
+
+typedef struct efdc_xm_drag_fields { /* per member and call                        */
+  const double *ub, *vb;            /* U(L,KSZU(L)), V(L,KSZV(L)): layer 1 here   */
+  const double *vu, *uv;            /* VU, UV                                      */
+  const double *h1u, *h1v;          /* H1U, H1V                                    */
+  double *stbx, *stby;              /* out (optional): STBX, STBY                  */
+  double *tbx, *tby;                /* out (optional): TBX, TBY                    */
+} efdc_xm_drag_fields;
+int32_t efdc_xm_bottom_stress_batch(efdc_xm_ctx *ctx, const efdc_xm_drag_params *prm,
+                                    efdc_xm_drag_fields *f);
 
 /* Standalone replacement of CONGRAD (congrad.f90:1-191) for callers that
  * assemble the scaled system themselves (e.g. calpuv9c.f90:446).  Arrays are

@@ -67,6 +67,12 @@ struct oracle_ctx {
   // and the buoyancy integrals, kept between calls like the module arrays
   int kc = 0;
   std::vector<double> dzc, zz, bi1, bi2, be;
+  // bottom-stress producer (CALTBXY): the bed, 1-based over 1..LC, and the
+  // drag coefficients kept between calls (zero before the first)
+  bool bed = false;
+  int bed_kc = 0;
+  double avcon = 0., vismud = 0., visfac = 0.;
+  std::vector<double> zbr, zbratu, zbratv, sgzuu, sgzvv, stbxo, stbyo, stbx, stby;
 };
 
 namespace {
@@ -1222,6 +1228,124 @@ int oracle_set_channels(oracle_ctx *c, const efdc_xm_channels *in) {
   for (auto *v : {&ch.cu, &ch.cv, &ch.chh, &ch.qut, &ch.qvt}) v->assign(n, 0.0);
   ch.iact.assign(n, 0);
   c->p1.assign(size_t(c->lc) + 2, 0.0);
+  return EFDC_XM_OK;
+}
+
+int oracle_set_bed(oracle_ctx *c, const efdc_xm_bed *b) {
+  if (!c || !b || !b->zbr || !b->stbxo || !b->stbyo || !b->dxp || !b->dyp || !b->dzc1 ||
+      !b->sgzu1 || !b->sgzv1 || b->kc < 1)
+    return EFDC_XM_BAD_ARGUMENT;
+  const int lc = c->lc, la = c->la;
+  copy1(c->zbr, b->zbr, lc);
+  copy1(c->stbxo, b->stbxo, lc);  // STBXO(L)=STBX(L) (caltbxy.f90:108-111)
+  copy1(c->stbyo, b->stbyo, lc);
+  std::vector<double> dxp, dyp, dzc1, sgzu1, sgzv1;
+  copy1(dxp, b->dxp, lc);
+  copy1(dyp, b->dyp, lc);
+  copy1(dzc1, b->dzc1, lc);
+  copy1(sgzu1, b->sgzu1, lc);
+  copy1(sgzv1, b->sgzv1, lc);
+  c->zbratu.assign(size_t(lc) + 2, 0.);
+  c->zbratv.assign(size_t(lc) + 2, 0.);
+  c->sgzuu.assign(size_t(lc) + 2, 0.);
+  c->sgzvv.assign(size_t(lc) + 2, 0.);
+  for (int L = 2; L <= la; ++L) {  // caltbxy.f90:81-90 (layer 1: KSZU = KSZV = 1)
+    const int LW = c->lwc[L], LS = c->lsc[L];
+    c->zbratu[L] = 0.5 * (dxp[LW] * c->zbr[LW] + dxp[L] * c->zbr[L]) * c->dxiu[L];
+    c->zbratv[L] = 0.5 * (dyp[LS] * c->zbr[LS] + dyp[L] * c->zbr[L]) * c->dyiv[L];
+    c->sgzuu[L] = 0.5 * std::max(dzc1[L], sgzu1[L]);
+    c->sgzvv[L] = 0.5 * std::max(dzc1[L], sgzv1[L]);
+  }
+  c->stbx.assign(size_t(lc) + 2, 0.);  // STBX(L)=0. (:112-116)
+  c->stby.assign(size_t(lc) + 2, 0.);
+  c->bed_kc = b->kc;
+  c->avcon = b->avcon;
+  c->vismud = b->vismud;
+  c->visfac = 0.0258 * std::pow(b->coeftsbl, 2. / 7.);  // :210-211
+  c->bed = true;
+  return EFDC_XM_OK;
+}
+
+int oracle_bottom_stress(oracle_ctx *c, const efdc_xm_drag_params *p, const efdc_xm_fields *st,
+                         efdc_xm_drag_fields *f) {
+  if (!c || !p || !st || !f || !c->bed || !st->hu || !st->hv || !f->ub || !f->vb || !f->vu ||
+      !f->uv || !f->h1u || !f->h1v || !f->tbx || !f->tby || !(p->delt > 0) ||
+      (p->isdry > 0 && !st->lmaskdry))
+    return EFDC_XM_BAD_ARGUMENT;
+  const int la = c->la;
+  const F<const double> HU{st->hu}, HV{st->hv}, U{f->ub}, V{f->vb}, VU{f->vu}, UV{f->uv},
+      H1U{f->h1u}, H1V{f->h1v};
+  F<double> TBX{f->tbx}, TBY{f->tby};
+  const double DELT = p->delt;
+  const double CDLIMIT = 0.5;        // ISITB = 0 (caltbxy.f90:172-180)
+  const double VISEXP = 2. / 7.;     // :210
+  const double VISFAC = c->visfac;
+  const double AVCON = c->avcon;
+  double *STBX = c->stbx.data(), *STBY = c->stby.data();
+  const double *STBXO = c->stbxo.data(), *STBYO = c->stbyo.data(), *ZBR = c->zbr.data();
+  auto wet = [&](int L) { return p->isdry == 0 || st->lmaskdry[L - 1] != 0; };
+  // :213-229 cells of LDRY (calpuv2c.f90:1061-1080): TBX, TBY of their faces to zero
+  if (p->isdry > 0)
+    for (int L = 2; L <= la; ++L) {
+      if (wet(L) || !(c->oldmask[L] || p->n < p->ntstbc + 1)) continue;
+      TBX[L] = 0.;
+      TBY[L] = 0.;
+      TBX[c->lec[L]] = 0.;
+      TBY[c->lnc[L]] = 0.;
+    }
+  for (int L = 2; L <= la; ++L) {  // :476-539 over LWET
+    if (!wet(L)) continue;
+    if (ZBR[L] <= 1.E-6) {  // :480-502 smooth (viscous) drag, ISMUD = 0
+      const double UMAGTMP = std::sqrt(U[L] * U[L] + VU[L] * VU[L] + 1.E-12);
+      const double VMAGTMP = std::sqrt(UV[L] * UV[L] + V[L] * V[L] + 1.E-12);
+      const double CDMAXU = CDLIMIT * STBXO[L] * HU[L] / (DELT * UMAGTMP);
+      const double CDMAXV = CDLIMIT * STBYO[L] * HV[L] / (DELT * VMAGTMP);
+      const double HUI = 1. / HU[L], HVI = 1. / HV[L];
+      double VISDHU = 0.0, VISDHV = 0.0;
+      if (UMAGTMP > 0.0) VISDHU = (c->vismud * HUI / UMAGTMP) * VISEXP;
+      if (VMAGTMP > 0.0) VISDHV = (c->vismud * HVI / VMAGTMP) * VISEXP;
+      STBX[L] = VISFAC * AVCON * STBXO[L] * VISDHU;
+      STBY[L] = VISFAC * AVCON * STBYO[L] * VISDHV;
+      STBX[L] = std::min(CDMAXU, STBX[L]);
+      STBY[L] = std::min(CDMAXV, STBY[L]);
+    } else {  // :504-537 rough (log-law) drag
+      const double UMAGTMP = std::sqrt(VU[L] * VU[L] + U[L] * U[L] + 1.E-12);
+      const double VMAGTMP = std::sqrt(UV[L] * UV[L] + V[L] * V[L] + 1.E-12);
+      const double CDMAXU = CDLIMIT * STBXO[L] * HU[L] / (DELT * UMAGTMP);
+      const double CDMAXV = CDLIMIT * STBYO[L] * HV[L] / (DELT * VMAGTMP);
+      const double HURTMP = std::max(c->zbratu[L], H1U[L]);
+      const double HVRTMP = std::max(c->zbratv[L], H1V[L]);
+      if (c->bed_kc == 1) {  // KSZ(L) == KC
+        double HUDZBR = 0.5 * HURTMP / c->zbratu[L];
+        HUDZBR = std::max(HUDZBR, 7.5);
+        double HVDZBR = 0.5 * HVRTMP / c->zbratv[L];
+        HVDZBR = std::max(HVDZBR, 7.5);
+        const double lu = std::log(HUDZBR) - 1., lv = std::log(HVDZBR) - 1.;
+        STBX[L] = STBXO[L] * .16 / (lu * lu);
+        STBY[L] = STBYO[L] * .16 / (lv * lv);
+      } else {
+        double DZHUDZBR = 1. + c->sgzuu[L] * HURTMP / c->zbratu[L];
+        double DZHVDZBR = 1. + c->sgzvv[L] * HVRTMP / c->zbratv[L];
+        DZHUDZBR = std::max(DZHUDZBR, 7.5);
+        DZHVDZBR = std::max(DZHVDZBR, 7.5);
+        const double lu = std::log(DZHUDZBR), lv = std::log(DZHVDZBR);
+        STBX[L] = AVCON * STBXO[L] * .16 / (lu * lu);
+        STBY[L] = AVCON * STBYO[L] * .16 / (lv * lv);
+      }
+      STBX[L] = std::min(CDMAXU, STBX[L]);
+      STBY[L] = std::min(CDMAXV, STBY[L]);
+    }
+  }
+  for (int L = 2; L <= la; ++L) {  // hdmt2t.f90:670-684 over LWET
+    if (!wet(L)) continue;
+    const double USGZ = U[L], VSGZ = V[L];
+    TBX[L] = (p->avcon1 * (1. / HU[L]) + STBX[L] * std::sqrt(VU[L] * VU[L] + USGZ * USGZ)) * USGZ;
+    TBY[L] = (p->avcon1 * (1. / HV[L]) + STBY[L] * std::sqrt(UV[L] * UV[L] + VSGZ * VSGZ)) * VSGZ;
+  }
+  for (int L = 1; L <= c->lc; ++L) {
+    if (f->stbx) f->stbx[L - 1] = STBX[L];
+    if (f->stby) f->stby[L - 1] = STBY[L];
+  }
   return EFDC_XM_OK;
 }
 

@@ -1,7 +1,8 @@
 /*
  * efdc_oracle.h -- TEST INFRASTRUCTURE ONLY (the checker, never the product).
  *
- * CPU FP64 restatement of EFDC+ 8.5's 2TL external mode, used by tests/ and by
+ * CPU FP64 restatement of EFDC+ 8.5's external mode (and its bottom-stress
+ * producer), used by tests/ and by
  * bench.py's CPU-baseline leg to check and time the CUDA library.  Nothing in
  * the shipped library links or calls this code.
  *
@@ -50,6 +51,16 @@ int oracle_set_channels(oracle_ctx *c, const efdc_xm_channels *ch);
 
 /* Layers of the standard sigma grid for CALEBI (efdc_xm_set_layers' contract). */
 int oracle_set_layers(oracle_ctx *c, const efdc_xm_layers *ly);
+
+/* The bed of the bottom-stress producer (efdc_xm_set_bed's contract). */
+int oracle_set_bed(oracle_ctx *c, const efdc_xm_bed *bed);
+
+/* CALTBXY's drag coefficients and the bottom stresses of hdmt2t.f90:670-684
+ * (efdc_xm_bottom_stress_batch's contract) on the state `st` the last
+ * oracle_step left (HU, HV, LMASKDRY; its entry mask is the context's);
+ * TBX, TBY in/out in f. */
+int oracle_bottom_stress(oracle_ctx *c, const efdc_xm_drag_params *p, const efdc_xm_fields *st,
+                         efdc_xm_drag_fields *f);
 
 int oracle_congrad(oracle_ctx *c, const double *ccc, const double *ccs,
                    const double *ccn, const double *ccw, const double *cce,

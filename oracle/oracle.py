@@ -46,6 +46,11 @@ def load():
         lib.oracle_set_layers.argtypes = [C.c_void_p, C.POINTER(X.Layers)]
         lib.oracle_set_channels.restype = C.c_int
         lib.oracle_set_channels.argtypes = [C.c_void_p, C.POINTER(X.Channels)]
+        lib.oracle_set_bed.restype = C.c_int
+        lib.oracle_set_bed.argtypes = [C.c_void_p, C.POINTER(X.Bed)]
+        lib.oracle_bottom_stress.restype = C.c_int
+        lib.oracle_bottom_stress.argtypes = [C.c_void_p, C.POINTER(X.DragParams),
+                                             C.POINTER(X.Fields), C.POINTER(X.DragFields)]
         lib.oracle_congrad.restype = C.c_int
         lib.oracle_congrad.argtypes = [C.c_void_p] + [pd] * 8 + [
             C.c_double, C.c_int, C.POINTER(C.c_int), pd]
@@ -91,6 +96,18 @@ class Oracle:
         rc = self.lib.oracle_set_channels(self.ctx, C.byref(s))
         if rc != 0:
             raise RuntimeError("oracle_set_channels: bad channel arrays")
+
+    def set_bed(self, bed: dict):
+        s, _keep = X.make_bed(bed)
+        if self.lib.oracle_set_bed(self.ctx, C.byref(s)) != 0:
+            raise RuntimeError("oracle_set_bed: bad bed arrays")
+
+    def bottom_stress(self, params: X.DragParams, state: dict, drag: dict) -> int:
+        """CALTBXY + TBX/TBY on the state the last step left; TBX, TBY of `drag`
+        in/out."""
+        f, _k = X.make_fields(state)
+        d = X.make_drag_fields(drag)
+        return self.lib.oracle_bottom_stress(self.ctx, C.byref(params), C.byref(f), C.byref(d))
 
     def congrad(self, ccc, ccs, ccn, ccw, cce, ccci, fptmp, p, rsqm, iterm):
         it = C.c_int(0)
