@@ -148,6 +148,7 @@ struct efdc_xm_ctx {
   // device addresses of the mapped pinned mirrors (null: copied by the copy engines)
   void *ctl_hd = nullptr, *glob_hd = nullptr, *act_hd = nullptr, *mpoly_hd = nullptr,
        *sc_hd = nullptr;
+  bool in_chunks = false;  // inside a chunked efdc_xm_step_batch (see to_device)
   double *part = nullptr;
   int *lidx = nullptr;
   int *tile_member = nullptr;
@@ -402,11 +403,12 @@ int download_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
 }
 
 // Control blocks between the device and their pinned host mirrors, on the
-// solver stream.  Where the mirror is mapped (dev_h: its device address) a
-// kernel moves them, so that a step's polls do not queue behind the bulk
-// copies of a chunked efdc_xm_step_batch in flight on the copy engines.
+// solver stream.  During a chunked efdc_xm_step_batch (c->in_chunks), where
+// the mirror is mapped (dev_h: its device address), a kernel moves them, so
+// that a step's polls do not queue behind the bulk copies in flight on the
+// copy engines; otherwise the copy engines do.
 int to_device(efdc_xm_ctx *c, void *dev, const void *host, const void *dev_h, size_t bytes) {
-  if (dev_h) {
+  if (dev_h && c->in_chunks) {
     xm::launch_words(c->stream, dev, dev_h, bytes);
     CK(cudaGetLastError());
   } else {
@@ -415,7 +417,7 @@ int to_device(efdc_xm_ctx *c, void *dev, const void *host, const void *dev_h, si
   return EFDC_XM_OK;
 }
 int to_host(efdc_xm_ctx *c, void *host, void *dev_h, const void *dev, size_t bytes) {
-  if (dev_h) {
+  if (dev_h && c->in_chunks) {
     xm::launch_words(c->stream, dev_h, dev, bytes);
     CK(cudaGetLastError());
   } else {
@@ -1593,15 +1595,28 @@ int step_range(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats, 
   }
   int rc = to_device(c, c->sc, c->sc_h, c->sc_hd, sizeof(xm::StepScalars) * M);
   if (rc) return rc;
-  xm::launch_words(c->stream, c->ctl, nullptr, sizeof(Ctl) * M);  // counters of this step
+  if (c->in_chunks)  // counters of this step (no copy engine: see to_device)
+    xm::launch_words(c->stream, c->ctl, nullptr, sizeof(Ctl) * M);
+  else
+    CK(cudaMemsetAsync(c->ctl, 0, sizeof(Ctl) * M, c->stream));
   rc = write_act(c);
   if (rc) return rc;
   if (istl == 0) {
-    // k_begin copies UHDY1E=UHDYE, VHDX1E=VHDXE, H1P=HP (calpuv2c.f90:256-264)
-    // cell by cell
+    // the two-level advance UHDY1E=UHDYE, VHDX1E=VHDXE, H1P=HP
+    // (calpuv2c.f90:256-264): a buffer swap when every member steps (then
+    // the others are rewritten for every water cell before they are read),
+    // per-cell copies in k_begin when a subset does, and always inside a
+    // chunked efdc_xm_step_batch, whose download was planned on the buffers
+    // as they are before the steps
+    const bool all = m0 == 0 && m1 == M && !c->in_chunks;
+    if (all) {
+      std::swap(c->X.uhdye, c->X.uhdy1e);
+      std::swap(c->X.vhdxe, c->X.vhdx1e);
+      std::swap(c->X.hp, c->X.h1p);
+    }
     set_views(c, 0);
     xm::launch_chan_entry(l, c->S, c->X, c->act);
-    xm::launch_begin(l, c->S, c->X, c->act);
+    xm::launch_begin(l, c->S, c->X, c->act, !all);
   } else {
     xm::launch_chan_entry(l, c->S, c->X, c->act);
     xm::launch_begin3(l, c->S, c->X, c->act);
@@ -1842,6 +1857,11 @@ int step_batch_chunks(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields 
   std::vector<Keep> keep;
   const bool recip = f[0].hpi || f[0].hui || f[0].hvi;
   q = 0;
+  struct Flag {  // c->in_chunks for the steps below, on every way out
+    bool &f;
+    explicit Flag(bool &x) : f(x) { f = true; }
+    ~Flag() { f = false; }
+  } in_chunks(c->in_chunks);
   for (int k = 0; k < K; ++k) {  // steps, each followed by its download, queued
     if (mb[k] == mb[k + 1]) continue;
     CK(cudaStreamWaitEvent(c->stream, c->ev_up[k], 0));

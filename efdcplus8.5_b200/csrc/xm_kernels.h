@@ -32,7 +32,10 @@ struct CopyJob {
   int is_int;              // 0 double, 1 LOGICAL (0/1), 2 raw int, 3 double water-only
 };
 
-void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const int *act);
+// copy: the two-level advance as per-cell copies (a subset of the members
+// steps), else the host has swapped the buffers
+void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const int *act,
+                  bool copy);
 // CALPUV9C: the kernels up to the time-level advance, and the copies of the advance
 void launch_begin3(const Launch &l, const DevStatic &S, const DevState &X, const int *act);
 void launch_advance3(const Launch &l, const DevStatic &S, const DevState &X);

@@ -131,16 +131,21 @@ __device__ __forceinline__ double assemble_cell(const DevStatic &S, const DevSta
 }
 
 // ---------------------------------------------------------------------------
-// calpuv2c.f90:164-293: switches, explicit transports, FP1, and the time-level
+// calpuv2c.f90:164-293: switches, explicit transports, FP1.  The time-level
 // advance of the 2D arrays this library owns (UHDY1E=UHDYE, VHDX1E=VHDXE,
-// H1P=HP, :256-264) as per-cell copies, so that any subset of the members
-// can step (act).
+// H1P=HP, :256-264) is either a buffer swap by the host before this kernel,
+// when every member steps (COPY = false: the *1 buffers hold the entry
+// values), or per-cell copies here (COPY = true: the entry values are in
+// UHDYE, VHDXE, HP), which lets a subset of the members step (act).
 // BARO: a member of the batch has baroclinic terms; the instance without them
 // is held to 32 registers (8 CTAs per SM), which sizes the grid of every cell
 // kernel (occupancy_blocks_per_sm).
-template <bool BARO>
+template <bool BARO, bool COPY>
 __global__ void __launch_bounds__(NT, BARO ? 4 : 8) k_begin(DevStatic S, DevState X, int ntile,
                                                            const int *act) {
+#define UE (COPY ? X.uhdye : X.uhdy1e)
+#define VE (COPY ? X.vhdxe : X.vhdx1e)
+#define HE (COPY ? X.hp : X.h1p)
   TILE_LOOP(ntile) {
     TILE_MEMBER(S);
     if (!act[m]) continue;
@@ -159,21 +164,26 @@ __global__ void __launch_bounds__(NT, BARO ? 4 : 8) k_begin(DevStatic S, DevStat
     const double P = X.p[d];
     double FPGXE = 0., FPGYE = 0.;
     if (BARO && c.baro)  // :192-201 (entry HP, HU, HV, SBX, SBY)
-      baro_faces(S, X, c, q, X.hp, FPGXE, FPGYE);
-    const double uh = X.uhdye[d], vh = X.vhdxe[d];
+      baro_faces(S, X, c, q, HE, FPGXE, FPGYE);
+    const double uh = UE[d], vh = VE[d];
     X.fuhdye[d] = fuh_face(S, X, c, d, uh, X.hu[d], P, X.p[q.w], sub, FPGXE, X.tsx[d], X.tbx[d]);
     X.fvhdxe[d] = fvh_face(S, X, c, d, vh, X.hv[d], P, X.p[q.s], svb, FPGYE, X.tsy[d], X.tby[d]);
-    X.uhdy1e[d] = uh;
-    X.vhdx1e[d] = vh;
-    X.h1p[d] = X.hp[d];
+    if (COPY) {
+      X.uhdy1e[d] = uh;
+      X.vhdx1e[d] = vh;
+      X.h1p[d] = HE[d];
+    }
     if (c.isdry > 0) {  // :246-253
       X.sub[d] = S.subo[d];
       X.svb[d] = S.svbo[d];
       X.sbx[d] = S.sbxo[d];
       X.sby[d] = S.sbyo[d];
     }
-    X.fp1[d] = fp1_cell(S, c, q, P, X.uhdye, X.vhdxe);
+    X.fp1[d] = fp1_cell(S, c, q, P, UE, VE);
   }
+#undef UE
+#undef VE
+#undef HE
 }
 
 // ---------------------------------------------------------------------------
@@ -1145,15 +1155,20 @@ void launch_put(cudaStream_t st, const int *idx, const double *val, int n, doubl
   count_launches(1);
 }
 
-void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const int *act) {
+void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const int *act,
+                  bool copy) {
   if (l.baro) {
     k_calebi<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
     count_launches(1);
   }
-  if (l.baro)
-    k_begin<true><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
+  if (l.baro && copy)
+    k_begin<true, true><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
+  else if (l.baro)
+    k_begin<true, false><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
+  else if (copy)
+    k_begin<false, true><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
   else
-    k_begin<false><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
+    k_begin<false, false><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
   count_launches(1);
 }
 void launch_begin3(const Launch &l, const DevStatic &S, const DevState &X, const int *act) {
@@ -1492,7 +1507,7 @@ void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y,
 int occupancy_blocks_per_sm() {
   int a = 0, b = 0, c = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_assemble, NT, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_begin<false>, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_begin<false, false>, NT, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_fin, NT, 0);
   const int m = std::min(a, std::min(b, c));
   return m > 0 ? m : 1;
