@@ -1785,8 +1785,18 @@ int step_batch_chunks(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields 
     fill_status(stats, M, rc);
     return rc;
   }
+  {  // the checks see the context as the upload will leave it; a refused call changes nothing
+    const bool wd = c->wd_stale, sbxy = c->sbxy_stale, lv = c->tl3_ready;
+    c->wd_stale = skip_wetdry;
+    c->sbxy_stale = skip_sbxy;
+    c->tl3_ready = false;
+    rc = validate_step(c, prm, stats);
+    c->wd_stale = wd;
+    c->sbxy_stale = sbxy;
+    c->tl3_ready = lv;
+    if (rc) return rc;
+  }
   upload_done(c, f, skip_wetdry, skip_sbxy, false);  // the state the step and download see
-  if ((rc = validate_step(c, prm, stats))) return rc;
   if ((rc = plan_download(c, f, skip_wetdry, 0, dn, ls))) {
     fill_status(stats, M, rc);
     return rc;
