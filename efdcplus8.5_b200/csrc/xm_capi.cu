@@ -1043,7 +1043,7 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   X.huc = X.hu; X.hvc = X.hv; X.hb = X.h1p; X.ub = X.uhdy1e; X.vb = X.vhdx1e; X.hp0 = X.h1p;
   xm::DevSystem &Y = c->Y;
   Y.ccc = D(); Y.ccs = D(); Y.ccw = D(); Y.cce = D(); Y.ccn = D(); Y.fptmp = D();
-  Y.r = D(); Y.pa = D(); Y.pb = D(); Y.ap = D();
+  Y.r = D(); Y.pa = D(); Y.pb = D(); Y.ap = D(); Y.z = D();
   Y.as32 = Fl(); Y.aw32 = Fl(); Y.ae32 = Fl(); Y.an32 = Fl();
   Y.r32 = Fl(); Y.pa32 = Fl(); Y.pb32 = Fl(); Y.ap32 = Fl(); Y.x32 = Fl(); Y.z32 = Fl();
   Y.r32b = Fl();

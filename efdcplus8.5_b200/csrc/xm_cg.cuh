@@ -207,6 +207,51 @@ __device__ __forceinline__ double matvec_row(const RowGeo &g, bool valid, const 
          double(a.w) * double(p.w);
 }
 
+// FP64: as matvec_row, with z = CCCI*r stored by the kernels that write r, so
+// that the halo rows need z and p_old only: p = z + beta*p_old has the same
+// roundings as CCCI*r + beta*p_old formed in place.
+__device__ __forceinline__ double matvec_row_z(const RowGeo &g, bool valid,
+                                               const double *__restrict__ z,
+                                               const double *__restrict__ ccc,
+                                               const double *__restrict__ pold,
+                                               double *__restrict__ pnew,
+                                               const double *__restrict__ ccs,
+                                               const double *__restrict__ ccw,
+                                               const double *__restrict__ cce,
+                                               const double *__restrict__ ccn,
+                                               double *__restrict__ ap, double beta, bool asym) {
+  const V4<double> z0 = ld4(z + g.d0), o0 = ld4(pold + g.d0);
+  const V4<double> zn = ld4(z + g.dn), on = ld4(pold + g.dn);
+  const V4<double> zs = ld4(z + g.ds), os = ld4(pold + g.ds);
+  auto pc = [&](double zz, double po) { return zz + beta * po; };
+  const V4<double> p = {pc(z0.x, o0.x), pc(z0.y, o0.y), pc(z0.z, o0.z), pc(z0.w, o0.w)};
+  const V4<double> pn = {pc(zn.x, on.x), pc(zn.y, on.y), pc(zn.z, on.z), pc(zn.w, on.w)};
+  const V4<double> ps = {pc(zs.x, os.x), pc(zs.y, os.y), pc(zs.z, os.z), pc(zs.w, os.w)};
+  double pw = from_west(p), pe = from_east(p);
+  if (g.cx == 0) pw = pc(z[g.dwe], pold[g.dwe]);
+  if (g.cx == ROWT - 1) pe = pc(z[g.dee], pold[g.dee]);
+  const V4<double> c0 = ld4(ccc + g.d0), ks = ld4(ccs + g.d0), kw = ld4(ccw + g.d0);
+  V4<double> kn, ke;
+  if (asym) {
+    kn = ld4(ccn + g.d0);
+    ke = ld4(cce + g.d0);
+  } else {
+    kn = ld4(ccs + g.dn);
+    double kwe = from_east(kw);
+    if (g.cx == ROWT - 1) kwe = ccw[g.dee];
+    ke = {kw.y, kw.z, kw.w, kwe};
+  }
+  V4<double> a;
+  a.x = c0.x * p.x + ks.x * ps.x + kn.x * pn.x + kw.x * pw + ke.x * p.y;
+  a.y = c0.y * p.y + ks.y * ps.y + kn.y * pn.y + kw.y * p.x + ke.y * p.z;
+  a.z = c0.z * p.z + ks.z * ps.z + kn.z * pn.z + kw.z * p.y + ke.z * p.w;
+  a.w = c0.w * p.w + ks.w * ps.w + kn.w * pn.w + kw.w * p.z + ke.w * pe;
+  if (!valid) return 0.0;
+  st4(pnew + g.d0, p);
+  st4(ap + g.d0, a);
+  return a.x * p.x + a.y * p.y + a.z * p.z + a.w * p.w;
+}
+
 // MIXED inner CG on the Jacobi-scaled system (unit diagonal): p = r + beta*p
 // at the row vector and its halo, Ap = p + AS*pS + AN*pN + AW*pW + AE*pE, and
 // the part of p.Ap.  Symmetric: AN(L) = AS(LN), AE(L) = AW(LE).
@@ -395,7 +440,8 @@ template <class T>
 __device__ __forceinline__ void update_row(const RowGeo &g, bool valid, T *__restrict__ x,
                                            const T *__restrict__ pnew, T *__restrict__ r,
                                            const T *__restrict__ ap, const T *__restrict__ ccc,
-                                           T alpha, double &rz, double &rr) {
+                                           T alpha, double &rz, double &rr,
+                                           T *__restrict__ zout = nullptr) {
   if (!valid) return;
   V4<T> xv = ld4(x + g.d0), rv = ld4(r + g.d0);
   const V4<T> pv = ld4(pnew + g.d0), av = ld4(ap + g.d0), cv = ld4(ccc + g.d0);
@@ -411,6 +457,7 @@ __device__ __forceinline__ void update_row(const RowGeo &g, bool valid, T *__res
   st4(r + g.d0, rv);
   const T z0 = rcpT(cv.x) * rv.x, z1 = rcpT(cv.y) * rv.y, z2 = rcpT(cv.z) * rv.z,
           z3 = rcpT(cv.w) * rv.w;
+  if (zout) st4(zout + g.d0, V4<T>{z0, z1, z2, z3});
   rz += double(rv.x) * double(z0) + double(rv.y) * double(z1) + double(rv.z) * double(z2) +
         double(rv.w) * double(z3);
   rr += double(rv.x) * double(rv.x) + double(rv.y) * double(rv.y) + double(rv.z) * double(rv.z) +

@@ -172,6 +172,7 @@ __global__ void k_chan_res64(DevStatic S, DevSystem Y, const double *P, const Ct
       const double z = r * rcpT(Y.ccc[d]);
       Y.r[d] = r;
       Y.pa[d] = z;
+      Y.z[d] = z;
       part[q] += r * z - r0 * z0;
     };
     for (int k = k0; k < k1; ++k) {

@@ -158,6 +158,7 @@ struct DevState {
 struct DevSystem {
   double *ccc, *ccs, *ccw, *cce, *ccn, *fptmp;  // FP64 scaled coefficients, b
   double *r, *pa, *pb, *ap;                      // FP64 CG vectors (p double-buffered)
+  double *z;                                     // FP64: z = CCCI*r, written with r
   // MIXED: the FP32 inner system is the Jacobi-scaled operator
   // Ahat = D^-1/2 A D^-1/2 (unit diagonal, D = CCC), so CG on it equals
   // Jacobi-PCG on A and needs no diagonal array:

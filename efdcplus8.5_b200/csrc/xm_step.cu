@@ -531,6 +531,7 @@ __global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double
         if (valid) {
           st4(Y.r + g.d0, r);
           st4(Y.pa + g.d0, z);
+          st4(Y.z + g.d0, z);
           v[0] = r.x * z.x + r.y * z.y + r.z * z.z + r.w * z.w;
         }
       });
@@ -559,7 +560,7 @@ __global__ void __launch_bounds__(NT) k_red_cg_init(DevStatic S, Ctl *ctl, Glob 
 
 // :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA).
 template <bool MA>
-__global__ void __launch_bounds__(NT, 2) k_cg_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
+__global__ void __launch_bounds__(NT, MA ? 2 : 3) k_cg_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
                                                  double *part) {
   struct A {
     bool skip, asym;
@@ -575,8 +576,8 @@ __global__ void __launch_bounds__(NT, 2) k_cg_matvec(DevStatic S, DevSystem Y, c
         return A{k.done != 0, unsym<MA>(k), k.beta, par ? Y.pb : Y.pa, par ? Y.pa : Y.pb};
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
-        v[0] = matvec_row<double>(g, valid, Y.r, Y.ccc, a.pold, a.pnew, Y.ccs, Y.ccw, Y.cce, Y.ccn,
-                                  Y.ap, a.beta, a.asym);
+        v[0] = matvec_row_z(g, valid, Y.z, Y.ccc, a.pold, a.pnew, Y.ccs, Y.ccw, Y.cce, Y.ccn,
+                            Y.ap, a.beta, a.asym);
       });
 }
 __global__ void __launch_bounds__(NT) k_red_cg_matvec(DevStatic S, Ctl *ctl, const double *part) {
@@ -605,7 +606,7 @@ __global__ void __launch_bounds__(NT, 5) k_cg_update(DevStatic S, DevSystem Y, d
         return A{k.done != 0, k.alpha, k.parity ? Y.pa : Y.pb};
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
-        update_row<double>(g, valid, P, a.pnew, Y.r, Y.ap, Y.ccc, a.alpha, v[0], v[1]);
+        update_row<double>(g, valid, P, a.pnew, Y.r, Y.ap, Y.ccc, a.alpha, v[0], v[1], Y.z);
       });
 }
 __global__ void __launch_bounds__(NT) k_red_cg_update(DevStatic S, Ctl *ctl, Glob *glob,
