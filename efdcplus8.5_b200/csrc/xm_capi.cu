@@ -114,7 +114,7 @@ struct efdc_xm_ctx {
   int M = 0;
   std::vector<Member> mem;
   int ntile = 0, nslot = 0, nquad = 0;
-  int grid = 1, grid_cg = 1, grid_mv64 = 1, grid_cg32 = 1, grid_up32 = 1, nsm = 0;
+  int grid = 1, grid_cg = 1, grid_cg32 = 1, grid_up32 = 1, nsm = 0;
   long long stage_len = 0;  // elements of one staging buffer
   cudaStream_t stream = nullptr;
   // host<->device copies: many per-member copies of small arrays run
@@ -223,8 +223,8 @@ struct efdc_xm_ctx {
     return static_cast<T *>(b.p);
   }
   xm::Launch L() const {
-    return xm::Launch{grid,    grid_cg, grid_mv64, grid_cg32,
-                      grid_up32, ntile, nsm,       stream,
+    return xm::Launch{grid,      grid_cg, grid_cg32, grid_up32,
+                      ntile,     nsm,     stream,
                       mx_jac,  mx_poly, any_may_asym || sys_external,
                       S.ch.n > 0 && !sys_external, step_baro && !sys_external};
   }
@@ -961,7 +961,6 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   c->grid = std::max(1, std::min(c->ntile - 1, c->nsm * occ));
   auto qgrid = [&](int per_sm) { return std::max(1, std::min(c->nquad, c->nsm * per_sm)); };
   c->grid_cg = qgrid(xm::occupancy_blocks_per_sm_cg());
-  c->grid_mv64 = qgrid(xm::occupancy_blocks_per_sm_mv64());
   c->grid_cg32 = qgrid(xm::occupancy_blocks_per_sm_mixed());
   c->grid_up32 = qgrid(xm::occupancy_blocks_per_sm_mixed_update());
 

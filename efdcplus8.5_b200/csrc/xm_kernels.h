@@ -12,7 +12,6 @@ namespace xm {
 struct Launch {
   int grid;          // CTAs of the grid-stride cell kernels (one tile per CTA pass)
   int grid_cg;       // CTAs of the FP64 CG kernels (one quad of 4 tiles per CTA pass)
-  int grid_mv64;     // CTAs of the FP64 matrix-vector kernel (register-heavy)
   int grid_cg32;     // CTAs of the FP32 matrix-vector kernel
   int grid_up32;     // CTAs of the FP32 update kernel
   int ntile;         // tiles including the ghost tile 0
@@ -134,7 +133,6 @@ void count_launches(int n);
 
 int occupancy_blocks_per_sm();
 int occupancy_blocks_per_sm_cg();
-int occupancy_blocks_per_sm_mv64();
 int occupancy_blocks_per_sm_mixed();
 int occupancy_blocks_per_sm_mixed_update();
 

@@ -1267,9 +1267,10 @@ void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, dou
 void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {
   if (l.may_asym)
-    k_cg_matvec<true><<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, ctl, part);
+    k_cg_matvec<true><<<quad_grid(l, S, k_cg_matvec<true>), NT, 0, l.stream>>>(S, Y, ctl, part);
   else
-    k_cg_matvec<false><<<l.grid_mv64, NT, 0, l.stream>>>(S, Y, ctl, part);
+    k_cg_matvec<false><<<quad_grid(l, S, k_cg_matvec<false>), NT, 0, l.stream>>>(S, Y, ctl,
+                                                                               part);
   launch_chan_mv64(l, S, Y, ctl, part);
   k_red_cg_matvec<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part);
   count_launches(2);
@@ -1512,12 +1513,6 @@ int occupancy_blocks_per_sm() {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_fin, NT, 0);
   const int m = std::min(a, std::min(b, c));
   return m > 0 ? m : 1;
-}
-
-int occupancy_blocks_per_sm_mv64() {
-  int a = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cg_matvec<true>, NT, 0);
-  return a > 0 ? a : 1;
 }
 
 int occupancy_blocks_per_sm_cg() {
