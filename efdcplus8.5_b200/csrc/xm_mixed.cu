@@ -23,7 +23,7 @@ namespace xm {
 // p = z + beta*p_old at the cell and its halo (z = r for Jacobi members),
 // Ahat*p, p.Ap (per member).
 template <bool MA>
-__global__ void __launch_bounds__(NT, 5) k_mx_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
+__global__ void __launch_bounds__(NT, 6) k_mx_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
                                                     double *part) {
   struct A {
     bool skip, asym;
@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(NT) k_red_mx_matvec(DevStatic S, Ctl *ctl, con
 
 // x += alpha*p, r -= alpha*Ap, z = (2I - Ahat) r (the two-term Neumann
 // polynomial), r.z and r.r (FP64 sums): the members that use it.
-__global__ void __launch_bounds__(NT, 5) k_mx_update_poly(DevStatic S, DevSystem Y,
+__global__ void __launch_bounds__(NT, 6) k_mx_update_poly(DevStatic S, DevSystem Y,
                                                          const Ctl *ctl, double *part) {
   struct A {
     bool skip;
