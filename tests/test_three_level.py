@@ -240,3 +240,18 @@ def test_gpu_three_level_argument_errors():
                 [scn.copy_state(), scn.copy_state()])
     bs.close()
     sol.close()
+
+
+def test_schedule_follows_hdmt():
+    """HDMT's order (hdmt.f90:299-305, 1009-1029): NCTBC starts at 1; after the
+    leapfrog step on which NCTBC reaches NTSTBC comes the trapezoidal
+    correction of the same step with NCTBC = 0 and ROLD = RNEW = 0.5."""
+    sch = S.three_level_schedule(9, 4)
+    assert [c[:3] for c in sch[:6]] == [(1, 3, 1), (2, 3, 2), (3, 3, 3), (4, 3, 4), (4, 2, 0),
+                                        (5, 3, 1)]
+    assert all(c[3:] == ((0.0, 1.0) if c[1] == 3 else (0.5, 0.5)) for c in sch)
+    assert [c[0] for c in sch if c[1] == 2] == [4, 8]
+    assert sch[-1][0] == 9
+    p = X.make_params(S.three_level_params(dict(cases.build("basin_fp64")[0].params), 3, 1, 0.0,
+                                           1.0), n=1, tn=0.0)
+    assert p.tl3_istl == 3 and p.delt == 2.0 * cases.build("basin_fp64")[0].params["dt"]
