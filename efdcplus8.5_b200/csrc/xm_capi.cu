@@ -1864,6 +1864,11 @@ int step_batch_chunks(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields 
     CK(cudaEventRecord(c->ev_up[k], c->up_x));
   }
   std::vector<Keep> keep;
+  auto fail = [&](int r) {  // the copies queued so far end; the caller's kept elements return
+    drain(c);
+    for (const Keep &kp : keep) std::memcpy(kp.at, kp.val, kp.n);
+    return r;
+  };
   const bool recip = f[0].hpi || f[0].hui || f[0].hvi;
   q = 0;
   struct Flag {  // c->in_chunks for the steps below, on every way out
@@ -1875,10 +1880,7 @@ int step_batch_chunks(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields 
     if (mb[k] == mb[k + 1]) continue;
     CK(cudaStreamWaitEvent(c->stream, c->ev_up[k], 0));
     rc = step_range(c, prm, stats, mb[k], mb[k + 1]);
-    if (rc == EFDC_XM_CUDA_ERROR || rc == EFDC_XM_BAD_ARGUMENT) {
-      drain(c);
-      return rc;
-    }
+    if (rc == EFDC_XM_CUDA_ERROR || rc == EFDC_XM_BAD_ARGUMENT) return fail(rc);
     if (recip)  // 1/HP, 1/HU, 1/HV are formed on request
       xm::launch_reciprocals(c->L(), c->S, c->X, c->mem[mb[k]].tile0,
                              c->mem[mb[k + 1] - 1].tile1);
@@ -1891,14 +1893,11 @@ int step_batch_chunks(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields 
     for (int s = 0; s < NPIPE; ++s) CK(cudaStreamWaitEvent(c->dn_stream[s], c->ev_g[k], 0));
     for (size_t j = 0; j < nd; ++j)
       if ((rc = d2h_range(c, dn[j], reinterpret_cast<const char *>(c->stage[j]), mb[k],
-                          mb[k + 1], c->dn_stream, q, keep, NPIPE))) {
-        drain(c);
-        return rc;
-      }
+                          mb[k + 1], c->dn_stream, q, keep, NPIPE)))
+        return fail(rc);
   }
-  drain(c);
+  fail(0);
   CK(cudaGetLastError());
-  for (const Keep &kp : keep) std::memcpy(kp.at, kp.val, kp.n);
   if ((rc = download_finish(c, f, ls))) return rc;
   return overall_status(stats, M);
 }

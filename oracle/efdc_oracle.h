@@ -39,8 +39,10 @@ oracle_ctx *oracle_create(const efdc_xm_grid *grid, int nthreads, int noptimal_c
 void oracle_destroy(oracle_ctx *c);
 int oracle_noptimal(const oracle_ctx *c);
 
-/* One CALPUV2C call (calpuv2c.f90:128-1187 restricted to BSC=0, MDCHH=0,
- * ISITB=0, ISVEG=0, ISGWIE=0, IGRIDV=0). Returns the status code. */
+/* One CALPUV2C call (calpuv2c.f90:128-1187 with ISITB=0, ISVEG=0, ISGWIE=0,
+ * IGRIDV=0; sub-grid channels and the baroclinic terms where set), or, with
+ * prm->tl3_istl = 3 or 2, one CALPUV9C(ISTL_) call (calpuv9c.f90:105-1069).
+ * Returns the status code. */
 int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
                 efdc_xm_stats *st);
 
