@@ -255,3 +255,26 @@ def test_schedule_follows_hdmt():
     p = X.make_params(S.three_level_params(dict(cases.build("basin_fp64")[0].params), 3, 1, 0.0,
                                            1.0), n=1, tn=0.0)
     assert p.tl3_istl == 3 and p.delt == 2.0 * cases.build("basin_fp64")[0].params["dt"]
+
+
+def test_oracle_fpgxe_blend():
+    """CALPUV9C's baroclinic gradients are blended with the last ones
+    (calpuv9c.f90:164-190): with ROLD = RNEW = 0.5 the result is the mean of
+    the FPGXE passed in and the gradient of the current state (ROLD = 0,
+    RNEW = 1 on a copy)."""
+    scn, _, tm = case("baroclinic")
+    o = O.Oracle(scn.grid)
+    o.set_layers(scn.layers)
+    st = scn.copy_state()
+    assert o.step(prm3(scn, (1, 3, 1, 0.0, 1.0), tm), st).status == X.OK
+    old = st["fpgxe"].copy()
+    fresh = {k: (v.copy() if isinstance(v, np.ndarray) else
+                 {q: a.copy() for q, a in v.items()} if isinstance(v, dict) else v)
+             for k, v in st.items()}
+    assert o.step(prm3(scn, (1, 2, 0, 0.0, 1.0), tm), fresh).status == X.OK
+    assert o.step(prm3(scn, (1, 2, 0, 0.5, 0.5), tm), st).status == X.OK
+    la = scn.la
+    want = 0.5 * old[1:la] + 0.5 * fresh["fpgxe"][1:la]
+    assert np.abs(old[1:la]).max() > 0
+    assert np.allclose(st["fpgxe"][1:la], want, rtol=1e-13, atol=1e-20)
+    o.close()
