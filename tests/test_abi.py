@@ -39,7 +39,9 @@ def test_abi_version():
 
 STRUCTS = {
     "efdc_xm_obc": X.Obc, "efdc_xm_grid": X.Grid, "efdc_xm_params": X.Params,
-    "efdc_xm_fields": X.Fields, "efdc_xm_stats": X.Stats,
+    "efdc_xm_fields": X.Fields, "efdc_xm_stats": X.Stats, "efdc_xm_channels": X.Channels,
+    "efdc_xm_layers": X.Layers, "efdc_xm_bed": X.Bed, "efdc_xm_drag_params": X.DragParams,
+    "efdc_xm_drag_fields": X.DragFields, "efdc_xm_ktime": X.KTime,
 }
 
 
@@ -87,3 +89,51 @@ def test_fortran_shim_binds_declared_symbols():
     f90 = (REPO / "efdcplus8.5_b200" / "fortran" / "efdc_xm_bind.f90").read_text()
     bound = set(re.findall(r"BIND\(C,\s*NAME='(efdc_xm_\w+)'\)", f90, flags=re.I))
     assert bound and bound <= set(declared_functions())
+
+
+FORTRAN_TYPES = {
+    "EFDC_XM_OBC_T": X.Obc, "EFDC_XM_GRID_T": X.Grid, "EFDC_XM_PARAMS_T": X.Params,
+    "EFDC_XM_FIELDS_T": X.Fields, "EFDC_XM_BED_T": X.Bed,
+    "EFDC_XM_DRAG_PARAMS_T": X.DragParams, "EFDC_XM_DRAG_FIELDS_T": X.DragFields,
+    "EFDC_XM_LAYERS_T": X.Layers, "EFDC_XM_CHANNELS_T": X.Channels, "EFDC_XM_STATS_T": X.Stats,
+}
+
+
+def _fortran_members(f90: str, tname: str):
+    """(name, kind, count) of the members of a BIND(C) derived type, in order."""
+    m = re.search(rf"TYPE,\s*BIND\(C\)\s*::\s*{tname}\s*\n(.*?)\n\s*END TYPE", f90, flags=re.S | re.I)
+    assert m, tname
+    out = []
+    for line in m.group(1).splitlines():
+        line = line.split("!")[0].strip()
+        if not line:
+            continue
+        decl, names = line.split("::")
+        decl = decl.strip().upper()
+        kind = ("double" if "C_DOUBLE" in decl else "int32" if "C_INT32_T" in decl else
+                "ptr" if "C_PTR" in decl else decl[decl.index("(") + 1:decl.index(")")].lower())
+        for nm in re.findall(r"(\w+)(?:\((\d+)\))?", names):
+            out.append((nm[0].lower(), kind, int(nm[1]) if nm[1] else 1))
+    return out
+
+
+def _ctypes_members(cls):
+    out = []
+    for name, t in cls._fields_:
+        n = 1
+        if issubclass(t, C.Array):
+            n, t = t._length_, t._type_
+        kind = ("double" if t is C.c_double else "int32" if t is C.c_int32 else
+                "ptr" if issubclass(t, C._Pointer) or t is C.c_void_p else
+                "efdc_xm_" + t.__name__.lower() + "_t")
+        out.append((name.lower(), kind, n))
+    return out
+
+
+def test_fortran_types_mirror_the_header():
+    """Every BIND(C) type of the Fortran module lists the C struct's members in
+    order, with matching kinds and array lengths (checked against the ctypes
+    mirror, whose layout test_ctypes_layout_matches_header checks)."""
+    f90 = (REPO / "efdcplus8.5_b200" / "fortran" / "efdc_xm_bind.f90").read_text()
+    for tname, cls in FORTRAN_TYPES.items():
+        assert _fortran_members(f90, tname) == _ctypes_members(cls), tname
