@@ -46,3 +46,29 @@ def test_config3_sizes():
     n = S.config3_sizes()
     assert n.size == 256 and n.min() >= 10_000 and n.max() <= 400_000
     assert 15e6 < n.sum() < 40e6
+
+
+def test_three_levels_start_at_level_n():
+    scn = S.add_three_levels(S.config1(seed=4))
+    st = scn.state
+    for dst, src in (("p1", "p"), ("h2p", "hp"), ("h1p", "hp"), ("uhdy1e", "uhdye"),
+                     ("uhdy2e", "uhdye"), ("vhdx2e", "vhdxe"), ("h1u", "hu"), ("h1v", "hv"),
+                     ("tbx1", "tbx"), ("tsy1", "tsy")):
+        assert np.array_equal(st[dst], st[src]) and st[dst] is not st[src], dst
+    assert "fpgxe" not in st  # no baroclinic terms: no gradient state
+
+
+def test_bed_and_drag_inputs():
+    scn = S.config1(seed=5)
+    bed = S.make_bed(scn, seed=2, kc=4, smooth_frac=0.2)
+    n = scn.lc + 1
+    for k in ("zbr", "stbxo", "stbyo", "dxp", "dyp", "dzc1", "sgzu1", "sgzv1"):
+        assert bed[k].shape == (n,) and bed[k].dtype == np.float64, k
+    z = bed["zbr"]
+    assert 0.1 < np.mean(z == 0.0) < 0.3 and z.max() <= 0.05
+    assert np.allclose(bed["dzc1"], 0.25)
+    st = scn.copy_state()
+    d = S.drag_inputs(scn, st, st["hu"], st["hv"], seed=1)
+    for k in ("ub", "vb", "vu", "uv", "h1u", "h1v"):
+        assert d[k].shape == (n,) and np.all(np.isfinite(d[k])), k
+    assert d["h1u"] is not st["hu"]
