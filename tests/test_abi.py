@@ -84,6 +84,12 @@ def test_create_without_gpu_fails_loudly():
         X.Solver(scn.grid)
 
 
+def test_missing_library_fails_loudly(tmp_path):
+    """No CPU fallback: a missing libefdc_xm.so is an error, not a slower path."""
+    with pytest.raises(X.CudaLibraryMissing, match="no CPU fallback"):
+        X.load(tmp_path / "libefdc_xm.so")
+
+
 def test_fortran_shim_binds_declared_symbols():
     """The Fortran binding module names exactly the C entry points it uses."""
     f90 = (REPO / "efdcplus8.5_b200" / "fortran" / "efdc_xm_bind.f90").read_text()
