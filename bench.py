@@ -73,7 +73,7 @@ def parse():
     ap.add_argument("--dropin-steps", type=int, default=10)
     ap.add_argument("--basin-steps", type=int, default=50,
                     help="single-domain side measurement (0: skip)")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--wetdry-members", type=int, default=64)
     ap.add_argument("--wetdry-steps", type=int, default=20,
                     help="wetting/drying batch side measurement, 1024x1024 flats (0: skip)")
@@ -85,6 +85,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="CPU baseline: seconds per thread setting (two settings)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-seconds", type=float, default=240.0,
+                    help="--impl reference: stop the timed steps after this many seconds")
     return ap.parse_args()
 
 
@@ -359,25 +361,28 @@ def reference_arm(args):
     rank, _, world = dist_env()
     if rank != 0:
         return
+    # the same workload as the GPU arm: every member (all ranks' members for
+    # N > 1, since rank 0 alone stands for the whole job here), the same
+    # warm-up and timed steps; the wall-time cap only bounds a long default run
     if args.workload == "ensemble":
         seed = 3
-        scns = ensemble(args.members, seed)
+        total = args.members * world
+        scns = ensemble(total, seed)
         cfg = ensemble_config(scns, seed)
-        samp = cpu_sample(scns)
-        what = (f"{len(samp)} members spread over the size range "
-                f"({sum(s.ncell for s in samp)} cells)")
+        cfg["members_all_ranks"] = total
+        samp = scns
+        what = f"all {len(samp)} members ({sum(s.ncell for s in samp)} cells)"
     else:
         scn = S.config2(n=args.size)
         cfg = basin_config(scn, args.size)
         samp = [scn]
         what = f"the {args.size}x{args.size} basin ({scn.ncell} cells)"
-    v, k, dt, nopt = cpu_run(samp, seconds=min(120.0, max(5.0, 1.0 * args.steps)),
-                             max_steps=args.steps,
-                             warmup=min(args.warmup, 1))
-    sample = (f"{k} CALPUV2C steps of {what} after {min(args.warmup, 1)} warm-up, FP64 C++ "
+    v, k, dt, nopt = cpu_run(samp, seconds=args.ref_seconds, max_steps=args.steps,
+                             warmup=args.warmup)
+    sample = (f"{k} CALPUV2C steps of {what} after {args.warmup} warm-up steps, FP64 C++ "
               f"restatement, {nopt} OpenMP threads")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": k, "warmup": min(args.warmup, 1), "ms_per_step": 1000 * dt / max(k, 1),
+            "steps": k, "warmup": args.warmup, "ms_per_step": 1000 * dt / max(k, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)", "config": cfg,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": nopt, "kind": "port",
@@ -635,31 +640,46 @@ def ours(args):
         del prep, pst, _buf
 
     # ---------------- roofline of the dominant kernel ----------------
-    # algorithmic bytes per water cell: the FP32 matvec of the Jacobi-scaled
-    # system reads r, p_old, AS, AW and writes p_new, Ap (6 x 4 B); the FP64
-    # drop-in's reads r, CCC, p_old, CCS, CCW and writes p_new, Ap (7 x 8 B)
-    bytes_mv = 24.0 * kt.ncells
-    # the update: 24 B per cell (x, p, r, Ap in; x, r out) for a Jacobi member,
-    # 36 B for a polynomial one (+ AS, AW in, z out)
-    bytes_up = 24.0 * kt.ncells + 12.0 * kt.ncells_poly
-    achieved = bytes_mv / (kt.ms_matvec * 1e-3) / 1e9
-    traffic = None
+    # The two FP32 kernels of the inner iteration launch once each per
+    # iteration, so the one with the longer launch has the larger share of the
+    # step (profiles/launch_list_ensemble256.md has the shares of every kernel).
+    # Algorithmic bytes per water cell: the matvec of the Jacobi-scaled system
+    # reads r (or z), p_old, AS, AW and writes p_new, Ap (6 x 4 B); the update
+    # reads x, p, r, Ap and writes x, r (24 B) for a Jacobi member, plus AS, AW
+    # in and z out (36 B) for a polynomial one; the FP64 drop-in's matvec reads
+    # z, CCC, p_old, CCS, CCW and writes p_new, Ap (7 x 8 B).
+    tj = {}
     tf = REPO / "profiles" / "traffic.json"
     if tf.exists():
         tj = json.loads(tf.read_text())
-        t = tj.get("k_mx_matvec")
-        if t and "k_mx_matvec" not in tj.get("stale_for", []):
-            traffic = float(t["dram_bytes_per_cell"]) * kt.ncells
-    roof = {"bound": "hbm", "kernel": "k_mx_matvec (FP32 p-update + Ahat*p + p.Ap, all members)",
-            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_kind": peak_kind, "traffic": traffic,
-            "ms_per_launch": kt.ms_matvec, "bytes_per_launch": bytes_mv,
-            "cells_per_launch": kt.ncells, "slots_per_launch": kt.nslots,
-            "update_kernel": {"ms_per_launch": kt.ms_update, "bytes_per_launch": bytes_up,
-                              "achieved": bytes_up / (kt.ms_update * 1e-3) / 1e9,
-                              "cells_polynomial": kt.ncells_poly},
-            "fp64_matvec": {"ms_per_launch": kt64.ms_matvec, "bytes_per_launch": 56.0 * kt.ncells,
-                            "achieved": 56.0 * kt.ncells / (kt64.ms_matvec * 1e-3) / 1e9}}
+
+    def traffic_of(name):
+        t = tj.get(name)
+        if t and name not in tj.get("stale_for", []):
+            return float(t["dram_bytes_per_cell"]) * kt.ncells
+        return None
+
+    def kentry(name, what, ms, nbytes):
+        a = nbytes / (ms * 1e-3) / 1e9
+        return {"bound": "hbm", "kernel": f"{name} ({what})", "achieved": a, "peak": peak,
+                "unit": "GB/s", "frac": a / peak, "peak_kind": peak_kind,
+                "traffic": traffic_of(name), "ms_per_launch": ms, "bytes_per_launch": nbytes,
+                "cells_per_launch": kt.ncells, "slots_per_launch": kt.nslots}
+
+    up_name = "k_mx_update_poly" if kt.ncells_poly > 0 else "k_mx_update_jac"
+    e_mv = kentry("k_mx_matvec", "FP32 p-update + Ahat*p + p.Ap, all members, + member reduce",
+                  kt.ms_matvec, 24.0 * kt.ncells)
+    e_up = kentry(up_name, "FP32 x, r updates, z = (2I - Ahat) r, r.z, r.r, all members, "
+                  "+ member reduce", kt.ms_update, 24.0 * kt.ncells + 12.0 * kt.ncells_poly)
+    e_up["cells_polynomial"] = kt.ncells_poly
+    first, second = (e_up, e_mv) if kt.ms_update >= kt.ms_matvec else (e_mv, e_up)
+    roof = dict(first)
+    roof["dominant_by"] = ("the larger device time per inner iteration of the two kernels "
+                           "that launch once per iteration")
+    roof["second_kernel"] = second
+    roof["fp64_matvec"] = {"ms_per_launch": kt64.ms_matvec, "bytes_per_launch": 56.0 * kt.ncells,
+                           "achieved": 56.0 * kt.ncells / (kt64.ms_matvec * 1e-3) / 1e9,
+                           "frac": 56.0 * kt.ncells / (kt64.ms_matvec * 1e-3) / 1e9 / peak}
     # ---------------- three time levels (CALPUV9C) on the same ensemble ----------------
     tl3_res = None
     if args.tl3_calls > 0 and args.workload == "ensemble":
@@ -737,12 +757,34 @@ def ours(args):
         kb = sol.time_kernels(X.PREC_MIXED, reps=20)
         t64b, tmxb = max_over_ranks(t64b, tmxb)
         cb, = sum_over_ranks(float(scn.ncell * sum(it64)))
+        # the MIXED step's elevation error against the FP64 step from the same
+        # state: the FP64 trajectory's state after the timed steps, one more
+        # step in each precision
+        nb_end = args.warmup + args.basin_steps
+        sol.upload(scn.state)
+        for n in range(1, nb_end + 1):
+            sol.step_device(X.make_params(scn.params, n=n, tn=scn.tn(n)))
+        st_end = scn.copy_state()
+        sol.download(st_end)
+        one = {}
+        for prec in (X.PREC_FP64, X.PREC_MIXED):
+            sol.upload(st_end)
+            sol.step_device(X.make_params(scn.params, n=nb_end + 1, tn=scn.tn(nb_end + 1),
+                                          precision=prec))
+            o = {"p": np.zeros(scn.lc + 1)}
+            sol.download(o)
+            one[prec] = o["p"]
+        eta_b = float(np.abs(one[X.PREC_MIXED][1:scn.la] - one[X.PREC_FP64][1:scn.la]).max()) / S.G
         single = {"config": basin_config(scn, 2048), "steps": args.basin_steps,
                   "value": cb / tmxb, "fp64_value": cb / t64b, "speedup_vs_fp64": t64b / tmxb,
                   "ms_per_step": 1000 * tmxb / args.basin_steps,
                   "fp64_ms_per_step": 1000 * t64b / args.basin_steps,
+                  "eta_err_per_step_mixed_vs_fp64_m": eta_b,
                   "k_mx_matvec_ms": kb.ms_matvec,
-                  "k_mx_matvec_frac": 24.0 * kb.ncells / (kb.ms_matvec * 1e-3) / 1e9 / peak}
+                  "k_mx_matvec_frac": 24.0 * kb.ncells / (kb.ms_matvec * 1e-3) / 1e9 / peak,
+                  "update_ms": kb.ms_update,
+                  "update_frac": (24.0 * kb.ncells + 12.0 * kb.ncells_poly) /
+                                 (kb.ms_update * 1e-3) / 1e9 / peak}
         sol.close()
         del fl
     wd_res = None

@@ -287,6 +287,8 @@ int32_t efdc_xm_congrad_noalloc(int32_t la, const int32_t *lnc, const int32_t *l
   if (!h.done) return EFDC_XM_CG_MAXITER;
   if (h.status == EFDC_XM_CG_MAXITER)
     na_error("efdc_xm_congrad_noalloc: maximum iterations exceeded (RSQ=%g)", h.rsq);
+  if (h.status == EFDC_XM_NONFINITE)
+    na_error("efdc_xm_congrad_noalloc: non-finite CG scalars at iteration %d", h.iter);
   return h.status;
 }
 

@@ -432,7 +432,10 @@ int32_t efdc_xm_time_kernels(efdc_xm_ctx *ctx, int32_t precision, int32_t reps,
  *     device before any stream capture;
  *   - all calls share the array: calls that overlap on the GPU (other
  *     streams, other host threads) race; the call returns after its work on
- *     `stream` (a cudaStream_t, NULL = legacy default stream) finished. */
+ *     `stream` (a cudaStream_t, NULL = legacy default stream) finished;
+ *   - every call reads its stop test back to the host: it copies the control
+ *     block to host memory and synchronizes `stream` after every 8
+ *     iterations. */
 #define EFDC_XM_NOALLOC_MAX_CELLS 524288
 int32_t efdc_xm_congrad_noalloc(int32_t la, const int32_t *lnc, const int32_t *lsc,
                                 const int32_t *lec, const int32_t *lwc, const double *ccc,

@@ -24,8 +24,26 @@ import scenario as S
 pytestmark = pytest.mark.gpu
 
 
-def _system(name):
+# LA-1 of the two large cases: exactly the fixed scratch's limit (a 1024 x 512
+# all-water basin, the last padded element of the scratch in use), and a basin
+# above 296 CTAs x 256 threads = 75,776 cells, so that every thread of the
+# fixed grid loops over several cells
+LIMIT = 524288
+
+
+def _build(name):
+    if name == "at_limit_1024x512":
+        return S.make_scenario(1024, 512, seed=41, land_frac=0.0, obc_sides=("W",), amp=0.5,
+                               dt=10.0), 1.0
+    if name == "multi_cell_320x300":
+        return S.make_scenario(320, 300, seed=41, land_frac=0.05, obc_sides=("W",), amp=0.5,
+                               dt=10.0), 1.0
     scn, _, tm = cases.build(name)
+    return scn, tm
+
+
+def _system(name):
+    scn, tm = _build(name)
     st = scn.copy_state()
     p_in = st["p"].copy()
     orc = O.Oracle(scn.grid)
@@ -36,11 +54,16 @@ def _system(name):
     return scn, st, ccci, p_in
 
 
-@pytest.mark.parametrize("name", ["noise_forcing", "basin_fp64"])
+@pytest.mark.parametrize("name", ["noise_forcing", "basin_fp64", "multi_cell_320x300",
+                                  "at_limit_1024x512"])
 def test_noalloc_matches_context_congrad_twice(name):
     import torch
     lib = X.load()
     scn, st, ccci, p_in = _system(name)
+    if name == "at_limit_1024x512":
+        assert scn.la - 1 == LIMIT
+    if name == "multi_cell_320x300":
+        assert scn.la - 1 > 296 * 256
     # the existing entry point
     sol = X.Solver(scn.grid)
     p_ref = p_in.copy()
@@ -72,7 +95,7 @@ def test_noalloc_matches_context_congrad_twice(name):
 
 def test_noalloc_rejects_oversize():
     lib = X.load()
-    big = 524288 + 2  # LA-1 one past the fixed scratch
+    big = LIMIT + 2  # LA-1 one past the fixed scratch
     dummy = C.c_void_p(16)  # never dereferenced: the size check comes first
     rc = lib.efdc_xm_congrad_noalloc(big, *([dummy] * 11), 1e-10, 10, None, None, None)
     assert rc == X.BAD_ARGUMENT
