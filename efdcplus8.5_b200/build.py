@@ -26,6 +26,7 @@ SOURCES = {
     "xm_noalloc.cu": ["-fmad=false"],
     "xm_adjoint.cu": [],
     "xm_chan.cu": ["-fmad=false"],
+    "xm_loop.cu": [],
 }
 
 

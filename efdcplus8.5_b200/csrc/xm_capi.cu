@@ -41,6 +41,7 @@ void set_error(const char *fmt, ...) {
 
 std::atomic<long long> g_launches{0};
 std::atomic<long long> g_h2d{0}, g_d2h{0};  // bytes of the callers' arrays copied
+std::atomic<long long> g_waits{0};  // host waits for the device inside step and solve calls
 
 using xm::CopyJob;
 using xm::Ctl;
@@ -100,6 +101,16 @@ struct Member {
   int last_n = 0, last_ntstbc = 0, last_isdry = 0;
   std::vector<int32_t> oldmask_h;
   std::vector<int> slot_of;  // slot of cell L (0 for L outside 2..LA)
+};
+
+// A step captured as one graph (see step_graph): the bytes it was built from
+// (flags and every device view its kernels take), and the kernels it
+// launches outside its loops and per body of each loop, for the launch count.
+struct StepGraph {
+  std::vector<char> key;
+  cudaGraphExec_t exec = nullptr;
+  long long n_top = 0;
+  long long n_body[xm::NLOOP] = {};
 };
 
 // One sub-grid channel of a member, as efdc_xm_set_channels received it.
@@ -169,6 +180,13 @@ struct efdc_xm_ctx {
   // [kinds | may_asym << 2 | chan << 3] (MIXED)
   cudaGraphExec_t graph_cg[4] = {}, graph_mx[16] = {};
   bool graph_cg_failed[4] = {}, graph_mx_failed[16] = {};
+  // device-driven steps: the whole step as one graph whose loops are
+  // conditional WHILE nodes (StepGraph), cached by what the graph holds
+  bool device_loops = true;     // efdc_xm_set_option(EFDC_XM_OPT_DEVICE_LOOPS)
+  int graph_iters = GRAPH_ITERS;  // CG iterations per loop body
+  std::vector<StepGraph> step_graphs;
+  std::vector<std::vector<char>> step_graph_failed;
+  cudaStream_t cap_stream[4] = {};  // capture streams of the nested loop bodies
   bool mx_jac = true, mx_poly = false;  // kinds of MIXED inner solve in use
   xm::SysView mxview{};  // the system the MIXED solve refines (the step's assembly, or CONGRAD's)
   bool last_mixed = false;  // the last step ran MIXED: the scaled FP64 system is formed on request
@@ -424,6 +442,7 @@ int to_host(efdc_xm_ctx *c, void *host, void *dev_h, const void *dev, size_t byt
     CK(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c->stream));
   }
   CK(cudaStreamSynchronize(c->stream));
+  g_waits.fetch_add(1, std::memory_order_relaxed);
   return EFDC_XM_OK;
 }
 
@@ -544,20 +563,18 @@ int solve_fp64(efdc_xm_ctx *c, double *P) {
   return EFDC_XM_OK;
 }
 
-// MIXED: FP64 refinement around the FP32 inner PCG, all active members in
-// lockstep outer passes.
-int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
+constexpr int MAX_OUTER = 30;        // MIXED refinement passes per solve
+constexpr double INNER_REL_TOL = 1e-6;  // inner: |r| down 1e-6 at least (FP32 reaches ~1e-7)
+
+// MIXED: each member's inner preconditioner for the next solve, and the kinds
+// of inner solve the launches need; uploads the choice.  The Neumann
+// polynomial halves the iterations at ~1.3x the cost of one; members whose
+// Jacobi solve takes few iterations keep Jacobi.  A member whose operator
+// turns out unsymmetric (its flag is set on the device) runs Jacobi whatever
+// the choice, so the Jacobi kernels are launched too wherever that can
+// happen: a radiation boundary, or a caller's standalone system.
+int choose_inner(efdc_xm_ctx *c) {
   const xm::Launch l = c->L();
-  const double fac = factor > 0 ? factor : 0.1;  // stop at fac*RSQM in FP64
-  const int max_outer = 30;
-  const double rel_tol = 1e-6;  // inner: |r| down 1e-6 at least (FP32 reaches ~1e-7 here)
-  xm::launch_solve_reset(l, c->ctl, c->glob, c->act, c->M);
-  // inner preconditioner per member: the Neumann polynomial halves the
-  // iterations at ~1.3x the cost of one; members whose Jacobi solve takes
-  // few iterations keep Jacobi.  A member whose operator turns out
-  // unsymmetric (its flag is set on the device) runs Jacobi whatever the
-  // choice, so the Jacobi kernels are launched too wherever that can happen:
-  // a radiation boundary, or a caller's standalone system.
   c->mx_jac = c->mx_poly = false;
   for (int m = 0; m < c->M; ++m) {
     // a member with sub-grid channels keeps Jacobi (the couplings enter A*p only)
@@ -570,13 +587,22 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
       if (c->mem[m].may_asym || c->sys_external) c->mx_jac = true;
     }
   }
-  if (int rc0 = to_device(c, c->mpoly, c->mpoly_h, c->mpoly_hd, sizeof(int) * c->M)) return rc0;
+  return to_device(c, c->mpoly, c->mpoly_h, c->mpoly_hd, sizeof(int) * c->M);
+}
+
+// MIXED: FP64 refinement around the FP32 inner PCG, all active members in
+// lockstep outer passes.
+int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
+  const double fac = factor > 0 ? factor : 0.1;  // stop at fac*RSQM in FP64
+  xm::launch_solve_reset(c->L(), c->ctl, c->glob, c->act, c->M);
+  if (int rc0 = choose_inner(c)) return rc0;
   const xm::Launch lk = c->L();  // with the kinds in use
   xm::launch_chan_p0(lk, c->S, c->mxview, P, c->act);
   int rc = 0;
-  for (int o = 0; o < max_outer; ++o) {
+  for (int o = 0; o < MAX_OUTER; ++o) {
     xm::launch_outer_reset(lk, c->glob);
-    xm::launch_mx_resid(lk, c->S, c->mxview, c->Y, P, c->ctl, c->glob, c->part, fac, rel_tol, 0);
+    xm::launch_mx_resid(lk, c->S, c->mxview, c->Y, P, c->ctl, c->glob, c->part, fac,
+                        INNER_REL_TOL, 0);
     CK(cudaGetLastError());
     if ((rc = read_glob(c))) return rc;
     if (c->glob_h->ndone >= c->M) break;
@@ -629,6 +655,7 @@ xm::StepScalars make_scalars(const Member &mb, const efdc_xm_params *p) {
   s.ndrystp = p->ndrystp;
   s.isbal = p->isbal;
   s.iterm = p->iterm;
+  s.max_sweeps = p->max_sweeps > 0 ? p->max_sweeps : 500;
   s.rlamn = p->qcherr;  // calpuv2c.f90:353 (RLAMN = QCHERR)
   s.baro = p->bsc > 1.E-6 ? 1 : 0;  // calpuv2c.f90:161, 192
   s.gp = p->gp;
@@ -774,6 +801,10 @@ void efdc_xm_destroy(efdc_xm_ctx *c) {
     if (g) cudaGraphExecDestroy(g);
   for (cudaGraphExec_t g : c->graph_mx)
     if (g) cudaGraphExecDestroy(g);
+  for (StepGraph &g : c->step_graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  for (cudaStream_t s : c->cap_stream)
+    if (s) cudaStreamDestroy(s);
   for (void *b : c->chan_bufs) cudaFree(b);
   for (cudaStream_t s : c->copy_stream)
     if (s) cudaStreamDestroy(s);
@@ -1509,6 +1540,338 @@ int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int l
 }  // extern "C"
 
 namespace {
+// ---------------------------------------------------------------------------
+// Device-driven step: one CALPUV2C (or CALPUV9C) call of every active member
+// as one CUDA graph.  The three data-dependent loops of the step -- the CG
+// iterations, the MIXED refinement passes with their inner iterations, and
+// the wet/dry re-solves -- are conditional WHILE nodes whose conditions the
+// loop-control kernels (xm_loop.cu) set on the device, so the host launches
+// the graph and waits once, for the stats.  Every loop has a body cap on the
+// device (ITERM-based for the solves, the members' NCORDRY cap for the
+// sweeps, MAX_OUTER for the passes).  The graph holds the kernels' arguments,
+// so it is cached by the bytes of every view it was built from (the two-level
+// buffer swap alternates between two such graphs).
+
+// What a step's graph depends on besides the context's device views.
+struct StepPlan {
+  int mixed, istl, all, any_isdry, any_legacy, any99, any_waste, iters;
+  int max_iterm, max_sweeps, grid, grid_cg, grid_cg32, grid_up32;
+  int mx_jac, mx_poly, may_asym, chan, baro, obc_serial, any_may_asym, nmember;
+  double fac;
+  const void *psol;
+};
+
+template <class T>
+void put_bytes(std::vector<char> &k, const T &v) {
+  const char *p = reinterpret_cast<const char *>(&v);
+  k.insert(k.end(), p, p + sizeof(T));
+}
+
+// The key of a step graph: the plan and every view its kernels take (DevState,
+// DevSystem and DevObc hold pointers and ints only, no padding; DevStatic
+// changes only through the set-up calls, which drop the graphs).
+std::vector<char> step_key(const efdc_xm_ctx *c, const StepPlan &pl) {
+  std::vector<char> k;
+  k.reserve(2048);
+  put_bytes(k, pl);
+  put_bytes(k, c->X);
+  put_bytes(k, c->Y);
+  put_bytes(k, c->B);
+  for (const void *p : {static_cast<const void *>(c->mxview.fp), static_cast<const void *>(c->mxview.cc),
+                        static_cast<const void *>(c->mxview.cs), static_cast<const void *>(c->mxview.cw),
+                        static_cast<const void *>(c->mxview.ce), static_cast<const void *>(c->mxview.cn)})
+    put_bytes(k, p);
+  put_bytes(k, c->mxview.unscaled);
+  return k;
+}
+
+// A conditional handle in the graph now being captured on `st`.
+cudaError_t cond_handle(cudaStream_t st, cudaGraphConditionalHandle *h) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr);
+  if (e != cudaSuccess) return e;
+  if (cs != cudaStreamCaptureStatusActive || !g) return cudaErrorStreamCaptureInvalidated;
+  return cudaGraphConditionalHandleCreate(h, g, 0, 0);
+}
+
+// Appends a WHILE node with handle h at the current end of the capture on
+// `st` (later work on `st` follows it) and starts capturing its body on `bs`.
+cudaError_t begin_while(cudaStream_t st, cudaGraphConditionalHandle h, cudaStream_t bs) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd);
+  if (e != cudaSuccess) return e;
+  cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};  // the rest zero
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node = nullptr;
+  if ((e = cudaGraphAddNode(&node, g, deps, nd, &p)) != cudaSuccess) return e;
+  if ((e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies)) !=
+      cudaSuccess)
+    return e;
+  return cudaStreamBeginCaptureToGraph(bs, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeThreadLocal);
+}
+
+cudaError_t end_body(cudaStream_t bs) {
+  cudaGraph_t g = nullptr;
+  return cudaStreamEndCapture(bs, &g);
+}
+
+// Records the kernels launched since `*mark` into `*n` and moves the mark.
+void take_count(long long *mark, long long *n) {
+  const long long now = g_launches.load();
+  *n += now - *mark;
+  *mark = now;
+}
+
+#define CKG(expr)                        \
+  do {                                   \
+    const cudaError_t e__ = (expr);      \
+    if (e__ != cudaSuccess) return e__; \
+  } while (0)
+
+// The solve of one sweep, captured on level d (stream c->cap_stream[d]).
+cudaError_t capture_solve(efdc_xm_ctx *c, const StepPlan &pl, int d, StepGraph &sg,
+                          long long *mark, long long *mine) {
+  cudaStream_t st = c->cap_stream[d];
+  xm::Launch l = c->L();
+  l.stream = st;
+  const int M = c->M, K = pl.iters;
+  double *P = c->X.p;
+  if (!pl.mixed) {
+    xm::launch_solve_reset(l, c->ctl, c->glob, c->act, M);
+    xm::launch_cg_init(l, c->S, c->Y, P, c->ctl, c->glob, c->part);
+    cudaGraphConditionalHandle h;
+    CKG(cond_handle(st, &h));
+    xm::launch_loop_enter(st, c->glob, xm::LOOP_CG, h, 1, M);
+    take_count(mark, mine);
+    CKG(begin_while(st, h, c->cap_stream[d + 1]));
+    xm::Launch lb = l;
+    lb.stream = c->cap_stream[d + 1];
+    for (int k = 0; k < K; ++k) xm::launch_cg_iter(lb, c->S, c->Y, P, c->ctl, c->glob, c->part);
+    xm::launch_loop_next(lb.stream, c->glob, xm::LOOP_CG, h, (pl.max_iterm + K - 1) / K + 1, 0,
+                         M);
+    take_count(mark, &sg.n_body[xm::LOOP_CG]);
+    return end_body(lb.stream);
+  }
+  xm::launch_solve_reset(l, c->ctl, c->glob, c->act, M);
+  xm::launch_chan_p0(l, c->S, c->mxview, P, c->act);
+  cudaGraphConditionalHandle ho, hi;
+  CKG(cond_handle(st, &ho));
+  xm::launch_loop_enter(st, c->glob, xm::LOOP_OUTER, ho, 0, M);
+  take_count(mark, mine);
+  CKG(begin_while(st, ho, c->cap_stream[d + 1]));
+  xm::Launch lo = l;
+  lo.stream = c->cap_stream[d + 1];
+  xm::launch_outer_reset(lo, c->glob);
+  xm::launch_mx_resid(lo, c->S, c->mxview, c->Y, P, c->ctl, c->glob, c->part, pl.fac,
+                      INNER_REL_TOL, 0);
+  CKG(cond_handle(lo.stream, &hi));
+  xm::launch_loop_enter(lo.stream, c->glob, xm::LOOP_INNER, hi, 1, M);
+  take_count(mark, &sg.n_body[xm::LOOP_OUTER]);
+  CKG(begin_while(lo.stream, hi, c->cap_stream[d + 2]));
+  xm::Launch li = l;
+  li.stream = c->cap_stream[d + 2];
+  for (int k = 0; k < K; ++k) xm::launch_mx_iter(li, c->S, c->Y, c->ctl, c->glob, c->part);
+  // the inner stop caps each member at 2*ITERM+50 inner iterations in all
+  xm::launch_loop_next(li.stream, c->glob, xm::LOOP_INNER, hi,
+                       (2 * pl.max_iterm + 50 + K - 1) / K + 2, 1, M);
+  take_count(mark, &sg.n_body[xm::LOOP_INNER]);
+  CKG(end_body(li.stream));
+  xm::launch_inner_done(lo.stream, c->ctl, c->act, M);
+  xm::launch_mx_apply(lo, c->S, c->mxview, c->Y, P, c->ctl);
+  xm::launch_loop_next(lo.stream, c->glob, xm::LOOP_OUTER, ho, MAX_OUTER, 0, M);
+  take_count(mark, &sg.n_body[xm::LOOP_OUTER]);
+  return end_body(lo.stream);
+}
+
+// Captures the whole step into sg (the host has set the views, the swaps,
+// the scalars and the members' activity; see step_range).
+// x_pre: the state views before the time-level rotation of CALPUV9C(3), on
+// which its first kernels run (as in step_range's host-driven order).
+cudaError_t capture_step(efdc_xm_ctx *c, const StepPlan &pl, const xm::DevState &x_pre,
+                         StepGraph &sg) {
+  for (cudaStream_t &s : c->cap_stream)
+    if (!s) CKG(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  cudaStream_t s0 = c->cap_stream[0], s1 = c->cap_stream[1];
+  const int M = c->M;
+  xm::Launch l = c->L();
+  l.stream = s0;
+  long long mark = g_launches.load();
+  const long long start = mark;
+  CKG(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+  cudaError_t err = cudaSuccess;
+  [&] {
+    xm::launch_step_enter(s0, c->ctl, c->act, c->glob, M);
+    if (pl.istl == 0) {
+      xm::launch_chan_entry(l, c->S, c->X, c->act);
+      xm::launch_begin(l, c->S, c->X, c->act, !pl.all);
+    } else {
+      xm::launch_chan_entry(l, c->S, x_pre, c->act);
+      xm::launch_begin3(l, c->S, x_pre, c->act);
+      if (pl.istl == 3) xm::launch_advance3(l, c->S, c->X);
+    }
+    if (pl.any_isdry) xm::launch_obc_reset(l, c->S, c->B, c->X, c->act);
+    cudaGraphConditionalHandle hs;
+    if ((err = cond_handle(s0, &hs)) != cudaSuccess) return;
+    xm::launch_loop_enter(s0, c->glob, xm::LOOP_SWEEP, hs, 0, M);
+    take_count(&mark, &sg.n_top);
+    if ((err = begin_while(s0, hs, s1)) != cudaSuccess) return;
+    // the sweep body (1000 CONTINUE of calpuv2c.f90)
+    xm::Launch lw = l;
+    lw.stream = s1;
+    xm::launch_sweep_reset(lw, c->ctl, c->act, M);
+    xm::launch_assemble(lw, c->S, c->X, c->ctl, c->act);
+    xm::launch_obc(lw, c->S, c->X, c->B, c->ctl, c->act, c->obc_serial, c->any_may_asym ? 1 : 0);
+    xm::launch_chan_sub(lw, c->S, c->X, c->ctl, c->act, -1);
+    xm::launch_scale(lw, c->S, c->X, c->Y, c->ctl, c->act, pl.mixed, c->any_may_asym ? 1 : 0);
+    if ((err = capture_solve(c, pl, 1, sg, &mark, &sg.n_body[xm::LOOP_SWEEP])) != cudaSuccess)
+      return;
+    if (c->psol) {  // calibration: the adjoint needs P' before P is refreshed from HP
+      if ((err = cudaMemcpyAsync(c->psol, c->X.p, size_t(c->nslot) * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, s1)) != cudaSuccess)
+        return;
+    }
+    xm::launch_after_solve(s1, c->ctl, c->act, M, pl.mixed);
+    xm::launch_chan_flow(lw, c->S, c->X, c->act);
+    xm::launch_backsub(lw, c->S, c->X, c->act);
+    xm::launch_obc_hp(lw, c->S, c->X, c->B, c->act);
+    xm::launch_chan_exch(lw, c->S, c->X, c->act);
+    if (pl.any_isdry) xm::launch_wetdry(lw, c->S, c->X, c->ctl, c->act, pl.any_legacy, pl.any99);
+    xm::launch_sweep_next(s1, c->S, c->ctl, c->act, c->glob, hs, pl.max_sweeps + 1, M);
+    take_count(&mark, &sg.n_body[xm::LOOP_SWEEP]);
+    if ((err = end_body(s1)) != cudaSuccess) return;
+    // finalisation of the members whose sweeps ended normally
+    xm::launch_fin_prepare(s0, c->ctl, c->act, M);
+    xm::launch_final(l, c->S, c->X, c->ctl, c->act, pl.any_waste);
+    take_count(&mark, &sg.n_top);
+  }();
+  cudaGraph_t g = nullptr;
+  const cudaError_t e_end = cudaStreamEndCapture(s0, &g);
+  // captured, not launched: the step's launches are counted when it runs
+  g_launches.fetch_sub(g_launches.load() - start);
+  if (err == cudaSuccess) err = e_end;
+  if (err == cudaSuccess && !g) err = cudaErrorStreamCaptureInvalidated;
+  if (err == cudaSuccess) err = cudaGraphInstantiate(&sg.exec, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (err != cudaSuccess) {
+    // a capture left open on a body stream would keep that stream capturing
+    for (cudaStream_t s : c->cap_stream) {
+      cudaStreamCaptureStatus cs;
+      if (s && cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+        cudaGraph_t t = nullptr;
+        cudaStreamEndCapture(s, &t);
+        if (t) cudaGraphDestroy(t);
+      }
+    }
+    cudaGetLastError();
+    sg.exec = nullptr;
+  }
+  return err;
+}
+#undef CKG
+
+constexpr size_t STEP_GRAPH_CACHE = 8;
+
+// The cached graph for this step, built on first use; null if graphs with
+// conditional nodes cannot be built here (the host-driven step then runs).
+StepGraph *step_graph(efdc_xm_ctx *c, const StepPlan &pl, const xm::DevState &x_pre) {
+  std::vector<char> key = step_key(c, pl);
+  if (pl.istl != 0) put_bytes(key, x_pre);
+  for (size_t i = 0; i < c->step_graphs.size(); ++i)
+    if (c->step_graphs[i].key == key) {
+      if (i + 1 != c->step_graphs.size())  // most recent last
+        std::rotate(c->step_graphs.begin() + i, c->step_graphs.begin() + i + 1,
+                    c->step_graphs.end());
+      return &c->step_graphs.back();
+    }
+  for (const auto &f : c->step_graph_failed)
+    if (f == key) return nullptr;
+  StepGraph sg;
+  if (capture_step(c, pl, x_pre, sg) != cudaSuccess || !sg.exec) {
+    c->step_graph_failed.push_back(std::move(key));
+    return nullptr;
+  }
+  sg.key = std::move(key);
+  if (c->step_graphs.size() >= STEP_GRAPH_CACHE) {
+    cudaGraphExecDestroy(c->step_graphs.front().exec);
+    c->step_graphs.erase(c->step_graphs.begin());
+  }
+  c->step_graphs.push_back(std::move(sg));
+  return &c->step_graphs.back();
+}
+
+void drop_step_graphs(efdc_xm_ctx *c) {
+  for (StepGraph &g : c->step_graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  c->step_graphs.clear();
+  c->step_graph_failed.clear();
+}
+
+// Runs the step's graph and reads the members' control blocks (one host
+// wait), then fills the stats of the members [m0, m1) as step_range's host
+// loop does.  Returns -1 (nothing launched) if the graph could not be built.
+int run_step_graph(efdc_xm_ctx *c, const StepPlan &pl, const xm::DevState &x_pre,
+                   const efdc_xm_params *prm, efdc_xm_stats *stats, int m0, int m1) {
+  StepGraph *sg = step_graph(c, pl, x_pre);
+  if (!sg) return -1;
+  CK(cudaGraphLaunch(sg->exec, c->stream));
+  if (c->in_chunks && c->ctl_hd && c->glob_hd) {
+    xm::launch_words(c->stream, c->ctl_hd, c->ctl, sizeof(Ctl) * c->M);
+    xm::launch_words(c->stream, c->glob_hd, c->glob, sizeof(Glob));
+  } else {
+    CK(cudaMemcpyAsync(c->ctl_h, c->ctl, sizeof(Ctl) * c->M, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(c->glob_h, c->glob, sizeof(Glob), cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  g_waits.fetch_add(1, std::memory_order_relaxed);
+  long long n = sg->n_top;
+  for (int i = 0; i < xm::NLOOP; ++i) n += sg->n_body[i] * c->glob_h->tot[i];
+  xm::count_launches(int(std::min<long long>(n, INT32_MAX)));
+  for (int m = m0; m < m1; ++m) {
+    const Ctl &k = c->ctl_h[m];
+    efdc_xm_stats &s = stats[m];
+    Member &mb = c->mem[m];
+    s.iters_last = k.iters_last;
+    s.iters_total += k.iters_total;
+    s.solves += k.solves;
+    s.rsq_last = k.rsq_last;
+    s.outer_refinements += k.outer_total;
+    s.ccmnm_last = k.ccmnm_last;
+    s.n_negdep = k.nneg;
+    s.n_wasted = k.nwasted;
+    if (k.iters_last > 0) mb.last_iters = k.iters_last;
+    if (pl.mixed && k.last_inner > 0) mb.last_inner = k.last_inner;
+    if (pl.mixed && k.inner_first > 0) {
+      const bool poly = c->mpoly_h[m] && !(k.asym & 1);
+      mb.jac_est = float(k.inner_first) * (poly ? 1.9f : 1.0f);
+    }
+    int st = k.mstatus;
+    if (st == EFDC_XM_UNSUPPORTED) {
+      set_error("member %d: the scaled operator is unsymmetric although the model has no "
+                "radiation boundary (check SUBO/SVBO next to the open-boundary cells)", m);
+    } else if (st == EFDC_XM_CG_MAXITER || (st == EFDC_XM_NONFINITE && k.status == st)) {
+      set_error("member %d: CONGRAD: %s after %d iterations (RSQ=%g, RSQM=%g)", m,
+                st == EFDC_XM_CG_MAXITER ? "maximum iterations exceeded" : "non-finite residual",
+                k.iter, s.rsq_last, prm[m].rsqm);
+    } else if (st == EFDC_XM_WETDRY_MAXSWEEP) {
+      set_error("member %d: wet/dry: NCORDRY reached %d", m, c->sc_h[m].max_sweeps);
+    }
+    if (st == EFDC_XM_OK && k.nnonfinite > 0) {
+      st = EFDC_XM_NONFINITE;
+      set_error("member %d: non-finite P in %d cells", m, k.nnonfinite);
+    }
+    if (st == EFDC_XM_OK && k.nneg > 0) st = EFDC_XM_NEG_DEPTH;
+    s.status = st;
+  }
+  return overall_status(stats + m0, m1 - m0);
+}
+
 // The argument checks of a device-resident step of every member (the stats
 // are filled with the status on failure).
 int validate_step(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats) {
@@ -1600,29 +1963,27 @@ int step_range(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats, 
     CK(cudaMemsetAsync(c->ctl, 0, sizeof(Ctl) * M, c->stream));
   rc = write_act(c);
   if (rc) return rc;
+  // the two-level advance UHDY1E=UHDYE, VHDX1E=VHDXE, H1P=HP
+  // (calpuv2c.f90:256-264): a buffer swap when every member steps (then the
+  // others are rewritten for every water cell before they are read), per-cell
+  // copies in k_begin when a subset does, and always inside a chunked
+  // efdc_xm_step_batch, whose download was planned on the buffers as they are
+  // before the steps
+  const bool all = istl == 0 && m0 == 0 && m1 == M && !c->in_chunks;
+  const xm::DevState x_pre = c->X;  // CALPUV9C's first kernels run before the rotation
   if (istl == 0) {
-    // the two-level advance UHDY1E=UHDYE, VHDX1E=VHDXE, H1P=HP
-    // (calpuv2c.f90:256-264): a buffer swap when every member steps (then
-    // the others are rewritten for every water cell before they are read),
-    // per-cell copies in k_begin when a subset does, and always inside a
-    // chunked efdc_xm_step_batch, whose download was planned on the buffers
-    // as they are before the steps
-    const bool all = m0 == 0 && m1 == M && !c->in_chunks;
     if (all) {
       std::swap(c->X.uhdye, c->X.uhdy1e);
       std::swap(c->X.vhdxe, c->X.vhdx1e);
       std::swap(c->X.hp, c->X.h1p);
     }
     set_views(c, 0);
-    xm::launch_chan_entry(l, c->S, c->X, c->act);
-    xm::launch_begin(l, c->S, c->X, c->act, !all);
   } else {
-    xm::launch_chan_entry(l, c->S, c->X, c->act);
-    xm::launch_begin3(l, c->S, c->X, c->act);
     if (istl == 3) {
       // calpuv9c.f90:282-311 by buffer rotation, UHDY2E <- UHDY1E <- UHDYE and
       // H2P <- H1P <- HP (UHDYE and HP are rewritten for every water cell
       // before they are read), and the copies P1 = P, H1U = HU, H1V = HV
+      // (k_advance3)
       xm::DevState &X = c->X;
       double *t = X.uhdy2e;
       X.uhdy2e = X.uhdy1e; X.uhdy1e = X.uhdye; X.uhdye = t;
@@ -1630,9 +1991,56 @@ int step_range(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats, 
       X.vhdx2e = X.vhdx1e; X.vhdx1e = X.vhdxe; X.vhdxe = t;
       t = X.h2p;
       X.h2p = X.h1p; X.h1p = X.hp; X.hp = t;
-      xm::launch_advance3(l, c->S, c->X);
     }
     set_views(c, istl);
+  }
+  if (c->device_loops) {
+    // the whole step as one graph, its loops on the device
+    if (mixed && (rc = choose_inner(c))) return rc;
+    StepPlan pl{};
+    const xm::Launch lk = c->L();
+    pl.mixed = mixed;
+    pl.istl = istl;
+    pl.all = all;
+    pl.any_isdry = any_isdry;
+    pl.any_legacy = any_legacy;
+    pl.any99 = any99;
+    pl.any_waste = any_waste;
+    pl.iters = c->graph_iters;
+    pl.max_iterm = 1;
+    pl.max_sweeps = 1;
+    for (int m = m0; m < m1; ++m) {
+      pl.max_iterm = std::max(pl.max_iterm, c->sc_h[m].iterm);
+      pl.max_sweeps = std::max(pl.max_sweeps, c->sc_h[m].max_sweeps);
+    }
+    pl.grid = lk.grid;
+    pl.grid_cg = lk.grid_cg;
+    pl.grid_cg32 = lk.grid_cg32;
+    pl.grid_up32 = lk.grid_up32;
+    pl.mx_jac = lk.mx_jac;
+    pl.mx_poly = lk.mx_poly;
+    pl.may_asym = lk.may_asym;
+    pl.chan = lk.chan;
+    pl.baro = lk.baro;
+    pl.obc_serial = c->obc_serial;
+    pl.any_may_asym = c->any_may_asym;
+    pl.nmember = M;
+    pl.fac = mixed ? (prm[0].mixed_rsq_factor > 0 ? prm[0].mixed_rsq_factor : 0.1) : 0.0;
+    pl.psol = c->psol;
+    rc = run_step_graph(c, pl, x_pre, prm, stats, m0, m1);
+    if (rc >= 0) {
+      if (istl == 0) c->tl3_ready = false;  // CALPUV2C does not keep the three levels
+      return rc;
+    }
+    // no graph with conditional nodes here: the host-driven step below
+  }
+  if (istl == 0) {
+    xm::launch_chan_entry(l, c->S, c->X, c->act);
+    xm::launch_begin(l, c->S, c->X, c->act, !all);
+  } else {
+    xm::launch_chan_entry(l, c->S, x_pre, c->act);
+    xm::launch_begin3(l, c->S, x_pre, c->act);
+    if (istl == 3) xm::launch_advance3(l, c->S, c->X);
   }
   if (any_isdry) xm::launch_obc_reset(l, c->S, c->B, c->X, c->act);
   CK(cudaGetLastError());
@@ -2062,6 +2470,7 @@ void drop_graphs(efdc_xm_ctx *c) {
     }
   for (bool &f : c->graph_cg_failed) f = false;
   for (bool &f : c->graph_mx_failed) f = false;
+  drop_step_graphs(c);
 }
 
 // S.ch from every member's channel list, and the slot kinds (channel cells
@@ -2241,6 +2650,7 @@ int32_t efdc_xm_set_layers(efdc_xm_ctx *c, int32_t member, const efdc_xm_layers 
     return EFDC_XM_CUDA_ERROR;
   }
   c->has_layers[member] = 1;
+  drop_graphs(c);  // the kernels' static views (the layer arrays) have changed
   return EFDC_XM_OK;
 }
 
@@ -2483,6 +2893,31 @@ int32_t efdc_xm_congrad(efdc_xm_ctx *c, const double *ccc, const double *ccs, co
 void *efdc_xm_stream(efdc_xm_ctx *c) { return c ? static_cast<void *>(c->stream) : nullptr; }
 
 int64_t efdc_xm_kernel_launches(void) { return g_launches.load(); }
+
+int64_t efdc_xm_host_waits(void) { return g_waits.load(); }
+
+int32_t efdc_xm_set_option(efdc_xm_ctx *c, int32_t option, int32_t value) {
+  if (!c) {
+    set_error("efdc_xm_set_option: NULL context");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  switch (option) {
+    case EFDC_XM_OPT_DEVICE_LOOPS:
+      c->device_loops = value != 0;
+      return EFDC_XM_OK;
+    case EFDC_XM_OPT_GRAPH_ITERS:
+      if (value < 1 || value > 32) break;
+      if (value != c->graph_iters) {
+        c->graph_iters = value;
+        drop_step_graphs(c);
+      }
+      return EFDC_XM_OK;
+    default:
+      break;
+  }
+  set_error("efdc_xm_set_option: unknown option %d or value %d out of range", option, value);
+  return EFDC_XM_BAD_ARGUMENT;
+}
 
 void efdc_xm_transfer_bytes(int64_t *h2d, int64_t *d2h) {
   if (h2d) *h2d = g_h2d.load();

@@ -61,7 +61,8 @@ __global__ void k_chan_entry(DevStatic S, DevState X, const int *act) {
 // CCCCHU, CCCCHV, CCCCHH and their entries in CC and FP of the host and guest
 // cells (after SETOPENBC, calpuv2c.f90:349-356); then the final CC of the
 // channels' cells into the member's minimum diagonal.  In the first sweep HP
-// is still the entry value (the view hp0).
+// is still the entry value (the view hp0).  first_sweep < 0: the member's
+// own sweep counter tells (a step whose sweep loop runs on the device).
 __global__ void k_chan_sub(DevStatic S, DevState X, Ctl *ctl, const int *act, int first_sweep) {
   const DevChan &C = S.ch;
   MEMBER_LOOP {
@@ -71,7 +72,8 @@ __global__ void k_chan_sub(DevStatic S, DevState X, Ctl *ctl, const int *act, in
     const double G = c.g, DE_T = c.delt, HDRY = c.hdry, RLAMN = c.rlamn;
     const double RLAMO = 1. - RLAMN;
     const double *H1P = X.h1p;
-    const double *HP = first_sweep ? X.hp0 : X.hp;
+    const bool first = first_sweep < 0 ? ctl[m].sweep == 0 : first_sweep != 0;
+    const double *HP = first ? X.hp0 : X.hp;
     for (int k = k0; k < k1; ++k) {
       const int lh = C.host[k], lg = C.guest[k];
       double cu = 0.0, cv = 0.0;

@@ -40,6 +40,8 @@ enum SlotKind : uint8_t { LAND = 0, WATER = 1, OPENBC = 2, CHAN = 3 };
 struct StepScalars {
   double delt, deltd2, delti, g, gi, hdry, rsqm, snlt, ritb1;
   int isdry, ndrystp, isbal, iterm;
+  int max_sweeps;       // wet/dry re-solve cap (the reference's 500)
+  int pad_sc;
   double rlamn;         // QCHERR: implicit weight of the channel flows
   int chan_consistent;  // channels: 1 = A*p with -CCCCHH (else as congradc.f90 writes it)
   int baro;             // BSC > 1e-6: the baroclinic terms FPGXE, FPGYE enter
@@ -63,15 +65,32 @@ struct Ctl {
   int active;                     // member takes part in the current sweep
   int nneg, nnonfinite, nwasted;
   unsigned int counter;           // last-CTA arrival counter
+  // the member's step, summed over its sweeps where the sweep loop runs on
+  // the device (k_after_solve, k_sweep_next); zero at the start of a step
+  int stepping;                   // the member takes part in this step
+  int mstatus;                    // its status (enum efdc_xm_status)
+  int sweep;                      // re-solves so far (NCORDRY)
+  int solves, iters_total, iters_last, outer_total;
+  int inner_first;                // MIXED: inner iterations of the first pass of the last solve
+  int last_inner;                 // MIXED: inner iterations of the last pass that had some
   int pad;
+  double rsq_last, ccmnm_last;
 };
 
-// Counters across members, polled by the host.
+// Loops of a step whose control runs on the device (conditional graph
+// nodes): the CG iterations, the MIXED outer passes and inner iterations, and
+// the wet/dry sweeps.
+enum Loop : int { LOOP_CG = 0, LOOP_OUTER = 1, LOOP_INNER = 2, LOOP_SWEEP = 3, NLOOP = 4 };
+
+// Counters across members, polled by the host (or read by the loop-control
+// kernels of a device-driven step).
 struct Glob {
   int ndone;     // members whose solve finished
   int nidone;    // members whose inner (FP32) solve finished
   int nicordry;  // members that need another wet/dry sweep
   int pad;
+  int loop[NLOOP];  // body executions of the loop now running (each loop's cap)
+  int tot[NLOOP];   // body executions in the step (the launch count)
 };
 
 // Static per-slot model data (FP64).  Land slots hold element LC.

@@ -125,6 +125,19 @@ void launch_adj_post(const Launch &l, const DevStatic &S, const DevState &X, con
                      const DevCalib &A);
 void launch_gather_slots(cudaStream_t st, const double *src, const int *slots, int n, double *out);
 
+// loop control of a step that runs as one graph (xm_loop.cu): each loop is a
+// conditional WHILE node whose handle these kernels set
+void launch_loop_enter(cudaStream_t st, Glob *g, int which, cudaGraphConditionalHandle h,
+                       int pending, int nmember);
+void launch_loop_next(cudaStream_t st, Glob *g, int which, cudaGraphConditionalHandle h, int cap,
+                      int inner, int nmember);
+void launch_step_enter(cudaStream_t st, Ctl *ctl, const int *act, Glob *g, int nmember);
+void launch_inner_done(cudaStream_t st, Ctl *ctl, const int *act, int nmember);
+void launch_after_solve(cudaStream_t st, Ctl *ctl, int *act, int nmember, int mixed);
+void launch_sweep_next(cudaStream_t st, const DevStatic &S, Ctl *ctl, int *act, Glob *g,
+                       cudaGraphConditionalHandle h, int cap, int nmember);
+void launch_fin_prepare(cudaStream_t st, const Ctl *ctl, int *act, int nmember);
+
 // sets the message returned by efdc_xm_last_error() for this thread
 void set_last_error_str(const char *msg);
 

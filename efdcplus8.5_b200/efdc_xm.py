@@ -316,6 +316,15 @@ def make_fields(st: dict, *, diag: bool = False, lists: bool = False):
     return s, keep
 
 
+OPT_DEVICE_LOOPS = 1
+OPT_GRAPH_ITERS = 2
+
+
+def host_waits() -> int:
+    """Host synchronisations made by step and solve calls so far."""
+    return int(load().efdc_xm_host_waits())
+
+
 class CudaLibraryMissing(RuntimeError):
     pass
 
@@ -362,6 +371,9 @@ def load(path: str | os.PathLike | None = None):
     lib.efdc_xm_stream.restype = C.c_void_p
     lib.efdc_xm_stream.argtypes = [C.c_void_p]
     lib.efdc_xm_kernel_launches.restype = C.c_int64
+    lib.efdc_xm_host_waits.restype = C.c_int64
+    lib.efdc_xm_set_option.restype = C.c_int32
+    lib.efdc_xm_set_option.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
     lib.efdc_xm_set_layers.restype = C.c_int32
     lib.efdc_xm_set_layers.argtypes = [C.c_void_p, C.c_int32, C.POINTER(Layers)]
     lib.efdc_xm_set_channels.restype = C.c_int32
@@ -472,6 +484,11 @@ class Solver:
 
     def stream(self) -> int:
         return int(self.lib.efdc_xm_stream(self.ctx) or 0)
+
+    def set_option(self, option: int, value: int):
+        rc = self.lib.efdc_xm_set_option(self.ctx, option, value)
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_set_option: {self.last_error()}")
 
     def set_layers(self, ly: dict, member: int = 0):
         s, _keep = make_layers(ly)
@@ -702,6 +719,11 @@ class BatchSolver:
 
     def stream(self) -> int:
         return int(self.lib.efdc_xm_stream(self.ctx) or 0)
+
+    def set_option(self, option: int, value: int):
+        rc = self.lib.efdc_xm_set_option(self.ctx, option, value)
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_set_option: {self.last_error()}")
 
     def time_kernels(self, precision: int, reps: int = 20) -> KTime:
         kt = KTime()

@@ -620,6 +620,84 @@ def add_baroclinic(scn: Scenario, kc: int = 4, *, seed: int = 0, front: float = 
     return scn
 
 
+def sample_model(f: dict, *, dt: float = 10.0, drawdown: float = 0.0,
+                 wind: tuple = (0.0, 0.0), manning: float = 0.025, u0: float = 0.05,
+                 seed: int = 0) -> Scenario:
+    """A scenario on one of EFDC+'s sample-model grids.
+
+    ``f`` holds the model's own arrays as tests/golden/make_sample_models.py
+    extracts them: the cell-type map IJCT (5 water, 9 land, 0 outside), DXP,
+    DYP, water depth and bottom elevation per cell (dxdy.inp), RSQM and ITERM
+    (card C3), ISDRY (C5), NDRYSTP (C7), HDRY (C11), the west elevation
+    boundary cells with their ISPBW (C19) and head (pser.inp at TBEGIN), and
+    the flow sources (C24 cells, qser.inp at TBEGIN times QSFACTOR).
+    Set here, not by the model files: the time step ``dt`` (the models step
+    dynamically or at 10 s), a uniform wind stress ``wind`` = (TSX, TSY), an
+    optional ``drawdown`` of the initial surface (so that shallow cells start
+    dry), and a bottom stress from Manning's ``manning`` on a seeded velocity
+    field of scale ``u0`` (as make_scenario)."""
+    rng = np.random.default_rng(seed)
+    ijct = np.where(np.asarray(f["ijct"]) == 5, WATER, LAND).astype(np.int32)
+    jc, ic = ijct.shape
+    dxp2d = np.where(ijct == WATER, f["dxp"], 0.0)
+    dyp2d = np.where(ijct == WATER, f["dyp"], 0.0)
+    belv2d = np.asarray(f["belv"], np.float64)
+    isdry = int(f["isdry"])
+    hdry = float(f["hdry"])
+    west = np.asarray(f["west"]).reshape(-1, 3)
+    obc = {"W": [(int(i), int(j), int(isp), [], []) for i, j, isp in west]}
+    wd = dxp2d[ijct == WATER]
+    la, lc, grid, lij, init = build_grid(ijct, dxp2d, dyp2d, belv2d, obc=obc, mtide=0, tcp=(),
+                                         dx=float(wd.mean()),
+                                         dy=float(dyp2d[ijct == WATER].mean()))
+    lcm = lc + 1
+    i0 = np.arange(1, la)
+    jj = grid["jl"][i0] - 1
+    ii = grid["il"][i0] - 1
+    belv = grid["belv"]
+    hp = np.zeros(lcm)
+    hp[i0] = np.maximum(np.asarray(f["depth"])[jj, ii] - drawdown,
+                        0.9 * hdry if isdry else 1e-3)
+    p = np.zeros(lcm)
+    p[i0] = G * (hp[i0] + belv[i0])
+    hu, hv, hpi, hui, hvi = face_depths(grid, hp)
+    tbx = np.zeros(lcm)
+    tby = np.zeros(lcm)
+    if manning and u0:
+        u = u0 * rng.uniform(-1.0, 1.0, la - 1)
+        v = u0 * rng.uniform(-1.0, 1.0, la - 1)
+        stbx = np.where(hu[i0] > 0, G * manning ** 2 / np.cbrt(np.maximum(hu[i0], 1e-3)), 0.0)
+        stby = np.where(hv[i0] > 0, G * manning ** 2 / np.cbrt(np.maximum(hv[i0], 1e-3)), 0.0)
+        sp = np.sqrt(u * u + v * v)
+        tbx[i0] = stbx * sp * u * grid["subo"][i0]
+        tby[i0] = stby * sp * v * grid["svbo"][i0]
+    qsume = np.zeros(lcm)
+    for i, j, q in np.asarray(f["sources"]).reshape(-1, 3):
+        qsume[int(lij[int(j) - 1, int(i) - 1]) - 1] += q
+    zeros = lambda: np.zeros(lcm)  # noqa: E731
+    tsx = zeros()
+    tsy = zeros()
+    tsx[i0] = wind[0]
+    tsy[i0] = wind[1]
+    head = float(f["west_head"]) if west.size else 0.0
+    state = dict(
+        p=p, hp=hp, h1p=hp.copy(), hu=hu, hv=hv, uhdye=zeros(), vhdxe=zeros(),
+        sub=init["sub"], svb=init["svb"], sbx=init["sbx"], sby=init["sby"],
+        lmaskdry=np.ones(lcm, np.int32), iscdry=np.zeros(lcm, np.int32),
+        lopenbcdry=np.zeros(lcm, np.int32), natdry=np.zeros(lcm, np.int32),
+        fcaxe=zeros(), fcaye=zeros(), fxe=zeros(), fye=zeros(),
+        tsx=tsx, tsy=tsy, tbx=tbx, tby=tby, qsume=qsume,
+        pser={s: np.full(len(grid["obc"][s]["l"]), G * head) for s in SIDES},
+        uhe=zeros(), vhe=zeros(), hpi=hpi, hui=hui, hvi=hvi,
+        qdwaste=zeros(), vdwaste=zeros(),
+    )
+    params = dict(dt=float(dt), g=G, hdry=hdry, rsqm=float(f["rsqm"]), iterm=int(f["iterm"]),
+                  isdry=isdry, ndrystp=int(f["ndrystp"]), isbal=1, snlt=0.0, ritb1=1.0,
+                  pi2=PI2, ntstbc=0, max_sweeps=500, kc=1)
+    return Scenario(ic=ic, jc=jc, la=la, lc=lc, grid=grid, state=state, params=params,
+                    ijct=ijct)
+
+
 def add_three_levels(scn: Scenario) -> Scenario:
     """The state of the three-time-level scheme (CALPUV9C) at its start, with
     level n-1 equal to level n: P1 = P, H2P = H1P = HP, UHDY1E = UHDY2E =

@@ -388,6 +388,24 @@ void *efdc_xm_stream(efdc_xm_ctx *ctx);
 /* Number of kernels this library has launched in the process so far. */
 int64_t efdc_xm_kernel_launches(void);
 
+/* Number of times a step or solve call of this library has waited for the
+ * device so far (host synchronisations).  A step whose loops run on the
+ * device (EFDC_XM_OPT_DEVICE_LOOPS) waits once, when it has finished. */
+int64_t efdc_xm_host_waits(void);
+
+/* Options of a context (no counterpart in the reference).
+ *   EFDC_XM_OPT_DEVICE_LOOPS (default 1): 1 runs each step as one CUDA graph
+ *     whose data-dependent loops -- the CG iterations (congrad.f90:91-169),
+ *     the MIXED refinement passes and the wet/dry re-solves (the GOTO 1000
+ *     of calpuv2c.f90:597-601, 726-749) -- are conditional nodes decided on
+ *     the device, so the host waits once per step; 0 drives those loops from
+ *     the host, polling the device between groups of iterations.  Both run
+ *     the same kernels in the same order.
+ *   EFDC_XM_OPT_GRAPH_ITERS (default 4, 1..32): CG iterations per loop body.
+ * Returns EFDC_XM_BAD_ARGUMENT for an unknown option or value. */
+enum { EFDC_XM_OPT_DEVICE_LOOPS = 1, EFDC_XM_OPT_GRAPH_ITERS = 2 };
+int32_t efdc_xm_set_option(efdc_xm_ctx *ctx, int32_t option, int32_t value);
+
 /* Bytes copied host->device (*h2d) and device->host (*d2h) by the upload,
  * download and step calls of every context since the library was loaded
  * (the caller's arrays only: no small control transfers). */

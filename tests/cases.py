@@ -72,6 +72,40 @@ def baroclinic(wetdry=False, *, closed=False, kc=4):
     return scn
 
 
+def copy_state(st):
+    return {k: (v.copy() if isinstance(v, np.ndarray) else
+                {s: a.copy() for s, a in v.items()} if isinstance(v, dict) else v)
+            for k, v in st.items()}
+
+
+def run_both(scn, steps, tm=1.0, precision=None, same_input=False, lists=False, n0=1,
+             nthreads=1, keep=None):
+    """Run the GPU library (efdc_xm_step on host arrays) and the oracle side by
+    side for `steps` steps.  Returns one (gpu stats, oracle stats, gpu state,
+    oracle state) tuple per step; `keep(n)` selects the steps whose states are
+    kept (default: all).  same_input=True starts every GPU step from the
+    oracle's state."""
+    import efdc_xm as X
+    import oracle as O
+    precision = X.PREC_FP64 if precision is None else precision
+    sol = X.Solver(scn.grid)
+    orc = O.Oracle(scn.grid, nthreads=nthreads)
+    sg, so = copy_state(scn.state), copy_state(scn.state)
+    out = []
+    for n in range(n0, n0 + steps):
+        if same_input:
+            sg = copy_state(so)
+        prm = X.make_params(scn.params, n=n, tn=scn.tn(n) * tm, precision=precision)
+        a = sol.step(prm, sg, lists=lists)
+        b = orc.step(X.make_params(scn.params, n=n, tn=scn.tn(n) * tm), so, lists=lists)
+        k = keep is None or keep(n)
+        out.append((a.as_dict(), b.as_dict(), copy_state(sg) if k else None,
+                    copy_state(so) if k else None))
+    sol.close()
+    orc.close()
+    return out
+
+
 def state_err(a, b, la, key="p", g=S.G):
     d = np.abs(a[key][1:la] - b[key][1:la])
     return float(d.max() / (g if key == "p" else 1.0))

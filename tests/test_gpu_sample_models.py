@@ -1,0 +1,121 @@
+"""GPU parity on the reference's own sample-model grids.
+
+EFDC+ ships three sample models (SampleModels/Lake_T_HYD_WQ, Lake_Washington,
+Ohio_River_4).  Their grids (cell.inp), metrics and bathymetry (dxdy.inp),
+solver constants (card C3: RSQM = 1e-9, ITERM = 200), wetting/drying set-up
+(C5 ISDRY, C11 HDRY, C7 NDRYSTP), west head boundary (C19, pser.inp) and flow
+sources (C24, qser.inp) are extracted into tests/golden/sample_*.npz by
+tests/golden/make_sample_models.py.  The time step (10 s), a uniform wind
+stress and, for one Lake_T case, a 0.6 m drawdown of the initial surface (so
+that its shallow margins dry and rewet) are this test's choices.
+
+These are irregular shorelines (lakes with bays and islands, a 106 x 9 river
+reach), whose tile layout, Morton order and land padding differ from the
+seeded rectangles of the other tests.
+
+Bars, as in test_gpu_parity.py: FP64 has the oracle's CG iteration count on
+every solve, the same sweeps, surface within 1e-9 m, and bit-exact masks,
+face switches and wet lists at every step; MIXED is within 1e-6 m of the FP64
+oracle from the same inputs with bit-exact masks; a batch of all four gives
+each member's single-basin result bit for bit.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import cases
+import efdc_xm as X
+import scenario as S
+
+pytestmark = pytest.mark.gpu
+
+GOLD = Path(__file__).resolve().parent / "golden"
+MASKS = ("sub", "svb", "sbx", "sby", "lmaskdry", "iscdry", "natdry")
+STATE = ("p", "hp", "hu", "hv", "uhdye", "vhdxe")
+
+VARIANTS = {
+    "lake_t": ("Lake_T_HYD_WQ", dict(wind=(2e-4, 1e-4))),
+    "lake_t_drawdown": ("Lake_T_HYD_WQ", dict(wind=(2e-4, 1e-4), drawdown=0.6)),
+    "lake_washington": ("Lake_Washington", dict(wind=(1e-4, 2e-4))),
+    "ohio_river": ("Ohio_River_4", dict()),
+}
+
+
+def model(name):
+    fname, kw = VARIANTS[name]
+    return S.sample_model(dict(np.load(GOLD / f"sample_{fname}.npz")), **kw)
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib():
+    X.load()
+
+
+@pytest.mark.parametrize("name", list(VARIANTS))
+def test_fp64_matches_oracle_every_step(name):
+    scn = model(name)
+    la = scn.la
+    res = cases.run_both(scn, 200, lists=True)
+    for n, (a, b, sg, so) in enumerate(res, 1):
+        assert a["status"] == b["status"] == X.OK, (n, a, b)
+        assert a["solves"] == b["solves"], (n, a, b)
+        assert a["iters_total"] == b["iters_total"], (n, a["iters_total"], b["iters_total"])
+        assert cases.state_err(sg, so, la) < 1e-9, n
+        for k in MASKS:
+            np.testing.assert_array_equal(sg[k][1:la], so[k][1:la], err_msg=f"{n}:{k}")
+        assert a["lawet"] == b["lawet"] and a["ladry"] == b["ladry"]
+        np.testing.assert_array_equal(sg["lwet"][:a["lawet"]], so["lwet"][:b["lawet"]])
+    a, b, sg, so = res[-1]
+    for k in STATE:
+        scale = max(1.0, float(np.abs(so[k][1:la]).max()))
+        assert np.abs(sg[k][1:la] - so[k][1:la]).max() <= 1e-9 * scale, k
+
+
+def test_wetting_and_drying_is_exercised():
+    """The drawn-down lake and Lake Washington toggle cells, so their mask
+    parity above covers real wet/dry sweeps on an irregular shoreline."""
+    for name in ("lake_t_drawdown", "lake_washington"):
+        scn = model(name)
+        res = cases.run_both(scn, 60)
+        toggles = sum(int(np.sum(r1[3]["lmaskdry"][1:scn.la] != r0[3]["lmaskdry"][1:scn.la]))
+                      for r0, r1 in zip(res[:-1], res[1:]))
+        sweeps = sum(b["solves"] for _, b, _, _ in res)
+        assert toggles > 0 and sweeps > len(res), (name, toggles, sweeps)
+
+
+@pytest.mark.parametrize("name", list(VARIANTS))
+def test_mixed_within_1e6_of_fp64_oracle(name):
+    scn = model(name)
+    res = cases.run_both(scn, 100, precision=X.PREC_MIXED, same_input=True)
+    for n, (a, b, sg, so) in enumerate(res, 1):
+        assert a["status"] == X.OK, (n, a)
+        assert cases.state_err(sg, so, scn.la) <= 1e-6, n
+        for k in ("lmaskdry", "sub", "svb", "iscdry"):
+            np.testing.assert_array_equal(sg[k][1:scn.la], so[k][1:scn.la], err_msg=f"{n}:{k}")
+
+
+def test_batch_of_sample_models_equals_single_runs():
+    scns = [model(nm) for nm in VARIANTS]
+    steps = 40
+    single = []
+    for scn in scns:
+        sol = X.Solver(scn.grid)
+        st = scn.copy_state()
+        its = []
+        for n in range(1, steps + 1):
+            its.append(sol.step(X.make_params(scn.params, n=n, tn=scn.tn(n)), st).iters_total)
+        sol.close()
+        single.append((st, its))
+    bs = X.BatchSolver([s.grid for s in scns])
+    sts = [s.copy_state() for s in scns]
+    its = [[] for _ in scns]
+    for n in range(1, steps + 1):
+        out = bs.step([X.make_params(s.params, n=n, tn=s.tn(n)) for s in scns], sts)
+        for m, r in enumerate(out):
+            its[m].append(r.iters_total)
+    bs.close()
+    for m, scn in enumerate(scns):
+        assert its[m] == single[m][1], m
+        for k in STATE + MASKS:
+            np.testing.assert_array_equal(sts[m][k], single[m][0][k], err_msg=f"{m}:{k}")
