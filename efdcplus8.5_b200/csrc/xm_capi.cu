@@ -220,6 +220,9 @@ struct efdc_xm_ctx {
   // ran without wetting and drying (and without baroclinic terms) and did
   // not upload them; the host holds them
   bool wd_stale = false, sbxy_stale = false;
+  // arrays (bits of enum efdc_xm_same) whose device copy is still what the
+  // caller's array held at its last upload or received at its last download
+  uint32_t synced = 0;
   // three time levels (CALPUV9C): their buffers are allocated by the first
   // upload that carries them (tl3_alloc); tl3_ready: the device holds a
   // consistent set of levels (uploaded, or advanced by CALPUV9C steps)
@@ -1245,10 +1248,31 @@ namespace {
 // Their device copies are then marked out of date.  levels: upload the three
 // time levels of CALPUV9C (P1, H2P, H1P, UHDY1E ... FPGYE) as well.
 // The arrays of an upload, with its argument checks.
+// Arrays written by a step without wetting and drying, and by any step
+// (their device copies stop matching the caller's).
+constexpr uint32_t STEP_WRITES_DRYFREE = EFDC_XM_SAME_P | EFDC_XM_SAME_HP | EFDC_XM_SAME_HU |
+                                         EFDC_XM_SAME_HV | EFDC_XM_SAME_UHDYE |
+                                         EFDC_XM_SAME_VHDXE | EFDC_XM_SAME_LOPENBCDRY;
+constexpr uint32_t STEP_WRITES =
+    EFDC_XM_SAME_P | EFDC_XM_SAME_HP | EFDC_XM_SAME_HU | EFDC_XM_SAME_HV | EFDC_XM_SAME_UHDYE |
+    EFDC_XM_SAME_VHDXE | EFDC_XM_SAME_SUB | EFDC_XM_SAME_SVB | EFDC_XM_SAME_SBX |
+    EFDC_XM_SAME_SBY | EFDC_XM_SAME_LMASKDRY | EFDC_XM_SAME_ISCDRY | EFDC_XM_SAME_LOPENBCDRY |
+    EFDC_XM_SAME_NATDRY | EFDC_XM_SAME_QDWASTE | EFDC_XM_SAME_VDWASTE;
+
+// The arrays of an upload.  An array whose bit the caller set in `unchanged`
+// and whose device copy is still its last transfer is left out; *sent gets
+// the bits of the arrays that go.
 int plan_upload(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool skip_sbxy,
-                bool levels, std::vector<Xfer> &xs) {
+                bool levels, std::vector<Xfer> &xs, uint32_t *sent = nullptr) {
   xm::DevState &X = c->X;
   const int M = c->M;
+  for (int m = 1; m < M; ++m)
+    if (f[m].unchanged != f[0].unchanged) {
+      set_error("efdc_xm_upload: member %d: the unchanged bits differ from member 0's", m);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+  const uint32_t skip = f[0].unchanged & c->synced;
+  uint32_t went = 0;
   for (int m = 0; m < M; ++m)
     if (!c->chans[m].empty() && (!f[m].qchanu || !f[m].qchanv || !f[m].qchanun || !f[m].qchanvn)) {
       set_error("efdc_xm_upload: member %d has sub-grid channels: QCHANU, QCHANV, QCHANUN and "
@@ -1262,19 +1286,34 @@ int plan_upload(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool 
     for (int m = 0; m < M; ++m) v[m] = f[m].name;                \
     if ((rc = collect(c, xs, v, dev, kind, #name))) return rc;   \
   }
-  XM_UP(p, X.p, 0) XM_UP(hp, X.hp, 0) XM_UP(hu, X.hu, 0) XM_UP(hv, X.hv, 0)
-  XM_UP(uhdye, X.uhdye, 0) XM_UP(vhdxe, X.vhdxe, 0) XM_UP(sub, X.sub, 0) XM_UP(svb, X.svb, 0)
-  XM_UP(lopenbcdry, X.lopenbcdry, 1)
-  XM_UP(fcaxe, X.fcaxe, 0) XM_UP(fcaye, X.fcaye, 0) XM_UP(fxe, X.fxe, 0) XM_UP(fye, X.fye, 0)
-  XM_UP(tsx, X.tsx, 0) XM_UP(tsy, X.tsy, 0) XM_UP(tbx, X.tbx, 0) XM_UP(tby, X.tby, 0)
-  XM_UP(qsume, X.qsume, 0)
+#define XM_UPB(name, dev, kind, bit)                             \
+  if (!(skip & (bit))) {                                         \
+    const size_t n0 = xs.size();                                 \
+    XM_UP(name, dev, kind)                                       \
+    if (xs.size() > n0) went |= (bit);                           \
+  }
+  XM_UPB(p, X.p, 0, EFDC_XM_SAME_P) XM_UPB(hp, X.hp, 0, EFDC_XM_SAME_HP)
+  XM_UPB(hu, X.hu, 0, EFDC_XM_SAME_HU) XM_UPB(hv, X.hv, 0, EFDC_XM_SAME_HV)
+  XM_UPB(uhdye, X.uhdye, 0, EFDC_XM_SAME_UHDYE) XM_UPB(vhdxe, X.vhdxe, 0, EFDC_XM_SAME_VHDXE)
+  XM_UPB(sub, X.sub, 0, EFDC_XM_SAME_SUB) XM_UPB(svb, X.svb, 0, EFDC_XM_SAME_SVB)
+  XM_UPB(lopenbcdry, X.lopenbcdry, 1, EFDC_XM_SAME_LOPENBCDRY)
+  XM_UPB(fcaxe, X.fcaxe, 0, EFDC_XM_SAME_FCAXE) XM_UPB(fcaye, X.fcaye, 0, EFDC_XM_SAME_FCAYE)
+  XM_UPB(fxe, X.fxe, 0, EFDC_XM_SAME_FXE) XM_UPB(fye, X.fye, 0, EFDC_XM_SAME_FYE)
+  XM_UPB(tsx, X.tsx, 0, EFDC_XM_SAME_TSX) XM_UPB(tsy, X.tsy, 0, EFDC_XM_SAME_TSY)
+  XM_UPB(tbx, X.tbx, 0, EFDC_XM_SAME_TBX) XM_UPB(tby, X.tby, 0, EFDC_XM_SAME_TBY)
+  XM_UPB(qsume, X.qsume, 0, EFDC_XM_SAME_QSUME)
   if (!skip_sbxy) {
-    XM_UP(sbx, X.sbx, 0) XM_UP(sby, X.sby, 0)
+    XM_UPB(sbx, X.sbx, 0, EFDC_XM_SAME_SBX) XM_UPB(sby, X.sby, 0, EFDC_XM_SAME_SBY)
   }
   if (!skip_wetdry) {
-    XM_UP(lmaskdry, X.lmaskdry, 1) XM_UP(iscdry, X.iscdry, 2) XM_UP(natdry, X.natdry, 2)
-    XM_UP(qdwaste, X.qdwaste, 0) XM_UP(vdwaste, X.vdwaste, 0)
+    XM_UPB(lmaskdry, X.lmaskdry, 1, EFDC_XM_SAME_LMASKDRY)
+    XM_UPB(iscdry, X.iscdry, 2, EFDC_XM_SAME_ISCDRY)
+    XM_UPB(natdry, X.natdry, 2, EFDC_XM_SAME_NATDRY)
+    XM_UPB(qdwaste, X.qdwaste, 0, EFDC_XM_SAME_QDWASTE)
+    XM_UPB(vdwaste, X.vdwaste, 0, EFDC_XM_SAME_VDWASTE)
   }
+  if (sent) *sent = went;
+#undef XM_UPB
   if (levels) {
     for (int m = 0; m < M; ++m) {
       const efdc_xm_fields &x = f[m];
@@ -1383,11 +1422,16 @@ int upload_batch(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool
   }
   CK(cudaSetDevice(c->device));
   std::vector<Xfer> xs;
-  int rc = plan_upload(c, f, skip_wetdry, skip_sbxy, levels, xs);
+  uint32_t sent = 0;
+  int rc = plan_upload(c, f, skip_wetdry, skip_sbxy, levels, xs, &sent);
   if (!rc) rc = upload_arrays(c, xs);
   if (!rc && !levels) rc = copy_levels(c, f, 0, size_t(c->nslot), c->stream);
   if (!rc) rc = upload_small(c, f);
-  if (rc) return rc;
+  if (rc) {
+    c->synced = 0;  // the device copies are not known to match anything
+    return rc;
+  }
+  c->synced |= sent;
   upload_done(c, f, skip_wetdry, skip_sbxy, levels);
   return EFDC_XM_OK;
 }
@@ -1416,32 +1460,48 @@ struct Lists {
 };
 
 // The arrays of a download.
+// The arrays of a download; *got: the bits (enum efdc_xm_same) of those that
+// come back, whose device copies then match the caller's arrays.
 int plan_download(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int levels,
-                  std::vector<Xfer> &xs, Lists &ls) {
+                  std::vector<Xfer> &xs, Lists &ls, uint32_t *got = nullptr) {
   xm::DevState &X = c->X;
   const xm::DevSystem &Y = c->Y;
   const int M = c->M;
   int rc = 0;
+  uint32_t back = 0;
 #define XM_DN(name, dev, kind)                                   \
   {                                                              \
     std::vector<const void *> v(M);                              \
     for (int m = 0; m < M; ++m) v[m] = f[m].name;                \
     if ((rc = collect(c, xs, v, dev, kind, #name))) return rc;   \
   }
-  XM_DN(p, X.p, 0) XM_DN(hp, X.hp, 0) XM_DN(h1p, X.h1p, 0) XM_DN(hu, X.hu, 0) XM_DN(hv, X.hv, 0)
-  XM_DN(uhdye, X.uhdye, 0) XM_DN(vhdxe, X.vhdxe, 0) XM_DN(lopenbcdry, X.lopenbcdry, 1)
+#define XM_DNB(name, dev, kind, bit)                             \
+  {                                                              \
+    const size_t n0 = xs.size();                                 \
+    XM_DN(name, dev, kind)                                       \
+    if (xs.size() > n0) back |= (bit);                           \
+  }
+  XM_DNB(p, X.p, 0, EFDC_XM_SAME_P) XM_DNB(hp, X.hp, 0, EFDC_XM_SAME_HP) XM_DN(h1p, X.h1p, 0)
+  XM_DNB(hu, X.hu, 0, EFDC_XM_SAME_HU) XM_DNB(hv, X.hv, 0, EFDC_XM_SAME_HV)
+  XM_DNB(uhdye, X.uhdye, 0, EFDC_XM_SAME_UHDYE) XM_DNB(vhdxe, X.vhdxe, 0, EFDC_XM_SAME_VHDXE)
+  XM_DNB(lopenbcdry, X.lopenbcdry, 1, EFDC_XM_SAME_LOPENBCDRY)
   XM_DN(uhe, X.uhe, 0) XM_DN(vhe, X.vhe, 0) XM_DN(hpi, X.hpi, 0) XM_DN(hui, X.hui, 0)
   XM_DN(hvi, X.hvi, 0)
   if (!skip_unchanged) {
-    XM_DN(sub, X.sub, 0) XM_DN(svb, X.svb, 0)
+    XM_DNB(sub, X.sub, 0, EFDC_XM_SAME_SUB) XM_DNB(svb, X.svb, 0, EFDC_XM_SAME_SVB)
     if (!c->sbxy_stale) {  // else the host holds them (see sbxy_stale)
-      XM_DN(sbx, X.sbx, 0) XM_DN(sby, X.sby, 0)
+      XM_DNB(sbx, X.sbx, 0, EFDC_XM_SAME_SBX) XM_DNB(sby, X.sby, 0, EFDC_XM_SAME_SBY)
     }
     if (!c->wd_stale) {
-      XM_DN(lmaskdry, X.lmaskdry, 1) XM_DN(iscdry, X.iscdry, 2) XM_DN(natdry, X.natdry, 2)
-      XM_DN(qdwaste, X.qdwaste, 0) XM_DN(vdwaste, X.vdwaste, 0)
+      XM_DNB(lmaskdry, X.lmaskdry, 1, EFDC_XM_SAME_LMASKDRY)
+      XM_DNB(iscdry, X.iscdry, 2, EFDC_XM_SAME_ISCDRY)
+      XM_DNB(natdry, X.natdry, 2, EFDC_XM_SAME_NATDRY)
+      XM_DNB(qdwaste, X.qdwaste, 0, EFDC_XM_SAME_QDWASTE)
+      XM_DNB(vdwaste, X.vdwaste, 0, EFDC_XM_SAME_VDWASTE)
     }
   }
+  if (got) *got = back;
+#undef XM_DNB
   XM_DN(ccc, Y.ccc, 0) XM_DN(ccs, Y.ccs, 0) XM_DN(ccw, Y.ccw, 0) XM_DN(cce, Y.cce, 0)
   XM_DN(ccn, Y.ccn, 0) XM_DN(fptmp, Y.fptmp, 0)
   if (levels && c->tl3_alloc) {
@@ -1521,7 +1581,8 @@ int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int l
   CK(cudaSetDevice(c->device));
   std::vector<Xfer> xs;
   Lists ls;
-  int rc = plan_download(c, f, skip_unchanged, levels, xs, ls);
+  uint32_t got = 0;
+  int rc = plan_download(c, f, skip_unchanged, levels, xs, ls, &got);
   if (rc) return rc;
   if (c->last_mixed && wants_system(f)) {
     // a MIXED step solves from the unscaled assembly: the scaled system
@@ -1533,6 +1594,7 @@ int download_batch(efdc_xm_ctx *c, efdc_xm_fields *f, bool skip_unchanged, int l
     CK(cudaGetLastError());
   }
   if ((rc = download_arrays(c, xs))) return rc;
+  c->synced |= got;
   return download_finish(c, f, ls);
 }
 }  // namespace
@@ -1955,6 +2017,8 @@ int step_range(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats, 
     any_waste |= (isd > 0 && prm[m].ndrystp < 0);
     c->act_h[m] = 1;
   }
+  // what the step writes no longer matches the caller's arrays
+  c->synced &= ~(any_isdry ? STEP_WRITES : STEP_WRITES_DRYFREE);
   int rc = to_device(c, c->sc, c->sc_h, c->sc_hd, sizeof(xm::StepScalars) * M);
   if (rc) return rc;
   if (c->in_chunks)  // counters of this step (no copy engine: see to_device)
@@ -2187,7 +2251,8 @@ int step_batch_chunks(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields 
   const int M = c->M;
   std::vector<Xfer> up, dn;
   Lists ls;
-  int rc = plan_upload(c, f, skip_wetdry, skip_sbxy, false, up);
+  uint32_t sent = 0, got = 0;
+  int rc = plan_upload(c, f, skip_wetdry, skip_sbxy, false, up, &sent);
   if (rc) {
     fill_status(stats, M, rc);
     return rc;
@@ -2204,7 +2269,9 @@ int step_batch_chunks(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields 
     if (rc) return rc;
   }
   upload_done(c, f, skip_wetdry, skip_sbxy, false);  // the state the step and download see
-  if ((rc = plan_download(c, f, skip_wetdry, 0, dn, ls))) {
+  const uint32_t sent_before_step = c->synced | sent;
+  c->synced = 0;  // until the call has finished (then: what went up or came back)
+  if ((rc = plan_download(c, f, skip_wetdry, 0, dn, ls, &got))) {
     fill_status(stats, M, rc);
     return rc;
   }
@@ -2307,6 +2374,9 @@ int step_batch_chunks(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields 
   fail(0);
   CK(cudaGetLastError());
   if ((rc = download_finish(c, f, ls))) return rc;
+  // the kept copies, those that went up and were not written by the steps,
+  // and those that came back
+  c->synced = (sent_before_step & ~(skip_wetdry ? STEP_WRITES_DRYFREE : STEP_WRITES)) | got;
   return overall_status(stats, M);
 }
 
@@ -2737,6 +2807,7 @@ int32_t efdc_xm_bottom_stress_batch(efdc_xm_ctx *c, const efdc_xm_drag_params *p
     set_error("efdc_xm_bottom_stress: NULL argument");
     return EFDC_XM_BAD_ARGUMENT;
   }
+  c->synced &= ~uint32_t(EFDC_XM_SAME_TBX | EFDC_XM_SAME_TBY);  // written on the device
   const int M = c->M;
   for (int m = 0; m < M; ++m) {
     const efdc_xm_drag_fields &x = f[m];
@@ -2850,6 +2921,7 @@ int32_t efdc_xm_congrad(efdc_xm_ctx *c, const double *ccc, const double *ccs, co
                         int32_t precision, int32_t *iters, double *rsq) {
   int rc = single_only(c, "efdc_xm_congrad");
   if (rc) return rc;
+  c->synced &= ~uint32_t(EFDC_XM_SAME_P);  // the solve runs in the state's P
   if (!ccc || !ccs || !ccn || !ccw || !cce || !fptmp || !p || iterm < 1) {
     set_error("efdc_xm_congrad: NULL argument or ITERM < 1");
     return EFDC_XM_BAD_ARGUMENT;
@@ -3152,10 +3224,13 @@ int32_t efdc_xm_calib_snapshot(efdc_xm_ctx *c, int32_t slot) {
 
 int32_t efdc_xm_calib_restore(efdc_xm_ctx *c, int32_t slot) {
   const int rc = calib_ready(c, "efdc_xm_calib_restore");
-  return rc ? rc : snap_copy(c, slot, false);
+  if (rc) return rc;
+  c->synced &= ~STEP_WRITES;  // the snapshot overwrites the state
+  return snap_copy(c, slot, false);
 }
 
 int32_t efdc_xm_calib_step(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats) {
+  if (c) c->synced &= ~uint32_t(EFDC_XM_SAME_TBX | EFDC_XM_SAME_TBY);  // the drag is written
   efdc_xm_stats dummy;
   if (!stats) stats = &dummy;
   std::memset(stats, 0, sizeof(*stats));

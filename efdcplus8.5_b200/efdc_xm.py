@@ -71,7 +71,8 @@ class Fields(C.Structure):
                 ("qchanvn", _pd), ("b", _pd), ("b_ld", C.c_int32), ("pad_b_", C.c_int32),
                 ("p1", _pd), ("h2p", _pd), ("uhdy1e", _pd), ("vhdx1e", _pd), ("uhdy2e", _pd),
                 ("vhdx2e", _pd), ("h1u", _pd), ("h1v", _pd), ("tsx1", _pd), ("tsy1", _pd),
-                ("tbx1", _pd), ("tby1", _pd), ("fpgxe", _pd), ("fpgye", _pd)]
+                ("tbx1", _pd), ("tby1", _pd), ("fpgxe", _pd), ("fpgye", _pd),
+                ("unchanged", C.c_int32), ("pad_u_", C.c_int32)]
 
 
 class Layers(C.Structure):
@@ -281,9 +282,26 @@ def make_channels(ch: dict | None):
     return s, keep
 
 
-def make_fields(st: dict, *, diag: bool = False, lists: bool = False):
-    """Build a Fields struct over the numpy arrays of a state dict (in place)."""
+# bits of efdc_xm_fields.unchanged (enum efdc_xm_same), one per array
+SAME = {k: 1 << i for i, k in enumerate((
+    "p", "hp", "hu", "hv", "uhdye", "vhdxe", "sub", "svb", "sbx", "sby", "lmaskdry", "iscdry",
+    "lopenbcdry", "natdry", "fcaxe", "fcaye", "fxe", "fye", "tsx", "tsy", "tbx", "tby", "qsume",
+    "qdwaste", "vdwaste"))}
+
+
+def same_bits(names) -> int:
+    """The efdc_xm_fields.unchanged bits of the named arrays."""
+    b = 0
+    for k in names:
+        b |= SAME[k]
+    return b
+
+
+def make_fields(st: dict, *, diag: bool = False, lists: bool = False, unchanged: int = 0):
+    """Build a Fields struct over the numpy arrays of a state dict (in place).
+    unchanged: efdc_xm_fields.unchanged (see same_bits)."""
     s = Fields()
+    s.unchanged = unchanged
     keep = []
     for k in FIELD_DOUBLE_INOUT + FIELD_IN + FIELD_OUT + FIELD_CHAN + FIELD_TL3:
         a = st.get(k)
@@ -683,11 +701,12 @@ class BatchSolver:
     def step(self, params: list, states: list, *, diag=False, lists=False) -> list:
         return self.step_prepared(params, self.prepare(states, diag=diag, lists=lists))
 
-    def prepare(self, states: list, *, diag=False, lists=False):
+    def prepare(self, states: list, *, diag=False, lists=False, unchanged: int = 0):
         """The members' Fields structs over `states`, for step_prepared: a driver
         whose arrays stay in place builds them once (256 members: ~30 ms of
-        Python per build)."""
-        return self._fields(states, diag=diag, lists=lists)
+        Python per build).  unchanged: the arrays (same_bits) the driver does
+        not touch between steps."""
+        return self._fields(states, diag=diag, lists=lists, unchanged=unchanged)
 
     def step_prepared(self, params: list, prepared) -> list:
         """efdc_xm_step_batch on the arrays of prepare(states)."""

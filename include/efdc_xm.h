@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define EFDC_XM_ABI_VERSION 4
+#define EFDC_XM_ABI_VERSION 5
 
 /* Status codes.  The reference STOPs where these are returned. */
 enum efdc_xm_status {
@@ -179,7 +179,30 @@ typedef struct efdc_xm_fields {
   double *h1u, *h1v;                  /* H1U, H1V                                     */
   const double *tsx1, *tsy1, *tbx1, *tby1;  /* TSX1, TSY1, TBX1, TBY1, in            */
   double *fpgxe, *fpgye;              /* FPGXE, FPGYE, in/out; required where BSC > 1e-6 */
+  /* in, optional (0: every given array is sent): bits of enum efdc_xm_same.
+   * A set bit promises that the caller's array holds exactly what this
+   * context last uploaded from it or downloaded into it; the library then
+   * skips its upload if its own device copy is still that transfer's (no step
+   * has written it since without a download).  No counterpart in the
+   * reference: it spares a host whose other modules did not touch an array
+   * between two steps the copy of it.  The members of a batch give the same
+   * bits. */
+  uint32_t unchanged;
+  int32_t pad_u_;
 } efdc_xm_fields;
+
+/* Bits of efdc_xm_fields.unchanged, one per array. */
+enum efdc_xm_same {
+  EFDC_XM_SAME_P = 1 << 0, EFDC_XM_SAME_HP = 1 << 1, EFDC_XM_SAME_HU = 1 << 2,
+  EFDC_XM_SAME_HV = 1 << 3, EFDC_XM_SAME_UHDYE = 1 << 4, EFDC_XM_SAME_VHDXE = 1 << 5,
+  EFDC_XM_SAME_SUB = 1 << 6, EFDC_XM_SAME_SVB = 1 << 7, EFDC_XM_SAME_SBX = 1 << 8,
+  EFDC_XM_SAME_SBY = 1 << 9, EFDC_XM_SAME_LMASKDRY = 1 << 10, EFDC_XM_SAME_ISCDRY = 1 << 11,
+  EFDC_XM_SAME_LOPENBCDRY = 1 << 12, EFDC_XM_SAME_NATDRY = 1 << 13,
+  EFDC_XM_SAME_FCAXE = 1 << 14, EFDC_XM_SAME_FCAYE = 1 << 15, EFDC_XM_SAME_FXE = 1 << 16,
+  EFDC_XM_SAME_FYE = 1 << 17, EFDC_XM_SAME_TSX = 1 << 18, EFDC_XM_SAME_TSY = 1 << 19,
+  EFDC_XM_SAME_TBX = 1 << 20, EFDC_XM_SAME_TBY = 1 << 21, EFDC_XM_SAME_QSUME = 1 << 22,
+  EFDC_XM_SAME_QDWASTE = 1 << 23, EFDC_XM_SAME_VDWASTE = 1 << 24
+};
 
 typedef struct efdc_xm_stats {
   int32_t status;       /* enum efdc_xm_status                                   */
