@@ -243,11 +243,17 @@ struct efdc_xm_ctx {
     bufs.push_back(b);
     return static_cast<T *>(b.p);
   }
+  // schedule of the FP32 CG kernels (efdc_xm_set_option: variant and CTA caps)
+  int kvariant = 0, ctas_mv = 0, ctas_up = 0;
   xm::Launch L() const {
-    return xm::Launch{grid,      grid_cg, grid_cg32, grid_up32,
-                      ntile,     nsm,     stream,
-                      mx_jac,  mx_poly, any_may_asym || sys_external,
-                      S.ch.n > 0 && !sys_external, step_baro && !sys_external};
+    xm::Launch l{grid,      grid_cg, grid_cg32, grid_up32,
+                 ntile,     nsm,     stream,
+                 mx_jac,  mx_poly, any_may_asym || sys_external,
+                 S.ch.n > 0 && !sys_external, step_baro && !sys_external};
+    l.variant = kvariant;
+    l.ctas_mv = ctas_mv;
+    l.ctas_up = ctas_up;
+    return l;
   }
 };
 
@@ -1081,6 +1087,7 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   Y.r32 = Fl(); Y.pa32 = Fl(); Y.pb32 = Fl(); Y.ap32 = Fl(); Y.x32 = Fl(); Y.z32 = Fl();
   Y.r32b = Fl();
   Y.mpoly = c->mpoly;
+  Y.err = c->glob ? &c->glob->err : nullptr;
   c->ptmp = D();
   c->mxview = xm::SysView{X.fp, X.cc, X.cs, X.cw, X.ce, X.cn, 1};
   if (!c->ptmp || !Y.x32 || !Y.z32 || !Y.r32b) return bail("cudaMalloc failed (device memory)");
@@ -1619,6 +1626,7 @@ struct StepPlan {
   int mixed, istl, all, any_isdry, any_legacy, any99, any_waste, iters;
   int max_iterm, max_sweeps, grid, grid_cg, grid_cg32, grid_up32;
   int mx_jac, mx_poly, may_asym, chan, baro, obc_serial, any_may_asym, nmember;
+  int variant, ctas_mv, ctas_up, pad;
   double fac;
   const void *psol;
 };
@@ -1875,6 +1883,16 @@ void drop_step_graphs(efdc_xm_ctx *c) {
   c->step_graph_failed.clear();
 }
 
+// A bounded wait in a kernel ran out (Glob::err): every member of the step
+// fails with EFDC_XM_DEVICE_TIMEOUT; the flag is cleared for the next call.
+int device_timeout(efdc_xm_ctx *c, efdc_xm_stats *stats, int m0, int m1) {
+  set_error("a bounded device-side wait ran out (bulk copies into shared memory did not "
+            "complete); the step's results are not valid");
+  for (int m = m0; m < m1; ++m) stats[m].status = EFDC_XM_DEVICE_TIMEOUT;
+  CK(cudaMemsetAsync(&c->glob->err, 0, sizeof(int), c->stream));
+  return EFDC_XM_DEVICE_TIMEOUT;
+}
+
 // Runs the step's graph and reads the members' control blocks (one host
 // wait), then fills the stats of the members [m0, m1) as step_range's host
 // loop does.  Returns -1 (nothing launched) if the graph could not be built.
@@ -1895,6 +1913,7 @@ int run_step_graph(efdc_xm_ctx *c, const StepPlan &pl, const xm::DevState &x_pre
   long long n = sg->n_top;
   for (int i = 0; i < xm::NLOOP; ++i) n += sg->n_body[i] * c->glob_h->tot[i];
   xm::count_launches(int(std::min<long long>(n, INT32_MAX)));
+  if (c->glob_h->err) return device_timeout(c, stats, m0, m1);
   for (int m = m0; m < m1; ++m) {
     const Ctl &k = c->ctl_h[m];
     efdc_xm_stats &s = stats[m];
@@ -2088,6 +2107,9 @@ int step_range(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats, 
     pl.baro = lk.baro;
     pl.obc_serial = c->obc_serial;
     pl.any_may_asym = c->any_may_asym;
+    pl.variant = lk.variant;
+    pl.ctas_mv = lk.ctas_mv;
+    pl.ctas_up = lk.ctas_up;
     pl.nmember = M;
     pl.fac = mixed ? (prm[0].mixed_rsq_factor > 0 ? prm[0].mixed_rsq_factor : 0.1) : 0.0;
     pl.psol = c->psol;
@@ -2117,6 +2139,8 @@ int step_range(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats, 
     CK(cudaGetLastError());
     rc = mixed ? solve_mixed(c, c->X.p, prm[0].mixed_rsq_factor) : solve_fp64(c, c->X.p);
     if (rc) return rc;
+    if ((rc = read_glob(c))) return rc;
+    if (c->glob_h->err) return device_timeout(c, stats, m0, m1);
     if (c->psol)  // calibration: the adjoint needs P' before P is refreshed from HP
       CK(cudaMemcpyAsync(c->psol, c->X.p, size_t(c->nslot) * sizeof(double),
                          cudaMemcpyDeviceToDevice, c->stream));
@@ -2984,6 +3008,18 @@ int32_t efdc_xm_set_option(efdc_xm_ctx *c, int32_t option, int32_t value) {
         drop_step_graphs(c);
       }
       return EFDC_XM_OK;
+    case EFDC_XM_OPT_KERNEL_VARIANT:
+    case EFDC_XM_OPT_CTAS_MATVEC:
+    case EFDC_XM_OPT_CTAS_UPDATE: {
+      const bool var = option == EFDC_XM_OPT_KERNEL_VARIANT;
+      if (var ? (value < 0 || value > 2) : (value < 0 || value > 32)) break;
+      int &v = var ? c->kvariant : option == EFDC_XM_OPT_CTAS_MATVEC ? c->ctas_mv : c->ctas_up;
+      if (v != value) {
+        v = value;
+        drop_graphs(c);  // the captured iterations hold the kernels and their grids
+      }
+      return EFDC_XM_OK;
+    }
     default:
       break;
   }

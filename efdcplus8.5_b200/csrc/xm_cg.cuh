@@ -9,6 +9,7 @@
 #pragma once
 
 #include "xm_common.cuh"
+#include "xm_tma.cuh"
 
 namespace xm {
 
@@ -128,6 +129,266 @@ __device__ __forceinline__ void quad_sweep(const DevStatic &S, double *part, Set
     nxt = nn;
   }
   if (n) quad_store<NS>(L, n, S, part);
+}
+
+// quad_sweep with the descriptors in batches: the CTA first loads, for its
+// next QB quads at once, each quad's table entry, its member's values and its
+// tiles' neighbour entries into shared memory (one round of dependent loads
+// per batch, by QB*4 threads in parallel), then runs the quads with no
+// dependent load ahead of their data loads.  Same results as quad_sweep: the
+// same rows, the same warp sums, the same per-quad partials.
+constexpr int QB = 32;  // quads per descriptor batch (QB * TILES_PER_CTA <= NT)
+
+template <int NS, class Setup, class Body>
+__device__ __forceinline__ void quad_sweep_batched(const DevStatic &S, double *part, Setup setup,
+                                                   Body body) {
+  using A = decltype(setup(0));
+  __shared__ QuadLog<NS> L;
+  __shared__ A da[QB];
+  __shared__ int4 dq[QB];
+  __shared__ int4 dnb[QB][TILES_PER_CTA];
+  static_assert(QB * TILES_PER_CTA <= NT, "one descriptor load per thread");
+  const int sub = threadIdx.x / TPT, q = threadIdx.x % TPT;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int G = gridDim.x, NQ = S.nquad;
+  int n = 0;
+  for (int b0 = blockIdx.x; b0 < NQ; b0 += G * QB) {
+    __syncthreads();  // the previous batch's descriptors are no longer read
+    if (threadIdx.x < QB * TILES_PER_CTA) {
+      const int k = threadIdx.x / TILES_PER_CTA, s = threadIdx.x % TILES_PER_CTA;
+      const int qd = b0 + k * G;
+      if (qd < NQ) {
+        const int4 cur = S.quads[qd];
+        if (s == 0) {
+          dq[k] = cur;
+          da[k] = setup(cur.x);
+        }
+        dnb[k][s] = __ldg(&S.tnbr[s < cur.z ? cur.y + s : 0]);
+      }
+    }
+    __syncthreads();
+    const int nk = min(QB, (NQ - b0 + G - 1) / G);
+    for (int k = 0; k < nk; ++k) {
+      const A a = da[k];
+      if (a.skip) continue;  // the same for the whole CTA
+      const int4 cur = dq[k];
+      const bool valid = sub < cur.z;
+      const RowGeo g = row_geo_nb(dnb[k][sub], valid ? cur.y + sub : 0, q);
+      double v[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) v[s] = 0.0;
+      body(a, g, valid, v);
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const double x = warp_sum(v[s]);
+        if (lane == 0) L.w[s][n][warp] = x;
+      }
+      if (threadIdx.x == 0) L.qd[n] = b0 + k * G;
+      if (++n == QCAP) {
+        quad_store<NS>(L, n, S, part);
+        n = 0;
+      }
+    }
+  }
+  if (n) quad_store<NS>(L, n, S, part);
+}
+
+// ---------------------------------------------------------------------------
+// Staged quad sweep (FP32 kernels, variant 2).  A quad's rows move into shared
+// memory by 1-D bulk copies that complete on an mbarrier, in a ring of two
+// stages: while the CTA computes one quad from one stage, the next quad's
+// copies are in flight into the other.  A stage holds, for the quad's (up to
+// 4) tiles, the whole tiles of NB arrays ("body": 1 KB per tile and array,
+// contiguous because a quad's tiles are), the row 0 of each tile's north
+// neighbour of NHN arrays and the row 7 of each tile's south neighbour of NHS
+// arrays (the N/S halo rows of the tile's edge rows).  The E/W edge columns
+// stay plain loads of the row body (L2 hits: the neighbour tiles are in
+// flight or just done in the same window of quads).  Only this GPU's memory
+// is read, each CTA for itself: no multicast.
+template <int NB, int NHN, int NHS>
+struct Stage {
+  float body[NB][TILES_PER_CTA * TILE];
+  float hn[NHN > 0 ? NHN : 1][TILES_PER_CTA][TX];
+  float hs[NHS > 0 ? NHS : 1][TILES_PER_CTA][TX];
+};
+
+// Where a thread's cells and their N/S rows are in a stage.
+struct StageRow {
+  int t;       // tile of the quad (0..3)
+  int r0;      // offset of the thread's 4 cells in a body array of the stage
+  bool north;  // the N row is the halo row (the thread's row is the tile's row 7)
+  bool south;  // the S row is the halo row (row 0)
+  int c0;      // first column of the thread's cells (offset in a halo row)
+};
+
+__device__ __forceinline__ StageRow stage_row(int sub, int q) {
+  const int cx = q & (ROWT - 1), ty = q / ROWT;
+  StageRow s;
+  s.t = sub;
+  s.r0 = sub * TILE + ty * TX + cx * CPT;
+  s.north = ty == TY - 1;
+  s.south = ty == 0;
+  s.c0 = cx * CPT;
+  return s;
+}
+
+template <int NB, int NHN, int NHS>
+__device__ __forceinline__ V4<float> st_body(const Stage<NB, NHN, NHS> &st, int i,
+                                             const StageRow &r) {
+  return ld4(&st.body[i][r.r0]);
+}
+// the row above (N) of the thread's cells in array i (i < NHN for the halo)
+template <int NB, int NHN, int NHS>
+__device__ __forceinline__ V4<float> st_north(const Stage<NB, NHN, NHS> &st, int i, int ih,
+                                              const StageRow &r) {
+  return r.north ? ld4(&st.hn[ih][r.t][r.c0]) : ld4(&st.body[i][r.r0 + TX]);
+}
+template <int NB, int NHN, int NHS>
+__device__ __forceinline__ V4<float> st_south(const Stage<NB, NHN, NHS> &st, int i, int ih,
+                                              const StageRow &r) {
+  return r.south ? ld4(&st.hs[ih][r.t][r.c0]) : ld4(&st.body[i][r.r0 - TX]);
+}
+
+constexpr int MBAR_TRIES = 1 << 16;  // bounded mbarrier waits (each try may suspend)
+
+// setup(m) returns the member's values (a struct with `bool skip` and the
+// source arrays: `const float *b[NB], *hn[NHN], *hs[NHS]`); pre(a, g) loads
+// the thread's E/W edge values from global memory before the stage is waited
+// for; body(a, st, row, g, valid, e, v) computes one quad row vector from
+// stage st and the edge values e.  On a wait that runs out, *err is set and
+// the CTA stops computing (the step then fails with a timeout status); the
+// copies it issued are waited for, again bounded, before it exits.
+template <int NS, int NB, int NHN, int NHS, class Setup, class Pre, class Body>
+__device__ __forceinline__ void quad_sweep_staged(const DevStatic &S, double *part, int *err,
+                                                  Setup setup, Pre pre, Body body) {
+  using A = decltype(setup(0));
+  using St = Stage<NB, NHN, NHS>;
+  extern __shared__ __align__(128) unsigned char dyn_smem[];
+  St *stg = reinterpret_cast<St *>(dyn_smem);
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ QuadLog<NS> L;
+  __shared__ A da[QB];
+  __shared__ int4 dq[QB];
+  __shared__ int4 dnb[QB][TILES_PER_CTA];
+  __shared__ int list[QB];
+  __shared__ int nlist;
+  const int sub = threadIdx.x / TPT, q = threadIdx.x % TPT;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int G = gridDim.x, NQ = S.nquad;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  uint32_t phase0 = 0, phase1 = 0;  // parity of the next phase to wait for, per stage
+  bool dead = false;                // a wait ran out
+  const StageRow row = stage_row(sub, q);
+  // thread 0: the copies of list entry j into stage j & 1
+  auto issue = [&](int j) {
+    const int k = list[j], s = j & 1;
+    const int4 cur = dq[k];
+    const A &a = da[k];
+    const uint32_t bb = uint32_t(cur.z) * TILE * sizeof(float);
+    mbar_arrive_expect(&bar[s], NB * bb + uint32_t(cur.z) * (NHN + NHS) * TX * sizeof(float));
+    const size_t off = size_t(cur.y) * TILE;
+#pragma unroll
+    for (int i = 0; i < NB; ++i) bulk_g2s(stg[s].body[i], a.b[i] + off, bb, &bar[s]);
+    for (int t = 0; t < cur.z; ++t) {
+      const int4 nb = dnb[k][t];
+#pragma unroll
+      for (int i = 0; i < NHN; ++i)
+        bulk_g2s(stg[s].hn[i][t], a.hn[i] + size_t(nb.w) * TILE, TX * sizeof(float), &bar[s]);
+#pragma unroll
+      for (int i = 0; i < NHS; ++i)
+        bulk_g2s(stg[s].hs[i][t], a.hs[i] + size_t(nb.z) * TILE + (TY - 1) * TX,
+                 TX * sizeof(float), &bar[s]);
+    }
+  };
+  int n = 0;
+  for (int b0 = blockIdx.x; b0 < NQ; b0 += G * QB) {
+    __syncthreads();  // the previous batch's descriptors are no longer read
+    if (threadIdx.x < QB * TILES_PER_CTA) {
+      const int k = threadIdx.x / TILES_PER_CTA, s = threadIdx.x % TILES_PER_CTA;
+      const int qd = b0 + k * G;
+      if (qd < NQ) {
+        const int4 cur = S.quads[qd];
+        if (s == 0) {
+          dq[k] = cur;
+          da[k] = setup(cur.x);
+        }
+        dnb[k][s] = __ldg(&S.tnbr[s < cur.z ? cur.y + s : 0]);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // the quads of the batch that run, in order
+      const int nk = min(QB, (NQ - b0 + G - 1) / G);
+      int c = 0;
+      for (int k = 0; k < nk; ++k)
+        if (!da[k].skip) list[c++] = k;
+      nlist = c;
+      if (!dead) {
+        if (c > 0) issue(0);
+        if (c > 1) issue(1);
+      }
+    }
+    __syncthreads();
+    const int nl = nlist;
+    for (int j = 0; j < nl; ++j) {
+      const int k = list[j], s = j & 1;
+      const A a = da[k];
+      const int4 cur = dq[k];
+      const bool valid = sub < cur.z;
+      const RowGeo g = row_geo_nb(dnb[k][sub], valid ? cur.y + sub : 0, q);
+      const auto e = pre(a, g);
+      if (!dead && !mbar_wait(&bar[s], s ? phase1 : phase0, MBAR_TRIES)) dead = true;
+      if (s)
+        phase1 ^= 1u;
+      else
+        phase0 ^= 1u;
+      double v[NS];
+#pragma unroll
+      for (int i = 0; i < NS; ++i) v[i] = 0.0;
+      if (!dead) body(a, stg[s], row, g, valid, e, v);
+#pragma unroll
+      for (int i = 0; i < NS; ++i) {
+        const double x = warp_sum(v[i]);
+        if (lane == 0) L.w[i][n][warp] = x;
+      }
+      if (threadIdx.x == 0) L.qd[n] = b0 + k * G;
+      __syncthreads();  // every thread is done with stage s: it may be refilled
+      if (threadIdx.x == 0 && !dead && j + 2 < nl) issue(j + 2);
+      if (++n == QCAP) {
+        quad_store<NS>(L, n, S, part);
+        n = 0;
+      }
+    }
+  }
+  if (n) quad_store<NS>(L, n, S, part);
+  // every phase issued has been waited for, unless a wait ran out: then the
+  // copies still in flight are waited for (bounded) before the CTA's shared
+  // memory goes
+  if (dead && threadIdx.x == 0) {
+    atomicExch(err, 1);
+    mbar_wait(&bar[0], phase0, MBAR_TRIES);
+    mbar_wait(&bar[1], phase1, MBAR_TRIES);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_inval(&bar[0]);
+    mbar_inval(&bar[1]);
+  }
+}
+
+// The quad sweep of a kernel variant: 0 prefetches one quad ahead in
+// registers, 1 loads the descriptors in batches (quad_sweep_batched).
+template <int NS, int VAR, class Setup, class Body>
+__device__ __forceinline__ void quad_sweep_v(const DevStatic &S, double *part, Setup setup,
+                                             Body body) {
+  if constexpr (VAR == 1)
+    quad_sweep_batched<NS>(S, part, setup, body);
+  else
+    quad_sweep<NS>(S, part, setup, body);
 }
 
 // The member-reduce kernels: member m (one CTA per member, grid-stride) sums

@@ -88,7 +88,7 @@ struct Glob {
   int ndone;     // members whose solve finished
   int nidone;    // members whose inner (FP32) solve finished
   int nicordry;  // members that need another wet/dry sweep
-  int pad;
+  int err;       // nonzero: a bounded device-side wait ran out (a timeout status)
   int loop[NLOOP];  // body executions of the loop now running (each loop's cap)
   int tot[NLOOP];   // body executions in the step (the launch count)
 };
@@ -186,6 +186,7 @@ struct DevSystem {
   float *z32;                                    // preconditioned residual z = M^-1 r
   float *r32b;                                   // second residual buffer (r32 / r32b by parity)
   const int *mpoly;                              // [M] 1: Neumann polynomial, 0: Jacobi (per solve)
+  int *err;                                      // Glob::err of the context
 };
 
 // The system a MIXED solve refines: a step's unscaled assembly (FP, CC, CS,

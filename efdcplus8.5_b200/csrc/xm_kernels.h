@@ -22,6 +22,11 @@ struct Launch {
   bool may_asym = true;  // some member's operator can be unsymmetric (else symmetric kernels)
   bool chan = false;     // sub-grid channel terms (a step of a context with channels)
   bool baro = false;     // some member of the step has the baroclinic terms (CALEBI)
+  // schedule (efdc_xm_set_schedule): the FP32 CG kernels' variant (0: quad
+  // descriptors prefetched one quad ahead, 1: in shared-memory batches) and,
+  // for variant 1, caps on their resident CTAs per SM (0: occupancy)
+  int variant = 0;
+  int ctas_mv = 0, ctas_up = 0;
 };
 
 // One array to move between host order and tile order (see k_scatter).

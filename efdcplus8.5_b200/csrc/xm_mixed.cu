@@ -12,6 +12,9 @@
 // The outer FP64 loop (xm_step.cu: k_mx_resid / k_mx_apply) keeps P in FP64
 // and stops on the reference's own criterion, the FP64 RSQ <= RSQM.
 
+#include <map>
+#include <mutex>
+
 #include "xm_cg.cuh"
 #include "xm_kernels.h"
 
@@ -22,8 +25,8 @@ namespace xm {
 
 // p = z + beta*p_old at the cell and its halo (z = r for Jacobi members),
 // Ahat*p, p.Ap (per member).
-template <bool MA>
-__global__ void __launch_bounds__(NT, 6) k_mx_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
+template <bool MA, int VAR>
+__global__ void __launch_bounds__(NT, VAR == 1 ? 5 : 6) k_mx_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
                                                     double *part) {
   struct A {
     bool skip, asym;
@@ -32,7 +35,7 @@ __global__ void __launch_bounds__(NT, 6) k_mx_matvec(DevStatic S, DevSystem Y, c
     float *pnew;
     const float *z;
   };
-  quad_sweep<1>(
+  quad_sweep_v<1, VAR>(
       S, part,
       [&](int m) {
         const Ctl &k = ctl[m];
@@ -60,7 +63,8 @@ __global__ void __launch_bounds__(NT) k_red_mx_matvec(DevStatic S, Ctl *ctl, con
 
 // x += alpha*p, r -= alpha*Ap, z = (2I - Ahat) r (the two-term Neumann
 // polynomial), r.z and r.r (FP64 sums): the members that use it.
-__global__ void __launch_bounds__(NT, 6) k_mx_update_poly(DevStatic S, DevSystem Y,
+template <int VAR>
+__global__ void __launch_bounds__(NT, VAR == 1 ? 5 : 6) k_mx_update_poly(DevStatic S, DevSystem Y,
                                                          const Ctl *ctl, double *part) {
   struct A {
     bool skip;
@@ -69,7 +73,7 @@ __global__ void __launch_bounds__(NT, 6) k_mx_update_poly(DevStatic S, DevSystem
     const float *r;
     float *rnew;
   };
-  quad_sweep<2>(
+  quad_sweep_v<2, VAR>(
       S, part,
       [&](int m) {
         const Ctl &k = ctl[m];
@@ -84,6 +88,7 @@ __global__ void __launch_bounds__(NT, 6) k_mx_update_poly(DevStatic S, DevSystem
       });
 }
 // The same for the Jacobi members (z = r): x, r and r.r only.
+template <int VAR>
 __global__ void __launch_bounds__(NT) k_mx_update_jac(DevStatic S, DevSystem Y, const Ctl *ctl,
                                                      double *part) {
   struct A {
@@ -93,7 +98,7 @@ __global__ void __launch_bounds__(NT) k_mx_update_jac(DevStatic S, DevSystem Y, 
     const float *r;
     float *rnew;
   };
-  quad_sweep<2>(
+  quad_sweep_v<2, VAR>(
       S, part,
       [&](int m) {
         const Ctl &k = ctl[m];
@@ -164,26 +169,328 @@ __global__ void __launch_bounds__(NT) k_red_mx_zinit(DevStatic S, DevSystem Y, C
       });
 }
 
+
+// ---------------------------------------------------------------------------
+// Variant 2: the same three kernels on the staged sweep (quad_sweep_staged):
+// the rows come from shared memory, filled by bulk copies one quad ahead.  The
+// arithmetic is the row functions' above, operand for operand, so the results
+// are those of variants 0 and 1 bit for bit.
+
+// E/W edge values of a thread's row vector (cx == 0: the west neighbour of
+// cell 0; cx == ROWT-1: the east neighbour of cell 3)
+struct Edge3 {
+  float w0, w1, e0, e1, e2;
+};
+
+using MvStage = Stage<4, 3, 2>;     // z, p_old, AS, AW; N rows z, p_old, AS; S rows z, p_old
+using PolyStage = Stage<6, 3, 2>;   // r, Ap, AS, AW, x, p; N rows r, Ap, AS; S rows r, Ap
+using JacStage = Stage<4, 0, 0>;    // x, p, r, Ap
+
+template <bool MA>
+__global__ void __launch_bounds__(NT, 4) k_mx_matvec_st(DevStatic S, DevSystem Y, const Ctl *ctl,
+                                                       double *part) {
+  struct A {
+    bool skip, asym;
+    float beta;
+    float *pnew;
+    const float *b[4], *hn[3], *hs[2];
+  };
+  quad_sweep_staged<1, 4, 3, 2>(
+      S, part, Y.err,
+      [&](int m) {
+        const Ctl &k = ctl[m];
+        const bool par = k.parity;
+        const bool asym = unsym<MA>(k);
+        const bool poly = Y.mpoly[m] && !asym;
+        const float *z = poly ? Y.z32 : (par ? Y.r32b : Y.r32);
+        const float *po = par ? Y.pb32 : Y.pa32;
+        return A{(k.done | k.idone) != 0, asym, float(k.beta), par ? Y.pa32 : Y.pb32,
+                 {z, po, Y.as32, Y.aw32}, {z, po, Y.as32}, {z, po}};
+      },
+      [&](const A &a, const RowGeo &g) {
+        Edge3 e{0.f, 0.f, 0.f, 0.f, 0.f};
+        if (g.cx == 0) {
+          e.w0 = a.b[0][g.dwe];
+          e.w1 = a.b[1][g.dwe];
+        }
+        if (g.cx == ROWT - 1) {
+          e.e0 = a.b[0][g.dee];
+          e.e1 = a.b[1][g.dee];
+          e.e2 = Y.aw32[g.dee];
+        }
+        return e;
+      },
+      [&](const A &a, const MvStage &st, const StageRow &row, const RowGeo &g, bool valid,
+          const Edge3 &e, double *v) {
+        const float beta = a.beta;
+        const V4<float> r0 = st_body(st, 0, row), o0 = st_body(st, 1, row);
+        const V4<float> rn = st_north(st, 0, 0, row), on = st_north(st, 1, 1, row);
+        const V4<float> rs = st_south(st, 0, 0, row), os = st_south(st, 1, 1, row);
+        const V4<float> p = {fmaf(beta, o0.x, r0.x), fmaf(beta, o0.y, r0.y),
+                             fmaf(beta, o0.z, r0.z), fmaf(beta, o0.w, r0.w)};
+        const V4<float> pn = {fmaf(beta, on.x, rn.x), fmaf(beta, on.y, rn.y),
+                              fmaf(beta, on.z, rn.z), fmaf(beta, on.w, rn.w)};
+        const V4<float> ps = {fmaf(beta, os.x, rs.x), fmaf(beta, os.y, rs.y),
+                              fmaf(beta, os.z, rs.z), fmaf(beta, os.w, rs.w)};
+        float pw = from_west(p), pe = from_east(p);
+        if (g.cx == 0) pw = fmaf(beta, e.w1, e.w0);
+        if (g.cx == ROWT - 1) pe = fmaf(beta, e.e1, e.e0);
+        const V4<float> ks = st_body(st, 2, row), kw = st_body(st, 3, row);
+        V4<float> kn, ke;
+        if (a.asym) {
+          kn = ld4(Y.an32 + g.d0);
+          ke = ld4(Y.ae32 + g.d0);
+        } else {
+          kn = st_north(st, 2, 2, row);
+          float kwe = from_east(kw);
+          if (g.cx == ROWT - 1) kwe = e.e2;
+          ke = {kw.y, kw.z, kw.w, kwe};
+        }
+        V4<float> ap;
+        ap.x = p.x + ks.x * ps.x + kn.x * pn.x + kw.x * pw + ke.x * p.y;
+        ap.y = p.y + ks.y * ps.y + kn.y * pn.y + kw.y * p.x + ke.y * p.z;
+        ap.z = p.z + ks.z * ps.z + kn.z * pn.z + kw.z * p.y + ke.z * p.w;
+        ap.w = p.w + ks.w * ps.w + kn.w * pn.w + kw.w * p.z + ke.w * pe;
+        if (!valid) return;
+        st4(a.pnew + g.d0, p);
+        st4(Y.ap32 + g.d0, ap);
+        v[0] = double(ap.x) * double(p.x) + double(ap.y) * double(p.y) +
+               double(ap.z) * double(p.z) + double(ap.w) * double(p.w);
+      });
+}
+
+__global__ void __launch_bounds__(NT, 3) k_mx_update_poly_st(DevStatic S, DevSystem Y,
+                                                            const Ctl *ctl, double *part) {
+  struct A {
+    bool skip;
+    float alpha;
+    float *rnew;
+    const float *b[6], *hn[3], *hs[2];
+  };
+  quad_sweep_staged<2, 6, 3, 2>(
+      S, part, Y.err,
+      [&](int m) {
+        const Ctl &k = ctl[m];
+        const bool par = k.parity;
+        const bool poly = Y.mpoly[m] && !unsym<true>(k);
+        const float *r = par ? Y.r32b : Y.r32;
+        return A{(k.done | k.idone) != 0 || !poly, float(k.alpha), par ? Y.r32 : Y.r32b,
+                 {r, Y.ap32, Y.as32, Y.aw32, Y.x32, par ? Y.pa32 : Y.pb32},
+                 {r, Y.ap32, Y.as32},
+                 {r, Y.ap32}};
+      },
+      [&](const A &a, const RowGeo &g) {
+        Edge3 e{0.f, 0.f, 0.f, 0.f, 0.f};
+        if (g.cx == 0) {
+          e.w0 = a.b[0][g.dwe];
+          e.w1 = Y.ap32[g.dwe];
+        }
+        if (g.cx == ROWT - 1) {
+          e.e0 = a.b[0][g.dee];
+          e.e1 = Y.ap32[g.dee];
+          e.e2 = Y.aw32[g.dee];
+        }
+        return e;
+      },
+      [&](const A &a, const PolyStage &st, const StageRow &row, const RowGeo &g, bool valid,
+          const Edge3 &e, double *v) {
+        const float alpha = a.alpha;
+        const V4<float> r0 = st_body(st, 0, row), a0 = st_body(st, 1, row);
+        const V4<float> rn0 = {fmaf(-alpha, a0.x, r0.x), fmaf(-alpha, a0.y, r0.y),
+                               fmaf(-alpha, a0.z, r0.z), fmaf(-alpha, a0.w, r0.w)};
+        const V4<float> rN = st_north(st, 0, 0, row), aN = st_north(st, 1, 1, row);
+        const V4<float> rS = st_south(st, 0, 0, row), aS = st_south(st, 1, 1, row);
+        const V4<float> nN = {fmaf(-alpha, aN.x, rN.x), fmaf(-alpha, aN.y, rN.y),
+                              fmaf(-alpha, aN.z, rN.z), fmaf(-alpha, aN.w, rN.w)};
+        const V4<float> nS = {fmaf(-alpha, aS.x, rS.x), fmaf(-alpha, aS.y, rS.y),
+                              fmaf(-alpha, aS.z, rS.z), fmaf(-alpha, aS.w, rS.w)};
+        float nw = from_west(rn0), ne = from_east(rn0);
+        if (g.cx == 0) nw = fmaf(-alpha, e.w1, e.w0);
+        if (g.cx == ROWT - 1) ne = fmaf(-alpha, e.e1, e.e0);
+        const V4<float> ks = st_body(st, 2, row), kw = st_body(st, 3, row);
+        const V4<float> kn = st_north(st, 2, 2, row);
+        float kwe = from_east(kw);
+        if (g.cx == ROWT - 1) kwe = e.e2;
+        const V4<float> ke = {kw.y, kw.z, kw.w, kwe};
+        V4<float> zv;
+        zv.x = rn0.x - (ks.x * nS.x + kn.x * nN.x + kw.x * nw + ke.x * rn0.y);
+        zv.y = rn0.y - (ks.y * nS.y + kn.y * nN.y + kw.y * rn0.x + ke.y * rn0.z);
+        zv.z = rn0.z - (ks.z * nS.z + kn.z * nN.z + kw.z * rn0.y + ke.z * rn0.w);
+        zv.w = rn0.w - (ks.w * nS.w + kn.w * nN.w + kw.w * rn0.z + ke.w * ne);
+        if (!valid) return;
+        V4<float> xv = st_body(st, 4, row);
+        const V4<float> pv = st_body(st, 5, row);
+        xv.x = fmaf(alpha, pv.x, xv.x);
+        xv.y = fmaf(alpha, pv.y, xv.y);
+        xv.z = fmaf(alpha, pv.z, xv.z);
+        xv.w = fmaf(alpha, pv.w, xv.w);
+        st4(Y.x32 + g.d0, xv);
+        st4(a.rnew + g.d0, rn0);
+        st4(Y.z32 + g.d0, zv);
+        v[0] = double(rn0.x) * double(zv.x) + double(rn0.y) * double(zv.y) +
+               double(rn0.z) * double(zv.z) + double(rn0.w) * double(zv.w);
+        v[1] = double(rn0.x) * double(rn0.x) + double(rn0.y) * double(rn0.y) +
+               double(rn0.z) * double(rn0.z) + double(rn0.w) * double(rn0.w);
+      });
+}
+
+__global__ void __launch_bounds__(NT, 4) k_mx_update_jac_st(DevStatic S, DevSystem Y,
+                                                           const Ctl *ctl, double *part) {
+  struct A {
+    bool skip;
+    float alpha;
+    float *rnew;
+    const float *b[4], *hn[1], *hs[1];
+  };
+  quad_sweep_staged<2, 4, 0, 0>(
+      S, part, Y.err,
+      [&](int m) {
+        const Ctl &k = ctl[m];
+        const bool par = k.parity;
+        const bool poly = Y.mpoly[m] && !unsym<true>(k);
+        return A{(k.done | k.idone) != 0 || poly, float(k.alpha), par ? Y.r32 : Y.r32b,
+                 {Y.x32, par ? Y.pa32 : Y.pb32, par ? Y.r32b : Y.r32, Y.ap32},
+                 {nullptr},
+                 {nullptr}};
+      },
+      [&](const A &, const RowGeo &) { return 0; },
+      [&](const A &a, const JacStage &st, const StageRow &row, const RowGeo &g, bool valid,
+          int, double *v) {
+        if (!valid) return;
+        const float alpha = a.alpha;
+        V4<float> xv = st_body(st, 0, row), rv = st_body(st, 2, row);
+        const V4<float> pv = st_body(st, 1, row), av = st_body(st, 3, row);
+        xv.x = fmaf(alpha, pv.x, xv.x);
+        xv.y = fmaf(alpha, pv.y, xv.y);
+        xv.z = fmaf(alpha, pv.z, xv.z);
+        xv.w = fmaf(alpha, pv.w, xv.w);
+        rv.x = fmaf(-alpha, av.x, rv.x);
+        rv.y = fmaf(-alpha, av.y, rv.y);
+        rv.z = fmaf(-alpha, av.z, rv.z);
+        rv.w = fmaf(-alpha, av.w, rv.w);
+        st4(Y.x32 + g.d0, xv);
+        st4(a.rnew + g.d0, rv);
+        const double rr = double(rv.x) * double(rv.x) + double(rv.y) * double(rv.y) +
+                          double(rv.z) * double(rv.z) + double(rv.w) * double(rv.w);
+        v[0] = rr;
+        v[1] = rr;
+      });
+}
+
+// Dynamic shared memory of a staged kernel (two stages), allowed once.
+template <class K>
+static size_t staged_smem(K kernel, size_t stage_bytes) {
+  static std::mutex mu;
+  static std::map<const void *, bool> done;
+  const size_t bytes = 2 * stage_bytes;
+  std::lock_guard<std::mutex> lock(mu);
+  const void *k = reinterpret_cast<const void *>(kernel);
+  if (!done[k]) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    done[k] = true;
+  }
+  return bytes;
+}
+template <class K>
+static int staged_grid(const Launch &l, const DevStatic &S, K kernel, size_t smem, int cap) {
+  static std::mutex mu;
+  static std::map<const void *, int> cache;
+  int b = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    const void *k = reinterpret_cast<const void *>(kernel);
+    const auto it = cache.find(k);
+    if (it != cache.end()) {
+      b = it->second;
+    } else {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, NT, smem);
+      b = b > 0 ? b : 1;
+      cache[k] = b;
+    }
+  }
+  if (cap > 0) b = std::min(b, cap);
+  return std::max(1, std::min(S.nquad, l.nsm * b));
+}
+
 static int reduce_grid(const DevStatic &S) { return std::min(S.nmember, 1024); }
+
+// Resident CTAs per SM of a kernel (cached per kernel), for the grids of the
+// kernel variants.
+static int per_sm(const void *kernel) {
+  static std::mutex mu;
+  static std::map<const void *, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto it = cache.find(kernel);
+  if (it != cache.end()) return it->second;
+  int a = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, kernel, NT, 0);
+  a = a > 0 ? a : 1;
+  cache[kernel] = a;
+  return a;
+}
+// The grid of a quad kernel: its resident CTAs per SM (at most `cap` when
+// cap > 0) times the SMs, at most one CTA per quad.
+template <class K>
+static int grid_of(const Launch &l, const DevStatic &S, K kernel, int cap) {
+  int b = per_sm(reinterpret_cast<const void *>(kernel));
+  if (cap > 0) b = std::min(b, cap);
+  return std::max(1, std::min(S.nquad, l.nsm * b));
+}
 
 void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {
-  if (l.may_asym)
-    k_mx_matvec<true><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
-  else
-    k_mx_matvec<false><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
+  if (l.variant == 2) {
+    if (l.may_asym) {
+      const size_t sm = staged_smem(k_mx_matvec_st<true>, sizeof(MvStage));
+      k_mx_matvec_st<true><<<staged_grid(l, S, k_mx_matvec_st<true>, sm, l.ctas_mv), NT, sm,
+                             l.stream>>>(S, Y, ctl, part);
+    } else {
+      const size_t sm = staged_smem(k_mx_matvec_st<false>, sizeof(MvStage));
+      k_mx_matvec_st<false><<<staged_grid(l, S, k_mx_matvec_st<false>, sm, l.ctas_mv), NT, sm,
+                              l.stream>>>(S, Y, ctl, part);
+    }
+  } else if (l.variant == 1) {
+    if (l.may_asym)
+      k_mx_matvec<true, 1><<<grid_of(l, S, k_mx_matvec<true, 1>, l.ctas_mv), NT, 0, l.stream>>>(
+          S, Y, ctl, part);
+    else
+      k_mx_matvec<false, 1><<<grid_of(l, S, k_mx_matvec<false, 1>, l.ctas_mv), NT, 0,
+                              l.stream>>>(S, Y, ctl, part);
+  } else if (l.may_asym) {
+    k_mx_matvec<true, 0><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
+  } else {
+    k_mx_matvec<false, 0><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
+  }
   launch_chan_mvmx(l, S, Y, ctl, part);
   k_red_mx_matvec<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part);
   count_launches(2);
 }
 void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       Glob *glob, double *part, int no_stop) {
-  if (l.mx_jac) {
-    k_mx_update_jac<<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part);
+  if (l.mx_jac && l.variant == 2) {
+    const size_t sm = staged_smem(k_mx_update_jac_st, sizeof(JacStage));
+    k_mx_update_jac_st<<<staged_grid(l, S, k_mx_update_jac_st, sm, l.ctas_up), NT, sm,
+                         l.stream>>>(S, Y, ctl, part);
+    count_launches(1);
+  } else if (l.mx_jac) {
+    if (l.variant == 1)
+      k_mx_update_jac<1><<<grid_of(l, S, k_mx_update_jac<1>, l.ctas_up), NT, 0, l.stream>>>(
+          S, Y, ctl, part);
+    else
+      k_mx_update_jac<0><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part);
     count_launches(1);
   }
-  if (l.mx_poly) {
-    k_mx_update_poly<<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part);
+  if (l.mx_poly && l.variant == 2) {
+    const size_t sm = staged_smem(k_mx_update_poly_st, sizeof(PolyStage));
+    k_mx_update_poly_st<<<staged_grid(l, S, k_mx_update_poly_st, sm, l.ctas_up), NT, sm,
+                          l.stream>>>(S, Y, ctl, part);
+    count_launches(1);
+  } else if (l.mx_poly) {
+    if (l.variant == 1)
+      k_mx_update_poly<1><<<grid_of(l, S, k_mx_update_poly<1>, l.ctas_up), NT, 0, l.stream>>>(
+          S, Y, ctl, part);
+    else
+      k_mx_update_poly<0><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part);
     count_launches(1);
   }
   k_red_mx_update<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, 2.0, no_stop);
@@ -204,13 +511,13 @@ void launch_mx_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl
 
 int occupancy_blocks_per_sm_mixed_update() {
   int b = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_mx_update_poly, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_mx_update_poly<0>, NT, 0);
   return b > 0 ? b : 1;
 }
 
 int occupancy_blocks_per_sm_mixed() {
   int a = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_mx_matvec<true>, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_mx_matvec<true, 0>, NT, 0);
   return a > 0 ? a : 1;
 }
 

@@ -336,6 +336,9 @@ def make_fields(st: dict, *, diag: bool = False, lists: bool = False, unchanged:
 
 OPT_DEVICE_LOOPS = 1
 OPT_GRAPH_ITERS = 2
+OPT_KERNEL_VARIANT = 3
+OPT_CTAS_MATVEC = 4
+OPT_CTAS_UPDATE = 5
 
 
 def host_waits() -> int:

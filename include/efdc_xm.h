@@ -425,8 +425,23 @@ int64_t efdc_xm_host_waits(void);
  *     the host, polling the device between groups of iterations.  Both run
  *     the same kernels in the same order.
  *   EFDC_XM_OPT_GRAPH_ITERS (default 4, 1..32): CG iterations per loop body.
+ *   EFDC_XM_OPT_KERNEL_VARIANT (default 0): the MIXED inner iteration's
+ *     kernels; 0 fetches each 4-tile unit's descriptors (its member's values,
+ *     its tiles' neighbours) one unit ahead, 1 fetches them for 32 units at a
+ *     time into shared memory, 2 does that and also stages each unit's rows
+ *     in shared memory with bulk copies issued one unit ahead.  All give the
+ *     same results bit for bit.
+ *   EFDC_XM_OPT_CTAS_MATVEC, EFDC_XM_OPT_CTAS_UPDATE (default 0, 0..32): with
+ *     variants 1 and 2, caps on the resident CTAs per SM of the inner
+ *     iteration's matrix-vector and update kernels (0: as many as fit).
  * Returns EFDC_XM_BAD_ARGUMENT for an unknown option or value. */
-enum { EFDC_XM_OPT_DEVICE_LOOPS = 1, EFDC_XM_OPT_GRAPH_ITERS = 2 };
+enum {
+  EFDC_XM_OPT_DEVICE_LOOPS = 1,
+  EFDC_XM_OPT_GRAPH_ITERS = 2,
+  EFDC_XM_OPT_KERNEL_VARIANT = 3,
+  EFDC_XM_OPT_CTAS_MATVEC = 4,
+  EFDC_XM_OPT_CTAS_UPDATE = 5
+};
 int32_t efdc_xm_set_option(efdc_xm_ctx *ctx, int32_t option, int32_t value);
 
 /* Bytes copied host->device (*h2d) and device->host (*d2h) by the upload,
