@@ -85,6 +85,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="CPU baseline: seconds per thread setting (two settings)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="MIXED inner-iteration kernel variant (EFDC_XM_OPT_KERNEL_VARIANT); "
+                         "-1: the schedule efdc_xm_autotune measures for the workload")
     ap.add_argument("--ref-seconds", type=float, default=240.0,
                     help="--impl reference: stop the timed steps after this many seconds")
     return ap.parse_args()
@@ -471,6 +474,8 @@ def ours(args):
     cells = np.array([s.ncell for s in scns], dtype=np.int64)
     M = len(scns)
     bs = X.BatchSolver([s.grid for s in scns], device=local)
+    if args.variant >= 0:
+        bs.set_option(X.OPT_KERNEL_VARIANT, args.variant)
     stream = torch.cuda.ExternalStream(bs.stream(), device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if M == 1 else None
 
@@ -520,6 +525,18 @@ def ours(args):
                     launches=launches, waits=waits, p=[o["p"] for o in out])
 
     r64 = run_batch(X.PREC_FP64, args.steps, args.warmup)
+    # the MIXED schedule for this workload: measured by efdc_xm_autotune on the
+    # system of a first MIXED step (the table is this run's own, not reused)
+    tune = None
+    if args.variant < 0:
+        bs.upload([s.state for s in scns])
+        bs.step_device(params(1, X.PREC_MIXED))
+        t0 = time.perf_counter()
+        with tempfile.TemporaryDirectory() as td:
+            sch, sms = bs.autotune(X.PREC_MIXED, Path(td) / "schedules.txt", measure=True)
+        tune = {"schedule": sch, "solve_ms": sms, "seconds": time.perf_counter() - t0,
+                "key": bs.tune_key(X.PREC_MIXED), "how": "efdc_xm_autotune (coordinate descent "
+                "over the options, each candidate the median of 3 timed solves)"}
     rmx = run_batch(X.PREC_MIXED, args.steps, args.warmup)
 
     # elevation error of the MIXED solver against the FP64 solve of the same
@@ -562,7 +579,18 @@ def ours(args):
     fp64_batched = credit_all / t_64
     eta_err = max(float(np.abs(a[1:s.la] - b[1:s.la]).max()) for a, b, s in
                   zip(rmx["p"], r64["p"], scns)) / S.G
-    # dominant kernel, live: on the last (mixed) system of every member
+    # dominant kernel, live: on the last (mixed) system of every member, with
+    # the variant the timed run used, and every variant for comparison
+    variants = {}
+    run_variant = tune["schedule"]["kernel_variant"] if tune else args.variant
+    for v in (0, 1, 2):
+        bs.set_option(X.OPT_KERNEL_VARIANT, v)
+        kv = bs.time_kernels(X.PREC_MIXED, reps=20)
+        variants[v] = {"ms_matvec": kv.ms_matvec, "ms_update": kv.ms_update,
+                       "frac_matvec": 24.0 * kv.ncells / (kv.ms_matvec * 1e-3) / 1e9 / peak,
+                       "frac_update": (24.0 * kv.ncells + 12.0 * kv.ncells_poly) /
+                                      (kv.ms_update * 1e-3) / 1e9 / peak}
+    bs.set_option(X.OPT_KERNEL_VARIANT, run_variant)
     kt = bs.time_kernels(X.PREC_MIXED, reps=20)
     kt64 = bs.time_kernels(X.PREC_FP64, reps=20)
 
@@ -689,6 +717,8 @@ def ours(args):
     roof["dominant_by"] = ("the larger device time per inner iteration of the two kernels "
                            "that launch once per iteration")
     roof["second_kernel"] = second
+    roof["variant"] = run_variant
+    roof["variants_measured"] = variants
     roof["fp64_matvec"] = {"ms_per_launch": kt64.ms_matvec, "bytes_per_launch": 56.0 * kt.ncells,
                            "achieved": 56.0 * kt.ncells / (kt64.ms_matvec * 1e-3) / 1e9,
                            "frac": 56.0 * kt.ncells / (kt64.ms_matvec * 1e-3) / 1e9 / peak}
@@ -854,6 +884,7 @@ def ours(args):
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(rmx["launches"]), "clocks": clocks,
             "host_waits_per_step": rmx["waits"] / args.steps,
+            "schedule": tune,
             "single_domain": single,
             "three_level": tl3_res,
             "wetdry": wd_res,

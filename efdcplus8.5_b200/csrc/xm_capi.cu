@@ -183,6 +183,7 @@ struct efdc_xm_ctx {
   // device-driven steps: the whole step as one graph whose loops are
   // conditional WHILE nodes (StepGraph), cached by what the graph holds
   bool device_loops = true;     // efdc_xm_set_option(EFDC_XM_OPT_DEVICE_LOOPS)
+  bool stepped = false;         // a step of every member has assembled the systems
   int graph_iters = GRAPH_ITERS;  // CG iterations per loop body
   std::vector<StepGraph> step_graphs;
   std::vector<std::vector<char>> step_graph_failed;
@@ -245,6 +246,8 @@ struct efdc_xm_ctx {
   }
   // schedule of the FP32 CG kernels (efdc_xm_set_option: variant and CTA caps)
   int kvariant = 0, ctas_mv = 0, ctas_up = 0;
+  int inner_margin_log10 = 0;   // MIXED inner target margin 10^-v
+  float poly_threshold = 10.f;  // MIXED: polynomial preconditioner above this Jacobi count
   xm::Launch L() const {
     xm::Launch l{grid,      grid_cg, grid_cg32, grid_up32,
                  ntile,     nsm,     stream,
@@ -253,6 +256,7 @@ struct efdc_xm_ctx {
     l.variant = kvariant;
     l.ctas_mv = ctas_mv;
     l.ctas_up = ctas_up;
+    l.inner_margin = std::pow(10.0, -double(inner_margin_log10));
     return l;
   }
 };
@@ -587,7 +591,8 @@ int choose_inner(efdc_xm_ctx *c) {
   c->mx_jac = c->mx_poly = false;
   for (int m = 0; m < c->M; ++m) {
     // a member with sub-grid channels keeps Jacobi (the couplings enter A*p only)
-    c->mpoly_h[m] = (c->mem[m].jac_est > 10.f && !(l.chan && !c->chans[m].empty())) ? 1 : 0;
+    c->mpoly_h[m] =
+        (c->mem[m].jac_est > c->poly_threshold && !(l.chan && !c->chans[m].empty())) ? 1 : 0;
     if (!c->act_h[m]) continue;
     if (!c->mpoly_h[m]) {
       c->mx_jac = true;
@@ -1627,7 +1632,7 @@ struct StepPlan {
   int max_iterm, max_sweeps, grid, grid_cg, grid_cg32, grid_up32;
   int mx_jac, mx_poly, may_asym, chan, baro, obc_serial, any_may_asym, nmember;
   int variant, ctas_mv, ctas_up, pad;
-  double fac;
+  double fac, inner_margin;
   const void *psol;
 };
 
@@ -1953,6 +1958,191 @@ int run_step_graph(efdc_xm_ctx *c, const StepPlan &pl, const xm::DevState &x_pre
   return overall_status(stats + m0, m1 - m0);
 }
 
+}  // namespace
+extern "C" {
+namespace {
+void drop_graphs(efdc_xm_ctx *c);  // (below, where it is defined with C linkage)
+}  // namespace
+}  // extern "C"
+namespace {
+
+// ---------------------------------------------------------------------------
+// Schedule autotuner (efdc_xm_autotune).  The reference's only schedule rule
+// is its thread count, NOPTIMAL = MIN(NTHREADS, 8, MAX(LA/100, 1))
+// (calpuv2c.f90:61-62); here the knobs are the MIXED inner iteration's kernel
+// variant and CTA caps, the CG iterations per loop body, the Jacobi /
+// polynomial threshold and the inner target margin.  The tuner times the
+// context's own solve -- the solve part of a device-driven step, captured as
+// a graph of the same kernels -- on the system the last step assembled, from
+// the P it left (restored before every run), and walks the knobs one at a
+// time (coordinate descent, each knob's candidates in a fixed order, the
+// first of equal times kept), so the same measurements give the same choice.
+
+void schedule_of(const efdc_xm_ctx *c, efdc_xm_schedule *s) {
+  s->kernel_variant = c->kvariant;
+  s->ctas_matvec = c->ctas_mv;
+  s->ctas_update = c->ctas_up;
+  s->graph_iters = c->graph_iters;
+  s->poly_threshold = int32_t(c->poly_threshold);
+  s->inner_margin = c->inner_margin_log10;
+}
+
+void apply_schedule(efdc_xm_ctx *c, const efdc_xm_schedule &s) {
+  if (s.kernel_variant != c->kvariant || s.ctas_matvec != c->ctas_mv ||
+      s.ctas_update != c->ctas_up || s.inner_margin != c->inner_margin_log10 ||
+      s.graph_iters != c->graph_iters)
+    drop_graphs(c);
+  c->kvariant = s.kernel_variant;
+  c->ctas_mv = s.ctas_matvec;
+  c->ctas_up = s.ctas_update;
+  c->graph_iters = s.graph_iters;
+  c->poly_threshold = float(s.poly_threshold);
+  c->inner_margin_log10 = s.inner_margin;
+}
+
+bool schedule_valid(const efdc_xm_schedule &s) {
+  return s.kernel_variant >= 0 && s.kernel_variant <= 2 && s.ctas_matvec >= 0 &&
+         s.ctas_matvec <= 32 && s.ctas_update >= 0 && s.ctas_update <= 32 &&
+         s.graph_iters >= 1 && s.graph_iters <= 32 && s.poly_threshold >= 0 &&
+         s.poly_threshold <= 100000 && s.inner_margin >= 0 && s.inner_margin <= 6;
+}
+
+// The workload key of a table line: the precision, the buckets (floor log2)
+// of the member count and of the water cells, and the operator's form.
+std::string tune_key(const efdc_xm_ctx *c, int precision) {
+  long long cells = 0;
+  for (const Member &mb : c->mem) cells += mb.la - 1;
+  auto lg = [](long long v) {
+    int b = 0;
+    while (v > 1) {
+      v >>= 1;
+      ++b;
+    }
+    return b;
+  };
+  char buf[160];
+  snprintf(buf, sizeof(buf), "prec=%s members=2^%d cells=2^%d asym=%d chan=%d",
+           precision == EFDC_XM_PREC_MIXED ? "mixed" : "fp64", lg(c->M), lg(cells),
+           c->any_may_asym ? 1 : 0, c->S.ch.n > 0 ? 1 : 0);
+  return buf;
+}
+
+// "key | variant=.. ctas_mv=.. ctas_up=.. iters=.. poly=.. margin=.. | ms=.."
+std::string table_line(const std::string &key, const efdc_xm_schedule &s, double ms) {
+  char buf[400];
+  snprintf(buf, sizeof(buf),
+           "%s | variant=%d ctas_mv=%d ctas_up=%d iters=%d poly=%d margin=%d | ms=%.4f",
+           key.c_str(), s.kernel_variant, s.ctas_matvec, s.ctas_update, s.graph_iters,
+           s.poly_threshold, s.inner_margin, ms);
+  return buf;
+}
+
+// The schedule of the last line of the table whose key is `key`.
+bool table_lookup(const char *path, const std::string &key, efdc_xm_schedule *out) {
+  FILE *f = path ? fopen(path, "r") : nullptr;
+  if (!f) return false;
+  char line[1024];
+  bool found = false;
+  while (fgets(line, sizeof(line), f)) {
+    std::string l(line);
+    const size_t bar = l.find(" | ");
+    if (bar == std::string::npos || l.compare(0, bar, key) != 0 || bar != key.size()) continue;
+    efdc_xm_schedule s{};
+    if (sscanf(l.c_str() + bar + 3, "variant=%d ctas_mv=%d ctas_up=%d iters=%d poly=%d margin=%d",
+               &s.kernel_variant, &s.ctas_matvec, &s.ctas_update, &s.graph_iters,
+               &s.poly_threshold, &s.inner_margin) == 6 &&
+        schedule_valid(s)) {
+      *out = s;
+      found = true;
+    }
+  }
+  fclose(f);
+  return found;
+}
+
+// The solve of every member as a graph (the solve part of a step's graph).
+cudaError_t capture_solve_graph(efdc_xm_ctx *c, const StepPlan &pl, cudaGraphExec_t *exec) {
+  for (cudaStream_t &s : c->cap_stream)
+    if (!s) {
+      const cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+      if (e != cudaSuccess) return e;
+    }
+  StepGraph sg;
+  long long mark = g_launches.load();
+  const long long start = mark;
+  long long mine = 0;
+  cudaError_t err = cudaStreamBeginCapture(c->cap_stream[0], cudaStreamCaptureModeThreadLocal);
+  if (err != cudaSuccess) return err;
+  err = capture_solve(c, pl, 0, sg, &mark, &mine);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e_end = cudaStreamEndCapture(c->cap_stream[0], &g);
+  g_launches.fetch_sub(g_launches.load() - start);
+  if (err == cudaSuccess) err = e_end;
+  if (err == cudaSuccess && !g) err = cudaErrorStreamCaptureInvalidated;
+  if (err == cudaSuccess) err = cudaGraphInstantiate(exec, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (err != cudaSuccess) {
+    for (cudaStream_t s : c->cap_stream) {
+      cudaStreamCaptureStatus cs;
+      if (s && cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+        cudaGraph_t t = nullptr;
+        cudaStreamEndCapture(s, &t);
+        if (t) cudaGraphDestroy(t);
+      }
+    }
+    cudaGetLastError();
+    *exec = nullptr;
+  }
+  return err;
+}
+
+// Median device time of `reps` solves of every member under the context's
+// current schedule, each from the saved P (*ms < 0: the schedule failed).
+int tune_time(efdc_xm_ctx *c, bool mixed, double fac, int reps, double *ms) {
+  *ms = -1.0;
+  for (int m = 0; m < c->M; ++m) c->act_h[m] = 1;
+  int rc = write_act(c);
+  if (rc) return rc;
+  if (mixed && (rc = choose_inner(c))) return rc;
+  const xm::Launch lk = c->L();
+  StepPlan pl{};
+  pl.mixed = mixed;
+  pl.iters = c->graph_iters;
+  pl.max_iterm = 1;
+  for (int m = 0; m < c->M; ++m) pl.max_iterm = std::max(pl.max_iterm, c->sc_h[m].iterm);
+  pl.fac = fac;
+  pl.inner_margin = lk.inner_margin;
+  pl.nmember = c->M;
+  cudaGraphExec_t ex = nullptr;
+  if (capture_solve_graph(c, pl, &ex) != cudaSuccess || !ex) return EFDC_XM_OK;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const size_t pb = size_t(c->nslot) * sizeof(double);
+  std::vector<double> t;
+  for (int r = 0; r <= reps; ++r) {  // run 0 warms up
+    CK(cudaMemcpyAsync(c->X.p, c->ptmp, pb, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaEventRecord(e0, c->stream));
+    CK(cudaGraphLaunch(ex, c->stream));
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    float f = 0.f;
+    CK(cudaEventElapsedTime(&f, e0, e1));
+    if (r > 0) t.push_back(f);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGraphExecDestroy(ex);
+  if ((rc = read_glob(c))) return rc;
+  if (c->glob_h->err) {  // a bounded wait ran out: this schedule is not usable here
+    CK(cudaMemsetAsync(&c->glob->err, 0, sizeof(int), c->stream));
+    return EFDC_XM_OK;
+  }
+  std::sort(t.begin(), t.end());
+  *ms = t[t.size() / 2];
+  return EFDC_XM_OK;
+}
+
 // The argument checks of a device-resident step of every member (the stats
 // are filled with the status on failure).
 int validate_step(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats) {
@@ -2108,6 +2298,7 @@ int step_range(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats, 
     pl.obc_serial = c->obc_serial;
     pl.any_may_asym = c->any_may_asym;
     pl.variant = lk.variant;
+    pl.inner_margin = lk.inner_margin;
     pl.ctas_mv = lk.ctas_mv;
     pl.ctas_up = lk.ctas_up;
     pl.nmember = M;
@@ -2116,6 +2307,7 @@ int step_range(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats, 
     rc = run_step_graph(c, pl, x_pre, prm, stats, m0, m1);
     if (rc >= 0) {
       if (istl == 0) c->tl3_ready = false;  // CALPUV2C does not keep the three levels
+      c->stepped |= m0 == 0 && m1 == M;
       return rc;
     }
     // no graph with conditional nodes here: the host-driven step below
@@ -2219,6 +2411,7 @@ int step_range(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats, 
   }
   if ((rc = read_ctl(c))) return rc;
   if (istl == 0) c->tl3_ready = false;  // CALPUV2C does not keep the three levels
+  c->stepped |= m0 == 0 && m1 == M;
   for (int m = m0; m < m1; ++m) {
     efdc_xm_stats &s = stats[m];
     const Ctl &k = c->ctl_h[m];
@@ -2401,6 +2594,7 @@ int step_batch_chunks(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields 
   // the kept copies, those that went up and were not written by the steps,
   // and those that came back
   c->synced = (sent_before_step & ~(skip_wetdry ? STEP_WRITES_DRYFREE : STEP_WRITES)) | got;
+  c->stepped = true;  // the chunks together stepped every member
   return overall_status(stats, M);
 }
 
@@ -2992,6 +3186,107 @@ int64_t efdc_xm_kernel_launches(void) { return g_launches.load(); }
 
 int64_t efdc_xm_host_waits(void) { return g_waits.load(); }
 
+int32_t efdc_xm_tune_key(const efdc_xm_ctx *c, int32_t precision, char *buf, int32_t len) {
+  if (!c || !buf || len < 1) {
+    set_error("efdc_xm_tune_key: NULL argument");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  snprintf(buf, size_t(len), "%s", tune_key(c, precision).c_str());
+  return EFDC_XM_OK;
+}
+
+int32_t efdc_xm_tune_lookup(const char *table, const char *key, efdc_xm_schedule *out) {
+  if (!table || !key || !out) {
+    set_error("efdc_xm_tune_lookup: NULL argument");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  if (!table_lookup(table, key, out)) {
+    set_error("efdc_xm_tune_lookup: no line for this key in %s", table);
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  return EFDC_XM_OK;
+}
+
+int32_t efdc_xm_autotune(efdc_xm_ctx *c, int32_t precision, const char *table, int32_t flags,
+                         efdc_xm_schedule *chosen, double *solve_ms) {
+  if (!c || (precision != EFDC_XM_PREC_FP64 && precision != EFDC_XM_PREC_MIXED)) {
+    set_error("efdc_xm_autotune: need a context and FP64 or MIXED");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  CK(cudaSetDevice(c->device));
+  const std::string key = tune_key(c, precision);
+  efdc_xm_schedule best{};
+  if (solve_ms) *solve_ms = 0.0;
+  if (!(flags & EFDC_XM_TUNE_MEASURE) && table && table_lookup(table, key, &best)) {
+    apply_schedule(c, best);  // replayed: no measurement
+    if (chosen) *chosen = best;
+    return EFDC_XM_OK;
+  }
+  if (!c->stepped) {
+    set_error("efdc_xm_autotune: step every member once first (the tuner times the solve of "
+              "the system the last step assembled)");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  const bool mixed = precision == EFDC_XM_PREC_MIXED;
+  if (mixed != c->last_mixed) {
+    set_error("efdc_xm_autotune: the last step's precision differs from the one to tune");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  c->sys_external = false;
+  c->mxview = xm::SysView{c->X.fp, c->X.cc, c->X.cs, c->X.cw, c->X.ce, c->X.cn, 1};
+  CK(cudaMemcpyAsync(c->ptmp, c->X.p, size_t(c->nslot) * sizeof(double),
+                     cudaMemcpyDeviceToDevice, c->stream));
+  schedule_of(c, &best);
+  double best_ms = 0.0;
+  int rc = tune_time(c, mixed, 0.1, 3, &best_ms);
+  if (rc) return rc;
+  // coordinate descent: each knob's candidates in order, the others held
+  auto knob = [&](int32_t efdc_xm_schedule::*f, std::initializer_list<int> vals) -> int {
+    for (int v : vals) {
+      efdc_xm_schedule s = best;
+      s.*f = v;
+      if (s.*f == best.*f) continue;
+      apply_schedule(c, s);
+      double ms = 0.0;
+      const int r = tune_time(c, mixed, 0.1, 3, &ms);
+      if (r) return r;
+      if (ms > 0 && (best_ms <= 0 || ms < best_ms)) {
+        best = s;
+        best_ms = ms;
+      }
+    }
+    apply_schedule(c, best);
+    return EFDC_XM_OK;
+  };
+  if (mixed) {
+    if ((rc = knob(&efdc_xm_schedule::kernel_variant, {0, 1, 2}))) return rc;
+    if (best.kernel_variant > 0) {
+      if ((rc = knob(&efdc_xm_schedule::ctas_matvec, {0, 2, 3, 4}))) return rc;
+      if ((rc = knob(&efdc_xm_schedule::ctas_update, {0, 2, 3, 4}))) return rc;
+    }
+    if ((rc = knob(&efdc_xm_schedule::poly_threshold, {0, 10, 40, 100000}))) return rc;
+    if ((rc = knob(&efdc_xm_schedule::inner_margin, {0, 1, 2}))) return rc;
+  }
+  if ((rc = knob(&efdc_xm_schedule::graph_iters, {2, 4, 8}))) return rc;
+  // P as the last step left it
+  CK(cudaMemcpyAsync(c->X.p, c->ptmp, size_t(c->nslot) * sizeof(double),
+                     cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  apply_schedule(c, best);
+  if (chosen) *chosen = best;
+  if (solve_ms) *solve_ms = best_ms;
+  if (table) {
+    FILE *f = fopen(table, "a");
+    if (!f) {
+      set_error("efdc_xm_autotune: cannot append to %s", table);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+    fprintf(f, "%s\n", table_line(key, best, best_ms).c_str());
+    fclose(f);
+  }
+  return EFDC_XM_OK;
+}
+
 int32_t efdc_xm_set_option(efdc_xm_ctx *c, int32_t option, int32_t value) {
   if (!c) {
     set_error("efdc_xm_set_option: NULL context");
@@ -3006,6 +3301,17 @@ int32_t efdc_xm_set_option(efdc_xm_ctx *c, int32_t option, int32_t value) {
       if (value != c->graph_iters) {
         c->graph_iters = value;
         drop_step_graphs(c);
+      }
+      return EFDC_XM_OK;
+    case EFDC_XM_OPT_POLY_THRESHOLD:
+      if (value < 0 || value > 100000) break;
+      c->poly_threshold = float(value);
+      return EFDC_XM_OK;
+    case EFDC_XM_OPT_INNER_MARGIN:
+      if (value < 0 || value > 6) break;
+      if (value != c->inner_margin_log10) {
+        c->inner_margin_log10 = value;
+        drop_graphs(c);
       }
       return EFDC_XM_OK;
     case EFDC_XM_OPT_KERNEL_VARIANT:

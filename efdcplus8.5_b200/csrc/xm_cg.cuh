@@ -194,78 +194,66 @@ __device__ __forceinline__ void quad_sweep_batched(const DevStatic &S, double *p
 }
 
 // ---------------------------------------------------------------------------
-// Staged quad sweep (FP32 kernels, variant 2).  A quad's rows move into shared
-// memory by 1-D bulk copies that complete on an mbarrier, in a ring of two
-// stages: while the CTA computes one quad from one stage, the next quad's
-// copies are in flight into the other.  A stage holds, for the quad's (up to
-// 4) tiles, the whole tiles of NB arrays ("body": 1 KB per tile and array,
-// contiguous because a quad's tiles are), the row 0 of each tile's north
-// neighbour of NHN arrays and the row 7 of each tile's south neighbour of NHS
-// arrays (the N/S halo rows of the tile's edge rows).  The E/W edge columns
-// stay plain loads of the row body (L2 hits: the neighbour tiles are in
-// flight or just done in the same window of quads).  Only this GPU's memory
-// is read, each CTA for itself: no multicast.
-template <int NB, int NHN, int NHS>
+// Staged quad sweep (FP32 kernels, variant 2).  A quad's tiles of NB arrays
+// (1 KB per tile and array, contiguous because a quad's tiles are) move into
+// shared memory by 1-D bulk copies that complete on an mbarrier, in a ring of
+// NSTG stages: while the CTA computes one quad, the copies of the next
+// NSTG - 1 quads are in flight.  The rows outside the quad's tiles -- the N/S
+// halo rows of a tile's edge rows and the E/W edge columns -- are plain loads
+// issued before the wait (L2 hits: the neighbour tiles are in flight or just
+// done in the same window of quads).  Only this GPU's memory is read, each
+// CTA for itself: no multicast.
+template <int NB>
 struct Stage {
   float body[NB][TILES_PER_CTA * TILE];
-  float hn[NHN > 0 ? NHN : 1][TILES_PER_CTA][TX];
-  float hs[NHS > 0 ? NHS : 1][TILES_PER_CTA][TX];
 };
 
-// Where a thread's cells and their N/S rows are in a stage.
+// Where a thread's cells are in a stage, and whether its N/S rows are outside
+// the tile (row 7: the N row is the north tile's row 0; row 0: the S row is
+// the south tile's row 7).
 struct StageRow {
-  int t;       // tile of the quad (0..3)
-  int r0;      // offset of the thread's 4 cells in a body array of the stage
-  bool north;  // the N row is the halo row (the thread's row is the tile's row 7)
-  bool south;  // the S row is the halo row (row 0)
-  int c0;      // first column of the thread's cells (offset in a halo row)
+  int r0;
+  bool north, south;
 };
 
 __device__ __forceinline__ StageRow stage_row(int sub, int q) {
   const int cx = q & (ROWT - 1), ty = q / ROWT;
-  StageRow s;
-  s.t = sub;
-  s.r0 = sub * TILE + ty * TX + cx * CPT;
-  s.north = ty == TY - 1;
-  s.south = ty == 0;
-  s.c0 = cx * CPT;
-  return s;
+  return StageRow{sub * TILE + ty * TX + cx * CPT, ty == TY - 1, ty == 0};
 }
 
-template <int NB, int NHN, int NHS>
-__device__ __forceinline__ V4<float> st_body(const Stage<NB, NHN, NHS> &st, int i,
-                                             const StageRow &r) {
+template <int NB>
+__device__ __forceinline__ V4<float> st_body(const Stage<NB> &st, int i, const StageRow &r) {
   return ld4(&st.body[i][r.r0]);
 }
-// the row above (N) of the thread's cells in array i (i < NHN for the halo)
-template <int NB, int NHN, int NHS>
-__device__ __forceinline__ V4<float> st_north(const Stage<NB, NHN, NHS> &st, int i, int ih,
-                                              const StageRow &r) {
-  return r.north ? ld4(&st.hn[ih][r.t][r.c0]) : ld4(&st.body[i][r.r0 + TX]);
+// the row above the thread's cells in array i: in the stage, or `halo`
+template <int NB>
+__device__ __forceinline__ V4<float> st_north(const Stage<NB> &st, int i, const StageRow &r,
+                                              const V4<float> &halo) {
+  return r.north ? halo : ld4(&st.body[i][r.r0 + TX]);
 }
-template <int NB, int NHN, int NHS>
-__device__ __forceinline__ V4<float> st_south(const Stage<NB, NHN, NHS> &st, int i, int ih,
-                                              const StageRow &r) {
-  return r.south ? ld4(&st.hs[ih][r.t][r.c0]) : ld4(&st.body[i][r.r0 - TX]);
+template <int NB>
+__device__ __forceinline__ V4<float> st_south(const Stage<NB> &st, int i, const StageRow &r,
+                                              const V4<float> &halo) {
+  return r.south ? halo : ld4(&st.body[i][r.r0 - TX]);
 }
 
 constexpr int MBAR_TRIES = 1 << 16;  // bounded mbarrier waits (each try may suspend)
 
-// setup(m) returns the member's values (a struct with `bool skip` and the
-// source arrays: `const float *b[NB], *hn[NHN], *hs[NHS]`); pre(a, g) loads
-// the thread's E/W edge values from global memory before the stage is waited
+// setup(m) returns the member's values (a struct with `bool skip` and the NB
+// source arrays `const float *b[NB]`); pre(a, g, row) loads the thread's
+// halo rows and edge values from global memory before the stage is waited
 // for; body(a, st, row, g, valid, e, v) computes one quad row vector from
-// stage st and the edge values e.  On a wait that runs out, *err is set and
-// the CTA stops computing (the step then fails with a timeout status); the
-// copies it issued are waited for, again bounded, before it exits.
-template <int NS, int NB, int NHN, int NHS, class Setup, class Pre, class Body>
+// stage st and those values e.  On a wait that runs out, *err is set and the
+// CTA stops computing (the step then fails with a timeout status); the copies
+// it issued are waited for, again bounded, before it exits.
+template <int NS, int NB, int NSTG, class Setup, class Pre, class Body>
 __device__ __forceinline__ void quad_sweep_staged(const DevStatic &S, double *part, int *err,
                                                   Setup setup, Pre pre, Body body) {
   using A = decltype(setup(0));
-  using St = Stage<NB, NHN, NHS>;
+  using St = Stage<NB>;
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   St *stg = reinterpret_cast<St *>(dyn_smem);
-  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ __align__(8) uint64_t bar[NSTG];
   __shared__ QuadLog<NS> L;
   __shared__ A da[QB];
   __shared__ int4 dq[QB];
@@ -276,34 +264,24 @@ __device__ __forceinline__ void quad_sweep_staged(const DevStatic &S, double *pa
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int G = gridDim.x, NQ = S.nquad;
   if (threadIdx.x == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+#pragma unroll
+    for (int i = 0; i < NSTG; ++i) mbar_init(&bar[i], 1);
     mbar_fence_init();
   }
   __syncthreads();
-  uint32_t phase0 = 0, phase1 = 0;  // parity of the next phase to wait for, per stage
-  bool dead = false;                // a wait ran out
+  uint32_t phase = 0;  // bit i: parity of stage i's next phase
+  bool dead = false;   // a wait ran out
   const StageRow row = stage_row(sub, q);
-  // thread 0: the copies of list entry j into stage j & 1
+  // thread 0: the copies of list entry j into stage j % NSTG
   auto issue = [&](int j) {
-    const int k = list[j], s = j & 1;
+    const int k = list[j], s = j % NSTG;
     const int4 cur = dq[k];
     const A &a = da[k];
     const uint32_t bb = uint32_t(cur.z) * TILE * sizeof(float);
-    mbar_arrive_expect(&bar[s], NB * bb + uint32_t(cur.z) * (NHN + NHS) * TX * sizeof(float));
+    mbar_arrive_expect(&bar[s], NB * bb);
     const size_t off = size_t(cur.y) * TILE;
 #pragma unroll
     for (int i = 0; i < NB; ++i) bulk_g2s(stg[s].body[i], a.b[i] + off, bb, &bar[s]);
-    for (int t = 0; t < cur.z; ++t) {
-      const int4 nb = dnb[k][t];
-#pragma unroll
-      for (int i = 0; i < NHN; ++i)
-        bulk_g2s(stg[s].hn[i][t], a.hn[i] + size_t(nb.w) * TILE, TX * sizeof(float), &bar[s]);
-#pragma unroll
-      for (int i = 0; i < NHS; ++i)
-        bulk_g2s(stg[s].hs[i][t], a.hs[i] + size_t(nb.z) * TILE + (TY - 1) * TX,
-                 TX * sizeof(float), &bar[s]);
-    }
   };
   int n = 0;
   for (int b0 = blockIdx.x; b0 < NQ; b0 += G * QB) {
@@ -327,25 +305,20 @@ __device__ __forceinline__ void quad_sweep_staged(const DevStatic &S, double *pa
       for (int k = 0; k < nk; ++k)
         if (!da[k].skip) list[c++] = k;
       nlist = c;
-      if (!dead) {
-        if (c > 0) issue(0);
-        if (c > 1) issue(1);
-      }
+      if (!dead)
+        for (int j = 0; j < NSTG && j < c; ++j) issue(j);
     }
     __syncthreads();
     const int nl = nlist;
     for (int j = 0; j < nl; ++j) {
-      const int k = list[j], s = j & 1;
+      const int k = list[j], s = j % NSTG;
       const A a = da[k];
       const int4 cur = dq[k];
       const bool valid = sub < cur.z;
       const RowGeo g = row_geo_nb(dnb[k][sub], valid ? cur.y + sub : 0, q);
-      const auto e = pre(a, g);
-      if (!dead && !mbar_wait(&bar[s], s ? phase1 : phase0, MBAR_TRIES)) dead = true;
-      if (s)
-        phase1 ^= 1u;
-      else
-        phase0 ^= 1u;
+      const auto e = pre(a, g, row);
+      if (!dead && !mbar_wait(&bar[s], (phase >> s) & 1u, MBAR_TRIES)) dead = true;
+      phase ^= 1u << s;
       double v[NS];
 #pragma unroll
       for (int i = 0; i < NS; ++i) v[i] = 0.0;
@@ -357,7 +330,7 @@ __device__ __forceinline__ void quad_sweep_staged(const DevStatic &S, double *pa
       }
       if (threadIdx.x == 0) L.qd[n] = b0 + k * G;
       __syncthreads();  // every thread is done with stage s: it may be refilled
-      if (threadIdx.x == 0 && !dead && j + 2 < nl) issue(j + 2);
+      if (threadIdx.x == 0 && !dead && j + NSTG < nl) issue(j + NSTG);
       if (++n == QCAP) {
         quad_store<NS>(L, n, S, part);
         n = 0;
@@ -370,13 +343,13 @@ __device__ __forceinline__ void quad_sweep_staged(const DevStatic &S, double *pa
   // memory goes
   if (dead && threadIdx.x == 0) {
     atomicExch(err, 1);
-    mbar_wait(&bar[0], phase0, MBAR_TRIES);
-    mbar_wait(&bar[1], phase1, MBAR_TRIES);
+#pragma unroll
+    for (int i = 0; i < NSTG; ++i) mbar_wait(&bar[i], (phase >> i) & 1u, MBAR_TRIES);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    mbar_inval(&bar[0]);
-    mbar_inval(&bar[1]);
+#pragma unroll
+    for (int i = 0; i < NSTG; ++i) mbar_inval(&bar[i]);
   }
 }
 

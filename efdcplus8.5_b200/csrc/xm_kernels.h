@@ -27,6 +27,10 @@ struct Launch {
   // for variant 1, caps on their resident CTAs per SM (0: occupancy)
   int variant = 0;
   int ctas_mv = 0, ctas_up = 0;
+  // MIXED: the inner solve's target is the reduction the FP64 residual needs
+  // to reach its stop, times this margin (< 1 over-solves the FP32 inner
+  // solve so that fewer refinement passes are needed)
+  double inner_margin = 1.0;
 };
 
 // One array to move between host order and tile order (see k_scatter).

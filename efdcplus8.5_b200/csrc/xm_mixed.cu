@@ -176,26 +176,30 @@ __global__ void __launch_bounds__(NT) k_red_mx_zinit(DevStatic S, DevSystem Y, C
 // arithmetic is the row functions' above, operand for operand, so the results
 // are those of variants 0 and 1 bit for bit.
 
-// E/W edge values of a thread's row vector (cx == 0: the west neighbour of
-// cell 0; cx == ROWT-1: the east neighbour of cell 3)
-struct Edge3 {
+// What a thread loads before its stage is waited for: the halo row of its
+// tile's edge row (h0..h2: three arrays' N row for a row-7 thread, two arrays'
+// S row for a row-0 thread) and its E/W edge values (cx == 0: the west
+// neighbour of cell 0; cx == ROWT-1: the east neighbour of cell 3).
+struct Halo {
+  V4<float> h0, h1, h2;
   float w0, w1, e0, e1, e2;
 };
 
-using MvStage = Stage<4, 3, 2>;     // z, p_old, AS, AW; N rows z, p_old, AS; S rows z, p_old
-using PolyStage = Stage<6, 3, 2>;   // r, Ap, AS, AW, x, p; N rows r, Ap, AS; S rows r, Ap
-using JacStage = Stage<4, 0, 0>;    // x, p, r, Ap
+constexpr int MV_STAGES = 3, POLY_STAGES = 2, JAC_STAGES = 2;
+using MvStage = Stage<4>;    // z, p_old, AS, AW
+using PolyStage = Stage<6>;  // r, Ap, AS, AW, x, p
+using JacStage = Stage<4>;   // x, p, r, Ap
 
 template <bool MA>
-__global__ void __launch_bounds__(NT, 4) k_mx_matvec_st(DevStatic S, DevSystem Y, const Ctl *ctl,
+__global__ void __launch_bounds__(NT, 3) k_mx_matvec_st(DevStatic S, DevSystem Y, const Ctl *ctl,
                                                        double *part) {
   struct A {
     bool skip, asym;
     float beta;
     float *pnew;
-    const float *b[4], *hn[3], *hs[2];
+    const float *b[4];
   };
-  quad_sweep_staged<1, 4, 3, 2>(
+  quad_sweep_staged<1, 4, MV_STAGES>(
       S, part, Y.err,
       [&](int m) {
         const Ctl &k = ctl[m];
@@ -203,29 +207,36 @@ __global__ void __launch_bounds__(NT, 4) k_mx_matvec_st(DevStatic S, DevSystem Y
         const bool asym = unsym<MA>(k);
         const bool poly = Y.mpoly[m] && !asym;
         const float *z = poly ? Y.z32 : (par ? Y.r32b : Y.r32);
-        const float *po = par ? Y.pb32 : Y.pa32;
         return A{(k.done | k.idone) != 0, asym, float(k.beta), par ? Y.pa32 : Y.pb32,
-                 {z, po, Y.as32, Y.aw32}, {z, po, Y.as32}, {z, po}};
+                 {z, par ? Y.pb32 : Y.pa32, Y.as32, Y.aw32}};
       },
-      [&](const A &a, const RowGeo &g) {
-        Edge3 e{0.f, 0.f, 0.f, 0.f, 0.f};
+      [&](const A &a, const RowGeo &g, const StageRow &row) {
+        Halo h{};
+        if (row.north) {
+          h.h0 = ld4(a.b[0] + g.dn);
+          h.h1 = ld4(a.b[1] + g.dn);
+          h.h2 = ld4(Y.as32 + g.dn);
+        } else if (row.south) {
+          h.h0 = ld4(a.b[0] + g.ds);
+          h.h1 = ld4(a.b[1] + g.ds);
+        }
         if (g.cx == 0) {
-          e.w0 = a.b[0][g.dwe];
-          e.w1 = a.b[1][g.dwe];
+          h.w0 = a.b[0][g.dwe];
+          h.w1 = a.b[1][g.dwe];
         }
         if (g.cx == ROWT - 1) {
-          e.e0 = a.b[0][g.dee];
-          e.e1 = a.b[1][g.dee];
-          e.e2 = Y.aw32[g.dee];
+          h.e0 = a.b[0][g.dee];
+          h.e1 = a.b[1][g.dee];
+          h.e2 = Y.aw32[g.dee];
         }
-        return e;
+        return h;
       },
       [&](const A &a, const MvStage &st, const StageRow &row, const RowGeo &g, bool valid,
-          const Edge3 &e, double *v) {
+          const Halo &e, double *v) {
         const float beta = a.beta;
         const V4<float> r0 = st_body(st, 0, row), o0 = st_body(st, 1, row);
-        const V4<float> rn = st_north(st, 0, 0, row), on = st_north(st, 1, 1, row);
-        const V4<float> rs = st_south(st, 0, 0, row), os = st_south(st, 1, 1, row);
+        const V4<float> rn = st_north(st, 0, row, e.h0), on = st_north(st, 1, row, e.h1);
+        const V4<float> rs = st_south(st, 0, row, e.h0), os = st_south(st, 1, row, e.h1);
         const V4<float> p = {fmaf(beta, o0.x, r0.x), fmaf(beta, o0.y, r0.y),
                              fmaf(beta, o0.z, r0.z), fmaf(beta, o0.w, r0.w)};
         const V4<float> pn = {fmaf(beta, on.x, rn.x), fmaf(beta, on.y, rn.y),
@@ -241,7 +252,7 @@ __global__ void __launch_bounds__(NT, 4) k_mx_matvec_st(DevStatic S, DevSystem Y
           kn = ld4(Y.an32 + g.d0);
           ke = ld4(Y.ae32 + g.d0);
         } else {
-          kn = st_north(st, 2, 2, row);
+          kn = st_north(st, 2, row, e.h2);
           float kwe = from_east(kw);
           if (g.cx == ROWT - 1) kwe = e.e2;
           ke = {kw.y, kw.z, kw.w, kwe};
@@ -265,41 +276,46 @@ __global__ void __launch_bounds__(NT, 3) k_mx_update_poly_st(DevStatic S, DevSys
     bool skip;
     float alpha;
     float *rnew;
-    const float *b[6], *hn[3], *hs[2];
+    const float *b[6];
   };
-  quad_sweep_staged<2, 6, 3, 2>(
+  quad_sweep_staged<2, 6, POLY_STAGES>(
       S, part, Y.err,
       [&](int m) {
         const Ctl &k = ctl[m];
         const bool par = k.parity;
         const bool poly = Y.mpoly[m] && !unsym<true>(k);
-        const float *r = par ? Y.r32b : Y.r32;
         return A{(k.done | k.idone) != 0 || !poly, float(k.alpha), par ? Y.r32 : Y.r32b,
-                 {r, Y.ap32, Y.as32, Y.aw32, Y.x32, par ? Y.pa32 : Y.pb32},
-                 {r, Y.ap32, Y.as32},
-                 {r, Y.ap32}};
+                 {par ? Y.r32b : Y.r32, Y.ap32, Y.as32, Y.aw32, Y.x32, par ? Y.pa32 : Y.pb32}};
       },
-      [&](const A &a, const RowGeo &g) {
-        Edge3 e{0.f, 0.f, 0.f, 0.f, 0.f};
+      [&](const A &a, const RowGeo &g, const StageRow &row) {
+        Halo h{};
+        if (row.north) {
+          h.h0 = ld4(a.b[0] + g.dn);
+          h.h1 = ld4(Y.ap32 + g.dn);
+          h.h2 = ld4(Y.as32 + g.dn);
+        } else if (row.south) {
+          h.h0 = ld4(a.b[0] + g.ds);
+          h.h1 = ld4(Y.ap32 + g.ds);
+        }
         if (g.cx == 0) {
-          e.w0 = a.b[0][g.dwe];
-          e.w1 = Y.ap32[g.dwe];
+          h.w0 = a.b[0][g.dwe];
+          h.w1 = Y.ap32[g.dwe];
         }
         if (g.cx == ROWT - 1) {
-          e.e0 = a.b[0][g.dee];
-          e.e1 = Y.ap32[g.dee];
-          e.e2 = Y.aw32[g.dee];
+          h.e0 = a.b[0][g.dee];
+          h.e1 = Y.ap32[g.dee];
+          h.e2 = Y.aw32[g.dee];
         }
-        return e;
+        return h;
       },
       [&](const A &a, const PolyStage &st, const StageRow &row, const RowGeo &g, bool valid,
-          const Edge3 &e, double *v) {
+          const Halo &e, double *v) {
         const float alpha = a.alpha;
         const V4<float> r0 = st_body(st, 0, row), a0 = st_body(st, 1, row);
         const V4<float> rn0 = {fmaf(-alpha, a0.x, r0.x), fmaf(-alpha, a0.y, r0.y),
                                fmaf(-alpha, a0.z, r0.z), fmaf(-alpha, a0.w, r0.w)};
-        const V4<float> rN = st_north(st, 0, 0, row), aN = st_north(st, 1, 1, row);
-        const V4<float> rS = st_south(st, 0, 0, row), aS = st_south(st, 1, 1, row);
+        const V4<float> rN = st_north(st, 0, row, e.h0), aN = st_north(st, 1, row, e.h1);
+        const V4<float> rS = st_south(st, 0, row, e.h0), aS = st_south(st, 1, row, e.h1);
         const V4<float> nN = {fmaf(-alpha, aN.x, rN.x), fmaf(-alpha, aN.y, rN.y),
                               fmaf(-alpha, aN.z, rN.z), fmaf(-alpha, aN.w, rN.w)};
         const V4<float> nS = {fmaf(-alpha, aS.x, rS.x), fmaf(-alpha, aS.y, rS.y),
@@ -308,7 +324,7 @@ __global__ void __launch_bounds__(NT, 3) k_mx_update_poly_st(DevStatic S, DevSys
         if (g.cx == 0) nw = fmaf(-alpha, e.w1, e.w0);
         if (g.cx == ROWT - 1) ne = fmaf(-alpha, e.e1, e.e0);
         const V4<float> ks = st_body(st, 2, row), kw = st_body(st, 3, row);
-        const V4<float> kn = st_north(st, 2, 2, row);
+        const V4<float> kn = st_north(st, 2, row, e.h2);
         float kwe = from_east(kw);
         if (g.cx == ROWT - 1) kwe = e.e2;
         const V4<float> ke = {kw.y, kw.z, kw.w, kwe};
@@ -340,20 +356,18 @@ __global__ void __launch_bounds__(NT, 4) k_mx_update_jac_st(DevStatic S, DevSyst
     bool skip;
     float alpha;
     float *rnew;
-    const float *b[4], *hn[1], *hs[1];
+    const float *b[4];
   };
-  quad_sweep_staged<2, 4, 0, 0>(
+  quad_sweep_staged<2, 4, JAC_STAGES>(
       S, part, Y.err,
       [&](int m) {
         const Ctl &k = ctl[m];
         const bool par = k.parity;
         const bool poly = Y.mpoly[m] && !unsym<true>(k);
         return A{(k.done | k.idone) != 0 || poly, float(k.alpha), par ? Y.r32 : Y.r32b,
-                 {Y.x32, par ? Y.pa32 : Y.pb32, par ? Y.r32b : Y.r32, Y.ap32},
-                 {nullptr},
-                 {nullptr}};
+                 {Y.x32, par ? Y.pa32 : Y.pb32, par ? Y.r32b : Y.r32, Y.ap32}};
       },
-      [&](const A &, const RowGeo &) { return 0; },
+      [&](const A &, const RowGeo &, const StageRow &) { return 0; },
       [&](const A &a, const JacStage &st, const StageRow &row, const RowGeo &g, bool valid,
           int, double *v) {
         if (!valid) return;
@@ -377,12 +391,12 @@ __global__ void __launch_bounds__(NT, 4) k_mx_update_jac_st(DevStatic S, DevSyst
       });
 }
 
-// Dynamic shared memory of a staged kernel (two stages), allowed once.
+// Dynamic shared memory of a staged kernel (its stages), allowed once.
 template <class K>
-static size_t staged_smem(K kernel, size_t stage_bytes) {
+static size_t staged_smem(K kernel, size_t stage_bytes, int stages) {
   static std::mutex mu;
   static std::map<const void *, bool> done;
-  const size_t bytes = 2 * stage_bytes;
+  const size_t bytes = size_t(stages) * stage_bytes;
   std::lock_guard<std::mutex> lock(mu);
   const void *k = reinterpret_cast<const void *>(kernel);
   if (!done[k]) {
@@ -441,11 +455,11 @@ void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, C
                       double *part) {
   if (l.variant == 2) {
     if (l.may_asym) {
-      const size_t sm = staged_smem(k_mx_matvec_st<true>, sizeof(MvStage));
+      const size_t sm = staged_smem(k_mx_matvec_st<true>, sizeof(MvStage), MV_STAGES);
       k_mx_matvec_st<true><<<staged_grid(l, S, k_mx_matvec_st<true>, sm, l.ctas_mv), NT, sm,
                              l.stream>>>(S, Y, ctl, part);
     } else {
-      const size_t sm = staged_smem(k_mx_matvec_st<false>, sizeof(MvStage));
+      const size_t sm = staged_smem(k_mx_matvec_st<false>, sizeof(MvStage), MV_STAGES);
       k_mx_matvec_st<false><<<staged_grid(l, S, k_mx_matvec_st<false>, sm, l.ctas_mv), NT, sm,
                               l.stream>>>(S, Y, ctl, part);
     }
@@ -468,7 +482,7 @@ void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, C
 void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       Glob *glob, double *part, int no_stop) {
   if (l.mx_jac && l.variant == 2) {
-    const size_t sm = staged_smem(k_mx_update_jac_st, sizeof(JacStage));
+    const size_t sm = staged_smem(k_mx_update_jac_st, sizeof(JacStage), JAC_STAGES);
     k_mx_update_jac_st<<<staged_grid(l, S, k_mx_update_jac_st, sm, l.ctas_up), NT, sm,
                          l.stream>>>(S, Y, ctl, part);
     count_launches(1);
@@ -481,7 +495,7 @@ void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, C
     count_launches(1);
   }
   if (l.mx_poly && l.variant == 2) {
-    const size_t sm = staged_smem(k_mx_update_poly_st, sizeof(PolyStage));
+    const size_t sm = staged_smem(k_mx_update_poly_st, sizeof(PolyStage), POLY_STAGES);
     k_mx_update_poly_st<<<staged_grid(l, S, k_mx_update_poly_st, sm, l.ctas_up), NT, sm,
                           l.stream>>>(S, Y, ctl, part);
     count_launches(1);

@@ -673,7 +673,8 @@ __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, SysView V, DevSyst
 }
 __global__ void __launch_bounds__(NT) k_red_mx_resid(DevStatic S, Ctl *ctl, Glob *glob,
                                                     const double *part, double rsqm_fac,
-                                                    double rel_tol, int no_stop, int unscaled) {
+                                                    double rel_tol, int no_stop, int unscaled,
+                                                    double margin) {
   member_reduce<2>(
       S, part, [&](int m) { return ctl[m].done != 0; },
       [&](int m, const double *sum) {
@@ -696,7 +697,7 @@ __global__ void __launch_bounds__(NT) k_red_mx_resid(DevStatic S, Ctl *ctl, Glob
         k.outer += 1;
         // inner stop on the scaled residual: reduce it by the factor the FP64
         // residual needs to reach 0.1*RSQM, and by at least rel_tol (in norm)
-        const double need = (rsq > 0.0) ? 0.1 * rsqm / rsq : 1.0;
+        const double need = (rsq > 0.0) ? margin * 0.1 * rsqm / rsq : 1.0;
         k.rsq_target = rz * fmax(fmin(need, 1.0), rel_tol * rel_tol);
         int fin = 0;
         if (!isfinite(rsq)) {
@@ -1296,7 +1297,7 @@ void launch_mx_resid(const Launch &l, const DevStatic &S, const SysView &V, cons
                                                                              part);
   launch_chan_resmx(l, S, V, Y, P, ctl, part);
   k_red_mx_resid<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, rsqm_fac, rel_tol,
-                                                      no_stop, V.unscaled);
+                                                      no_stop, V.unscaled, l.inner_margin);
   count_launches(2);
   launch_mx_zinit(l, S, Y, ctl, part);  // z0 = M^-1 r0 of the inner solve
 }

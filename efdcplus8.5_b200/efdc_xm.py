@@ -75,6 +75,15 @@ class Fields(C.Structure):
                 ("unchanged", C.c_int32), ("pad_u_", C.c_int32)]
 
 
+class Schedule(C.Structure):
+    _fields_ = [("kernel_variant", C.c_int32), ("ctas_matvec", C.c_int32),
+                ("ctas_update", C.c_int32), ("graph_iters", C.c_int32),
+                ("poly_threshold", C.c_int32), ("inner_margin", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Layers(C.Structure):
     _fields_ = [("kc", C.c_int32), ("ld", C.c_int32), ("dzc", _pd), ("zz", _pd)]
 
@@ -339,6 +348,35 @@ OPT_GRAPH_ITERS = 2
 OPT_KERNEL_VARIANT = 3
 OPT_CTAS_MATVEC = 4
 OPT_CTAS_UPDATE = 5
+OPT_POLY_THRESHOLD = 6
+OPT_INNER_MARGIN = 7
+
+
+TUNE_MEASURE = 1
+
+
+def tune_lookup(table, key: str):
+    """The schedule (a dict) the tuning table holds for `key`, or None."""
+    sch = Schedule()
+    rc = load().efdc_xm_tune_lookup(str(table).encode(), key.encode(), C.byref(sch))
+    return sch.as_dict() if rc == OK else None
+
+
+def _autotune(lib, ctx, precision, table, measure):
+    sch = Schedule()
+    ms = C.c_double(0.0)
+    rc = lib.efdc_xm_autotune(ctx, precision, str(table).encode() if table else None,
+                              TUNE_MEASURE if measure else 0, C.byref(sch), C.byref(ms))
+    if rc != OK:
+        raise RuntimeError(f"efdc_xm_autotune: {lib.efdc_xm_last_error().decode()}")
+    return sch.as_dict(), ms.value
+
+
+def _tune_key(lib, ctx, precision):
+    buf = C.create_string_buffer(256)
+    if lib.efdc_xm_tune_key(ctx, precision, buf, 256) != OK:
+        raise RuntimeError("efdc_xm_tune_key failed")
+    return buf.value.decode()
 
 
 def host_waits() -> int:
@@ -393,6 +431,13 @@ def load(path: str | os.PathLike | None = None):
     lib.efdc_xm_stream.argtypes = [C.c_void_p]
     lib.efdc_xm_kernel_launches.restype = C.c_int64
     lib.efdc_xm_host_waits.restype = C.c_int64
+    lib.efdc_xm_autotune.restype = C.c_int32
+    lib.efdc_xm_autotune.argtypes = [C.c_void_p, C.c_int32, C.c_char_p, C.c_int32,
+                                     C.POINTER(Schedule), C.POINTER(C.c_double)]
+    lib.efdc_xm_tune_key.restype = C.c_int32
+    lib.efdc_xm_tune_key.argtypes = [C.c_void_p, C.c_int32, C.c_char_p, C.c_int32]
+    lib.efdc_xm_tune_lookup.restype = C.c_int32
+    lib.efdc_xm_tune_lookup.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(Schedule)]
     lib.efdc_xm_set_option.restype = C.c_int32
     lib.efdc_xm_set_option.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
     lib.efdc_xm_set_layers.restype = C.c_int32
@@ -510,6 +555,13 @@ class Solver:
         rc = self.lib.efdc_xm_set_option(self.ctx, option, value)
         if rc != OK:
             raise RuntimeError(f"efdc_xm_set_option: {self.last_error()}")
+
+    def autotune(self, precision: int, table=None, measure: bool = False):
+        """efdc_xm_autotune: (schedule dict, measured solve ms or 0 if replayed)."""
+        return _autotune(self.lib, self.ctx, precision, table, measure)
+
+    def tune_key(self, precision: int) -> str:
+        return _tune_key(self.lib, self.ctx, precision)
 
     def set_layers(self, ly: dict, member: int = 0):
         s, _keep = make_layers(ly)
@@ -746,6 +798,13 @@ class BatchSolver:
         rc = self.lib.efdc_xm_set_option(self.ctx, option, value)
         if rc != OK:
             raise RuntimeError(f"efdc_xm_set_option: {self.last_error()}")
+
+    def autotune(self, precision: int, table=None, measure: bool = False):
+        """efdc_xm_autotune: (schedule dict, measured solve ms or 0 if replayed)."""
+        return _autotune(self.lib, self.ctx, precision, table, measure)
+
+    def tune_key(self, precision: int) -> str:
+        return _tune_key(self.lib, self.ctx, precision)
 
     def time_kernels(self, precision: int, reps: int = 20) -> KTime:
         kt = KTime()

@@ -411,6 +411,37 @@ void *efdc_xm_stream(efdc_xm_ctx *ctx);
 /* Number of kernels this library has launched in the process so far. */
 int64_t efdc_xm_kernel_launches(void);
 
+/* Schedule autotuner.  No counterpart in the reference, whose only schedule
+ * rule is its thread count NOPTIMAL = MIN(NTHREADS,8,MAX(LA/100,1))
+ * (calpuv2c.f90:61-62).  A schedule is the set of options above that change
+ * the speed of a step but not its results (beyond the MIXED form's error
+ * bar).  efdc_xm_autotune picks one for the context's workload: it looks the
+ * workload's key up in the text file `table` and applies the schedule found
+ * there (no measurement), or, when the key is absent or flags has
+ * EFDC_XM_TUNE_MEASURE, times the solve of the system the last step assembled
+ * (every member must have stepped once with `precision`; P is put back) under
+ * candidate schedules -- one option at a time, candidates in a fixed order --
+ * applies the fastest and appends it to the table.  *solve_ms: the measured
+ * solve time of the chosen schedule (0 when replayed).  The key holds the
+ * precision, the floor log2 of the member count and of the water cells, and
+ * whether the operator may be unsymmetric or has sub-grid channels. */
+typedef struct efdc_xm_schedule {
+  int32_t kernel_variant;  /* EFDC_XM_OPT_KERNEL_VARIANT */
+  int32_t ctas_matvec;     /* EFDC_XM_OPT_CTAS_MATVEC */
+  int32_t ctas_update;     /* EFDC_XM_OPT_CTAS_UPDATE */
+  int32_t graph_iters;     /* EFDC_XM_OPT_GRAPH_ITERS */
+  int32_t poly_threshold;  /* EFDC_XM_OPT_POLY_THRESHOLD */
+  int32_t inner_margin;    /* EFDC_XM_OPT_INNER_MARGIN */
+} efdc_xm_schedule;
+enum { EFDC_XM_TUNE_MEASURE = 1 };
+int32_t efdc_xm_autotune(efdc_xm_ctx *ctx, int32_t precision, const char *table, int32_t flags,
+                         efdc_xm_schedule *chosen, double *solve_ms);
+/* The table key of a context's workload (NUL-terminated into buf). */
+int32_t efdc_xm_tune_key(const efdc_xm_ctx *ctx, int32_t precision, char *buf, int32_t len);
+/* The schedule `table` holds for `key` (its last line with that key);
+ * EFDC_XM_BAD_ARGUMENT when there is none.  Reads the file only: no GPU. */
+int32_t efdc_xm_tune_lookup(const char *table, const char *key, efdc_xm_schedule *out);
+
 /* Number of times a step or solve call of this library has waited for the
  * device so far (host synchronisations).  A step whose loops run on the
  * device (EFDC_XM_OPT_DEVICE_LOOPS) waits once, when it has finished. */
@@ -434,13 +465,23 @@ int64_t efdc_xm_host_waits(void);
  *   EFDC_XM_OPT_CTAS_MATVEC, EFDC_XM_OPT_CTAS_UPDATE (default 0, 0..32): with
  *     variants 1 and 2, caps on the resident CTAs per SM of the inner
  *     iteration's matrix-vector and update kernels (0: as many as fit).
+ *   EFDC_XM_OPT_POLY_THRESHOLD (default 10, 0..100000): a MIXED member whose
+ *     last solve took more than this many Jacobi-equivalent inner iterations
+ *     uses the polynomial preconditioner (0: always, 100000: never).
+ *   EFDC_XM_OPT_INNER_MARGIN (default 0, 0..6): the MIXED inner solve reduces
+ *     its residual 10^value times further than the FP64 residual needs to
+ *     reach its stop, trading inner iterations for refinement passes.
+ * Results stay within the MIXED form's error bar whatever the schedule; the
+ * FP64 form's results do not depend on it.
  * Returns EFDC_XM_BAD_ARGUMENT for an unknown option or value. */
 enum {
   EFDC_XM_OPT_DEVICE_LOOPS = 1,
   EFDC_XM_OPT_GRAPH_ITERS = 2,
   EFDC_XM_OPT_KERNEL_VARIANT = 3,
   EFDC_XM_OPT_CTAS_MATVEC = 4,
-  EFDC_XM_OPT_CTAS_UPDATE = 5
+  EFDC_XM_OPT_CTAS_UPDATE = 5,
+  EFDC_XM_OPT_POLY_THRESHOLD = 6,
+  EFDC_XM_OPT_INNER_MARGIN = 7
 };
 int32_t efdc_xm_set_option(efdc_xm_ctx *ctx, int32_t option, int32_t value);
 

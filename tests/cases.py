@@ -79,12 +79,13 @@ def copy_state(st):
 
 
 def run_both(scn, steps, tm=1.0, precision=None, same_input=False, lists=False, n0=1,
-             nthreads=1, keep=None):
+             nthreads=1, keep=None, oracle_rsqm_scale=1.0):
     """Run the GPU library (efdc_xm_step on host arrays) and the oracle side by
     side for `steps` steps.  Returns one (gpu stats, oracle stats, gpu state,
     oracle state) tuple per step; `keep(n)` selects the steps whose states are
     kept (default: all).  same_input=True starts every GPU step from the
-    oracle's state."""
+    oracle's state.  oracle_rsqm_scale scales the oracle's RSQM (a tighter
+    FP64 solve as the reference solution of the same system)."""
     import efdc_xm as X
     import oracle as O
     precision = X.PREC_FP64 if precision is None else precision
@@ -97,7 +98,9 @@ def run_both(scn, steps, tm=1.0, precision=None, same_input=False, lists=False, 
             sg = copy_state(so)
         prm = X.make_params(scn.params, n=n, tn=scn.tn(n) * tm, precision=precision)
         a = sol.step(prm, sg, lists=lists)
-        b = orc.step(X.make_params(scn.params, n=n, tn=scn.tn(n) * tm), so, lists=lists)
+        po = X.make_params(scn.params, n=n, tn=scn.tn(n) * tm)
+        po.rsqm *= oracle_rsqm_scale
+        b = orc.step(po, so, lists=lists)
         k = keep is None or keep(n)
         out.append((a.as_dict(), b.as_dict(), copy_state(sg) if k else None,
                     copy_state(so) if k else None))

@@ -86,8 +86,15 @@ def test_wetting_and_drying_is_exercised():
 
 @pytest.mark.parametrize("name", list(VARIANTS))
 def test_mixed_within_1e6_of_fp64_oracle(name):
+    """From the oracle's state every step, the MIXED step's surface is within
+    1e-6 m of the FP64 solution of the same system.  These models use the
+    reference's RSQM = 1e-9, ten times looser than the seeded cases, so the
+    FP64 solve stopped at RSQM is itself that far from its system's solution
+    (Ohio_River_4: 1.1e-6 m); the reference solution here is the oracle's
+    FP64 solve at RSQM/100."""
     scn = model(name)
-    res = cases.run_both(scn, 100, precision=X.PREC_MIXED, same_input=True)
+    res = cases.run_both(scn, 100, precision=X.PREC_MIXED, same_input=True,
+                         oracle_rsqm_scale=0.01)
     for n, (a, b, sg, so) in enumerate(res, 1):
         assert a["status"] == X.OK, (n, a)
         assert cases.state_err(sg, so, scn.la) <= 1e-6, n

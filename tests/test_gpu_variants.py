@@ -5,7 +5,7 @@ batches of 32 units into shared memory, variant 2 also stages the units' rows
 in shared memory with bulk copies issued one unit ahead.  They run the same
 arithmetic on the same values, so a batch steps to the same state bit for
 bit: Jacobi and polynomial members, an unsymmetric (radiation) member, and
-wetting and drying.  Each variant's kernels also time through
+wetting and drying.  The staged variant's kernels also time through
 efdc_xm_time_kernels.
 """
 import numpy as np
@@ -24,7 +24,7 @@ def _lib():
     X.load()
 
 
-def run(mem, steps, tm, variant, caps=(0, 0)):
+def run(mem, steps, tm, variant, caps=(0, 0), timed=False):
     bs = X.BatchSolver([m.grid for m in mem])
     bs.set_option(X.OPT_KERNEL_VARIANT, variant)
     bs.set_option(X.OPT_CTAS_MATVEC, caps[0])
@@ -35,7 +35,8 @@ def run(mem, steps, tm, variant, caps=(0, 0)):
         r = bs.step([X.make_params(m.params, n=n, tn=m.tn(n) * tm, precision=X.PREC_MIXED)
                      for m in mem], sts)
         stats.append([(x.status, x.iters_total, x.solves, x.outer_refinements) for x in r])
-    kt = bs.time_kernels(X.PREC_MIXED, reps=3)
+    # (kernel timing iterates past convergence: only on a system far from it)
+    kt = bs.time_kernels(X.PREC_MIXED, reps=3) if timed else None
     bs.close()
     return sts, stats, kt
 
@@ -50,7 +51,6 @@ def test_variants_equal_variant0(variant, caps):
     for m in range(len(mem)):
         for k in FIELDS:
             np.testing.assert_array_equal(a[0][m][k], b[0][m][k], err_msg=f"{m}:{k}")
-    assert b[2].ms_matvec > 0 and b[2].ms_update > 0
 
 
 def test_variant2_several_batches_per_cta():
@@ -60,7 +60,8 @@ def test_variant2_several_batches_per_cta():
     import scenario as S
     mem = [S.config2(seed=2), S.config2(seed=3)]
     a = run(mem, 3, 1.0, 0)
-    b = run(mem, 3, 1.0, 2, caps=(1, 1))
+    b = run(mem, 3, 1.0, 2, caps=(1, 1), timed=True)
     assert a[1] == b[1]
+    assert b[2].ms_matvec > 0 and b[2].ms_update > 0
     for m in range(len(mem)):
         np.testing.assert_array_equal(a[0][m]["p"], b[0][m]["p"])
