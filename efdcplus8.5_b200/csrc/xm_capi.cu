@@ -174,6 +174,7 @@ struct efdc_xm_ctx {
   double *pser_d = nullptr;
   double *pser_h = nullptr;  // pinned
   double *ptmp = nullptr;    // scratch P for kernel timing
+  double *ptune = nullptr;   // the autotuner's copy of P (allocated on first use)
   // CUDA graphs of GRAPH_ITERS consecutive CG iterations on X.p (FP64) and
   // of the FP32 inner iteration, captured on first use
   // CG iteration graphs: [may_asym | chan << 1] (FP64),
@@ -3234,8 +3235,16 @@ int32_t efdc_xm_autotune(efdc_xm_ctx *c, int32_t precision, const char *table, i
   }
   c->sys_external = false;
   c->mxview = xm::SysView{c->X.fp, c->X.cc, c->X.cs, c->X.cw, c->X.ce, c->X.cn, 1};
-  CK(cudaMemcpyAsync(c->ptmp, c->X.p, size_t(c->nslot) * sizeof(double),
+  if (!c->ptune && !(c->ptune = c->alloc<double>(size_t(c->nslot), false))) {
+    set_error("efdc_xm_autotune: cudaMalloc failed");
+    return EFDC_XM_CUDA_ERROR;
+  }
+  // P as the step left it is its system's solution: the timed solves start
+  // from the step's own initial guess (ptmp), and P is put back at the end
+  CK(cudaMemcpyAsync(c->ptune, c->X.p, size_t(c->nslot) * sizeof(double),
                      cudaMemcpyDeviceToDevice, c->stream));
+  xm::launch_tune_guess(c->L(), c->S, c->X, c->ptmp);
+  CK(cudaGetLastError());
   schedule_of(c, &best);
   double best_ms = 0.0;
   int rc = tune_time(c, mixed, 0.1, 3, &best_ms);
@@ -3269,7 +3278,7 @@ int32_t efdc_xm_autotune(efdc_xm_ctx *c, int32_t precision, const char *table, i
   }
   if ((rc = knob(&efdc_xm_schedule::graph_iters, {2, 4, 8}))) return rc;
   // P as the last step left it
-  CK(cudaMemcpyAsync(c->X.p, c->ptmp, size_t(c->nslot) * sizeof(double),
+  CK(cudaMemcpyAsync(c->X.p, c->ptune, size_t(c->nslot) * sizeof(double),
                      cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   apply_schedule(c, best);

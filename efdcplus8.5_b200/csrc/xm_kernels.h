@@ -104,6 +104,8 @@ void launch_wetdry(const Launch &l, const DevStatic &S, const DevState &X, Ctl *
 void launch_final(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
                   const int *act, bool any_waste);
 void launch_reciprocals(const Launch &l, const DevStatic &S, const DevState &X, int t0, int t1);
+// the autotuner's initial guess of a timed solve: P at the last step's entry
+void launch_tune_guess(const Launch &l, const DevStatic &S, const DevState &X, double *out);
 // the bed's derived arrays (ZBRATU, ZBRATV, SGZUU, SGZVV) of the tiles [t0, t1)
 void launch_bed(cudaStream_t st, const DevStatic &S, const DevBed &Bd, const double *dxp,
                 const double *dyp, const double *dzc1, const double *sgzu1, const double *sgzv1,

@@ -1342,6 +1342,22 @@ void launch_final(const Launch &l, const DevStatic &S, const DevState &X, Ctl *c
   k_fin<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, ctl, act);
   count_launches(1);
 }
+// The autotuner's initial guess for timing a solve: P at the entry of the
+// last step, which a step without wetting and drying left as G*(HP+BELV)
+// (calpuv2c.f90:893-896) and whose HP the time-level advance kept in H1P.
+__global__ void __launch_bounds__(NT) k_tune_guess(DevStatic S, DevState X, double *out,
+                                                  int ntile) {
+  TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    const int d = tile * TILE + threadIdx.x;
+    out[d] = (S.kind[d] == LAND) ? X.p[d] : c.g * (X.h1p[d] + S.belv[d]);
+  }
+}
+void launch_tune_guess(const Launch &l, const DevStatic &S, const DevState &X, double *out) {
+  k_tune_guess<<<l.grid, NT, 0, l.stream>>>(S, X, out, l.ntile);
+  count_launches(1);
+}
+
 // HPI, HUI, HVI (calpuv2c.f90:896-906) from the final HP, HU, HV: outputs
 // only (nothing on the device reads them), formed when they are downloaded;
 // tiles [t0, t1).
