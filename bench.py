@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--tl3-calls", type=int, default=40,
                     help="three-time-level (CALPUV9C) side measurement on the ensemble: timed "
                          "calls of the leapfrog/correction schedule (0: skip)")
+    ap.add_argument("--small-steps", type=int, default=200,
+                    help="small-basin latency side measurement: steps per model (0: skip)")
     ap.add_argument("--calib-steps", type=int, default=200,
                     help="adjoint calibration side measurement, 512x512 basin (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
@@ -320,6 +322,65 @@ def wetdry(args, torch, dev, rank):
             "volume_residual_max_2_members": vres}
 
 
+def small_basins(args, torch, dev):
+    """Per-step latency of the FP64 drop-in on small real-size models: the
+    100x60 basin of the CPU-runnable configuration (~5,600 cells) and the
+    reference's three sample-model grids (tests/golden/sample_*.npz: 355 to
+    1,183 cells, their own RSQM and ISDRY), as a host that calls CALPUV2C once
+    per time step sees it -- device-resident (efdc_xm_step_device) and on host
+    arrays (efdc_xm_step) -- beside the CPU restatement on 1 thread and at
+    the reference's thread cap NOPTIMAL = MIN(NTHREADS, 8, MAX(LA/100, 1))."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as O
+    gold = REPO / "tests" / "golden"
+    models = [("config1_100x60", S.config1(), 1.0)]
+    for name, kw in (("Lake_T_HYD_WQ", dict(wind=(2e-4, 1e-4))),
+                     ("Lake_Washington", dict(wind=(1e-4, 2e-4))), ("Ohio_River_4", {})):
+        f = gold / f"sample_{name}.npz"
+        if f.exists():
+            models.append((name, S.sample_model(dict(np.load(f)), **kw), 1.0))
+    K = args.small_steps
+    out = {}
+    for name, scn, tm in models:
+        prm = [X.make_params(scn.params, n=n, tn=scn.tn(n) * tm) for n in range(1, K + 4)]
+        sol = X.Solver(scn.grid, device=dev.index)
+        sol.upload(scn.copy_state())
+        for k in range(3):
+            sol.step_device(prm[k])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        its = 0
+        for k in range(3, K + 3):
+            its += sol.step_device(prm[k]).iters_total
+        t_dev = (time.perf_counter() - t0) / K
+        st = scn.copy_state()
+        for k in range(3):
+            sol.step(prm[k], st)
+        t0 = time.perf_counter()
+        for k in range(3, K + 3):
+            sol.step(prm[k], st)
+        t_host = (time.perf_counter() - t0) / K
+        sol.close()
+        cpu = {}
+        for label, nt in (("1_thread", 1), ("noptimal", min(os.cpu_count() or 1, 8))):
+            o = O.Oracle(scn.grid, nthreads=nt, noptimal_cap=8)
+            so = scn.copy_state()
+            for k in range(3):
+                o.step(prm[k], so)
+            t0 = time.perf_counter()
+            for k in range(3, K + 3):
+                o.step(prm[k], so)
+            cpu[label] = {"ms_per_step": 1000 * (time.perf_counter() - t0) / K,
+                          "threads": o.noptimal}
+            o.close()
+        out[name] = {"cells": int(scn.ncell), "steps": K, "cg_iters_per_step": its / K,
+                     "gpu_device_resident_ms_per_step": 1000 * t_dev,
+                     "gpu_host_arrays_ms_per_step": 1000 * t_host, "cpu": cpu,
+                     "how": "wall clock per step over the timed steps after 3 warm-up "
+                            "steps; one host wait per GPU step"}
+    return out
+
+
 def calibration(args, torch):
     """Config-4 adjoint: gradient of a 20-gauge elevation misfit over
     `calib_steps` steps w.r.t. per-cell log Manning n and four boundary
@@ -536,7 +597,8 @@ def ours(args):
             sch, sms = bs.autotune(X.PREC_MIXED, Path(td) / "schedules.txt", measure=True)
         tune = {"schedule": sch, "solve_ms": sms, "seconds": time.perf_counter() - t0,
                 "key": bs.tune_key(X.PREC_MIXED), "how": "efdc_xm_autotune (coordinate descent "
-                "over the options, each candidate the median of 3 timed solves)"}
+                "over the options, each candidate the median of 5 timed solves, kept when 2 % "
+                "faster than the incumbent)"}
     rmx = run_batch(X.PREC_MIXED, args.steps, args.warmup)
 
     # elevation error of the MIXED solver against the FP64 solve of the same
@@ -835,6 +897,9 @@ def ours(args):
     calib_res = None
     if rank == 0 and world == 1 and args.calib_steps > 0:
         calib_res = calibration(args, torch)
+    small = None
+    if rank == 0 and world == 1 and args.small_steps > 0:
+        small = small_basins(args, torch, dev)
     clocks = ck.stop()
 
     # ---------------- CPU baseline (rank 0, N=1) ----------------
@@ -889,6 +954,7 @@ def ours(args):
             "three_level": tl3_res,
             "wetdry": wd_res,
             "calibration": calib_res,
+            "small_basins": small,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

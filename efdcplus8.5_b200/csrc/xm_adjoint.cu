@@ -114,15 +114,15 @@ __global__ void __launch_bounds__(NT) k_adj_pre(DevStatic S, DevState X, DevCali
     const double cvn = D2 * (S.dxyip[q.n] * hpe(q.n) - S.dxyip[d] * hd);
     const double aun = A.au_in[d] + cu, avn = A.av_in[d] + cv;
     const double aune = A.au_in[q.e] + cue, avnn = A.av_in[q.n] + cvn;
-    auto au_ = [&](int x) { return X.sub[x] * D2 * S.hruo[x] * S.rcx[x] * A.hu0[x]; };
-    auto av_ = [&](int x) { return X.svb[x] * D2 * S.hrvo[x] * S.rcx[x] * A.hv0[x]; };
+    auto au_ = [&](int x) { return X.sub[x] * D2 * S.hruo[x] * X.rcx[x] * A.hu0[x]; };
+    auto av_ = [&](int x) { return X.svb[x] * D2 * S.hrvo[x] * X.rcy[x] * A.hv0[x]; };
     A.au_out[d] = cu;
     A.av_out[d] = cv;
     A.ahp_out[d] = (kd == WATER) ? A.ahpe[d] : 0.0;
     A.afu[d] = X.sub[d] * aun;
     A.afv[d] = X.svb[d] * avn;
-    A.ahu_out[d] = -X.sub[d] * D2 * S.hruo[d] * S.rcx[d] * (A.psol[d] - A.psol[q.w]) * aun;
-    A.ahv_out[d] = -X.svb[d] * D2 * S.hrvo[d] * S.rcx[d] * (A.psol[d] - A.psol[q.s]) * avn;
+    A.ahu_out[d] = -X.sub[d] * D2 * S.hruo[d] * X.rcx[d] * (A.psol[d] - A.psol[q.w]) * aun;
+    A.ahv_out[d] = -X.svb[d] * D2 * S.hrvo[d] * X.rcy[d] * (A.psol[d] - A.psol[q.s]) * avn;
     double rhs = -au_(d) * aun + au_(q.e) * aune - av_(d) * avn + av_(q.n) * avnn;
     if (kd == OPENBC) {  // HP' = P'/G - BELV on the boundary cells
       rhs += A.ahpe[d] * c.gi;
@@ -162,15 +162,15 @@ __global__ void __launch_bounds__(NT) k_adj_coef(DevStatic S, DevState X, DevCal
     const double ld = lt(d);
     const double wu = (ld - lt(q.w)) * (A.psol[d] - A.psol[q.w]);
     const double wv = (ld - lt(q.s)) * (A.psol[d] - A.psol[q.s]);
-    A.ahu_out[d] += C1 * X.sub[d] * S.hruo[d] * S.rcx[d] * wu;
-    A.ahv_out[d] += C1 * X.svb[d] * S.hrvo[d] * S.rcx[d] * wv;
+    A.ahu_out[d] += C1 * X.sub[d] * S.hruo[d] * X.rcx[d] * wu;
+    A.ahv_out[d] += C1 * X.svb[d] * S.hrvo[d] * X.rcy[d] * wv;
     A.afp[d] = ld;
   }
 }
 
 // Boundary targets: d(loss)/d(fp) = lambda_bc*DELTI*DXYP + lambda_nb*CT,
 // accumulated onto the harmonic amplitudes PCB/PSB.
-__global__ void k_adj_obc(DevStatic S, DevObc B, DevCalib A) {
+__global__ void k_adj_obc(DevStatic S, DevState X, DevObc B, DevCalib A) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B.n; k += gridDim.x * blockDim.x) {
     const StepScalars &c = S.sc[0];
     const int d = B.slot[k], nb = B.nbr[k], side = B.side[k];
@@ -186,13 +186,13 @@ __global__ void k_adj_obc(DevStatic S, DevObc B, DevCalib A) {
     const double D = c.deltd2, G = c.g;
     double CT;
     if (side == 0)
-      CT = 0.5 * D * G * S.hruo[nb] * S.rcx[nb] * A.hu0[nb];
+      CT = 0.5 * D * G * S.hruo[nb] * X.rcx[nb] * A.hu0[nb];
     else if (side == 1)
-      CT = 0.5 * D * G * S.hruo[d] * S.rcx[d] * A.hu0[d];
+      CT = 0.5 * D * G * S.hruo[d] * X.rcx[d] * A.hu0[d];
     else if (side == 2)
-      CT = 0.5 * D * G * S.hrvo[nb] * S.rcx[nb] * A.hv0[nb];
+      CT = 0.5 * D * G * S.hrvo[nb] * X.rcy[nb] * A.hv0[nb];
     else
-      CT = 0.5 * D * G * S.hrvo[d] * S.rcx[d] * A.hv0[d];
+      CT = 0.5 * D * G * S.hrvo[d] * X.rcy[d] * A.hv0[d];
     const double fbar = A.lam[d] * c.delti * S.dxyp[d] + A.lam[nb] * CT;
     for (int t = 0; t < mt; ++t) {
       A.apcb[k * B.mtmax + t] += fbar * c.cosv[t];
@@ -332,7 +332,7 @@ void launch_adj_rhs(const Launch &l, const DevStatic &S, const DevSystem &Y, con
 void launch_adj_post(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B,
                      const DevCalib &A) {
   k_adj_coef<<<l.grid, NT, 0, l.stream>>>(S, X, A, l.ntile);
-  if (B.n > 0) k_adj_obc<<<(B.n + 255) / 256, 256, 0, l.stream>>>(S, B, A);
+  if (B.n > 0) k_adj_obc<<<(B.n + 255) / 256, 256, 0, l.stream>>>(S, X, B, A);
   k_adj_fp<<<l.grid, NT, 0, l.stream>>>(S, X, A, l.ntile);
   k_adj_gath<<<l.grid, NT, 0, l.stream>>>(S, A, l.ntile);
   count_launches(B.n > 0 ? 4 : 3);

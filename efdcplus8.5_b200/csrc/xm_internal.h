@@ -49,6 +49,8 @@ struct StepScalars {
   int istl;             // 0: CALPUV2C; 3 or 2: CALPUV9C(ISTL_) (the same for every member)
   int nctbc;            // NCTBC (CALPUV9C, ISTL_ = 3: 1 halves UHDYE, VHDXE on advancing)
   double rold, rnew;    // ROLD, RNEW: blend of FPGXE, FPGYE (CALPUV9C)
+  int isitb, isveg;     // ISITB >= 1: implicit bottom drag; ISVEG > 0: vegetation drag
+  double ritb;          // RITB
   double cosv[MT_MAX], sinv[MT_MAX];
 };
 
@@ -140,7 +142,6 @@ struct DevStatic {
   int nmember;
   const double *dxyp, *dxyip, *dxiu, *dyiu, *dxiv, *dyiv, *dxyu, *dxyv;
   const double *hruo, *hrvo, *subo, *svbo, *sbxo, *sbyo, *belv;
-  const double *rcx;      // RCX = RCY: 1 on water, 0 on ghosts (calpuv2c.f90:97-102)
   const double *fsgzu, *fsgzv;  // 0.5/DXYU, 0.5/DXYV (calpuv2c.f90:111-116)
   DevChan ch;                   // sub-grid channels (ch.n == 0: none)
   DevBaro baro;                 // layers and buoyancy integrals (baro.kc == 0: none)
@@ -171,6 +172,13 @@ struct DevState {
   // hp0: HP at entry (the H1P buffer after the time-level advance; HP in
   //   CALPUV9C(2), which does not advance).
   const double *huc, *hvc, *hb, *ub, *vb, *hp0;
+  // RCX, RCY: the implicit drag coefficients of the faces (calpuv2c.f90:
+  // 222-243), 1 on water and 0 on land slots until a step with ISITB >= 1 or
+  // ISVEG > 0 sets them; kept between steps like the reference's module arrays
+  double *rcx, *rcy;
+  // the implicit drag's inputs (allocated by the first upload that carries
+  // them): U(L,KSZU(L)), V(L,KSZV(L)), VU, UV, STBX, STBY, FXVEGE, FYVEGE
+  const double *ubot, *vbot, *vu, *uv, *stbx, *stby, *fxvege, *fyvege;
 };
 
 // Scaled system and CG vectors.

@@ -47,6 +47,10 @@ void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const 
 // CALPUV9C: the kernels up to the time-level advance, and the copies of the advance
 void launch_begin3(const Launch &l, const DevStatic &S, const DevState &X, const int *act);
 void launch_advance3(const Launch &l, const DevStatic &S, const DevState &X);
+// the implicit bottom / vegetation drag (RCX, RCY) of the members with ISITB >= 1
+// or ISVEG > 0, after the begin kernel
+void launch_implicit_drag(const Launch &l, const DevStatic &S, const DevState &X,
+                          const int *act);
 void launch_put(cudaStream_t st, const int *idx, const double *val, int n, double *dst);
 // sub-grid channels (xm_chan.cu); each does nothing unless l.chan
 void launch_chan_entry(const Launch &l, const DevStatic &S, const DevState &X, const int *act);

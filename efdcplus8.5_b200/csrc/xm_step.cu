@@ -117,10 +117,10 @@ __device__ __forceinline__ double assemble_cell(const DevStatic &S, const DevSta
   const double sub = X.sub[d], svb = X.svb[d], sube = X.sub[q.e], svbn = X.svb[q.n];
   X.fp[d] = fp1 - C1 * (sube * fuhe - sub * fuh + svbn * fvhn - svb * fvh - 2.0 * X.qsume[d]);
   C1 = -0.5 * c.deltd2 * c.g;
-  const double cs = C1 * svb * S.hrvo[d] * S.rcx[d] * X.hvc[d];
-  const double cw = C1 * sub * S.hruo[d] * S.rcx[d] * X.huc[d];
-  const double ce = C1 * sube * S.hruo[q.e] * S.rcx[q.e] * X.huc[q.e];
-  const double cn = C1 * svbn * S.hrvo[q.n] * S.rcx[q.n] * X.hvc[q.n];
+  const double cs = C1 * svb * S.hrvo[d] * X.rcy[d] * X.hvc[d];
+  const double cw = C1 * sub * S.hruo[d] * X.rcx[d] * X.huc[d];
+  const double ce = C1 * sube * S.hruo[q.e] * X.rcx[q.e] * X.huc[q.e];
+  const double cn = C1 * svbn * S.hrvo[q.n] * X.rcy[q.n] * X.hvc[q.n];
   const double cc = c.delti * S.dxyp[d] - cs - cw - ce - cn;
   X.cs[d] = cs;
   X.cw[d] = cw;
@@ -240,6 +240,50 @@ __global__ void __launch_bounds__(NT) k_begin3(DevStatic S, DevState X, int ntil
   }
 }
 
+// calpuv2c.f90:222-243 (calpuv9c.f90:220-240): the implicit bottom drag with
+// vegetation (ISITB >= 1) or the vegetation drag alone (ISVEG > 0) of the
+// members that have them, after the explicit transports: RCX, RCY of each
+// water cell, and FUHDYE, FVHDXE multiplied by them.  HU, HV, UHE, VHE are
+// still the entry values here; HUI(L) is 1./HU(L), as the previous step left
+// it (:902-906).  Compiled without FMA contraction, in the reference's
+// operand order.
+__global__ void __launch_bounds__(NT) k_implicit_drag(DevStatic S, DevState X, int ntile,
+                                                     const int *act) {
+  TILE_LOOP(ntile) {
+    TILE_MEMBER(S);
+    if (!act[m] || !(c.isitb >= 1 || c.isveg > 0)) continue;
+    const int d = tile * TILE + threadIdx.x;
+    if (S.kind[d] == LAND) continue;
+    const double DELT = c.delt;
+    double rx, ry;
+    if (c.isitb >= 1) {
+      const double U = X.ubot[d], V = X.vbot[d];
+      double TMPX = 1.0, TMPY = 1.0;
+      if (X.uhe[d] != 0.0) TMPX = U * X.hu[d] / X.uhe[d];
+      if (X.vhe[d] != 0.0) TMPY = V * X.hv[d] / X.vhe[d];
+      const double HUI = 1. / X.hu[d], HVI = 1. / X.hv[d];
+      rx = 1. / (1. + TMPX * c.ritb * DELT * HUI * X.stbx[d] *
+                          sqrt(X.vu[d] * X.vu[d] + U * U) +
+                 DELT * X.fxvege[d]);
+      ry = 1. / (1. + TMPY * c.ritb * DELT * HVI * X.stby[d] *
+                          sqrt(X.uv[d] * X.uv[d] + V * V) +
+                 DELT * X.fyvege[d]);
+    } else {
+      rx = 1. / (1. + DELT * X.fxvege[d]);
+      ry = 1. / (1. + DELT * X.fyvege[d]);
+    }
+    X.rcx[d] = rx;
+    X.rcy[d] = ry;
+    X.fuhdye[d] = X.fuhdye[d] * rx;
+    X.fvhdxe[d] = X.fvhdxe[d] * ry;
+  }
+}
+void launch_implicit_drag(const Launch &l, const DevStatic &S, const DevState &X,
+                          const int *act) {
+  k_implicit_drag<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
+  count_launches(1);
+}
+
 // CALPUV9C(3), the copies of the time-level advance (calpuv9c.f90:282-311);
 // the host has rotated the buffers UHDY2E <- UHDY1E <- UHDYE and
 // H2P <- H1P <- HP before it.  NCTBC = 1 halves UHDYE on the way (:289-294).
@@ -314,25 +358,25 @@ __device__ __forceinline__ double obc_cell(const DevStatic &S, const DevState &X
     }
     if (ispb == 1 || ispb == 2) {  // radiation
       if (side == 0) {  // W, face at LEC(L)
-        const double CET = 0.5 * D * G * S.hruo[nb] * S.rcx[nb] * X.huc[nb];
+        const double CET = 0.5 * D * G * S.hruo[nb] * X.rcx[nb] * X.huc[nb];
         const double TMP = D * sqrt(G * X.huc[nb]) * S.dxiu[nb];
         X.cc[d] = CET * (1. + TMP) / TMP;
         X.ce[d] = -CET;
         fp = CET * (2. * fp - sqrt(G * X.huc[nb]) * X.fuhdye[nb] * S.dyiu[nb] / X.huc[nb]) / TMP;
       } else if (side == 1) {  // E, own west face
-        const double CWT = 0.5 * D * G * S.hruo[d] * S.rcx[d] * X.huc[d];
+        const double CWT = 0.5 * D * G * S.hruo[d] * X.rcx[d] * X.huc[d];
         const double TMP = D * sqrt(G * X.huc[d]) * S.dxiu[d];
         X.cc[d] = CWT * (1. + TMP) / TMP;
         X.cw[d] = -CWT;
         fp = CWT * (2. * fp + sqrt(G * X.huc[d]) * X.fuhdye[d] * S.dyiu[d] / X.huc[d]) / TMP;
       } else if (side == 2) {  // S, face at LNC(L)
-        const double CNT = 0.5 * D * G * S.hrvo[nb] * S.rcx[nb] * X.hvc[nb];
+        const double CNT = 0.5 * D * G * S.hrvo[nb] * X.rcy[nb] * X.hvc[nb];
         const double TMP = D * sqrt(G * X.hvc[nb]) * S.dyiv[nb];
         X.cc[d] = CNT * (1. + TMP) / TMP;
         X.cn[d] = -CNT;
         fp = CNT * (2. * fp - sqrt(G * X.hvc[nb]) * X.fvhdxe[nb] * S.dxiv[nb] / X.hvc[nb]) / TMP;
       } else {  // N, own south face
-        const double CST = 0.5 * D * G * S.hrvo[d] * S.rcx[d] * X.hvc[d];
+        const double CST = 0.5 * D * G * S.hrvo[d] * X.rcy[d] * X.hvc[d];
         const double TMP = D * sqrt(G * X.hvc[d]) * S.dyiv[d];
         X.cc[d] = CST * (1. + TMP) / TMP;
         X.cs[d] = -CST;
@@ -346,13 +390,13 @@ __device__ __forceinline__ double obc_cell(const DevStatic &S, const DevState &X
         CT = 0.;
         X.lopenbcdry[d] = 1;
       } else if (side == 0) {
-        CT = 0.5 * D * G * S.hruo[nb] * S.rcx[nb] * X.huc[nb];
+        CT = 0.5 * D * G * S.hruo[nb] * X.rcx[nb] * X.huc[nb];
       } else if (side == 1) {
-        CT = 0.5 * D * G * S.hruo[d] * S.rcx[d] * X.huc[d];
+        CT = 0.5 * D * G * S.hruo[d] * X.rcx[d] * X.huc[d];
       } else if (side == 2) {
-        CT = 0.5 * D * G * S.hrvo[nb] * S.rcx[nb] * X.hvc[nb];
+        CT = 0.5 * D * G * S.hrvo[nb] * X.rcy[nb] * X.hvc[nb];
       } else {
-        CT = 0.5 * D * G * S.hrvo[d] * S.rcx[d] * X.hvc[d];
+        CT = 0.5 * D * G * S.hrvo[d] * X.rcy[d] * X.hvc[d];
       }
       X.fp[nb] = X.fp[nb] + CT * fp;
       fp = c.delti * S.dxyp[d] * fp;
@@ -769,9 +813,9 @@ __global__ void __launch_bounds__(NT) k_backsub(DevStatic S, DevState X, int nti
     if (S.kind[d] == LAND) continue;
     const double P = X.p[d];
     const double u = X.sub[d] *
-                     (X.fuhdye[d] - c.deltd2 * S.hruo[d] * S.rcx[d] * X.huc[d] * (P - X.p[q.w]));
+                     (X.fuhdye[d] - c.deltd2 * S.hruo[d] * X.rcx[d] * X.huc[d] * (P - X.p[q.w]));
     const double v = X.svb[d] *
-                     (X.fvhdxe[d] - c.deltd2 * S.hrvo[d] * S.rcx[d] * X.hvc[d] * (P - X.p[q.s]));
+                     (X.fvhdxe[d] - c.deltd2 * S.hrvo[d] * X.rcy[d] * X.hvc[d] * (P - X.p[q.s]));
     X.uhdye[d] = u;
     X.vhdxe[d] = v;
     X.uhe[d] = u * S.dyiu[d];

@@ -54,7 +54,8 @@ class Params(C.Structure):
                 ("precision", C.c_int32), ("mixed_rsq_factor", C.c_double),
                 ("qcherr", C.c_double), ("chan_consistent", C.c_int32), ("pad_", C.c_int32),
                 ("bsc", C.c_double), ("gp", C.c_double), ("tl3_istl", C.c_int32),
-                ("nctbc", C.c_int32), ("rold", C.c_double), ("rnew", C.c_double)]
+                ("nctbc", C.c_int32), ("rold", C.c_double), ("rnew", C.c_double),
+                ("isitb", C.c_int32), ("isveg", C.c_int32), ("ritb", C.c_double)]
 
 
 class Fields(C.Structure):
@@ -72,6 +73,8 @@ class Fields(C.Structure):
                 ("p1", _pd), ("h2p", _pd), ("uhdy1e", _pd), ("vhdx1e", _pd), ("uhdy2e", _pd),
                 ("vhdx2e", _pd), ("h1u", _pd), ("h1v", _pd), ("tsx1", _pd), ("tsy1", _pd),
                 ("tbx1", _pd), ("tby1", _pd), ("fpgxe", _pd), ("fpgye", _pd),
+                ("ubot", _pd), ("vbot", _pd), ("vu", _pd), ("uv", _pd), ("stbx", _pd),
+                ("stby", _pd), ("fxvege", _pd), ("fyvege", _pd),
                 ("unchanged", C.c_int32), ("pad_u_", C.c_int32)]
 
 
@@ -140,6 +143,8 @@ FIELD_DIAG = ("ccc", "ccs", "ccw", "cce", "ccn", "fptmp")
 # three time levels (CALPUV9C): in/out, and the in-only wind and bed stresses
 FIELD_TL3 = ("p1", "h2p", "uhdy1e", "vhdx1e", "uhdy2e", "vhdx2e", "h1u", "h1v", "tsx1",
              "tsy1", "tbx1", "tby1", "fpgxe", "fpgye")
+# implicit bottom / vegetation drag (ISITB >= 1, ISVEG > 0): in
+FIELD_DRAG = ("ubot", "vbot", "vu", "uv", "stbx", "stby", "fxvege", "fyvege")
 
 
 def _dp(a):
@@ -223,6 +228,9 @@ def make_params(p: dict, *, n: int, tn: float, precision: int = PREC_FP64):
     s.nctbc = int(p.get("nctbc", 0))
     s.rold = p.get("rold", 0.0)
     s.rnew = p.get("rnew", 1.0)
+    s.isitb = int(p.get("isitb", 0))
+    s.isveg = int(p.get("isveg", 0))
+    s.ritb = p.get("ritb", 0.0)
     return s
 
 
@@ -312,7 +320,7 @@ def make_fields(st: dict, *, diag: bool = False, lists: bool = False, unchanged:
     s = Fields()
     s.unchanged = unchanged
     keep = []
-    for k in FIELD_DOUBLE_INOUT + FIELD_IN + FIELD_OUT + FIELD_CHAN + FIELD_TL3:
+    for k in FIELD_DOUBLE_INOUT + FIELD_IN + FIELD_OUT + FIELD_CHAN + FIELD_TL3 + FIELD_DRAG:
         a = st.get(k)
         if a is not None:
             setattr(s, k, _dp(a))

@@ -10,8 +10,11 @@
 !     SUB3D/SVB3D (calpuv2c.f90:958-1187), the layer depths of the cells whose
 !     volume was wasted (calpuv2c.f90:874-878, 1010-1015), and the
 !     negative-depth message of NEGDEP.
+! The implicit bottom and vegetation drag (ISITB>=1, ISVEG>0) pass their
+! inputs: the bottom-layer velocities U(L,KSZU(L)), V(L,KSZV(L)) gathered per
+! cell, VU, UV, STBX, STBY, FXVEGE, FYVEGE (calpuv2c.f90:222-243).
 ! Restrictions (the library returns EFDC_XM_UNSUPPORTED or XM_OPEN stops):
-! ISITB=0, ISVEG=0, ISGWIE=0, IGRIDV=0 (the baroclinic terms of BSC>1E-6 on
+! ISGWIE=0, IGRIDV=0 (the baroclinic terms of BSC>1E-6 on
 ! the standard sigma grid), no periodic (ISCONNECT) links; sub-grid channels
 ! (MDCHH>=1) of MDCHTYP 1 and 2, whose cells are not open-boundary cells.
 MODULE EFDC_XM_HOST
@@ -24,6 +27,7 @@ MODULE EFDC_XM_HOST
   TYPE(EFDC_XM_GRID_T), SAVE, TARGET :: XM_GRD
   REAL(C_DOUBLE), SAVE, ALLOCATABLE, TARGET :: PSERW(:), PSERE(:), PSERS(:), PSERN(:)
   INTEGER(C_INT32_T), SAVE, ALLOCATABLE, TARGET :: LMASKI(:), ISCDRYI(:), LOBCDRYI(:)
+  REAL(C_DOUBLE), SAVE, ALLOCATABLE, TARGET :: UBOTI(:), VBOTI(:)
 
 CONTAINS
 
@@ -32,8 +36,8 @@ CONTAINS
     TYPE(EFDC_XM_CHANNELS_T) :: CHN
     TYPE(EFDC_XM_LAYERS_T) :: LYR
 
-    IF( ISITB > 0 .OR. ISVEG > 0 .OR. ISGWIE > 0 .OR. IGRIDV > 0 )THEN
-      WRITE(6,'(2A)') WHO, ' (GPU): ISITB, ISVEG, ISGWIE, IGRIDV options are not supported'
+    IF( ISGWIE > 0 .OR. IGRIDV > 0 )THEN
+      WRITE(6,'(2A)') WHO, ' (GPU): ISGWIE, IGRIDV options are not supported'
       STOP '*** EXTERNAL MODE (GPU): unsupported options'
     ENDIF
     IF( C_ASSOCIATED(XM_CTX) ) RETURN
@@ -87,6 +91,9 @@ CONTAINS
     ENDIF
     ALLOCATE(PSERW(MAX(NPBW,1)), PSERE(MAX(NPBE,1)), PSERS(MAX(NPBS,1)), PSERN(MAX(NPBN,1)))
     ALLOCATE(LMASKI(LCM), ISCDRYI(LCM), LOBCDRYI(LCM))
+    ALLOCATE(UBOTI(LCM), VBOTI(LCM))
+    UBOTI = 0.0
+    VBOTI = 0.0
   END SUBROUTINE XM_OPEN
 
   ! The scalars and arrays both steps pass; the caller sets DELT, TN and the
@@ -120,6 +127,9 @@ CONTAINS
     PRM%NCTBC = 0
     PRM%ROLD = 0.0
     PRM%RNEW = 1.0
+    PRM%ISITB = ISITB
+    PRM%ISVEG = ISVEG
+    PRM%RITB = RITB
 
     ! *** time series part of the open-boundary targets (setopenbc.f90:41-46)
     DO LL=1,NPBW
@@ -186,6 +196,28 @@ CONTAINS
     FLD%TSX1 = C_NULL_PTR;   FLD%TSY1 = C_NULL_PTR
     FLD%TBX1 = C_NULL_PTR;   FLD%TBY1 = C_NULL_PTR
     FLD%FPGXE = C_NULL_PTR;  FLD%FPGYE = C_NULL_PTR
+    IF( ISITB >= 1 .OR. ISVEG > 0 )THEN
+      ! *** the implicit drag's inputs (calpuv2c.f90:222-243): the bottom layer's
+      ! *** velocities per cell, the rest as MODULE GLOBAL holds them
+      DO L=2,LA
+        UBOTI(L) = U(L,KSZU(L))
+        VBOTI(L) = V(L,KSZV(L))
+      ENDDO
+      FLD%UBOT = C_LOC(UBOTI(1)); FLD%VBOT = C_LOC(VBOTI(1))
+      FLD%VU = C_LOC(VU(1));      FLD%UV = C_LOC(UV(1))
+      FLD%STBX = C_LOC(STBX(1));  FLD%STBY = C_LOC(STBY(1))
+      IF( ISVEG > 0 )THEN
+        FLD%FXVEGE = C_LOC(FXVEGE(1)); FLD%FYVEGE = C_LOC(FYVEGE(1))
+      ELSE
+        FLD%FXVEGE = C_NULL_PTR;       FLD%FYVEGE = C_NULL_PTR
+      ENDIF
+    ELSE
+      FLD%UBOT = C_NULL_PTR; FLD%VBOT = C_NULL_PTR; FLD%VU = C_NULL_PTR; FLD%UV = C_NULL_PTR
+      FLD%STBX = C_NULL_PTR; FLD%STBY = C_NULL_PTR
+      FLD%FXVEGE = C_NULL_PTR; FLD%FYVEGE = C_NULL_PTR
+    ENDIF
+    FLD%UNCHANGED = 0    ! every array is sent each step
+    FLD%PAD_U_ = 0
   END SUBROUTINE XM_FIELDS
 
   SUBROUTINE XM_FINISH(IRC, ST, WHO)

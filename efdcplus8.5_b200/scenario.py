@@ -698,6 +698,46 @@ def sample_model(f: dict, *, dt: float = 10.0, drawdown: float = 0.0,
                     ijct=ijct)
 
 
+def add_implicit_drag(scn: Scenario, isitb: int = 1, *, isveg: int = 0, seed: int = 0,
+                      u_scale: float = 0.3, manning: float = 0.03,
+                      veg: float = 0.0) -> Scenario:
+    """The implicit bottom drag of ISITB >= 1 (calpuv2c.f90:222-233) and/or the
+    implicit vegetation drag of ISVEG > 0 (:234-242): seeded bottom-layer
+    velocities U(L,KSZU(L)), V(L,KSZV(L)) (``ubot``, ``vbot``) and the
+    interpolated VU, UV of scale ``u_scale`` m/s, Manning drag coefficients
+    STBX = STBY = g n^2 / H^(1/3) on the face depths, vegetative resistances
+    FXVEGE, FYVEGE uniform in [0, veg] 1/s, and RITB, RITB1 as CALTBXY sets
+    them for ISITB (caltbxy.f90:93-106: 0.55, 0.45 for 1; 1, 0 above).  The
+    explicit stresses TBX, TBY stay as they are (weighted by RITB1).  Fixed
+    over a run, like the other upstream terms of these scenarios."""
+    rng = np.random.default_rng(seed + 7)
+    la, lcm = scn.la, scn.lc + 1
+    i0 = np.arange(1, la)
+    st = scn.state
+
+    def field(scale):
+        a = np.zeros(lcm)
+        a[i0] = scale * rng.uniform(-1.0, 1.0, la - 1)
+        return a
+
+    st["ubot"], st["vbot"] = field(u_scale), field(u_scale)
+    st["vu"], st["uv"] = field(u_scale), field(u_scale)
+    for k, h in (("stbx", st["hu"]), ("stby", st["hv"])):
+        a = np.zeros(lcm)
+        a[i0] = G * manning ** 2 / np.cbrt(np.maximum(h[i0], 1e-3))
+        st[k] = a
+    for k in ("fxvege", "fyvege"):
+        a = np.zeros(lcm)
+        a[i0] = veg * rng.uniform(0.0, 1.0, la - 1)
+        st[k] = a
+    if isitb >= 1:
+        ritb, ritb1 = (0.55, 0.45) if isitb == 1 else (1.0, 0.0)
+    else:
+        ritb, ritb1 = 0.0, 1.0
+    scn.params.update(isitb=int(isitb), isveg=int(isveg), ritb=ritb, ritb1=ritb1)
+    return scn
+
+
 def add_three_levels(scn: Scenario) -> Scenario:
     """The state of the three-time-level scheme (CALPUV9C) at its start, with
     level n-1 equal to level n: P1 = P, H2P = H1P = HP, UHDY1E = UHDY2E =

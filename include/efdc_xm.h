@@ -128,6 +128,12 @@ typedef struct efdc_xm_params {
   double rold, rnew; /* ROLD, RNEW (CALPUV9C, BSC > 1e-6): FPGXE = ROLD*FPGXE +
                         RNEW*(new gradient) (calpuv9c.f90:157-163; hdmt.f90:304-305,
                         1018-1028: 0 and 1 for ISTL_ = 3, 0.5 and 0.5 for 2)          */
+  int32_t isitb;     /* ISITB >= 1: implicit bottom drag with vegetation, RCX, RCY of
+                        calpuv2c.f90:222-233 (calpuv9c.f90:220-231); RITB1 is then
+                        caltbxy.f90:95-100's (0.45 or 0) and TBX, TBY the explicit part */
+  int32_t isveg;     /* ISVEG > 0 (with ISITB = 0): implicit vegetation drag only,
+                        calpuv2c.f90:234-242                                         */
+  double ritb;       /* RITB (caltbxy.f90:95-105): weight of the implicit bottom drag */
 } efdc_xm_params;
 
 /* Per-call arrays.  "in/out" arrays are read and overwritten.  Optional outputs
@@ -179,6 +185,13 @@ typedef struct efdc_xm_fields {
   double *h1u, *h1v;                  /* H1U, H1V                                     */
   const double *tsx1, *tsy1, *tbx1, *tby1;  /* TSX1, TSY1, TBX1, TBY1, in            */
   double *fpgxe, *fpgye;              /* FPGXE, FPGYE, in/out; required where BSC > 1e-6 */
+  /* implicit drag (params.isitb >= 1 or params.isveg > 0), in: U(L,KSZU(L)) and
+   * V(L,KSZV(L)), the bottom-layer velocities; VU, UV; STBX, STBY (the bed drag
+   * coefficients of CALTBXY); FXVEGE, FYVEGE (the vegetative resistance, NULL =
+   * 0).  UHE, VHE above are then also read at entry (calpuv2c.f90:226-227).
+   * The drag coefficients RCX, RCY stay on the device between steps, as the
+   * reference's module arrays do. */
+  const double *ubot, *vbot, *vu, *uv, *stbx, *stby, *fxvege, *fyvege;
   /* in, optional (0: every given array is sent): bits of enum efdc_xm_same.
    * A set bit promises that the caller's array holds exactly what this
    * context last uploaded from it or downloaded into it; the library then
@@ -420,8 +433,9 @@ int64_t efdc_xm_kernel_launches(void);
  * there (no measurement), or, when the key is absent or flags has
  * EFDC_XM_TUNE_MEASURE, times the solve of the system the last step assembled
  * (every member must have stepped once with `precision`; P is put back) under
- * candidate schedules -- one option at a time, candidates in a fixed order --
- * applies the fastest and appends it to the table.  *solve_ms: the measured
+ * candidate schedules -- one option at a time, candidates in a fixed order,
+ * each the median of 5 timed solves, a candidate replacing the incumbent only
+ * when 2 % faster -- applies the result and appends it to the table.  *solve_ms: the measured
  * solve time of the chosen schedule (0 when replayed).  The key holds the
  * precision, the floor log2 of the member count and of the water cells, and
  * whether the operator may be unsymmetric or has sub-grid channels. */

@@ -449,6 +449,11 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
   F<const double> FCAXE = cin(f->fcaxe), FCAYE = cin(f->fcaye), FXE = cin(f->fxe),
                   FYE = cin(f->fye), TSX = cin(f->tsx), TSY = cin(f->tsy),
                   TBX = cin(f->tbx), TBY = cin(f->tby), QSUME = cin(f->qsume);
+  // implicit drag inputs (ISITB >= 1, ISVEG > 0): U(L,KSZU(L)), V(L,KSZV(L)),
+  // VU, UV, STBX, STBY, FXVEGE, FYVEGE
+  F<const double> UBOT = cin(f->ubot), VBOT = cin(f->vbot), VU = cin(f->vu), UV = cin(f->uv),
+                  STBX = cin(f->stbx), STBY = cin(f->stby), FXVEGE = cin(f->fxvege),
+                  FYVEGE = cin(f->fyvege);
   std::vector<double> qdw_local, vdw_local, uhe_l, vhe_l, hpi_l, hui_l, hvi_l;
   auto opt = [&](double *p, std::vector<double> &store) {
     if (p) return F<double>{p};
@@ -478,6 +483,32 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
   const double HDRY = prm->hdry;
   const int ISDRY = prm->isdry, NDRYSTP = prm->ndrystp;
   const double RITB1 = prm->ritb1, SNLT = prm->snlt;
+  const int ISITB = prm->isitb, ISVEG = prm->isveg;
+  const double RITB = prm->ritb;
+  // calpuv2c.f90:222-243 (calpuv9c.f90:220-240): the implicit bottom drag with
+  // vegetation, or the vegetation drag alone, of cell L; HUI(L) = 1./HU(L) as
+  // the previous step left it (:902-906)
+  auto implicit_drag = [&](int L) {
+    if (ISITB >= 1) {
+      double TMPX = 1.0, TMPY = 1.0;
+      if (UHE[L] != 0.0) TMPX = UBOT[L] * HU[L] / UHE[L];
+      if (VHE[L] != 0.0) TMPY = VBOT[L] * HV[L] / VHE[L];
+      const double HUIL = 1. / HU[L], HVIL = 1. / HV[L];
+      RCX[L] = 1. / (1. + TMPX * RITB * DELT * HUIL * STBX[L] *
+                              std::sqrt(VU[L] * VU[L] + UBOT[L] * UBOT[L]) +
+                     DELT * FXVEGE[L]);
+      RCY[L] = 1. / (1. + TMPY * RITB * DELT * HVIL * STBY[L] *
+                              std::sqrt(UV[L] * UV[L] + VBOT[L] * VBOT[L]) +
+                     DELT * FYVEGE[L]);
+      FUHDYE[L] = FUHDYE[L] * RCX[L];
+      FVHDXE[L] = FVHDXE[L] * RCY[L];
+    } else if (ISVEG > 0) {
+      RCX[L] = 1. / (1. + DELT * FXVEGE[L]);
+      RCY[L] = 1. / (1. + DELT * FYVEGE[L]);
+      FUHDYE[L] = FUHDYE[L] * RCX[L];
+      FVHDXE[L] = FVHDXE[L] * RCY[L];
+    }
+  };
   const bool baro = prm->bsc > 1.E-6;
   if (baro && (c->kc < 1 || !f->b || (tl3 && (!f->fpgxe || !f->fpgye)))) {
     st->status = EFDC_XM_BAD_ARGUMENT;
@@ -586,6 +617,7 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
                   SVB[L] * DELT * DYIV[L] *
                       (DXYV[L] * (TSY1[L] - RITB1 * TBY1[L]) - FCAYE[L] + FPGYE -
                        SNLT * FYE[L]);
+      implicit_drag(L);  // :220-240
     });
     if (ISDRY > 0)  // :246-262
       for_domains(c, [&](int L) {
@@ -648,6 +680,7 @@ int oracle_step(oracle_ctx *c, const efdc_xm_params *prm, efdc_xm_fields *f,
                       (DXYV[L] * (TSY[L] - RITB1 * TBY[L]) - FCAYE[L] + FPGYE -
                        SNLT * FYE[L]);
     }
+    implicit_drag(L);  // :222-243
     if (ISDRY > 0) {  // :246-253
       SUB[L] = SUBO[L];
       SVB[L] = SVBO[L];
