@@ -1460,12 +1460,19 @@ int upload_small(efdc_xm_ctx *c, const efdc_xm_fields *f) {
 
 // What the context records of an upload: which device copies are out of
 // date, whether it holds the three time levels, the entry masks (OLDMASK).
-void upload_done(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool skip_sbxy,
-                 bool levels) {
+// The implicit drag inputs (DRAG_*) an upload of f sends.
+unsigned drag_in_of(const efdc_xm_fields *f) {
+  unsigned b = 0;
   if (f[0].ubot && f[0].vbot && f[0].vu && f[0].uv && f[0].stbx && f[0].stby && f[0].uhe &&
       f[0].vhe)
-    c->drag_in |= DRAG_BED;
-  if (f[0].fxvege && f[0].fyvege) c->drag_in |= DRAG_VEG;
+    b |= DRAG_BED;
+  if (f[0].fxvege && f[0].fyvege) b |= DRAG_VEG;
+  return b;
+}
+
+void upload_done(efdc_xm_ctx *c, const efdc_xm_fields *f, bool skip_wetdry, bool skip_sbxy,
+                 bool levels) {
+  c->drag_in |= drag_in_of(f);
   c->wd_stale = skip_wetdry;
   c->sbxy_stale = skip_sbxy;
   c->tl3_ready = levels;
@@ -2544,13 +2551,16 @@ int step_batch_chunks(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields 
   }
   {  // the checks see the context as the upload will leave it; a refused call changes nothing
     const bool wd = c->wd_stale, sbxy = c->sbxy_stale, lv = c->tl3_ready;
+    const unsigned dr = c->drag_in;
     c->wd_stale = skip_wetdry;
     c->sbxy_stale = skip_sbxy;
     c->tl3_ready = false;
+    c->drag_in |= drag_in_of(f);
     rc = validate_step(c, prm, stats);
     c->wd_stale = wd;
     c->sbxy_stale = sbxy;
     c->tl3_ready = lv;
+    c->drag_in = dr;
     if (rc) return rc;
   }
   upload_done(c, f, skip_wetdry, skip_sbxy, false);  // the state the step and download see

@@ -20,6 +20,35 @@ import oracle as O
 import scenario as S
 
 
+def bottom_velocity(scn, st):
+    """U(L,KSZU(L)), V(L,KSZV(L)) from the current transports, as the internal
+    mode provides them: 0.8 of the depth-averaged velocity UHE/HU (a host
+    update before each step; then TMPX = 0.8 wherever UHE /= 0)."""
+    la = scn.la
+    for b, q, h in (("ubot", "uhe", "hu"), ("vbot", "vhe", "hv")):
+        a = np.zeros_like(st[q])
+        a[1:la] = 0.8 * st[q][1:la] / st[h][1:la]
+        st[b] = a
+
+
+def run_both_drag(scn, steps, precision=X.PREC_FP64, same_input=False):
+    """cases.run_both with the bottom velocities updated before each step."""
+    sol, orc = X.Solver(scn.grid), O.Oracle(scn.grid)
+    sg, so = scn.copy_state(), scn.copy_state()
+    out = []
+    for n in range(1, steps + 1):
+        if same_input:
+            sg = cases.copy_state(so)
+        bottom_velocity(scn, sg)
+        bottom_velocity(scn, so)
+        a = sol.step(X.make_params(scn.params, n=n, tn=scn.tn(n), precision=precision), sg)
+        b = orc.step(X.make_params(scn.params, n=n, tn=scn.tn(n)), so)
+        out.append((a.as_dict(), b.as_dict(), cases.copy_state(sg), cases.copy_state(so)))
+    sol.close()
+    orc.close()
+    return out
+
+
 def drag_case(isitb=1, isveg=0, veg=0.0, seed=0):
     scn = S.make_scenario(50, 36, seed=61 + seed, obc_sides=("W",), amp=0.4, dt=10.0,
                           explicit_noise=1e-4)
@@ -75,7 +104,7 @@ def test_oracle_drag_coefficients_and_assembly(isitb, isveg, veg):
 def test_gpu_drag_matches_oracle(isitb, isveg, veg):
     X.load()
     scn = drag_case(isitb, isveg, veg)
-    res = cases.run_both(scn, 30)
+    res = run_both_drag(scn, 30)
     for n, (a, b, sg, so) in enumerate(res, 1):
         assert a["status"] == b["status"] == X.OK, (n, a, b)
         assert a["iters_total"] == b["iters_total"], (n, a["iters_total"], b["iters_total"])
@@ -84,7 +113,7 @@ def test_gpu_drag_matches_oracle(isitb, isveg, veg):
     for k in ("uhdye", "vhdxe", "uhe", "vhe", "hu", "hv"):
         scale = max(1.0, float(np.abs(so[k][1:scn.la]).max()))
         assert np.abs(sg[k][1:scn.la] - so[k][1:scn.la]).max() <= 1e-9 * scale, k
-    resm = cases.run_both(scn, 15, precision=X.PREC_MIXED, same_input=True)
+    resm = run_both_drag(scn, 15, precision=X.PREC_MIXED, same_input=True)
     assert max(cases.state_err(sg, so, scn.la) for _, _, sg, so in resm) <= 1e-6
 
 
@@ -99,12 +128,15 @@ def test_gpu_drag_in_batch_with_plain_members():
         sol = X.Solver(m.grid)
         st = m.copy_state()
         for n in range(1, 11):
+            bottom_velocity(m, st)
             sol.step(X.make_params(m.params, n=n, tn=m.tn(n)), st)
         sol.close()
         single.append(st)
     bs = X.BatchSolver([m.grid for m in mem])
     sts = [m.copy_state() for m in mem]
     for n in range(1, 11):
+        for m, st in zip(mem, sts):
+            bottom_velocity(m, st)
         out = bs.step([X.make_params(m.params, n=n, tn=m.tn(n)) for m in mem], sts)
         assert all(r.status == X.OK for r in out)
     bs.close()
@@ -124,6 +156,8 @@ def test_gpu_drag_three_levels():
     for (n, istl, nctbc, rold, rnew) in sched:
         prm = X.make_params(S.three_level_params(scn.params, istl, nctbc, rold, rnew), n=n,
                             tn=scn.tn(n))
+        bottom_velocity(scn, sg)
+        bottom_velocity(scn, so)
         a = sol.step(prm, sg)
         b = o.step(prm, so)
         assert a.status == b.status == X.OK and a.iters_total == b.iters_total
