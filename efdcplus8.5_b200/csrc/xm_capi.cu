@@ -89,7 +89,7 @@ static_assert(sizeof(Ctl) % 4 == 0 && sizeof(Glob) % 4 == 0 &&
 
 struct Member {
   int la = 0, lc = 0;
-  int tile0 = 0, tile1 = 0;  // its tiles [tile0, tile1)
+  int tile0 = 0, tile1 = 0;  // its tiles [tile0, tile1); tile0 - 1 is its ghost tile
   long long off = 0;         // element offset of its arrays in the staging buffers
   int nobc = 0, b0 = 0;      // its open-boundary cells [b0, b0+nobc) of the packed list
   int side_n[4] = {0, 0, 0, 0};
@@ -871,12 +871,15 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   c->device = device;
   c->M = M;
   c->mem.resize(M);
-  int ntile = 1;  // tile 0: the ghost tile
+  // each member: its ghost tile (all land slots, holding the member's own
+  // ghost cell LC), then its water tiles; tile 0 is member 0's ghost tile
+  int ntile = 0;
   long long off = 0;
   for (int m = 0; m < M; ++m) {
     Member &mb = c->mem[m];
     mb.la = grids[m].la;
     mb.lc = grids[m].lc;
+    ntile += 1;
     mb.tile0 = ntile;
     ntile += int(ml[m].tiles.size());
     mb.tile1 = ntile;
@@ -935,15 +938,18 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
     Member &mb = c->mem[m];
     for (size_t k = 0; k < ly.tiles.size(); ++k) {
       const int id = ly.tiles[k].second, tx = id % ly.ntx, ty = id / ly.ntx;
+      const int ghost = mb.tile0 - 1;  // a missing neighbour tile: the member's ghost
       auto tl = [&](int x, int y) {
-        if (x < 0 || y < 0 || x >= ly.ntx || y >= ly.nty) return 0;
+        if (x < 0 || y < 0 || x >= ly.ntx || y >= ly.nty) return ghost;
         const int t = ly.tile_of[size_t(y) * ly.ntx + x];
-        return t > 0 ? mb.tile0 + t - 1 : 0;
+        return t > 0 ? mb.tile0 + t - 1 : ghost;
       };
       const int gt = mb.tile0 + int(k);
       tnbr[gt] = int4{tl(tx - 1, ty), tl(tx + 1, ty), tl(tx, ty - 1), tl(tx, ty + 1)};
       tile_member[gt] = m;
     }
+    tnbr[mb.tile0 - 1] = int4{mb.tile0 - 1, mb.tile0 - 1, mb.tile0 - 1, mb.tile0 - 1};
+    tile_member[mb.tile0 - 1] = m;
     tend[m] = mb.tile1;
     qstart[m] = int(quads.size());
     for (int t = mb.tile0; t < mb.tile1; t += 4)
@@ -987,7 +993,8 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
         const int nbL = (s == 0) ? g->lec[L - 1] : (s == 1) ? g->lwc[L - 1]
                         : (s == 2) ? g->lnc[L - 1] : g->lsc[L - 1];
         bslot.push_back(slot_of[m][L]);
-        bnbr.push_back(nbL == mb.lc ? 0 : slot_of[m][nbL]);  // 0 = a slot of the ghost tile
+        // the ghost cell LC: a slot of the member's ghost tile
+        bnbr.push_back(nbL == mb.lc ? (mb.tile0 - 1) * TILE : slot_of[m][nbL]);
         bside.push_back(s);
         bispb.push_back(o.ispb[ll]);
         bmember.push_back(m);
@@ -2600,8 +2607,8 @@ int step_batch_chunks(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields 
       if (acc * K >= tot * k) mb[k++] = m + 1;
     }
   }
-  auto slots = [&](int k, int &d0, int &d1) {  // chunk 0 covers the ghost tile too
-    d0 = mb[k] == 0 ? 0 : c->mem[mb[k]].tile0 * xm::TILE;
+  auto slots = [&](int k, int &d0, int &d1) {  // the members' ghost tiles included
+    d0 = (c->mem[mb[k]].tile0 - 1) * xm::TILE;
     d1 = c->mem[mb[k + 1] - 1].tile1 * xm::TILE;
   };
   // the transfer streams start after the solver stream's earlier work
@@ -3080,7 +3087,7 @@ int32_t efdc_xm_set_bed(efdc_xm_ctx *c, int32_t member, const efdc_xm_bed *bed) 
   if (!rc) rc = compute_after_copies(c);
   if (rc) return rc;
   const Member &mb = c->mem[member];
-  const int d0 = member == 0 ? 0 : mb.tile0 * xm::TILE, d1 = mb.tile1 * xm::TILE;
+  const int d0 = (mb.tile0 - 1) * xm::TILE, d1 = mb.tile1 * xm::TILE;  // with its ghost tile
   xm::launch_scatter(c->stream, c->jobs_d, int(xs.size()), c->lidx, c->tile_member, c->moff,
                      c->mlc, d0, d1);
   const size_t g = size_t(mb.lc) - 1;  // the ghost cell LC
@@ -3488,7 +3495,7 @@ int32_t efdc_xm_time_kernels(efdc_xm_ctx *c, int32_t precision, int32_t reps, ef
   long long ncell = 0;
   for (const Member &mb : c->mem) ncell += mb.la - 1;
   out->ncells = int32_t(std::min<long long>(ncell, INT32_MAX));
-  out->nslots = (c->ntile - 1) * TILE;
+  out->nslots = (c->ntile - c->M) * TILE;  // the water tiles' slots
   long long npoly = 0;
   for (int m = 0; m < c->M; ++m)
     if (mixed && c->mpoly_h[m] && !(c->ctl_h[m].asym & 1)) npoly += c->mem[m].la - 1;

@@ -19,7 +19,7 @@ __device__ __forceinline__ double rcpT(double x) { return 1. / x; }
 // The CG kernels loop over "quads": 4 consecutive tiles of one member, one
 // CTA pass each (a thread owns 4 cells of a row, 64 threads per tile), quads
 // dealt to the CTAs cyclically.  Past the member's last tile a thread works
-// on tile 0 (the ghost tile, all inert) with stores off, so that every lane
+// on tile 0 (member 0's ghost tile, all inert) with stores off, so that every lane
 // of a row takes part in the shuffles.  A quad whose member is finished (or
 // not in this sweep) is skipped by the whole CTA.
 //

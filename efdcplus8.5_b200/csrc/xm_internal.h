@@ -3,8 +3,9 @@
 // Layout ("bricks"): each basin's structured grid is cut into 32x8-cell
 // tiles.  Tiles holding at least one water cell are stored contiguously,
 // member after member, each member's tiles ordered along a Morton (Z) curve of
-// their tile coordinates; inside a tile a cell's slot is ty*32+tx.  Slot
-// d = tile*256 + ty*32 + tx.  Tile 0 is a ghost tile (all land).  Neighbours
+// their tile coordinates and preceded by the member's ghost tile (all land);
+// inside a tile a cell's slot is ty*32+tx.  Slot d = tile*256 + ty*32 + tx.
+// Tile 0 is member 0's ghost tile.  Neighbours
 // come from the slot position plus a 4-entry tile neighbour table, so no
 // per-cell index arrays are read in the solver: E/W neighbours are adjacent
 // words and N/S neighbours are the rows above and below, which keeps every
@@ -15,9 +16,10 @@
 // reduces over a basin (CCMNM, the CG dot products, the wet/dry re-solve flag,
 // the negative-depth count) is reduced per member.
 //
-// Land slots (padding inside a tile, and tile 0) stand for EFDC+'s ghost cell
-// LC (a missing neighbour maps to LC, EFDC/cellmap.f90:80-134): they hold the
-// host's element-LC values and are never written by the solver.
+// Land slots (padding inside a tile, and the member's ghost tile, which a
+// missing neighbour tile maps to) stand for EFDC+'s ghost cell LC (a missing
+// neighbour maps to LC, EFDC/cellmap.f90:80-134): they hold the member's
+// element-LC values and are never written by the solver.
 #pragma once
 
 #include <cstdint>
@@ -129,7 +131,7 @@ struct DevBaro {
 };
 
 struct DevStatic {
-  const int4 *tnbr;       // [ntile] (w, e, s, n) neighbour tiles, 0 = ghost tile
+  const int4 *tnbr;       // [ntile] (w, e, s, n) neighbour tiles (missing: the member's ghost tile)
   const uint8_t *kind;    // [nslot]
   const int *lidx;        // [nslot] member-local L of the slot, 0 for land
   const int *tile_member; // [ntile] member of each tile

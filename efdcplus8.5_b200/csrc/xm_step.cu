@@ -5,11 +5,12 @@
 // the global dot products differs (fixed-order tree instead of serial).
 //
 // The cell kernels are grid-stride loops over tiles (one 256-thread CTA
-// processes a whole 32x8 tile per pass; tile 0 is the ghost tile and is
-// skipped).  A tile belongs to one member of the ensemble; the member's
-// scalars come from S.sc[m] and its reductions go to ctl[m].  `act[m]` says
-// whether member m takes part in the current wet/dry sweep (or, for the
-// finalisation kernels, whether its step is to be finalised).
+// processes a whole 32x8 tile per pass; tile 0, member 0's ghost tile, is
+// skipped, and the other members' ghost tiles hold land slots only).  A tile
+// belongs to one member of the ensemble; the member's scalars come from
+// S.sc[m] and its reductions go to ctl[m].  `act[m]` says whether member m
+// takes part in the current wet/dry sweep (or, for the finalisation kernels,
+// whether its step is to be finalised).
 
 #include <map>
 #include <mutex>
@@ -97,6 +98,21 @@ __global__ void __launch_bounds__(NT) k_calebi(DevStatic S, DevState X, int ntil
   }
 }
 
+// RCX (u face of slot x) and RCY (v face): the implicit-drag factors of a
+// member with ISITB >= 1 or ISVEG > 0 (k_implicit_drag), else 1.0 without a
+// load (calpuv2c.f90:97-102: RCX = RCY = 1 on water cells; a land slot's 0
+// only ever multiplies its own zero switch SUB(LC) = SVB(LC) = 0, so 1.0 gives
+// the same product there).
+__device__ __forceinline__ bool has_drag(const StepScalars &c) {
+  return c.isitb >= 1 || c.isveg > 0;
+}
+__device__ __forceinline__ double rc_x(const DevState &X, const StepScalars &c, int x) {
+  return has_drag(c) ? X.rcx[x] : 1.0;
+}
+__device__ __forceinline__ double rc_y(const DevState &X, const StepScalars &c, int x) {
+  return has_drag(c) ? X.rcy[x] : 1.0;
+}
+
 // calpuv2c.f90:282-290 (calpuv9c.f90:277, from P1, UHDY1E, VHDX1E); U, V: the
 // transports at entry
 __device__ __forceinline__ double fp1_cell(const DevStatic &S, const StepScalars &c,
@@ -117,10 +133,10 @@ __device__ __forceinline__ double assemble_cell(const DevStatic &S, const DevSta
   const double sub = X.sub[d], svb = X.svb[d], sube = X.sub[q.e], svbn = X.svb[q.n];
   X.fp[d] = fp1 - C1 * (sube * fuhe - sub * fuh + svbn * fvhn - svb * fvh - 2.0 * X.qsume[d]);
   C1 = -0.5 * c.deltd2 * c.g;
-  const double cs = C1 * svb * S.hrvo[d] * X.rcy[d] * X.hvc[d];
-  const double cw = C1 * sub * S.hruo[d] * X.rcx[d] * X.huc[d];
-  const double ce = C1 * sube * S.hruo[q.e] * X.rcx[q.e] * X.huc[q.e];
-  const double cn = C1 * svbn * S.hrvo[q.n] * X.rcy[q.n] * X.hvc[q.n];
+  const double cs = C1 * svb * S.hrvo[d] * rc_y(X, c, d) * X.hvc[d];
+  const double cw = C1 * sub * S.hruo[d] * rc_x(X, c, d) * X.huc[d];
+  const double ce = C1 * sube * S.hruo[q.e] * rc_x(X, c, q.e) * X.huc[q.e];
+  const double cn = C1 * svbn * S.hrvo[q.n] * rc_y(X, c, q.n) * X.hvc[q.n];
   const double cc = c.delti * S.dxyp[d] - cs - cw - ce - cn;
   X.cs[d] = cs;
   X.cw[d] = cw;
@@ -358,25 +374,25 @@ __device__ __forceinline__ double obc_cell(const DevStatic &S, const DevState &X
     }
     if (ispb == 1 || ispb == 2) {  // radiation
       if (side == 0) {  // W, face at LEC(L)
-        const double CET = 0.5 * D * G * S.hruo[nb] * X.rcx[nb] * X.huc[nb];
+        const double CET = 0.5 * D * G * S.hruo[nb] * rc_x(X, c, nb) * X.huc[nb];
         const double TMP = D * sqrt(G * X.huc[nb]) * S.dxiu[nb];
         X.cc[d] = CET * (1. + TMP) / TMP;
         X.ce[d] = -CET;
         fp = CET * (2. * fp - sqrt(G * X.huc[nb]) * X.fuhdye[nb] * S.dyiu[nb] / X.huc[nb]) / TMP;
       } else if (side == 1) {  // E, own west face
-        const double CWT = 0.5 * D * G * S.hruo[d] * X.rcx[d] * X.huc[d];
+        const double CWT = 0.5 * D * G * S.hruo[d] * rc_x(X, c, d) * X.huc[d];
         const double TMP = D * sqrt(G * X.huc[d]) * S.dxiu[d];
         X.cc[d] = CWT * (1. + TMP) / TMP;
         X.cw[d] = -CWT;
         fp = CWT * (2. * fp + sqrt(G * X.huc[d]) * X.fuhdye[d] * S.dyiu[d] / X.huc[d]) / TMP;
       } else if (side == 2) {  // S, face at LNC(L)
-        const double CNT = 0.5 * D * G * S.hrvo[nb] * X.rcy[nb] * X.hvc[nb];
+        const double CNT = 0.5 * D * G * S.hrvo[nb] * rc_y(X, c, nb) * X.hvc[nb];
         const double TMP = D * sqrt(G * X.hvc[nb]) * S.dyiv[nb];
         X.cc[d] = CNT * (1. + TMP) / TMP;
         X.cn[d] = -CNT;
         fp = CNT * (2. * fp - sqrt(G * X.hvc[nb]) * X.fvhdxe[nb] * S.dxiv[nb] / X.hvc[nb]) / TMP;
       } else {  // N, own south face
-        const double CST = 0.5 * D * G * S.hrvo[d] * X.rcy[d] * X.hvc[d];
+        const double CST = 0.5 * D * G * S.hrvo[d] * rc_y(X, c, d) * X.hvc[d];
         const double TMP = D * sqrt(G * X.hvc[d]) * S.dyiv[d];
         X.cc[d] = CST * (1. + TMP) / TMP;
         X.cs[d] = -CST;
@@ -390,13 +406,13 @@ __device__ __forceinline__ double obc_cell(const DevStatic &S, const DevState &X
         CT = 0.;
         X.lopenbcdry[d] = 1;
       } else if (side == 0) {
-        CT = 0.5 * D * G * S.hruo[nb] * X.rcx[nb] * X.huc[nb];
+        CT = 0.5 * D * G * S.hruo[nb] * rc_x(X, c, nb) * X.huc[nb];
       } else if (side == 1) {
-        CT = 0.5 * D * G * S.hruo[d] * X.rcx[d] * X.huc[d];
+        CT = 0.5 * D * G * S.hruo[d] * rc_x(X, c, d) * X.huc[d];
       } else if (side == 2) {
-        CT = 0.5 * D * G * S.hrvo[nb] * X.rcy[nb] * X.hvc[nb];
+        CT = 0.5 * D * G * S.hrvo[nb] * rc_y(X, c, nb) * X.hvc[nb];
       } else {
-        CT = 0.5 * D * G * S.hrvo[d] * X.rcy[d] * X.hvc[d];
+        CT = 0.5 * D * G * S.hrvo[d] * rc_y(X, c, d) * X.hvc[d];
       }
       X.fp[nb] = X.fp[nb] + CT * fp;
       fp = c.delti * S.dxyp[d] * fp;
@@ -813,9 +829,9 @@ __global__ void __launch_bounds__(NT) k_backsub(DevStatic S, DevState X, int nti
     if (S.kind[d] == LAND) continue;
     const double P = X.p[d];
     const double u = X.sub[d] *
-                     (X.fuhdye[d] - c.deltd2 * S.hruo[d] * X.rcx[d] * X.huc[d] * (P - X.p[q.w]));
+                     (X.fuhdye[d] - c.deltd2 * S.hruo[d] * rc_x(X, c, d) * X.huc[d] * (P - X.p[q.w]));
     const double v = X.svb[d] *
-                     (X.fvhdxe[d] - c.deltd2 * S.hrvo[d] * X.rcy[d] * X.hvc[d] * (P - X.p[q.s]));
+                     (X.fvhdxe[d] - c.deltd2 * S.hrvo[d] * rc_y(X, c, d) * X.hvc[d] * (P - X.p[q.s]));
     X.uhdye[d] = u;
     X.vhdxe[d] = v;
     X.uhe[d] = u * S.dyiu[d];
