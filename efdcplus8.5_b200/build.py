@@ -27,6 +27,7 @@ SOURCES = {
     "xm_adjoint.cu": [],
     "xm_chan.cu": ["-fmad=false"],
     "xm_loop.cu": [],
+    "xm_explicit.cu": ["-fmad=false"],
 }
 
 

@@ -101,6 +101,10 @@ struct Member {
   int last_n = 0, last_ntstbc = 0, last_isdry = 0;
   std::vector<int32_t> oldmask_h;
   std::vector<int> slot_of;  // slot of cell L (0 for L outside 2..LA)
+  // CALEXP2T's type-2 open boundaries (calexp2t.f90:605-645), W, E, S, N in
+  // list order: (side, L of the modified cell, its neighbour the form reads
+  // (LNC for W, LWC for E, LEC for S, LSC for N), 0)
+  std::vector<int4> t2;
 };
 
 // A step captured as one graph (see step_graph): the bytes it was built from
@@ -236,6 +240,19 @@ struct efdc_xm_ctx {
   // bottom-stress producer (efdc_xm_set_bed, efdc_xm_bottom_stress_batch)
   xm::DevBed bed{};
   bool bed_alloc = false;
+  // explicit momentum producer (efdc_xm_set_momentum): device arrays, the
+  // per-member layer count and leading dimension, the serial lists
+  bool mom_alloc = false;
+  int mom_kc = 0;
+  xm::MomDev md{};
+  double *mom_hp = nullptr;
+  void *mom_lists = nullptr;  // the serial lists on the device (rebuilt after a set-up call)
+  char *pack_h = nullptr, *pack_d = nullptr;  // packed small transfers (page-locked, device)
+  bool mom_inputs = false;    // a call has left U, V, UHDY, VHDX on the device
+  std::vector<char> has_mom;
+  std::vector<int> mom_ld;
+  std::vector<std::vector<int4>> mom_t2, mom_bc;
+  std::vector<xm::MomScalars> mom_sc_h;
   std::vector<char> has_bed;         // [M]
   std::vector<xm::DragScalars> bed_sc;  // [M] the bed's scalars (delt ... filled per call)
   xm::DragScalars *ds = nullptr;     // [M] device
@@ -252,6 +269,7 @@ struct efdc_xm_ctx {
   // schedule of the FP32 CG kernels (efdc_xm_set_option: variant and CTA caps)
   int kvariant = 0, ctas_mv = 0, ctas_up = 0;
   int inner_margin_log10 = 0;   // MIXED inner target margin 10^-v
+  int inner_tol_x10 = 60;       // MIXED inner relative tolerance 10^(-v/10) at least
   float poly_threshold = 10.f;  // MIXED: polynomial preconditioner above this Jacobi count
   xm::Launch L() const {
     xm::Launch l{grid,      grid_cg, grid_cg32, grid_up32,
@@ -380,12 +398,85 @@ int d2h_range(efdc_xm_ctx *c, const Xfer &x, const char *stage, int m0, int m1, 
   return EFDC_XM_OK;
 }
 
+// Small transfers (the fields of small basins): the call's arrays go through
+// one page-locked host buffer and one device buffer, a host copy per array and
+// member, one copy over the link and one scatter (or one gather, one copy back
+// and host copies out).  A few link operations per call instead of one per
+// array: those, not bytes, bound a small basin's step on host arrays.
+constexpr size_t PACK_MAX = size_t(4) << 20;  // bytes of one packed transfer
+
+bool packed(efdc_xm_ctx *c, size_t njobs) {
+  const size_t bytes = njobs * size_t(c->stage_len) * sizeof(double);
+  if (bytes > PACK_MAX) return false;
+  if (!c->pack_h) {
+    if (cudaHostAlloc(&c->pack_h, PACK_MAX, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      c->pack_h = nullptr;
+      return false;
+    }
+    if (!(c->pack_d = c->alloc<char>(PACK_MAX, false))) {
+      cudaFreeHost(c->pack_h);
+      c->pack_h = nullptr;
+      return false;
+    }
+  }
+  return true;
+}
+
+int upload_packed(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
+  const size_t L = size_t(c->stage_len), n = xs.size();
+  for (size_t j = 0; j < n; ++j) {
+    const size_t es = esize(xs[j].kind);
+    char *dst = c->pack_h + j * L * sizeof(double);
+    for (int m = 0; m < c->M; ++m)
+      if (xs[j].host[m])
+        std::memcpy(dst + size_t(c->mem[m].off) * es, xs[j].host[m], size_t(c->mem[m].lc) * es);
+    c->jobs_h[j] = CopyJob{reinterpret_cast<double *>(c->pack_d + j * L * sizeof(double)),
+                           xs[j].dev, xs[j].kind};
+  }
+  const size_t bytes = n * L * sizeof(double);
+  CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, n * sizeof(CopyJob), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaMemcpyAsync(c->pack_d, c->pack_h, bytes, cudaMemcpyHostToDevice, c->stream));
+  g_h2d.fetch_add(static_cast<long long>(bytes), std::memory_order_relaxed);
+  xm::launch_scatter(c->stream, c->jobs_d, int(n), c->lidx, c->tile_member, c->moff, c->mlc, 0,
+                     c->nslot);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));  // the host buffer is reused by the next call
+  return EFDC_XM_OK;
+}
+
+int download_packed(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
+  const size_t L = size_t(c->stage_len), n = xs.size();
+  for (size_t j = 0; j < n; ++j)
+    c->jobs_h[j] = CopyJob{reinterpret_cast<double *>(c->pack_d + j * L * sizeof(double)),
+                           xs[j].dev, xs[j].kind};
+  const size_t bytes = n * L * sizeof(double);
+  CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, n * sizeof(CopyJob), cudaMemcpyHostToDevice,
+                     c->stream));
+  xm::launch_gather(c->stream, c->jobs_d, int(n), c->lidx, c->tile_member, c->moff, 0, c->nslot);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(c->pack_h, c->pack_d, bytes, cudaMemcpyDeviceToHost, c->stream));
+  g_d2h.fetch_add(static_cast<long long>(bytes), std::memory_order_relaxed);
+  CK(cudaStreamSynchronize(c->stream));
+  for (size_t j = 0; j < n; ++j) {  // the water elements L = 2..LA of each member
+    const size_t es = esize(xs[j].kind);
+    const char *src = c->pack_h + j * L * sizeof(double);
+    for (int m = 0; m < c->M; ++m)
+      if (xs[j].host[m])
+        std::memcpy(static_cast<char *>(const_cast<void *>(xs[j].host[m])) + es,
+                    src + size_t(c->mem[m].off + 1) * es, size_t(c->mem[m].la - 1) * es);
+  }
+  return EFDC_XM_OK;
+}
+
 int upload_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
   if (xs.empty()) return EFDC_XM_OK;
   if (xs.size() > size_t(MAX_JOBS)) {
     set_error("internal: too many arrays in one transfer");
     return EFDC_XM_CUDA_ERROR;
   }
+  if (packed(c, xs.size())) return upload_packed(c, xs);
   for (size_t j = 0; j < xs.size(); ++j)
     c->jobs_h[j] = CopyJob{c->stage[j % NSTAGE], xs[j].dev, xs[j].kind};
   CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, xs.size() * sizeof(CopyJob), cudaMemcpyHostToDevice,
@@ -414,6 +505,7 @@ int download_arrays(efdc_xm_ctx *c, const std::vector<Xfer> &xs) {
     set_error("internal: too many arrays in one transfer");
     return EFDC_XM_CUDA_ERROR;
   }
+  if (packed(c, xs.size())) return download_packed(c, xs);
   for (size_t j = 0; j < xs.size(); ++j)
     c->jobs_h[j] = CopyJob{c->stage[j % NSTAGE], xs[j].dev, xs[j].kind};
   CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, xs.size() * sizeof(CopyJob), cudaMemcpyHostToDevice,
@@ -582,7 +674,8 @@ int solve_fp64(efdc_xm_ctx *c, double *P) {
 }
 
 constexpr int MAX_OUTER = 30;        // MIXED refinement passes per solve
-constexpr double INNER_REL_TOL = 1e-6;  // inner: |r| down 1e-6 at least (FP32 reaches ~1e-7)
+// inner: |r| down by at least 10^(-inner_tol_x10/10) (default 1e-6; FP32 reaches ~1e-7)
+double inner_rel_tol(const efdc_xm_ctx *c) { return std::pow(10.0, -0.1 * c->inner_tol_x10); }
 
 // MIXED: each member's inner preconditioner for the next solve, and the kinds
 // of inner solve the launches need; uploads the choice.  The Neumann
@@ -621,7 +714,7 @@ int solve_mixed(efdc_xm_ctx *c, double *P, double factor) {
   for (int o = 0; o < MAX_OUTER; ++o) {
     xm::launch_outer_reset(lk, c->glob);
     xm::launch_mx_resid(lk, c->S, c->mxview, c->Y, P, c->ctl, c->glob, c->part, fac,
-                        INNER_REL_TOL, 0);
+                        inner_rel_tol(c), 0);
     CK(cudaGetLastError());
     if ((rc = read_glob(c))) return rc;
     if (c->glob_h->ndone >= c->M) break;
@@ -814,6 +907,8 @@ void efdc_xm_destroy(efdc_xm_ctx *c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (auto &b : c->bufs) cudaFree(b.p);
+  if (c->mom_lists) cudaFree(c->mom_lists);
+  if (c->pack_h) cudaFreeHost(c->pack_h);
   void *pinned[] = {c->ctl_h, c->glob_h, c->act_h, c->mpoly_h, c->sc_h, c->jobs_h, c->pser_h};
   for (void *p : pinned)
     if (p) cudaFreeHost(p);
@@ -1005,6 +1100,15 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
         }
         kind[slot_of[m][L]] = xm::OPENBC;
         if (o.ispb[ll] == 1 || o.ispb[ll] == 2) mb.may_asym = true;
+        if (o.ispb[ll] == 2) {
+          // W: the cell after L in the numbering; S: L's north neighbour
+          const int Lm = s == 0 ? L + 1 : s == 2 ? g->lnc[L - 1] : L;
+          if (Lm >= 2 && Lm <= mb.la) {
+            const int nb2 = s == 0 ? g->lnc[Lm - 1] : s == 1 ? g->lwc[Lm - 1]
+                            : s == 2 ? g->lec[Lm - 1] : g->lsc[Lm - 1];
+            mb.t2.push_back(int4{s, Lm, nb2, 0});
+          }
+        }
         // hazard: a ghost or boundary-cell target, or a target shared by two
         // boundary cells, needs the reference's serial loop order
         if (nbL == mb.lc || bcells.count(nbL) || !targets.insert(nbL).second) c->obc_serial = true;
@@ -1808,7 +1912,7 @@ cudaError_t capture_solve(efdc_xm_ctx *c, const StepPlan &pl, int d, StepGraph &
   lo.stream = c->cap_stream[d + 1];
   xm::launch_outer_reset(lo, c->glob);
   xm::launch_mx_resid(lo, c->S, c->mxview, c->Y, P, c->ctl, c->glob, c->part, pl.fac,
-                      INNER_REL_TOL, 0);
+                      inner_rel_tol(c), 0);
   CKG(cond_handle(lo.stream, &hi));
   xm::launch_loop_enter(lo.stream, c->glob, xm::LOOP_INNER, hi, 1, M);
   take_count(mark, &sg.n_body[xm::LOOP_OUTER]);
@@ -3169,6 +3273,417 @@ int32_t efdc_xm_bottom_stress_batch(efdc_xm_ctx *c, const efdc_xm_drag_params *p
   return download_arrays(c, dn);
 }
 
+// Arrays of one member into tile order: its slots and its ghost tile (which
+// takes element LC), NSTAGE arrays per round through the staging buffers.
+int upload_member(efdc_xm_ctx *c, int member, const std::vector<Xfer> &xs) {
+  const Member &mb = c->mem[member];
+  const int d0 = (mb.tile0 - 1) * xm::TILE, d1 = mb.tile1 * xm::TILE;
+  for (size_t g0 = 0; g0 < xs.size(); g0 += NSTAGE) {
+    const size_t g1 = std::min(xs.size(), g0 + NSTAGE);
+    for (size_t j = g0; j < g1; ++j)
+      c->jobs_h[j - g0] = CopyJob{c->stage[j - g0], xs[j].dev, xs[j].kind};
+    CK(cudaMemcpyAsync(c->jobs_d, c->jobs_h, (g1 - g0) * sizeof(CopyJob),
+                       cudaMemcpyHostToDevice, c->stream));
+    int rc = copies_after_compute(c), k = 0;
+    for (size_t j = g0; !rc && j < g1; ++j)
+      rc = h2d_range(c, xs[j], reinterpret_cast<char *>(c->stage[j - g0]), member, member + 1,
+                     c->copy_stream, k);
+    if (!rc) rc = compute_after_copies(c);
+    if (rc) return rc;
+    xm::launch_scatter(c->stream, c->jobs_d, int(g1 - g0), c->lidx, c->tile_member, c->moff,
+                       c->mlc, d0, d1);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));  // the staging buffers and jobs are reused
+  }
+  return EFDC_XM_OK;
+}
+
+// Per-layer arrays as transfers: layer k of member m at host[m] + k*ld[m].
+void layer_xfers(std::vector<Xfer> &out, const std::vector<const double *> &host,
+                 const std::vector<int> &ld, double *dev, size_t ls, int kc) {
+  for (int k = 0; k < kc; ++k) {
+    std::vector<const void *> v(host.size());
+    for (size_t m = 0; m < host.size(); ++m)
+      v[m] = host[m] ? static_cast<const void *>(host[m] + size_t(k) * ld[m]) : nullptr;
+    out.push_back(Xfer{v, dev + size_t(k) * ls, 0});
+  }
+}
+
+int32_t efdc_xm_set_momentum(efdc_xm_ctx *c, int32_t member, const efdc_xm_momentum *mo) {
+  if (!c || !mo || member < 0 || member >= c->M) {
+    set_error("efdc_xm_set_momentum: need a context, a member index and the static part");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  const Member &mb = c->mem[member];
+  if (mo->kc < 1 || mo->kc > 64 || mo->ld < mb.lc || !mo->fcorc || !mo->dydi || !mo->dxdj ||
+      !mo->scax || !mo->scay || !mo->saax || !mo->saay || !mo->sgzu || !mo->sgzv || !mo->fsgzu ||
+      !mo->fsgzv || !mo->lnwc || !mo->lsec || mo->nbcs < 0 ||
+      (mo->nbcs > 0 && (!mo->lbcs || !mo->lberc || !mo->lbnrc)) || (!mo->sdx != !mo->sdy) ||
+      (mo->sdx && !mo->lhdmf)) {
+    set_error("efdc_xm_set_momentum: member %d: need 1 <= KC <= 64, LD >= LC, FCORC, DYDI, "
+              "DXDJ, SCAX, SCAY, SAAX, SAAY, the SGZU, SGZV, FSGZU, FSGZV layers, LNWC, LSEC, "
+              "the NBCS boundary lists, and SDX with SDY and LHDMF or none", member);
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  if (c->mom_alloc && mo->kc > c->mom_kc) {
+    set_error("efdc_xm_set_momentum: member %d has KC = %d, more than the %d layers of the "
+              "context's first member with momentum", member, mo->kc, c->mom_kc);
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  for (const int32_t *a : {mo->lnwc, mo->lsec})
+    for (int L = 2; L <= mb.la; ++L)
+      if (a[L - 1] < 1 || a[L - 1] > mb.lc) {
+        set_error("efdc_xm_set_momentum: member %d: LNWC/LSEC(%d) = %d is outside 1..LC", member,
+                  L, a[L - 1]);
+        return EFDC_XM_BAD_ARGUMENT;
+      }
+  for (int j = 0; j < mo->nbcs; ++j)
+    for (const int32_t *a : {mo->lbcs, mo->lberc, mo->lbnrc})
+      if (a[j] > mb.lc) {
+        set_error("efdc_xm_set_momentum: member %d: a boundary list entry %d exceeds LC", member,
+                  a[j]);
+        return EFDC_XM_BAD_ARGUMENT;
+      }
+  CK(cudaSetDevice(c->device));
+  const int M = c->M;
+  const size_t ns = size_t(c->nslot);
+  xm::MomDev &D = c->md;
+  if (!c->mom_alloc) {  // zeroed: land slots and cells outside the wet set stay 0
+    const int kc = mo->kc;
+    c->mom_kc = kc;
+    auto A = [&](size_t n) { return c->alloc<double>(n); };
+    double *st[10];
+    for (double *&q : st) q = A(ns);
+    int *in[4];
+    for (int *&q : in) q = c->alloc<int>(ns);
+    double *ly[23];
+    for (double *&q : ly) q = A(ns * kc);
+    c->mom_hp = A(ns);
+    D.cacsum = A(size_t(M));
+    xm::MomScalars *sc = c->alloc<xm::MomScalars>(size_t(M));
+    for (double *q : st) if (!q) sc = nullptr;
+    for (int *q : in) if (!q) sc = nullptr;
+    for (double *q : ly) if (!q) sc = nullptr;
+    if (!sc || !c->mom_hp || !D.cacsum) {
+      set_error("efdc_xm_set_momentum: device allocation failed (%d layers)", kc);
+      return EFDC_XM_CUDA_ERROR;
+    }
+    D.fcorc = st[0]; D.dydi = st[1]; D.dxdj = st[2]; D.scax = st[3]; D.scay = st[4];
+    D.saax = st[5]; D.saay = st[6]; D.stcuv = st[7]; D.sdx = st[8]; D.sdy = st[9];
+    D.lhdmf = in[0]; D.nw = in[1]; D.se = in[2]; D.wet = in[3];
+    D.sgzu = ly[0]; D.sgzv = ly[1]; D.fsgzu = ly[2]; D.fsgzv = ly[3];
+    D.u = ly[4]; D.v = ly[5]; D.uhdy = ly[6]; D.vhdx = ly[7]; D.fuhj = ly[8]; D.fvhj = ly[9];
+    D.fmdux = ly[10]; D.fmduy = ly[11]; D.fmdvx = ly[12]; D.fmdvy = ly[13];
+    D.fuhu = ly[14]; D.fvhu = ly[15]; D.fvhv = ly[16]; D.fuhv = ly[17]; D.cac = ly[18];
+    D.fcax = ly[19]; D.fcay = ly[20]; D.fx = ly[21]; D.fy = ly[22];
+    D.sc = sc;
+    D.ls = ns;
+    c->has_mom.assign(M, 0);
+    c->mom_ld.assign(M, 0);
+    c->mom_t2.assign(M, {});
+    c->mom_bc.assign(M, {});
+    c->mom_sc_h.assign(M, xm::MomScalars{});
+    CK(cudaDeviceSynchronize());  // the zeroing ran on the legacy stream
+    c->mom_alloc = true;
+  }
+  const int kc = mo->kc;
+  auto one = [&](const void *a) {
+    std::vector<const void *> v(M, nullptr);
+    v[member] = a;
+    return v;
+  };
+  std::vector<Xfer> xs = {
+      Xfer{one(mo->fcorc), const_cast<double *>(D.fcorc), 0},
+      Xfer{one(mo->dydi), const_cast<double *>(D.dydi), 0},
+      Xfer{one(mo->dxdj), const_cast<double *>(D.dxdj), 0},
+      Xfer{one(mo->scax), const_cast<double *>(D.scax), 0},
+      Xfer{one(mo->scay), const_cast<double *>(D.scay), 0},
+      Xfer{one(mo->saax), const_cast<double *>(D.saax), 0},
+      Xfer{one(mo->saay), const_cast<double *>(D.saay), 0}};
+  if (mo->stcuv) xs.push_back(Xfer{one(mo->stcuv), const_cast<double *>(D.stcuv), 0});
+  if (mo->sdx) {
+    xs.push_back(Xfer{one(mo->sdx), const_cast<double *>(D.sdx), 0});
+    xs.push_back(Xfer{one(mo->sdy), const_cast<double *>(D.sdy), 0});
+    xs.push_back(Xfer{one(mo->lhdmf), const_cast<int *>(D.lhdmf), 1});
+  }
+  std::vector<const double *> h(M, nullptr);
+  std::vector<int> ld(M, 0);
+  ld[member] = mo->ld;
+  const double *const lay[4] = {mo->sgzu, mo->sgzv, mo->fsgzu, mo->fsgzv};
+  const double *const dl[4] = {D.sgzu, D.sgzv, D.fsgzu, D.fsgzv};
+  for (int a = 0; a < 4; ++a) {
+    h[member] = lay[a];
+    layer_xfers(xs, h, ld, const_cast<double *>(dl[a]), D.ls, kc);
+  }
+  int rc = upload_member(c, member, xs);
+  if (rc) return rc;
+  // the diagonal neighbours' slots (LC: the member's ghost slot)
+  auto slot = [&](int L) { return (L >= 2 && L <= mb.la) ? mb.slot_of[L] : (mb.tile0 - 1) * xm::TILE; };
+  {
+    std::vector<int> idx, nw, se;
+    for (int L = 2; L <= mb.la; ++L) {
+      idx.push_back(mb.slot_of[L]);
+      nw.push_back(slot(mo->lnwc[L - 1]));
+      se.push_back(slot(mo->lsec[L - 1]));
+    }
+    const size_t n = idx.size();
+    int *t = nullptr;
+    CK(cudaMalloc(&t, std::max<size_t>(1, 3 * n) * sizeof(int)));
+    cudaError_t e = cudaMemcpy(t, idx.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(t + n, nw.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(t + 2 * n, se.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      xm::launch_put_int(c->stream, t, t + n, int(n), const_cast<int *>(D.nw));
+      xm::launch_put_int(c->stream, t, t + 2 * n, int(n), const_cast<int *>(D.se));
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    }
+    cudaFree(t);
+    CK(e);
+  }
+  // the serial lists: type-2 boundaries (with LNWC, LSEC) and flow-boundary edges
+  std::vector<int4> &t2 = c->mom_t2[member], &bc = c->mom_bc[member];
+  t2.clear();
+  for (const int4 &e : mb.t2) {
+    const int L = e.y;
+    const int b = e.x == 1 ? slot(mo->lnwc[L - 1]) : e.x == 3 ? slot(mo->lsec[L - 1]) : 0;
+    t2.push_back(int4{e.x, mb.slot_of[L], slot(e.z), b});
+  }
+  bc.clear();
+  auto wslot = [&](int L) { return (L >= 2 && L <= mb.la) ? mb.slot_of[L] : -1; };
+  for (int j = 0; j < mo->nbcs; ++j)
+    bc.push_back(int4{wslot(mo->lbcs[j]), wslot(std::max(1, mo->lberc[j])),
+                      wslot(std::max(1, mo->lbnrc[j])), 0});
+  c->has_mom[member] = 1;
+  c->mom_ld[member] = mo->ld;
+  xm::MomScalars &q = c->mom_sc_h[member];
+  q.kc = kc;
+  q.tri = mo->stcuv ? 1 : 0;
+  q.hdmf = mo->sdx ? 1 : 0;  // may diffuse; each call's ISHDMF decides
+  // the lists move to the device with the next call
+  if (c->mom_lists) {
+    cudaFree(c->mom_lists);
+    c->mom_lists = nullptr;
+  }
+  c->md.t2 = nullptr;
+  return EFDC_XM_OK;
+}
+
+int32_t efdc_xm_explicit_batch(efdc_xm_ctx *c, const efdc_xm_explicit_params *prm,
+                               efdc_xm_explicit_fields *f) {
+  if (!c || !prm || !f) {
+    set_error("efdc_xm_explicit_batch: NULL argument");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  const int M = c->M;
+  // U, V, UHDY, VHDX NULL in every member: the previous call's, still on the device
+  bool reuse = true;
+  for (int m = 0; m < M; ++m) reuse &= !f[m].u && !f[m].v && !f[m].uhdy && !f[m].vhdx;
+  if (reuse && !c->mom_inputs) {
+    set_error("efdc_xm_explicit_batch: no U, V, UHDY, VHDX on the device yet");
+    return EFDC_XM_BAD_ARGUMENT;
+  }
+  for (int m = 0; m < M; ++m) {
+    const efdc_xm_explicit_fields &x = f[m];
+    if (!c->mom_alloc || !c->has_mom[m] || (!reuse && (!x.u || !x.v || !x.uhdy || !x.vhdx)) ||
+        (!x.fuhj != !x.fvhj)) {
+      set_error("efdc_xm_explicit_batch: member %d: needs its static part "
+                "(efdc_xm_set_momentum), U, V, UHDY, VHDX, and FUHJ with FVHJ or neither", m);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+    if (prm[m].ishdmf >= 1 && (!c->mom_sc_h[m].hdmf || !x.fmdux || !x.fmduy || !x.fmdvx ||
+                               !x.fmdvy)) {
+      set_error("efdc_xm_explicit_batch: member %d has ISHDMF >= 1: needs SDX, SDY, LHDMF in "
+                "its static part and FMDUX, FMDUY, FMDVX, FMDVY", m);
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+    if ((!x.hp) != (!f[0].hp) || (!x.wet) != (!f[0].wet) || (!x.fuhj) != (!f[0].fuhj)) {
+      set_error("efdc_xm_explicit_batch: HP, WET and FUHJ are given for all members or none");
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+  }
+  CK(cudaSetDevice(c->device));
+  xm::MomDev &D = c->md;
+  if (!D.t2) {  // the serial lists, packed per member
+    std::vector<int4> t2, bc;
+    std::vector<int> t2s(M + 1, 0), bcs(M + 1, 0);
+    for (int m = 0; m < M; ++m) {
+      t2s[m] = int(t2.size());
+      bcs[m] = int(bc.size());
+      t2.insert(t2.end(), c->mom_t2[m].begin(), c->mom_t2[m].end());
+      bc.insert(bc.end(), c->mom_bc[m].begin(), c->mom_bc[m].end());
+    }
+    t2s[M] = int(t2.size());
+    bcs[M] = int(bc.size());
+    const size_t n4 = std::max<size_t>(1, t2.size()) + std::max<size_t>(1, bc.size());
+    void *buf = nullptr;
+    CK(cudaMalloc(&buf, n4 * sizeof(int4) + 2 * size_t(M + 1) * sizeof(int)));
+    c->mom_lists = buf;
+    int4 *t2d = static_cast<int4 *>(buf);
+    int *sd = reinterpret_cast<int *>(t2d + n4);
+    int4 *bcd = t2d + std::max<size_t>(1, t2.size());
+    if (!t2.empty()) CK(cudaMemcpy(t2d, t2.data(), t2.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    if (!bc.empty()) CK(cudaMemcpy(bcd, bc.data(), bc.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(sd, t2s.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(sd + M + 1, bcs.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    D.t2 = t2d;
+    D.bc = bcd;
+    D.t2start = sd;
+    D.bcstart = sd + M + 1;
+  }
+  // the call's inputs
+  std::vector<Xfer> xs;
+  int kcmax = 1;
+  for (int m = 0; m < M; ++m) {
+    xm::MomScalars &q = c->mom_sc_h[m];
+    q.snlt = prm[m].snlt;
+    q.on = 1;
+    q.curv = prm[m].iscurvature != 0;
+    q.fuhj = f[m].fuhj ? 1 : 0;
+    q.hdmf = (prm[m].ishdmf >= 1 && c->mom_sc_h[m].hdmf) ? 1 : 0;
+    kcmax = std::max(kcmax, q.kc);
+  }
+  auto per = [&](const double *efdc_xm_explicit_fields::*a) {
+    std::vector<const double *> v(M);
+    for (int m = 0; m < M; ++m) v[m] = f[m].*a;
+    return v;
+  };
+  std::vector<Xfer> layers;
+  if (!reuse) {
+    layer_xfers(layers, per(&efdc_xm_explicit_fields::u), c->mom_ld, const_cast<double *>(D.u), D.ls, kcmax);
+    layer_xfers(layers, per(&efdc_xm_explicit_fields::v), c->mom_ld, const_cast<double *>(D.v), D.ls, kcmax);
+    layer_xfers(layers, per(&efdc_xm_explicit_fields::uhdy), c->mom_ld, const_cast<double *>(D.uhdy), D.ls, kcmax);
+    layer_xfers(layers, per(&efdc_xm_explicit_fields::vhdx), c->mom_ld, const_cast<double *>(D.vhdx), D.ls, kcmax);
+  }
+  if (f[0].fuhj) {
+    layer_xfers(layers, per(&efdc_xm_explicit_fields::fuhj), c->mom_ld, const_cast<double *>(D.fuhj), D.ls, kcmax);
+    layer_xfers(layers, per(&efdc_xm_explicit_fields::fvhj), c->mom_ld, const_cast<double *>(D.fvhj), D.ls, kcmax);
+  }
+  bool any_hdmf = false;
+  for (int m = 0; m < M; ++m) any_hdmf |= c->mom_sc_h[m].hdmf != 0;
+  if (any_hdmf) {
+    using In = const double *efdc_xm_explicit_fields::*;
+    const In fm[4] = {
+        &efdc_xm_explicit_fields::fmdux, &efdc_xm_explicit_fields::fmduy,
+        &efdc_xm_explicit_fields::fmdvx, &efdc_xm_explicit_fields::fmdvy};
+    const double *dv[4] = {D.fmdux, D.fmduy, D.fmdvx, D.fmdvy};
+    for (int a = 0; a < 4; ++a) {
+      std::vector<const double *> v = per(fm[a]);
+      for (int m = 0; m < M; ++m)
+        if (!c->mom_sc_h[m].hdmf) v[m] = nullptr;
+      layer_xfers(layers, v, c->mom_ld, const_cast<double *>(dv[a]), D.ls, kcmax);
+    }
+  }
+  // a member with fewer layers gives no array for the upper ones
+  for (Xfer &x : layers) {
+    bool any = false;
+    for (const void *p : x.host) any |= p != nullptr;
+    if (any) xs.push_back(x);
+  }
+  xm::MomDev Dc = D;  // this call's view
+  if (f[0].hp) {
+    std::vector<const void *> v(M);
+    for (int m = 0; m < M; ++m) v[m] = f[m].hp;
+    xs.push_back(Xfer{v, c->mom_hp, 0});
+    Dc.hp = c->mom_hp;
+  } else {
+    Dc.hp = c->X.hp;  // the HP the last step left
+  }
+  if (f[0].wet) {
+    std::vector<const void *> v(M);
+    for (int m = 0; m < M; ++m) v[m] = f[m].wet;
+    xs.push_back(Xfer{v, const_cast<int *>(D.wet), 1});
+  } else {
+    Dc.wet = nullptr;
+  }
+  // a member with fewer layers than another moves only its own: the per-member
+  // transfers of a field must all be given, so the upper layers go member-wise
+  int rc = 0;
+  {
+    std::vector<Xfer> full, partial;
+    for (const Xfer &x : xs) {
+      int n = 0;
+      for (const void *p : x.host) n += p ? 1 : 0;
+      (n == M ? full : partial).push_back(x);
+    }
+    for (size_t g0 = 0; !rc && g0 < full.size(); g0 += MAX_JOBS)
+      rc = upload_arrays(c, std::vector<Xfer>(full.begin() + g0,
+                                              full.begin() + std::min(full.size(), g0 + MAX_JOBS)));
+    for (int m = 0; !rc && m < M; ++m) {
+      std::vector<Xfer> mine;
+      for (const Xfer &x : partial)
+        if (x.host[m]) mine.push_back(x);
+      if (!mine.empty()) rc = upload_member(c, m, mine);
+    }
+  }
+  if (rc) return rc;
+  c->mom_inputs = true;
+  CK(cudaMemcpyAsync(const_cast<xm::MomScalars *>(D.sc), c->mom_sc_h.data(),
+                     sizeof(xm::MomScalars) * M, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(D.cacsum, 0, sizeof(double) * M, c->stream));
+  xm::launch_explicit(c->L(), c->S, Dc, c->X, kcmax, M);
+  CK(cudaGetLastError());
+  // the sums now differ from what the caller's arrays held
+  c->synced &= ~uint32_t(EFDC_XM_SAME_FCAXE | EFDC_XM_SAME_FCAYE | EFDC_XM_SAME_FXE |
+                         EFDC_XM_SAME_FYE);
+  std::vector<Xfer> dn;
+#define XM_DN(name, dev)                                                        \
+  {                                                                             \
+    std::vector<const void *> v(M);                                             \
+    for (int m = 0; m < M; ++m) v[m] = f[m].name;                               \
+    if ((rc = collect(c, dn, v, dev, 0, #name))) return rc;                     \
+  }
+  XM_DN(fcaxe, c->X.fcaxe) XM_DN(fcaye, c->X.fcaye) XM_DN(fxe, c->X.fxe) XM_DN(fye, c->X.fye)
+#undef XM_DN
+  auto per_out = [&](double *efdc_xm_explicit_fields::*a) {
+    std::vector<const double *> v(M);
+    for (int m = 0; m < M; ++m) v[m] = f[m].*a;
+    return v;
+  };
+  std::vector<Xfer> ldn;
+  using Out = double *efdc_xm_explicit_fields::*;
+  const Out outs[5] = {
+      &efdc_xm_explicit_fields::fcax, &efdc_xm_explicit_fields::fcay, &efdc_xm_explicit_fields::fx,
+      &efdc_xm_explicit_fields::fy, &efdc_xm_explicit_fields::cac};
+  double *devs[5] = {D.fcax, D.fcay, D.fx, D.fy, D.cac};
+  for (int a = 0; a < 5; ++a) {
+    std::vector<const double *> v = per_out(outs[a]);
+    int n = 0;
+    for (const double *p : v) n += p ? 1 : 0;
+    if (n == 0) continue;
+    if (n != M) {
+      set_error("efdc_xm_explicit_batch: a layer output is given for some members only");
+      return EFDC_XM_BAD_ARGUMENT;
+    }
+    for (int k = 0; k < kcmax; ++k) {  // members with fewer layers: below
+      std::vector<const void *> hv(M);
+      bool all = true;
+      for (int m = 0; m < M; ++m) {
+        hv[m] = k < c->mom_sc_h[m].kc ? static_cast<const void *>(v[m] + size_t(k) * c->mom_ld[m])
+                                      : nullptr;
+        all &= hv[m] != nullptr;
+      }
+      if (!all) {
+        set_error("efdc_xm_explicit_batch: layer outputs need the same KC in every member");
+        return EFDC_XM_BAD_ARGUMENT;
+      }
+      ldn.push_back(Xfer{hv, devs[a] + size_t(k) * D.ls, 0});
+    }
+  }
+  dn.insert(dn.end(), ldn.begin(), ldn.end());
+  for (size_t g0 = 0; !rc && g0 < dn.size(); g0 += MAX_JOBS)
+    rc = download_arrays(c, std::vector<Xfer>(dn.begin() + g0,
+                                              dn.begin() + std::min(dn.size(), g0 + MAX_JOBS)));
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  // the sums the caller received now equal the device's copies
+  const uint32_t got = (f[0].fcaxe ? EFDC_XM_SAME_FCAXE : 0u) | (f[0].fcaye ? EFDC_XM_SAME_FCAYE : 0u) |
+                       (f[0].fxe ? EFDC_XM_SAME_FXE : 0u) | (f[0].fye ? EFDC_XM_SAME_FYE : 0u);
+  c->synced |= got;
+  return EFDC_XM_OK;
+}
+
 int32_t efdc_xm_set_channels(efdc_xm_ctx *c, int32_t member, const efdc_xm_channels *ch) {
   if (!c || !ch || member < 0 || member >= (c ? c->M : 0) || ch->n < 0) {
     set_error("efdc_xm_set_channels: need a context, a member index and a channel struct");
@@ -3406,6 +3921,13 @@ int32_t efdc_xm_set_option(efdc_xm_ctx *c, int32_t option, int32_t value) {
       if (value < 0 || value > 6) break;
       if (value != c->inner_margin_log10) {
         c->inner_margin_log10 = value;
+        drop_graphs(c);
+      }
+      return EFDC_XM_OK;
+    case EFDC_XM_OPT_INNER_TOL:
+      if (value < 40 || value > 75) break;
+      if (value != c->inner_tol_x10) {
+        c->inner_tol_x10 = value;
         drop_graphs(c);
       }
       return EFDC_XM_OK;

@@ -218,6 +218,37 @@ struct DevBed {
   double *ub, *vb, *vu, *uv, *h1u, *h1v;    // U, V of the bottom layer, VU, UV, H1U, H1V
 };
 
+// Explicit momentum producer (CALEXP2T's external-mode terms): per-member
+// scalars of one call, and the device arrays in tile order.  Layer arrays
+// are [k][slot] with stride ls; per-slot int arrays hold 0/1 or slots.
+struct MomScalars {
+  double snlt;  // SNLT
+  int kc;       // layers of the member
+  int on;       // the member takes part (it has its static part)
+  int curv;     // ISCURVATURE
+  int tri;      // STCUV given (ITRICELL > 0)
+  int hdmf;     // ISHDMF >= 1
+  int fuhj;     // FUHJ, FVHJ given
+};
+
+struct MomDev {
+  const double *fcorc, *dydi, *dxdj, *scax, *scay, *saax, *saay, *stcuv, *sdx, *sdy;
+  const int *lhdmf;   // LHDMF as 0/1
+  const int *nw, *se; // slots of LNWC(L), LSEC(L) (the member's ghost slot for LC)
+  const double *sgzu, *sgzv, *fsgzu, *fsgzv;                   // static layers
+  const double *u, *v, *uhdy, *vhdx, *fuhj, *fvhj;             // per-call layers
+  const double *fmdux, *fmduy, *fmdvx, *fmdvy;
+  const double *hp;   // HP of the call (the step's HP when the caller gives none)
+  const int *wet;     // the wet set as 0/1
+  double *fuhu, *fvhu, *fvhv, *fuhv, *cac;                      // work layers
+  double *fcax, *fcay, *fx, *fy;                                // output layers
+  double *cacsum;     // [M] the members' sums of CAC
+  const MomScalars *sc;
+  const int4 *t2, *bc;            // the serial lists (see k_mom_edges)
+  const int *t2start, *bcstart;   // [M+1]
+  size_t ls;                      // layer stride (slots)
+};
+
 // Per-member scalars of one bottom-stress call.
 struct DragScalars {
   double delt, avcon1, avcon, vismud, visfac;

@@ -49,9 +49,14 @@ void launch_begin3(const Launch &l, const DevStatic &S, const DevState &X, const
 void launch_advance3(const Launch &l, const DevStatic &S, const DevState &X);
 // the implicit bottom / vegetation drag (RCX, RCY) of the members with ISITB >= 1
 // or ISVEG > 0, after the begin kernel
+// CALEXP2T's external-mode terms of every member with its static part; the
+// depth sums go to X.fcaxe, X.fcaye, X.fxe, X.fye.
+void launch_explicit(const Launch &l, const DevStatic &S, const MomDev &M, const DevState &X,
+                     int kcmax, int nmember);
 void launch_implicit_drag(const Launch &l, const DevStatic &S, const DevState &X,
                           const int *act);
 void launch_put(cudaStream_t st, const int *idx, const double *val, int n, double *dst);
+void launch_put_int(cudaStream_t st, const int *idx, const int *val, int n, int *dst);
 // sub-grid channels (xm_chan.cu); each does nothing unless l.chan
 void launch_chan_entry(const Launch &l, const DevStatic &S, const DevState &X, const int *act);
 void launch_chan_sub(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,

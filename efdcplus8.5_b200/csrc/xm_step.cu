@@ -1216,6 +1216,15 @@ void launch_put(cudaStream_t st, const int *idx, const double *val, int n, doubl
   k_put<<<std::min((n + 255) / 256, 4096), 256, 0, st>>>(idx, val, n, dst);
   count_launches(1);
 }
+__global__ void k_put_int(const int *idx, const int *val, int n, int *dst) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    dst[idx[i]] = val[i];
+}
+void launch_put_int(cudaStream_t st, const int *idx, const int *val, int n, int *dst) {
+  if (n <= 0) return;
+  k_put_int<<<std::min((n + 255) / 256, 4096), 256, 0, st>>>(idx, val, n, dst);
+  count_launches(1);
+}
 
 void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const int *act,
                   bool copy) {

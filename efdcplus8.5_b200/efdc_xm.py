@@ -112,6 +112,34 @@ DRAG_IN = ("ub", "vb", "vu", "uv", "h1u", "h1v")
 DRAG_OUT = ("stbx", "stby", "tbx", "tby")
 
 
+class Momentum(C.Structure):
+    _fields_ = [("kc", C.c_int32), ("ld", C.c_int32), ("fcorc", _pd), ("dydi", _pd),
+                ("dxdj", _pd), ("scax", _pd), ("scay", _pd), ("saax", _pd), ("saay", _pd),
+                ("sgzu", _pd), ("sgzv", _pd), ("fsgzu", _pd), ("fsgzv", _pd), ("stcuv", _pd),
+                ("sdx", _pd), ("sdy", _pd), ("lhdmf", _pi), ("lnwc", _pi), ("lsec", _pi),
+                ("nbcs", C.c_int32), ("pad_", C.c_int32), ("lbcs", _pi), ("lberc", _pi),
+                ("lbnrc", _pi)]
+
+
+class ExplicitParams(C.Structure):
+    _fields_ = [("snlt", C.c_double), ("iscurvature", C.c_int32), ("ishdmf", C.c_int32)]
+
+
+class ExplicitFields(C.Structure):
+    _fields_ = [("u", _pd), ("v", _pd), ("uhdy", _pd), ("vhdx", _pd), ("hp", _pd),
+                ("wet", _pi), ("fuhj", _pd), ("fvhj", _pd), ("fmdux", _pd), ("fmduy", _pd),
+                ("fmdvx", _pd), ("fmdvy", _pd), ("fcaxe", _pd), ("fcaye", _pd), ("fxe", _pd),
+                ("fye", _pd), ("fcax", _pd), ("fcay", _pd), ("fx", _pd), ("fy", _pd),
+                ("cac", _pd)]
+
+
+MOM_D = ("fcorc", "dydi", "dxdj", "scax", "scay", "saax", "saay", "sgzu", "sgzv", "fsgzu",
+         "fsgzv", "stcuv", "sdx", "sdy")
+MOM_I = ("lhdmf", "lnwc", "lsec", "lbcs", "lberc", "lbnrc")
+EXP_IN = ("u", "v", "uhdy", "vhdx", "hp", "fuhj", "fvhj", "fmdux", "fmduy", "fmdvx", "fmdvy")
+EXP_OUT = ("fcaxe", "fcaye", "fxe", "fye", "fcax", "fcay", "fx", "fy", "cac")
+
+
 class Channels(C.Structure):
     _fields_ = [("n", C.c_int32), ("type", _pi), ("lhost", _pi), ("lu", _pi), ("lv", _pi),
                 ("chanlen", _pd), ("chanfric", _pd), ("dxp", _pd), ("dyp", _pd)]
@@ -282,6 +310,50 @@ def make_drag_fields(d: dict):
     return s
 
 
+def make_momentum(mo: dict):
+    """A Momentum struct over a dict: kc, ld and the arrays of MOM_D (float64;
+    the layer ones sgzu, sgzv, fsgzu, fsgzv as [kc, ld] C-order = Fortran
+    (ld, kc)) and MOM_I (int32); stcuv, sdx, sdy, lhdmf may be absent.
+    Returns (struct, kept arrays)."""
+    s = Momentum()
+    keep = []
+    s.kc = int(mo["kc"])
+    s.ld = int(mo["ld"])
+    for k in MOM_D:
+        if mo.get(k) is not None:
+            a = np.ascontiguousarray(mo[k], dtype=np.float64)
+            keep.append(a)
+            setattr(s, k, _dp(a))
+    for k in MOM_I:
+        if mo.get(k) is not None:
+            a = np.ascontiguousarray(mo[k], dtype=np.int32)
+            keep.append(a)
+            setattr(s, k, _ip(a))
+    s.nbcs = int(len(mo["lbcs"])) if mo.get("lbcs") is not None else 0
+    return s, keep
+
+
+def make_explicit_params(snlt=1.0, iscurvature=1, ishdmf=0):
+    return ExplicitParams(snlt=float(snlt), iscurvature=int(iscurvature), ishdmf=int(ishdmf))
+
+
+def make_explicit_fields(d: dict):
+    """An ExplicitFields struct over the arrays of d (EXP_IN in, EXP_OUT out,
+    "wet" int32); absent keys are NULL.  Returns (struct, kept arrays)."""
+    s = ExplicitFields()
+    keep = []
+    for k in EXP_IN + EXP_OUT:
+        a = d.get(k)
+        if a is not None:
+            assert a.dtype == np.float64 and a.flags.c_contiguous, k
+            setattr(s, k, _dp(a))
+    if d.get("wet") is not None:
+        w = np.ascontiguousarray(d["wet"], dtype=np.int32)
+        keep.append(w)
+        s.wet = _ip(w)
+    return s, keep
+
+
 def make_channels(ch: dict | None):
     """A Channels struct over a dict of numpy arrays (type, lhost, lu, lv:
     int32; chanlen, chanfric: float64 per channel; dxp, dyp: float64 over
@@ -358,6 +430,7 @@ OPT_CTAS_MATVEC = 4
 OPT_CTAS_UPDATE = 5
 OPT_POLY_THRESHOLD = 6
 OPT_INNER_MARGIN = 7
+OPT_INNER_TOL = 8
 
 
 TUNE_MEASURE = 1
@@ -496,6 +569,11 @@ def load(path: str | os.PathLike | None = None):
     lib.efdc_xm_bottom_stress_batch.restype = C.c_int32
     lib.efdc_xm_bottom_stress_batch.argtypes = [C.c_void_p, C.POINTER(DragParams),
                                                 C.POINTER(DragFields)]
+    lib.efdc_xm_set_momentum.restype = C.c_int32
+    lib.efdc_xm_set_momentum.argtypes = [C.c_void_p, C.c_int32, C.POINTER(Momentum)]
+    lib.efdc_xm_explicit_batch.restype = C.c_int32
+    lib.efdc_xm_explicit_batch.argtypes = [C.c_void_p, C.POINTER(ExplicitParams),
+                                           C.POINTER(ExplicitFields)]
     if path is None:
         _lib = lib
     return lib
@@ -591,6 +669,22 @@ class Solver:
         rc = self.lib.efdc_xm_bottom_stress_batch(self.ctx, C.byref(params), C.byref(f))
         if rc != OK:
             raise RuntimeError(f"efdc_xm_bottom_stress_batch: {STATUS_NAMES.get(rc, rc)}: "
+                               f"{self.last_error()}")
+
+    def set_momentum(self, mo: dict, member: int = 0):
+        s, _keep = make_momentum(mo)
+        rc = self.lib.efdc_xm_set_momentum(self.ctx, member, C.byref(s))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_set_momentum: {STATUS_NAMES.get(rc, rc)}: "
+                               f"{self.last_error()}")
+
+    def explicit(self, params: ExplicitParams, fields: dict):
+        """CALEXP2T's external-mode terms on the device (efdc_xm_explicit_batch);
+        the outputs present in `fields` are written."""
+        f, _keep = make_explicit_fields(fields)
+        rc = self.lib.efdc_xm_explicit_batch(self.ctx, C.byref(params), C.byref(f))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_explicit_batch: {STATUS_NAMES.get(rc, rc)}: "
                                f"{self.last_error()}")
 
     def set_channels(self, ch: dict | None, member: int = 0):
@@ -737,6 +831,22 @@ class BatchSolver:
         rc = self.lib.efdc_xm_bottom_stress_batch(self.ctx, pa, fa)
         if rc != OK:
             raise RuntimeError(f"efdc_xm_bottom_stress_batch: {STATUS_NAMES.get(rc, rc)}: "
+                               f"{self.last_error()}")
+
+    def set_momentum(self, mo: dict, member: int):
+        s, _keep = make_momentum(mo)
+        rc = self.lib.efdc_xm_set_momentum(self.ctx, member, C.byref(s))
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_set_momentum: {STATUS_NAMES.get(rc, rc)}: "
+                               f"{self.last_error()}")
+
+    def explicit(self, params: list, fields: list):
+        made = [make_explicit_fields(d) for d in fields]
+        fa = (ExplicitFields * self.m)(*[x[0] for x in made])
+        pa = (ExplicitParams * self.m)(*params)
+        rc = self.lib.efdc_xm_explicit_batch(self.ctx, pa, fa)
+        if rc != OK:
+            raise RuntimeError(f"efdc_xm_explicit_batch: {STATUS_NAMES.get(rc, rc)}: "
                                f"{self.last_error()}")
 
     def set_channels(self, ch: dict | None, member: int):

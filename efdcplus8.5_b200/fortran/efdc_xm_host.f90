@@ -28,6 +28,9 @@ MODULE EFDC_XM_HOST
   REAL(C_DOUBLE), SAVE, ALLOCATABLE, TARGET :: PSERW(:), PSERE(:), PSERS(:), PSERN(:)
   INTEGER(C_INT32_T), SAVE, ALLOCATABLE, TARGET :: LMASKI(:), ISCDRYI(:), LOBCDRYI(:)
   REAL(C_DOUBLE), SAVE, ALLOCATABLE, TARGET :: UBOTI(:), VBOTI(:)
+  ! set by the CALEXP2T drop-in: FCAXE, FCAYE, FXE, FYE hold what the library
+  ! computed and returned, so the next step passes them as unchanged
+  LOGICAL, SAVE :: XM_SUMS_ON_DEVICE = .FALSE.
 
 CONTAINS
 
@@ -216,7 +219,10 @@ CONTAINS
       FLD%STBX = C_NULL_PTR; FLD%STBY = C_NULL_PTR
       FLD%FXVEGE = C_NULL_PTR; FLD%FYVEGE = C_NULL_PTR
     ENDIF
-    FLD%UNCHANGED = 0    ! every array is sent each step
+    FLD%UNCHANGED = 0    ! every array is sent each step, but the sums of the CALEXP2T drop-in
+    IF( XM_SUMS_ON_DEVICE ) FLD%UNCHANGED = IOR(IOR(EFDC_XM_SAME_FCAXE, EFDC_XM_SAME_FCAYE), &
+                                                IOR(EFDC_XM_SAME_FXE, EFDC_XM_SAME_FYE))
+    XM_SUMS_ON_DEVICE = .FALSE.
     FLD%PAD_U_ = 0
   END SUBROUTINE XM_FIELDS
 

@@ -738,6 +738,122 @@ def add_implicit_drag(scn: Scenario, isitb: int = 1, *, isveg: int = 0, seed: in
     return scn
 
 
+def add_momentum(scn: Scenario, kc: int = 1, *, seed: int = 0, lat: float = 45.0,
+                 tri: bool = False, hdmf: bool = False, nbcs: int = 8,
+                 type2: tuple = ()) -> dict:
+    """The static part of the explicit momentum producer (efdc_xm_set_momentum)
+    for a scenario, as ``scn.momentum``: the f-plane Coriolis parameter at
+    ``lat`` times nothing else (FCORC), seeded curvature metrics DYDI, DXDJ of
+    a gently curvilinear grid (+-2 % of the cell sizes), SCAX, SCAY = 1 and
+    SAAX, SAAY = 1 except on the flow-boundary cells, ``kc`` equal sigma
+    layers (SGZU = SGZV = 1/kc, FSGZU = FSGZV = kc), the NW and SE diagonal
+    cells LNWC, LSEC from the cell coordinates (LC where land), ``nbcs``
+    flow-boundary cells (the open-boundary cells first, then seeded interior
+    cells) with their E/W and N/S adjacent cells (1 where none), and, with
+    ``tri``, a seeded 0/1 STCUV, with ``hdmf``, SDX, SDY and LHDMF.  The open-
+    boundary sides in ``type2`` get ISPBW.. = 2 (their open-boundary cells
+    take CALEXP2T's type-2 forms)."""
+    rng = np.random.default_rng(seed + 11)
+    g = scn.grid
+    la, lc, lcm = scn.la, scn.lc, scn.lc + 1
+    i0 = np.arange(1, la)
+    for side in type2:
+        g["obc"][side]["ispb"][:] = 2
+
+    def cellf(vals):
+        a = np.zeros(lcm)
+        a[i0] = vals
+        return a
+
+    il, jl = g["il"][i0].astype(np.int64), g["jl"][i0].astype(np.int64)
+    at = np.full((int(il.max()) + 3, int(jl.max()) + 3), lc, np.int32)  # cell (i, j) -> L
+    at[il + 1, jl + 1] = np.arange(2, la + 1, dtype=np.int32)
+    lnwc = np.full(lcm, lc, np.int32)
+    lsec = np.full(lcm, lc, np.int32)
+    lnwc[i0] = at[il, jl + 2]
+    lsec[i0] = at[il + 2, jl]
+    dxp, dyp = g["dxp"], g["dyp"]
+    fcor = 2.0 * 7.292e-5 * np.sin(np.radians(lat))
+    sgz = np.full((kc, lcm), 1.0 / kc)
+    mo = {"kc": kc, "ld": lcm,
+          "fcorc": cellf(np.full(la - 1, fcor)),
+          "dydi": cellf(0.02 * dyp[i0] * rng.uniform(-1.0, 1.0, la - 1)),
+          "dxdj": cellf(0.02 * dxp[i0] * rng.uniform(-1.0, 1.0, la - 1)),
+          "scax": cellf(np.ones(la - 1)), "scay": cellf(np.ones(la - 1)),
+          "saax": cellf(np.ones(la - 1)), "saay": cellf(np.ones(la - 1)),
+          "sgzu": sgz, "sgzv": sgz.copy(), "fsgzu": np.full((kc, lcm), float(kc)),
+          "fsgzv": np.full((kc, lcm), float(kc)), "lnwc": lnwc, "lsec": lsec}
+    obc_cells = [int(L) for sd in ("W", "E", "S", "N") for L in g["obc"][sd]["l"]]
+    extra = [int(L) for L in rng.choice(np.arange(2, la + 1), size=max(0, nbcs), replace=False)]
+    lbcs = (obc_cells + extra)[:max(nbcs, 0)]
+    lberc = [int(g["lec"][L - 1]) if k % 2 == 0 else int(g["lwc"][L - 1])
+             for k, L in enumerate(lbcs)]
+    lbnrc = [int(g["lnc"][L - 1]) if k % 3 else 1 for k, L in enumerate(lbcs)]
+    lberc = [L if L <= la else 1 for L in lberc]
+    lbnrc = [L if L <= la else 1 for L in lbnrc]
+    mo["lbcs"] = np.array(lbcs, np.int32)
+    mo["lberc"] = np.array(lberc, np.int32)
+    mo["lbnrc"] = np.array(lbnrc, np.int32)
+    for L in lbcs:
+        mo["saax"][L - 1] = 0.0
+        mo["saay"][L - 1] = 0.0
+    if tri:
+        mo["stcuv"] = cellf((rng.uniform(size=la - 1) > 0.1).astype(float))
+    if hdmf:
+        mo["sdx"] = cellf(g["dyu"][i0] * rng.uniform(0.5, 1.5, la - 1))
+        mo["sdy"] = cellf(g["dxv"][i0] * rng.uniform(0.5, 1.5, la - 1))
+        lh = np.zeros(lcm, np.int32)
+        lh[i0] = (rng.uniform(size=la - 1) > 0.05).astype(np.int32)
+        mo["lhdmf"] = lh
+    scn.momentum = mo
+    return mo
+
+
+def momentum_fields(scn: Scenario, *, seed: int = 0, u_scale: float = 0.4, wet_frac: float = 1.0,
+                    fuhj: bool = False, hdmf: bool = False) -> dict:
+    """One call's inputs of the explicit momentum producer for ``scn``: seeded
+    layer velocities U, V of scale ``u_scale`` m/s, transports UHDY = U*DYU*HU/kc
+    and VHDX = V*DXV*HV/kc, HP from the state, a wet set of ``wet_frac`` of the
+    cells (None for all), sparse FUHJ, FVHJ with ``fuhj``, the CALHDMF terms with
+    ``hdmf``, and zeroed output arrays (FCAXE.. and the layer outputs)."""
+    rng = np.random.default_rng(seed + 13)
+    mo = scn.momentum
+    kc, lcm = mo["kc"], mo["ld"]
+    la = scn.la
+    i0 = np.arange(1, la)
+    st, g = scn.state, scn.grid
+
+    def lay(scale):
+        a = np.zeros((kc, lcm))
+        a[:, i0] = scale * rng.uniform(-1.0, 1.0, (kc, la - 1))
+        return a
+
+    u, v = lay(u_scale), lay(u_scale)
+    f = {"u": u, "v": v, "uhdy": u * (g["dyu"][:lcm] * st["hu"][:lcm]) / kc,
+         "vhdx": v * (g["dxv"][:lcm] * st["hv"][:lcm]) / kc,
+         "hp": st["hp"].copy()}
+    f["uhdy"] = np.ascontiguousarray(f["uhdy"])
+    f["vhdx"] = np.ascontiguousarray(f["vhdx"])
+    if wet_frac < 1.0:
+        w = np.zeros(lcm, np.int32)
+        w[i0] = (rng.uniform(size=la - 1) < wet_frac).astype(np.int32)
+        f["wet"] = w
+    if fuhj:
+        for k in ("fuhj", "fvhj"):
+            a = np.zeros((kc, lcm))
+            pick = rng.choice(i0, size=max(1, (la - 1) // 50), replace=False)
+            a[:, pick] = rng.uniform(-5.0, 5.0, (kc, pick.size))
+            f[k] = a
+    if hdmf:
+        for k in ("fmdux", "fmduy", "fmdvx", "fmdvy"):
+            f[k] = lay(1e-3)
+    for k in ("fcaxe", "fcaye", "fxe", "fye"):
+        f[k] = np.zeros(lcm)
+    for k in ("fcax", "fcay", "fx", "fy", "cac"):
+        f[k] = np.zeros((kc, lcm))
+    return f
+
+
 def add_three_levels(scn: Scenario) -> Scenario:
     """The state of the three-time-level scheme (CALPUV9C) at its start, with
     level n-1 equal to level n: P1 = P, H2P = H1P = HP, UHDY1E = UHDY2E =

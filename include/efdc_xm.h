@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define EFDC_XM_ABI_VERSION 5
+#define EFDC_XM_ABI_VERSION 6
 
 /* Status codes.  The reference STOPs where these are returned. */
 enum efdc_xm_status {
@@ -335,6 +335,73 @@ typedef struct efdc_xm_drag_fields { /* per member and call                     
 int32_t efdc_xm_bottom_stress_batch(efdc_xm_ctx *ctx, const efdc_xm_drag_params *prm,
                                     efdc_xm_drag_fields *f);
 
+/* Explicit momentum producer: CALEXP2T's external-mode terms (calexp2t.f90:
+ * 129-956 for IS2LMC = 0, ISVEG = 0, ISBODYF = 0, ISPNHYDS = 0, IATMP = 0,
+ * ISWAVE < 2, ISCHAN /= 3): the upwind momentum fluxes FUHU, FVHU, FVHV, FUHV
+ * (:202-237), the triangular-cell blocking STCUV (ITRICELL, :460-472), the
+ * Coriolis-curvature coefficients CAC and their domain sum (:481-535), the
+ * accelerations FCAX, FCAY (:545-562) with the type-2 open-boundary forms
+ * (:605-645), the layer forcings FX, FY with the momentum of withdrawals and
+ * sources FUHJ, FVHJ (:648-662), the flow-boundary edges (:664-689), the
+ * horizontal momentum diffusion (ISHDMF >= 1, :797-811), and the depth sums
+ * FCAXE, FCAYE, FXE, FYE (:940-956), on the device.  The sums stay on the
+ * device for the next step: a step given FCAXE, FCAYE, FXE, FYE = NULL uses
+ * them without an upload.  The internal-mode parts of CALEXP2T with KC > 1
+ * (the vertical momentum fluxes FWU, FWV added to FX after the sums, :429-
+ * 457 and :960-975, the buoyancy forcing and the shears DU, DV) stay with the
+ * host's internal mode, which takes FX, FY, FCAX, FCAY per layer from here.
+ * Layer arrays hold K = 1..kc at [(K-1)*ld + L-1] (ld = LCM for a Fortran
+ * A(LCM,KCM)).  Cells outside the wet set hold 0 in every output, as the
+ * reference's arrays of dry cells do (zeroed on drying, :131-175, and never
+ * written while dry); the flow-boundary edges still apply to them.
+ *
+ * Static part, per member (efdc_xm_set_momentum): */
+typedef struct efdc_xm_momentum {
+  int32_t kc;                         /* KC (1..64)                                   */
+  int32_t ld;                         /* leading dimension of the layer arrays (LCM)  */
+  const double *fcorc, *dydi, *dxdj;  /* FCORC, DYDI, DXDJ (:489)                     */
+  const double *scax, *scay;          /* SCAX, SCAY (:558-559)                        */
+  const double *saax, *saay;          /* SAAX, SAAY (:668-688)                        */
+  const double *sgzu, *sgzv;          /* SGZU(L,K), SGZV(L,K): layers (:944-947)      */
+  const double *fsgzu, *fsgzv;        /* FSGZU(L,K), FSGZV(L,K): layers (:657-658)    */
+  const double *stcuv;                /* STCUV (ITRICELL > 0) or NULL                 */
+  const double *sdx, *sdy;            /* SDX, SDY (ISHDMF >= 1) or NULL               */
+  const int32_t *lhdmf;               /* LHDMF(L,KC) as 0/1 (ISHDMF >= 1) or NULL     */
+  const int32_t *lnwc, *lsec;         /* LNWC, LSEC: the NW and SE diagonal cells     */
+  int32_t nbcs;                       /* NBCS: flow-boundary cells                    */
+  int32_t pad_;
+  const int32_t *lbcs, *lberc, *lbnrc; /* LBCS, LBERC, LBNRC [nbcs]                   */
+} efdc_xm_momentum;
+int32_t efdc_xm_set_momentum(efdc_xm_ctx *ctx, int32_t member, const efdc_xm_momentum *mo);
+
+typedef struct efdc_xm_explicit_params { /* per member and call                    */
+  double snlt;                        /* SNLT                                         */
+  int32_t iscurvature;                /* ISCURVATURE                                  */
+  int32_t ishdmf;                     /* ISHDMF                                       */
+} efdc_xm_explicit_params;
+
+typedef struct efdc_xm_explicit_fields { /* per member and call                    */
+  const double *u, *v;                /* U(L,K), V(L,K) at entry: layers (these four
+                                         NULL in every member: the previous call's)   */
+  const double *uhdy, *vhdx;          /* UHDY(L,K), VHDX(L,K) at entry: layers        */
+  const double *hp;                   /* HP                                           */
+  const int32_t *wet;                 /* 0/1: the wet set LWET (LMASKDRY with ISDRY >
+                                         0); NULL: every water cell                   */
+  const double *fuhj, *fvhj;          /* FUHJ, FVHJ: layers (withdrawal/return and
+                                         source momentum, :334-424) or NULL (zero)    */
+  const double *fmdux, *fmduy;        /* ISHDMF >= 1: CALHDMF's FMDUX, FMDUY, FMDVX,  */
+  const double *fmdvx, *fmdvy;        /*   FMDVY (layers)                             */
+  double *fcaxe, *fcaye, *fxe, *fye;  /* out, or NULL (kept on the device)            */
+  double *fcax, *fcay, *fx, *fy;      /* out: layers, or NULL                         */
+  double *cac;                        /* out: layers, or NULL                         */
+} efdc_xm_explicit_fields;
+
+/* One call per time step, before the step that reads its sums (the order of
+ * hdmt2t.f90:494-509).  Replaces CALL CALEXP2T for the options above (the
+ * Fortran shim stops on the others); kc may differ by member. */
+int32_t efdc_xm_explicit_batch(efdc_xm_ctx *ctx, const efdc_xm_explicit_params *prm,
+                               efdc_xm_explicit_fields *f);
+
 /* Standalone replacement of CONGRAD (congrad.f90:1-191) for callers that
  * assemble the scaled system themselves (e.g. calpuv9c.f90:446).  Arrays are
  * 1-based Fortran arrays as above; P is the initial guess and the result.
@@ -485,6 +552,9 @@ int64_t efdc_xm_host_waits(void);
  *   EFDC_XM_OPT_INNER_MARGIN (default 0, 0..6): the MIXED inner solve reduces
  *     its residual 10^value times further than the FP64 residual needs to
  *     reach its stop, trading inner iterations for refinement passes.
+ *   EFDC_XM_OPT_INNER_TOL (default 60, 40..75): a MIXED inner solve reduces
+ *     its residual by at least 10^(-value/10) in norm before the next FP64
+ *     refinement pass, where the FP64 stop needs more than that.
  * Results stay within the MIXED form's error bar whatever the schedule; the
  * FP64 form's results do not depend on it.
  * Returns EFDC_XM_BAD_ARGUMENT for an unknown option or value. */
@@ -495,7 +565,8 @@ enum {
   EFDC_XM_OPT_CTAS_MATVEC = 4,
   EFDC_XM_OPT_CTAS_UPDATE = 5,
   EFDC_XM_OPT_POLY_THRESHOLD = 6,
-  EFDC_XM_OPT_INNER_MARGIN = 7
+  EFDC_XM_OPT_INNER_MARGIN = 7,
+  EFDC_XM_OPT_INNER_TOL = 8
 };
 int32_t efdc_xm_set_option(efdc_xm_ctx *ctx, int32_t option, int32_t value);
 

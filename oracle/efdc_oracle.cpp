@@ -1,6 +1,7 @@
 // efdc_oracle.cpp -- TEST INFRASTRUCTURE ONLY: CPU FP64 restatement of EFDC+
 // 8.5 CALPUV2C / CALPUV9C / CONGRAD / CONGRADC / SUBCHAN / CALEBI (standard sigma) /
-// SETOPENBC / SETOPENBC2 / NEGDEP (check part).
+// SETOPENBC / SETOPENBC2 / NEGDEP (check part) / CALTBXY (bed drag) / CALEXP2T
+// (external-mode terms).
 // Parity against the reference is UNPINNED (no compiler, no reference tests);
 // see efdc_oracle.h.  Each block cites the Fortran it restates.
 //
@@ -73,6 +74,17 @@ struct oracle_ctx {
   int bed_kc = 0;
   double avcon = 0., vismud = 0., visfac = 0.;
   std::vector<double> zbr, zbratu, zbratv, sgzuu, sgzvv, stbxo, stbyo, stbx, stby;
+  // explicit momentum producer (CALEXP2T): the static part, layer k (0-based)
+  // of a layer array at [k*(lc+2) + L], and the SAVEd / module layer arrays
+  // kept between calls (zero before the first), with the wet set of the
+  // previous call (its newly dry cells are LDRY)
+  bool mom = false;
+  int mkc = 0, mld = 0;
+  std::vector<double> fcorc, dydi, dxdj, scax, scay, saax, saay, stcuv, sdx, sdy;
+  std::vector<double> msgzu, msgzv, mfsgzu, mfsgzv;
+  std::vector<int> lhdmf, lnwc, lsec, lbcs, lberc, lbnrc;
+  std::vector<double> fuhu, fvhu, fvhv, fuhv, cac, fcax, fcay, fx, fy;
+  std::vector<int> mwet_prev;
 };
 
 namespace {
@@ -1379,6 +1391,242 @@ int oracle_bottom_stress(oracle_ctx *c, const efdc_xm_drag_params *p, const efdc
     if (f->stbx) f->stbx[L - 1] = STBX[L];
     if (f->stby) f->stby[L - 1] = STBY[L];
   }
+  return EFDC_XM_OK;
+}
+
+int oracle_set_momentum(oracle_ctx *c, const efdc_xm_momentum *mo) {
+  const int lc = c->lc;
+  if (!mo || mo->kc < 1 || mo->kc > 64 || mo->ld < lc || !mo->fcorc || !mo->dydi ||
+      !mo->dxdj || !mo->scax || !mo->scay || !mo->saax || !mo->saay || !mo->sgzu ||
+      !mo->sgzv || !mo->fsgzu || !mo->fsgzv || !mo->lnwc || !mo->lsec || mo->nbcs < 0)
+    return EFDC_XM_BAD_ARGUMENT;
+  const int kc = mo->kc, n1 = lc + 2;
+  c->mom = true;
+  c->mkc = kc;
+  c->mld = mo->ld;
+  copy1(c->fcorc, mo->fcorc, lc);
+  copy1(c->dydi, mo->dydi, lc);
+  copy1(c->dxdj, mo->dxdj, lc);
+  copy1(c->scax, mo->scax, lc);
+  copy1(c->scay, mo->scay, lc);
+  copy1(c->saax, mo->saax, lc);
+  copy1(c->saay, mo->saay, lc);
+  copy1(c->stcuv, mo->stcuv, lc);
+  if (!mo->stcuv) c->stcuv.clear();
+  copy1(c->sdx, mo->sdx, lc);
+  copy1(c->sdy, mo->sdy, lc);
+  copy1(c->lhdmf, mo->lhdmf, lc);
+  copy1(c->lnwc, mo->lnwc, lc);
+  copy1(c->lsec, mo->lsec, lc);
+  for (auto *v : {&c->msgzu, &c->msgzv, &c->mfsgzu, &c->mfsgzv}) v->assign(size_t(kc) * n1, 0.);
+  for (int k = 0; k < kc; ++k)
+    for (int L = 1; L <= lc; ++L) {
+      const size_t i = size_t(k) * n1 + L, j = size_t(k) * mo->ld + L - 1;
+      c->msgzu[i] = mo->sgzu[j];
+      c->msgzv[i] = mo->sgzv[j];
+      c->mfsgzu[i] = mo->fsgzu[j];
+      c->mfsgzv[i] = mo->fsgzv[j];
+    }
+  c->lbcs.assign(mo->lbcs, mo->lbcs + mo->nbcs);
+  c->lberc.assign(mo->lberc, mo->lberc + mo->nbcs);
+  c->lbnrc.assign(mo->lbnrc, mo->lbnrc + mo->nbcs);
+  for (auto *v : {&c->fuhu, &c->fvhu, &c->fvhv, &c->fuhv, &c->cac, &c->fcax, &c->fcay, &c->fx,
+                  &c->fy})
+    v->assign(size_t(kc) * n1, 0.);
+  c->mwet_prev.assign(n1, 0);
+  return EFDC_XM_OK;
+}
+
+// CALEXP2T (calexp2t.f90:129-956) for IS2LMC = 0 and the options of
+// efdc_xm_explicit_batch, serially in the reference's statement order.  The
+// layer arrays are the context's, kept between calls; the caller's FCAXE,
+// FCAYE, FXE, FYE are in/out like the module arrays.
+int oracle_explicit(oracle_ctx *c, const efdc_xm_explicit_params *p,
+                    efdc_xm_explicit_fields *f) {
+  if (!c->mom || !p || !f || !f->u || !f->v || !f->uhdy || !f->vhdx || !f->hp || !f->fcaxe ||
+      !f->fcaye || !f->fxe || !f->fye)
+    return EFDC_XM_BAD_ARGUMENT;
+  if (p->ishdmf >= 1 && (c->sdx.empty() || !f->fmdux || !f->fmduy || !f->fmdvx || !f->fmdvy ||
+                         c->lhdmf.empty()))
+    return EFDC_XM_BAD_ARGUMENT;
+  const int la = c->la, lc = c->lc, kc = c->mkc, n1 = lc + 2;
+  auto K_ = [&](std::vector<double> &v, int k) { return F<double>{v.data() + size_t(k) * n1 + 1}; };
+  std::vector<int> wet(n1, 0);
+  for (int L = 2; L <= la; ++L) wet[L] = f->wet ? (f->wet[L - 1] != 0) : 1;
+  std::vector<int> lwet;  // LWET in L order
+  for (int L = 2; L <= la; ++L)
+    if (wet[L]) lwet.push_back(L);
+  F<double> FCAXE{f->fcaxe}, FCAYE{f->fcaye}, FXE{f->fxe}, FYE{f->fye}, HP{const_cast<double *>(f->hp)};
+  F<double> DXYP{c->dxyp.data() + 1}, FCORC{c->fcorc.data() + 1}, DYDI{c->dydi.data() + 1},
+      DXDJ{c->dxdj.data() + 1}, SCAX{c->scax.data() + 1}, SCAY{c->scay.data() + 1},
+      SAAX{c->saax.data() + 1}, SAAY{c->saay.data() + 1};
+  F<int> LEC{c->lec.data() + 1}, LWC{c->lwc.data() + 1}, LNC{c->lnc.data() + 1},
+      LSC{c->lsc.data() + 1}, LNWC{c->lnwc.data() + 1}, LSEC{c->lsec.data() + 1};
+  // the caller's layer arrays (leading dimension LCM), layer k (0-based) of element L
+  const long cld = c->mld;
+  auto in = [&](const double *a, int k, int L) { return a ? a[size_t(k) * cld + L - 1] : 0.0; };
+  const double SNLT = p->snlt;
+  // :131-175 newly dry cells (wet at the previous call, not now): zero the
+  // sums and every layer array
+  for (int L = 2; L <= la; ++L)
+    if (c->mwet_prev[L] && !wet[L]) {
+      FCAXE[L] = 0.;
+      FCAYE[L] = 0.;
+      FXE[L] = 0.;
+      FYE[L] = 0.;
+      for (int k = 0; k < kc; ++k)
+        for (auto *v : {&c->fuhu, &c->fvhu, &c->fvhv, &c->fuhv, &c->cac, &c->fcax, &c->fcay,
+                        &c->fx, &c->fy})
+          K_(*v, k)[L] = 0.;
+    }
+  c->mwet_prev = wet;
+  // :187-197
+  for (int L : lwet) {
+    FCAXE[L] = 0.;
+    FCAYE[L] = 0.;
+    FXE[L] = 0.;
+    FYE[L] = 0.;
+  }
+  // :205-237 upwind momentum fluxes
+  for (int k = 0; k < kc; ++k) {
+    F<double> FUHU = K_(c->fuhu, k), FVHU = K_(c->fvhu, k), FVHV = K_(c->fvhv, k),
+              FUHV = K_(c->fuhv, k);
+    for (int L : lwet) {
+      const int LE = LEC[L], LN = LNC[L], LS = LSC[L], LW = LWC[L];
+      const double UHB = 0.5 * (in(f->uhdy, k, L) + in(f->uhdy, k, LE));
+      const double VHC = 0.5 * (in(f->vhdx, k, L) + in(f->vhdx, k, LW));
+      FUHU[L] = std::max(UHB, 0.) * in(f->u, k, L) + std::min(UHB, 0.) * in(f->u, k, LE);
+      FVHU[L] = std::max(VHC, 0.) * in(f->u, k, LS) + std::min(VHC, 0.) * in(f->u, k, L);
+      const double VHB = 0.5 * (in(f->vhdx, k, L) + in(f->vhdx, k, LN));
+      const double UHC = 0.5 * (in(f->uhdy, k, L) + in(f->uhdy, k, LS));
+      FVHV[L] = std::max(VHB, 0.) * in(f->v, k, L) + std::min(VHB, 0.) * in(f->v, k, LN);
+      FUHV[L] = std::max(UHC, 0.) * in(f->v, k, LW) + std::min(UHC, 0.) * in(f->v, k, L);
+    }
+  }
+  // :460-472 triangular cells
+  if (!c->stcuv.empty())
+    for (int k = 0; k < kc; ++k)
+      for (int L : lwet) {
+        K_(c->fuhu, k)[L] = c->stcuv[L] * K_(c->fuhu, k)[L];
+        K_(c->fvhv, k)[L] = c->stcuv[L] * K_(c->fvhv, k)[L];
+      }
+  // :481-535 Coriolis-curvature coefficients and their sum
+  double CACSUMT = 0.;
+  if (p->iscurvature) {
+    double sum = 0.;
+    for (int k = 0; k < kc; ++k) {
+      F<double> CAC = K_(c->cac, k);
+      for (int L : lwet) {
+        const int LE = LEC[L], LN = LNC[L];
+        CAC[L] = (FCORC[L] * DXYP[L] + 0.5 * SNLT * (in(f->v, k, LN) + in(f->v, k, L)) * DYDI[L] -
+                  0.5 * SNLT * (in(f->u, k, LE) + in(f->u, k, L)) * DXDJ[L]) *
+                 HP[L];
+        sum = sum + CAC[L];
+      }
+    }
+    CACSUMT = std::fabs(sum);
+    if (CACSUMT < 1.E-7)
+      for (int k = 0; k < kc; ++k)
+        for (int L : lwet) {
+          K_(c->fcax, k)[L] = 0.;
+          K_(c->fcay, k)[L] = 0.;
+        }
+  }
+  // :545-562
+  if (CACSUMT > 1.E-7)
+    for (int k = 0; k < kc; ++k) {
+      F<double> CAC = K_(c->cac, k), FCAX = K_(c->fcax, k), FCAY = K_(c->fcay, k);
+      for (int L : lwet) {
+        const int LE = LEC[L], LN = LNC[L], LS = LSC[L], LW = LWC[L], LNW = LNWC[L],
+                  LSE = LSEC[L];
+        FCAX[L] = 0.25 * SCAX[L] *
+                  (CAC[L] * (in(f->v, k, LN) + in(f->v, k, L)) +
+                   CAC[LW] * (in(f->v, k, LNW) + in(f->v, k, LW)));
+        FCAY[L] = 0.25 * SCAY[L] *
+                  (CAC[L] * (in(f->u, k, LE) + in(f->u, k, L)) +
+                   CAC[LS] * (in(f->u, k, LSE) + in(f->u, k, LS)));
+      }
+    }
+  // :605-645 type-2 open boundaries
+  for (int s = 0; s < 4; ++s) {
+    const Side &sd = c->side[s];
+    for (int ll = 0; ll < sd.n; ++ll) {
+      if (sd.ispb[ll] != 2) continue;
+      const int LB = sd.l[ll];
+      for (int k = 0; k < kc; ++k) {
+        F<double> CAC = K_(c->cac, k), FCAX = K_(c->fcax, k), FCAY = K_(c->fcay, k);
+        if (s == 0) {  // W: the cell after the boundary cell in L order (:607-614)
+          const int L = LB + 1, LN = LNC[L];
+          FCAX[L] = 0.5 * SCAX[L] * CAC[L] * (in(f->v, k, LN) + in(f->v, k, L));
+        } else if (s == 1) {  // E (:617-624)
+          const int L = LB, LNW = LNWC[L], LW = LWC[L];
+          FCAX[L] = 0.5 * SCAX[L] * CAC[LW] * (in(f->v, k, LNW) + in(f->v, k, LW));
+        } else if (s == 2) {  // S: the boundary cell's north neighbour (:627-633)
+          const int L = LNC[LB], LE = LEC[L];
+          FCAY[L] = 0.5 * SCAY[L] * CAC[L] * (in(f->u, k, LE) + in(f->u, k, L));
+        } else {  // N (:636-643)
+          const int L = LB, LS = LSC[L], LSE = LSEC[L];
+          FCAY[L] = 0.5 * SCAY[L] * CAC[LS] * (in(f->u, k, LSE) + in(f->u, k, LS));
+        }
+      }
+    }
+  }
+  // :648-662 layer forcings with the gross momentum
+  for (int k = 0; k < kc; ++k) {
+    F<double> FUHU = K_(c->fuhu, k), FVHU = K_(c->fvhu, k), FVHV = K_(c->fvhv, k),
+              FUHV = K_(c->fuhv, k), FX = K_(c->fx, k), FY = K_(c->fy, k);
+    F<double> FSGZU{c->mfsgzu.data() + size_t(k) * n1 + 1},
+        FSGZV{c->mfsgzv.data() + size_t(k) * n1 + 1};
+    for (int L : lwet) {
+      const int LE = LEC[L], LN = LNC[L], LS = LSC[L], LW = LWC[L];
+      FX[L] = FSGZU[L] * (FUHU[L] - FUHU[LW] + FVHU[LN] - FVHU[L]) + in(f->fuhj, k, L);
+      FY[L] = FSGZV[L] * (FVHV[L] - FVHV[LS] + FUHV[LE] - FUHV[L]) + in(f->fvhj, k, L);
+    }
+  }
+  // :664-689 flow-boundary edges
+  for (size_t ll = 0; ll < c->lbcs.size(); ++ll)
+    for (int k = 0; k < kc; ++k) {
+      F<double> FX = K_(c->fx, k), FY = K_(c->fy, k);
+      int L = c->lbcs[ll];
+      FX[L] = SAAX[L] * FX[L] + in(f->fuhj, k, L);
+      FY[L] = SAAY[L] * FY[L] + in(f->fvhj, k, L);
+      L = std::max(1, c->lberc[ll]);
+      FX[L] = SAAX[L] * FX[L] + in(f->fuhj, k, L);
+      L = std::max(1, c->lbnrc[ll]);
+      FY[L] = SAAY[L] * FY[L] + in(f->fvhj, k, L);
+    }
+  // :797-811 horizontal momentum diffusion
+  if (p->ishdmf >= 1)
+    for (int k = 0; k < kc; ++k) {
+      F<double> FX = K_(c->fx, k), FY = K_(c->fy, k);
+      for (int L : lwet) {
+        if (!c->lhdmf[L]) continue;
+        FX[L] = FX[L] - c->sdx[L] * (in(f->fmdux, k, L) + in(f->fmduy, k, L));
+        FY[L] = FY[L] - c->sdy[L] * (in(f->fmdvx, k, L) + in(f->fmdvy, k, L));
+      }
+    }
+  // :940-956 the depth sums
+  for (int k = 0; k < kc; ++k) {
+    F<double> FCAX = K_(c->fcax, k), FCAY = K_(c->fcay, k), FX = K_(c->fx, k),
+              FY = K_(c->fy, k);
+    F<double> SGZU{c->msgzu.data() + size_t(k) * n1 + 1},
+        SGZV{c->msgzv.data() + size_t(k) * n1 + 1};
+    for (int L : lwet) {
+      FCAXE[L] = FCAXE[L] + FCAX[L] * SGZU[L];
+      FCAYE[L] = FCAYE[L] + FCAY[L] * SGZV[L];
+      FXE[L] = FXE[L] + FX[L] * SGZU[L];
+      FYE[L] = FYE[L] + FY[L] * SGZV[L];
+    }
+  }
+  for (int k = 0; k < kc; ++k)
+    for (int L = 1; L <= lc; ++L) {
+      const size_t o = size_t(k) * cld + L - 1;
+      if (f->fcax) f->fcax[o] = K_(c->fcax, k)[L];
+      if (f->fcay) f->fcay[o] = K_(c->fcay, k)[L];
+      if (f->fx) f->fx[o] = K_(c->fx, k)[L];
+      if (f->fy) f->fy[o] = K_(c->fy, k)[L];
+      if (f->cac) f->cac[o] = K_(c->cac, k)[L];
+    }
   return EFDC_XM_OK;
 }
 

@@ -2,7 +2,7 @@
  * efdc_oracle.h -- TEST INFRASTRUCTURE ONLY (the checker, never the product).
  *
  * CPU FP64 restatement of EFDC+ 8.5's external mode (and its bottom-stress
- * producer), used by tests/ and by
+ * and explicit-momentum producers), used by tests/ and by
  * bench.py's CPU-baseline leg to check and time the CUDA library.  Nothing in
  * the shipped library links or calls this code.
  *
@@ -64,6 +64,10 @@ int oracle_set_bed(oracle_ctx *c, const efdc_xm_bed *bed);
 int oracle_bottom_stress(oracle_ctx *c, const efdc_xm_drag_params *p, const efdc_xm_fields *st,
                          efdc_xm_drag_fields *f);
 
+/* CALEXP2T's external-mode terms (efdc_xm_set_momentum / efdc_xm_explicit_batch
+ * for one basin). */
+int oracle_set_momentum(oracle_ctx *c, const efdc_xm_momentum *mo);
+int oracle_explicit(oracle_ctx *c, const efdc_xm_explicit_params *p, efdc_xm_explicit_fields *f);
 int oracle_congrad(oracle_ctx *c, const double *ccc, const double *ccs,
                    const double *ccn, const double *ccw, const double *cce,
                    const double *ccci, const double *fptmp, double *p,

@@ -51,6 +51,11 @@ def load():
         lib.oracle_bottom_stress.restype = C.c_int
         lib.oracle_bottom_stress.argtypes = [C.c_void_p, C.POINTER(X.DragParams),
                                              C.POINTER(X.Fields), C.POINTER(X.DragFields)]
+        lib.oracle_set_momentum.restype = C.c_int
+        lib.oracle_set_momentum.argtypes = [C.c_void_p, C.POINTER(X.Momentum)]
+        lib.oracle_explicit.restype = C.c_int
+        lib.oracle_explicit.argtypes = [C.c_void_p, C.POINTER(X.ExplicitParams),
+                                        C.POINTER(X.ExplicitFields)]
         lib.oracle_congrad.restype = C.c_int
         lib.oracle_congrad.argtypes = [C.c_void_p] + [pd] * 8 + [
             C.c_double, C.c_int, C.POINTER(C.c_int), pd]
@@ -108,6 +113,17 @@ class Oracle:
         f, _k = X.make_fields(state)
         d = X.make_drag_fields(drag)
         return self.lib.oracle_bottom_stress(self.ctx, C.byref(params), C.byref(f), C.byref(d))
+
+    def set_momentum(self, mo: dict):
+        s, _keep = X.make_momentum(mo)
+        if self.lib.oracle_set_momentum(self.ctx, C.byref(s)) != 0:
+            raise RuntimeError("oracle_set_momentum: bad momentum arrays")
+
+    def explicit(self, params: X.ExplicitParams, fields: dict) -> int:
+        """CALEXP2T's external-mode terms; FCAXE, FCAYE, FXE, FYE of `fields`
+        in/out, the layer outputs present written."""
+        f, _k = X.make_explicit_fields(fields)
+        return self.lib.oracle_explicit(self.ctx, C.byref(params), C.byref(f))
 
     def congrad(self, ccc, ccs, ccn, ccw, cce, ccci, fptmp, p, rsqm, iterm):
         it = C.c_int(0)

@@ -42,6 +42,8 @@ STRUCTS = {
     "efdc_xm_fields": X.Fields, "efdc_xm_stats": X.Stats, "efdc_xm_channels": X.Channels,
     "efdc_xm_layers": X.Layers, "efdc_xm_bed": X.Bed, "efdc_xm_drag_params": X.DragParams,
     "efdc_xm_drag_fields": X.DragFields, "efdc_xm_ktime": X.KTime,
+    "efdc_xm_momentum": X.Momentum, "efdc_xm_explicit_params": X.ExplicitParams,
+    "efdc_xm_explicit_fields": X.ExplicitFields,
 }
 
 
@@ -102,6 +104,8 @@ FORTRAN_TYPES = {
     "EFDC_XM_FIELDS_T": X.Fields, "EFDC_XM_BED_T": X.Bed,
     "EFDC_XM_DRAG_PARAMS_T": X.DragParams, "EFDC_XM_DRAG_FIELDS_T": X.DragFields,
     "EFDC_XM_LAYERS_T": X.Layers, "EFDC_XM_CHANNELS_T": X.Channels, "EFDC_XM_STATS_T": X.Stats,
+    "EFDC_XM_MOMENTUM_T": X.Momentum, "EFDC_XM_EXPLICIT_PARAMS_T": X.ExplicitParams,
+    "EFDC_XM_EXPLICIT_FIELDS_T": X.ExplicitFields,
 }
 
 
