@@ -90,6 +90,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="CPU baseline: seconds per thread setting (two settings)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--host-loops", action="store_true",
+                    help="drive the CG, refinement and wet/dry loops from the host "
+                         "(EFDC_XM_OPT_DEVICE_LOOPS 0): the same kernels, each launch visible to "
+                         "a kernel profiler (kernels inside graphs with conditional nodes are not)")
     ap.add_argument("--variant", type=int, default=-1,
                     help="MIXED inner-iteration kernel variant (EFDC_XM_OPT_KERNEL_VARIANT); "
                          "-1: the schedule efdc_xm_autotune measures for the workload")
@@ -413,11 +417,13 @@ def explicit_producer(args, torch, dev, bs, scns, peak):
     K = args.explicit_calls
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.profiler.start()  # the timed calls are a profiler range too
     e0.record(stream)
     for _ in range(K):
         bs.explicit(prm, none)
     e1.record(stream)
     e1.synchronize()
+    torch.cuda.profiler.stop()
     ms = e0.elapsed_time(e1) / K
     cells = float(sum(s.ncell for s in scns))
     gbs = 200.0 * cells / (ms * 1e-3) / 1e9
@@ -586,6 +592,9 @@ def ours(args):
     bs = X.BatchSolver([s.grid for s in scns], device=local)
     if args.variant >= 0:
         bs.set_option(X.OPT_KERNEL_VARIANT, args.variant)
+    if args.host_loops:
+        bs.set_option(X.OPT_DEVICE_LOOPS, 0)
+        cfg["loops"] = "host-driven (EFDC_XM_OPT_DEVICE_LOOPS 0)"
     stream = torch.cuda.ExternalStream(bs.stream(), device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if M == 1 else None
 
@@ -694,7 +703,7 @@ def ours(args):
     # the variant the timed run used, and every variant for comparison
     variants = {}
     run_variant = tune["schedule"]["kernel_variant"] if tune else args.variant
-    for v in (0, 1, 2):
+    for v in (0, 1, 2, 3):
         bs.set_option(X.OPT_KERNEL_VARIANT, v)
         kv = bs.time_kernels(X.PREC_MIXED, reps=20)
         variants[v] = {"ms_matvec": kv.ms_matvec, "ms_update": kv.ms_update,

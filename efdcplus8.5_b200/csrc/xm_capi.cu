@@ -2173,7 +2173,7 @@ void apply_schedule(efdc_xm_ctx *c, const efdc_xm_schedule &s) {
 }
 
 bool schedule_valid(const efdc_xm_schedule &s) {
-  return s.kernel_variant >= 0 && s.kernel_variant <= 2 && s.ctas_matvec >= 0 &&
+  return s.kernel_variant >= 0 && s.kernel_variant <= 3 && s.ctas_matvec >= 0 &&
          s.ctas_matvec <= 32 && s.ctas_update >= 0 && s.ctas_update <= 32 &&
          s.graph_iters >= 1 && s.graph_iters <= 32 && s.poly_threshold >= 0 &&
          s.poly_threshold <= 100000 && s.inner_margin >= 0 && s.inner_margin <= 6;
@@ -3869,7 +3869,7 @@ int32_t efdc_xm_autotune(efdc_xm_ctx *c, int32_t precision, const char *table, i
     return EFDC_XM_OK;
   };
   if (mixed) {
-    if ((rc = knob(&efdc_xm_schedule::kernel_variant, {0, 1, 2}))) return rc;
+    if ((rc = knob(&efdc_xm_schedule::kernel_variant, {0, 1, 2, 3}))) return rc;
     if (best.kernel_variant > 0) {
       if ((rc = knob(&efdc_xm_schedule::ctas_matvec, {0, 2, 3, 4}))) return rc;
       if ((rc = knob(&efdc_xm_schedule::ctas_update, {0, 2, 3, 4}))) return rc;
@@ -3935,7 +3935,7 @@ int32_t efdc_xm_set_option(efdc_xm_ctx *c, int32_t option, int32_t value) {
     case EFDC_XM_OPT_CTAS_MATVEC:
     case EFDC_XM_OPT_CTAS_UPDATE: {
       const bool var = option == EFDC_XM_OPT_KERNEL_VARIANT;
-      if (var ? (value < 0 || value > 2) : (value < 0 || value > 32)) break;
+      if (var ? (value < 0 || value > 3) : (value < 0 || value > 32)) break;
       int &v = var ? c->kvariant : option == EFDC_XM_OPT_CTAS_MATVEC ? c->ctas_mv : c->ctas_up;
       if (v != value) {
         v = value;

@@ -354,11 +354,11 @@ __device__ __forceinline__ void quad_sweep_staged(const DevStatic &S, double *pa
 }
 
 // The quad sweep of a kernel variant: 0 prefetches one quad ahead in
-// registers, 1 loads the descriptors in batches (quad_sweep_batched).
+// registers, 1 and 3 load the descriptors in batches (quad_sweep_batched).
 template <int NS, int VAR, class Setup, class Body>
 __device__ __forceinline__ void quad_sweep_v(const DevStatic &S, double *part, Setup setup,
                                              Body body) {
-  if constexpr (VAR == 1)
+  if constexpr (VAR == 1 || VAR == 3)
     quad_sweep_batched<NS>(S, part, setup, body);
   else
     quad_sweep<NS>(S, part, setup, body);
@@ -620,6 +620,127 @@ __device__ __forceinline__ double zinit_row(const RowGeo &g, bool valid,
          double(r0.w) * double(zv.w);
 }
 
+// Variant 3 of the MIXED inner iteration: matvec_row_scaled and
+// update_row_poly with every global load of the row issued before the first
+// shuffle or dependent operation (above, the coefficient rows and x, p_new
+// wait for the first loads' values), so that one round trip to memory serves
+// the row; the same operations on the same values, hence the same results.
+// It holds more values live: its kernels run at fewer CTAs per SM.
+__device__ __forceinline__ double matvec_row_scaled_eager(const RowGeo &g, bool valid,
+                                                    const float *__restrict__ r,
+                                                    const float *__restrict__ pold,
+                                                    float *__restrict__ pnew,
+                                                    const float *__restrict__ as,
+                                                    const float *__restrict__ aw,
+                                                    const float *__restrict__ ae,
+                                                    const float *__restrict__ an,
+                                                    float *__restrict__ ap, float beta, bool asym) {
+  // every load first, so that one round trip serves the row
+  const V4<float> r0 = ld4(r + g.d0), o0 = ld4(pold + g.d0);
+  const V4<float> rn = ld4(r + g.dn), on = ld4(pold + g.dn);
+  const V4<float> rs = ld4(r + g.ds), os = ld4(pold + g.ds);
+  const V4<float> ks = ld4(as + g.d0), kw = ld4(aw + g.d0);
+  const V4<float> kn = asym ? ld4(an + g.d0) : ld4(as + g.dn);
+  V4<float> ke = asym ? ld4(ae + g.d0) : V4<float>{0.f, 0.f, 0.f, 0.f};
+  const bool west = g.cx == 0, east = g.cx == ROWT - 1;
+  const float rw = west ? r[g.dwe] : 0.f, ow = west ? pold[g.dwe] : 0.f;
+  const float re = east ? r[g.dee] : 0.f, oe = east ? pold[g.dee] : 0.f;
+  const float kwe_edge = (east && !asym) ? aw[g.dee] : 0.f;
+  const V4<float> p = {fmaf(beta, o0.x, r0.x), fmaf(beta, o0.y, r0.y), fmaf(beta, o0.z, r0.z),
+                       fmaf(beta, o0.w, r0.w)};
+  const V4<float> pn = {fmaf(beta, on.x, rn.x), fmaf(beta, on.y, rn.y), fmaf(beta, on.z, rn.z),
+                        fmaf(beta, on.w, rn.w)};
+  const V4<float> ps = {fmaf(beta, os.x, rs.x), fmaf(beta, os.y, rs.y), fmaf(beta, os.z, rs.z),
+                        fmaf(beta, os.w, rs.w)};
+  float pw = from_west(p), pe = from_east(p);
+  if (west) pw = fmaf(beta, ow, rw);
+  if (east) pe = fmaf(beta, oe, re);
+  if (!asym) {
+    float kwe = from_east(kw);
+    if (east) kwe = kwe_edge;
+    ke = {kw.y, kw.z, kw.w, kwe};
+  }
+  V4<float> a;
+  a.x = p.x + ks.x * ps.x + kn.x * pn.x + kw.x * pw + ke.x * p.y;
+  a.y = p.y + ks.y * ps.y + kn.y * pn.y + kw.y * p.x + ke.y * p.z;
+  a.z = p.z + ks.z * ps.z + kn.z * pn.z + kw.z * p.y + ke.z * p.w;
+  a.w = p.w + ks.w * ps.w + kn.w * pn.w + kw.w * p.z + ke.w * pe;
+  if (!valid) return 0.0;
+  st4(pnew + g.d0, p);
+  st4(ap + g.d0, a);
+  return double(a.x) * double(p.x) + double(a.y) * double(p.y) + double(a.z) * double(p.z) +
+         double(a.w) * double(p.w);
+}
+
+__device__ __forceinline__ void update_row_poly_eager(const RowGeo &g, bool valid,
+                                                float *__restrict__ x,
+                                                const float *__restrict__ pnew,
+                                                const float *__restrict__ r,
+                                                float *__restrict__ rnew,
+                                                const float *__restrict__ ap,
+                                                const float *__restrict__ as,
+                                                const float *__restrict__ aw,
+                                                float *__restrict__ z, float alpha, bool poly,
+                                                double &rz, double &rr) {
+  // every load first, so that one round trip serves the row (x and p_new
+  // are read at the ghost tile's inert slots too when the row is not valid)
+  const V4<float> r0 = ld4(r + g.d0), a0 = ld4(ap + g.d0);
+  V4<float> xv = ld4(x + g.d0);
+  const V4<float> pv = ld4(pnew + g.d0);
+  V4<float> rN{}, aN{}, rS{}, aS{}, ks{}, kw{}, kn{};
+  float rw = 0.f, aw_ = 0.f, re = 0.f, ae_ = 0.f, kwe_edge = 0.f;
+  const bool west = g.cx == 0, east = g.cx == ROWT - 1;
+  if (poly) {
+    rN = ld4(r + g.dn);
+    aN = ld4(ap + g.dn);
+    rS = ld4(r + g.ds);
+    aS = ld4(ap + g.ds);
+    ks = ld4(as + g.d0);
+    kw = ld4(aw + g.d0);
+    kn = ld4(as + g.dn);
+    if (west) {
+      rw = r[g.dwe];
+      aw_ = ap[g.dwe];
+    }
+    if (east) {
+      re = r[g.dee];
+      ae_ = ap[g.dee];
+      kwe_edge = aw[g.dee];
+    }
+  }
+  const V4<float> rn0 = {fmaf(-alpha, a0.x, r0.x), fmaf(-alpha, a0.y, r0.y),
+                         fmaf(-alpha, a0.z, r0.z), fmaf(-alpha, a0.w, r0.w)};
+  V4<float> zv = rn0;
+  if (poly) {
+    const V4<float> nN = {fmaf(-alpha, aN.x, rN.x), fmaf(-alpha, aN.y, rN.y),
+                          fmaf(-alpha, aN.z, rN.z), fmaf(-alpha, aN.w, rN.w)};
+    const V4<float> nS = {fmaf(-alpha, aS.x, rS.x), fmaf(-alpha, aS.y, rS.y),
+                          fmaf(-alpha, aS.z, rS.z), fmaf(-alpha, aS.w, rS.w)};
+    float nw = from_west(rn0), ne = from_east(rn0);
+    if (west) nw = fmaf(-alpha, aw_, rw);
+    if (east) ne = fmaf(-alpha, ae_, re);
+    float kwe = from_east(kw);
+    if (east) kwe = kwe_edge;
+    const V4<float> ke = {kw.y, kw.z, kw.w, kwe};
+    zv.x = rn0.x - (ks.x * nS.x + kn.x * nN.x + kw.x * nw + ke.x * rn0.y);
+    zv.y = rn0.y - (ks.y * nS.y + kn.y * nN.y + kw.y * rn0.x + ke.y * rn0.z);
+    zv.z = rn0.z - (ks.z * nS.z + kn.z * nN.z + kw.z * rn0.y + ke.z * rn0.w);
+    zv.w = rn0.w - (ks.w * nS.w + kn.w * nN.w + kw.w * rn0.z + ke.w * ne);
+  }
+  if (!valid) return;
+  xv.x = fmaf(alpha, pv.x, xv.x);
+  xv.y = fmaf(alpha, pv.y, xv.y);
+  xv.z = fmaf(alpha, pv.z, xv.z);
+  xv.w = fmaf(alpha, pv.w, xv.w);
+  st4(x + g.d0, xv);
+  st4(rnew + g.d0, rn0);
+  st4(z + g.d0, zv);
+  rz += double(rn0.x) * double(zv.x) + double(rn0.y) * double(zv.y) +
+        double(rn0.z) * double(zv.z) + double(rn0.w) * double(zv.w);
+  rr += double(rn0.x) * double(rn0.x) + double(rn0.y) * double(rn0.y) +
+        double(rn0.z) * double(rn0.z) + double(rn0.w) * double(rn0.w);
+}
+
 // MIXED, Jacobi: x += alpha*p, r -= alpha*Ap (into the other residual buffer)
 // and the part of r.r (= r.z on the unit-diagonal system).
 __device__ __forceinline__ void update_row_jac(const RowGeo &g, bool valid, float *__restrict__ x,
@@ -736,6 +857,83 @@ __device__ __forceinline__ V4<double> residual_row(const RowGeo &g, const uint8_
                                                    const double *__restrict__ P,
                                                    const DevSystem &Y, bool asym) {
   return residual_row(g, kind, P, SysView{Y.fptmp, Y.ccc, Y.ccs, Y.ccw, Y.cce, Y.ccn, 0}, asym);
+}
+
+// residual_row and zinit_row with every load of the row issued first (the
+// refinement kernels of variant 3, see matvec_row_scaled_eager).
+__device__ __forceinline__ V4<double> residual_row_eager(const RowGeo &g, const uint8_t *kind,
+                                                   const double *__restrict__ P,
+                                                   const SysView &V, bool asym) {
+  // every load first, so that one round trip serves the row
+  const V4<double> x = ld4(P + g.d0), xn = ld4(P + g.dn), xs = ld4(P + g.ds);
+  const V4<double> b = ld4(V.fp + g.d0), c = ld4(V.cc + g.d0), ks = ld4(V.cs + g.d0),
+                   kw = ld4(V.cw + g.d0);
+  const V4<double> kn = asym ? ld4(V.cn + g.d0) : ld4(V.cs + g.dn);  // CCN(L) = CCS(LN)
+  V4<double> ke = asym ? ld4(V.ce + g.d0) : V4<double>{0., 0., 0., 0.};
+  const uchar4 kd = *reinterpret_cast<const uchar4 *>(kind + g.d0);
+  const bool west = g.cx == 0, east = g.cx == ROWT - 1;
+  const double xw_edge = west ? P[g.dwe] : 0., xe_edge = east ? P[g.dee] : 0.;
+  const double kwe_edge = (east && !asym) ? V.cw[g.dee] : 0.;
+  double xw = from_west(x), xe = from_east(x);
+  if (west) xw = xw_edge;
+  if (east) xe = xe_edge;
+  if (!asym) {  // CCE(L) = CCW(LE)
+    double kwe = from_east(kw);
+    if (east) kwe = kwe_edge;
+    ke = {kw.y, kw.z, kw.w, kwe};
+  }
+  V4<double> r;
+  r.x = b.x - c.x * x.x - kn.x * xn.x - ks.x * xs.x - kw.x * xw - ke.x * x.y;
+  r.y = b.y - c.y * x.y - kn.y * xn.y - ks.y * xs.y - kw.y * x.x - ke.y * x.z;
+  r.z = b.z - c.z * x.z - kn.z * xn.z - ks.z * xs.z - kw.z * x.y - ke.z * x.w;
+  r.w = b.w - c.w * x.w - kn.w * xn.w - ks.w * xs.w - kw.w * x.z - ke.w * xe;
+  if (kd.x == LAND) r.x = 0.;
+  if (kd.y == LAND) r.y = 0.;
+  if (kd.z == LAND) r.z = 0.;
+  if (kd.w == LAND) r.w = 0.;
+  return r;
+}
+
+__device__ __forceinline__ double zinit_row_eager(const RowGeo &g, bool valid,
+                                           const float *__restrict__ r,
+                                           const float *__restrict__ as,
+                                           const float *__restrict__ aw, float *__restrict__ z,
+                                           float *__restrict__ pold, bool poly) {
+  // every load first, so that one round trip serves the row
+  const V4<float> r0 = ld4(r + g.d0);
+  V4<float> rN{}, rS{}, ks{}, kw{}, kn{};
+  float rw_edge = 0.f, re_edge = 0.f, kwe_edge = 0.f;
+  const bool west = g.cx == 0, east = g.cx == ROWT - 1;
+  if (poly) {
+    rN = ld4(r + g.dn);
+    rS = ld4(r + g.ds);
+    ks = ld4(as + g.d0);
+    kw = ld4(aw + g.d0);
+    kn = ld4(as + g.dn);
+    if (west) rw_edge = r[g.dwe];
+    if (east) {
+      re_edge = r[g.dee];
+      kwe_edge = aw[g.dee];
+    }
+  }
+  V4<float> zv = r0;
+  if (poly) {
+    float rw = from_west(r0), re = from_east(r0);
+    if (west) rw = rw_edge;
+    if (east) re = re_edge;
+    float kwe = from_east(kw);
+    if (east) kwe = kwe_edge;
+    const V4<float> ke = {kw.y, kw.z, kw.w, kwe};
+    zv.x = r0.x - (ks.x * rS.x + kn.x * rN.x + kw.x * rw + ke.x * r0.y);
+    zv.y = r0.y - (ks.y * rS.y + kn.y * rN.y + kw.y * r0.x + ke.y * r0.z);
+    zv.z = r0.z - (ks.z * rS.z + kn.z * rN.z + kw.z * r0.y + ke.z * r0.w);
+    zv.w = r0.w - (ks.w * rS.w + kn.w * rN.w + kw.w * r0.z + ke.w * re);
+  }
+  if (!valid) return 0.0;
+  st4(z + g.d0, zv);
+  st4(pold + g.d0, V4<float>{0.f, 0.f, 0.f, 0.f});
+  return double(r0.x) * double(zv.x) + double(r0.y) * double(zv.y) + double(r0.z) * double(zv.z) +
+         double(r0.w) * double(zv.w);
 }
 
 // The Jacobi scaling of the MIXED inner system, 1/sqrt(c) for a diagonal c

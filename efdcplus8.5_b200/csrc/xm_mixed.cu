@@ -25,8 +25,11 @@ namespace xm {
 
 // p = z + beta*p_old at the cell and its halo (z = r for Jacobi members),
 // Ahat*p, p.Ap (per member).
+// CTAs per SM the launch bounds ask for, by variant (3 holds more values live)
+constexpr int mx_ctas(int var) { return var == 1 ? 5 : var == 3 ? 4 : 6; }
+
 template <bool MA, int VAR>
-__global__ void __launch_bounds__(NT, VAR == 1 ? 5 : 6) k_mx_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
+__global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
                                                     double *part) {
   struct A {
     bool skip, asym;
@@ -46,8 +49,12 @@ __global__ void __launch_bounds__(NT, VAR == 1 ? 5 : 6) k_mx_matvec(DevStatic S,
                  par ? Y.pa32 : Y.pb32, poly ? Y.z32 : (par ? Y.r32b : Y.r32)};
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
-        v[0] = matvec_row_scaled(g, valid, a.z, a.pold, a.pnew, Y.as32, Y.aw32, Y.ae32, Y.an32,
-                                 Y.ap32, a.beta, a.asym);
+        if constexpr (VAR == 3)
+          v[0] = matvec_row_scaled_eager(g, valid, a.z, a.pold, a.pnew, Y.as32, Y.aw32, Y.ae32,
+                                         Y.an32, Y.ap32, a.beta, a.asym);
+        else
+          v[0] = matvec_row_scaled(g, valid, a.z, a.pold, a.pnew, Y.as32, Y.aw32, Y.ae32,
+                                   Y.an32, Y.ap32, a.beta, a.asym);
       });
 }
 // ALPHA = RPCG / p.Ap
@@ -64,7 +71,7 @@ __global__ void __launch_bounds__(NT) k_red_mx_matvec(DevStatic S, Ctl *ctl, con
 // x += alpha*p, r -= alpha*Ap, z = (2I - Ahat) r (the two-term Neumann
 // polynomial), r.z and r.r (FP64 sums): the members that use it.
 template <int VAR>
-__global__ void __launch_bounds__(NT, VAR == 1 ? 5 : 6) k_mx_update_poly(DevStatic S, DevSystem Y,
+__global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_update_poly(DevStatic S, DevSystem Y,
                                                          const Ctl *ctl, double *part) {
   struct A {
     bool skip;
@@ -83,8 +90,12 @@ __global__ void __launch_bounds__(NT, VAR == 1 ? 5 : 6) k_mx_update_poly(DevStat
                  par ? Y.r32b : Y.r32, par ? Y.r32 : Y.r32b};
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
-        update_row_poly(g, valid, Y.x32, a.pnew, a.r, a.rnew, Y.ap32, Y.as32, Y.aw32, Y.z32,
-                        a.alpha, true, v[0], v[1]);
+        if constexpr (VAR == 3)
+          update_row_poly_eager(g, valid, Y.x32, a.pnew, a.r, a.rnew, Y.ap32, Y.as32, Y.aw32,
+                                Y.z32, a.alpha, true, v[0], v[1]);
+        else
+          update_row_poly(g, valid, Y.x32, a.pnew, a.r, a.rnew, Y.ap32, Y.as32, Y.aw32, Y.z32,
+                          a.alpha, true, v[0], v[1]);
       });
 }
 // The same for the Jacobi members (z = r): x, r and r.r only.
@@ -148,6 +159,7 @@ __global__ void __launch_bounds__(NT) k_red_mx_update(DevStatic S, Ctl *ctl, Glo
 
 // First inner iteration of the polynomial members: z0 = (2I - Ahat) r0,
 // p_old = 0, RPCG = r0.z0 (Jacobi members start from k_mx_resid's p0 = r0).
+template <bool EAGER>
 __global__ void __launch_bounds__(NT) k_mx_zinit(DevStatic S, DevSystem Y, const Ctl *ctl,
                                                 double *part) {
   struct A {
@@ -157,7 +169,10 @@ __global__ void __launch_bounds__(NT) k_mx_zinit(DevStatic S, DevSystem Y, const
       S, part,
       [&](int m) { return A{ctl[m].done != 0 || !Y.mpoly[m] || unsym<true>(ctl[m]), false}; },
       [&](const A &, const RowGeo &g, bool valid, double *v) {
-        v[0] = zinit_row(g, valid, Y.r32, Y.as32, Y.aw32, Y.z32, Y.pa32, true);
+        if constexpr (EAGER)
+          v[0] = zinit_row_eager(g, valid, Y.r32, Y.as32, Y.aw32, Y.z32, Y.pa32, true);
+        else
+          v[0] = zinit_row(g, valid, Y.r32, Y.as32, Y.aw32, Y.z32, Y.pa32, true);
       });
 }
 __global__ void __launch_bounds__(NT) k_red_mx_zinit(DevStatic S, DevSystem Y, Ctl *ctl,
@@ -470,6 +485,13 @@ void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, C
     else
       k_mx_matvec<false, 1><<<grid_of(l, S, k_mx_matvec<false, 1>, l.ctas_mv), NT, 0,
                               l.stream>>>(S, Y, ctl, part);
+  } else if (l.variant == 3) {
+    if (l.may_asym)
+      k_mx_matvec<true, 3><<<grid_of(l, S, k_mx_matvec<true, 3>, l.ctas_mv), NT, 0, l.stream>>>(
+          S, Y, ctl, part);
+    else
+      k_mx_matvec<false, 3><<<grid_of(l, S, k_mx_matvec<false, 3>, l.ctas_mv), NT, 0,
+                              l.stream>>>(S, Y, ctl, part);
   } else if (l.may_asym) {
     k_mx_matvec<true, 0><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
   } else {
@@ -487,7 +509,7 @@ void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, C
                          l.stream>>>(S, Y, ctl, part);
     count_launches(1);
   } else if (l.mx_jac) {
-    if (l.variant == 1)
+    if (l.variant == 1 || l.variant == 3)  // the Jacobi row already loads first
       k_mx_update_jac<1><<<grid_of(l, S, k_mx_update_jac<1>, l.ctas_up), NT, 0, l.stream>>>(
           S, Y, ctl, part);
     else
@@ -503,6 +525,9 @@ void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, C
     if (l.variant == 1)
       k_mx_update_poly<1><<<grid_of(l, S, k_mx_update_poly<1>, l.ctas_up), NT, 0, l.stream>>>(
           S, Y, ctl, part);
+    else if (l.variant == 3)
+      k_mx_update_poly<3><<<grid_of(l, S, k_mx_update_poly<3>, l.ctas_up), NT, 0, l.stream>>>(
+          S, Y, ctl, part);
     else
       k_mx_update_poly<0><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part);
     count_launches(1);
@@ -513,7 +538,10 @@ void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, C
 void launch_mx_zinit(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                      double *part) {
   if (!l.mx_poly) return;
-  k_mx_zinit<<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part);
+  if (l.variant == 3)
+    k_mx_zinit<true><<<grid_of(l, S, k_mx_zinit<true>, 0), NT, 0, l.stream>>>(S, Y, ctl, part);
+  else
+    k_mx_zinit<false><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part);
   k_red_mx_zinit<<<reduce_grid(S), NT, 0, l.stream>>>(S, Y, ctl, part);
   count_launches(2);
 }

@@ -129,15 +129,21 @@ __device__ __forceinline__ double assemble_cell(const DevStatic &S, const DevSta
                                                 double fuh, double fuhe, double fvh,
                                                 double fvhn) {
   const int d = q.d;
-  double C1 = 0.5 * c.g;
+  // the loads first (the stores below could alias them for the compiler)
   const double sub = X.sub[d], svb = X.svb[d], sube = X.sub[q.e], svbn = X.svb[q.n];
-  X.fp[d] = fp1 - C1 * (sube * fuhe - sub * fuh + svbn * fvhn - svb * fvh - 2.0 * X.qsume[d]);
+  const double qsume = X.qsume[d], dxyp = S.dxyp[d];
+  const double hrvo = S.hrvo[d], hruo = S.hruo[d], hruoe = S.hruo[q.e], hrvon = S.hrvo[q.n];
+  const double hvc = X.hvc[d], huc = X.huc[d], huce = X.huc[q.e], hvcn = X.hvc[q.n];
+  const double ry = rc_y(X, c, d), rx = rc_x(X, c, d), rxe = rc_x(X, c, q.e),
+               ryn = rc_y(X, c, q.n);
+  double C1 = 0.5 * c.g;
+  X.fp[d] = fp1 - C1 * (sube * fuhe - sub * fuh + svbn * fvhn - svb * fvh - 2.0 * qsume);
   C1 = -0.5 * c.deltd2 * c.g;
-  const double cs = C1 * svb * S.hrvo[d] * rc_y(X, c, d) * X.hvc[d];
-  const double cw = C1 * sub * S.hruo[d] * rc_x(X, c, d) * X.huc[d];
-  const double ce = C1 * sube * S.hruo[q.e] * rc_x(X, c, q.e) * X.huc[q.e];
-  const double cn = C1 * svbn * S.hrvo[q.n] * rc_y(X, c, q.n) * X.hvc[q.n];
-  const double cc = c.delti * S.dxyp[d] - cs - cw - ce - cn;
+  const double cs = C1 * svb * hrvo * ry * hvc;
+  const double cw = C1 * sub * hruo * rx * huc;
+  const double ce = C1 * sube * hruoe * rxe * huce;
+  const double cn = C1 * svbn * hrvon * ryn * hvcn;
+  const double cc = c.delti * dxyp - cs - cw - ce - cn;
   X.cs[d] = cs;
   X.cw[d] = cw;
   X.ce[d] = ce;
@@ -168,7 +174,19 @@ __global__ void __launch_bounds__(NT, BARO ? 4 : 8) k_begin(DevStatic S, DevStat
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
     if (S.kind[d] == LAND) continue;
+    // every result first, the stores after (a store before a load would keep
+    // the compiler from issuing the load early: the arrays could alias)
     const double sub = X.sub[d], svb = X.svb[d];
+    const double P = X.p[d];
+    double FPGXE = 0., FPGYE = 0.;
+    if (BARO && c.baro)  // :192-201 (entry HP, HU, HV, SBX, SBY)
+      baro_faces(S, X, c, q, HE, FPGXE, FPGYE);
+    const double uh = UE[d], vh = VE[d];
+    const double fuh =
+        fuh_face(S, X, c, d, uh, X.hu[d], P, X.p[q.w], sub, FPGXE, X.tsx[d], X.tbx[d]);
+    const double fvh =
+        fvh_face(S, X, c, d, vh, X.hv[d], P, X.p[q.s], svb, FPGYE, X.tsy[d], X.tby[d]);
+    const double fp1 = fp1_cell(S, c, q, P, UE, VE);
     if (c.isdry > 0) {  // :172-190
       X.iscdry[d] = 0;
       X.sub1[d] = sub;
@@ -177,13 +195,8 @@ __global__ void __launch_bounds__(NT, BARO ? 4 : 8) k_begin(DevStatic S, DevStat
       if (c.ndrystp < 0 && c.isbal > 0) X.qdwaste[d] = 0.;
       X.wasted[d] = 0;
     }
-    const double P = X.p[d];
-    double FPGXE = 0., FPGYE = 0.;
-    if (BARO && c.baro)  // :192-201 (entry HP, HU, HV, SBX, SBY)
-      baro_faces(S, X, c, q, HE, FPGXE, FPGYE);
-    const double uh = UE[d], vh = VE[d];
-    X.fuhdye[d] = fuh_face(S, X, c, d, uh, X.hu[d], P, X.p[q.w], sub, FPGXE, X.tsx[d], X.tbx[d]);
-    X.fvhdxe[d] = fvh_face(S, X, c, d, vh, X.hv[d], P, X.p[q.s], svb, FPGYE, X.tsy[d], X.tby[d]);
+    X.fuhdye[d] = fuh;
+    X.fvhdxe[d] = fvh;
     if (COPY) {
       X.uhdy1e[d] = uh;
       X.vhdx1e[d] = vh;
@@ -195,7 +208,7 @@ __global__ void __launch_bounds__(NT, BARO ? 4 : 8) k_begin(DevStatic S, DevStat
       X.sbx[d] = S.sbxo[d];
       X.sby[d] = S.sbyo[d];
     }
-    X.fp1[d] = fp1_cell(S, c, q, P, UE, VE);
+    X.fp1[d] = fp1;
   }
 #undef UE
 #undef VE
@@ -505,15 +518,28 @@ __global__ void __launch_bounds__(NT) k_scale32(DevStatic S, SysView V, DevSyste
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
     if (S.kind[d] == LAND) continue;
-    const double di = inv_sqrt_diag(V.cc[d]);
-    auto off = [&](double cnb, int x) {
-      return S.kind[x] == LAND ? 0.f : float(cnb * di * inv_sqrt_diag(V.cc[x]));
-    };
-    Y.as32[d] = off(V.cs[d], q.s);
-    Y.aw32[d] = off(V.cw[d], q.w);
+    // the loads first (the stores below could alias them for the compiler)
+    const double cc = V.cc[d], cs = V.cs[d], cw = V.cw[d], ccs = V.cc[q.s], ccw = V.cc[q.w];
+    const bool ls = S.kind[q.s] == LAND, lw = S.kind[q.w] == LAND;
+    double ce = 0., cn = 0., cce = 1., ccn = 1.;
+    bool le = true, ln = true;
     if (write_cross) {
-      Y.ae32[d] = off(V.ce[d], q.e);
-      Y.an32[d] = off(V.cn[d], q.n);
+      ce = V.ce[d];
+      cn = V.cn[d];
+      cce = V.cc[q.e];
+      ccn = V.cc[q.n];
+      le = S.kind[q.e] == LAND;
+      ln = S.kind[q.n] == LAND;
+    }
+    const double di = inv_sqrt_diag(cc);
+    auto off = [&](double cnb, bool land, double cx) {
+      return land ? 0.f : float(cnb * di * inv_sqrt_diag(cx));
+    };
+    Y.as32[d] = off(cs, ls, ccs);
+    Y.aw32[d] = off(cw, lw, ccw);
+    if (write_cross) {
+      Y.ae32[d] = off(ce, le, cce);
+      Y.an32[d] = off(cn, ln, ccn);
     }
   }
 }
@@ -707,8 +733,8 @@ __global__ void __launch_bounds__(NT) k_red_cg_update(DevStatic S, Ctl *ctl, Glo
 // in FP64, and the FP32 scaled inner system's rhs rhat = D^-1/2 r with
 // x = 0 and p0 = rhat (k_mx_zinit then forms z0 = M^-1 rhat and p_old = 0 for
 // the polynomial members).  rsqm_fac scales the member's RSQM (the MIXED stop,
-// below RSQM).
-template <bool MA>
+// below RSQM).  EAGER: the row's loads issued first (kernel variant 3).
+template <bool MA, bool EAGER>
 __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, SysView V, DevSystem Y,
                                                 const double *P, const Ctl *ctl, double *part) {
   struct A {
@@ -717,7 +743,11 @@ __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, SysView V, DevSyst
   quad_sweep<2>(
       S, part, [&](int m) { return A{ctl[m].done != 0, unsym<MA>(ctl[m])}; },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
-        const V4<double> r = residual_row(g, S.kind, P, V, a.asym);
+        V4<double> r;
+        if constexpr (EAGER)
+          r = residual_row_eager(g, S.kind, P, V, a.asym);
+        else
+          r = residual_row(g, S.kind, P, V, a.asym);
         const V4<double> c = ld4(V.cc + g.d0);
         const V4<float> r32 = {float(r.x * inv_sqrt_diag(c.x)), float(r.y * inv_sqrt_diag(c.y)),
                                float(r.z * inv_sqrt_diag(c.z)), float(r.w * inv_sqrt_diag(c.w))};
@@ -827,15 +857,17 @@ __global__ void __launch_bounds__(NT) k_backsub(DevStatic S, DevState X, int nti
     const Nb q = neighbours(S.tnbr, tile, threadIdx.x);
     const int d = q.d;
     if (S.kind[d] == LAND) continue;
-    const double P = X.p[d];
-    const double u = X.sub[d] *
-                     (X.fuhdye[d] - c.deltd2 * S.hruo[d] * rc_x(X, c, d) * X.huc[d] * (P - X.p[q.w]));
-    const double v = X.svb[d] *
-                     (X.fvhdxe[d] - c.deltd2 * S.hrvo[d] * rc_y(X, c, d) * X.hvc[d] * (P - X.p[q.s]));
+    // the loads first (the stores below could alias them for the compiler)
+    const double P = X.p[d], PW = X.p[q.w], PS = X.p[q.s];
+    const double sub = X.sub[d], svb = X.svb[d], fuh = X.fuhdye[d], fvh = X.fvhdxe[d];
+    const double hruo = S.hruo[d], hrvo = S.hrvo[d], huc = X.huc[d], hvc = X.hvc[d];
+    const double rx = rc_x(X, c, d), ry = rc_y(X, c, d), dyiu = S.dyiu[d], dxiv = S.dxiv[d];
+    const double u = sub * (fuh - c.deltd2 * hruo * rx * huc * (P - PW));
+    const double v = svb * (fvh - c.deltd2 * hrvo * ry * hvc * (P - PS));
     X.uhdye[d] = u;
     X.vhdxe[d] = v;
-    X.uhe[d] = u * S.dyiu[d];
-    X.vhe[d] = v * S.dxiv[d];
+    X.uhe[d] = u * dyiu;
+    X.vhe[d] = v * dxiv;
   }
 }
 
@@ -1132,11 +1164,13 @@ __global__ void __launch_bounds__(NT) k_fin(DevStatic S, DevState X, int ntile, 
     const int d = q.d;
     int neg = 0, bad = 0;
     if (S.kind[d] != LAND) {
-      const double hp = X.hp[d];
-      if (c.isdry == 0) X.p[d] = c.g * (hp + S.belv[d]);
-      const double dxyp = S.dxyp[d];
-      const double hu = (dxyp * hp + S.dxyp[q.w] * X.hp[q.w]) * S.fsgzu[d];
-      const double hv = (dxyp * hp + S.dxyp[q.s] * X.hp[q.s]) * S.fsgzv[d];
+      // the loads first (the stores below could alias them for the compiler)
+      const double hp = X.hp[d], hpw = X.hp[q.w], hps = X.hp[q.s], belv = S.belv[d];
+      const double dxyp = S.dxyp[d], dxypw = S.dxyp[q.w], dxyps = S.dxyp[q.s];
+      const double fsgzu = S.fsgzu[d], fsgzv = S.fsgzv[d];
+      if (c.isdry == 0) X.p[d] = c.g * (hp + belv);
+      const double hu = (dxyp * hp + dxypw * hpw) * fsgzu;
+      const double hv = (dxyp * hp + dxyps * hps) * fsgzv;
       X.hu[d] = hu;
       X.hv[d] = hv;
       if (c.isdry > 0) {
@@ -1260,9 +1294,17 @@ void launch_sweep_reset(const Launch &l, Ctl *ctl, const int *act, int nmember) 
   k_sweep_reset<<<(nmember + 255) / 256, 256, 0, l.stream>>>(ctl, act, nmember);
   count_launches(1);
 }
+static int blocks_per_sm(const void *kernel);
+// The grid of a cell kernel whose resident CTAs per SM differ from the
+// others': its own occupancy times the SMs, at most one CTA per tile.
+template <class K>
+static int cell_grid(const Launch &l, K kernel) {
+  const int per_sm = blocks_per_sm(reinterpret_cast<const void *>(kernel));
+  return std::max(1, std::min(l.ntile - 1, l.nsm * per_sm));
+}
 void launch_assemble(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
                      const int *act) {
-  k_assemble<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, ctl, act);
+  k_assemble<<<cell_grid(l, k_assemble), NT, 0, l.stream>>>(S, X, l.ntile, ctl, act);
   count_launches(1);
 }
 void launch_obc(const Launch &l, const DevStatic &S, const DevState &X, const DevObc &B, Ctl *ctl,
@@ -1359,11 +1401,20 @@ void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, dou
 void launch_mx_resid(const Launch &l, const DevStatic &S, const SysView &V, const DevSystem &Y,
                      const double *P, Ctl *ctl, Glob *glob, double *part, double rsqm_fac,
                      double rel_tol, int no_stop) {
-  if (l.may_asym)
-    k_mx_resid<true><<<quad_grid(l, S, k_mx_resid<true>), NT, 0, l.stream>>>(S, V, Y, P, ctl, part);
-  else
-    k_mx_resid<false><<<quad_grid(l, S, k_mx_resid<false>), NT, 0, l.stream>>>(S, V, Y, P, ctl,
-                                                                             part);
+  if (l.variant == 3) {
+    if (l.may_asym)
+      k_mx_resid<true, true><<<quad_grid(l, S, k_mx_resid<true, true>), NT, 0, l.stream>>>(
+          S, V, Y, P, ctl, part);
+    else
+      k_mx_resid<false, true><<<quad_grid(l, S, k_mx_resid<false, true>), NT, 0, l.stream>>>(
+          S, V, Y, P, ctl, part);
+  } else if (l.may_asym) {
+    k_mx_resid<true, false><<<quad_grid(l, S, k_mx_resid<true, false>), NT, 0, l.stream>>>(
+        S, V, Y, P, ctl, part);
+  } else {
+    k_mx_resid<false, false><<<quad_grid(l, S, k_mx_resid<false, false>), NT, 0, l.stream>>>(
+        S, V, Y, P, ctl, part);
+  }
   launch_chan_resmx(l, S, V, Y, P, ctl, part);
   k_red_mx_resid<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, rsqm_fac, rel_tol,
                                                       no_stop, V.unscaled, l.inner_margin);
@@ -1592,12 +1643,11 @@ void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y,
   }
 }
 
-int occupancy_blocks_per_sm() {
-  int a = 0, b = 0, c = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_assemble, NT, 0);
+int occupancy_blocks_per_sm() {  // k_assemble holds more values: its own grid (cell_grid)
+  int b = 0, c = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_begin<false, false>, NT, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_fin, NT, 0);
-  const int m = std::min(a, std::min(b, c));
+  const int m = std::min(b, c);
   return m > 0 ? m : 1;
 }
 
@@ -1606,7 +1656,7 @@ int occupancy_blocks_per_sm_cg() {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_mx_apply, NT, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cg_update, NT, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_cg_init<true>, NT, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_mx_resid<true>, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_mx_resid<true, false>, NT, 0);
   const int m = std::min(std::min(a, b), std::min(c, d));
   return m > 0 ? m : 1;
 }

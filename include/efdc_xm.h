@@ -541,10 +541,12 @@ int64_t efdc_xm_host_waits(void);
  *     kernels; 0 fetches each 4-tile unit's descriptors (its member's values,
  *     its tiles' neighbours) one unit ahead, 1 fetches them for 32 units at a
  *     time into shared memory, 2 does that and also stages each unit's rows
- *     in shared memory with bulk copies issued one unit ahead.  All give the
- *     same results bit for bit.
+ *     in shared memory with bulk copies issued one unit ahead, 3 fetches them
+ *     as 1 does and issues every load of a row before the row's first
+ *     dependent operation (at fewer CTAs per SM).  All give the same results
+ *     bit for bit.
  *   EFDC_XM_OPT_CTAS_MATVEC, EFDC_XM_OPT_CTAS_UPDATE (default 0, 0..32): with
- *     variants 1 and 2, caps on the resident CTAs per SM of the inner
+ *     variants 1, 2 and 3, caps on the resident CTAs per SM of the inner
  *     iteration's matrix-vector and update kernels (0: as many as fit).
  *   EFDC_XM_OPT_POLY_THRESHOLD (default 10, 0..100000): a MIXED member whose
  *     last solve took more than this many Jacobi-equivalent inner iterations

@@ -2,7 +2,8 @@
 
 Variant 0 fetches each 4-tile unit's descriptors one unit ahead, variant 1 in
 batches of 32 units into shared memory, variant 2 also stages the units' rows
-in shared memory with bulk copies issued one unit ahead.  They run the same
+in shared memory with bulk copies issued one unit ahead, variant 3 fetches them
+as 1 does and issues all of a row's loads before its first dependent operation.  They run the same
 arithmetic on the same values, so a batch steps to the same state bit for
 bit: Jacobi and polynomial members, an unsymmetric (radiation) member, and
 wetting and drying.  The staged variant's kernels also time through
@@ -41,7 +42,8 @@ def run(mem, steps, tm, variant, caps=(0, 0), timed=False):
     return sts, stats, kt
 
 
-@pytest.mark.parametrize("variant,caps", [(1, (0, 0)), (2, (0, 0)), (2, (2, 2))])
+@pytest.mark.parametrize("variant,caps", [(1, (0, 0)), (2, (0, 0)), (2, (2, 2)), (3, (0, 0)),
+                                           (3, (2, 2))])
 def test_variants_equal_variant0(variant, caps):
     mem = [cases.build(n)[0] for n in ("basin_fp64", "noise_forcing", "radiation_all_sides",
                                        "tidal_flat_99")]
