@@ -287,6 +287,13 @@ def wetdry(args, torch, dev, rank):
         return t, its, sweeps, out
 
     t64, it64, sw64, m64 = run(X.PREC_FP64)
+    if args.variant < 0:  # the MIXED schedule for this batch, as for the ensemble
+        bs.upload([sc.state for sc in scns])
+        bs.step_device(prm(1, X.PREC_MIXED))
+        with tempfile.TemporaryDirectory() as td:
+            bs.autotune(X.PREC_MIXED, Path(td) / "schedules.txt", measure=True)
+    else:
+        bs.set_option(X.OPT_KERNEL_VARIANT, args.variant)
     tmx, _itmx, swmx, mmx = run(X.PREC_MIXED)
     credit = float((cells * it64).sum())
     free_diff = sum(int(np.sum(a[k][1:sc.la] != b[k][1:sc.la])) for a, b, sc in
@@ -918,6 +925,16 @@ def ours(args):
             return sum(ts) / 1e3, its
 
         t64b, it64 = run1(X.PREC_FP64)
+        # the MIXED schedule for this basin, as for the ensemble
+        sched_b = None
+        if args.variant < 0:
+            sol.upload(scn.state)
+            sol.step_device(X.make_params(scn.params, n=1, tn=scn.tn(1), precision=X.PREC_MIXED))
+            with tempfile.TemporaryDirectory() as td:
+                sched_b, _ms = sol.autotune(X.PREC_MIXED, Path(td) / "schedules.txt",
+                                            measure=True)
+        elif args.variant >= 0:
+            sol.set_option(X.OPT_KERNEL_VARIANT, args.variant)
         tmxb, _ = run1(X.PREC_MIXED)
         kb = sol.time_kernels(X.PREC_MIXED, reps=20)
         t64b, tmxb = max_over_ranks(t64b, tmxb)
@@ -949,7 +966,8 @@ def ours(args):
                   "k_mx_matvec_frac": 24.0 * kb.ncells / (kb.ms_matvec * 1e-3) / 1e9 / peak,
                   "update_ms": kb.ms_update,
                   "update_frac": (24.0 * kb.ncells + 12.0 * kb.ncells_poly) /
-                                 (kb.ms_update * 1e-3) / 1e9 / peak}
+                                 (kb.ms_update * 1e-3) / 1e9 / peak,
+                  "schedule": sched_b}
         sol.close()
         del fl
     wd_res = None
