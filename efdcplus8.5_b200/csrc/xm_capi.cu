@@ -270,6 +270,8 @@ struct efdc_xm_ctx {
   int kvariant = 0, ctas_mv = 0, ctas_up = 0;
   int inner_margin_log10 = 0;   // MIXED inner target margin 10^-v
   int inner_tol_x10 = 60;       // MIXED inner relative tolerance 10^(-v/10) at least
+  bool small_solve = true;      // FP64: members small enough solve in one CTA each
+  int small_slots = 0;          // the largest member window (its ghost tile and tiles)
   float poly_threshold = 10.f;  // MIXED: polynomial preconditioner above this Jacobi count
   xm::Launch L() const {
     xm::Launch l{grid,      grid_cg, grid_cg32, grid_up32,
@@ -639,9 +641,30 @@ int scaled_system(efdc_xm_ctx *c) {
 // FP64 CONGRAD of every active member on the scaled system in c->Y.  The
 // members iterate in lockstep launches; a member that has stopped is skipped
 // by the kernels.  On return c->ctl_h holds each member's outcome.
+// FP64 solves in one CTA per member (k_cg_small): every member's window fits
+// in a CTA's shared memory and no member has sub-grid channels (their terms
+// are separate kernels of the multi-kernel CG).
+bool small_solve(const efdc_xm_ctx *c) {
+  return c->small_solve && c->small_slots > 0 && xm::cg_small_fits(c->small_slots) &&
+         c->S.ch.n == 0;
+}
+
 int solve_fp64(efdc_xm_ctx *c, double *P) {
   const xm::Launch l = c->L();
   xm::launch_solve_reset(l, c->ctl, c->glob, c->act, c->M);
+  if (small_solve(c)) {  // the whole CG of each member in one CTA (k_cg_small)
+    xm::launch_cg_small(l, c->S, c->Y, P, c->ctl, c->glob, c->part, c->small_slots, c->M);
+    CK(cudaGetLastError());
+    int rc = read_ctl(c);
+    if (rc) return rc;
+    for (int m = 0; m < c->M; ++m) {
+      if (!c->act_h[m]) continue;
+      Ctl &k = c->ctl_h[m];
+      if (!k.done && k.status == 0) k.status = EFDC_XM_CG_MAXITER;
+      if (k.iter > 0) c->mem[m].last_iters = k.iter;
+    }
+    return EFDC_XM_OK;
+  }
   xm::launch_cg_init(l, c->S, c->Y, P, c->ctl, c->glob, c->part);
   CK(cudaGetLastError());
   int chunk = 1, cap = 1;
@@ -986,6 +1009,8 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   c->ntile = ntile;
   c->nslot = ntile * TILE;
   c->stage_len = off;
+  for (const Member &mb : c->mem)  // the member windows of k_cg_small
+    c->small_slots = std::max(c->small_slots, (mb.tile1 - mb.tile0 + 1) * TILE);
   auto bail = [&](const char *what) -> efdc_xm_ctx * {
     if (g_last_error.empty()) set_error("efdc_xm_create: %s", what);
     efdc_xm_destroy(c);
@@ -1798,7 +1823,7 @@ struct StepPlan {
   int mixed, istl, all, any_isdry, any_legacy, any99, any_waste, iters;
   int max_iterm, max_sweeps, grid, grid_cg, grid_cg32, grid_up32;
   int mx_jac, mx_poly, may_asym, chan, baro, obc_serial, any_may_asym, nmember;
-  int variant, ctas_mv, ctas_up, any_drag;
+  int variant, ctas_mv, ctas_up, any_drag, small;
   double fac, inner_margin;
   const void *psol;
 };
@@ -1885,6 +1910,12 @@ cudaError_t capture_solve(efdc_xm_ctx *c, const StepPlan &pl, int d, StepGraph &
   l.stream = st;
   const int M = c->M, K = pl.iters;
   double *P = c->X.p;
+  if (!pl.mixed && pl.small) {  // one CTA per member, its loop inside (k_cg_small)
+    xm::launch_solve_reset(l, c->ctl, c->glob, c->act, M);
+    xm::launch_cg_small(l, c->S, c->Y, P, c->ctl, c->glob, c->part, c->small_slots, M);
+    take_count(mark, mine);
+    return cudaGetLastError();
+  }
   if (!pl.mixed) {
     xm::launch_solve_reset(l, c->ctl, c->glob, c->act, M);
     xm::launch_cg_init(l, c->S, c->Y, P, c->ctl, c->glob, c->part);
@@ -2279,6 +2310,7 @@ int tune_time(efdc_xm_ctx *c, bool mixed, double fac, int reps, double *ms) {
   const xm::Launch lk = c->L();
   StepPlan pl{};
   pl.mixed = mixed;
+  pl.small = !mixed && small_solve(c);
   pl.iters = c->graph_iters;
   pl.max_iterm = 1;
   for (int m = 0; m < c->M; ++m) pl.max_iterm = std::max(pl.max_iterm, c->sc_h[m].iterm);
@@ -2456,6 +2488,7 @@ int step_range(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_stats *stats, 
     StepPlan pl{};
     const xm::Launch lk = c->L();
     pl.mixed = mixed;
+    pl.small = !mixed && small_solve(c);
     pl.istl = istl;
     pl.all = all;
     pl.any_isdry = any_isdry;
@@ -3921,6 +3954,13 @@ int32_t efdc_xm_set_option(efdc_xm_ctx *c, int32_t option, int32_t value) {
       if (value < 0 || value > 6) break;
       if (value != c->inner_margin_log10) {
         c->inner_margin_log10 = value;
+        drop_graphs(c);
+      }
+      return EFDC_XM_OK;
+    case EFDC_XM_OPT_SMALL_SOLVE:
+      if (value < 0 || value > 1) break;
+      if ((value != 0) != c->small_solve) {
+        c->small_solve = value != 0;
         drop_graphs(c);
       }
       return EFDC_XM_OK;

@@ -441,9 +441,12 @@ __device__ __forceinline__ double matvec_row(const RowGeo &g, bool valid, const 
          double(a.w) * double(p.w);
 }
 
+
 // FP64: as matvec_row, with z = CCCI*r stored by the kernels that write r, so
 // that the halo rows need z and p_old only: p = z + beta*p_old has the same
-// roundings as CCCI*r + beta*p_old formed in place.
+// roundings as CCCI*r + beta*p_old formed in place.  Every load of the row is
+// issued before its first shuffle or dependent operation (see
+// matvec_row_scaled_eager): one round trip to memory per row.
 __device__ __forceinline__ double matvec_row_z(const RowGeo &g, bool valid,
                                                const double *__restrict__ z,
                                                const double *__restrict__ ccc,
@@ -454,25 +457,27 @@ __device__ __forceinline__ double matvec_row_z(const RowGeo &g, bool valid,
                                                const double *__restrict__ cce,
                                                const double *__restrict__ ccn,
                                                double *__restrict__ ap, double beta, bool asym) {
+  // every load first, so that one round trip serves the row
   const V4<double> z0 = ld4(z + g.d0), o0 = ld4(pold + g.d0);
   const V4<double> zn = ld4(z + g.dn), on = ld4(pold + g.dn);
   const V4<double> zs = ld4(z + g.ds), os = ld4(pold + g.ds);
+  const V4<double> c0 = ld4(ccc + g.d0), ks = ld4(ccs + g.d0), kw = ld4(ccw + g.d0);
+  const V4<double> kn = asym ? ld4(ccn + g.d0) : ld4(ccs + g.dn);
+  V4<double> ke = asym ? ld4(cce + g.d0) : V4<double>{0., 0., 0., 0.};
+  const bool west = g.cx == 0, east = g.cx == ROWT - 1;
+  const double zw = west ? z[g.dwe] : 0., ow = west ? pold[g.dwe] : 0.;
+  const double ze = east ? z[g.dee] : 0., oe = east ? pold[g.dee] : 0.;
+  const double kwe_edge = (east && !asym) ? ccw[g.dee] : 0.;
   auto pc = [&](double zz, double po) { return zz + beta * po; };
   const V4<double> p = {pc(z0.x, o0.x), pc(z0.y, o0.y), pc(z0.z, o0.z), pc(z0.w, o0.w)};
   const V4<double> pn = {pc(zn.x, on.x), pc(zn.y, on.y), pc(zn.z, on.z), pc(zn.w, on.w)};
   const V4<double> ps = {pc(zs.x, os.x), pc(zs.y, os.y), pc(zs.z, os.z), pc(zs.w, os.w)};
   double pw = from_west(p), pe = from_east(p);
-  if (g.cx == 0) pw = pc(z[g.dwe], pold[g.dwe]);
-  if (g.cx == ROWT - 1) pe = pc(z[g.dee], pold[g.dee]);
-  const V4<double> c0 = ld4(ccc + g.d0), ks = ld4(ccs + g.d0), kw = ld4(ccw + g.d0);
-  V4<double> kn, ke;
-  if (asym) {
-    kn = ld4(ccn + g.d0);
-    ke = ld4(cce + g.d0);
-  } else {
-    kn = ld4(ccs + g.dn);
+  if (west) pw = pc(zw, ow);
+  if (east) pe = pc(ze, oe);
+  if (!asym) {
     double kwe = from_east(kw);
-    if (g.cx == ROWT - 1) kwe = ccw[g.dee];
+    if (east) kwe = kwe_edge;
     ke = {kw.y, kw.z, kw.w, kwe};
   }
   V4<double> a;

@@ -56,6 +56,13 @@ void launch_explicit(const Launch &l, const DevStatic &S, const MomDev &M, const
 void launch_implicit_drag(const Launch &l, const DevStatic &S, const DevState &X,
                           const int *act);
 void launch_put(cudaStream_t st, const int *idx, const double *val, int n, double *dst);
+// CONGRAD of small members, one CTA each with its vectors in shared memory
+// (k_cg_small): the windows of every member fit when cg_small_fits(the
+// largest window's slots); the same iterates as the multi-kernel CG.
+constexpr int SMALL_SMEM_MAX = 200 * 1024;
+bool cg_small_fits(int slots);
+void launch_cg_small(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
+                     Ctl *ctl, Glob *glob, double *part, int max_slots, int nmember);
 void launch_put_int(cudaStream_t st, const int *idx, const int *val, int n, int *dst);
 // sub-grid channels (xm_chan.cu); each does nothing unless l.chan
 void launch_chan_entry(const Launch &l, const DevStatic &S, const DevState &X, const int *act);

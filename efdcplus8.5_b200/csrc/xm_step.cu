@@ -14,6 +14,7 @@
 
 #include <map>
 #include <mutex>
+#include <type_traits>
 
 #include "xm_cg.cuh"
 #include "xm_kernels.h"
@@ -600,6 +601,51 @@ __global__ void k_outer_reset(Glob *glob) { glob->nidone = 0; }
 // p double-buffered (pa/pb, selected by ctl[m].parity), Ap.  z = CCCI*r with
 // CCCI = 1./CCC is recomputed where needed instead of stored.
 
+// The members' epilogues of the three reductions (thread 0 of the member):
+// :88 RETURN on RPCG = 0; :124 ALPHA; :143-169 BETA, RSQ and the stop test.
+// With no_stop the iteration continues past RSQM and ITERM (kernel timing).
+__device__ __forceinline__ void cg_init_epi(Ctl &k, Glob *glob, double rpcg) {
+  k.rpcg = rpcg;
+  k.beta = 0.0;
+  k.parity = 0;
+  k.iter = 0;
+  k.rsq = 0.0;
+  k.status = 0;
+  if (rpcg == 0.0 || !isfinite(rpcg)) {  // :88 RETURN
+    if (!isfinite(rpcg)) k.status = EFDC_XM_NONFINITE;
+    k.done = 1;
+    atomicAdd(&glob->ndone, 1);
+  }
+}
+__device__ __forceinline__ void cg_matvec_epi(Ctl &k, double pap) {
+  k.papcg = pap;
+  k.alpha = k.rpcg / pap;  // :124
+}
+__device__ __forceinline__ void cg_update_epi(Ctl &k, Glob *glob, const StepScalars &c,
+                                              double rpcgn, double rsq, int no_stop) {
+  k.beta = rpcgn / k.rpcg;
+  k.rpcg = rpcgn;
+  k.rsq = rsq;
+  const int it = k.iter + 1;
+  k.iter = it;
+  int fin = 0;
+  if (!isfinite(rsq) || !isfinite(k.alpha)) {
+    k.status = EFDC_XM_NONFINITE;
+    fin = 1;
+  } else if (!no_stop && rsq <= c.rsqm) {
+    fin = 1;
+  } else if (!no_stop && it >= c.iterm) {
+    k.status = EFDC_XM_CG_MAXITER;
+    fin = 1;
+  } else {
+    k.parity ^= 1;
+  }
+  if (fin) {
+    k.done = 1;
+    atomicAdd(&glob->ndone, 1);
+  }
+}
+
 // :54-88 initial residual, z0 = CCCI*r, RPCG.
 template <bool MA>
 __global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double *P, Ctl *ctl,
@@ -627,27 +673,14 @@ __global__ void __launch_bounds__(NT) k_red_cg_init(DevStatic S, Ctl *ctl, Glob 
   member_reduce<1>(
       S, part, [&](int m) { return ctl[m].done != 0; },
       [&](int m, const double *sum) {
-        if (threadIdx.x != 0) return;
-        Ctl &k = ctl[m];
-        const double rpcg = sum[0];
-        k.rpcg = rpcg;
-        k.beta = 0.0;
-        k.parity = 0;
-        k.iter = 0;
-        k.rsq = 0.0;
-        k.status = 0;
-        if (rpcg == 0.0 || !isfinite(rpcg)) {  // :88 RETURN
-          if (!isfinite(rpcg)) k.status = EFDC_XM_NONFINITE;
-          k.done = 1;
-          atomicAdd(&glob->ndone, 1);
-        }
+        if (threadIdx.x == 0) cg_init_epi(ctl[m], glob, sum[0]);
       });
 }
 
 // :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA).
 template <bool MA>
-__global__ void __launch_bounds__(NT, MA ? 2 : 3) k_cg_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
-                                                 double *part) {
+__global__ void __launch_bounds__(NT, 2) k_cg_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
+                                                    double *part) {
   struct A {
     bool skip, asym;
     double beta;
@@ -670,9 +703,7 @@ __global__ void __launch_bounds__(NT) k_red_cg_matvec(DevStatic S, Ctl *ctl, con
   member_reduce<1>(
       S, part, [&](int m) { return ctl[m].done != 0; },
       [&](int m, const double *sum) {
-        if (threadIdx.x != 0) return;
-        ctl[m].papcg = sum[0];
-        ctl[m].alpha = ctl[m].rpcg / sum[0];  // :124
+        if (threadIdx.x == 0) cg_matvec_epi(ctl[m], sum[0]);
       });
 }
 
@@ -700,32 +731,176 @@ __global__ void __launch_bounds__(NT) k_red_cg_update(DevStatic S, Ctl *ctl, Glo
   member_reduce<2>(
       S, part, [&](int m) { return ctl[m].done != 0; },
       [&](int m, const double *sum) {
-        if (threadIdx.x != 0) return;
-        Ctl &k = ctl[m];
-        const StepScalars &c = S.sc[m];
-        const double rpcgn = sum[0], rsq = sum[1];
-        k.beta = rpcgn / k.rpcg;
-        k.rpcg = rpcgn;
-        k.rsq = rsq;
-        const int it = k.iter + 1;
-        k.iter = it;
-        int fin = 0;
-        if (!isfinite(rsq) || !isfinite(k.alpha)) {
-          k.status = EFDC_XM_NONFINITE;
-          fin = 1;
-        } else if (!no_stop && rsq <= c.rsqm) {
-          fin = 1;
-        } else if (!no_stop && it >= c.iterm) {
-          k.status = EFDC_XM_CG_MAXITER;
-          fin = 1;
-        } else {
-          k.parity ^= 1;
-        }
-        if (fin) {
-          k.done = 1;
-          atomicAdd(&glob->ndone, 1);
-        }
+        if (threadIdx.x == 0) cg_update_epi(ctl[m], glob, S.sc[m], sum[0], sum[1], no_stop);
       });
+}
+
+// ---------------------------------------------------------------------------
+// CONGRAD of small members, the whole solve in one CTA per member: the
+// member's CG vectors (P, r, z, p double-buffered, Ap) stay in shared memory
+// from the first residual to the stop test, its units run SMALL_UNITS at a
+// time, and the coefficient arrays are read from global memory.  The rows
+// (the same row functions), the per-unit partial sums (warp sums added in
+// warp order), the member sums (reduce_partials of a 256-thread CTA) and the
+// epilogues are those of k_cg_init, k_cg_matvec, k_cg_update and their member
+// reductions, so the iterates equal theirs bit for bit; one launch replaces
+// 2 + 4 per iteration.  The rows of a unit past the member's last tile work
+// on the member's ghost tile with stores off, so that every access stays in
+// the member's window of slots, [its ghost tile, its last tile].
+constexpr int SMALL_UNITS = 2;
+constexpr int SMALL_NT = SMALL_UNITS * NT;
+
+// reduce_partials of a 256-thread CTA, by a CTA of SMALL_NT threads (the
+// threads past the first 256 add nothing, as block_sum's last stage reads 8
+// warps), from the partials in shared memory
+constexpr int SMALL_MAX_UNITS = 64;
+__device__ __forceinline__ double reduce_partials_256(const double *part, int nblk, double *sh) {
+  double s = 0.0;
+  for (int base = 0; base < nblk; base += 8 * NT) {
+    double v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int i = base + j * NT + int(threadIdx.x);
+      v[j] = (threadIdx.x < NT && i < nblk) ? part[i] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s += v[j];
+  }
+  return block_sum(s, sh);
+}
+
+template <bool MA>
+__global__ void __launch_bounds__(SMALL_NT) k_cg_small(DevStatic S, DevSystem Y, double *P,
+                                                      Ctl *ctl, Glob *glob, double *part) {
+  extern __shared__ double smv[];
+  __shared__ double sh[32];
+  __shared__ double wp[2][SMALL_NT / 32];
+  __shared__ double qp[2][SMALL_MAX_UNITS];  // the member's per-unit partials
+  __shared__ double s_beta, s_alpha;          // the member's control values, as thread 0
+  __shared__ int s_done, s_parity;            // leaves them in ctl[m]
+  const int m = blockIdx.x;
+  if (ctl[m].done) return;  // not in this sweep
+  // thread 0 runs the epilogues on ctl[m] and shares what the loop reads
+  auto share = [&] {
+    if (threadIdx.x == 0) {
+      const Ctl &k = ctl[m];
+      s_done = k.done;
+      s_parity = k.parity;
+      s_beta = k.beta;
+      s_alpha = k.alpha;
+    }
+    __syncthreads();
+  };
+  const int q0 = S.qstart[m], q1 = S.qstart[m + 1], nq = q1 - q0;
+  const int ghost = S.quads[q0].y - 1;  // the member's ghost tile, before its tiles
+  const int base = ghost * TILE, nsl = (S.tend[m] - ghost) * TILE;
+  double *gv[6] = {P, Y.r, Y.z, Y.pa, Y.pb, Y.ap};
+  for (int i = threadIdx.x; i < nsl; i += SMALL_NT)
+#pragma unroll
+    for (int k = 0; k < 6; ++k) smv[k * nsl + i] = gv[k][base + i];
+  __syncthreads();
+  // pointers that take the slot d of the window to shared memory
+  double *const Ps = smv - base;
+  DevSystem Ys = Y;
+  Ys.r = smv + nsl - base;
+  Ys.z = smv + 2 * nsl - base;
+  Ys.pa = smv + 3 * nsl - base;
+  Ys.pb = smv + 4 * nsl - base;
+  Ys.ap = smv + 5 * nsl - base;
+  const int qi = threadIdx.x / NT, tq = threadIdx.x % NT;
+  const int sub = tq / TPT, q = tq % TPT;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool asym = unsym<MA>(ctl[m]);
+
+  // one sweep of a row body over the member's units, as quad_sweep makes it
+  auto sweep = [&](auto body, auto ns_tag) {
+    constexpr int NS = decltype(ns_tag)::value;
+    for (int u0 = q0; u0 < q1; u0 += SMALL_UNITS) {
+      const int qd = u0 + qi;
+      const bool have = qd < q1;
+      const int4 cur = have ? S.quads[qd] : int4{m, ghost, 0, 0};
+      const bool valid = have && sub < cur.z;
+      const int ti = valid ? cur.y + sub : ghost;
+      const RowGeo g = row_geo_nb(__ldg(&S.tnbr[ti]), ti, q);
+      double v[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) v[s] = 0.0;
+      body(g, valid, v);
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const double x = warp_sum(v[s]);
+        if (lane == 0) wp[s][warp] = x;
+      }
+      __syncthreads();
+      if (tq == 0 && have) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          double a = 0.0;
+#pragma unroll
+          for (int w = 0; w < NWARP; ++w) a += wp[s][qi * NWARP + w];
+          qp[s][qd - q0] = a;
+        }
+      }
+      __syncthreads();
+    }
+  };
+  using One = std::integral_constant<int, 1>;
+  using Two = std::integral_constant<int, 2>;
+
+  // :54-88
+  sweep(
+      [&](const RowGeo &g, bool valid, double *v) {
+        const V4<double> r = residual_row(g, S.kind, Ps, Ys, asym);
+        const V4<double> c = ld4(Y.ccc + g.d0);
+        const V4<double> z = {r.x * rcpT(c.x), r.y * rcpT(c.y), r.z * rcpT(c.z),
+                              r.w * rcpT(c.w)};
+        if (valid) {
+          st4(Ys.r + g.d0, r);
+          st4(Ys.pa + g.d0, z);
+          st4(Ys.z + g.d0, z);
+          v[0] = r.x * z.x + r.y * z.y + r.z * z.z + r.w * z.w;
+        }
+      },
+      One{});
+  {
+    const double rpcg = reduce_partials_256(qp[0], nq, sh);
+    if (threadIdx.x == 0) cg_init_epi(ctl[m], glob, rpcg);
+    share();
+  }
+  // :91-169, ITERM bounds the loop (cg_update_epi sets done)
+  while (!s_done) {
+    {
+      const bool par = s_parity;
+      const double beta = s_beta;
+      const double *pold = par ? Ys.pb : Ys.pa;
+      double *pnew = par ? Ys.pa : Ys.pb;
+      sweep(
+          [&](const RowGeo &g, bool valid, double *v) {
+            v[0] = matvec_row_z(g, valid, Ys.z, Y.ccc, pold, pnew, Y.ccs, Y.ccw, Y.cce, Y.ccn,
+                                Ys.ap, beta, asym);
+          },
+          One{});
+      const double pap = reduce_partials_256(qp[0], nq, sh);
+      if (threadIdx.x == 0) cg_matvec_epi(ctl[m], pap);
+      share();
+    }
+    {
+      const double alpha = s_alpha;
+      const double *pnew = s_parity ? Ys.pa : Ys.pb;
+      sweep(
+          [&](const RowGeo &g, bool valid, double *v) {
+            update_row<double>(g, valid, Ps, pnew, Ys.r, Ys.ap, Y.ccc, alpha, v[0], v[1], Ys.z);
+          },
+          Two{});
+      const double rz = reduce_partials_256(qp[0], nq, sh);
+      const double rr = reduce_partials_256(qp[1], nq, sh);
+      if (threadIdx.x == 0) cg_update_epi(ctl[m], glob, S.sc[m], rz, rr, 0);
+      share();
+    }
+  }
+  for (int i = threadIdx.x; i < nsl; i += SMALL_NT)
+#pragma unroll
+    for (int k = 0; k < 6; ++k) gv[k][base + i] = smv[k * nsl + i];
 }
 
 // ---------------------------------------------------------------------------
@@ -1375,6 +1550,35 @@ void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, dou
   launch_chan_res64(l, S, Y, P, ctl, part);
   k_red_cg_init<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part);
   count_launches(2);
+}
+// Shared memory of k_cg_small for windows of up to `slots` slots (its six
+// vectors); false when that is more than a CTA can have.
+bool cg_small_fits(int slots) {
+  return size_t(slots) * 6 * sizeof(double) <= size_t(SMALL_SMEM_MAX) &&
+         slots / (TILES_PER_CTA * TILE) <= SMALL_MAX_UNITS;
+}
+void launch_cg_small(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
+                     Ctl *ctl, Glob *glob, double *part, int max_slots, int nmember) {
+  const size_t smem = size_t(max_slots) * 6 * sizeof(double);
+  static std::mutex mu;
+  static bool set[2] = {false, false};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!set[l.may_asym ? 1 : 0]) {
+      if (l.may_asym)
+        cudaFuncSetAttribute(k_cg_small<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             SMALL_SMEM_MAX);
+      else
+        cudaFuncSetAttribute(k_cg_small<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             SMALL_SMEM_MAX);
+      set[l.may_asym ? 1 : 0] = true;
+    }
+  }
+  if (l.may_asym)
+    k_cg_small<true><<<nmember, SMALL_NT, smem, l.stream>>>(S, Y, P, ctl, glob, part);
+  else
+    k_cg_small<false><<<nmember, SMALL_NT, smem, l.stream>>>(S, Y, P, ctl, glob, part);
+  count_launches(1);
 }
 void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {

@@ -431,6 +431,7 @@ OPT_CTAS_UPDATE = 5
 OPT_POLY_THRESHOLD = 6
 OPT_INNER_MARGIN = 7
 OPT_INNER_TOL = 8
+OPT_SMALL_SOLVE = 9
 
 
 TUNE_MEASURE = 1

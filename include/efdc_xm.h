@@ -557,6 +557,12 @@ int64_t efdc_xm_host_waits(void);
  *   EFDC_XM_OPT_INNER_TOL (default 60, 40..75): a MIXED inner solve reduces
  *     its residual by at least 10^(-value/10) in norm before the next FP64
  *     refinement pass, where the FP64 stop needs more than that.
+ *   EFDC_XM_OPT_SMALL_SOLVE (default 1): 1 runs the FP64 CG of contexts
+ *     whose members are all small (up to about 4,000 slots of 32x8 tiles,
+ *     e.g. basins of a few thousand cells) and have no sub-grid channels as
+ *     one launch with one CTA per member, its vectors in shared memory; 0
+ *     runs it as the kernels of every other context.  Both give the same
+ *     results bit for bit.
  * Results stay within the MIXED form's error bar whatever the schedule; the
  * FP64 form's results do not depend on it.
  * Returns EFDC_XM_BAD_ARGUMENT for an unknown option or value. */
@@ -568,7 +574,8 @@ enum {
   EFDC_XM_OPT_CTAS_UPDATE = 5,
   EFDC_XM_OPT_POLY_THRESHOLD = 6,
   EFDC_XM_OPT_INNER_MARGIN = 7,
-  EFDC_XM_OPT_INNER_TOL = 8
+  EFDC_XM_OPT_INNER_TOL = 8,
+  EFDC_XM_OPT_SMALL_SOLVE = 9
 };
 int32_t efdc_xm_set_option(efdc_xm_ctx *ctx, int32_t option, int32_t value);
 
