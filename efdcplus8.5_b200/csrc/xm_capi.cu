@@ -62,8 +62,14 @@ uint64_t morton2(uint32_t x, uint32_t y) {
 }
 
 constexpr int NSTAGE = 8;     // staging buffers (each holds one array of every member)
-constexpr int NCHUNK = 8;     // member chunks of a pipelined efdc_xm_step_batch
+constexpr int NCHUNK = 32;    // most member chunks of a pipelined efdc_xm_step_batch
 constexpr int NCOPY = 4;      // streams for host<->device copies
+// Contexts of at most this many members fold the member reductions into the
+// CG kernels by default.  In a larger batch the CTA that stores last often
+// completes many members at once and sums them one after another at the end
+// of the kernel (measured on 256 members: the inner iteration's kernels 40-60 %
+// slower), where one member-reduce kernel sums them all in parallel.
+constexpr int FOLD_MEMBERS = 4;
 constexpr int MAX_JOBS = 128;  // arrays moved by one upload/download call
 constexpr int GRAPH_ITERS = 4;  // CG iterations per graph launch
 constexpr int KERNELS_PER_ITER = 4;  // matvec, its reduce, update, its reduce
@@ -271,6 +277,9 @@ struct efdc_xm_ctx {
   int inner_margin_log10 = 0;   // MIXED inner target margin 10^-v
   int inner_tol_x10 = 60;       // MIXED inner relative tolerance 10^(-v/10) at least
   bool small_solve = true;      // FP64: members small enough solve in one CTA each
+  int fold_reduce = 1;          // member reductions folded into the CG kernels:
+                                // 0 never, 1 up to FOLD_MEMBERS members, 2 always
+  int nchunk = 8;               // member chunks of a pipelined efdc_xm_step_batch
   int small_slots = 0;          // the largest member window (its ghost tile and tiles)
   float poly_threshold = 10.f;  // MIXED: polynomial preconditioner above this Jacobi count
   xm::Launch L() const {
@@ -282,6 +291,7 @@ struct efdc_xm_ctx {
     l.ctas_mv = ctas_mv;
     l.ctas_up = ctas_up;
     l.inner_margin = std::pow(10.0, -double(inner_margin_log10));
+    l.fold = (fold_reduce == 2 || (fold_reduce == 1 && M <= FOLD_MEMBERS)) && !l.chan;
     return l;
   }
 };
@@ -2673,7 +2683,7 @@ void drain(efdc_xm_ctx *c) {
 // direction at the same time.
 constexpr int NPIPE = 1;
 
-// efdc_xm_step_batch of a CALPUV2C step in NCHUNK member chunks of about
+// efdc_xm_step_batch of a CALPUV2C step in c->nchunk member chunks of about
 // equal cell counts, so that the upload of one chunk, the step of an earlier
 // one and the download of a still earlier one overlap (the link carries both
 // directions at once).  Every array of the two transfers has its own staging
@@ -2733,7 +2743,7 @@ int step_batch_chunks(efdc_xm_ctx *c, const efdc_xm_params *prm, efdc_xm_fields 
     return rc;
   }
   // chunk k holds the members [mb[k], mb[k+1]), about equal cell counts
-  const int K = std::min(NCHUNK, M);
+  const int K = std::min(std::min(c->nchunk, NCHUNK), M);
   std::vector<int> mb(K + 1, M);
   mb[0] = 0;
   {
@@ -3961,6 +3971,17 @@ int32_t efdc_xm_set_option(efdc_xm_ctx *c, int32_t option, int32_t value) {
       if (value < 0 || value > 1) break;
       if ((value != 0) != c->small_solve) {
         c->small_solve = value != 0;
+        drop_graphs(c);
+      }
+      return EFDC_XM_OK;
+    case EFDC_XM_OPT_CHUNKS:
+      if (value < 1 || value > NCHUNK) break;
+      c->nchunk = value;
+      return EFDC_XM_OK;
+    case EFDC_XM_OPT_FOLD_REDUCE:
+      if (value < 0 || value > 2) break;
+      if (value != c->fold_reduce) {
+        c->fold_reduce = value;
         drop_graphs(c);
       }
       return EFDC_XM_OK;

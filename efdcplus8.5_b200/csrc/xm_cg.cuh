@@ -8,6 +8,7 @@
 // land slots (P(LC), the ghost value), mask with the slot kind.
 #pragma once
 
+#include "../../include/efdc_xm.h"
 #include "xm_common.cuh"
 #include "xm_tma.cuh"
 
@@ -23,14 +24,19 @@ __device__ __forceinline__ double rcpT(double x) { return 1. / x; }
 // of a row takes part in the shuffles.  A quad whose member is finished (or
 // not in this sweep) is skipped by the whole CTA.
 //
-// Reductions in two kernels: the CG kernel leaves one partial per warp in
-// shared memory (warp shuffles only, no CTA barrier per quad) and, every
-// QCAP quads and at its end, adds the warp partials of each quad in fixed
-// warp order into part[quad] (plain stores).  A member-reduce kernel then
-// reduces each member's per-quad partials in fixed quad order (one CTA per
-// member) and finishes the member (its Ctl).  No fences, atomics or
-// "last CTA" in the CG kernels, and sums that depend neither on the grid size
-// nor on which other members share the context.
+// Reductions: the CG kernel leaves one partial per warp in shared memory
+// (warp shuffles only, no CTA barrier per quad) and, every QCAP quads and at
+// its end, adds the warp partials of each quad in fixed warp order into
+// part[quad] (plain stores).  Each member's per-quad partials are then summed
+// in fixed quad order and the member finished (its Ctl), either
+//  * folded into the CG kernel (Fold): each stored quad counts towards its
+//    member's arrivals (Ctl::counter, after a fence), and the CTA whose store
+//    completes a member's quads sums that member and runs its epilogue, or
+//  * by a member-reduce kernel after it (one CTA per member), where sub-grid
+//    channel kernels add their terms to the partials in between.
+// Both run the same sum (reduce_partials) and the same epilogue, so the two
+// forms give the same iterates bit for bit, and neither depends on the grid
+// size or on which other members share the context.
 // A member's operator is handled as unsymmetric (the four-array form) when
 // its flag's bit 1 is set; MA = false compiles the symmetric form only, for
 // batches in which no member can be unsymmetric (no radiation boundary).
@@ -46,7 +52,47 @@ template <int NS>
 struct QuadLog {
   double w[NS][QCAP][NWARP];  // per-warp partials of NS sums
   int qd[QCAP];               // quad of each entry
+  int m[QCAP];                // its member
 };
+
+// atomicAdd with acquire-release semantics at GPU scope: the partial sums
+// this thread stored are visible to whoever observes the increment, and
+// those the earlier arrivals stored are visible to this thread.
+__device__ __forceinline__ unsigned int atomic_add_acq_rel(unsigned int *p, unsigned int v) {
+  unsigned int old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
+               : "=r"(old)
+               : "l"(p), "r"(v)
+               : "memory");
+  return old;
+}
+
+// The member reduction folded into a CG kernel: ctl holds the members'
+// arrival counters (nullptr: not folded, a member-reduce kernel follows) and
+// epi(m, sums) finishes member m (all threads call it; the sums are valid in
+// thread 0).
+template <class Epi>
+struct Fold {
+  Ctl *ctl;
+  Epi epi;
+};
+template <class Epi>
+__device__ __forceinline__ Fold<Epi> fold_with(Ctl *ctl, Epi epi) {
+  return Fold<Epi>{ctl, epi};
+}
+struct NoEpi {
+  __device__ void operator()(int, const double *) const {}
+};
+// What the epilogues of the update and residual kernels read besides the Ctl
+// (kernel arguments of the folded form and of the member-reduce kernels).
+struct RedArgs {
+  Glob *glob;
+  double rsqm_fac, rel_tol, margin;  // MIXED refinement residual (k_mx_resid)
+  int no_stop;                       // iterate past the stop tests (kernel timing)
+  int unscaled;                      // MIXED residual of the unscaled system
+  int fold;                          // the member reduction folded into the kernel
+};
+__device__ __forceinline__ Fold<NoEpi> no_fold() { return Fold<NoEpi>{nullptr, NoEpi{}}; }
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -54,9 +100,13 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-template <int NS>
+template <int NS, class Epi>
 __device__ __forceinline__ void quad_store(QuadLog<NS> &L, int n, const DevStatic &S,
-                                           double *part) {
+                                           double *part, const Fold<Epi> &f) {
+  __shared__ int nfin;
+  __shared__ int fin[QCAP];
+  __shared__ double sh[32];
+  if (threadIdx.x == 0) nfin = 0;
   __syncthreads();  // the warp partials and the entries are in shared memory
   const int t = threadIdx.x;
   if (t < n) {
@@ -66,6 +116,25 @@ __device__ __forceinline__ void quad_store(QuadLog<NS> &L, int n, const DevStati
 #pragma unroll
       for (int w = 0; w < NWARP; ++w) a += L.w[s][t][w];
       part[size_t(s) * S.nquad + L.qd[t]] = a;
+    }
+    if (f.ctl) {  // this quad arrives (release: after its partials)
+      const int m = L.m[t];
+      const unsigned int nq = unsigned(S.qstart[m + 1] - S.qstart[m]);
+      if (atomic_add_acq_rel(&f.ctl[m].counter, 1u) == nq - 1u) fin[atomicAdd(&nfin, 1)] = m;
+    }
+  }
+  __syncthreads();  // orders the acquiring thread's view before the CTA's reads
+  if (f.ctl) {
+    const int k = nfin;
+    for (int i = 0; i < k; ++i) {  // the members this CTA completed (any order)
+      const int m = fin[i];
+      const int q0 = S.qstart[m], nq = S.qstart[m + 1] - q0;
+      double r[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s)
+        r[s] = reduce_partials<>(part + size_t(s) * S.nquad + q0, nq, sh);
+      f.epi(m, r);
+      if (t == 0) f.ctl[m].counter = 0u;  // for the next kernel
     }
   }
   __syncthreads();  // the log is reused after this
@@ -80,9 +149,9 @@ __device__ __forceinline__ void quad_store(QuadLog<NS> &L, int n, const DevStati
 // is fetched one quad ahead, so that those small dependent loads overlap the
 // current quad's memory traffic instead of preceding the next one's.  In an
 // ensemble nearly every quad of a CTA belongs to another member.
-template <int NS, class Setup, class Body>
+template <int NS, class Setup, class Body, class Epi = NoEpi>
 __device__ __forceinline__ void quad_sweep(const DevStatic &S, double *part, Setup setup,
-                                           Body body) {
+                                           Body body, Fold<Epi> f = no_fold()) {
   __shared__ QuadLog<NS> L;
   const int sub = threadIdx.x / TPT, q = threadIdx.x % TPT;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -115,9 +184,12 @@ __device__ __forceinline__ void quad_sweep(const DevStatic &S, double *part, Set
         const double x = warp_sum(v[s]);
         if (lane == 0) L.w[s][n][warp] = x;
       }
-      if (threadIdx.x == 0) L.qd[n] = qd;
+      if (threadIdx.x == 0) {
+        L.qd[n] = qd;
+        L.m[n] = cur.x;
+      }
       if (++n == QCAP) {
-        quad_store<NS>(L, n, S, part);
+        quad_store<NS>(L, n, S, part, f);
         n = 0;
       }
     }
@@ -128,7 +200,7 @@ __device__ __forceinline__ void quad_sweep(const DevStatic &S, double *part, Set
     nb = nbn;
     nxt = nn;
   }
-  if (n) quad_store<NS>(L, n, S, part);
+  if (n) quad_store<NS>(L, n, S, part, f);
 }
 
 // quad_sweep with the descriptors in batches: the CTA first loads, for its
@@ -139,9 +211,9 @@ __device__ __forceinline__ void quad_sweep(const DevStatic &S, double *part, Set
 // same rows, the same warp sums, the same per-quad partials.
 constexpr int QB = 32;  // quads per descriptor batch (QB * TILES_PER_CTA <= NT)
 
-template <int NS, class Setup, class Body>
+template <int NS, class Setup, class Body, class Epi>
 __device__ __forceinline__ void quad_sweep_batched(const DevStatic &S, double *part, Setup setup,
-                                                   Body body) {
+                                                   Body body, const Fold<Epi> &f) {
   using A = decltype(setup(0));
   __shared__ QuadLog<NS> L;
   __shared__ A da[QB];
@@ -183,14 +255,17 @@ __device__ __forceinline__ void quad_sweep_batched(const DevStatic &S, double *p
         const double x = warp_sum(v[s]);
         if (lane == 0) L.w[s][n][warp] = x;
       }
-      if (threadIdx.x == 0) L.qd[n] = b0 + k * G;
+      if (threadIdx.x == 0) {
+        L.qd[n] = b0 + k * G;
+        L.m[n] = cur.x;
+      }
       if (++n == QCAP) {
-        quad_store<NS>(L, n, S, part);
+        quad_store<NS>(L, n, S, part, f);
         n = 0;
       }
     }
   }
-  if (n) quad_store<NS>(L, n, S, part);
+  if (n) quad_store<NS>(L, n, S, part, f);
 }
 
 // ---------------------------------------------------------------------------
@@ -246,9 +321,10 @@ constexpr int MBAR_TRIES = 1 << 16;  // bounded mbarrier waits (each try may sus
 // stage st and those values e.  On a wait that runs out, *err is set and the
 // CTA stops computing (the step then fails with a timeout status); the copies
 // it issued are waited for, again bounded, before it exits.
-template <int NS, int NB, int NSTG, class Setup, class Pre, class Body>
+template <int NS, int NB, int NSTG, class Setup, class Pre, class Body, class Epi>
 __device__ __forceinline__ void quad_sweep_staged(const DevStatic &S, double *part, int *err,
-                                                  Setup setup, Pre pre, Body body) {
+                                                  Setup setup, Pre pre, Body body,
+                                                  const Fold<Epi> &f) {
   using A = decltype(setup(0));
   using St = Stage<NB>;
   extern __shared__ __align__(128) unsigned char dyn_smem[];
@@ -328,16 +404,19 @@ __device__ __forceinline__ void quad_sweep_staged(const DevStatic &S, double *pa
         const double x = warp_sum(v[i]);
         if (lane == 0) L.w[i][n][warp] = x;
       }
-      if (threadIdx.x == 0) L.qd[n] = b0 + k * G;
+      if (threadIdx.x == 0) {
+        L.qd[n] = b0 + k * G;
+        L.m[n] = cur.x;
+      }
       __syncthreads();  // every thread is done with stage s: it may be refilled
       if (threadIdx.x == 0 && !dead && j + NSTG < nl) issue(j + NSTG);
       if (++n == QCAP) {
-        quad_store<NS>(L, n, S, part);
+        quad_store<NS>(L, n, S, part, f);
         n = 0;
       }
     }
   }
-  if (n) quad_store<NS>(L, n, S, part);
+  if (n) quad_store<NS>(L, n, S, part, f);
   // every phase issued has been waited for, unless a wait ran out: then the
   // copies still in flight are waited for (bounded) before the CTA's shared
   // memory goes
@@ -355,13 +434,83 @@ __device__ __forceinline__ void quad_sweep_staged(const DevStatic &S, double *pa
 
 // The quad sweep of a kernel variant: 0 prefetches one quad ahead in
 // registers, 1 and 3 load the descriptors in batches (quad_sweep_batched).
-template <int NS, int VAR, class Setup, class Body>
+template <int NS, int VAR, class Setup, class Body, class Epi>
 __device__ __forceinline__ void quad_sweep_v(const DevStatic &S, double *part, Setup setup,
-                                             Body body) {
+                                             Body body, const Fold<Epi> &f) {
   if constexpr (VAR == 1 || VAR == 3)
-    quad_sweep_batched<NS>(S, part, setup, body);
+    quad_sweep_batched<NS>(S, part, setup, body, f);
   else
-    quad_sweep<NS>(S, part, setup, body);
+    quad_sweep<NS>(S, part, setup, body, f);
+}
+
+// The members' epilogues of the reductions (thread 0 of the member), run by
+// the member-reduce kernels and by the folded form alike.
+// FP64 CONGRAD (congrad.f90): :88 RETURN on RPCG = 0; :124 ALPHA (also the
+// MIXED inner ALPHA); :143-169 BETA, RSQ and the stop test.  With no_stop the
+// iteration continues past RSQM and ITERM (kernel timing).
+__device__ __forceinline__ void cg_init_epi(Ctl &k, Glob *glob, double rpcg) {
+  k.rpcg = rpcg;
+  k.beta = 0.0;
+  k.parity = 0;
+  k.iter = 0;
+  k.rsq = 0.0;
+  k.status = 0;
+  if (rpcg == 0.0 || !isfinite(rpcg)) {  // :88 RETURN
+    if (!isfinite(rpcg)) k.status = EFDC_XM_NONFINITE;
+    k.done = 1;
+    atomicAdd(&glob->ndone, 1);
+  }
+}
+__device__ __forceinline__ void cg_matvec_epi(Ctl &k, double pap) {
+  k.papcg = pap;
+  k.alpha = k.rpcg / pap;  // :124
+}
+__device__ __forceinline__ void cg_update_epi(Ctl &k, Glob *glob, const StepScalars &c,
+                                              double rpcgn, double rsq, int no_stop) {
+  k.beta = rpcgn / k.rpcg;
+  k.rpcg = rpcgn;
+  k.rsq = rsq;
+  const int it = k.iter + 1;
+  k.iter = it;
+  int fin = 0;
+  if (!isfinite(rsq) || !isfinite(k.alpha)) {
+    k.status = EFDC_XM_NONFINITE;
+    fin = 1;
+  } else if (!no_stop && rsq <= c.rsqm) {
+    fin = 1;
+  } else if (!no_stop && it >= c.iterm) {
+    k.status = EFDC_XM_CG_MAXITER;
+    fin = 1;
+  } else {
+    k.parity ^= 1;
+  }
+  if (fin) {
+    k.done = 1;
+    atomicAdd(&glob->ndone, 1);
+  }
+}
+
+// MIXED inner iteration: BETA = r.z / r.z_old and the inner stop test on r.r
+// (its target, ITERM, or cap_fac*ITERM + 50 inner iterations over all passes).
+__device__ __forceinline__ void mx_update_epi(Ctl &k, Glob *glob, int iterm, double rz, double rr,
+                                              double cap_fac, int no_stop) {
+  k.beta = rz / k.rpcg;
+  k.rpcg = rz;
+  k.rsq = rr;
+  const int it = k.inner_iter + 1;
+  k.inner_iter = it;
+  k.iter += 1;
+  if (!isfinite(rr) || !isfinite(rz) || !isfinite(k.alpha)) {
+    k.status = EFDC_XM_NONFINITE;
+    k.done = 1;
+    atomicAdd(&glob->ndone, 1);
+  } else if (!no_stop && (rr <= k.rsq_target || it >= iterm ||
+                          k.iter >= int(cap_fac * iterm) + 50)) {
+    k.idone = 1;
+    atomicAdd(&glob->nidone, 1);
+  } else {
+    k.parity ^= 1;
+  }
 }
 
 // The member-reduce kernels: member m (one CTA per member, grid-stride) sums
@@ -376,7 +525,7 @@ __device__ __forceinline__ void member_reduce(const DevStatic &S, const double *
     const int q0 = S.qstart[m], nq = S.qstart[m + 1] - q0;
     double r[NS];
 #pragma unroll
-    for (int s = 0; s < NS; ++s) r[s] = reduce_partials(part + size_t(s) * S.nquad + q0, nq, sh);
+    for (int s = 0; s < NS; ++s) r[s] = reduce_partials<>(part + size_t(s) * S.nquad + q0, nq, sh);
     epi(m, r);
   }
 }

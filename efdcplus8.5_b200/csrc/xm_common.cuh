@@ -74,18 +74,21 @@ __device__ __forceinline__ bool arrive_last(unsigned int *counter) {
 }
 
 // Fixed-order sum of nblk partials by one CTA: thread i adds partials
-// i, i+NT, ... in order, then the fixed block tree.  Deterministic.
+// i, i+NT, ... in order, then the fixed block tree.  Deterministic; W, the
+// loads a thread issues before adding them (in order), changes only speed
+// and registers.
+template <int W = 8>
 __device__ __forceinline__ double reduce_partials(const double *part, int nblk, double *sh) {
   double s = 0.0;
-  for (int base = 0; base < nblk; base += 8 * NT) {
-    double v[8];  // a pass's loads are all issued before the (ordered) adds
+  for (int base = 0; base < nblk; base += W * NT) {
+    double v[W];  // a pass's loads are all issued before the (ordered) adds
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < W; ++j) {
       const int i = base + j * NT + int(threadIdx.x);
       v[j] = (i < nblk) ? __ldcg(&part[i]) : 0.0;
     }
 #pragma unroll
-    for (int j = 0; j < 8; ++j) s += v[j];
+    for (int j = 0; j < W; ++j) s += v[j];
   }
   return block_sum(s, sh);
 }

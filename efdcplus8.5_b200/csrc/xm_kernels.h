@@ -31,6 +31,9 @@ struct Launch {
   // to reach its stop, times this margin (< 1 over-solves the FP32 inner
   // solve so that fewer refinement passes are needed)
   double inner_margin = 1.0;
+  // the member reductions folded into the CG kernels (no member-reduce
+  // kernels); off where sub-grid channel kernels add to the partials
+  bool fold = false;
 };
 
 // One array to move between host order and tile order (see k_scatter).

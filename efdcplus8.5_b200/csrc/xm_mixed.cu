@@ -29,8 +29,8 @@ namespace xm {
 constexpr int mx_ctas(int var) { return var == 1 ? 5 : var == 3 ? 4 : 6; }
 
 template <bool MA, int VAR>
-__global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
-                                                    double *part) {
+__global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_matvec(DevStatic S, DevSystem Y, Ctl *ctl,
+                                                    double *part, int fold) {
   struct A {
     bool skip, asym;
     float beta;
@@ -55,16 +55,17 @@ __global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_matvec(DevStatic S, Dev
         else
           v[0] = matvec_row_scaled(g, valid, a.z, a.pold, a.pnew, Y.as32, Y.aw32, Y.ae32,
                                    Y.an32, Y.ap32, a.beta, a.asym);
-      });
+      },
+      fold_with(fold ? ctl : nullptr, [&](int m, const double *sum) {
+        if (threadIdx.x == 0) cg_matvec_epi(ctl[m], sum[0]);
+      }));
 }
 // ALPHA = RPCG / p.Ap
 __global__ void __launch_bounds__(NT) k_red_mx_matvec(DevStatic S, Ctl *ctl, const double *part) {
   member_reduce<1>(
       S, part, [&](int m) { return (ctl[m].done | ctl[m].idone) != 0; },
       [&](int m, const double *sum) {
-        if (threadIdx.x != 0) return;
-        ctl[m].papcg = sum[0];
-        ctl[m].alpha = ctl[m].rpcg / sum[0];
+        if (threadIdx.x == 0) cg_matvec_epi(ctl[m], sum[0]);
       });
 }
 
@@ -72,7 +73,7 @@ __global__ void __launch_bounds__(NT) k_red_mx_matvec(DevStatic S, Ctl *ctl, con
 // polynomial), r.z and r.r (FP64 sums): the members that use it.
 template <int VAR>
 __global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_update_poly(DevStatic S, DevSystem Y,
-                                                         const Ctl *ctl, double *part) {
+                                                         Ctl *ctl, double *part, RedArgs ra) {
   struct A {
     bool skip;
     float alpha;
@@ -96,12 +97,16 @@ __global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_update_poly(DevStatic S
         else
           update_row_poly(g, valid, Y.x32, a.pnew, a.r, a.rnew, Y.ap32, Y.as32, Y.aw32, Y.z32,
                           a.alpha, true, v[0], v[1]);
-      });
+      },
+      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+        if (threadIdx.x == 0)
+          mx_update_epi(ctl[m], ra.glob, S.sc[m].iterm, sum[0], sum[1], 2.0, ra.no_stop);
+      }));
 }
 // The same for the Jacobi members (z = r): x, r and r.r only.
 template <int VAR>
-__global__ void __launch_bounds__(NT) k_mx_update_jac(DevStatic S, DevSystem Y, const Ctl *ctl,
-                                                     double *part) {
+__global__ void __launch_bounds__(NT, 8) k_mx_update_jac(DevStatic S, DevSystem Y, Ctl *ctl,
+                                                     double *part, RedArgs ra) {
   struct A {
     bool skip;
     float alpha;
@@ -123,7 +128,11 @@ __global__ void __launch_bounds__(NT) k_mx_update_jac(DevStatic S, DevSystem Y, 
         update_row_jac(g, valid, Y.x32, a.pnew, a.r, a.rnew, Y.ap32, a.alpha, rr);
         v[0] = rr;
         v[1] = rr;
-      });
+      },
+      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+        if (threadIdx.x == 0)
+          mx_update_epi(ctl[m], ra.glob, S.sc[m].iterm, sum[0], sum[1], 2.0, ra.no_stop);
+      }));
 }
 // BETA = r.z / r.z_old and the inner stop test on r.r.  With no_stop the
 // inner solve runs past its target (kernel timing only).
@@ -133,35 +142,16 @@ __global__ void __launch_bounds__(NT) k_red_mx_update(DevStatic S, Ctl *ctl, Glo
   member_reduce<2>(
       S, part, [&](int m) { return (ctl[m].done | ctl[m].idone) != 0; },
       [&](int m, const double *sum) {
-        if (threadIdx.x != 0) return;
-        Ctl &k = ctl[m];
-        const double rz = sum[0], rr = sum[1];
-        const int iterm = S.sc[m].iterm;
-        k.beta = rz / k.rpcg;
-        k.rpcg = rz;
-        k.rsq = rr;
-        const int it = k.inner_iter + 1;
-        k.inner_iter = it;
-        k.iter += 1;
-        if (!isfinite(rr) || !isfinite(rz) || !isfinite(k.alpha)) {
-          k.status = EFDC_XM_NONFINITE;
-          k.done = 1;
-          atomicAdd(&glob->ndone, 1);
-        } else if (!no_stop && (rr <= k.rsq_target || it >= iterm ||
-                                k.iter >= int(total_cap_fac * iterm) + 50)) {
-          k.idone = 1;
-          atomicAdd(&glob->nidone, 1);
-        } else {
-          k.parity ^= 1;
-        }
+        if (threadIdx.x == 0)
+          mx_update_epi(ctl[m], glob, S.sc[m].iterm, sum[0], sum[1], total_cap_fac, no_stop);
       });
 }
 
 // First inner iteration of the polynomial members: z0 = (2I - Ahat) r0,
 // p_old = 0, RPCG = r0.z0 (Jacobi members start from k_mx_resid's p0 = r0).
 template <bool EAGER>
-__global__ void __launch_bounds__(NT) k_mx_zinit(DevStatic S, DevSystem Y, const Ctl *ctl,
-                                                double *part) {
+__global__ void __launch_bounds__(NT) k_mx_zinit(DevStatic S, DevSystem Y, Ctl *ctl,
+                                                double *part, int fold) {
   struct A {
     bool skip, asym;
   };
@@ -173,7 +163,10 @@ __global__ void __launch_bounds__(NT) k_mx_zinit(DevStatic S, DevSystem Y, const
           v[0] = zinit_row_eager(g, valid, Y.r32, Y.as32, Y.aw32, Y.z32, Y.pa32, true);
         else
           v[0] = zinit_row(g, valid, Y.r32, Y.as32, Y.aw32, Y.z32, Y.pa32, true);
-      });
+      },
+      fold_with(fold ? ctl : nullptr, [&](int m, const double *sum) {
+        if (threadIdx.x == 0) ctl[m].rpcg = sum[0];
+      }));
 }
 __global__ void __launch_bounds__(NT) k_red_mx_zinit(DevStatic S, DevSystem Y, Ctl *ctl,
                                                      const double *part) {
@@ -206,8 +199,8 @@ using PolyStage = Stage<6>;  // r, Ap, AS, AW, x, p
 using JacStage = Stage<4>;   // x, p, r, Ap
 
 template <bool MA>
-__global__ void __launch_bounds__(NT, 3) k_mx_matvec_st(DevStatic S, DevSystem Y, const Ctl *ctl,
-                                                       double *part) {
+__global__ void __launch_bounds__(NT, 3) k_mx_matvec_st(DevStatic S, DevSystem Y, Ctl *ctl,
+                                                       double *part, int fold) {
   struct A {
     bool skip, asym;
     float beta;
@@ -282,11 +275,14 @@ __global__ void __launch_bounds__(NT, 3) k_mx_matvec_st(DevStatic S, DevSystem Y
         st4(Y.ap32 + g.d0, ap);
         v[0] = double(ap.x) * double(p.x) + double(ap.y) * double(p.y) +
                double(ap.z) * double(p.z) + double(ap.w) * double(p.w);
-      });
+      },
+      fold_with(fold ? ctl : nullptr, [&](int m, const double *sum) {
+        if (threadIdx.x == 0) cg_matvec_epi(ctl[m], sum[0]);
+      }));
 }
 
 __global__ void __launch_bounds__(NT, 3) k_mx_update_poly_st(DevStatic S, DevSystem Y,
-                                                            const Ctl *ctl, double *part) {
+                                                            Ctl *ctl, double *part, RedArgs ra) {
   struct A {
     bool skip;
     float alpha;
@@ -362,11 +358,15 @@ __global__ void __launch_bounds__(NT, 3) k_mx_update_poly_st(DevStatic S, DevSys
                double(rn0.z) * double(zv.z) + double(rn0.w) * double(zv.w);
         v[1] = double(rn0.x) * double(rn0.x) + double(rn0.y) * double(rn0.y) +
                double(rn0.z) * double(rn0.z) + double(rn0.w) * double(rn0.w);
-      });
+      },
+      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+        if (threadIdx.x == 0)
+          mx_update_epi(ctl[m], ra.glob, S.sc[m].iterm, sum[0], sum[1], 2.0, ra.no_stop);
+      }));
 }
 
 __global__ void __launch_bounds__(NT, 4) k_mx_update_jac_st(DevStatic S, DevSystem Y,
-                                                           const Ctl *ctl, double *part) {
+                                                           Ctl *ctl, double *part, RedArgs ra) {
   struct A {
     bool skip;
     float alpha;
@@ -403,7 +403,11 @@ __global__ void __launch_bounds__(NT, 4) k_mx_update_jac_st(DevStatic S, DevSyst
                           double(rv.z) * double(rv.z) + double(rv.w) * double(rv.w);
         v[0] = rr;
         v[1] = rr;
-      });
+      },
+      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+        if (threadIdx.x == 0)
+          mx_update_epi(ctl[m], ra.glob, S.sc[m].iterm, sum[0], sum[1], 2.0, ra.no_stop);
+      }));
 }
 
 // Dynamic shared memory of a staged kernel (its stages), allowed once.
@@ -468,70 +472,78 @@ static int grid_of(const Launch &l, const DevStatic &S, K kernel, int cap) {
 
 void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {
+  const int f = l.fold;
   if (l.variant == 2) {
     if (l.may_asym) {
       const size_t sm = staged_smem(k_mx_matvec_st<true>, sizeof(MvStage), MV_STAGES);
       k_mx_matvec_st<true><<<staged_grid(l, S, k_mx_matvec_st<true>, sm, l.ctas_mv), NT, sm,
-                             l.stream>>>(S, Y, ctl, part);
+                             l.stream>>>(S, Y, ctl, part, f);
     } else {
       const size_t sm = staged_smem(k_mx_matvec_st<false>, sizeof(MvStage), MV_STAGES);
       k_mx_matvec_st<false><<<staged_grid(l, S, k_mx_matvec_st<false>, sm, l.ctas_mv), NT, sm,
-                              l.stream>>>(S, Y, ctl, part);
+                              l.stream>>>(S, Y, ctl, part, f);
     }
   } else if (l.variant == 1) {
     if (l.may_asym)
       k_mx_matvec<true, 1><<<grid_of(l, S, k_mx_matvec<true, 1>, l.ctas_mv), NT, 0, l.stream>>>(
-          S, Y, ctl, part);
+          S, Y, ctl, part, f);
     else
       k_mx_matvec<false, 1><<<grid_of(l, S, k_mx_matvec<false, 1>, l.ctas_mv), NT, 0,
-                              l.stream>>>(S, Y, ctl, part);
+                              l.stream>>>(S, Y, ctl, part, f);
   } else if (l.variant == 3) {
     if (l.may_asym)
       k_mx_matvec<true, 3><<<grid_of(l, S, k_mx_matvec<true, 3>, l.ctas_mv), NT, 0, l.stream>>>(
-          S, Y, ctl, part);
+          S, Y, ctl, part, f);
     else
       k_mx_matvec<false, 3><<<grid_of(l, S, k_mx_matvec<false, 3>, l.ctas_mv), NT, 0,
-                              l.stream>>>(S, Y, ctl, part);
+                              l.stream>>>(S, Y, ctl, part, f);
   } else if (l.may_asym) {
-    k_mx_matvec<true, 0><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
+    k_mx_matvec<true, 0><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part, f);
   } else {
-    k_mx_matvec<false, 0><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
+    k_mx_matvec<false, 0><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part, f);
   }
+  count_launches(1);
+  if (f) return;
   launch_chan_mvmx(l, S, Y, ctl, part);
   k_red_mx_matvec<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part);
-  count_launches(2);
+  count_launches(1);
 }
 void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       Glob *glob, double *part, int no_stop) {
+  RedArgs ra{};
+  ra.glob = glob;
+  ra.no_stop = no_stop;
+  ra.fold = l.fold;
   if (l.mx_jac && l.variant == 2) {
     const size_t sm = staged_smem(k_mx_update_jac_st, sizeof(JacStage), JAC_STAGES);
     k_mx_update_jac_st<<<staged_grid(l, S, k_mx_update_jac_st, sm, l.ctas_up), NT, sm,
-                         l.stream>>>(S, Y, ctl, part);
+                         l.stream>>>(S, Y, ctl, part, ra);
     count_launches(1);
   } else if (l.mx_jac) {
     if (l.variant == 1 || l.variant == 3)  // the Jacobi row already loads first
       k_mx_update_jac<1><<<grid_of(l, S, k_mx_update_jac<1>, l.ctas_up), NT, 0, l.stream>>>(
-          S, Y, ctl, part);
+          S, Y, ctl, part, ra);
     else
-      k_mx_update_jac<0><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part);
+      k_mx_update_jac<0><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part, ra);
     count_launches(1);
   }
   if (l.mx_poly && l.variant == 2) {
     const size_t sm = staged_smem(k_mx_update_poly_st, sizeof(PolyStage), POLY_STAGES);
     k_mx_update_poly_st<<<staged_grid(l, S, k_mx_update_poly_st, sm, l.ctas_up), NT, sm,
-                          l.stream>>>(S, Y, ctl, part);
+                          l.stream>>>(S, Y, ctl, part, ra);
     count_launches(1);
   } else if (l.mx_poly) {
     if (l.variant == 1)
       k_mx_update_poly<1><<<grid_of(l, S, k_mx_update_poly<1>, l.ctas_up), NT, 0, l.stream>>>(
-          S, Y, ctl, part);
+          S, Y, ctl, part, ra);
     else if (l.variant == 3)
       k_mx_update_poly<3><<<grid_of(l, S, k_mx_update_poly<3>, l.ctas_up), NT, 0, l.stream>>>(
-          S, Y, ctl, part);
+          S, Y, ctl, part, ra);
     else
-      k_mx_update_poly<0><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part);
+      k_mx_update_poly<0><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part, ra);
     count_launches(1);
   }
+  if (l.fold) return;
   k_red_mx_update<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, 2.0, no_stop);
   count_launches(1);
 }
@@ -539,11 +551,14 @@ void launch_mx_zinit(const Launch &l, const DevStatic &S, const DevSystem &Y, Ct
                      double *part) {
   if (!l.mx_poly) return;
   if (l.variant == 3)
-    k_mx_zinit<true><<<grid_of(l, S, k_mx_zinit<true>, 0), NT, 0, l.stream>>>(S, Y, ctl, part);
+    k_mx_zinit<true><<<grid_of(l, S, k_mx_zinit<true>, 0), NT, 0, l.stream>>>(S, Y, ctl, part,
+                                                                             l.fold);
   else
-    k_mx_zinit<false><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part);
+    k_mx_zinit<false><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part, l.fold);
+  count_launches(1);
+  if (l.fold) return;
   k_red_mx_zinit<<<reduce_grid(S), NT, 0, l.stream>>>(S, Y, ctl, part);
-  count_launches(2);
+  count_launches(1);
 }
 void launch_mx_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl, Glob *glob,
                     double *part) {

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(NT) k_na_init(NaArgs a) {
   acc = block_sum(acc, sh);
   if (threadIdx.x == 0) a.part[blockIdx.x] = acc;
   if (arrive_last(&a.ctl->counter)) {
-    const double rpcg = reduce_partials(a.part, gridDim.x, sh);
+    const double rpcg = reduce_partials<>(a.part, gridDim.x, sh);
     if (threadIdx.x == 0) {
       a.ctl->rpcg = rpcg;
       a.ctl->iter = 0;
@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(NT) k_na_matvec(NaArgs a) {
   acc = block_sum(acc, sh);
   if (threadIdx.x == 0) a.part[blockIdx.x] = acc;
   if (arrive_last(&a.ctl->counter)) {
-    const double papcg = reduce_partials(a.part, gridDim.x, sh);
+    const double papcg = reduce_partials<>(a.part, gridDim.x, sh);
     if (threadIdx.x == 0) {
       a.ctl->alpha = a.ctl->rpcg / papcg;
       a.ctl->counter = 0;
@@ -140,8 +140,8 @@ __global__ void __launch_bounds__(NT) k_na_update(NaArgs a, double rsqm, int ite
   a2 = block_sum(a2, sh);
   if (threadIdx.x == 0) a.part[gridDim.x + blockIdx.x] = a2;
   if (arrive_last(&a.ctl->counter)) {
-    const double rpcgn = reduce_partials(a.part, gridDim.x, sh);
-    const double rsq = reduce_partials(a.part + gridDim.x, gridDim.x, sh);
+    const double rpcgn = reduce_partials<>(a.part, gridDim.x, sh);
+    const double rsq = reduce_partials<>(a.part + gridDim.x, gridDim.x, sh);
     if (threadIdx.x == 0) {
       a.ctl->beta = rpcgn / a.ctl->rpcg;
       a.ctl->rpcg = rpcgn;

@@ -601,55 +601,10 @@ __global__ void k_outer_reset(Glob *glob) { glob->nidone = 0; }
 // p double-buffered (pa/pb, selected by ctl[m].parity), Ap.  z = CCCI*r with
 // CCCI = 1./CCC is recomputed where needed instead of stored.
 
-// The members' epilogues of the three reductions (thread 0 of the member):
-// :88 RETURN on RPCG = 0; :124 ALPHA; :143-169 BETA, RSQ and the stop test.
-// With no_stop the iteration continues past RSQM and ITERM (kernel timing).
-__device__ __forceinline__ void cg_init_epi(Ctl &k, Glob *glob, double rpcg) {
-  k.rpcg = rpcg;
-  k.beta = 0.0;
-  k.parity = 0;
-  k.iter = 0;
-  k.rsq = 0.0;
-  k.status = 0;
-  if (rpcg == 0.0 || !isfinite(rpcg)) {  // :88 RETURN
-    if (!isfinite(rpcg)) k.status = EFDC_XM_NONFINITE;
-    k.done = 1;
-    atomicAdd(&glob->ndone, 1);
-  }
-}
-__device__ __forceinline__ void cg_matvec_epi(Ctl &k, double pap) {
-  k.papcg = pap;
-  k.alpha = k.rpcg / pap;  // :124
-}
-__device__ __forceinline__ void cg_update_epi(Ctl &k, Glob *glob, const StepScalars &c,
-                                              double rpcgn, double rsq, int no_stop) {
-  k.beta = rpcgn / k.rpcg;
-  k.rpcg = rpcgn;
-  k.rsq = rsq;
-  const int it = k.iter + 1;
-  k.iter = it;
-  int fin = 0;
-  if (!isfinite(rsq) || !isfinite(k.alpha)) {
-    k.status = EFDC_XM_NONFINITE;
-    fin = 1;
-  } else if (!no_stop && rsq <= c.rsqm) {
-    fin = 1;
-  } else if (!no_stop && it >= c.iterm) {
-    k.status = EFDC_XM_CG_MAXITER;
-    fin = 1;
-  } else {
-    k.parity ^= 1;
-  }
-  if (fin) {
-    k.done = 1;
-    atomicAdd(&glob->ndone, 1);
-  }
-}
-
 // :54-88 initial residual, z0 = CCCI*r, RPCG.
 template <bool MA>
 __global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double *P, Ctl *ctl,
-                                               double *part) {
+                                               double *part, RedArgs ra) {
   struct A {
     bool skip, asym;
   };
@@ -666,7 +621,10 @@ __global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double
           st4(Y.z + g.d0, z);
           v[0] = r.x * z.x + r.y * z.y + r.z * z.z + r.w * z.w;
         }
-      });
+      },
+      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+        if (threadIdx.x == 0) cg_init_epi(ctl[m], ra.glob, sum[0]);
+      }));
 }
 __global__ void __launch_bounds__(NT) k_red_cg_init(DevStatic S, Ctl *ctl, Glob *glob,
                                                    const double *part) {
@@ -679,8 +637,8 @@ __global__ void __launch_bounds__(NT) k_red_cg_init(DevStatic S, Ctl *ctl, Glob 
 
 // :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA).
 template <bool MA>
-__global__ void __launch_bounds__(NT, 2) k_cg_matvec(DevStatic S, DevSystem Y, const Ctl *ctl,
-                                                    double *part) {
+__global__ void __launch_bounds__(NT, 2) k_cg_matvec(DevStatic S, DevSystem Y, Ctl *ctl,
+                                                    double *part, int fold) {
   struct A {
     bool skip, asym;
     double beta;
@@ -697,7 +655,10 @@ __global__ void __launch_bounds__(NT, 2) k_cg_matvec(DevStatic S, DevSystem Y, c
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         v[0] = matvec_row_z(g, valid, Y.z, Y.ccc, a.pold, a.pnew, Y.ccs, Y.ccw, Y.cce, Y.ccn,
                             Y.ap, a.beta, a.asym);
-      });
+      },
+      fold_with(fold ? ctl : nullptr, [&](int m, const double *sum) {
+        if (threadIdx.x == 0) cg_matvec_epi(ctl[m], sum[0]);
+      }));
 }
 __global__ void __launch_bounds__(NT) k_red_cg_matvec(DevStatic S, Ctl *ctl, const double *part) {
   member_reduce<1>(
@@ -710,7 +671,7 @@ __global__ void __launch_bounds__(NT) k_red_cg_matvec(DevStatic S, Ctl *ctl, con
 // :127-149 (P, RCG update, RPCGN, RSQ, BETA) and the stop test :165.  With
 // no_stop the iteration continues past RSQM and ITERM (kernel timing only).
 __global__ void __launch_bounds__(NT, 5) k_cg_update(DevStatic S, DevSystem Y, double *P,
-                                                    const Ctl *ctl, double *part) {
+                                                    Ctl *ctl, double *part, RedArgs ra) {
   struct A {
     bool skip;
     double alpha;
@@ -724,7 +685,10 @@ __global__ void __launch_bounds__(NT, 5) k_cg_update(DevStatic S, DevSystem Y, d
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         update_row<double>(g, valid, P, a.pnew, Y.r, Y.ap, Y.ccc, a.alpha, v[0], v[1], Y.z);
-      });
+      },
+      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+        if (threadIdx.x == 0) cg_update_epi(ctl[m], ra.glob, S.sc[m], sum[0], sum[1], ra.no_stop);
+      }));
 }
 __global__ void __launch_bounds__(NT) k_red_cg_update(DevStatic S, Ctl *ctl, Glob *glob,
                                                      const double *part, int no_stop) {
@@ -909,9 +873,48 @@ __global__ void __launch_bounds__(SMALL_NT) k_cg_small(DevStatic S, DevSystem Y,
 // x = 0 and p0 = rhat (k_mx_zinit then forms z0 = M^-1 rhat and p_old = 0 for
 // the polynomial members).  rsqm_fac scales the member's RSQM (the MIXED stop,
 // below RSQM).  EAGER: the row's loads issued first (kernel variant 3).
+// The member's epilogue of the refinement residual: RSQ (of the scaled system,
+// as CONGRAD measures it), the stop test on the FP64 RSQ, and the inner
+// solve's target.
+__device__ __forceinline__ void mx_resid_epi(Ctl &k, const StepScalars &c, const RedArgs &ra,
+                                             double rsq, double rz) {
+  if (ra.unscaled) {
+    const double ccmnm = fmin(k.ccmnm_int, k.ccmnm_bc);
+    rsq = rsq / (ccmnm * ccmnm);
+  }
+  const double rsqm = c.rsqm * ra.rsqm_fac;
+  k.rsq64 = rsq;
+  k.rsq = rsq;
+  k.rpcg = rz;
+  k.beta = 0.0;
+  k.parity = 0;
+  k.inner_iter = 0;
+  k.idone = 0;
+  k.outer += 1;
+  // inner stop on the scaled residual: reduce it by the factor the FP64
+  // residual needs to reach 0.1*RSQM, and by at least rel_tol (in norm)
+  const double need = (rsq > 0.0) ? ra.margin * 0.1 * rsqm / rsq : 1.0;
+  k.rsq_target = rz * fmax(fmin(need, 1.0), ra.rel_tol * ra.rel_tol);
+  int fin = 0;
+  if (!isfinite(rsq)) {
+    k.status = EFDC_XM_NONFINITE;
+    fin = 1;
+  } else if (!ra.no_stop && (rsq <= rsqm || rz == 0.0)) {
+    fin = 1;
+  } else if (!ra.no_stop && k.iter >= 2 * c.iterm + 50) {
+    k.status = EFDC_XM_CG_MAXITER;  // inner iterations of all passes exhausted
+    fin = 1;
+  }
+  if (fin) {
+    k.done = 1;
+    atomicAdd(&ra.glob->ndone, 1);
+  }
+}
+
 template <bool MA, bool EAGER>
 __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, SysView V, DevSystem Y,
-                                                const double *P, const Ctl *ctl, double *part) {
+                                                const double *P, Ctl *ctl, double *part,
+                                                RedArgs ra) {
   struct A {
     bool skip, asym;
   };
@@ -934,50 +937,17 @@ __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, SysView V, DevSyst
           v[1] = double(r32.x) * double(r32.x) + double(r32.y) * double(r32.y) +
                  double(r32.z) * double(r32.z) + double(r32.w) * double(r32.w);
         }
-      });
+      },
+      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+        if (threadIdx.x == 0) mx_resid_epi(ctl[m], S.sc[m], ra, sum[0], sum[1]);
+      }));
 }
-__global__ void __launch_bounds__(NT) k_red_mx_resid(DevStatic S, Ctl *ctl, Glob *glob,
-                                                    const double *part, double rsqm_fac,
-                                                    double rel_tol, int no_stop, int unscaled,
-                                                    double margin) {
+__global__ void __launch_bounds__(NT) k_red_mx_resid(DevStatic S, Ctl *ctl, const double *part,
+                                                    RedArgs ra) {
   member_reduce<2>(
       S, part, [&](int m) { return ctl[m].done != 0; },
       [&](int m, const double *sum) {
-        if (threadIdx.x != 0) return;
-        Ctl &k = ctl[m];
-        double rsq = sum[0];
-        if (unscaled) {  // RSQ of the scaled system, as CONGRAD measures it
-          const double ccmnm = fmin(k.ccmnm_int, k.ccmnm_bc);
-          rsq = rsq / (ccmnm * ccmnm);
-        }
-        const double rz = sum[1];
-        const double rsqm = S.sc[m].rsqm * rsqm_fac;
-        k.rsq64 = rsq;
-        k.rsq = rsq;
-        k.rpcg = rz;
-        k.beta = 0.0;
-        k.parity = 0;
-        k.inner_iter = 0;
-        k.idone = 0;
-        k.outer += 1;
-        // inner stop on the scaled residual: reduce it by the factor the FP64
-        // residual needs to reach 0.1*RSQM, and by at least rel_tol (in norm)
-        const double need = (rsq > 0.0) ? margin * 0.1 * rsqm / rsq : 1.0;
-        k.rsq_target = rz * fmax(fmin(need, 1.0), rel_tol * rel_tol);
-        int fin = 0;
-        if (!isfinite(rsq)) {
-          k.status = EFDC_XM_NONFINITE;
-          fin = 1;
-        } else if (!no_stop && (rsq <= rsqm || rz == 0.0)) {
-          fin = 1;
-        } else if (!no_stop && k.iter >= 2 * S.sc[m].iterm + 50) {
-          k.status = EFDC_XM_CG_MAXITER;  // inner iterations of all passes exhausted
-          fin = 1;
-        }
-        if (fin) {
-          k.done = 1;
-          atomicAdd(&glob->ndone, 1);
-        }
+        if (threadIdx.x == 0) mx_resid_epi(ctl[m], S.sc[m], ra, sum[0], sum[1]);
       });
 }
 
@@ -1543,13 +1513,20 @@ static int quad_grid(const Launch &l, const DevStatic &S, K kernel) {
 
 void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                     Glob *glob, double *part) {
+  RedArgs ra{};
+  ra.glob = glob;
+  ra.fold = l.fold;
   if (l.may_asym)
-    k_cg_init<true><<<quad_grid(l, S, k_cg_init<true>), NT, 0, l.stream>>>(S, Y, P, ctl, part);
+    k_cg_init<true><<<quad_grid(l, S, k_cg_init<true>), NT, 0, l.stream>>>(S, Y, P, ctl, part,
+                                                                          ra);
   else
-    k_cg_init<false><<<quad_grid(l, S, k_cg_init<false>), NT, 0, l.stream>>>(S, Y, P, ctl, part);
+    k_cg_init<false><<<quad_grid(l, S, k_cg_init<false>), NT, 0, l.stream>>>(S, Y, P, ctl, part,
+                                                                            ra);
+  count_launches(1);
+  if (l.fold) return;
   launch_chan_res64(l, S, Y, P, ctl, part);
   k_red_cg_init<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part);
-  count_launches(2);
+  count_launches(1);
 }
 // Shared memory of k_cg_small for windows of up to `slots` slots (its six
 // vectors); false when that is more than a CTA can have.
@@ -1583,19 +1560,28 @@ void launch_cg_small(const Launch &l, const DevStatic &S, const DevSystem &Y, do
 void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {
   if (l.may_asym)
-    k_cg_matvec<true><<<quad_grid(l, S, k_cg_matvec<true>), NT, 0, l.stream>>>(S, Y, ctl, part);
+    k_cg_matvec<true><<<quad_grid(l, S, k_cg_matvec<true>), NT, 0, l.stream>>>(S, Y, ctl, part,
+                                                                              l.fold);
   else
     k_cg_matvec<false><<<quad_grid(l, S, k_cg_matvec<false>), NT, 0, l.stream>>>(S, Y, ctl,
-                                                                               part);
+                                                                               part, l.fold);
+  count_launches(1);
+  if (l.fold) return;
   launch_chan_mv64(l, S, Y, ctl, part);
   k_red_cg_matvec<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part);
-  count_launches(2);
+  count_launches(1);
 }
 void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                       Glob *glob, double *part, int no_stop) {
-  k_cg_update<<<quad_grid(l, S, k_cg_update), NT, 0, l.stream>>>(S, Y, P, ctl, part);
+  RedArgs ra{};
+  ra.glob = glob;
+  ra.no_stop = no_stop;
+  ra.fold = l.fold;
+  k_cg_update<<<quad_grid(l, S, k_cg_update), NT, 0, l.stream>>>(S, Y, P, ctl, part, ra);
+  count_launches(1);
+  if (l.fold) return;
   k_red_cg_update<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, no_stop);
-  count_launches(2);
+  count_launches(1);
 }
 void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                     Glob *glob, double *part) {
@@ -1605,24 +1591,34 @@ void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, dou
 void launch_mx_resid(const Launch &l, const DevStatic &S, const SysView &V, const DevSystem &Y,
                      const double *P, Ctl *ctl, Glob *glob, double *part, double rsqm_fac,
                      double rel_tol, int no_stop) {
+  RedArgs ra{};
+  ra.glob = glob;
+  ra.rsqm_fac = rsqm_fac;
+  ra.rel_tol = rel_tol;
+  ra.margin = l.inner_margin;
+  ra.no_stop = no_stop;
+  ra.unscaled = V.unscaled;
+  ra.fold = l.fold;
   if (l.variant == 3) {
     if (l.may_asym)
       k_mx_resid<true, true><<<quad_grid(l, S, k_mx_resid<true, true>), NT, 0, l.stream>>>(
-          S, V, Y, P, ctl, part);
+          S, V, Y, P, ctl, part, ra);
     else
       k_mx_resid<false, true><<<quad_grid(l, S, k_mx_resid<false, true>), NT, 0, l.stream>>>(
-          S, V, Y, P, ctl, part);
+          S, V, Y, P, ctl, part, ra);
   } else if (l.may_asym) {
     k_mx_resid<true, false><<<quad_grid(l, S, k_mx_resid<true, false>), NT, 0, l.stream>>>(
-        S, V, Y, P, ctl, part);
+        S, V, Y, P, ctl, part, ra);
   } else {
     k_mx_resid<false, false><<<quad_grid(l, S, k_mx_resid<false, false>), NT, 0, l.stream>>>(
-        S, V, Y, P, ctl, part);
+        S, V, Y, P, ctl, part, ra);
   }
-  launch_chan_resmx(l, S, V, Y, P, ctl, part);
-  k_red_mx_resid<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, rsqm_fac, rel_tol,
-                                                      no_stop, V.unscaled, l.inner_margin);
-  count_launches(2);
+  count_launches(1);
+  if (!l.fold) {
+    launch_chan_resmx(l, S, V, Y, P, ctl, part);
+    k_red_mx_resid<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part, ra);
+    count_launches(1);
+  }
   launch_mx_zinit(l, S, Y, ctl, part);  // z0 = M^-1 r0 of the inner solve
 }
 void launch_mx_apply(const Launch &l, const DevStatic &S, const SysView &V, const DevSystem &Y,

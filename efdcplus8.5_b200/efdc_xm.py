@@ -432,6 +432,8 @@ OPT_POLY_THRESHOLD = 6
 OPT_INNER_MARGIN = 7
 OPT_INNER_TOL = 8
 OPT_SMALL_SOLVE = 9
+OPT_FOLD_REDUCE = 10
+OPT_CHUNKS = 11
 
 
 TUNE_MEASURE = 1

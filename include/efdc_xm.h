@@ -563,6 +563,18 @@ int64_t efdc_xm_host_waits(void);
  *     one launch with one CTA per member, its vectors in shared memory; 0
  *     runs it as the kernels of every other context.  Both give the same
  *     results bit for bit.
+ *   EFDC_XM_OPT_FOLD_REDUCE (default 1, 0..2): 2 finishes each member's CG
+ *     sums (its dot products, ALPHA, BETA and stop tests) inside the kernel
+ *     that forms them, in the CTA that stores the member's last partial sum;
+ *     0 runs a separate member-reduce kernel after each CG kernel; 1 takes
+ *     the first form for contexts of up to 4 members and the second for
+ *     larger batches.  Contexts with sub-grid channels always take the
+ *     second form.  Both give the same results bit for bit.
+ *   EFDC_XM_OPT_CHUNKS (default 8, 1..32): efdc_xm_step_batch of two or
+ *     more members steps them in this many member chunks of about equal cell
+ *     counts, so that the upload of one chunk, the step of an earlier one and
+ *     the download of a still earlier one overlap.  Results do not depend on
+ *     it.
  * Results stay within the MIXED form's error bar whatever the schedule; the
  * FP64 form's results do not depend on it.
  * Returns EFDC_XM_BAD_ARGUMENT for an unknown option or value. */
@@ -575,7 +587,9 @@ enum {
   EFDC_XM_OPT_POLY_THRESHOLD = 6,
   EFDC_XM_OPT_INNER_MARGIN = 7,
   EFDC_XM_OPT_INNER_TOL = 8,
-  EFDC_XM_OPT_SMALL_SOLVE = 9
+  EFDC_XM_OPT_SMALL_SOLVE = 9,
+  EFDC_XM_OPT_FOLD_REDUCE = 10,
+  EFDC_XM_OPT_CHUNKS = 11
 };
 int32_t efdc_xm_set_option(efdc_xm_ctx *ctx, int32_t option, int32_t value);
 
