@@ -8,6 +8,8 @@
 // land slots (P(LC), the ghost value), mask with the slot kind.
 #pragma once
 
+#include <type_traits>
+
 #include "../../include/efdc_xm.h"
 #include "xm_common.cuh"
 #include "xm_tma.cuh"
@@ -68,18 +70,14 @@ __device__ __forceinline__ unsigned int atomic_add_acq_rel(unsigned int *p, unsi
 }
 
 // The member reduction folded into a CG kernel: ctl holds the members'
-// arrival counters (nullptr: not folded, a member-reduce kernel follows) and
-// epi(m, sums) finishes member m (all threads call it; the sums are valid in
-// thread 0).
+// arrival counters and epi(m, sums) finishes member m (all threads call it;
+// the sums are valid in thread 0).  Fold<NoEpi>: not folded, a member-reduce
+// kernel follows.
 template <class Epi>
 struct Fold {
   Ctl *ctl;
   Epi epi;
 };
-template <class Epi>
-__device__ __forceinline__ Fold<Epi> fold_with(Ctl *ctl, Epi epi) {
-  return Fold<Epi>{ctl, epi};
-}
 struct NoEpi {
   __device__ void operator()(int, const double *) const {}
 };
@@ -90,9 +88,17 @@ struct RedArgs {
   double rsqm_fac, rel_tol, margin;  // MIXED refinement residual (k_mx_resid)
   int no_stop;                       // iterate past the stop tests (kernel timing)
   int unscaled;                      // MIXED residual of the unscaled system
-  int fold;                          // the member reduction folded into the kernel
 };
 __device__ __forceinline__ Fold<NoEpi> no_fold() { return Fold<NoEpi>{nullptr, NoEpi{}}; }
+// The fold of a kernel compiled with FOLD, else none (the kernel then has no
+// trace of it: no counters, no atomics, no registers held for it).
+template <bool FOLD, class Epi>
+__device__ __forceinline__ auto fold_if(Ctl *ctl, Epi epi) {
+  if constexpr (FOLD)
+    return Fold<Epi>{ctl, epi};
+  else
+    return no_fold();
+}
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -103,10 +109,13 @@ __device__ __forceinline__ double warp_sum(double v) {
 template <int NS, class Epi>
 __device__ __forceinline__ void quad_store(QuadLog<NS> &L, int n, const DevStatic &S,
                                            double *part, const Fold<Epi> &f) {
+  constexpr bool kFold = !std::is_same<Epi, NoEpi>::value;
   __shared__ int nfin;
   __shared__ int fin[QCAP];
   __shared__ double sh[32];
-  if (threadIdx.x == 0) nfin = 0;
+  if constexpr (kFold) {
+    if (threadIdx.x == 0) nfin = 0;
+  }
   __syncthreads();  // the warp partials and the entries are in shared memory
   const int t = threadIdx.x;
   if (t < n) {
@@ -117,14 +126,15 @@ __device__ __forceinline__ void quad_store(QuadLog<NS> &L, int n, const DevStati
       for (int w = 0; w < NWARP; ++w) a += L.w[s][t][w];
       part[size_t(s) * S.nquad + L.qd[t]] = a;
     }
-    if (f.ctl) {  // this quad arrives (release: after its partials)
+    if constexpr (kFold) {  // this quad arrives (release: after its partials)
       const int m = L.m[t];
       const unsigned int nq = unsigned(S.qstart[m + 1] - S.qstart[m]);
       if (atomic_add_acq_rel(&f.ctl[m].counter, 1u) == nq - 1u) fin[atomicAdd(&nfin, 1)] = m;
     }
   }
-  __syncthreads();  // orders the acquiring thread's view before the CTA's reads
-  if (f.ctl) {
+  __syncthreads();  // the log is reused after this (folded: the list is complete, and the
+                    // acquiring threads' view orders the CTA's reads below)
+  if constexpr (kFold) {
     const int k = nfin;
     for (int i = 0; i < k; ++i) {  // the members this CTA completed (any order)
       const int m = fin[i];
@@ -136,8 +146,8 @@ __device__ __forceinline__ void quad_store(QuadLog<NS> &L, int n, const DevStati
       f.epi(m, r);
       if (t == 0) f.ctl[m].counter = 0u;  // for the next kernel
     }
+    __syncthreads();  // the list is reused after this
   }
-  __syncthreads();  // the log is reused after this
 }
 
 // One CG kernel over all quads.  setup(m) returns the member's values for the
@@ -186,7 +196,7 @@ __device__ __forceinline__ void quad_sweep(const DevStatic &S, double *part, Set
       }
       if (threadIdx.x == 0) {
         L.qd[n] = qd;
-        L.m[n] = cur.x;
+        if constexpr (!std::is_same<Epi, NoEpi>::value) L.m[n] = cur.x;
       }
       if (++n == QCAP) {
         quad_store<NS>(L, n, S, part, f);
@@ -257,7 +267,7 @@ __device__ __forceinline__ void quad_sweep_batched(const DevStatic &S, double *p
       }
       if (threadIdx.x == 0) {
         L.qd[n] = b0 + k * G;
-        L.m[n] = cur.x;
+        if constexpr (!std::is_same<Epi, NoEpi>::value) L.m[n] = cur.x;
       }
       if (++n == QCAP) {
         quad_store<NS>(L, n, S, part, f);
@@ -406,7 +416,7 @@ __device__ __forceinline__ void quad_sweep_staged(const DevStatic &S, double *pa
       }
       if (threadIdx.x == 0) {
         L.qd[n] = b0 + k * G;
-        L.m[n] = cur.x;
+        if constexpr (!std::is_same<Epi, NoEpi>::value) L.m[n] = cur.x;
       }
       __syncthreads();  // every thread is done with stage s: it may be refilled
       if (threadIdx.x == 0 && !dead && j + NSTG < nl) issue(j + NSTG);
@@ -593,9 +603,7 @@ __device__ __forceinline__ double matvec_row(const RowGeo &g, bool valid, const 
 
 // FP64: as matvec_row, with z = CCCI*r stored by the kernels that write r, so
 // that the halo rows need z and p_old only: p = z + beta*p_old has the same
-// roundings as CCCI*r + beta*p_old formed in place.  Every load of the row is
-// issued before its first shuffle or dependent operation (see
-// matvec_row_scaled_eager): one round trip to memory per row.
+// roundings as CCCI*r + beta*p_old formed in place.
 __device__ __forceinline__ double matvec_row_z(const RowGeo &g, bool valid,
                                                const double *__restrict__ z,
                                                const double *__restrict__ ccc,
@@ -606,27 +614,25 @@ __device__ __forceinline__ double matvec_row_z(const RowGeo &g, bool valid,
                                                const double *__restrict__ cce,
                                                const double *__restrict__ ccn,
                                                double *__restrict__ ap, double beta, bool asym) {
-  // every load first, so that one round trip serves the row
   const V4<double> z0 = ld4(z + g.d0), o0 = ld4(pold + g.d0);
   const V4<double> zn = ld4(z + g.dn), on = ld4(pold + g.dn);
   const V4<double> zs = ld4(z + g.ds), os = ld4(pold + g.ds);
-  const V4<double> c0 = ld4(ccc + g.d0), ks = ld4(ccs + g.d0), kw = ld4(ccw + g.d0);
-  const V4<double> kn = asym ? ld4(ccn + g.d0) : ld4(ccs + g.dn);
-  V4<double> ke = asym ? ld4(cce + g.d0) : V4<double>{0., 0., 0., 0.};
-  const bool west = g.cx == 0, east = g.cx == ROWT - 1;
-  const double zw = west ? z[g.dwe] : 0., ow = west ? pold[g.dwe] : 0.;
-  const double ze = east ? z[g.dee] : 0., oe = east ? pold[g.dee] : 0.;
-  const double kwe_edge = (east && !asym) ? ccw[g.dee] : 0.;
   auto pc = [&](double zz, double po) { return zz + beta * po; };
   const V4<double> p = {pc(z0.x, o0.x), pc(z0.y, o0.y), pc(z0.z, o0.z), pc(z0.w, o0.w)};
   const V4<double> pn = {pc(zn.x, on.x), pc(zn.y, on.y), pc(zn.z, on.z), pc(zn.w, on.w)};
   const V4<double> ps = {pc(zs.x, os.x), pc(zs.y, os.y), pc(zs.z, os.z), pc(zs.w, os.w)};
   double pw = from_west(p), pe = from_east(p);
-  if (west) pw = pc(zw, ow);
-  if (east) pe = pc(ze, oe);
-  if (!asym) {
+  if (g.cx == 0) pw = pc(z[g.dwe], pold[g.dwe]);
+  if (g.cx == ROWT - 1) pe = pc(z[g.dee], pold[g.dee]);
+  const V4<double> c0 = ld4(ccc + g.d0), ks = ld4(ccs + g.d0), kw = ld4(ccw + g.d0);
+  V4<double> kn, ke;
+  if (asym) {
+    kn = ld4(ccn + g.d0);
+    ke = ld4(cce + g.d0);
+  } else {
+    kn = ld4(ccs + g.dn);
     double kwe = from_east(kw);
-    if (east) kwe = kwe_edge;
+    if (g.cx == ROWT - 1) kwe = ccw[g.dee];
     ke = {kw.y, kw.z, kw.w, kwe};
   }
   V4<double> a;

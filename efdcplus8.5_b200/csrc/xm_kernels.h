@@ -50,12 +50,12 @@ void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const 
 // CALPUV9C: the kernels up to the time-level advance, and the copies of the advance
 void launch_begin3(const Launch &l, const DevStatic &S, const DevState &X, const int *act);
 void launch_advance3(const Launch &l, const DevStatic &S, const DevState &X);
-// the implicit bottom / vegetation drag (RCX, RCY) of the members with ISITB >= 1
-// or ISVEG > 0, after the begin kernel
 // CALEXP2T's external-mode terms of every member with its static part; the
 // depth sums go to X.fcaxe, X.fcaye, X.fxe, X.fye.
 void launch_explicit(const Launch &l, const DevStatic &S, const MomDev &M, const DevState &X,
                      int kcmax, int nmember);
+// the implicit bottom / vegetation drag (RCX, RCY) of the members with ISITB >= 1
+// or ISVEG > 0, after the begin kernel
 void launch_implicit_drag(const Launch &l, const DevStatic &S, const DevState &X,
                           const int *act);
 void launch_put(cudaStream_t st, const int *idx, const double *val, int n, double *dst);

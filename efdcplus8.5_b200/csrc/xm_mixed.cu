@@ -28,9 +28,9 @@ namespace xm {
 // CTAs per SM the launch bounds ask for, by variant (3 holds more values live)
 constexpr int mx_ctas(int var) { return var == 1 ? 5 : var == 3 ? 4 : 6; }
 
-template <bool MA, int VAR>
+template <bool MA, int VAR, bool FOLD>
 __global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_matvec(DevStatic S, DevSystem Y, Ctl *ctl,
-                                                    double *part, int fold) {
+                                                    double *part) {
   struct A {
     bool skip, asym;
     float beta;
@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_matvec(DevStatic S, Dev
           v[0] = matvec_row_scaled(g, valid, a.z, a.pold, a.pnew, Y.as32, Y.aw32, Y.ae32,
                                    Y.an32, Y.ap32, a.beta, a.asym);
       },
-      fold_with(fold ? ctl : nullptr, [&](int m, const double *sum) {
+      fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0) cg_matvec_epi(ctl[m], sum[0]);
       }));
 }
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(NT) k_red_mx_matvec(DevStatic S, Ctl *ctl, con
 
 // x += alpha*p, r -= alpha*Ap, z = (2I - Ahat) r (the two-term Neumann
 // polynomial), r.z and r.r (FP64 sums): the members that use it.
-template <int VAR>
+template <int VAR, bool FOLD>
 __global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_update_poly(DevStatic S, DevSystem Y,
                                                          Ctl *ctl, double *part, RedArgs ra) {
   struct A {
@@ -98,14 +98,14 @@ __global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_update_poly(DevStatic S
           update_row_poly(g, valid, Y.x32, a.pnew, a.r, a.rnew, Y.ap32, Y.as32, Y.aw32, Y.z32,
                           a.alpha, true, v[0], v[1]);
       },
-      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+      fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0)
           mx_update_epi(ctl[m], ra.glob, S.sc[m].iterm, sum[0], sum[1], 2.0, ra.no_stop);
       }));
 }
 // The same for the Jacobi members (z = r): x, r and r.r only.
-template <int VAR>
-__global__ void __launch_bounds__(NT, 8) k_mx_update_jac(DevStatic S, DevSystem Y, Ctl *ctl,
+template <int VAR, bool FOLD>
+__global__ void __launch_bounds__(NT) k_mx_update_jac(DevStatic S, DevSystem Y, Ctl *ctl,
                                                      double *part, RedArgs ra) {
   struct A {
     bool skip;
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(NT, 8) k_mx_update_jac(DevStatic S, DevSystem 
         v[0] = rr;
         v[1] = rr;
       },
-      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+      fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0)
           mx_update_epi(ctl[m], ra.glob, S.sc[m].iterm, sum[0], sum[1], 2.0, ra.no_stop);
       }));
@@ -149,9 +149,9 @@ __global__ void __launch_bounds__(NT) k_red_mx_update(DevStatic S, Ctl *ctl, Glo
 
 // First inner iteration of the polynomial members: z0 = (2I - Ahat) r0,
 // p_old = 0, RPCG = r0.z0 (Jacobi members start from k_mx_resid's p0 = r0).
-template <bool EAGER>
+template <bool EAGER, bool FOLD>
 __global__ void __launch_bounds__(NT) k_mx_zinit(DevStatic S, DevSystem Y, Ctl *ctl,
-                                                double *part, int fold) {
+                                                double *part) {
   struct A {
     bool skip, asym;
   };
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(NT) k_mx_zinit(DevStatic S, DevSystem Y, Ctl *
         else
           v[0] = zinit_row(g, valid, Y.r32, Y.as32, Y.aw32, Y.z32, Y.pa32, true);
       },
-      fold_with(fold ? ctl : nullptr, [&](int m, const double *sum) {
+      fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0) ctl[m].rpcg = sum[0];
       }));
 }
@@ -198,9 +198,9 @@ using MvStage = Stage<4>;    // z, p_old, AS, AW
 using PolyStage = Stage<6>;  // r, Ap, AS, AW, x, p
 using JacStage = Stage<4>;   // x, p, r, Ap
 
-template <bool MA>
+template <bool MA, bool FOLD>
 __global__ void __launch_bounds__(NT, 3) k_mx_matvec_st(DevStatic S, DevSystem Y, Ctl *ctl,
-                                                       double *part, int fold) {
+                                                       double *part) {
   struct A {
     bool skip, asym;
     float beta;
@@ -276,11 +276,12 @@ __global__ void __launch_bounds__(NT, 3) k_mx_matvec_st(DevStatic S, DevSystem Y
         v[0] = double(ap.x) * double(p.x) + double(ap.y) * double(p.y) +
                double(ap.z) * double(p.z) + double(ap.w) * double(p.w);
       },
-      fold_with(fold ? ctl : nullptr, [&](int m, const double *sum) {
+      fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0) cg_matvec_epi(ctl[m], sum[0]);
       }));
 }
 
+template <bool FOLD>
 __global__ void __launch_bounds__(NT, 3) k_mx_update_poly_st(DevStatic S, DevSystem Y,
                                                             Ctl *ctl, double *part, RedArgs ra) {
   struct A {
@@ -359,12 +360,13 @@ __global__ void __launch_bounds__(NT, 3) k_mx_update_poly_st(DevStatic S, DevSys
         v[1] = double(rn0.x) * double(rn0.x) + double(rn0.y) * double(rn0.y) +
                double(rn0.z) * double(rn0.z) + double(rn0.w) * double(rn0.w);
       },
-      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+      fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0)
           mx_update_epi(ctl[m], ra.glob, S.sc[m].iterm, sum[0], sum[1], 2.0, ra.no_stop);
       }));
 }
 
+template <bool FOLD>
 __global__ void __launch_bounds__(NT, 4) k_mx_update_jac_st(DevStatic S, DevSystem Y,
                                                            Ctl *ctl, double *part, RedArgs ra) {
   struct A {
@@ -404,7 +406,7 @@ __global__ void __launch_bounds__(NT, 4) k_mx_update_jac_st(DevStatic S, DevSyst
         v[0] = rr;
         v[1] = rr;
       },
-      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+      fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0)
           mx_update_epi(ctl[m], ra.glob, S.sc[m].iterm, sum[0], sum[1], 2.0, ra.no_stop);
       }));
@@ -470,95 +472,116 @@ static int grid_of(const Launch &l, const DevStatic &S, K kernel, int cap) {
   return std::max(1, std::min(S.nquad, l.nsm * b));
 }
 
-void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
-                      double *part) {
-  const int f = l.fold;
+template <bool F>
+static void mx_matvec_kernel(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
+                             double *part) {
   if (l.variant == 2) {
     if (l.may_asym) {
-      const size_t sm = staged_smem(k_mx_matvec_st<true>, sizeof(MvStage), MV_STAGES);
-      k_mx_matvec_st<true><<<staged_grid(l, S, k_mx_matvec_st<true>, sm, l.ctas_mv), NT, sm,
-                             l.stream>>>(S, Y, ctl, part, f);
+      const size_t sm = staged_smem(k_mx_matvec_st<true, F>, sizeof(MvStage), MV_STAGES);
+      k_mx_matvec_st<true, F><<<staged_grid(l, S, k_mx_matvec_st<true, F>, sm, l.ctas_mv), NT,
+                                sm, l.stream>>>(S, Y, ctl, part);
     } else {
-      const size_t sm = staged_smem(k_mx_matvec_st<false>, sizeof(MvStage), MV_STAGES);
-      k_mx_matvec_st<false><<<staged_grid(l, S, k_mx_matvec_st<false>, sm, l.ctas_mv), NT, sm,
-                              l.stream>>>(S, Y, ctl, part, f);
+      const size_t sm = staged_smem(k_mx_matvec_st<false, F>, sizeof(MvStage), MV_STAGES);
+      k_mx_matvec_st<false, F><<<staged_grid(l, S, k_mx_matvec_st<false, F>, sm, l.ctas_mv), NT,
+                                 sm, l.stream>>>(S, Y, ctl, part);
     }
   } else if (l.variant == 1) {
     if (l.may_asym)
-      k_mx_matvec<true, 1><<<grid_of(l, S, k_mx_matvec<true, 1>, l.ctas_mv), NT, 0, l.stream>>>(
-          S, Y, ctl, part, f);
+      k_mx_matvec<true, 1, F><<<grid_of(l, S, k_mx_matvec<true, 1, F>, l.ctas_mv), NT, 0,
+                                l.stream>>>(S, Y, ctl, part);
     else
-      k_mx_matvec<false, 1><<<grid_of(l, S, k_mx_matvec<false, 1>, l.ctas_mv), NT, 0,
-                              l.stream>>>(S, Y, ctl, part, f);
+      k_mx_matvec<false, 1, F><<<grid_of(l, S, k_mx_matvec<false, 1, F>, l.ctas_mv), NT, 0,
+                                 l.stream>>>(S, Y, ctl, part);
   } else if (l.variant == 3) {
     if (l.may_asym)
-      k_mx_matvec<true, 3><<<grid_of(l, S, k_mx_matvec<true, 3>, l.ctas_mv), NT, 0, l.stream>>>(
-          S, Y, ctl, part, f);
+      k_mx_matvec<true, 3, F><<<grid_of(l, S, k_mx_matvec<true, 3, F>, l.ctas_mv), NT, 0,
+                                l.stream>>>(S, Y, ctl, part);
     else
-      k_mx_matvec<false, 3><<<grid_of(l, S, k_mx_matvec<false, 3>, l.ctas_mv), NT, 0,
-                              l.stream>>>(S, Y, ctl, part, f);
+      k_mx_matvec<false, 3, F><<<grid_of(l, S, k_mx_matvec<false, 3, F>, l.ctas_mv), NT, 0,
+                                 l.stream>>>(S, Y, ctl, part);
   } else if (l.may_asym) {
-    k_mx_matvec<true, 0><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part, f);
+    k_mx_matvec<true, 0, F><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
   } else {
-    k_mx_matvec<false, 0><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part, f);
+    k_mx_matvec<false, 0, F><<<l.grid_cg32, NT, 0, l.stream>>>(S, Y, ctl, part);
   }
   count_launches(1);
-  if (f) return;
+}
+void launch_mx_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
+                      double *part) {
+  if (l.fold) {
+    mx_matvec_kernel<true>(l, S, Y, ctl, part);
+    return;
+  }
+  mx_matvec_kernel<false>(l, S, Y, ctl, part);
   launch_chan_mvmx(l, S, Y, ctl, part);
   k_red_mx_matvec<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part);
   count_launches(1);
+}
+template <bool F>
+static void mx_update_kernels(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
+                              double *part, const RedArgs &ra) {
+  if (l.mx_jac && l.variant == 2) {
+    const size_t sm = staged_smem(k_mx_update_jac_st<F>, sizeof(JacStage), JAC_STAGES);
+    k_mx_update_jac_st<F><<<staged_grid(l, S, k_mx_update_jac_st<F>, sm, l.ctas_up), NT, sm,
+                            l.stream>>>(S, Y, ctl, part, ra);
+    count_launches(1);
+  } else if (l.mx_jac) {
+    if (l.variant == 1 || l.variant == 3)  // the Jacobi row already loads first
+      k_mx_update_jac<1, F><<<grid_of(l, S, k_mx_update_jac<1, F>, l.ctas_up), NT, 0,
+                              l.stream>>>(S, Y, ctl, part, ra);
+    else
+      k_mx_update_jac<0, F><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part, ra);
+    count_launches(1);
+  }
+  if (l.mx_poly && l.variant == 2) {
+    const size_t sm = staged_smem(k_mx_update_poly_st<F>, sizeof(PolyStage), POLY_STAGES);
+    k_mx_update_poly_st<F><<<staged_grid(l, S, k_mx_update_poly_st<F>, sm, l.ctas_up), NT, sm,
+                             l.stream>>>(S, Y, ctl, part, ra);
+    count_launches(1);
+  } else if (l.mx_poly) {
+    if (l.variant == 1)
+      k_mx_update_poly<1, F><<<grid_of(l, S, k_mx_update_poly<1, F>, l.ctas_up), NT, 0,
+                               l.stream>>>(S, Y, ctl, part, ra);
+    else if (l.variant == 3)
+      k_mx_update_poly<3, F><<<grid_of(l, S, k_mx_update_poly<3, F>, l.ctas_up), NT, 0,
+                               l.stream>>>(S, Y, ctl, part, ra);
+    else
+      k_mx_update_poly<0, F><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part, ra);
+    count_launches(1);
+  }
 }
 void launch_mx_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       Glob *glob, double *part, int no_stop) {
   RedArgs ra{};
   ra.glob = glob;
   ra.no_stop = no_stop;
-  ra.fold = l.fold;
-  if (l.mx_jac && l.variant == 2) {
-    const size_t sm = staged_smem(k_mx_update_jac_st, sizeof(JacStage), JAC_STAGES);
-    k_mx_update_jac_st<<<staged_grid(l, S, k_mx_update_jac_st, sm, l.ctas_up), NT, sm,
-                         l.stream>>>(S, Y, ctl, part, ra);
-    count_launches(1);
-  } else if (l.mx_jac) {
-    if (l.variant == 1 || l.variant == 3)  // the Jacobi row already loads first
-      k_mx_update_jac<1><<<grid_of(l, S, k_mx_update_jac<1>, l.ctas_up), NT, 0, l.stream>>>(
-          S, Y, ctl, part, ra);
-    else
-      k_mx_update_jac<0><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part, ra);
-    count_launches(1);
+  if (l.fold) {
+    mx_update_kernels<true>(l, S, Y, ctl, part, ra);
+    return;
   }
-  if (l.mx_poly && l.variant == 2) {
-    const size_t sm = staged_smem(k_mx_update_poly_st, sizeof(PolyStage), POLY_STAGES);
-    k_mx_update_poly_st<<<staged_grid(l, S, k_mx_update_poly_st, sm, l.ctas_up), NT, sm,
-                          l.stream>>>(S, Y, ctl, part, ra);
-    count_launches(1);
-  } else if (l.mx_poly) {
-    if (l.variant == 1)
-      k_mx_update_poly<1><<<grid_of(l, S, k_mx_update_poly<1>, l.ctas_up), NT, 0, l.stream>>>(
-          S, Y, ctl, part, ra);
-    else if (l.variant == 3)
-      k_mx_update_poly<3><<<grid_of(l, S, k_mx_update_poly<3>, l.ctas_up), NT, 0, l.stream>>>(
-          S, Y, ctl, part, ra);
-    else
-      k_mx_update_poly<0><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part, ra);
-    count_launches(1);
-  }
-  if (l.fold) return;
+  mx_update_kernels<false>(l, S, Y, ctl, part, ra);
   k_red_mx_update<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, 2.0, no_stop);
   count_launches(1);
 }
 void launch_mx_zinit(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                      double *part) {
   if (!l.mx_poly) return;
+  if (l.fold) {
+    if (l.variant == 3)
+      k_mx_zinit<true, true><<<grid_of(l, S, k_mx_zinit<true, true>, 0), NT, 0, l.stream>>>(
+          S, Y, ctl, part);
+    else
+      k_mx_zinit<false, true><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part);
+    count_launches(1);
+    return;
+  }
   if (l.variant == 3)
-    k_mx_zinit<true><<<grid_of(l, S, k_mx_zinit<true>, 0), NT, 0, l.stream>>>(S, Y, ctl, part,
-                                                                             l.fold);
+    k_mx_zinit<true, false><<<grid_of(l, S, k_mx_zinit<true, false>, 0), NT, 0, l.stream>>>(
+        S, Y, ctl, part);
   else
-    k_mx_zinit<false><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part, l.fold);
-  count_launches(1);
-  if (l.fold) return;
+    k_mx_zinit<false, false><<<l.grid_up32, NT, 0, l.stream>>>(S, Y, ctl, part);
   k_red_mx_zinit<<<reduce_grid(S), NT, 0, l.stream>>>(S, Y, ctl, part);
-  count_launches(1);
+  count_launches(2);
 }
 void launch_mx_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl, Glob *glob,
                     double *part) {
@@ -568,13 +591,13 @@ void launch_mx_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl
 
 int occupancy_blocks_per_sm_mixed_update() {
   int b = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_mx_update_poly<0>, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_mx_update_poly<0, false>, NT, 0);
   return b > 0 ? b : 1;
 }
 
 int occupancy_blocks_per_sm_mixed() {
   int a = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_mx_matvec<true, 0>, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_mx_matvec<true, 0, false>, NT, 0);
   return a > 0 ? a : 1;
 }
 

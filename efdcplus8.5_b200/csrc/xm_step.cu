@@ -602,7 +602,7 @@ __global__ void k_outer_reset(Glob *glob) { glob->nidone = 0; }
 // CCCI = 1./CCC is recomputed where needed instead of stored.
 
 // :54-88 initial residual, z0 = CCCI*r, RPCG.
-template <bool MA>
+template <bool MA, bool FOLD>
 __global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double *P, Ctl *ctl,
                                                double *part, RedArgs ra) {
   struct A {
@@ -622,7 +622,7 @@ __global__ void __launch_bounds__(NT) k_cg_init(DevStatic S, DevSystem Y, double
           v[0] = r.x * z.x + r.y * z.y + r.z * z.z + r.w * z.w;
         }
       },
-      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+      fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0) cg_init_epi(ctl[m], ra.glob, sum[0]);
       }));
 }
@@ -636,9 +636,9 @@ __global__ void __launch_bounds__(NT) k_red_cg_init(DevStatic S, Ctl *ctl, Glob 
 }
 
 // :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA).
-template <bool MA>
-__global__ void __launch_bounds__(NT, 2) k_cg_matvec(DevStatic S, DevSystem Y, Ctl *ctl,
-                                                    double *part, int fold) {
+template <bool MA, bool FOLD>
+__global__ void __launch_bounds__(NT, MA ? 2 : 3) k_cg_matvec(DevStatic S, DevSystem Y, Ctl *ctl,
+                                                    double *part) {
   struct A {
     bool skip, asym;
     double beta;
@@ -656,7 +656,7 @@ __global__ void __launch_bounds__(NT, 2) k_cg_matvec(DevStatic S, DevSystem Y, C
         v[0] = matvec_row_z(g, valid, Y.z, Y.ccc, a.pold, a.pnew, Y.ccs, Y.ccw, Y.cce, Y.ccn,
                             Y.ap, a.beta, a.asym);
       },
-      fold_with(fold ? ctl : nullptr, [&](int m, const double *sum) {
+      fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0) cg_matvec_epi(ctl[m], sum[0]);
       }));
 }
@@ -670,6 +670,7 @@ __global__ void __launch_bounds__(NT) k_red_cg_matvec(DevStatic S, Ctl *ctl, con
 
 // :127-149 (P, RCG update, RPCGN, RSQ, BETA) and the stop test :165.  With
 // no_stop the iteration continues past RSQM and ITERM (kernel timing only).
+template <bool FOLD>
 __global__ void __launch_bounds__(NT, 5) k_cg_update(DevStatic S, DevSystem Y, double *P,
                                                     Ctl *ctl, double *part, RedArgs ra) {
   struct A {
@@ -686,7 +687,7 @@ __global__ void __launch_bounds__(NT, 5) k_cg_update(DevStatic S, DevSystem Y, d
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         update_row<double>(g, valid, P, a.pnew, Y.r, Y.ap, Y.ccc, a.alpha, v[0], v[1], Y.z);
       },
-      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+      fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0) cg_update_epi(ctl[m], ra.glob, S.sc[m], sum[0], sum[1], ra.no_stop);
       }));
 }
@@ -911,7 +912,7 @@ __device__ __forceinline__ void mx_resid_epi(Ctl &k, const StepScalars &c, const
   }
 }
 
-template <bool MA, bool EAGER>
+template <bool MA, bool EAGER, bool FOLD>
 __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, SysView V, DevSystem Y,
                                                 const double *P, Ctl *ctl, double *part,
                                                 RedArgs ra) {
@@ -938,7 +939,7 @@ __global__ void __launch_bounds__(NT) k_mx_resid(DevStatic S, SysView V, DevSyst
                  double(r32.z) * double(r32.z) + double(r32.w) * double(r32.w);
         }
       },
-      fold_with(ra.fold ? ctl : nullptr, [&](int m, const double *sum) {
+      fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0) mx_resid_epi(ctl[m], S.sc[m], ra, sum[0], sum[1]);
       }));
 }
@@ -1511,19 +1512,26 @@ static int quad_grid(const Launch &l, const DevStatic &S, K kernel) {
   return std::max(1, std::min(S.nquad, l.nsm * per_sm));
 }
 
+template <bool F>
+static void cg_init_kernel(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
+                           Ctl *ctl, double *part, const RedArgs &ra) {
+  if (l.may_asym)
+    k_cg_init<true, F><<<quad_grid(l, S, k_cg_init<true, F>), NT, 0, l.stream>>>(S, Y, P, ctl,
+                                                                                part, ra);
+  else
+    k_cg_init<false, F><<<quad_grid(l, S, k_cg_init<false, F>), NT, 0, l.stream>>>(S, Y, P, ctl,
+                                                                                  part, ra);
+  count_launches(1);
+}
 void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                     Glob *glob, double *part) {
   RedArgs ra{};
   ra.glob = glob;
-  ra.fold = l.fold;
-  if (l.may_asym)
-    k_cg_init<true><<<quad_grid(l, S, k_cg_init<true>), NT, 0, l.stream>>>(S, Y, P, ctl, part,
-                                                                          ra);
-  else
-    k_cg_init<false><<<quad_grid(l, S, k_cg_init<false>), NT, 0, l.stream>>>(S, Y, P, ctl, part,
-                                                                            ra);
-  count_launches(1);
-  if (l.fold) return;
+  if (l.fold) {
+    cg_init_kernel<true>(l, S, Y, P, ctl, part, ra);
+    return;
+  }
+  cg_init_kernel<false>(l, S, Y, P, ctl, part, ra);
   launch_chan_res64(l, S, Y, P, ctl, part);
   k_red_cg_init<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part);
   count_launches(1);
@@ -1557,16 +1565,24 @@ void launch_cg_small(const Launch &l, const DevStatic &S, const DevSystem &Y, do
     k_cg_small<false><<<nmember, SMALL_NT, smem, l.stream>>>(S, Y, P, ctl, glob, part);
   count_launches(1);
 }
+template <bool F>
+static void cg_matvec_kernel(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
+                             double *part) {
+  if (l.may_asym)
+    k_cg_matvec<true, F><<<quad_grid(l, S, k_cg_matvec<true, F>), NT, 0, l.stream>>>(S, Y, ctl,
+                                                                                    part);
+  else
+    k_cg_matvec<false, F><<<quad_grid(l, S, k_cg_matvec<false, F>), NT, 0, l.stream>>>(S, Y, ctl,
+                                                                                      part);
+  count_launches(1);
+}
 void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       double *part) {
-  if (l.may_asym)
-    k_cg_matvec<true><<<quad_grid(l, S, k_cg_matvec<true>), NT, 0, l.stream>>>(S, Y, ctl, part,
-                                                                              l.fold);
-  else
-    k_cg_matvec<false><<<quad_grid(l, S, k_cg_matvec<false>), NT, 0, l.stream>>>(S, Y, ctl,
-                                                                               part, l.fold);
-  count_launches(1);
-  if (l.fold) return;
+  if (l.fold) {
+    cg_matvec_kernel<true>(l, S, Y, ctl, part);
+    return;
+  }
+  cg_matvec_kernel<false>(l, S, Y, ctl, part);
   launch_chan_mv64(l, S, Y, ctl, part);
   k_red_cg_matvec<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part);
   count_launches(1);
@@ -1576,17 +1592,41 @@ void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, d
   RedArgs ra{};
   ra.glob = glob;
   ra.no_stop = no_stop;
-  ra.fold = l.fold;
-  k_cg_update<<<quad_grid(l, S, k_cg_update), NT, 0, l.stream>>>(S, Y, P, ctl, part, ra);
-  count_launches(1);
-  if (l.fold) return;
+  if (l.fold) {
+    k_cg_update<true><<<quad_grid(l, S, k_cg_update<true>), NT, 0, l.stream>>>(S, Y, P, ctl, part,
+                                                                              ra);
+    count_launches(1);
+    return;
+  }
+  k_cg_update<false><<<quad_grid(l, S, k_cg_update<false>), NT, 0, l.stream>>>(S, Y, P, ctl,
+                                                                              part, ra);
   k_red_cg_update<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, no_stop);
-  count_launches(1);
+  count_launches(2);
 }
 void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                     Glob *glob, double *part) {
   launch_cg_matvec(l, S, Y, ctl, part);
   launch_cg_update(l, S, Y, P, ctl, glob, part, 0);
+}
+template <bool F>
+static void mx_resid_kernel(const Launch &l, const DevStatic &S, const SysView &V,
+                            const DevSystem &Y, const double *P, Ctl *ctl, double *part,
+                            const RedArgs &ra) {
+  if (l.variant == 3) {
+    if (l.may_asym)
+      k_mx_resid<true, true, F><<<quad_grid(l, S, k_mx_resid<true, true, F>), NT, 0,
+                                  l.stream>>>(S, V, Y, P, ctl, part, ra);
+    else
+      k_mx_resid<false, true, F><<<quad_grid(l, S, k_mx_resid<false, true, F>), NT, 0,
+                                   l.stream>>>(S, V, Y, P, ctl, part, ra);
+  } else if (l.may_asym) {
+    k_mx_resid<true, false, F><<<quad_grid(l, S, k_mx_resid<true, false, F>), NT, 0,
+                                 l.stream>>>(S, V, Y, P, ctl, part, ra);
+  } else {
+    k_mx_resid<false, false, F><<<quad_grid(l, S, k_mx_resid<false, false, F>), NT, 0,
+                                  l.stream>>>(S, V, Y, P, ctl, part, ra);
+  }
+  count_launches(1);
 }
 void launch_mx_resid(const Launch &l, const DevStatic &S, const SysView &V, const DevSystem &Y,
                      const double *P, Ctl *ctl, Glob *glob, double *part, double rsqm_fac,
@@ -1598,23 +1638,10 @@ void launch_mx_resid(const Launch &l, const DevStatic &S, const SysView &V, cons
   ra.margin = l.inner_margin;
   ra.no_stop = no_stop;
   ra.unscaled = V.unscaled;
-  ra.fold = l.fold;
-  if (l.variant == 3) {
-    if (l.may_asym)
-      k_mx_resid<true, true><<<quad_grid(l, S, k_mx_resid<true, true>), NT, 0, l.stream>>>(
-          S, V, Y, P, ctl, part, ra);
-    else
-      k_mx_resid<false, true><<<quad_grid(l, S, k_mx_resid<false, true>), NT, 0, l.stream>>>(
-          S, V, Y, P, ctl, part, ra);
-  } else if (l.may_asym) {
-    k_mx_resid<true, false><<<quad_grid(l, S, k_mx_resid<true, false>), NT, 0, l.stream>>>(
-        S, V, Y, P, ctl, part, ra);
+  if (l.fold) {
+    mx_resid_kernel<true>(l, S, V, Y, P, ctl, part, ra);
   } else {
-    k_mx_resid<false, false><<<quad_grid(l, S, k_mx_resid<false, false>), NT, 0, l.stream>>>(
-        S, V, Y, P, ctl, part, ra);
-  }
-  count_launches(1);
-  if (!l.fold) {
+    mx_resid_kernel<false>(l, S, V, Y, P, ctl, part, ra);
     launch_chan_resmx(l, S, V, Y, P, ctl, part);
     k_red_mx_resid<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part, ra);
     count_launches(1);
@@ -1854,9 +1881,9 @@ int occupancy_blocks_per_sm() {  // k_assemble holds more values: its own grid (
 int occupancy_blocks_per_sm_cg() {
   int a = 0, b = 0, c = 0, d = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_mx_apply, NT, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cg_update, NT, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_cg_init<true>, NT, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_mx_resid<true, false>, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cg_update<false>, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_cg_init<true, false>, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_mx_resid<true, false, false>, NT, 0);
   const int m = std::min(std::min(a, b), std::min(c, d));
   return m > 0 ? m : 1;
 }
