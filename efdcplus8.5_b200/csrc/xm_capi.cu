@@ -281,6 +281,7 @@ struct efdc_xm_ctx {
                                 // 0 never, 1 up to FOLD_MEMBERS members, 2 always
   int nchunk = 8;               // member chunks of a pipelined efdc_xm_step_batch
   int small_slots = 0;          // the largest member window (its ghost tile and tiles)
+  int small_units = 0;          // the most 4-tile units of a member
   float poly_threshold = 10.f;  // MIXED: polynomial preconditioner above this Jacobi count
   xm::Launch L() const {
     xm::Launch l{grid,      grid_cg, grid_cg32, grid_up32,
@@ -663,7 +664,8 @@ int solve_fp64(efdc_xm_ctx *c, double *P) {
   const xm::Launch l = c->L();
   xm::launch_solve_reset(l, c->ctl, c->glob, c->act, c->M);
   if (small_solve(c)) {  // the whole CG of each member in one CTA (k_cg_small)
-    xm::launch_cg_small(l, c->S, c->Y, P, c->ctl, c->glob, c->part, c->small_slots, c->M);
+    xm::launch_cg_small(l, c->S, c->Y, P, c->ctl, c->glob, c->part, c->small_slots,
+                        c->small_units, c->M);
     CK(cudaGetLastError());
     int rc = read_ctl(c);
     if (rc) return rc;
@@ -1201,6 +1203,7 @@ efdc_xm_ctx *efdc_xm_create_batch(const efdc_xm_grid *grids, int32_t nmembers, i
   c->hp1_h.assign(M, 1.0);
   c->chan_start.assign(M + 1, 0);
   c->qstart_h = qstart;
+  for (int m = 0; m < M; ++m) c->small_units = std::max(c->small_units, qstart[m + 1] - qstart[m]);
   c->has_layers.assign(M, 0);
   cudaMemcpy(quads_d, quads.data(), quads.size() * sizeof(int4), cudaMemcpyHostToDevice);
   cudaMemcpy(qstart_d, qstart.data(), (M + 1) * sizeof(int), cudaMemcpyHostToDevice);
@@ -1922,7 +1925,8 @@ cudaError_t capture_solve(efdc_xm_ctx *c, const StepPlan &pl, int d, StepGraph &
   double *P = c->X.p;
   if (!pl.mixed && pl.small) {  // one CTA per member, its loop inside (k_cg_small)
     xm::launch_solve_reset(l, c->ctl, c->glob, c->act, M);
-    xm::launch_cg_small(l, c->S, c->Y, P, c->ctl, c->glob, c->part, c->small_slots, M);
+    xm::launch_cg_small(l, c->S, c->Y, P, c->ctl, c->glob, c->part, c->small_slots,
+                        c->small_units, M);
     take_count(mark, mine);
     return cudaGetLastError();
   }
@@ -2181,7 +2185,7 @@ namespace {
 // is its thread count, NOPTIMAL = MIN(NTHREADS, 8, MAX(LA/100, 1))
 // (calpuv2c.f90:61-62); here the knobs are the MIXED inner iteration's kernel
 // variant and CTA caps, the CG iterations per loop body, the Jacobi /
-// polynomial threshold and the inner target margin.  The tuner times the
+// polynomial threshold and the inner target margin and tolerance.  The tuner times the
 // context's own solve -- the solve part of a device-driven step, captured as
 // a graph of the same kernels -- on the system the last step assembled, from
 // the P it left (restored before every run), and walks the knobs one at a
@@ -2190,6 +2194,7 @@ namespace {
 
 constexpr int TUNE_REPS = 5;          // timed solves per candidate (the median counts)
 constexpr double TUNE_GAIN = 0.98;    // a candidate must be 2 % faster to replace the incumbent
+constexpr double TUNE_MIN_MS = 20.0;  // timed solve time per candidate sought (see tune_time)
 
 void schedule_of(const efdc_xm_ctx *c, efdc_xm_schedule *s) {
   s->kernel_variant = c->kvariant;
@@ -2198,12 +2203,13 @@ void schedule_of(const efdc_xm_ctx *c, efdc_xm_schedule *s) {
   s->graph_iters = c->graph_iters;
   s->poly_threshold = int32_t(c->poly_threshold);
   s->inner_margin = c->inner_margin_log10;
+  s->inner_tol = c->inner_tol_x10;
 }
 
 void apply_schedule(efdc_xm_ctx *c, const efdc_xm_schedule &s) {
   if (s.kernel_variant != c->kvariant || s.ctas_matvec != c->ctas_mv ||
       s.ctas_update != c->ctas_up || s.inner_margin != c->inner_margin_log10 ||
-      s.graph_iters != c->graph_iters)
+      s.graph_iters != c->graph_iters || s.inner_tol != c->inner_tol_x10)
     drop_graphs(c);
   c->kvariant = s.kernel_variant;
   c->ctas_mv = s.ctas_matvec;
@@ -2211,13 +2217,15 @@ void apply_schedule(efdc_xm_ctx *c, const efdc_xm_schedule &s) {
   c->graph_iters = s.graph_iters;
   c->poly_threshold = float(s.poly_threshold);
   c->inner_margin_log10 = s.inner_margin;
+  c->inner_tol_x10 = s.inner_tol;
 }
 
 bool schedule_valid(const efdc_xm_schedule &s) {
   return s.kernel_variant >= 0 && s.kernel_variant <= 3 && s.ctas_matvec >= 0 &&
          s.ctas_matvec <= 32 && s.ctas_update >= 0 && s.ctas_update <= 32 &&
          s.graph_iters >= 1 && s.graph_iters <= 32 && s.poly_threshold >= 0 &&
-         s.poly_threshold <= 100000 && s.inner_margin >= 0 && s.inner_margin <= 6;
+         s.poly_threshold <= 100000 && s.inner_margin >= 0 && s.inner_margin <= 6 &&
+         s.inner_tol >= 40 && s.inner_tol <= 75;
 }
 
 // The workload key of a table line: the precision, the buckets (floor log2)
@@ -2240,13 +2248,13 @@ std::string tune_key(const efdc_xm_ctx *c, int precision) {
   return buf;
 }
 
-// "key | variant=.. ctas_mv=.. ctas_up=.. iters=.. poly=.. margin=.. | ms=.."
+// "key | variant=.. ctas_mv=.. ctas_up=.. iters=.. poly=.. margin=.. tol=.. | ms=.."
 std::string table_line(const std::string &key, const efdc_xm_schedule &s, double ms) {
   char buf[400];
   snprintf(buf, sizeof(buf),
-           "%s | variant=%d ctas_mv=%d ctas_up=%d iters=%d poly=%d margin=%d | ms=%.4f",
+           "%s | variant=%d ctas_mv=%d ctas_up=%d iters=%d poly=%d margin=%d tol=%d | ms=%.4f",
            key.c_str(), s.kernel_variant, s.ctas_matvec, s.ctas_update, s.graph_iters,
-           s.poly_threshold, s.inner_margin, ms);
+           s.poly_threshold, s.inner_margin, s.inner_tol, ms);
   return buf;
 }
 
@@ -2261,10 +2269,12 @@ bool table_lookup(const char *path, const std::string &key, efdc_xm_schedule *ou
     const size_t bar = l.find(" | ");
     if (bar == std::string::npos || l.compare(0, bar, key) != 0 || bar != key.size()) continue;
     efdc_xm_schedule s{};
-    if (sscanf(l.c_str() + bar + 3, "variant=%d ctas_mv=%d ctas_up=%d iters=%d poly=%d margin=%d",
-               &s.kernel_variant, &s.ctas_matvec, &s.ctas_update, &s.graph_iters,
-               &s.poly_threshold, &s.inner_margin) == 6 &&
-        schedule_valid(s)) {
+    s.inner_tol = 60;  // lines written before the tolerance was a knob
+    const int n = sscanf(l.c_str() + bar + 3,
+                         "variant=%d ctas_mv=%d ctas_up=%d iters=%d poly=%d margin=%d tol=%d",
+                         &s.kernel_variant, &s.ctas_matvec, &s.ctas_update, &s.graph_iters,
+                         &s.poly_threshold, &s.inner_margin, &s.inner_tol);
+    if (n >= 6 && schedule_valid(s)) {
       *out = s;
       found = true;
     }
@@ -2334,7 +2344,8 @@ int tune_time(efdc_xm_ctx *c, bool mixed, double fac, int reps, double *ms) {
   CK(cudaEventCreate(&e1));
   const size_t pb = size_t(c->nslot) * sizeof(double);
   std::vector<double> t;
-  for (int r = 0; r <= reps; ++r) {  // run 0 warms up
+  int n = reps;
+  for (int r = 0; r <= n; ++r) {  // run 0 warms up
     CK(cudaMemcpyAsync(c->X.p, c->ptmp, pb, cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaEventRecord(e0, c->stream));
     CK(cudaGraphLaunch(ex, c->stream));
@@ -2343,6 +2354,9 @@ int tune_time(efdc_xm_ctx *c, bool mixed, double fac, int reps, double *ms) {
     float f = 0.f;
     CK(cudaEventElapsedTime(&f, e0, e1));
     if (r > 0) t.push_back(f);
+    // short solves take more runs (about TUNE_MIN_MS of them, up to 4x reps):
+    // their run-to-run spread is a larger share of their time
+    if (r == 0 && f > 0.f) n = std::min(4 * reps, std::max(reps, int(TUNE_MIN_MS / f) + 1));
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -3919,6 +3933,7 @@ int32_t efdc_xm_autotune(efdc_xm_ctx *c, int32_t precision, const char *table, i
     }
     if ((rc = knob(&efdc_xm_schedule::poly_threshold, {0, 10, 40, 100000}))) return rc;
     if ((rc = knob(&efdc_xm_schedule::inner_margin, {0, 1, 2}))) return rc;
+    if ((rc = knob(&efdc_xm_schedule::inner_tol, {40, 50, 60, 70}))) return rc;
   }
   if ((rc = knob(&efdc_xm_schedule::graph_iters, {2, 4, 8}))) return rc;
   // P as the last step left it

@@ -65,7 +65,8 @@ void launch_put(cudaStream_t st, const int *idx, const double *val, int n, doubl
 constexpr int SMALL_SMEM_MAX = 200 * 1024;
 bool cg_small_fits(int slots);
 void launch_cg_small(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
-                     Ctl *ctl, Glob *glob, double *part, int max_slots, int nmember);
+                     Ctl *ctl, Glob *glob, double *part, int max_slots, int max_units,
+                     int nmember);
 void launch_put_int(cudaStream_t st, const int *idx, const int *val, int n, int *dst);
 // sub-grid channels (xm_chan.cu); each does nothing unless l.chan
 void launch_chan_entry(const Launch &l, const DevStatic &S, const DevState &X, const int *act);

@@ -714,6 +714,7 @@ __global__ void __launch_bounds__(NT) k_red_cg_update(DevStatic S, Ctl *ctl, Glo
 // the member's window of slots, [its ghost tile, its last tile].
 constexpr int SMALL_UNITS = 2;
 constexpr int SMALL_NT = SMALL_UNITS * NT;
+constexpr int SMALL_CACHED = 2;  // passes whose geometry a thread keeps in registers
 
 // reduce_partials of a 256-thread CTA, by a CTA of SMALL_NT threads (the
 // threads past the first 256 add nothing, as block_sum's last stage reads 8
@@ -734,7 +735,7 @@ __device__ __forceinline__ double reduce_partials_256(const double *part, int nb
   return block_sum(s, sh);
 }
 
-template <bool MA>
+template <bool MA, int NP>
 __global__ void __launch_bounds__(SMALL_NT) k_cg_small(DevStatic S, DevSystem Y, double *P,
                                                       Ctl *ctl, Glob *glob, double *part) {
   extern __shared__ double smv[];
@@ -777,27 +778,44 @@ __global__ void __launch_bounds__(SMALL_NT) k_cg_small(DevStatic S, DevSystem Y,
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool asym = unsym<MA>(ctl[m]);
 
+  // where a thread's rows are in pass p (units u0 + qi, u0 = q0 + p*SMALL_UNITS)
+  struct Pass {
+    RowGeo g;
+    bool have, valid;
+  };
+  auto pass_of = [&](int u0) {
+    const int qd = u0 + qi;
+    const bool have = qd < q1;
+    const int4 cur = have ? S.quads[qd] : int4{m, ghost, 0, 0};
+    const bool valid = have && sub < cur.z;
+    const int ti = valid ? cur.y + sub : ghost;
+    return Pass{row_geo_nb(__ldg(&S.tnbr[ti]), ti, q), have, valid};
+  };
+  // NP > 0: the member has at most NP passes, whose geometry is formed once
+  // here and kept in registers (the loop then has no dependent loads of the
+  // unit table and the tile neighbours)
+  Pass pc[NP > 0 ? NP : 1];
+  if constexpr (NP > 0) {
+#pragma unroll
+    for (int p = 0; p < NP; ++p) pc[p] = pass_of(q0 + p * SMALL_UNITS);
+  }
+
   // one sweep of a row body over the member's units, as quad_sweep makes it
   auto sweep = [&](auto body, auto ns_tag) {
     constexpr int NS = decltype(ns_tag)::value;
-    for (int u0 = q0; u0 < q1; u0 += SMALL_UNITS) {
+    auto unit = [&](int u0, const Pass &ps) {
       const int qd = u0 + qi;
-      const bool have = qd < q1;
-      const int4 cur = have ? S.quads[qd] : int4{m, ghost, 0, 0};
-      const bool valid = have && sub < cur.z;
-      const int ti = valid ? cur.y + sub : ghost;
-      const RowGeo g = row_geo_nb(__ldg(&S.tnbr[ti]), ti, q);
       double v[NS];
 #pragma unroll
       for (int s = 0; s < NS; ++s) v[s] = 0.0;
-      body(g, valid, v);
+      body(ps.g, ps.valid, v);
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
         const double x = warp_sum(v[s]);
         if (lane == 0) wp[s][warp] = x;
       }
       __syncthreads();
-      if (tq == 0 && have) {
+      if (tq == 0 && ps.have) {
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
           double a = 0.0;
@@ -807,6 +825,13 @@ __global__ void __launch_bounds__(SMALL_NT) k_cg_small(DevStatic S, DevSystem Y,
         }
       }
       __syncthreads();
+    };
+    if constexpr (NP > 0) {
+#pragma unroll
+      for (int p = 0; p < NP; ++p)
+        if (q0 + p * SMALL_UNITS < q1) unit(q0 + p * SMALL_UNITS, pc[p]);  // CTA-uniform
+    } else {
+      for (int u0 = q0; u0 < q1; u0 += SMALL_UNITS) unit(u0, pass_of(u0));
     }
   };
   using One = std::integral_constant<int, 1>;
@@ -1543,26 +1568,34 @@ bool cg_small_fits(int slots) {
          slots / (TILES_PER_CTA * TILE) <= SMALL_MAX_UNITS;
 }
 void launch_cg_small(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
-                     Ctl *ctl, Glob *glob, double *part, int max_slots, int nmember) {
+                     Ctl *ctl, Glob *glob, double *part, int max_slots, int max_units,
+                     int nmember) {
   const size_t smem = size_t(max_slots) * 6 * sizeof(double);
   static std::mutex mu;
-  static bool set[2] = {false, false};
+  static bool set = false;
   {
     std::lock_guard<std::mutex> lock(mu);
-    if (!set[l.may_asym ? 1 : 0]) {
-      if (l.may_asym)
-        cudaFuncSetAttribute(k_cg_small<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             SMALL_SMEM_MAX);
-      else
-        cudaFuncSetAttribute(k_cg_small<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             SMALL_SMEM_MAX);
-      set[l.may_asym ? 1 : 0] = true;
+    if (!set) {
+      for (const void *k : {reinterpret_cast<const void *>(k_cg_small<true, 0>),
+                            reinterpret_cast<const void *>(k_cg_small<false, 0>),
+                            reinterpret_cast<const void *>(k_cg_small<true, SMALL_CACHED>),
+                            reinterpret_cast<const void *>(k_cg_small<false, SMALL_CACHED>)})
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMALL_SMEM_MAX);
+      set = true;
     }
   }
-  if (l.may_asym)
-    k_cg_small<true><<<nmember, SMALL_NT, smem, l.stream>>>(S, Y, P, ctl, glob, part);
+  // members of at most SMALL_CACHED passes keep their geometry in registers
+  const bool cached = max_units <= SMALL_CACHED * SMALL_UNITS;
+  if (l.may_asym && cached)
+    k_cg_small<true, SMALL_CACHED><<<nmember, SMALL_NT, smem, l.stream>>>(S, Y, P, ctl, glob,
+                                                                         part);
+  else if (l.may_asym)
+    k_cg_small<true, 0><<<nmember, SMALL_NT, smem, l.stream>>>(S, Y, P, ctl, glob, part);
+  else if (cached)
+    k_cg_small<false, SMALL_CACHED><<<nmember, SMALL_NT, smem, l.stream>>>(S, Y, P, ctl, glob,
+                                                                          part);
   else
-    k_cg_small<false><<<nmember, SMALL_NT, smem, l.stream>>>(S, Y, P, ctl, glob, part);
+    k_cg_small<false, 0><<<nmember, SMALL_NT, smem, l.stream>>>(S, Y, P, ctl, glob, part);
   count_launches(1);
 }
 template <bool F>

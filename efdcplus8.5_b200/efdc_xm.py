@@ -81,7 +81,8 @@ class Fields(C.Structure):
 class Schedule(C.Structure):
     _fields_ = [("kernel_variant", C.c_int32), ("ctas_matvec", C.c_int32),
                 ("ctas_update", C.c_int32), ("graph_iters", C.c_int32),
-                ("poly_threshold", C.c_int32), ("inner_margin", C.c_int32)]
+                ("poly_threshold", C.c_int32), ("inner_margin", C.c_int32),
+                ("inner_tol", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define EFDC_XM_ABI_VERSION 6
+#define EFDC_XM_ABI_VERSION 7
 
 /* Status codes.  The reference STOPs where these are returned. */
 enum efdc_xm_status {
@@ -513,6 +513,7 @@ typedef struct efdc_xm_schedule {
   int32_t graph_iters;     /* EFDC_XM_OPT_GRAPH_ITERS */
   int32_t poly_threshold;  /* EFDC_XM_OPT_POLY_THRESHOLD */
   int32_t inner_margin;    /* EFDC_XM_OPT_INNER_MARGIN */
+  int32_t inner_tol;       /* EFDC_XM_OPT_INNER_TOL */
 } efdc_xm_schedule;
 enum { EFDC_XM_TUNE_MEASURE = 1 };
 int32_t efdc_xm_autotune(efdc_xm_ctx *ctx, int32_t precision, const char *table, int32_t flags,
