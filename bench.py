@@ -94,6 +94,9 @@ def parse():
                     help="drive the CG, refinement and wet/dry loops from the host "
                          "(EFDC_XM_OPT_DEVICE_LOOPS 0): the same kernels, each launch visible to "
                          "a kernel profiler (kernels inside graphs with conditional nodes are not)")
+    ap.add_argument("--profile-prec", choices=("mixed", "fp64", "both"), default="mixed",
+                    help="which timed steps of the headline workload are the profiler range "
+                         "(ncu --profile-from-start off)")
     ap.add_argument("--variant", type=int, default=-1,
                     help="MIXED inner-iteration kernel variant (EFDC_XM_OPT_KERNEL_VARIANT); "
                          "-1: the schedule efdc_xm_autotune measures for the workload")
@@ -621,8 +624,11 @@ def ours(args):
         w0 = X.host_waits()
         times, iters, outer = [], np.zeros(M, np.int64), 0
         per_step_iters = []
-        # the timed MIXED steps are the profiler range (ncu --profile-from-start off)
-        if prec == X.PREC_MIXED:
+        # the timed steps are the profiler range (ncu --profile-from-start off): the
+        # MIXED ones by default, see --profile-prec
+        prof = args.profile_prec == "both" or \
+            (args.profile_prec == "mixed") == (prec == X.PREC_MIXED)
+        if prof:
             torch.cuda.profiler.start()
         for _ in range(steps):
             n += 1
@@ -640,7 +646,7 @@ def ours(args):
             outer += sum(st.outer_refinements for st in sts)
             times.append(tm.ms)
         torch.cuda.synchronize()
-        if prec == X.PREC_MIXED:
+        if prof:
             torch.cuda.profiler.stop()
         barrier()
         launches = lib.efdc_xm_kernel_launches() - l0
