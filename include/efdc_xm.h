@@ -634,14 +634,14 @@ int32_t efdc_xm_time_kernels(efdc_xm_ctx *ctx, int32_t precision, int32_t reps,
  *     the library holds it until the process exits.  Larger LA is rejected
  *     with EFDC_XM_BAD_ARGUMENT and a message (efdc_xm_last_error);
  *   - the first call on a device looks up that array's device address (with
- *     that device current) and keeps it, so make the first call on each
- *     device before any stream capture;
+ *     that device current) and keeps it;
  *   - all calls share the array: calls that overlap on the GPU (other
  *     streams, other host threads) race; the call returns after its work on
  *     `stream` (a cudaStream_t, NULL = legacy default stream) finished;
  *   - every call reads its stop test back to the host: it copies the control
  *     block to host memory and synchronizes `stream` after every 8
- *     iterations. */
+ *     iterations, so it must not be called while a stream capture is active
+ *     (on `stream` or, in global capture mode, anywhere in the process). */
 #define EFDC_XM_NOALLOC_MAX_CELLS 524288
 int32_t efdc_xm_congrad_noalloc(int32_t la, const int32_t *lnc, const int32_t *lsc,
                                 const int32_t *lec, const int32_t *lwc, const double *ccc,
