@@ -59,6 +59,12 @@ import scenario as S  # noqa: E402
 
 METRIC = "external-mode cell-iter/s on 1 B200: mixed/batched vs plain FP64 at 1e-6 m err"
 UNIT = "cell-iter/s"
+# Algorithmic bytes per water cell of the MIXED inner iteration's two kernels
+# (FP32, 4 B per value): the matvec reads z (r for Jacobi members), p_old, AS,
+# AW and x and writes p_new, Ap and x (the previous iteration's x += alpha*p
+# rides on it); the update reads r, Ap and writes r (Jacobi), plus AS, AW in
+# and z out for a polynomial member.
+MV_B, UP_B, UP_POLY_B = 32.0, 12.0, 12.0
 
 
 def parse():
@@ -720,8 +726,8 @@ def ours(args):
         bs.set_option(X.OPT_KERNEL_VARIANT, v)
         kv = bs.time_kernels(X.PREC_MIXED, reps=20)
         variants[v] = {"ms_matvec": kv.ms_matvec, "ms_update": kv.ms_update,
-                       "frac_matvec": 24.0 * kv.ncells / (kv.ms_matvec * 1e-3) / 1e9 / peak,
-                       "frac_update": (24.0 * kv.ncells + 12.0 * kv.ncells_poly) /
+                       "frac_matvec": MV_B * kv.ncells / (kv.ms_matvec * 1e-3) / 1e9 / peak,
+                       "frac_update": (UP_B * kv.ncells + UP_POLY_B * kv.ncells_poly) /
                                       (kv.ms_update * 1e-3) / 1e9 / peak}
     bs.set_option(X.OPT_KERNEL_VARIANT, run_variant)
     kt = bs.time_kernels(X.PREC_MIXED, reps=20)
@@ -816,11 +822,9 @@ def ours(args):
     # The two FP32 kernels of the inner iteration launch once each per
     # iteration, so the one with the longer launch has the larger share of the
     # step (profiles/launch_list_ensemble256.md has the shares of every kernel).
-    # Algorithmic bytes per water cell: the matvec of the Jacobi-scaled system
-    # reads r (or z), p_old, AS, AW and writes p_new, Ap (6 x 4 B); the update
-    # reads x, p, r, Ap and writes x, r (24 B) for a Jacobi member, plus AS, AW
-    # in and z out (36 B) for a polynomial one; the FP64 drop-in's matvec reads
-    # z, CCC, p_old, CCS, CCW and writes p_new, Ap (7 x 8 B).
+    # Algorithmic bytes per water cell (MV_B, UP_B, UP_POLY_B at the top of the
+    # file); the FP64 drop-in's matvec reads z, CCC, p_old, CCS, CCW and
+    # writes p_new, Ap (7 x 8 B).
     tj = {}
     tf = REPO / "profiles" / "traffic.json"
     if tf.exists():
@@ -840,10 +844,10 @@ def ours(args):
                 "cells_per_launch": kt.ncells, "slots_per_launch": kt.nslots}
 
     up_name = "k_mx_update_poly" if kt.ncells_poly > 0 else "k_mx_update_jac"
-    e_mv = kentry("k_mx_matvec", "FP32 p-update + Ahat*p + p.Ap, all members, + member reduce",
-                  kt.ms_matvec, 24.0 * kt.ncells)
-    e_up = kentry(up_name, "FP32 x, r updates, z = (2I - Ahat) r, r.z, r.r, all members, "
-                  "+ member reduce", kt.ms_update, 24.0 * kt.ncells + 12.0 * kt.ncells_poly)
+    e_mv = kentry("k_mx_matvec", "FP32 p-update + Ahat*p + p.Ap + the previous x += alpha*p, "
+                  "all members, + member reduce", kt.ms_matvec, MV_B * kt.ncells)
+    e_up = kentry(up_name, "FP32 r update, z = (2I - Ahat) r, r.z, r.r, all members, "
+                  "+ member reduce", kt.ms_update, UP_B * kt.ncells + UP_POLY_B * kt.ncells_poly)
     e_up["cells_polynomial"] = kt.ncells_poly
     first, second = (e_up, e_mv) if kt.ms_update >= kt.ms_matvec else (e_mv, e_up)
     roof = dict(first)
@@ -969,9 +973,9 @@ def ours(args):
                   "fp64_ms_per_step": 1000 * t64b / args.basin_steps,
                   "eta_err_per_step_mixed_vs_fp64_m": eta_b,
                   "k_mx_matvec_ms": kb.ms_matvec,
-                  "k_mx_matvec_frac": 24.0 * kb.ncells / (kb.ms_matvec * 1e-3) / 1e9 / peak,
+                  "k_mx_matvec_frac": MV_B * kb.ncells / (kb.ms_matvec * 1e-3) / 1e9 / peak,
                   "update_ms": kb.ms_update,
-                  "update_frac": (24.0 * kb.ncells + 12.0 * kb.ncells_poly) /
+                  "update_frac": (UP_B * kb.ncells + UP_POLY_B * kb.ncells_poly) /
                                  (kb.ms_update * 1e-3) / 1e9 / peak,
                   "schedule": sched_b}
         sol.close()

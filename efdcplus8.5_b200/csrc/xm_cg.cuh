@@ -646,9 +646,21 @@ __device__ __forceinline__ double matvec_row_z(const RowGeo &g, bool valid,
   return a.x * p.x + a.y * p.y + a.z * p.z + a.w * p.w;
 }
 
+// MIXED inner iteration: x += alpha*p of the previous iteration, which the
+// next matrix-vector pass applies (its p_old is that p, already loaded), so
+// that the update pass reads neither x nor p; the last iteration's term is
+// applied with the correction (k_mx_apply).  The same fmaf on the same
+// values as in the update pass, hence the same x.
+__device__ __forceinline__ V4<float> x_plus_alpha_p(const V4<float> &x, float alpha,
+                                                    const V4<float> &p) {
+  return {fmaf(alpha, p.x, x.x), fmaf(alpha, p.y, x.y), fmaf(alpha, p.z, x.z),
+          fmaf(alpha, p.w, x.w)};
+}
+
 // MIXED inner CG on the Jacobi-scaled system (unit diagonal): p = r + beta*p
 // at the row vector and its halo, Ap = p + AS*pS + AN*pN + AW*pW + AE*pE, and
-// the part of p.Ap.  Symmetric: AN(L) = AS(LN), AE(L) = AW(LE).
+// the part of p.Ap.  Symmetric: AN(L) = AS(LN), AE(L) = AW(LE).  With dox,
+// also the previous iteration's x += alpha*p (x_plus_alpha_p).
 __device__ __forceinline__ double matvec_row_scaled(const RowGeo &g, bool valid,
                                                     const float *__restrict__ r,
                                                     const float *__restrict__ pold,
@@ -657,8 +669,11 @@ __device__ __forceinline__ double matvec_row_scaled(const RowGeo &g, bool valid,
                                                     const float *__restrict__ aw,
                                                     const float *__restrict__ ae,
                                                     const float *__restrict__ an,
-                                                    float *__restrict__ ap, float beta, bool asym) {
+                                                    float *__restrict__ ap, float beta, bool asym,
+                                                    float *__restrict__ x, float alpha_prev,
+                                                    bool dox) {
   const V4<float> r0 = ld4(r + g.d0), o0 = ld4(pold + g.d0);
+  const V4<float> x0 = dox ? ld4(x + g.d0) : V4<float>{0.f, 0.f, 0.f, 0.f};
   const V4<float> rn = ld4(r + g.dn), on = ld4(pold + g.dn);
   const V4<float> rs = ld4(r + g.ds), os = ld4(pold + g.ds);
   const V4<float> p = {fmaf(beta, o0.x, r0.x), fmaf(beta, o0.y, r0.y), fmaf(beta, o0.z, r0.z),
@@ -687,23 +702,23 @@ __device__ __forceinline__ double matvec_row_scaled(const RowGeo &g, bool valid,
   a.z = p.z + ks.z * ps.z + kn.z * pn.z + kw.z * p.y + ke.z * p.w;
   a.w = p.w + ks.w * ps.w + kn.w * pn.w + kw.w * p.z + ke.w * pe;
   if (!valid) return 0.0;
+  if (dox) st4(x + g.d0, x_plus_alpha_p(x0, alpha_prev, o0));
   st4(pnew + g.d0, p);
   st4(ap + g.d0, a);
   return double(a.x) * double(p.x) + double(a.y) * double(p.y) + double(a.z) * double(p.z) +
          double(a.w) * double(p.w);
 }
 
-// MIXED, polynomial-preconditioned: x += alpha*p, r -= alpha*Ap at the cell
+// MIXED, polynomial-preconditioned: r -= alpha*Ap at the cell
 // and (recomputed from r and Ap) at its four neighbours, then
 // z = (2I - Ahat) r = r - N r (N: the couplings AS, AW, AN = AS(LN),
 // AE = AW(LE)) -- the two-term Neumann series of Ahat^-1, symmetric positive
 // definite for a symmetric unit-diagonal Ahat with eigenvalues in (0, 2).
-// With poly == false z = r (Jacobi; unsymmetric operators).  Stores x, the
-// new r (into the other residual buffer: neighbours still read the old r for
-// their own halo) and z; adds r.z and r.r.
+// With poly == false z = r (Jacobi; unsymmetric operators).  Stores the new
+// r (into the other residual buffer: neighbours still read the old r for
+// their own halo) and z; adds r.z and r.r.  (x += alpha*p: the next
+// matrix-vector pass, x_plus_alpha_p.)
 __device__ __forceinline__ void update_row_poly(const RowGeo &g, bool valid,
-                                                float *__restrict__ x,
-                                                const float *__restrict__ pnew,
                                                 const float *__restrict__ r,
                                                 float *__restrict__ rnew,
                                                 const float *__restrict__ ap,
@@ -735,13 +750,6 @@ __device__ __forceinline__ void update_row_poly(const RowGeo &g, bool valid,
     zv.w = rn0.w - (ks.w * nS.w + kn.w * nN.w + kw.w * rn0.z + ke.w * ne);
   }
   if (!valid) return;
-  V4<float> xv = ld4(x + g.d0);
-  const V4<float> pv = ld4(pnew + g.d0);
-  xv.x = fmaf(alpha, pv.x, xv.x);
-  xv.y = fmaf(alpha, pv.y, xv.y);
-  xv.z = fmaf(alpha, pv.z, xv.z);
-  xv.w = fmaf(alpha, pv.w, xv.w);
-  st4(x + g.d0, xv);
   st4(rnew + g.d0, rn0);
   st4(z + g.d0, zv);
   rz += double(rn0.x) * double(zv.x) + double(rn0.y) * double(zv.y) +
@@ -794,9 +802,13 @@ __device__ __forceinline__ double matvec_row_scaled_eager(const RowGeo &g, bool 
                                                     const float *__restrict__ aw,
                                                     const float *__restrict__ ae,
                                                     const float *__restrict__ an,
-                                                    float *__restrict__ ap, float beta, bool asym) {
-  // every load first, so that one round trip serves the row
+                                                    float *__restrict__ ap, float beta, bool asym,
+                                                    float *__restrict__ x, float alpha_prev,
+                                                    bool dox) {
+  // every load first, so that one round trip serves the row (x is read at
+  // the ghost tile's inert slots too when the row is not valid)
   const V4<float> r0 = ld4(r + g.d0), o0 = ld4(pold + g.d0);
+  const V4<float> x0 = dox ? ld4(x + g.d0) : V4<float>{0.f, 0.f, 0.f, 0.f};
   const V4<float> rn = ld4(r + g.dn), on = ld4(pold + g.dn);
   const V4<float> rs = ld4(r + g.ds), os = ld4(pold + g.ds);
   const V4<float> ks = ld4(as + g.d0), kw = ld4(aw + g.d0);
@@ -826,6 +838,7 @@ __device__ __forceinline__ double matvec_row_scaled_eager(const RowGeo &g, bool 
   a.z = p.z + ks.z * ps.z + kn.z * pn.z + kw.z * p.y + ke.z * p.w;
   a.w = p.w + ks.w * ps.w + kn.w * pn.w + kw.w * p.z + ke.w * pe;
   if (!valid) return 0.0;
+  if (dox) st4(x + g.d0, x_plus_alpha_p(x0, alpha_prev, o0));
   st4(pnew + g.d0, p);
   st4(ap + g.d0, a);
   return double(a.x) * double(p.x) + double(a.y) * double(p.y) + double(a.z) * double(p.z) +
@@ -833,8 +846,6 @@ __device__ __forceinline__ double matvec_row_scaled_eager(const RowGeo &g, bool 
 }
 
 __device__ __forceinline__ void update_row_poly_eager(const RowGeo &g, bool valid,
-                                                float *__restrict__ x,
-                                                const float *__restrict__ pnew,
                                                 const float *__restrict__ r,
                                                 float *__restrict__ rnew,
                                                 const float *__restrict__ ap,
@@ -842,11 +853,8 @@ __device__ __forceinline__ void update_row_poly_eager(const RowGeo &g, bool vali
                                                 const float *__restrict__ aw,
                                                 float *__restrict__ z, float alpha, bool poly,
                                                 double &rz, double &rr) {
-  // every load first, so that one round trip serves the row (x and p_new
-  // are read at the ghost tile's inert slots too when the row is not valid)
+  // every load first, so that one round trip serves the row
   const V4<float> r0 = ld4(r + g.d0), a0 = ld4(ap + g.d0);
-  V4<float> xv = ld4(x + g.d0);
-  const V4<float> pv = ld4(pnew + g.d0);
   V4<float> rN{}, aN{}, rS{}, aS{}, ks{}, kw{}, kn{};
   float rw = 0.f, aw_ = 0.f, re = 0.f, ae_ = 0.f, kwe_edge = 0.f;
   const bool west = g.cx == 0, east = g.cx == ROWT - 1;
@@ -888,11 +896,6 @@ __device__ __forceinline__ void update_row_poly_eager(const RowGeo &g, bool vali
     zv.w = rn0.w - (ks.w * nS.w + kn.w * nN.w + kw.w * rn0.z + ke.w * ne);
   }
   if (!valid) return;
-  xv.x = fmaf(alpha, pv.x, xv.x);
-  xv.y = fmaf(alpha, pv.y, xv.y);
-  xv.z = fmaf(alpha, pv.z, xv.z);
-  xv.w = fmaf(alpha, pv.w, xv.w);
-  st4(x + g.d0, xv);
   st4(rnew + g.d0, rn0);
   st4(z + g.d0, zv);
   rz += double(rn0.x) * double(zv.x) + double(rn0.y) * double(zv.y) +
@@ -901,50 +904,22 @@ __device__ __forceinline__ void update_row_poly_eager(const RowGeo &g, bool vali
         double(rn0.z) * double(rn0.z) + double(rn0.w) * double(rn0.w);
 }
 
-// MIXED, Jacobi: x += alpha*p, r -= alpha*Ap (into the other residual buffer)
-// and the part of r.r (= r.z on the unit-diagonal system).
-__device__ __forceinline__ void update_row_jac(const RowGeo &g, bool valid, float *__restrict__ x,
-                                               const float *__restrict__ pnew,
+// MIXED, Jacobi: r -= alpha*Ap (into the other residual buffer) and the part
+// of r.r (= r.z on the unit-diagonal system).  (x += alpha*p: the next
+// matrix-vector pass, x_plus_alpha_p.)
+__device__ __forceinline__ void update_row_jac(const RowGeo &g, bool valid,
                                                const float *__restrict__ r,
                                                float *__restrict__ rnew,
                                                const float *__restrict__ ap, float alpha,
                                                double &rr) {
   if (!valid) return;
-  V4<float> xv = ld4(x + g.d0), rv = ld4(r + g.d0);
-  const V4<float> pv = ld4(pnew + g.d0), av = ld4(ap + g.d0);
-  xv.x = fmaf(alpha, pv.x, xv.x);
-  xv.y = fmaf(alpha, pv.y, xv.y);
-  xv.z = fmaf(alpha, pv.z, xv.z);
-  xv.w = fmaf(alpha, pv.w, xv.w);
+  V4<float> rv = ld4(r + g.d0);
+  const V4<float> av = ld4(ap + g.d0);
   rv.x = fmaf(-alpha, av.x, rv.x);
   rv.y = fmaf(-alpha, av.y, rv.y);
   rv.z = fmaf(-alpha, av.z, rv.z);
   rv.w = fmaf(-alpha, av.w, rv.w);
-  st4(x + g.d0, xv);
   st4(rnew + g.d0, rv);
-  rr += double(rv.x) * double(rv.x) + double(rv.y) * double(rv.y) + double(rv.z) * double(rv.z) +
-        double(rv.w) * double(rv.w);
-}
-
-// MIXED: x += alpha*p, r -= alpha*Ap and the part of r.r (= r.z, unit diagonal).
-__device__ __forceinline__ void update_row_scaled(const RowGeo &g, bool valid, float *__restrict__ x,
-                                                  const float *__restrict__ pnew,
-                                                  float *__restrict__ r,
-                                                  const float *__restrict__ ap, float alpha,
-                                                  double &rr) {
-  if (!valid) return;
-  V4<float> xv = ld4(x + g.d0), rv = ld4(r + g.d0);
-  const V4<float> pv = ld4(pnew + g.d0), av = ld4(ap + g.d0);
-  xv.x = fmaf(alpha, pv.x, xv.x);
-  xv.y = fmaf(alpha, pv.y, xv.y);
-  xv.z = fmaf(alpha, pv.z, xv.z);
-  xv.w = fmaf(alpha, pv.w, xv.w);
-  rv.x = fmaf(-alpha, av.x, rv.x);
-  rv.y = fmaf(-alpha, av.y, rv.y);
-  rv.z = fmaf(-alpha, av.z, rv.z);
-  rv.w = fmaf(-alpha, av.w, rv.w);
-  st4(x + g.d0, xv);
-  st4(r + g.d0, rv);
   rr += double(rv.x) * double(rv.x) + double(rv.y) * double(rv.y) + double(rv.z) * double(rv.z) +
         double(rv.w) * double(rv.w);
 }

@@ -32,8 +32,8 @@ template <bool MA, int VAR, bool FOLD>
 __global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_matvec(DevStatic S, DevSystem Y, Ctl *ctl,
                                                     double *part) {
   struct A {
-    bool skip, asym;
-    float beta;
+    bool skip, asym, dox;
+    float beta, alpha;
     const float *pold;
     float *pnew;
     const float *z;
@@ -45,16 +45,19 @@ __global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_matvec(DevStatic S, Dev
         const bool par = k.parity;
         const bool asym = unsym<MA>(k);
         const bool poly = Y.mpoly[m] && !asym;
-        return A{(k.done | k.idone) != 0, asym, float(k.beta), par ? Y.pb32 : Y.pa32,
-                 par ? Y.pa32 : Y.pb32, poly ? Y.z32 : (par ? Y.r32b : Y.r32)};
+        // after the pass's first iteration: the previous x += alpha*p, with
+        // p_old that p and alpha still the previous ALPHA
+        return A{(k.done | k.idone) != 0, asym, k.inner_iter > 0, float(k.beta),
+                 float(k.alpha), par ? Y.pb32 : Y.pa32, par ? Y.pa32 : Y.pb32,
+                 poly ? Y.z32 : (par ? Y.r32b : Y.r32)};
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         if constexpr (VAR == 3)
           v[0] = matvec_row_scaled_eager(g, valid, a.z, a.pold, a.pnew, Y.as32, Y.aw32, Y.ae32,
-                                         Y.an32, Y.ap32, a.beta, a.asym);
+                                         Y.an32, Y.ap32, a.beta, a.asym, Y.x32, a.alpha, a.dox);
         else
           v[0] = matvec_row_scaled(g, valid, a.z, a.pold, a.pnew, Y.as32, Y.aw32, Y.ae32,
-                                   Y.an32, Y.ap32, a.beta, a.asym);
+                                   Y.an32, Y.ap32, a.beta, a.asym, Y.x32, a.alpha, a.dox);
       },
       fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0) cg_matvec_epi(ctl[m], sum[0]);
@@ -69,15 +72,15 @@ __global__ void __launch_bounds__(NT) k_red_mx_matvec(DevStatic S, Ctl *ctl, con
       });
 }
 
-// x += alpha*p, r -= alpha*Ap, z = (2I - Ahat) r (the two-term Neumann
-// polynomial), r.z and r.r (FP64 sums): the members that use it.
+// r -= alpha*Ap, z = (2I - Ahat) r (the two-term Neumann polynomial), r.z
+// and r.r (FP64 sums): the members that use it.  x += alpha*p is the next
+// matrix-vector kernel's (or, after the last iteration, k_mx_apply's).
 template <int VAR, bool FOLD>
 __global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_update_poly(DevStatic S, DevSystem Y,
                                                          Ctl *ctl, double *part, RedArgs ra) {
   struct A {
     bool skip;
     float alpha;
-    const float *pnew;
     const float *r;
     float *rnew;
   };
@@ -87,30 +90,29 @@ __global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_update_poly(DevStatic S
         const Ctl &k = ctl[m];
         const bool par = k.parity;
         const bool poly = Y.mpoly[m] && !unsym<true>(k);
-        return A{(k.done | k.idone) != 0 || !poly, float(k.alpha), par ? Y.pa32 : Y.pb32,
-                 par ? Y.r32b : Y.r32, par ? Y.r32 : Y.r32b};
+        return A{(k.done | k.idone) != 0 || !poly, float(k.alpha), par ? Y.r32b : Y.r32,
+                 par ? Y.r32 : Y.r32b};
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         if constexpr (VAR == 3)
-          update_row_poly_eager(g, valid, Y.x32, a.pnew, a.r, a.rnew, Y.ap32, Y.as32, Y.aw32,
-                                Y.z32, a.alpha, true, v[0], v[1]);
+          update_row_poly_eager(g, valid, a.r, a.rnew, Y.ap32, Y.as32, Y.aw32, Y.z32, a.alpha,
+                                true, v[0], v[1]);
         else
-          update_row_poly(g, valid, Y.x32, a.pnew, a.r, a.rnew, Y.ap32, Y.as32, Y.aw32, Y.z32,
-                          a.alpha, true, v[0], v[1]);
+          update_row_poly(g, valid, a.r, a.rnew, Y.ap32, Y.as32, Y.aw32, Y.z32, a.alpha, true,
+                          v[0], v[1]);
       },
       fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0)
           mx_update_epi(ctl[m], ra.glob, S.sc[m].iterm, sum[0], sum[1], 2.0, ra.no_stop);
       }));
 }
-// The same for the Jacobi members (z = r): x, r and r.r only.
+// The same for the Jacobi members (z = r): r and r.r only.
 template <int VAR, bool FOLD>
 __global__ void __launch_bounds__(NT) k_mx_update_jac(DevStatic S, DevSystem Y, Ctl *ctl,
                                                      double *part, RedArgs ra) {
   struct A {
     bool skip;
     float alpha;
-    const float *pnew;
     const float *r;
     float *rnew;
   };
@@ -120,12 +122,12 @@ __global__ void __launch_bounds__(NT) k_mx_update_jac(DevStatic S, DevSystem Y, 
         const Ctl &k = ctl[m];
         const bool par = k.parity;
         const bool poly = Y.mpoly[m] && !unsym<true>(k);
-        return A{(k.done | k.idone) != 0 || poly, float(k.alpha), par ? Y.pa32 : Y.pb32,
-                 par ? Y.r32b : Y.r32, par ? Y.r32 : Y.r32b};
+        return A{(k.done | k.idone) != 0 || poly, float(k.alpha), par ? Y.r32b : Y.r32,
+                 par ? Y.r32 : Y.r32b};
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         double rr = 0.0;
-        update_row_jac(g, valid, Y.x32, a.pnew, a.r, a.rnew, Y.ap32, a.alpha, rr);
+        update_row_jac(g, valid, a.r, a.rnew, Y.ap32, a.alpha, rr);
         v[0] = rr;
         v[1] = rr;
       },
@@ -195,15 +197,15 @@ struct Halo {
 
 constexpr int MV_STAGES = 3, POLY_STAGES = 2, JAC_STAGES = 2;
 using MvStage = Stage<4>;    // z, p_old, AS, AW
-using PolyStage = Stage<6>;  // r, Ap, AS, AW, x, p
-using JacStage = Stage<4>;   // x, p, r, Ap
+using PolyStage = Stage<4>;  // r, Ap, AS, AW
+using JacStage = Stage<2>;   // r, Ap
 
 template <bool MA, bool FOLD>
 __global__ void __launch_bounds__(NT, 3) k_mx_matvec_st(DevStatic S, DevSystem Y, Ctl *ctl,
                                                        double *part) {
   struct A {
-    bool skip, asym;
-    float beta;
+    bool skip, asym, dox;
+    float beta, alpha;
     float *pnew;
     const float *b[4];
   };
@@ -215,8 +217,8 @@ __global__ void __launch_bounds__(NT, 3) k_mx_matvec_st(DevStatic S, DevSystem Y
         const bool asym = unsym<MA>(k);
         const bool poly = Y.mpoly[m] && !asym;
         const float *z = poly ? Y.z32 : (par ? Y.r32b : Y.r32);
-        return A{(k.done | k.idone) != 0, asym, float(k.beta), par ? Y.pa32 : Y.pb32,
-                 {z, par ? Y.pb32 : Y.pa32, Y.as32, Y.aw32}};
+        return A{(k.done | k.idone) != 0, asym, k.inner_iter > 0, float(k.beta), float(k.alpha),
+                 par ? Y.pa32 : Y.pb32, {z, par ? Y.pb32 : Y.pa32, Y.as32, Y.aw32}};
       },
       [&](const A &a, const RowGeo &g, const StageRow &row) {
         Halo h{};
@@ -271,6 +273,7 @@ __global__ void __launch_bounds__(NT, 3) k_mx_matvec_st(DevStatic S, DevSystem Y
         ap.z = p.z + ks.z * ps.z + kn.z * pn.z + kw.z * p.y + ke.z * p.w;
         ap.w = p.w + ks.w * ps.w + kn.w * pn.w + kw.w * p.z + ke.w * pe;
         if (!valid) return;
+        if (a.dox) st4(Y.x32 + g.d0, x_plus_alpha_p(ld4(Y.x32 + g.d0), a.alpha, o0));
         st4(a.pnew + g.d0, p);
         st4(Y.ap32 + g.d0, ap);
         v[0] = double(ap.x) * double(p.x) + double(ap.y) * double(p.y) +
@@ -288,16 +291,16 @@ __global__ void __launch_bounds__(NT, 3) k_mx_update_poly_st(DevStatic S, DevSys
     bool skip;
     float alpha;
     float *rnew;
-    const float *b[6];
+    const float *b[4];
   };
-  quad_sweep_staged<2, 6, POLY_STAGES>(
+  quad_sweep_staged<2, 4, POLY_STAGES>(
       S, part, Y.err,
       [&](int m) {
         const Ctl &k = ctl[m];
         const bool par = k.parity;
         const bool poly = Y.mpoly[m] && !unsym<true>(k);
         return A{(k.done | k.idone) != 0 || !poly, float(k.alpha), par ? Y.r32 : Y.r32b,
-                 {par ? Y.r32b : Y.r32, Y.ap32, Y.as32, Y.aw32, Y.x32, par ? Y.pa32 : Y.pb32}};
+                 {par ? Y.r32b : Y.r32, Y.ap32, Y.as32, Y.aw32}};
       },
       [&](const A &a, const RowGeo &g, const StageRow &row) {
         Halo h{};
@@ -346,13 +349,6 @@ __global__ void __launch_bounds__(NT, 3) k_mx_update_poly_st(DevStatic S, DevSys
         zv.z = rn0.z - (ks.z * nS.z + kn.z * nN.z + kw.z * rn0.y + ke.z * rn0.w);
         zv.w = rn0.w - (ks.w * nS.w + kn.w * nN.w + kw.w * rn0.z + ke.w * ne);
         if (!valid) return;
-        V4<float> xv = st_body(st, 4, row);
-        const V4<float> pv = st_body(st, 5, row);
-        xv.x = fmaf(alpha, pv.x, xv.x);
-        xv.y = fmaf(alpha, pv.y, xv.y);
-        xv.z = fmaf(alpha, pv.z, xv.z);
-        xv.w = fmaf(alpha, pv.w, xv.w);
-        st4(Y.x32 + g.d0, xv);
         st4(a.rnew + g.d0, rn0);
         st4(Y.z32 + g.d0, zv);
         v[0] = double(rn0.x) * double(zv.x) + double(rn0.y) * double(zv.y) +
@@ -373,33 +369,28 @@ __global__ void __launch_bounds__(NT, 4) k_mx_update_jac_st(DevStatic S, DevSyst
     bool skip;
     float alpha;
     float *rnew;
-    const float *b[4];
+    const float *b[2];
   };
-  quad_sweep_staged<2, 4, JAC_STAGES>(
+  quad_sweep_staged<2, 2, JAC_STAGES>(
       S, part, Y.err,
       [&](int m) {
         const Ctl &k = ctl[m];
         const bool par = k.parity;
         const bool poly = Y.mpoly[m] && !unsym<true>(k);
         return A{(k.done | k.idone) != 0 || poly, float(k.alpha), par ? Y.r32 : Y.r32b,
-                 {Y.x32, par ? Y.pa32 : Y.pb32, par ? Y.r32b : Y.r32, Y.ap32}};
+                 {par ? Y.r32b : Y.r32, Y.ap32}};
       },
       [&](const A &, const RowGeo &, const StageRow &) { return 0; },
       [&](const A &a, const JacStage &st, const StageRow &row, const RowGeo &g, bool valid,
           int, double *v) {
         if (!valid) return;
         const float alpha = a.alpha;
-        V4<float> xv = st_body(st, 0, row), rv = st_body(st, 2, row);
-        const V4<float> pv = st_body(st, 1, row), av = st_body(st, 3, row);
-        xv.x = fmaf(alpha, pv.x, xv.x);
-        xv.y = fmaf(alpha, pv.y, xv.y);
-        xv.z = fmaf(alpha, pv.z, xv.z);
-        xv.w = fmaf(alpha, pv.w, xv.w);
+        V4<float> rv = st_body(st, 0, row);
+        const V4<float> av = st_body(st, 1, row);
         rv.x = fmaf(-alpha, av.x, rv.x);
         rv.y = fmaf(-alpha, av.y, rv.y);
         rv.z = fmaf(-alpha, av.z, rv.z);
         rv.w = fmaf(-alpha, av.w, rv.w);
-        st4(Y.x32 + g.d0, xv);
         st4(a.rnew + g.d0, rv);
         const double rr = double(rv.x) * double(rv.x) + double(rv.y) * double(rv.y) +
                           double(rv.z) * double(rv.z) + double(rv.w) * double(rv.w);

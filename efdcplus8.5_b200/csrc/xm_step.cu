@@ -160,11 +160,11 @@ __device__ __forceinline__ double assemble_cell(const DevStatic &S, const DevSta
 // when every member steps (COPY = false: the *1 buffers hold the entry
 // values), or per-cell copies here (COPY = true: the entry values are in
 // UHDYE, VHDXE, HP), which lets a subset of the members step (act).
-// BARO: a member of the batch has baroclinic terms; the instance without them
-// is held to 32 registers (8 CTAs per SM), which sizes the grid of every cell
-// kernel (occupancy_blocks_per_sm).
+// BARO: a member of the batch has baroclinic terms.  Each instance runs on a
+// grid of its own occupancy (cell_grid).
+constexpr int BEGIN_CTAS = 6;  // CTAs per SM the instance without BARO is held to (40 registers, no spills)
 template <bool BARO, bool COPY>
-__global__ void __launch_bounds__(NT, BARO ? 4 : 8) k_begin(DevStatic S, DevState X, int ntile,
+__global__ void __launch_bounds__(NT, BARO ? 4 : BEGIN_CTAS) k_begin(DevStatic S, DevState X, int ntile,
                                                            const int *act) {
 #define UE (COPY ? X.uhdye : X.uhdy1e)
 #define VE (COPY ? X.vhdxe : X.vhdx1e)
@@ -983,10 +983,15 @@ __global__ void __launch_bounds__(NT) k_mx_apply(DevStatic S, SysView V, DevSyst
                                                 const Ctl *ctl) {
   quad_apply(
       S, [&](int m) { return ctl[m].done || !ctl[m].idone; },
-      [&](int, const RowGeo &g) {
+      [&](int m, const RowGeo &g) {
+        const Ctl &k = ctl[m];
         V4<double> x = ld4(P + g.d0);
         const V4<double> c = ld4(V.cc + g.d0);
-        const V4<float> d = ld4(Y.x32 + g.d0);
+        // the inner solution with its last iteration's alpha*p (which the
+        // matrix-vector pass of a next iteration would have added)
+        V4<float> d = ld4(Y.x32 + g.d0);
+        if (k.inner_iter > 0)
+          d = x_plus_alpha_p(d, float(k.alpha), ld4((k.parity ? Y.pa32 : Y.pb32) + g.d0));
         x.x = x.x + double(d.x) * inv_sqrt_diag(c.x);
         x.y = x.y + double(d.y) * inv_sqrt_diag(c.y);
         x.z = x.z + double(d.z) * inv_sqrt_diag(c.z);
@@ -1431,6 +1436,14 @@ void launch_put_int(cudaStream_t st, const int *idx, const int *val, int n, int 
   count_launches(1);
 }
 
+static int blocks_per_sm(const void *kernel);
+// The grid of a cell kernel whose resident CTAs per SM differ from the
+// others': its own occupancy times the SMs, at most one CTA per tile.
+template <class K>
+static int cell_grid(const Launch &l, K kernel) {
+  const int per_sm = blocks_per_sm(reinterpret_cast<const void *>(kernel));
+  return std::max(1, std::min(l.ntile - 1, l.nsm * per_sm));
+}
 void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const int *act,
                   bool copy) {
   if (l.baro) {
@@ -1438,22 +1451,26 @@ void launch_begin(const Launch &l, const DevStatic &S, const DevState &X, const 
     count_launches(1);
   }
   if (l.baro && copy)
-    k_begin<true, true><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
+    k_begin<true, true><<<cell_grid(l, k_begin<true, true>), NT, 0, l.stream>>>(S, X, l.ntile,
+                                                                              act);
   else if (l.baro)
-    k_begin<true, false><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
+    k_begin<true, false><<<cell_grid(l, k_begin<true, false>), NT, 0, l.stream>>>(S, X, l.ntile,
+                                                                                act);
   else if (copy)
-    k_begin<false, true><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
+    k_begin<false, true><<<cell_grid(l, k_begin<false, true>), NT, 0, l.stream>>>(S, X, l.ntile,
+                                                                                act);
   else
-    k_begin<false, false><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
+    k_begin<false, false><<<cell_grid(l, k_begin<false, false>), NT, 0, l.stream>>>(
+        S, X, l.ntile, act);
   count_launches(1);
 }
 void launch_begin3(const Launch &l, const DevStatic &S, const DevState &X, const int *act) {
   if (l.baro) {
     k_calebi<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);  // calpuv9c.f90:145
     count_launches(1);
-    k_begin3<true><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+    k_begin3<true><<<cell_grid(l, k_begin3<true>), NT, 0, l.stream>>>(S, X, l.ntile);
   } else {
-    k_begin3<false><<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile);
+    k_begin3<false><<<cell_grid(l, k_begin3<false>), NT, 0, l.stream>>>(S, X, l.ntile);
   }
   count_launches(1);
 }
@@ -1464,14 +1481,6 @@ void launch_advance3(const Launch &l, const DevStatic &S, const DevState &X) {
 void launch_sweep_reset(const Launch &l, Ctl *ctl, const int *act, int nmember) {
   k_sweep_reset<<<(nmember + 255) / 256, 256, 0, l.stream>>>(ctl, act, nmember);
   count_launches(1);
-}
-static int blocks_per_sm(const void *kernel);
-// The grid of a cell kernel whose resident CTAs per SM differ from the
-// others': its own occupancy times the SMs, at most one CTA per tile.
-template <class K>
-static int cell_grid(const Launch &l, K kernel) {
-  const int per_sm = blocks_per_sm(reinterpret_cast<const void *>(kernel));
-  return std::max(1, std::min(l.ntile - 1, l.nsm * per_sm));
 }
 void launch_assemble(const Launch &l, const DevStatic &S, const DevState &X, Ctl *ctl,
                      const int *act) {
@@ -1687,7 +1696,7 @@ void launch_mx_apply(const Launch &l, const DevStatic &S, const SysView &V, cons
   count_launches(1);
 }
 void launch_backsub(const Launch &l, const DevStatic &S, const DevState &X, const int *act) {
-  k_backsub<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
+  k_backsub<<<cell_grid(l, k_backsub), NT, 0, l.stream>>>(S, X, l.ntile, act);
   count_launches(1);
   k_continuity<<<l.grid, NT, 0, l.stream>>>(S, X, l.ntile, act);
   count_launches(1);
@@ -1858,7 +1867,7 @@ void launch_bed(cudaStream_t st, const DevStatic &S, const DevBed &Bd, const dou
 
 void launch_tbxy(const Launch &l, const DevStatic &S, const DevState &X, const DevBed &Bd,
                  const DragScalars *ds) {
-  k_tbxy<<<l.grid, NT, 0, l.stream>>>(S, X, Bd, ds, l.ntile);
+  k_tbxy<<<cell_grid(l, k_tbxy), NT, 0, l.stream>>>(S, X, Bd, ds, l.ntile);
   count_launches(1);
 }
 
@@ -1903,12 +1912,12 @@ void launch_sys_prepare(const Launch &l, const DevStatic &S, const DevSystem &Y,
   }
 }
 
-int occupancy_blocks_per_sm() {  // k_assemble holds more values: its own grid (cell_grid)
-  int b = 0, c = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_begin<false, false>, NT, 0);
+// the CTAs per SM of the grid-stride cell kernels (k_begin and k_assemble hold
+// more values and run on grids of their own, cell_grid)
+int occupancy_blocks_per_sm() {
+  int c = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_fin, NT, 0);
-  const int m = std::min(b, c);
-  return m > 0 ? m : 1;
+  return c > 0 ? c : 1;
 }
 
 int occupancy_blocks_per_sm_cg() {
