@@ -27,9 +27,15 @@ namespace xm {
 // Ahat*p, p.Ap (per member).
 // CTAs per SM the launch bounds ask for, by variant (3 holds more values live)
 constexpr int mx_ctas(int var) { return var == 1 ? 5 : var == 3 ? 4 : 6; }
+// variant 3's matrix-vector and update kernels (measured on the 256-member
+// ensemble: 3 for the first, no spills at 72 registers, is even; 5 for the
+// second spills and is 3 % slower)
+constexpr int MV3_CTAS = 4, UP3_CTAS = 4;
+constexpr int mv_ctas(int var) { return var == 3 ? MV3_CTAS : mx_ctas(var); }
+constexpr int up_ctas(int var) { return var == 3 ? UP3_CTAS : mx_ctas(var); }
 
 template <bool MA, int VAR, bool FOLD>
-__global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_matvec(DevStatic S, DevSystem Y, Ctl *ctl,
+__global__ void __launch_bounds__(NT, mv_ctas(VAR)) k_mx_matvec(DevStatic S, DevSystem Y, Ctl *ctl,
                                                     double *part) {
   struct A {
     bool skip, asym, dox;
@@ -76,7 +82,7 @@ __global__ void __launch_bounds__(NT) k_red_mx_matvec(DevStatic S, Ctl *ctl, con
 // and r.r (FP64 sums): the members that use it.  x += alpha*p is the next
 // matrix-vector kernel's (or, after the last iteration, k_mx_apply's).
 template <int VAR, bool FOLD>
-__global__ void __launch_bounds__(NT, mx_ctas(VAR)) k_mx_update_poly(DevStatic S, DevSystem Y,
+__global__ void __launch_bounds__(NT, up_ctas(VAR)) k_mx_update_poly(DevStatic S, DevSystem Y,
                                                          Ctl *ctl, double *part, RedArgs ra) {
   struct A {
     bool skip;
