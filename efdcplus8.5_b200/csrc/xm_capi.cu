@@ -697,6 +697,8 @@ int solve_fp64(efdc_xm_ctx *c, double *P) {
     if (c->glob_h->ndone >= c->M || launched >= cap) break;
     chunk = 4;
   }
+  xm::launch_cg_finish(l, c->S, c->Y, P, c->ctl);  // the last iteration's P += alpha*p
+  CK(cudaGetLastError());
   int rc = read_ctl(c);
   if (rc) return rc;
   for (int m = 0; m < c->M; ++m) {
@@ -1944,7 +1946,10 @@ cudaError_t capture_solve(efdc_xm_ctx *c, const StepPlan &pl, int d, StepGraph &
     xm::launch_loop_next(lb.stream, c->glob, xm::LOOP_CG, h, (pl.max_iterm + K - 1) / K + 1, 0,
                          M);
     take_count(mark, &sg.n_body[xm::LOOP_CG]);
-    return end_body(lb.stream);
+    CKG(end_body(lb.stream));
+    xm::launch_cg_finish(l, c->S, c->Y, P, c->ctl);  // the last iteration's P += alpha*p
+    take_count(mark, mine);
+    return cudaGetLastError();
   }
   xm::launch_solve_reset(l, c->ctl, c->glob, c->act, M);
   xm::launch_chan_p0(l, c->S, c->mxview, P, c->act);
@@ -4066,9 +4071,9 @@ int32_t efdc_xm_time_kernels(efdc_xm_ctx *c, int32_t precision, int32_t reps, ef
       if (k >= 0) cudaEventRecord(ev[2 * k + 1], c->stream);
       xm::launch_mx_update(l, c->S, c->Y, c->ctl, c->glob, c->part, 1);
     } else {
-      xm::launch_cg_matvec(l, c->S, c->Y, c->ctl, c->part);
+      xm::launch_cg_matvec(l, c->S, c->Y, c->ptmp, c->ctl, c->part);
       if (k >= 0) cudaEventRecord(ev[2 * k + 1], c->stream);
-      xm::launch_cg_update(l, c->S, c->Y, c->ptmp, c->ctl, c->glob, c->part, 1);
+      xm::launch_cg_update(l, c->S, c->Y, c->ctl, c->glob, c->part, 1);
     }
     if (k >= 0) cudaEventRecord(ev[2 * k + 2], c->stream);
   };

@@ -603,7 +603,10 @@ __device__ __forceinline__ double matvec_row(const RowGeo &g, bool valid, const 
 
 // FP64: as matvec_row, with z = CCCI*r stored by the kernels that write r, so
 // that the halo rows need z and p_old only: p = z + beta*p_old has the same
-// roundings as CCCI*r + beta*p_old formed in place.
+// roundings as CCCI*r + beta*p_old formed in place.  With x and dox, also the
+// previous iteration's x += alpha*p_old, the statement the update pass would
+// have run (same operands, same rounding): that pass then reads neither x nor
+// p, and the last iteration's term is applied after the loop (k_cg_finish).
 __device__ __forceinline__ double matvec_row_z(const RowGeo &g, bool valid,
                                                const double *__restrict__ z,
                                                const double *__restrict__ ccc,
@@ -613,8 +616,11 @@ __device__ __forceinline__ double matvec_row_z(const RowGeo &g, bool valid,
                                                const double *__restrict__ ccw,
                                                const double *__restrict__ cce,
                                                const double *__restrict__ ccn,
-                                               double *__restrict__ ap, double beta, bool asym) {
+                                               double *__restrict__ ap, double beta, bool asym,
+                                               double *__restrict__ x = nullptr,
+                                               double alpha_prev = 0., bool dox = false) {
   const V4<double> z0 = ld4(z + g.d0), o0 = ld4(pold + g.d0);
+  const V4<double> x0 = (x && dox) ? ld4(x + g.d0) : V4<double>{0., 0., 0., 0.};
   const V4<double> zn = ld4(z + g.dn), on = ld4(pold + g.dn);
   const V4<double> zs = ld4(z + g.ds), os = ld4(pold + g.ds);
   auto pc = [&](double zz, double po) { return zz + beta * po; };
@@ -641,6 +647,9 @@ __device__ __forceinline__ double matvec_row_z(const RowGeo &g, bool valid,
   a.z = c0.z * p.z + ks.z * ps.z + kn.z * pn.z + kw.z * p.y + ke.z * p.w;
   a.w = c0.w * p.w + ks.w * ps.w + kn.w * pn.w + kw.w * p.z + ke.w * pe;
   if (!valid) return 0.0;
+  if (x && dox)  // the previous iteration's X = X + ALPHA*PCG (congrad.f90:133)
+    st4(x + g.d0, V4<double>{x0.x + alpha_prev * o0.x, x0.y + alpha_prev * o0.y,
+                             x0.z + alpha_prev * o0.z, x0.w + alpha_prev * o0.w});
   st4(pnew + g.d0, p);
   st4(ap + g.d0, a);
   return a.x * p.x + a.y * p.y + a.z * p.z + a.w * p.w;
@@ -933,17 +942,21 @@ __device__ __forceinline__ void update_row(const RowGeo &g, bool valid, T *__res
                                            T alpha, double &rz, double &rr,
                                            T *__restrict__ zout = nullptr) {
   if (!valid) return;
-  V4<T> xv = ld4(x + g.d0), rv = ld4(r + g.d0);
-  const V4<T> pv = ld4(pnew + g.d0), av = ld4(ap + g.d0), cv = ld4(ccc + g.d0);
-  xv.x = xv.x + alpha * pv.x;
-  xv.y = xv.y + alpha * pv.y;
-  xv.z = xv.z + alpha * pv.z;
-  xv.w = xv.w + alpha * pv.w;
+  V4<T> rv = ld4(r + g.d0);
+  const V4<T> av = ld4(ap + g.d0), cv = ld4(ccc + g.d0);
+  if (x) {  // (nullptr: the next matrix-vector pass adds alpha*p, matvec_row_z)
+    V4<T> xv = ld4(x + g.d0);
+    const V4<T> pv = ld4(pnew + g.d0);
+    xv.x = xv.x + alpha * pv.x;
+    xv.y = xv.y + alpha * pv.y;
+    xv.z = xv.z + alpha * pv.z;
+    xv.w = xv.w + alpha * pv.w;
+    st4(x + g.d0, xv);
+  }
   rv.x = rv.x - alpha * av.x;
   rv.y = rv.y - alpha * av.y;
   rv.z = rv.z - alpha * av.z;
   rv.w = rv.w - alpha * av.w;
-  st4(x + g.d0, xv);
   st4(r + g.d0, rv);
   const T z0 = rcpT(cv.x) * rv.x, z1 = rcpT(cv.y) * rv.y, z2 = rcpT(cv.z) * rv.z,
           z3 = rcpT(cv.w) * rv.w;

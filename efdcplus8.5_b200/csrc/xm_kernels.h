@@ -99,10 +99,14 @@ void launch_cg_init(const Launch &l, const DevStatic &S, const DevSystem &Y, dou
                     Glob *glob, double *part);
 void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                     Glob *glob, double *part);
-void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
-                      double *part);
-void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
+void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
+                      Ctl *ctl, double *part);
+void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       Glob *glob, double *part, int no_stop);
+// after the FP64 CG loop: the last iteration's P += alpha*p of every member
+// that iterated (each matrix-vector kernel adds the previous iteration's)
+void launch_cg_finish(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
+                      const Ctl *ctl);
 void launch_mx_resid(const Launch &l, const DevStatic &S, const SysView &V, const DevSystem &Y,
                      const double *P, Ctl *ctl, Glob *glob, double *part, double rsqm_fac,
                      double rel_tol, int no_stop);

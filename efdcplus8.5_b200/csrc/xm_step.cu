@@ -635,13 +635,15 @@ __global__ void __launch_bounds__(NT) k_red_cg_init(DevStatic S, Ctl *ctl, Glob 
       });
 }
 
-// :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA).
+// :93-125 (p update from the previous iteration, A*p, p.Ap, ALPHA), and the
+// previous iteration's X = X + ALPHA*PCG (:133), which needs no other load
+// here than X itself (p_old is that PCG, ALPHA still the previous one).
 template <bool MA, bool FOLD>
-__global__ void __launch_bounds__(NT, MA ? 2 : 3) k_cg_matvec(DevStatic S, DevSystem Y, Ctl *ctl,
-                                                    double *part) {
+__global__ void __launch_bounds__(NT, MA ? 2 : 3) k_cg_matvec(DevStatic S, DevSystem Y, double *P,
+                                                    Ctl *ctl, double *part) {
   struct A {
-    bool skip, asym;
-    double beta;
+    bool skip, asym, dox;
+    double beta, alpha;
     const double *pold;
     double *pnew;
   };
@@ -650,11 +652,12 @@ __global__ void __launch_bounds__(NT, MA ? 2 : 3) k_cg_matvec(DevStatic S, DevSy
       [&](int m) {
         const Ctl &k = ctl[m];
         const bool par = k.parity;
-        return A{k.done != 0, unsym<MA>(k), k.beta, par ? Y.pb : Y.pa, par ? Y.pa : Y.pb};
+        return A{k.done != 0, unsym<MA>(k), k.iter > 0, k.beta, k.alpha, par ? Y.pb : Y.pa,
+                 par ? Y.pa : Y.pb};
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
         v[0] = matvec_row_z(g, valid, Y.z, Y.ccc, a.pold, a.pnew, Y.ccs, Y.ccw, Y.cce, Y.ccn,
-                            Y.ap, a.beta, a.asym);
+                            Y.ap, a.beta, a.asym, P, a.alpha, a.dox);
       },
       fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0) cg_matvec_epi(ctl[m], sum[0]);
@@ -668,24 +671,25 @@ __global__ void __launch_bounds__(NT) k_red_cg_matvec(DevStatic S, Ctl *ctl, con
       });
 }
 
-// :127-149 (P, RCG update, RPCGN, RSQ, BETA) and the stop test :165.  With
+// :134-149 (RCG update, RPCGN, RSQ, BETA) and the stop test :165; the P
+// update of :133 is the next matrix-vector kernel's (or k_cg_finish's).  With
 // no_stop the iteration continues past RSQM and ITERM (kernel timing only).
 template <bool FOLD>
-__global__ void __launch_bounds__(NT, 5) k_cg_update(DevStatic S, DevSystem Y, double *P,
-                                                    Ctl *ctl, double *part, RedArgs ra) {
+__global__ void __launch_bounds__(NT, 5) k_cg_update(DevStatic S, DevSystem Y, Ctl *ctl,
+                                                    double *part, RedArgs ra) {
   struct A {
     bool skip;
     double alpha;
-    const double *pnew;
   };
   quad_sweep<2>(
       S, part,
       [&](int m) {
         const Ctl &k = ctl[m];
-        return A{k.done != 0, k.alpha, k.parity ? Y.pa : Y.pb};
+        return A{k.done != 0, k.alpha};
       },
       [&](const A &a, const RowGeo &g, bool valid, double *v) {
-        update_row<double>(g, valid, P, a.pnew, Y.r, Y.ap, Y.ccc, a.alpha, v[0], v[1], Y.z);
+        update_row<double>(g, valid, nullptr, nullptr, Y.r, Y.ap, Y.ccc, a.alpha, v[0], v[1],
+                           Y.z);
       },
       fold_if<FOLD>(ctl, [&](int m, const double *sum) {
         if (threadIdx.x == 0) cg_update_epi(ctl[m], ra.glob, S.sc[m], sum[0], sum[1], ra.no_stop);
@@ -697,6 +701,25 @@ __global__ void __launch_bounds__(NT) k_red_cg_update(DevStatic S, Ctl *ctl, Glo
       S, part, [&](int m) { return ctl[m].done != 0; },
       [&](int m, const double *sum) {
         if (threadIdx.x == 0) cg_update_epi(ctl[m], glob, S.sc[m], sum[0], sum[1], no_stop);
+      });
+}
+
+// After the CG loop: the last iteration's X = X + ALPHA*PCG (congrad.f90:133)
+// of every member that iterated, which no further matrix-vector kernel adds.
+__global__ void __launch_bounds__(NT) k_cg_finish(DevStatic S, DevSystem Y, double *P,
+                                                 const Ctl *ctl) {
+  quad_apply(
+      S, [&](int m) { return ctl[m].iter == 0; },
+      [&](int m, const RowGeo &g) {
+        const Ctl &k = ctl[m];
+        const double alpha = k.alpha;
+        V4<double> x = ld4(P + g.d0);
+        const V4<double> p = ld4((k.parity ? Y.pa : Y.pb) + g.d0);
+        x.x = x.x + alpha * p.x;
+        x.y = x.y + alpha * p.y;
+        x.z = x.z + alpha * p.z;
+        x.w = x.w + alpha * p.w;
+        st4(P + g.d0, x);
       });
 }
 
@@ -1608,47 +1631,52 @@ void launch_cg_small(const Launch &l, const DevStatic &S, const DevSystem &Y, do
   count_launches(1);
 }
 template <bool F>
-static void cg_matvec_kernel(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
-                             double *part) {
+static void cg_matvec_kernel(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
+                             Ctl *ctl, double *part) {
   if (l.may_asym)
-    k_cg_matvec<true, F><<<quad_grid(l, S, k_cg_matvec<true, F>), NT, 0, l.stream>>>(S, Y, ctl,
+    k_cg_matvec<true, F><<<quad_grid(l, S, k_cg_matvec<true, F>), NT, 0, l.stream>>>(S, Y, P, ctl,
                                                                                     part);
   else
-    k_cg_matvec<false, F><<<quad_grid(l, S, k_cg_matvec<false, F>), NT, 0, l.stream>>>(S, Y, ctl,
-                                                                                      part);
+    k_cg_matvec<false, F><<<quad_grid(l, S, k_cg_matvec<false, F>), NT, 0, l.stream>>>(S, Y, P,
+                                                                                      ctl, part);
   count_launches(1);
 }
-void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
-                      double *part) {
+void launch_cg_matvec(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
+                      Ctl *ctl, double *part) {
   if (l.fold) {
-    cg_matvec_kernel<true>(l, S, Y, ctl, part);
+    cg_matvec_kernel<true>(l, S, Y, P, ctl, part);
     return;
   }
-  cg_matvec_kernel<false>(l, S, Y, ctl, part);
+  cg_matvec_kernel<false>(l, S, Y, P, ctl, part);
   launch_chan_mv64(l, S, Y, ctl, part);
   k_red_cg_matvec<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, part);
   count_launches(1);
 }
-void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
+void launch_cg_update(const Launch &l, const DevStatic &S, const DevSystem &Y, Ctl *ctl,
                       Glob *glob, double *part, int no_stop) {
   RedArgs ra{};
   ra.glob = glob;
   ra.no_stop = no_stop;
   if (l.fold) {
-    k_cg_update<true><<<quad_grid(l, S, k_cg_update<true>), NT, 0, l.stream>>>(S, Y, P, ctl, part,
+    k_cg_update<true><<<quad_grid(l, S, k_cg_update<true>), NT, 0, l.stream>>>(S, Y, ctl, part,
                                                                               ra);
     count_launches(1);
     return;
   }
-  k_cg_update<false><<<quad_grid(l, S, k_cg_update<false>), NT, 0, l.stream>>>(S, Y, P, ctl,
-                                                                              part, ra);
+  k_cg_update<false><<<quad_grid(l, S, k_cg_update<false>), NT, 0, l.stream>>>(S, Y, ctl, part,
+                                                                              ra);
   k_red_cg_update<<<reduce_grid(S), NT, 0, l.stream>>>(S, ctl, glob, part, no_stop);
   count_launches(2);
 }
+void launch_cg_finish(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P,
+                      const Ctl *ctl) {
+  k_cg_finish<<<quad_grid(l, S, k_cg_finish), NT, 0, l.stream>>>(S, Y, P, ctl);
+  count_launches(1);
+}
 void launch_cg_iter(const Launch &l, const DevStatic &S, const DevSystem &Y, double *P, Ctl *ctl,
                     Glob *glob, double *part) {
-  launch_cg_matvec(l, S, Y, ctl, part);
-  launch_cg_update(l, S, Y, P, ctl, glob, part, 0);
+  launch_cg_matvec(l, S, Y, P, ctl, part);
+  launch_cg_update(l, S, Y, ctl, glob, part, 0);
 }
 template <bool F>
 static void mx_resid_kernel(const Launch &l, const DevStatic &S, const SysView &V,
